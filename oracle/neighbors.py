@@ -1,0 +1,168 @@
+"""Neighbour-list oracle (TEST INFRASTRUCTURE ONLY; never the product path).
+
+FP64 numpy restatement of the reference's pure-torch neighbour lists:
+
+* ``wrap_positions``   <- torch_sim/transforms.py:160-210
+  (pbc_wrap_batched_and_get_lattice_shifts)
+* ``cell_repeats``     <- torch_sim/transforms.py:435-467 (get_number_of_cell_repeats)
+* ``neighbor_list``    <- torch_sim/neighbors/torch_nl.py:156-215 (torch_nl_linked_cell)
+  with the strict cutoff of torch_nl.py:25-91 and the shift correction of
+  torch_nl.py:214.  The candidate set is all image shifts in
+  ``[-rep, rep]^3`` per system (rep from ``cell_repeats``), which is exactly the
+  set of images the reference's linked cell replicates (transforms.py:886-899);
+  the pair set is therefore identical (checked against the reference's own
+  output in tests/test_oracle_golden.py).
+* ``full_to_half_list`` <- torch_sim/models/pair_potential.py:86-127
+
+Pair-set convention (torch_nl.py:214, pair_potential.py:182): a triple
+``(i, j, S)`` is a neighbour when ``|r_j - r_i + S @ cell_row| < cutoff``
+for the *unwrapped* positions ``r``; the unshifted self pair ``(i, i, 0)`` is
+excluded unless ``self_interaction``.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+
+def normalize_inputs(cell, pbc, n_systems):
+    """Broadcast cell to [S,3,3] and pbc to [S,3] (neighbors/utils.py:7-34)."""
+    cell = np.asarray(cell, dtype=np.float64)
+    pbc = np.asarray(pbc, dtype=bool)
+    if cell.ndim == 2:
+        cell = (np.broadcast_to(cell, (n_systems, 3, 3)) if cell.shape[0] == 3
+                else cell.reshape(n_systems, 3, 3))
+    if pbc.ndim == 1:
+        pbc = (np.broadcast_to(pbc, (n_systems, 3)) if pbc.shape[0] == 3
+               else pbc.reshape(n_systems, 3))
+    return np.ascontiguousarray(cell), np.ascontiguousarray(pbc)
+
+
+def wrap_positions(positions, cell_row, system_idx, pbc):
+    """Wrap into the primary cell; return (wrapped, integer lattice shifts).
+
+    transforms.py:160-210: ``f = inv(cell_row.T) r``; on periodic axes of systems
+    with an invertible cell and any periodic axis, ``shift = floor(f)`` and
+    ``wrapped = cell_row.T (f - shift)``; other atoms are returned unchanged.
+    """
+    pos = np.asarray(positions, dtype=np.float64)
+    cell_T = np.transpose(cell_row, (0, 2, 1))
+    dets = np.linalg.det(cell_T)
+    invertible = np.isfinite(dets) & (np.abs(dets) > 1e-12)
+    active = pbc.any(axis=1) & invertible
+    if not active.any():
+        return pos.copy(), np.zeros_like(pos)
+    B = np.zeros_like(cell_row)
+    B[active] = np.linalg.inv(cell_T[active])
+    frac = np.einsum("nij,nj->ni", B[system_idx], pos)
+    mask = pbc[system_idx] & active[system_idx][:, None]
+    shifts = np.where(mask, np.floor(frac), 0.0)
+    wrapped = np.einsum("nij,nj->ni", cell_T[system_idx], frac - shifts)
+    act = active[system_idx][:, None]
+    return np.where(act, wrapped, pos), np.where(act, shifts, 0.0)
+
+
+def cell_repeats(cutoff, cell_row, pbc):
+    """ceil(cutoff * |row k of inv(cell)^T|) on periodic axes (transforms.py:435-467)."""
+    has_pbc = pbc.any(axis=1)
+    recip = np.zeros_like(cell_row)
+    if has_pbc.any():
+        recip[has_pbc] = np.transpose(np.linalg.inv(cell_row[has_pbc]), (0, 2, 1))
+    inv_d = np.linalg.norm(recip, axis=-1)
+    rep = np.ceil(cutoff * inv_d).astype(np.int64)
+    return np.where(pbc, rep, 0)
+
+
+def _system_offsets(system_idx, n_systems):
+    counts = np.bincount(system_idx, minlength=n_systems)
+    off = np.zeros(n_systems + 1, dtype=np.int64)
+    off[1:] = np.cumsum(counts)
+    return off
+
+
+def neighbor_list(positions, cell, pbc, cutoff, system_idx, self_interaction=False,
+                  chunk=256):
+    """Full neighbour list (both directions) as in torch_nl.py:156-215.
+
+    Returns ``mapping [2,P] int64, system_mapping [P] int64, shifts [P,3] float64``
+    sorted lexicographically by (system, i, j, shift) so two lists compare with
+    ``np.array_equal``.
+    """
+    system_idx = np.asarray(system_idx, dtype=np.int64)
+    if system_idx.size == 0:
+        return (np.zeros((2, 0), np.int64), np.zeros(0, np.int64), np.zeros((0, 3)))
+    n_systems = int(system_idx.max()) + 1
+    cell_row, pbc = normalize_inputs(cell, pbc, n_systems)
+    wrapped, wshift = wrap_positions(positions, cell_row, system_idx, pbc)
+    rep = cell_repeats(cutoff, cell_row, pbc)
+    off = _system_offsets(system_idx, n_systems)
+    rc2 = cutoff * cutoff
+    out_i, out_j, out_s, out_sys = [], [], [], []
+    for s in range(n_systems):
+        a0, a1 = off[s], off[s + 1]
+        n = a1 - a0
+        if n == 0:
+            continue
+        ax = [np.arange(-r, r + 1) for r in rep[s]]
+        shifts = np.stack(np.meshgrid(*ax, indexing="ij"), -1).reshape(-1, 3)
+        cs = shifts.astype(np.float64) @ cell_row[s]          # [K,3]
+        w = wrapped[a0:a1]
+        for c0 in range(0, n, chunk):
+            c1 = min(n, c0 + chunk)
+            # d = w_i - w_j - S@cell   (torch_nl.py:80-86 / transforms.py:540-566)
+            d = (w[c0:c1, None, None, :] - w[None, :, None, :]
+                 - cs[None, None, :, :])
+            d2 = np.einsum("ijkx,ijkx->ijk", d, d)
+            m = d2 < rc2
+            if not self_interaction:
+                zero = np.all(shifts == 0, axis=1)
+                ii = np.arange(c0, c1)
+                m[ii - c0, ii, :] &= ~zero[None, :]
+            li, lj, lk = np.nonzero(m)
+            out_i.append(li + c0 + a0)
+            out_j.append(lj + a0)
+            out_s.append(shifts[lk])
+            out_sys.append(np.full(li.shape, s, dtype=np.int64))
+    if not out_i:
+        return (np.zeros((2, 0), np.int64), np.zeros(0, np.int64), np.zeros((0, 3)))
+    i = np.concatenate(out_i)
+    j = np.concatenate(out_j)
+    S = np.concatenate(out_s).astype(np.float64)
+    sysm = np.concatenate(out_sys)
+    # shift correction to unwrapped positions (torch_nl.py:214)
+    S = S + wshift[i] - wshift[j]
+    return sort_pairs(np.stack([i, j]), sysm, S)
+
+
+def sort_pairs(mapping, system_mapping, shifts):
+    """Canonical order for set comparison: by (system, i, j, sx, sy, sz)."""
+    mapping = np.asarray(mapping, dtype=np.int64)
+    shifts = np.asarray(shifts, dtype=np.float64)
+    system_mapping = np.asarray(system_mapping, dtype=np.int64)
+    if mapping.shape[1] == 0:
+        return mapping, system_mapping, shifts.reshape(0, 3)
+    si = np.rint(shifts).astype(np.int64)
+    order = np.lexsort((si[:, 2], si[:, 1], si[:, 0], mapping[1], mapping[0],
+                        system_mapping))
+    return mapping[:, order], system_mapping[order], shifts[order]
+
+
+def full_to_half_list(mapping, system_mapping, shifts):
+    """Keep i<j, and for i==j the copy whose first non-zero shift is > 0.
+
+    pair_potential.py:86-127.
+    """
+    i, j = mapping
+    keep = i < j
+    same = i == j
+    if same.any():
+        s = shifts[same]
+        first = np.zeros(len(s))
+        resolved = np.zeros(len(s), dtype=bool)
+        for d in range(3):
+            nz = (s[:, d] != 0) & ~resolved
+            first = np.where(nz, s[:, d], first)
+            resolved |= nz
+        keep = keep.copy()
+        keep[same] = first > 0
+    return mapping[:, keep], system_mapping[keep], shifts[keep]
