@@ -1,0 +1,153 @@
+/*
+ * tsb.h -- C ABI of the B200-native TorchSim classical-potential hot path.
+ *
+ * Every entry point takes raw device pointers, element counts, a caller-owned
+ * device workspace and a CUDA stream (passed as void*), launches asynchronously
+ * on that stream and returns an int status (TSB_OK on a successful launch).
+ * No function allocates or frees device memory, synchronises the device or the
+ * stream, or throws across the ABI.  Buffers are owned by the caller.
+ *
+ * Conventions (TorchSim metal units: Angstrom, eV, amu):
+ *   positions  [n_atoms,3]   dtype TSB_F32 or TSB_F64, unwrapped Cartesian
+ *   cell_row   [n_systems,3,3] row-vector cell (rows are lattice vectors) --
+ *              the neighbour-list/pair-model convention of the reference
+ *              (torch_sim/models/pair_potential.py:154,170)
+ *   pbc        [n_systems,3] uint8 (0/1)
+ *   system_idx [n_atoms] int64, contiguous and non-decreasing (state.py:223-254)
+ *   table      [n_species,n_species,5] float64 rows (p0,p1,p2,rc,eshift):
+ *              LJ:    p0=sigma p1=epsilon
+ *              MORSE: p0=sigma p1=epsilon p2=alpha
+ *              SOFT:  p0=sigma p1=epsilon p2=alpha
+ *              rc = per-pair truncation radius, eshift subtracted inside rc.
+ *   species    [n_atoms] int32 species index (NULL = all species 0)
+ */
+#ifndef TSB_H_
+#define TSB_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define TSB_OK 0
+#define TSB_ERR_INVALID_ARG 1
+#define TSB_ERR_CAPACITY 2     /* output/scratch capacity too small: regrow + retry */
+#define TSB_ERR_NONFINITE 3    /* non-finite input detected on the device          */
+#define TSB_ERR_TIMEOUT 4      /* a bounded device wait gave up                     */
+#define TSB_ERR_CUDA 5         /* a CUDA launch failed                              */
+#define TSB_ERR_UNSUPPORTED 6  /* configuration outside what the kernels handle     */
+#define TSB_ERR_WORKSPACE 7    /* workspace smaller than *_workspace_size()         */
+
+/* ---- dtypes / potentials / flags --------------------------------------- */
+#define TSB_F32 0
+#define TSB_F64 1
+
+#define TSB_POT_LJ 0
+#define TSB_POT_MORSE 1
+#define TSB_POT_SOFT 2
+
+#define TSB_NL_SELF_INTERACTION 1 /* also emit (i, i, 0) pairs                     */
+#define TSB_NL_HALF 2             /* emit each unordered pair once (half list)      */
+
+#define TSB_OUT_FORCES 1
+#define TSB_OUT_STRESS 2
+#define TSB_OUT_ENERGIES 4   /* per-atom energies                                */
+#define TSB_OUT_STRESSES 8   /* per-atom stresses                                */
+#define TSB_MATH_FP64 16     /* FP64 pair arithmetic (default: FP32 pair math,
+                                FP64 displacements and FP64 per-system sums)    */
+
+#define TSB_INT_NVE 0
+#define TSB_INT_LANGEVIN 1
+
+const char *tsb_version(void);
+const char *tsb_status_string(int status);
+
+/* ---- neighbour list ------------------------------------------------------
+ * Replaces torch_sim/neighbors/torch_nl.py:156-215 (torch_nl_linked_cell, the
+ * default backend behind torch_sim/neighbors/__init__.py:46-98 torchsim_nl).
+ * Pair set: every (i, j, S) with |r_j - r_i + S @ cell_row| < cutoff, S integer
+ * and zero on non-periodic axes, excluding (i, i, 0) unless
+ * TSB_NL_SELF_INTERACTION; with TSB_NL_HALF only the copy full_to_half_list
+ * keeps (torch_sim/models/pair_potential.py:86-127).
+ * Outputs: mapping rows at mapping[0..cap) and mapping[mapping_stride..), the
+ * system of each pair, integer shifts (as dtype) valid for the unwrapped
+ * positions, grouped by i in ascending order.  *n_pairs (device int64) gets
+ * the total; when it exceeds `capacity` nothing past capacity is written and
+ * the caller regrows and calls again. */
+size_t tsb_nl_workspace_size(int64_t n_atoms, int64_t n_systems);
+int tsb_nl_build(const void *positions, const void *cell_row, const uint8_t *pbc,
+                 const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
+                 int dtype, double cutoff, int flags, int64_t *mapping,
+                 int64_t mapping_stride, int64_t *system_mapping, void *shifts,
+                 int64_t capacity, int64_t *n_pairs, void *workspace,
+                 size_t workspace_bytes, void *stream);
+
+/* ---- pair potential energy / forces / virial -----------------------------
+ * Replaces PairPotentialModel.forward (torch_sim/models/pair_potential.py:351-464)
+ * for the pair functions of lennard_jones.py:23-47, morse.py:23-47,
+ * soft_sphere.py:35-59 and the species-matrix lookup of soft_sphere.py:90-167.
+ * The neighbour search is fused with the force evaluation (no pair list is
+ * stored).  energy [S], stress [S,3,3], forces [N,3], energies [N],
+ * stresses [N,3,3] are written in `dtype`; outputs not requested by
+ * `out_flags` may be NULL. */
+size_t tsb_pair_workspace_size(int64_t n_atoms, int64_t n_systems);
+int tsb_pair_forward(int potential, const double *table, int n_species,
+                     const int32_t *species, const void *positions,
+                     const void *cell_row, const uint8_t *pbc,
+                     const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
+                     int dtype, double cutoff, int out_flags, void *energy,
+                     void *forces, void *stress, void *energies, void *stresses,
+                     void *workspace, size_t workspace_bytes, void *stream);
+
+/* ---- integrator steps (elementwise, per-system parameters) ---------------
+ * dt_sys, kT_sys, gamma_sys are device float64 arrays of length n_systems.
+ * tsb_md_kick:    p += F * (scale * dt)          (md.py:169-187, momentum_step)
+ * tsb_md_drift:   q += p / m * (scale * dt)      (md.py:190-208, position_step)
+ * tsb_md_baoab_boa: the B(dt/2) A(dt/2) O(dt) A(dt/2) part of nvt_langevin_step
+ *   (torch_sim/integrators/nvt.py:144-240, _ou_step :27-86).  The O-step noise
+ *   is read from `noise` [N,3] when non-NULL, else drawn from a counter-based
+ *   Philox4x32-10 stream keyed by (seed, atom, counter). */
+int tsb_md_kick(void *momenta, const void *forces, const int64_t *system_idx,
+                const double *dt_sys, double scale, int64_t n_atoms, int dtype,
+                void *stream);
+int tsb_md_drift(void *positions, const void *momenta, const void *masses,
+                 const int64_t *system_idx, const double *dt_sys, double scale,
+                 int64_t n_atoms, int dtype, void *stream);
+int tsb_md_baoab_boa(void *positions, void *momenta, const void *forces,
+                     const void *masses, const int64_t *system_idx,
+                     const double *dt_sys, const double *kT_sys,
+                     const double *gamma_sys, const void *noise, uint64_t seed,
+                     uint64_t counter, int64_t n_atoms, int dtype, void *stream);
+
+/* ---- fused persistent batched MD ----------------------------------------
+ * Advances every system by n_steps of velocity Verlet (TSB_INT_NVE,
+ * nve.py:74-130) or BAOAB Langevin (TSB_INT_LANGEVIN, nvt.py:144-240) in one
+ * persistent launch: one CTA owns one system at a time, keeps its atoms and a
+ * Verlet list (cutoff + skin, rebuilt on the device when an atom moved more
+ * than skin/2) in shared memory, and steps it without leaving the kernel.
+ * positions/momenta/forces are float64 [N,3] in/out; energy [S] float64 out
+ * (potential energy after the last step); n_rebuilds [S] int32 out (optional).
+ * `order` [S] int32 (optional) is the order in which CTAs pick systems
+ * (largest first balances the tail).  `status` [2] int32 device out: status[0]
+ * is TSB_OK or TSB_ERR_CAPACITY / TSB_ERR_UNSUPPORTED for a system that did
+ * not fit (that system is left unchanged), status[1] its index.
+ * Requirements: pbc all true, n_atoms per system <= tsb_fused_max_atoms(). */
+int tsb_fused_max_atoms(void);
+size_t tsb_fused_workspace_size(int64_t n_atoms, int64_t n_systems);
+int tsb_fused_md(int integrator, int potential, const double *table, int n_species,
+                 const int32_t *species, double *positions, double *momenta,
+                 double *forces, const double *masses, const double *cell_row,
+                 const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
+                 const int32_t *order, double cutoff, double skin, int64_t n_steps,
+                 const double *dt_sys, const double *kT_sys, const double *gamma_sys,
+                 uint64_t seed, uint64_t counter, double *energy, int32_t *n_rebuilds,
+                 int32_t *status, void *workspace, size_t workspace_bytes,
+                 void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TSB_H_ */

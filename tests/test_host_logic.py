@@ -1,0 +1,72 @@
+"""Host-side logic that needs no GPU: workloads, state mirror, half-list rule."""
+
+import numpy as np
+import torch
+
+from oracle import neighbors as onl
+
+
+def test_copper_batch_shapes_and_sizes():
+    from tsb import workloads
+
+    d = workloads.copper_batch(64, 8, 512, seed=0)
+    counts = np.bincount(d["system_idx"])
+    assert len(counts) == 64 and counts.min() >= 4 and counts.max() <= 512
+    assert np.all(counts % 4 == 0)
+    assert d["cell"].shape == (64, 3, 3)
+    # triclinic: off-diagonal shear present, small strain on the diagonal
+    cr = np.transpose(d["cell"], (0, 2, 1))
+    assert np.abs(cr[:, 0, 1]).max() > 0
+
+
+def test_nearest_fcc_shape():
+    from tsb import workloads
+
+    for t in (8, 32, 100, 256, 500, 512):
+        n1, n2, n3 = workloads.nearest_fcc_shape(t)
+        assert abs(4 * n1 * n2 * n3 - t) <= max(4, 0.2 * t)
+
+
+def test_kob_andersen_density_and_ratio():
+    from tsb import workloads
+
+    d = workloads.kob_andersen_batch(8, 64, 1000, seed=1)
+    for s in range(8):
+        sel = d["system_idx"] == s
+        n = sel.sum()
+        L = d["cell"][s, 0, 0]
+        assert abs(n / L ** 3 - 1.2 / 3.4 ** 3) < 1e-9
+        assert abs((d["atomic_numbers"][sel] == 2).sum() - round(0.2 * n)) == 0
+
+
+def test_state_mirror_properties():
+    from tsb.state import MDState, SimState
+
+    st = SimState(positions=torch.zeros((4, 3)), masses=torch.ones(4),
+                  cell=torch.eye(3) * 5, pbc=True, atomic_numbers=torch.ones(4, dtype=int),
+                  system_idx=torch.tensor([0, 0, 1, 1]))
+    assert st.cell.shape == (1, 3, 3) and st.pbc.tolist() == [True] * 3
+    md = MDState.from_state(st, momenta=torch.ones((4, 3)), energy=torch.zeros(1),
+                            forces=torch.zeros((4, 3)))
+    assert torch.equal(md.velocities, torch.ones((4, 3)))
+    assert torch.equal(md.row_vector_cell, st.cell.mT)
+
+
+def test_torch_full_to_half_matches_oracle(golden):
+    from tsb import neighbors
+
+    g = golden["nl"]["tiny_self_images"]
+    m, sm, sh = g["mapping"].astype(np.int64), g["system_mapping"].astype(np.int64), g["shifts"]
+    ref = onl.sort_pairs(*onl.full_to_half_list(m, sm, sh.astype(float)))
+    got = neighbors.full_to_half_list(torch.as_tensor(m), torch.as_tensor(sm),
+                                      torch.as_tensor(sh.astype(float)))
+    got = onl.sort_pairs(*(t.numpy() for t in got))
+    np.testing.assert_array_equal(got[0], ref[0])
+    np.testing.assert_array_equal(got[2], ref[2])
+
+
+def test_units_match_reference_constants():
+    from tsb import workloads
+
+    assert abs(workloads.METAL_TIME - 98.22694788464062) < 1e-9
+    assert abs(workloads.KB_EV - 8.617330337217213e-05) < 1e-18

@@ -1,0 +1,214 @@
+// Fused neighbour search + pair energy/force/virial (drop-in for
+// PairPotentialModel.forward, torch_sim/models/pair_potential.py:351-464).
+//
+// One thread per atom i (launched in bin order so neighbouring threads share
+// candidate bins in L1/L2) walks the full neighbour set of i, so forces need no
+// atomics and the summation order is fixed (deterministic results).  Each
+// unordered pair is evaluated from both ends; per-atom energies/virials take
+// half of each visit, matching the half-list weights of pair_potential.py:402-441.
+// Displacements are formed in FP64 from the wrapped FP64 positions; the pair
+// function runs in R (float by default, double with TSB_MATH_FP64).
+#include "tsb_pair.cuh"
+#include "tsb_search.cuh"
+
+namespace tsb {
+
+template <int POT, class R, class P>
+__global__ void __launch_bounds__(128)
+    k_pair_forces(BinData b, int64_t n, const double *__restrict__ table, int ns_species,
+                  const int32_t *__restrict__ species, double cutoff, int flags, P *forces,
+                  P *energies, P *stresses, double *e_half, double *vir_half) {
+  __shared__ PairPrm<R> prm[kMaxSpecies * kMaxSpecies];
+  for (int k = threadIdx.x; k < ns_species * ns_species; k += blockDim.x)
+    prm[k] = make_prm<R>(POT, table + 5 * k, cutoff);
+  __syncthreads();
+  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const double4 w = b.spos[p];
+  const int i = (int)__double_as_longlong(w.w);
+  const int s = b.sys_of[i];
+  const SysGeom &G = b.geom[s];
+  const int si = species ? min(max(species[i], 0), ns_species - 1) : 0;
+  const PairPrm<R> *row = prm + si * ns_species;
+  R fx = 0, fy = 0, fz = 0, ei = 0;
+  R vxx = 0, vyy = 0, vzz = 0, vyz = 0, vxz = 0, vxy = 0;
+  search_neighbors(G, b.spos, b.bin_start, i, w.x, w.y, w.z, cutoff * cutoff, false,
+                   [&](int j, int, int, int, double dx, double dy, double dz, double) {
+                     const int sj = species ? min(max(species[j], 0), ns_species - 1) : 0;
+                     const PairPrm<R> &q = row[sj];
+                     const R rx = (R)dx, ry = (R)dy, rz = (R)dz;
+                     const R r2 = rx * rx + ry * ry + rz * rz;
+                     if (!(r2 < q.a3)) return;
+                     R e, fr;
+                     pair_eval<POT, R>(q, r2, e, fr);
+                     const R gx = fr * rx, gy = fr * ry, gz = fr * rz;  // force on j
+                     fx -= gx;
+                     fy -= gy;
+                     fz -= gz;
+                     ei += e;
+                     vxx += rx * gx;
+                     vyy += ry * gy;
+                     vzz += rz * gz;
+                     vyz += ry * gz;
+                     vxz += rx * gz;
+                     vxy += rx * gy;
+                   });
+  if (flags & TSB_OUT_FORCES) {
+    forces[3 * i] = (P)fx;
+    forces[3 * i + 1] = (P)fy;
+    forces[3 * i + 2] = (P)fz;
+  }
+  // reference per-atom energies: each endpoint receives the full pair energy
+  // (pair_potential.py:411-417 with weight 1 on both mapping rows)
+  if (flags & TSB_OUT_ENERGIES) energies[i] = (P)ei;
+  if (flags & TSB_OUT_STRESSES) {
+    // per-atom stress: -1/2 sum_j r_ij (x) f_ij / V (pair_potential.py:262-272)
+    const double c = -0.5 / G.vol;
+    P *o = stresses + 9 * i;
+    o[0] = (P)(c * vxx); o[1] = (P)(c * vxy); o[2] = (P)(c * vxz);
+    o[3] = (P)(c * vxy); o[4] = (P)(c * vyy); o[5] = (P)(c * vyz);
+    o[6] = (P)(c * vxz); o[7] = (P)(c * vyz); o[8] = (P)(c * vzz);
+  }
+  e_half[i] = 0.5 * (double)ei;
+  double *v = vir_half + 6 * i;
+  v[0] = 0.5 * (double)vxx;
+  v[1] = 0.5 * (double)vyy;
+  v[2] = 0.5 * (double)vzz;
+  v[3] = 0.5 * (double)vyz;
+  v[4] = 0.5 * (double)vxz;
+  v[5] = 0.5 * (double)vxy;
+}
+
+// One block per system, fixed-order tree reduction in FP64 (deterministic).
+template <class P>
+__global__ void k_sys_reduce(const SysGeom *g, const double *e_half, const double *vir_half,
+                             int flags, P *energy, P *stress) {
+  __shared__ double sh[7][kBlock / 32];
+  const int s = blockIdx.x;
+  const SysGeom &G = g[s];
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int a = threadIdx.x; a < G.count; a += blockDim.x) {
+    int64_t i = G.start + a;
+    acc[0] += e_half[i];
+    for (int k = 0; k < 6; ++k) acc[1 + k] += vir_half[6 * i + k];
+  }
+  for (int k = 0; k < 7; ++k) {
+    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+    if ((threadIdx.x & 31) == 0) sh[k][threadIdx.x >> 5] = acc[k];
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  double t[7];
+  for (int k = 0; k < 7; ++k) {
+    t[k] = 0;
+    for (int w = 0; w < kBlock / 32; ++w) t[k] += sh[k][w];
+  }
+  energy[s] = (P)t[0];
+  if (flags & TSB_OUT_STRESS) {
+    const double c = -1.0 / G.vol;  // stress = -1/V sum r (x) f (pair_potential.py:226-232)
+    P *o = stress + 9 * s;
+    o[0] = (P)(c * t[1]); o[1] = (P)(c * t[6]); o[2] = (P)(c * t[5]);
+    o[3] = (P)(c * t[6]); o[4] = (P)(c * t[2]); o[5] = (P)(c * t[4]);
+    o[6] = (P)(c * t[5]); o[7] = (P)(c * t[4]); o[8] = (P)(c * t[3]);
+  }
+}
+
+struct PairWork {
+  BinData b;
+  double *e_half;
+  double *vir_half;
+};
+
+static void carve_pair(Carver &c, PairWork &w, int64_t n, int64_t ns) {
+  carve_bins(c, w.b, n, ns);
+  w.e_half = c.take<double>(n);
+  w.vir_half = c.take<double>(6 * n);
+}
+
+template <int POT, class R, class P>
+static void launch_forces(PairWork &w, int64_t n, const double *table, int nsp,
+                          const int32_t *species, double cutoff, int flags, P *forces,
+                          P *energies, P *stresses, cudaStream_t st) {
+  k_pair_forces<POT, R, P><<<grid_for(n, 128), 128, 0, st>>>(
+      w.b, n, table, nsp, species, cutoff, flags, forces, energies, stresses, w.e_half,
+      w.vir_half);
+}
+
+template <class P>
+static int pair_forward(int pot, const double *table, int nsp, const int32_t *species,
+                        const P *pos, const P *cell, const uint8_t *pbc, const int64_t *sys,
+                        int64_t n, int64_t ns, double cutoff, int flags, P *energy,
+                        P *forces, P *stress, P *energies, P *stresses, PairWork &w,
+                        cudaStream_t st) {
+  TSB_TRY(prepare_bins<P>(pos, cell, pbc, sys, n, ns, cutoff, w.b, st));
+  const bool f64 = flags & TSB_MATH_FP64;
+  if (n > 0) {
+#define TSB_LAUNCH(POT)                                                                    \
+  if (f64)                                                                                 \
+    launch_forces<POT, double, P>(w, n, table, nsp, species, cutoff, flags, forces,       \
+                                  energies, stresses, st);                                 \
+  else                                                                                     \
+    launch_forces<POT, float, P>(w, n, table, nsp, species, cutoff, flags, forces,        \
+                                 energies, stresses, st);
+    if (pot == TSB_POT_LJ) {
+      TSB_LAUNCH(TSB_POT_LJ)
+    } else if (pot == TSB_POT_MORSE) {
+      TSB_LAUNCH(TSB_POT_MORSE)
+    } else {
+      TSB_LAUNCH(TSB_POT_SOFT)
+    }
+#undef TSB_LAUNCH
+  }
+  k_sys_reduce<P><<<(unsigned)ns, kBlock, 0, st>>>(w.b.geom, w.e_half, w.vir_half, flags,
+                                                  energy, stress);
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
+
+}  // namespace tsb
+
+using namespace tsb;
+
+extern "C" size_t tsb_pair_workspace_size(int64_t n_atoms, int64_t n_systems) {
+  Carver c(nullptr, (size_t)-1);
+  PairWork w;
+  carve_pair(c, w, n_atoms, n_systems);
+  return c.off + 256;
+}
+
+extern "C" int tsb_pair_forward(int potential, const double *table, int n_species,
+                                const int32_t *species, const void *positions,
+                                const void *cell_row, const uint8_t *pbc,
+                                const int64_t *system_idx, int64_t n_atoms,
+                                int64_t n_systems, int dtype, double cutoff, int out_flags,
+                                void *energy, void *forces, void *stress, void *energies,
+                                void *stresses, void *workspace, size_t workspace_bytes,
+                                void *stream) {
+  if (potential < TSB_POT_LJ || potential > TSB_POT_SOFT) return TSB_ERR_INVALID_ARG;
+  if (n_species < 1 || n_species > kMaxSpecies || !table) return TSB_ERR_INVALID_ARG;
+  if (n_species > 1 && !species) return TSB_ERR_INVALID_ARG;
+  if (n_atoms < 0 || n_systems < 1 || !(cutoff > 0.0) || !cell_row || !pbc || !energy)
+    return TSB_ERR_INVALID_ARG;
+  if (n_atoms > 0 && (!positions || !system_idx)) return TSB_ERR_INVALID_ARG;
+  if ((out_flags & TSB_OUT_FORCES) && !forces) return TSB_ERR_INVALID_ARG;
+  if ((out_flags & TSB_OUT_STRESS) && !stress) return TSB_ERR_INVALID_ARG;
+  if ((out_flags & TSB_OUT_ENERGIES) && !energies) return TSB_ERR_INVALID_ARG;
+  if ((out_flags & TSB_OUT_STRESSES) && !stresses) return TSB_ERR_INVALID_ARG;
+  if (dtype != TSB_F32 && dtype != TSB_F64) return TSB_ERR_INVALID_ARG;
+  if (n_atoms >= (int64_t)1 << 30) return TSB_ERR_UNSUPPORTED;
+  Carver c(workspace, workspace_bytes);
+  PairWork w;
+  carve_pair(c, w, n_atoms, n_systems);
+  if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == TSB_F64)
+    return pair_forward<double>(potential, table, n_species, species,
+                                (const double *)positions, (const double *)cell_row, pbc,
+                                system_idx, n_atoms, n_systems, cutoff, out_flags,
+                                (double *)energy, (double *)forces, (double *)stress,
+                                (double *)energies, (double *)stresses, w, st);
+  return pair_forward<float>(potential, table, n_species, species, (const float *)positions,
+                             (const float *)cell_row, pbc, system_idx, n_atoms, n_systems,
+                             cutoff, out_flags, (float *)energy, (float *)forces,
+                             (float *)stress, (float *)energies, (float *)stresses, w, st);
+}

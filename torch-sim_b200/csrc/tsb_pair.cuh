@@ -1,0 +1,95 @@
+// Pair-potential arithmetic shared by the fused-search force kernel and the
+// persistent MD kernel.
+//
+// Parameter rows (derived on the device from the caller's (p0,p1,p2,rc,eshift)):
+//   LJ    (lennard_jones.py:23-47):  a0=sigma^2 a1=4eps a2=24eps
+//   MORSE (morse.py:23-47):          a0=sigma  a1=eps  a2=alpha a5=2*alpha*eps
+//   SOFT  (soft_sphere.py:35-59):    a0=sigma  a1=1/sigma a2=alpha a5=eps/alpha a6=eps/sigma
+//   a3 = effective cutoff^2 = min(cutoff, rc)^2 (SOFT also min with sigma), a4 = eshift
+#pragma once
+
+#include "tsb_common.cuh"
+
+namespace tsb {
+
+constexpr int kMaxSpecies = 16;
+
+template <class R>
+struct PairPrm {
+  R a0, a1, a2, a3, a4, a5, a6, a7;
+};
+
+template <class R>
+__device__ inline PairPrm<R> make_prm(int pot, const double *t, double cutoff) {
+  // t = (p0, p1, p2, rc, eshift)
+  PairPrm<R> q;
+  double rc = fmin(cutoff, t[3]);
+  q.a4 = (R)t[4];
+  q.a7 = (R)0;
+  if (pot == TSB_POT_LJ) {
+    q.a0 = (R)(t[0] * t[0]);
+    q.a1 = (R)(4.0 * t[1]);
+    q.a2 = (R)(24.0 * t[1]);
+    q.a5 = q.a6 = (R)0;
+  } else if (pot == TSB_POT_MORSE) {
+    q.a0 = (R)t[0];
+    q.a1 = (R)t[1];
+    q.a2 = (R)t[2];
+    q.a5 = (R)(2.0 * t[2] * t[1]);
+    q.a6 = (R)0;
+  } else {
+    rc = fmin(rc, t[0]);
+    q.a0 = (R)t[0];
+    q.a1 = (R)(1.0 / t[0]);
+    q.a2 = (R)t[2];
+    q.a5 = (R)(t[1] / t[2]);
+    q.a6 = (R)(t[1] / t[0]);
+  }
+  q.a3 = (R)(rc * rc);
+  return q;
+}
+
+__device__ inline float rsqrt_r(float x) { return rsqrtf(x); }
+__device__ inline double rsqrt_r(double x) { return rsqrt(x); }
+__device__ inline float exp_r(float x) { return expf(x); }
+__device__ inline double exp_r(double x) { return exp(x); }
+__device__ inline float pow_r(float x, float y) { return powf(x, y); }
+__device__ inline double pow_r(double x, double y) { return pow(x, y); }
+
+// Returns pair energy e and fr = -(dV/dr)/r, so that the force on j due to i is
+// fr * (r_j - r_i) (pair_potential.py:426-428).  Caller guarantees r2 < a3.
+template <int POT, class R>
+__device__ __forceinline__ void pair_eval(const PairPrm<R> &q, R r2, R &e, R &fr) {
+  if (POT == TSB_POT_LJ) {
+    if (r2 > R(0)) {
+      R ir2 = R(1) / r2;
+      R s2 = q.a0 * ir2;
+      R s6 = s2 * s2 * s2;
+      e = q.a1 * (s6 * s6 - s6) - q.a4;
+      fr = q.a2 * (R(2) * s6 * s6 - s6) * ir2;
+    } else {
+      e = R(0) - q.a4;
+      fr = R(0);
+    }
+  } else if (POT == TSB_POT_MORSE) {
+    if (r2 > R(0)) {
+      R ir = rsqrt_r(r2);
+      R r = r2 * ir;
+      R ex = exp_r(-q.a2 * (r - q.a0));
+      R om = R(1) - ex;
+      e = q.a1 * om * om - q.a1 - q.a4;
+      fr = -q.a5 * ex * om * ir;
+    } else {
+      e = R(0) - q.a4;
+      fr = R(0);
+    }
+  } else {  // SOFT: V = eps/alpha (1 - r/sigma)^alpha for r < sigma
+    R r = (r2 > R(0)) ? r2 * rsqrt_r(r2) : R(0);
+    R base = R(1) - r * q.a1;
+    R bam1 = (q.a2 == R(2)) ? base : pow_r(base, q.a2 - R(1));
+    e = q.a5 * bam1 * base - q.a4;
+    fr = (r2 > R(0)) ? q.a6 * bam1 / r : R(0);
+  }
+}
+
+}  // namespace tsb

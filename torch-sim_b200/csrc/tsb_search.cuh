@@ -1,0 +1,74 @@
+// Cell-list neighbour search over the binned, wrapped positions.
+#pragma once
+
+#include "tsb_common.cuh"
+
+namespace tsb {
+
+__device__ inline void frame_coords(const SysGeom &G, double x, double y, double z,
+                                    double *u) {
+  u[0] = G.T[0] * x + G.T[1] * y + G.T[2] * z;
+  u[1] = G.T[3] * x + G.T[4] * y + G.T[5] * z;
+  u[2] = G.T[6] * x + G.T[7] * y + G.T[8] * z;
+}
+
+__device__ inline int floordiv_dev(int a, int b) {
+  int q = a / b;
+  return (a % b != 0 && ((a < 0) != (b < 0))) ? q - 1 : q;
+}
+
+// Visit every image (j, S) with |w_j + S @ cell - w_i|^2 < rc2 (FP64), where w
+// are the wrapped positions.  The unshifted self image is skipped unless
+// `self_pairs`.  Callback: f(j, Sx, Sy, Sz, dx, dy, dz, d2) with d = w_j + S@cell - w_i.
+template <class F>
+__device__ inline void search_neighbors(const SysGeom &G, const double4 *__restrict__ spos,
+                                        const int64_t *__restrict__ bin_start, int i,
+                                        double wx, double wy, double wz, double rc2,
+                                        bool self_pairs, F &&f) {
+  double u[3];
+  frame_coords(G, wx, wy, wz, u);
+  int lo[3], hi[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    double a = floor((u[k] - G.h[k] - G.org[k]) * G.scale[k]);
+    double b = floor((u[k] + G.h[k] - G.org[k]) * G.scale[k]);
+    if (!G.per[k]) {
+      a = fmax(a, 0.0);
+      b = fmin(b, (double)(G.nb[k] - 1));
+    }
+    lo[k] = (int)a;
+    hi[k] = (int)b;
+  }
+  for (int cx = lo[0]; cx <= hi[0]; ++cx) {
+    int ix = G.per[0] ? floordiv_dev(cx, G.nb[0]) : 0;
+    int bx = cx - ix * G.nb[0];
+    for (int cy = lo[1]; cy <= hi[1]; ++cy) {
+      int iy = G.per[1] ? floordiv_dev(cy, G.nb[1]) : 0;
+      int by = cy - iy * G.nb[1];
+      for (int cz = lo[2]; cz <= hi[2]; ++cz) {
+        int iz = G.per[2] ? floordiv_dev(cz, G.nb[2]) : 0;
+        int bz = cz - iz * G.nb[2];
+        const double sx = ix * G.cell[0] + iy * G.cell[3] + iz * G.cell[6];
+        const double sy = ix * G.cell[1] + iy * G.cell[4] + iz * G.cell[7];
+        const double sz = ix * G.cell[2] + iy * G.cell[5] + iz * G.cell[8];
+        const bool zero_shift = (ix | iy | iz) == 0;
+        const int bin = G.bin_base + (bx * G.nb[1] + by) * G.nb[2] + bz;
+        const int64_t p1 = bin_start[bin + 1];
+        for (int64_t p = bin_start[bin]; p < p1; ++p) {
+          const double4 q = spos[p];
+          const double dx = (q.x + sx) - wx;
+          const double dy = (q.y + sy) - wy;
+          const double dz = (q.z + sz) - wz;
+          const double d2 = dx * dx + dy * dy + dz * dz;
+          if (d2 < rc2) {
+            const int j = (int)__double_as_longlong(q.w);
+            if (j == i && zero_shift && !self_pairs) continue;
+            f(j, ix, iy, iz, dx, dy, dz, d2);
+          }
+        }
+      }
+    }
+  }
+}
+
+}  // namespace tsb

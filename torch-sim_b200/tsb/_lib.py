@@ -1,0 +1,148 @@
+"""ctypes binding of the C ABI in ``include/tsb.h`` (library ``libtsb.so``).
+
+This is the only way Python reaches the kernels: every op passes raw device
+pointers, sizes and the current CUDA stream.  There is no CPU fallback -- if
+the library is missing or a CUDA device is absent the ops raise.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import torch
+
+from .build import LIB_PATH
+
+TSB_OK = 0
+TSB_ERR_INVALID_ARG = 1
+TSB_ERR_CAPACITY = 2
+TSB_ERR_NONFINITE = 3
+TSB_ERR_TIMEOUT = 4
+TSB_ERR_CUDA = 5
+TSB_ERR_UNSUPPORTED = 6
+TSB_ERR_WORKSPACE = 7
+
+F32, F64 = 0, 1
+POT_LJ, POT_MORSE, POT_SOFT = 0, 1, 2
+NL_SELF_INTERACTION, NL_HALF = 1, 2
+OUT_FORCES, OUT_STRESS, OUT_ENERGIES, OUT_STRESSES, MATH_FP64 = 1, 2, 4, 8, 16
+INT_NVE, INT_LANGEVIN = 0, 1
+
+_vp, _i64, _u64, _i32, _dbl, _sz, _int = (C.c_void_p, C.c_int64, C.c_uint64, C.c_int32,
+                                         C.c_double, C.c_size_t, C.c_int)
+
+# name -> (restype, argtypes); mirrors include/tsb.h exactly
+PROTOTYPES = {
+    "tsb_version": (C.c_char_p, []),
+    "tsb_status_string": (C.c_char_p, [_int]),
+    "tsb_nl_workspace_size": (_sz, [_i64, _i64]),
+    "tsb_nl_build": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _int, _dbl, _int, _vp, _i64,
+                            _vp, _vp, _i64, _vp, _vp, _sz, _vp]),
+    "tsb_pair_workspace_size": (_sz, [_i64, _i64]),
+    "tsb_pair_forward": (_int, [_int, _vp, _int, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _int,
+                                _dbl, _int, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "tsb_md_kick": (_int, [_vp, _vp, _vp, _vp, _dbl, _i64, _int, _vp]),
+    "tsb_md_drift": (_int, [_vp, _vp, _vp, _vp, _vp, _dbl, _i64, _int, _vp]),
+    "tsb_md_baoab_boa": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _u64, _u64,
+                                _i64, _int, _vp]),
+    "tsb_fused_max_atoms": (_int, []),
+    "tsb_fused_workspace_size": (_sz, [_i64, _i64]),
+    "tsb_fused_md": (_int, [_int, _int, _vp, _int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64,
+                            _i64, _vp, _dbl, _dbl, _i64, _vp, _vp, _vp, _u64, _u64, _vp,
+                            _vp, _vp, _vp, _sz, _vp]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+class TsbError(RuntimeError):
+    """A tsb C-ABI call returned a non-zero status."""
+
+    def __init__(self, name, status, msg=""):
+        self.status = status
+        super().__init__(f"{name} failed: status {status} ({status_string(status)}) {msg}")
+
+
+def lib_path() -> str:
+    return os.environ.get("TSB_LIB", LIB_PATH)
+
+
+def load(path: str | None = None):
+    """Load libtsb.so (raises if it has not been built)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        p = path or lib_path()
+        if not os.path.exists(p):
+            raise RuntimeError(
+                f"tsb CUDA library not found at {p}; build it with "
+                "`python -m tsb.build` (nvcc, sm_100a). There is no CPU fallback.")
+        lib = C.CDLL(p)
+        for name, (res, args) in PROTOTYPES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def status_string(status: int) -> str:
+    try:
+        return load().tsb_status_string(int(status)).decode()
+    except Exception:  # noqa: BLE001
+        return "?"
+
+
+def call(name: str, *args):
+    st = getattr(load(), name)(*args)
+    if st != TSB_OK:
+        raise TsbError(name, st)
+    return st
+
+
+def ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def stream_ptr(device: torch.device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def dtype_code(dtype: torch.dtype) -> int:
+    if dtype == torch.float64:
+        return F64
+    if dtype == torch.float32:
+        return F32
+    raise TypeError(f"tsb kernels support float32/float64, got {dtype}")
+
+
+def require_cuda(t: torch.Tensor, what: str = "tensor") -> None:
+    if not t.is_cuda:
+        raise RuntimeError(f"tsb ops run on CUDA only ({what} is on {t.device}); "
+                           "there is no CPU fallback")
+
+
+class Workspace:
+    """Per-device grow-only scratch buffer handed to the C ABI."""
+
+    _bufs: dict = {}
+
+    @classmethod
+    def get(cls, device: torch.device, nbytes: int) -> torch.Tensor:
+        # one buffer per (device, stream): calls are stream-ordered, so reuse on
+        # the same stream is safe and concurrent streams never share scratch
+        key = (device.type, device.index, stream_ptr(device))
+        buf = cls._bufs.get(key)
+        if buf is None or buf.numel() < nbytes:
+            buf = torch.empty(max(int(nbytes * 1.25), 1 << 20), dtype=torch.uint8,
+                              device=device)
+            cls._bufs[key] = buf
+        return buf
+
+    @classmethod
+    def clear(cls) -> None:
+        cls._bufs.clear()

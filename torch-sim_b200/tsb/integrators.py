@@ -1,0 +1,243 @@
+"""MD step functions on the tsb kernels (drop-ins for torch_sim.integrators).
+
+Signatures follow the reference registry entries (internal units, runners.py
+converts user units, torch_sim/integrators/__init__.py:193-255):
+
+* ``nve_init(state, model, *, kT)`` / ``nve_step(state, model, *, dt)``
+  <- torch_sim/integrators/nve.py:19-130 (velocity Verlet)
+* ``nvt_langevin_init(state, model, *, kT)`` /
+  ``nvt_langevin_step(state, model, *, dt, kT, gamma=None)``
+  <- torch_sim/integrators/nvt.py:89-240 (BAOAB, gamma default 1/(100 dt))
+* ``initialize_momenta`` <- md.py:113-166
+
+Steps mutate ``state`` in place and return it (md.py:184-187).  ``dt``, ``kT``
+and ``gamma`` may be scalars or per-system tensors.
+
+Langevin noise: by default the O-step draws counter-based Philox4x32-10
+normals on the device (key = the state's seed, counter = its step count), so a
+trajectory is reproducible from (seed, step).  Passing ``noise=[N,3]`` uses
+those normals instead -- e.g. the reference's own ``torch.randn`` draws, which
+makes one step agree with the reference to rounding.
+
+``run_md`` is the persistent fused path: many steps of many systems in one
+kernel launch (see csrc/tsb_fused.cu).
+"""
+
+from __future__ import annotations
+
+import torch
+
+from . import _lib as L
+from .state import MDState
+
+
+def _per_system(x, n_sys: int, device) -> torch.Tensor:
+    t = torch.as_tensor(x, dtype=torch.float64, device=device)
+    if t.ndim == 0:
+        t = t.expand(n_sys)
+    return t.contiguous()
+
+
+def initialize_momenta(positions, masses, system_idx, kT, generator=None):
+    """p = sqrt(m kT) N(0,1) minus the per-system mean (md.py:113-166)."""
+    kT = torch.as_tensor(kT, device=positions.device, dtype=positions.dtype)
+    if kT.ndim > 0:
+        kT = kT[system_idx]
+    p = torch.randn(positions.shape, device=positions.device, dtype=positions.dtype,
+                    generator=generator) * torch.sqrt(masses * kT).unsqueeze(-1)
+    n_sys = int(system_idx[-1]) + 1
+    counts = torch.bincount(system_idx, minlength=n_sys)
+    mean = torch.zeros((n_sys, 3), device=p.device, dtype=p.dtype).index_add_(
+        0, system_idx, p) / counts.view(-1, 1)
+    return torch.where((counts > 1)[system_idx].view(-1, 1), p - mean[system_idx], p)
+
+
+def _seed_of(state) -> int:
+    rng = getattr(state, "_rng", None)
+    if isinstance(rng, int):
+        return rng
+    if isinstance(rng, torch.Generator):
+        return int(rng.initial_seed())
+    return 0
+
+
+def _md_init(state, model, kT):
+    out = model(state)
+    kT_t = torch.as_tensor(kT, device=state.device, dtype=state.dtype)
+    momenta = getattr(state, "momenta", None)
+    if momenta is None:
+        momenta = initialize_momenta(state.positions, state.masses, state.system_idx, kT_t,
+                                     state.rng)
+    md = MDState.from_state(state, momenta=momenta, energy=out["energy"],
+                            forces=out["forces"])
+    md._philox_seed = _seed_of(state)
+    md._philox_counter = 0
+    return md
+
+
+def nve_init(state, model, *, kT, **_kw) -> MDState:
+    return _md_init(state, model, kT)
+
+
+def nvt_langevin_init(state, model, *, kT, **_kw) -> MDState:
+    return _md_init(state, model, kT)
+
+
+def _kick(state, dt_s, scale):
+    L.call("tsb_md_kick", L.ptr(state.momenta), L.ptr(state.forces),
+           L.ptr(state.system_idx), L.ptr(dt_s), float(scale), state.n_atoms,
+           L.dtype_code(state.dtype), L.stream_ptr(state.device))
+
+
+def _drift(state, dt_s, scale):
+    L.call("tsb_md_drift", L.ptr(state.positions), L.ptr(state.momenta),
+           L.ptr(state.masses), L.ptr(state.system_idx), L.ptr(dt_s), float(scale),
+           state.n_atoms, L.dtype_code(state.dtype), L.stream_ptr(state.device))
+
+
+def _prepare(state):
+    L.require_cuda(state.positions, "state.positions")
+    for name in ("positions", "momenta", "forces", "masses"):
+        t = getattr(state, name)
+        if not t.is_contiguous() or t.dtype != state.dtype:
+            setattr(state, name, t.to(state.dtype).contiguous())
+    if not state.system_idx.is_contiguous():
+        state.system_idx = state.system_idx.contiguous()
+
+
+def _apply_model(state, model):
+    out = model(state)
+    state.energy = out["energy"]
+    state.forces = out["forces"].contiguous()
+    return out
+
+
+def nve_step(state, model, *, dt, **_kw):
+    """B(dt/2) A(dt) force B(dt/2) (nve.py:74-130)."""
+    _prepare(state)
+    dt_s = _per_system(dt, state.n_systems, state.device)
+    _kick(state, dt_s, 0.5)
+    _drift(state, dt_s, 1.0)
+    _apply_model(state, model)
+    _kick(state, dt_s, 0.5)
+    return state
+
+
+def nvt_langevin_step(state, model, *, dt, kT, gamma=None, noise=None, **_kw):
+    """BAOAB: B(dt/2) A(dt/2) O(dt) A(dt/2) force B(dt/2) (nvt.py:144-240)."""
+    _prepare(state)
+    n_sys = state.n_systems
+    dt_s = _per_system(dt, n_sys, state.device)
+    kT_s = _per_system(kT, n_sys, state.device)
+    if gamma is None:
+        gamma = 1.0 / (100.0 * torch.as_tensor(dt, dtype=torch.float64))
+    g_s = _per_system(gamma, n_sys, state.device)
+    if noise is not None:
+        noise = noise.to(device=state.device, dtype=state.dtype).contiguous()
+    seed = getattr(state, "_philox_seed", _seed_of(state))
+    counter = getattr(state, "_philox_counter", 0)
+    L.call("tsb_md_baoab_boa", L.ptr(state.positions), L.ptr(state.momenta),
+           L.ptr(state.forces), L.ptr(state.masses), L.ptr(state.system_idx), L.ptr(dt_s),
+           L.ptr(kT_s), L.ptr(g_s), L.ptr(noise), seed & (2**64 - 1), counter,
+           state.n_atoms, L.dtype_code(state.dtype), L.stream_ptr(state.device))
+    state._philox_seed, state._philox_counter = seed, counter + 1
+    _apply_model(state, model)
+    _kick(state, dt_s, 0.5)
+    return state
+
+
+# ---------------------------------------------------------------------------
+# Persistent fused batched MD
+# ---------------------------------------------------------------------------
+class FusedMDError(RuntimeError):
+    pass
+
+
+def _system_order(state):
+    """Largest systems first (longest-processing-time order balances the tail)."""
+    cache = getattr(state, "_tsb_order", None)
+    key = (state.system_idx.data_ptr(), state.n_atoms)
+    if cache is not None and cache[0] == key:
+        return cache[1], cache[2]
+    counts = torch.bincount(state.system_idx, minlength=state.n_systems)
+    order = torch.argsort(counts, descending=True, stable=True).to(torch.int32).contiguous()
+    max_atoms = int(counts.max())
+    try:
+        state._tsb_order = (key, order, max_atoms)
+    except AttributeError:
+        pass
+    return order, max_atoms
+
+
+def run_md(state, model, n_steps: int, *, integrator: str = "nvt_langevin", dt, kT=None,
+           gamma=None, skin: float = 1.0, seed: int | None = None, check: bool = True,
+           return_rebuilds: bool = False):
+    """Advance every system ``n_steps`` in ONE persistent kernel launch.
+
+    Same update rules as ``nve_step`` / ``nvt_langevin_step`` (Langevin noise
+    from the Philox stream), with a device-side Verlet list (cutoff + skin)
+    rebuilt when any atom of a system moved more than skin/2.  ``model`` must be
+    a :class:`tsb.models.PairTableModel` (LJ / Morse / soft sphere, any species
+    table); all axes must be periodic and systems may have up to
+    ``tsb_fused_max_atoms()`` (512) atoms.  ``state`` is updated in place
+    (positions, momenta, forces, energy).
+    """
+    from .models.pair_potential import PairTableModel
+
+    if not isinstance(model, PairTableModel):
+        raise TypeError("run_md needs a tsb PairTableModel (LJ / Morse / soft sphere)")
+    integ = {"nve": L.INT_NVE, "nvt_langevin": L.INT_LANGEVIN}[integrator]
+    L.require_cuda(state.positions, "state.positions")
+    if not bool(torch.as_tensor(state.pbc).all()):
+        raise FusedMDError("run_md requires periodic boundaries on all axes")
+    dev = state.device
+    n, n_sys = state.n_atoms, state.n_systems
+    order, max_atoms = _system_order(state)
+    lib = L.load()
+    if max_atoms > lib.tsb_fused_max_atoms():
+        raise FusedMDError(f"systems with {max_atoms} atoms exceed the fused-kernel limit "
+                           f"of {lib.tsb_fused_max_atoms()}")
+    dt_s = _per_system(dt, n_sys, dev)
+    if integ == L.INT_LANGEVIN:
+        if kT is None:
+            raise ValueError("kT is required for nvt_langevin")
+        kT_s = _per_system(kT, n_sys, dev)
+        if gamma is None:
+            gamma = 1.0 / (100.0 * torch.as_tensor(dt, dtype=torch.float64))
+        g_s = _per_system(gamma, n_sys, dev)
+    else:
+        kT_s = g_s = None
+    f64 = torch.float64
+    x = state.positions.to(f64).contiguous()
+    p = state.momenta.to(f64).contiguous()
+    f = state.forces.to(f64).contiguous()
+    m = state.masses.to(f64).contiguous()
+    cell_row = state.cell.mT.to(f64).contiguous()
+    sys_idx = state.system_idx.contiguous()
+    species = model._species(state.atomic_numbers)
+    table = model.table if model.table.device == dev else model.table.to(dev)
+    energy = torch.empty(n_sys, dtype=f64, device=dev)
+    rebuilds = torch.zeros(n_sys, dtype=torch.int32, device=dev)
+    status = torch.zeros(2, dtype=torch.int32, device=dev)
+    ws = L.Workspace.get(dev, lib.tsb_fused_workspace_size(n, n_sys))
+    if seed is None:
+        seed = getattr(state, "_philox_seed", _seed_of(state))
+    counter = getattr(state, "_philox_counter", 0)
+    L.call("tsb_fused_md", integ, model.kind, L.ptr(table), model.n_species, L.ptr(species),
+           L.ptr(x), L.ptr(p), L.ptr(f), L.ptr(m), L.ptr(cell_row), L.ptr(sys_idx), n, n_sys,
+           L.ptr(order), model.cutoff, float(skin), int(n_steps), L.ptr(dt_s), L.ptr(kT_s),
+           L.ptr(g_s), seed & (2**64 - 1), counter, L.ptr(energy), L.ptr(rebuilds),
+           L.ptr(status), L.ptr(ws), ws.numel(), L.stream_ptr(dev))
+    if check:
+        st = status.tolist()
+        if st[0] != 0:
+            raise FusedMDError(f"fused MD: system {st[1]}: {L.status_string(st[0])}")
+    dt_in = state.positions.dtype
+    state.positions = x if dt_in == f64 else x.to(dt_in)
+    state.momenta = p if dt_in == f64 else p.to(dt_in)
+    state.forces = f if dt_in == f64 else f.to(dt_in)
+    state.energy = energy if dt_in == f64 else energy.to(dt_in)
+    state._philox_seed, state._philox_counter = seed, counter + int(n_steps)
+    if return_rebuilds:
+        return state, rebuilds
+    return state

@@ -1,0 +1,12 @@
+"""Classical pair-potential models on the tsb CUDA kernels."""
+
+from .interface import ModelInterface
+from .lennard_jones import (LennardJonesModel, LennardJonesMultiModel,
+                            UnbatchedLennardJonesModel, kob_andersen_model)
+from .morse import MorseModel
+from .pair_potential import PairTableModel
+from .soft_sphere import SoftSphereModel, SoftSphereMultiModel
+
+__all__ = ["LennardJonesModel", "LennardJonesMultiModel", "ModelInterface", "MorseModel",
+           "PairTableModel", "SoftSphereModel", "SoftSphereMultiModel",
+           "UnbatchedLennardJonesModel", "kob_andersen_model"]

@@ -1,0 +1,163 @@
+"""Pair-potential models on the fused GPU neighbour-search + force kernel.
+
+``PairTableModel`` is the drop-in for torch_sim/models/pair_potential.py:277-464
+(PairPotentialModel with reduce_to_half_list=True) restricted to the analytic
+pair functions the kernels implement: Lennard-Jones, Morse and soft sphere,
+each with an optional species matrix (soft_sphere.py:90-167).  Outputs follow
+the reference exactly:
+
+* ``energy [S]``        sum of pair energies per system (:402-409)
+* ``forces [N,3]``      -dE/dr_i (:420-441)
+* ``stress [S,3,3]``    -1/V sum_pairs r_ij (x) f_ij (:200-232)
+* ``energies [N]``      each endpoint receives the full pair energy (:411-417)
+* ``stresses [N,3,3]``  each endpoint receives half the pair virial (:262-272)
+
+Precision: ``precision="mixed"`` (default) evaluates the pair function in FP32
+from FP64 displacements and accumulates per-system energy/virial in FP64;
+``precision="fp64"`` runs the pair function in FP64 as well.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .. import _lib as L
+from .interface import ModelInterface
+
+KIND = {"lj": L.POT_LJ, "morse": L.POT_MORSE, "soft_sphere": L.POT_SOFT}
+
+
+class PairTableModel(ModelInterface):
+    """Species-matrix pair potential evaluated by ``tsb_pair_forward``.
+
+    Args:
+        potential: "lj", "morse" or "soft_sphere".
+        table: [n_species, n_species, 5] rows (p0, p1, p2, rc, eshift), see
+            include/tsb.h (LJ: sigma, epsilon; Morse/soft sphere: sigma, epsilon,
+            alpha; rc per-pair truncation; eshift subtracted inside rc).
+        species_atomic_numbers: atomic number of each species row (sorted unique
+            Z, as SoftSphereMultiModel does, soft_sphere.py:308-312); None means a
+            single species for every atom.
+        cutoff: neighbour cutoff (pairs at r >= cutoff are ignored, pair_potential.py:194).
+    """
+
+    def __init__(self, potential: str, table, *, cutoff: float,
+                 species_atomic_numbers=None, device=None, dtype=torch.float64,
+                 compute_forces: bool = True, compute_stress: bool = False,
+                 per_atom_energies: bool = False, per_atom_stresses: bool = False,
+                 neighbor_list_fn=None, retain_graph: bool = False,
+                 precision: str = "mixed") -> None:
+        super().__init__()
+        if retain_graph:
+            raise NotImplementedError(
+                "retain_graph: tsb kernels are not traced by autograd; use "
+                "tsb.adjoint for differentiable trajectories")
+        if precision not in ("mixed", "fp64"):
+            raise ValueError(f"precision must be 'mixed' or 'fp64', got {precision!r}")
+        self._device = torch.device(device) if device is not None else torch.device("cuda")
+        self._dtype = dtype
+        self._compute_forces = compute_forces
+        self._compute_stress = compute_stress
+        self.per_atom_energies = per_atom_energies
+        self.per_atom_stresses = per_atom_stresses
+        self.potential = potential
+        self.kind = KIND[potential]
+        self.cutoff = float(cutoff)
+        self.precision = precision
+        # neighbor_list_fn is accepted for signature compatibility: the kernel
+        # builds the identical pair set itself (fused search + force).
+        self.neighbor_list_fn = neighbor_list_fn
+        tab = np.asarray(table, dtype=np.float64)
+        if tab.ndim != 3 or tab.shape[0] != tab.shape[1] or tab.shape[2] != 5:
+            raise ValueError("table must have shape [n_species, n_species, 5]")
+        if tab.shape[0] > 16:
+            raise ValueError("at most 16 species are supported")
+        self.n_species = tab.shape[0]
+        self.table_np = tab
+        self.register_buffer("table", torch.as_tensor(tab, device=self._device), persistent=False)
+        if species_atomic_numbers is None:
+            self.z_lut = None
+        else:
+            z = torch.as_tensor(species_atomic_numbers, dtype=torch.int64).cpu()
+            lut = torch.full((int(z.max()) + 1,), -1, dtype=torch.int32)
+            lut[z] = torch.arange(len(z), dtype=torch.int32)
+            self.z_lut = lut.to(self._device)
+        self._species_cache = (None, None)
+
+    def _species(self, atomic_numbers: torch.Tensor):
+        if self.z_lut is None:
+            return None
+        key = (atomic_numbers.data_ptr(), atomic_numbers._version, atomic_numbers.shape[0])
+        if self._species_cache[0] == key:
+            return self._species_cache[1]
+        z = atomic_numbers.to(self.z_lut.device)
+        if bool((z < 0).any() | (z >= len(self.z_lut)).any()):
+            raise ValueError("atomic number outside the model's species table")
+        sp = self.z_lut[z].contiguous()
+        if bool((sp < 0).any()):
+            raise ValueError("atomic number not in the model's species table")
+        self._species_cache = (key, sp)
+        return sp
+
+    def forward(self, state, **_kwargs) -> dict[str, torch.Tensor]:
+        if state.dtype != self._dtype:
+            raise TypeError(
+                f"SimState dtype {state.dtype} does not match model dtype {self._dtype}.")
+        pos = state.positions
+        L.require_cuda(pos, "state.positions")
+        dev, dt = pos.device, pos.dtype
+        n = pos.shape[0]
+        n_sys = state.n_systems
+        cell_row = state.cell.mT.contiguous()
+        pbc = state.pbc
+        if pbc.ndim == 1:
+            pbc = pbc.unsqueeze(0).expand(n_sys, 3)
+        pbc = pbc.to(torch.uint8).contiguous()
+        sys_idx = state.system_idx.contiguous()
+        species = self._species(state.atomic_numbers)
+        table = self.table if self.table.device == dev else self.table.to(dev)
+        flags = 0
+        if self._compute_forces:
+            flags |= L.OUT_FORCES
+        if self._compute_stress:
+            flags |= L.OUT_STRESS
+        if self.per_atom_energies:
+            flags |= L.OUT_ENERGIES
+        if self.per_atom_stresses:
+            flags |= L.OUT_STRESSES
+        if self.precision == "fp64":
+            flags |= L.MATH_FP64
+        energy = torch.empty(n_sys, dtype=dt, device=dev)
+        forces = torch.empty((n, 3), dtype=dt, device=dev) if self._compute_forces else None
+        stress = torch.empty((n_sys, 3, 3), dtype=dt, device=dev) if self._compute_stress else None
+        energies = torch.empty(n, dtype=dt, device=dev) if self.per_atom_energies else None
+        stresses = (torch.empty((n, 3, 3), dtype=dt, device=dev)
+                    if self.per_atom_stresses else None)
+        ws_bytes = L.load().tsb_pair_workspace_size(n, n_sys)
+        ws = L.Workspace.get(dev, ws_bytes)
+        pos = pos.contiguous()
+        L.call("tsb_pair_forward", self.kind, L.ptr(table), self.n_species, L.ptr(species),
+               L.ptr(pos), L.ptr(cell_row), L.ptr(pbc), L.ptr(sys_idx), n, n_sys,
+               L.dtype_code(dt), self.cutoff, flags, L.ptr(energy), L.ptr(forces),
+               L.ptr(stress), L.ptr(energies), L.ptr(stresses), L.ptr(ws), ws.numel(),
+               L.stream_ptr(dev))
+        out = {"energy": energy}
+        if forces is not None:
+            out["forces"] = forces
+        if stress is not None:
+            out["stress"] = stress
+        if energies is not None:
+            out["energies"] = energies
+        if stresses is not None:
+            out["stresses"] = stresses
+        return out
+
+
+def single_species_table(sigma, epsilon, alpha=0.0, rc=np.inf, eshift=0.0):
+    return np.array([[[sigma, epsilon, alpha, rc, eshift]]], dtype=np.float64)
+
+
+def lj_energy(r, sigma, epsilon):
+    x6 = (sigma / r) ** 6
+    return 4.0 * epsilon * (x6 * x6 - x6)

@@ -1,0 +1,187 @@
+"""Batched simulation-state containers mirroring TorchSim's SimState family.
+
+Field names, shapes and conventions follow the reference so that code written
+against ``torch_sim.SimState`` works unchanged:
+
+* ``SimState``      <- torch_sim/state.py:120-860 (positions [N,3], masses [N],
+  cell [S,3,3] in the COLUMN-vector convention (state.py:138-142), pbc [3],
+  atomic_numbers [N], system_idx [N] contiguous)
+* ``MDState``       <- torch_sim/integrators/md.py:31-110 (+ momenta, energy, forces)
+* ``FireState``     <- torch_sim/optimizers/state.py:38-51
+* ``CellFireState`` <- torch_sim/optimizers/cell_filters.py:457-467
+
+The tsb models and step functions only read attributes, so a reference
+``torch_sim.SimState`` can be passed in directly as well.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+from dataclasses import dataclass, field
+
+import torch
+
+
+@dataclass(kw_only=True)
+class SimState:
+    positions: torch.Tensor
+    masses: torch.Tensor
+    cell: torch.Tensor
+    pbc: torch.Tensor | bool | list = True
+    atomic_numbers: torch.Tensor
+    system_idx: torch.Tensor | None = None
+    _rng: object = field(default=None, repr=False)
+    _n_systems: int | None = field(default=None, repr=False)
+
+    def __post_init__(self) -> None:
+        dev = self.positions.device
+        if not isinstance(self.pbc, torch.Tensor):
+            p = [self.pbc] * 3 if isinstance(self.pbc, bool) else list(self.pbc)
+            self.pbc = torch.tensor(p, dtype=torch.bool, device=dev)
+        if self.system_idx is None:
+            self.system_idx = torch.zeros(self.positions.shape[0], dtype=torch.int64,
+                                          device=dev)
+        if self.cell.ndim == 2:
+            self.cell = self.cell.unsqueeze(0)
+        n = {self.positions.shape[0], self.masses.shape[0], self.atomic_numbers.shape[0]}
+        if len(n) != 1:
+            raise ValueError(f"Incompatible shapes: {n}")
+
+    # --- reference properties -------------------------------------------------
+    @property
+    def device(self) -> torch.device:
+        return self.positions.device
+
+    @property
+    def dtype(self) -> torch.dtype:
+        return self.positions.dtype
+
+    @property
+    def n_atoms(self) -> int:
+        return self.positions.shape[0]
+
+    @property
+    def n_systems(self) -> int:
+        if self._n_systems is None:
+            self._n_systems = self.cell.shape[0]
+        return self._n_systems
+
+    @property
+    def n_atoms_per_system(self) -> torch.Tensor:
+        return self.system_idx.bincount(minlength=self.n_systems)
+
+    @property
+    def row_vector_cell(self) -> torch.Tensor:
+        return self.cell.mT
+
+    @row_vector_cell.setter
+    def row_vector_cell(self, value: torch.Tensor) -> None:
+        self.cell = value.mT
+
+    @property
+    def volume(self) -> torch.Tensor:
+        return torch.det(self.cell)
+
+    @property
+    def rng(self) -> torch.Generator:
+        if not isinstance(self._rng, torch.Generator):
+            g = torch.Generator(device=self.device)
+            if isinstance(self._rng, int):
+                g.manual_seed(self._rng)
+            self._rng = g
+        return self._rng
+
+    @rng.setter
+    def rng(self, value) -> None:
+        self._rng = value
+
+    @property
+    def constraints(self) -> list:
+        return []
+
+    def set_constrained_positions(self, new_positions: torch.Tensor) -> None:
+        self.positions = new_positions
+
+    def clone(self):
+        kw = {f.name: (getattr(self, f.name).clone()
+                       if isinstance(getattr(self, f.name), torch.Tensor)
+                       else getattr(self, f.name))
+              for f in dataclasses.fields(self)}
+        return type(self)(**kw)
+
+    def to(self, device=None, dtype=None):
+        kw = {}
+        for f in dataclasses.fields(self):
+            v = getattr(self, f.name)
+            if isinstance(v, torch.Tensor):
+                v = v.to(device=device) if device is not None else v
+                if dtype is not None and v.is_floating_point():
+                    v = v.to(dtype=dtype)
+            kw[f.name] = v
+        return type(self)(**kw)
+
+    @classmethod
+    def from_state(cls, state, **extra):
+        """Build ``cls`` from any SimState-like object (tsb or torch_sim)."""
+        names = {f.name for f in dataclasses.fields(cls)}
+        kw = {}
+        for k in ("positions", "masses", "cell", "pbc", "atomic_numbers", "system_idx"):
+            kw[k] = getattr(state, k)
+        if "_rng" in names:
+            kw["_rng"] = getattr(state, "_rng", None)
+        for k in names:
+            if k not in kw and k not in extra and hasattr(state, k) and not k.startswith("_"):
+                kw[k] = getattr(state, k)
+        kw.update(extra)
+        return cls(**kw)
+
+
+@dataclass(kw_only=True)
+class MDState(SimState):
+    momenta: torch.Tensor
+    energy: torch.Tensor
+    forces: torch.Tensor
+
+    @property
+    def velocities(self) -> torch.Tensor:
+        return self.momenta / self.masses.unsqueeze(-1)
+
+    def set_constrained_momenta(self, new_momenta: torch.Tensor) -> None:
+        self.momenta = new_momenta
+
+
+@dataclass(kw_only=True)
+class FireState(SimState):
+    forces: torch.Tensor
+    energy: torch.Tensor
+    stress: torch.Tensor | None
+    velocities: torch.Tensor
+    dt: torch.Tensor
+    alpha: torch.Tensor
+    n_pos: torch.Tensor
+
+    def set_constrained_forces(self, new_forces: torch.Tensor) -> None:
+        self.forces = new_forces
+
+
+@dataclass(kw_only=True)
+class CellFireState(FireState):
+    reference_cell: torch.Tensor
+    cell_filter: str = "frechet"
+    cell_factor: torch.Tensor | None = None
+    pressure: torch.Tensor | None = None
+    cell_positions: torch.Tensor | None = None
+    cell_forces: torch.Tensor | None = None
+    cell_velocities: torch.Tensor | None = None
+    cell_masses: torch.Tensor | None = None
+    hydrostatic_strain: bool = False
+    constant_volume: bool = False
+
+
+def state_from_arrays(d: dict, device="cuda", dtype=torch.float64) -> SimState:
+    """SimState from the numpy dicts produced by :mod:`tsb.workloads`."""
+    t = lambda x, dt=dtype: torch.as_tensor(x, dtype=dt, device=device)  # noqa: E731
+    return SimState(positions=t(d["positions"]), masses=t(d["masses"]), cell=t(d["cell"]),
+                    pbc=torch.as_tensor(d["pbc"], dtype=torch.bool, device=device),
+                    atomic_numbers=t(d["atomic_numbers"], torch.int64),
+                    system_idx=t(d["system_idx"], torch.int64))
