@@ -1,0 +1,347 @@
+#!/usr/bin/env python
+"""Benchmark: batched uneven Morse NVT-Langevin MD on B200.
+
+Workload (seeded synthetic, no dataset): 2048 Cu fcc supercells (a = 3.61 A)
+with atom counts uniform in [8, 512] rounded to 4*n1*n2*n3, random diagonal
+strain +-2 % and triclinic shear +-3 deg; Morse D = 0.3429 eV,
+alpha = 1.3588 1/A, r0 = 2.866 A, cutoff 6.0 A; NVT Langevin (BAOAB) at
+1000 K, dt = 2 fs, gamma = 0.01 1/fs; FP32 pair arithmetic with FP64
+positions, momenta and per-system energy.
+
+One bench "step" is one launch of the persistent fused kernel that advances
+every system by --md-steps MD steps (default 500; 10 timed steps = the 5,000
+MD steps of the workload).  Metric: atom-steps/s = atoms x MD steps / time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl tsb|reference]
+
+N > 1 runs under torchrun, one rank per GPU, each rank advancing its own
+2048-system batch (independent systems, no collective in the step: weak
+scaling).  --impl reference times the reference algorithm's CPU restatement
+(the oracle port) on the host cores.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "torch-sim_b200"))
+
+METRIC = "atom-steps/s on 1 B200 (batched fused vs plain path) at force err ≤1e-5 vs FP64"
+UNIT = "atom-steps/s"
+WORKLOAD = ("2048 Cu fcc systems (8-512 atoms, strain +-2%, shear +-3deg), Morse "
+            "(D=0.3429 eV, alpha=1.3588/A, r0=2.866 A, rc=6.0 A), NVT-Langevin BAOAB "
+            "1000 K, dt=2 fs, gamma=0.01/fs")
+ALG_BYTES_PER_ATOM_STEP = 76  # streaming state r/w: 48 B FP64 pos + 24 B mom + 4 B type/mass
+SKIN = 1.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="tsb", choices=["tsb", "reference"])
+    ap.add_argument("--md-steps", type=int, default=500)
+    ap.add_argument("--n-systems", type=int, default=2048)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms in a thread."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(
+                    ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                     "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                    timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:  # noqa: BLE001
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if len(r) > 5 + k and r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:  # noqa: BLE001
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per fused launch from the committed ncu summary (or None)."""
+    p = os.path.join(REPO, "profiles", "fused_md_ncu.md")
+    try:
+        for line in open(p):
+            if line.startswith("dram_bytes_per_launch_full_workload:"):
+                return float(line.split(":")[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+def build_workload(n_systems, seed, device):
+    import torch
+
+    from tsb import integrators, models, workloads
+    from tsb.state import state_from_arrays
+
+    d = workloads.copper_batch(n_systems, 8, 512, seed=seed)
+    st = state_from_arrays(d, device=device)
+    st.rng = 1000 + seed
+    model = models.MorseModel(sigma=2.866, epsilon=0.3429, alpha=1.3588, cutoff=6.0,
+                              device=device)
+    kT = 1000.0 * workloads.KB_EV
+    md = integrators.nvt_langevin_init(st, model, kT=kT)
+    torch.cuda.synchronize(device)
+    return d, md, model
+
+
+def cpu_baseline(d, budget_s=20.0, processes=1, n_steps=2, seed=0):
+    """Oracle port on the host: a bounded sample of systems (see oracle/cpu_md.py)."""
+    import numpy as np
+
+    sys.path.insert(0, REPO)
+    from oracle import cpu_md
+    from tsb import workloads as W
+
+    rng = np.random.default_rng(seed)
+    n_sys = int(d["system_idx"].max()) + 1
+    systems = rng.permutation(n_sys)
+    dt, kT, g = 0.002 * W.METAL_TIME, 1000 * W.KB_EV, 10.0 / W.METAL_TIME
+    take = 4 * processes
+    a, t = cpu_md.time_sample(d, systems[:take], n_steps, dt, kT, g, 6.0, processes)
+    # grow the sample toward the time budget, keeping the same per-system mix
+    if t < budget_s / 4:
+        take = int(min(n_sys, max(take, take * budget_s / 2 / max(t, 1e-3))))
+        a, t = cpu_md.time_sample(d, systems[:take], n_steps, dt, kT, g, 6.0, processes)
+    atoms = int(np.bincount(d["system_idx"])[systems[:take]].sum())
+    return {"value": a / t, "unit": UNIT, "cores": processes, "kind": "port",
+            "sample": f"{take} of {n_sys} systems ({atoms} atoms) x {n_steps} BAOAB steps, "
+                      f"numpy oracle (NL + Morse + BAOAB), {t:.1f} s"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    sys.path.insert(0, REPO)
+    from oracle import cpu_md
+    from tsb import workloads as W
+
+    import numpy as np
+
+    d = W.copper_batch(args.n_systems, 8, 512, seed=0)
+    procs = cpu_md.cpu_count()
+    n_sys = args.n_systems
+    rng = np.random.default_rng(0)
+    perm = rng.permutation(n_sys)
+    dt, kT, g = 0.002 * W.METAL_TIME, 1000 * W.KB_EV, 10.0 / W.METAL_TIME
+    per = 2 * procs  # systems per step: a bounded sample of the workload
+    times, work = [], []
+    for k in range(args.warmup + args.steps):
+        systems = perm[(k * per) % n_sys:][:per]
+        a, t = cpu_md.time_sample(d, systems, 1, dt, kT, g, 6.0, procs)
+        if k >= args.warmup:
+            times.append(t)
+            work.append(a)
+    value = sum(work) / sum(times)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": WORKLOAD, "n_systems": n_sys,
+                       "sample_systems_per_step": per, "md_steps_per_step": 1},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "port",
+                             "sample": f"{per} systems x 1 BAOAB step per bench step, "
+                                       "numpy oracle of the reference path"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    device = torch.device("cuda", local if ws > 1 else 0)
+    torch.cuda.set_device(device)
+    from tsb import integrators
+
+    d, md, model = build_workload(args.n_systems, seed=rank, device=device)
+    n_atoms = md.n_atoms
+    from tsb import workloads as W
+
+    runner = integrators.FusedMD(md, model, integrator="nvt_langevin",
+                                 dt=0.002 * W.METAL_TIME, kT=1000 * W.KB_EV,
+                                 gamma=10.0 / W.METAL_TIME, skin=SKIN, seed=1234 + rank)
+    stream = torch.cuda.current_stream(device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+
+    for _ in range(args.warmup):
+        runner.launch(args.md_steps)
+    torch.cuda.synchronize(device)
+    runner.check()
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize(device)
+    with ClockSampler(device.index) as clocks:
+        for k in range(args.steps):
+            flush.fill_(float(k))  # 256 MB write: evicts L2 between timed launches
+            starts[k].record(stream)
+            runner.launch(args.md_steps)
+            ends[k].record(stream)
+        torch.cuda.synchronize(device)
+    barrier()
+    runner.check()
+    per_launch_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    t_rank = sum(per_launch_ms) / 1e3
+    t = torch.tensor([t_rank], dtype=torch.float64, device=device)
+    if ws > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    t_max = float(t)
+    total_atom_steps = n_atoms * args.md_steps * args.steps * ws
+    value = total_atom_steps / t_max
+    avg_launch_s = statistics.mean(per_launch_ms) / 1e3
+
+    # ---- end to end through the C ABI with host buffers (pinned), copies timed
+    f64 = torch.float64
+    hx = md.positions.to(f64).cpu().pin_memory()
+    hp = md.momenta.to(f64).cpu().pin_memory()
+    hf = md.forces.to(f64).cpu().pin_memory()
+    ox = torch.empty_like(hx).pin_memory()
+    op = torch.empty_like(hp).pin_memory()
+    oe = torch.empty(md.n_systems, dtype=f64).pin_memory()
+    e2e_steps = max(2, min(args.steps, 5))
+    es = [torch.cuda.Event(enable_timing=True) for _ in range(e2e_steps)]
+    ee = [torch.cuda.Event(enable_timing=True) for _ in range(e2e_steps)]
+    barrier()
+    torch.cuda.synchronize(device)
+    for k in range(e2e_steps):
+        flush.fill_(float(k))
+        es[k].record(stream)
+        runner.x.copy_(hx, non_blocking=True)
+        runner.p.copy_(hp, non_blocking=True)
+        runner.f.copy_(hf, non_blocking=True)
+        runner.launch(args.md_steps)
+        ox.copy_(runner.x, non_blocking=True)
+        op.copy_(runner.p, non_blocking=True)
+        oe.copy_(runner.energy, non_blocking=True)
+        ee[k].record(stream)
+    torch.cuda.synchronize(device)
+    barrier()
+    runner.check()
+    te = torch.tensor([sum(s.elapsed_time(e) for s, e in zip(es, ee)) / 1e3],
+                      dtype=torch.float64, device=device)
+    if ws > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = n_atoms * args.md_steps * e2e_steps * ws / float(te)
+    h2d = 3 * hx.numel() * 8
+    d2h = 2 * hx.numel() * 8 + oe.numel() * 8
+
+    if rank == 0:
+        peak, peak_kind = measured_peak_hbm()
+        alg_bytes = n_atoms * args.md_steps * ALG_BYTES_PER_ATOM_STEP
+        achieved = alg_bytes / avg_launch_s / 1e9
+        traffic = profiled_traffic()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded Cu supercells)",
+            "config": {"workload": WORKLOAD, "n_systems": args.n_systems,
+                       "atoms_per_gpu": n_atoms, "md_steps_per_step": args.md_steps,
+                       "verlet_skin_A": SKIN, "precision": "FP32 pair math, FP64 state",
+                       "l2": "256 MB buffer written between timed launches",
+                       "parallelism": f"replicas x{ws} (independent systems per rank)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "algorithmic_bytes_per_atom_step": ALG_BYTES_PER_ATOM_STEP,
+                         "kernel": "k_fused_md"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": 2 * args.steps,
+            "clocks": clocks.summary(),
+            "per_launch_ms": per_launch_ms,
+        }
+        if not args.no_cpu_baseline and ws == 1:
+            line["cpu_baseline"] = cpu_baseline(d)
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -49,9 +49,9 @@ def _make(key, precision):
         alp = [[2.0, 3.0], [3.0, 2.0]] if key.endswith("int") else [[2.0, 2.5], [2.5, 3.0]]
         return models.SoftSphereMultiModel(
             atomic_numbers=torch.tensor([18, 36]),
-            sigma_matrix=torch.tensor([[2.6, 2.9], [2.9, 3.1]]),
-            epsilon_matrix=torch.tensor([[0.05, 0.07], [0.07, 0.04]]),
-            alpha_matrix=torch.tensor(alp), **kw)
+            sigma_matrix=torch.tensor([[2.6, 2.9], [2.9, 3.1]], dtype=torch.float64),
+            epsilon_matrix=torch.tensor([[0.05, 0.07], [0.07, 0.04]], dtype=torch.float64),
+            alpha_matrix=torch.tensor(alp, dtype=torch.float64), **kw)
     if key == "ka_lj":
         return models.kob_andersen_model(**kw)
     raise KeyError(key)

@@ -30,8 +30,9 @@ __global__ void __launch_bounds__(128)
   const SysGeom &G = b.geom[s];
   const int si = species ? min(max(species[i], 0), ns_species - 1) : 0;
   const PairPrm<R> *row = prm + si * ns_species;
-  R fx = 0, fy = 0, fz = 0, ei = 0;
-  R vxx = 0, vyy = 0, vzz = 0, vyz = 0, vxz = 0, vxy = 0;
+  // forces accumulate in R; energy and virial in FP64 (per-system sums in FP64)
+  R fx = 0, fy = 0, fz = 0;
+  double ei = 0, vxx = 0, vyy = 0, vzz = 0, vyz = 0, vxz = 0, vxy = 0;
   search_neighbors(G, b.spos, b.bin_start, i, w.x, w.y, w.z, cutoff * cutoff, false,
                    [&](int j, int, int, int, double dx, double dy, double dz, double) {
                      const int sj = species ? min(max(species[j], 0), ns_species - 1) : 0;
@@ -45,13 +46,13 @@ __global__ void __launch_bounds__(128)
                      fx -= gx;
                      fy -= gy;
                      fz -= gz;
-                     ei += e;
-                     vxx += rx * gx;
-                     vyy += ry * gy;
-                     vzz += rz * gz;
-                     vyz += ry * gz;
-                     vxz += rx * gz;
-                     vxy += rx * gy;
+                     ei += (double)e;
+                     vxx += (double)(rx * gx);
+                     vyy += (double)(ry * gy);
+                     vzz += (double)(rz * gz);
+                     vyz += (double)(ry * gz);
+                     vxz += (double)(rx * gz);
+                     vxy += (double)(rx * gy);
                    });
   if (flags & TSB_OUT_FORCES) {
     forces[3 * i] = (P)fx;
@@ -69,14 +70,14 @@ __global__ void __launch_bounds__(128)
     o[3] = (P)(c * vxy); o[4] = (P)(c * vyy); o[5] = (P)(c * vyz);
     o[6] = (P)(c * vxz); o[7] = (P)(c * vyz); o[8] = (P)(c * vzz);
   }
-  e_half[i] = 0.5 * (double)ei;
+  e_half[i] = 0.5 * ei;
   double *v = vir_half + 6 * i;
-  v[0] = 0.5 * (double)vxx;
-  v[1] = 0.5 * (double)vyy;
-  v[2] = 0.5 * (double)vzz;
-  v[3] = 0.5 * (double)vyz;
-  v[4] = 0.5 * (double)vxz;
-  v[5] = 0.5 * (double)vxy;
+  v[0] = 0.5 * vxx;
+  v[1] = 0.5 * vyy;
+  v[2] = 0.5 * vzz;
+  v[3] = 0.5 * vyz;
+  v[4] = 0.5 * vxz;
+  v[5] = 0.5 * vxy;
 }
 
 // One block per system, fixed-order tree reduction in FP64 (deterministic).

@@ -169,6 +169,89 @@ def _system_order(state):
     return order, max_atoms
 
 
+class FusedMD:
+    """Preallocated persistent fused-MD runner (no host synchronisation per launch).
+
+    Holds FP64 copies of positions/momenta/forces and every buffer the C ABI
+    needs, so :meth:`launch` is a single ``tsb_fused_md`` call that can be
+    timed, overlapped or replayed; :meth:`check` synchronises and raises on a
+    device-reported failure; :meth:`write_back` copies the results into the
+    state.
+    """
+
+    def __init__(self, state, model, *, integrator: str = "nvt_langevin", dt, kT=None,
+                 gamma=None, skin: float = 1.0, seed: int | None = None):
+        from .models.pair_potential import PairTableModel
+
+        if not isinstance(model, PairTableModel):
+            raise TypeError("the fused path needs a tsb PairTableModel (LJ / Morse / soft sphere)")
+        self.integ = {"nve": L.INT_NVE, "nvt_langevin": L.INT_LANGEVIN}[integrator]
+        L.require_cuda(state.positions, "state.positions")
+        if not bool(torch.as_tensor(state.pbc).all()):
+            raise FusedMDError("the fused path requires periodic boundaries on all axes")
+        self.state, self.model = state, model
+        dev = self.dev = state.device
+        self.n, self.n_sys = state.n_atoms, state.n_systems
+        self.order, max_atoms = _system_order(state)
+        self.lib = L.load()
+        if max_atoms > self.lib.tsb_fused_max_atoms():
+            raise FusedMDError(f"systems with {max_atoms} atoms exceed the fused-kernel "
+                               f"limit of {self.lib.tsb_fused_max_atoms()}")
+        self.dt_s = _per_system(dt, self.n_sys, dev)
+        if self.integ == L.INT_LANGEVIN:
+            if kT is None:
+                raise ValueError("kT is required for nvt_langevin")
+            self.kT_s = _per_system(kT, self.n_sys, dev)
+            if gamma is None:
+                gamma = 1.0 / (100.0 * torch.as_tensor(dt, dtype=torch.float64))
+            self.g_s = _per_system(gamma, self.n_sys, dev)
+        else:
+            self.kT_s = self.g_s = None
+        f64 = torch.float64
+        self.x = state.positions.to(f64).contiguous().clone()
+        self.p = state.momenta.to(f64).contiguous().clone()
+        self.f = state.forces.to(f64).contiguous().clone()
+        self.m = state.masses.to(f64).contiguous()
+        self.cell_row = state.cell.mT.to(f64).contiguous()
+        self.sys_idx = state.system_idx.contiguous()
+        self.species = model._species(state.atomic_numbers)
+        self.table = model.table if model.table.device == dev else model.table.to(dev)
+        self.energy = torch.zeros(self.n_sys, dtype=f64, device=dev)
+        self.rebuilds = torch.zeros(self.n_sys, dtype=torch.int32, device=dev)
+        self.status = torch.zeros(2, dtype=torch.int32, device=dev)
+        self.ws = torch.empty(self.lib.tsb_fused_workspace_size(self.n, self.n_sys),
+                              dtype=torch.uint8, device=dev)
+        self.skin = float(skin)
+        self.seed = (seed if seed is not None
+                     else getattr(state, "_philox_seed", _seed_of(state))) & (2**64 - 1)
+        self.counter = getattr(state, "_philox_counter", 0)
+
+    def launch(self, n_steps: int, stream: int | None = None) -> None:
+        m = self.model
+        L.call("tsb_fused_md", self.integ, m.kind, L.ptr(self.table), m.n_species,
+               L.ptr(self.species), L.ptr(self.x), L.ptr(self.p), L.ptr(self.f), L.ptr(self.m),
+               L.ptr(self.cell_row), L.ptr(self.sys_idx), self.n, self.n_sys,
+               L.ptr(self.order), m.cutoff, self.skin, int(n_steps), L.ptr(self.dt_s),
+               L.ptr(self.kT_s), L.ptr(self.g_s), self.seed, self.counter, L.ptr(self.energy),
+               L.ptr(self.rebuilds), L.ptr(self.status), L.ptr(self.ws), self.ws.numel(),
+               stream if stream is not None else L.stream_ptr(self.dev))
+        self.counter += int(n_steps)
+
+    def check(self) -> None:
+        st = self.status.tolist()
+        if st[0] != 0:
+            raise FusedMDError(f"fused MD: system {st[1]}: {L.status_string(st[0])}")
+
+    def write_back(self):
+        s = self.state
+        dt_in = s.positions.dtype
+        cast = (lambda t: t.clone()) if dt_in == torch.float64 else (lambda t: t.to(dt_in))
+        s.positions, s.momenta, s.forces = cast(self.x), cast(self.p), cast(self.f)
+        s.energy = cast(self.energy)
+        s._philox_seed, s._philox_counter = self.seed, self.counter
+        return s
+
+
 def run_md(state, model, n_steps: int, *, integrator: str = "nvt_langevin", dt, kT=None,
            gamma=None, skin: float = 1.0, seed: int | None = None, check: bool = True,
            return_rebuilds: bool = False):
@@ -182,62 +265,12 @@ def run_md(state, model, n_steps: int, *, integrator: str = "nvt_langevin", dt, 
     ``tsb_fused_max_atoms()`` (512) atoms.  ``state`` is updated in place
     (positions, momenta, forces, energy).
     """
-    from .models.pair_potential import PairTableModel
-
-    if not isinstance(model, PairTableModel):
-        raise TypeError("run_md needs a tsb PairTableModel (LJ / Morse / soft sphere)")
-    integ = {"nve": L.INT_NVE, "nvt_langevin": L.INT_LANGEVIN}[integrator]
-    L.require_cuda(state.positions, "state.positions")
-    if not bool(torch.as_tensor(state.pbc).all()):
-        raise FusedMDError("run_md requires periodic boundaries on all axes")
-    dev = state.device
-    n, n_sys = state.n_atoms, state.n_systems
-    order, max_atoms = _system_order(state)
-    lib = L.load()
-    if max_atoms > lib.tsb_fused_max_atoms():
-        raise FusedMDError(f"systems with {max_atoms} atoms exceed the fused-kernel limit "
-                           f"of {lib.tsb_fused_max_atoms()}")
-    dt_s = _per_system(dt, n_sys, dev)
-    if integ == L.INT_LANGEVIN:
-        if kT is None:
-            raise ValueError("kT is required for nvt_langevin")
-        kT_s = _per_system(kT, n_sys, dev)
-        if gamma is None:
-            gamma = 1.0 / (100.0 * torch.as_tensor(dt, dtype=torch.float64))
-        g_s = _per_system(gamma, n_sys, dev)
-    else:
-        kT_s = g_s = None
-    f64 = torch.float64
-    x = state.positions.to(f64).contiguous()
-    p = state.momenta.to(f64).contiguous()
-    f = state.forces.to(f64).contiguous()
-    m = state.masses.to(f64).contiguous()
-    cell_row = state.cell.mT.to(f64).contiguous()
-    sys_idx = state.system_idx.contiguous()
-    species = model._species(state.atomic_numbers)
-    table = model.table if model.table.device == dev else model.table.to(dev)
-    energy = torch.empty(n_sys, dtype=f64, device=dev)
-    rebuilds = torch.zeros(n_sys, dtype=torch.int32, device=dev)
-    status = torch.zeros(2, dtype=torch.int32, device=dev)
-    ws = L.Workspace.get(dev, lib.tsb_fused_workspace_size(n, n_sys))
-    if seed is None:
-        seed = getattr(state, "_philox_seed", _seed_of(state))
-    counter = getattr(state, "_philox_counter", 0)
-    L.call("tsb_fused_md", integ, model.kind, L.ptr(table), model.n_species, L.ptr(species),
-           L.ptr(x), L.ptr(p), L.ptr(f), L.ptr(m), L.ptr(cell_row), L.ptr(sys_idx), n, n_sys,
-           L.ptr(order), model.cutoff, float(skin), int(n_steps), L.ptr(dt_s), L.ptr(kT_s),
-           L.ptr(g_s), seed & (2**64 - 1), counter, L.ptr(energy), L.ptr(rebuilds),
-           L.ptr(status), L.ptr(ws), ws.numel(), L.stream_ptr(dev))
+    r = FusedMD(state, model, integrator=integrator, dt=dt, kT=kT, gamma=gamma, skin=skin,
+                seed=seed)
+    r.launch(n_steps)
     if check:
-        st = status.tolist()
-        if st[0] != 0:
-            raise FusedMDError(f"fused MD: system {st[1]}: {L.status_string(st[0])}")
-    dt_in = state.positions.dtype
-    state.positions = x if dt_in == f64 else x.to(dt_in)
-    state.momenta = p if dt_in == f64 else p.to(dt_in)
-    state.forces = f if dt_in == f64 else f.to(dt_in)
-    state.energy = energy if dt_in == f64 else energy.to(dt_in)
-    state._philox_seed, state._philox_counter = seed, counter + int(n_steps)
+        r.check()
+    r.write_back()
     if return_rebuilds:
-        return state, rebuilds
+        return state, r.rebuilds
     return state
