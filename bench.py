@@ -40,7 +40,7 @@ WORKLOAD = ("2048 Cu fcc systems (8-512 atoms, strain +-2%, shear +-3deg), Morse
             "(D=0.3429 eV, alpha=1.3588/A, r0=2.866 A, rc=6.0 A), NVT-Langevin BAOAB "
             "1000 K, dt=2 fs, gamma=0.01/fs")
 ALG_BYTES_PER_ATOM_STEP = 76  # streaming state r/w: 48 B FP64 pos + 24 B mom + 4 B type/mass
-SKIN = 1.0
+SKIN = 0.7  # Verlet skin (A): list capacity sized for rc + skin = 6.7 A
 
 
 def parse():
@@ -263,6 +263,8 @@ def main():
         torch.cuda.synchronize(device)
     barrier()
     runner.check()
+    rebuilds = runner.rebuilds.double()
+    rebuild_interval = args.md_steps / max(float(rebuilds.mean()), 1e-9)
     per_launch_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     t_rank = sum(per_launch_ms) / 1e3
     t = torch.tensor([t_rank], dtype=torch.float64, device=device)
@@ -322,6 +324,7 @@ def main():
             "config": {"workload": WORKLOAD, "n_systems": args.n_systems,
                        "atoms_per_gpu": n_atoms, "md_steps_per_step": args.md_steps,
                        "verlet_skin_A": SKIN, "precision": "FP32 pair math, FP64 state",
+                       "mean_steps_between_list_rebuilds": rebuild_interval,
                        "l2": "256 MB buffer written between timed launches",
                        "parallelism": f"replicas x{ws} (independent systems per rank)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

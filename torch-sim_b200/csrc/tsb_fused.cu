@@ -11,21 +11,20 @@
 // Design (B200, sm_100a):
 //   * One CTA (512 threads) owns one system at a time and runs all n_steps for
 //     it before taking the next system from a global work counter (systems are
-//     independent; no grid-wide synchronisation, no host round trips).
-//   * Shared memory holds the system's atoms and the periodic images ("ghosts")
-//     that lie within cutoff+skin of the cell, as float4 (x, y, z, species) in
-//     cell-centre-relative FP32 coordinates, plus FP64 copies of the positions.
-//     FP64 master positions/momenta live in registers of the owning threads.
-//   * The Verlet list (cutoff + skin) is an ELL table of uint16 indices into the
-//     atom+ghost array in per-CTA global scratch; it is written and read only by
-//     the owning thread, so it stays in L1/L2.  It is rebuilt on the device when
-//     any atom moved more than skin/2 since the last build.
-//   * Small systems use 2..16 threads per atom (lanes split the neighbour list
-//     and reduce with warp shuffles), so a 512-thread CTA stays busy for any
-//     system size.  Summation orders are fixed: results are deterministic and a
-//     system's trajectory does not depend on the rest of the batch.
-//   * Pair arithmetic is FP32; positions, momenta and the per-system energy are
-//     FP64.
+//     independent: no grid-wide synchronisation, no host round trips).
+//   * Everything the step loop touches lives in shared memory: the system's
+//     atoms and the periodic images ("ghosts") within cutoff+skin of the cell as
+//     float4 (x, y, z, species) in cell-centre-relative FP32 coordinates, FP64
+//     copies of the positions for refreshing the ghosts, and the Verlet list
+//     (cutoff + skin) as a uint16 ELL table [slot group][thread] that each thread
+//     reads four entries per 64-bit load.  FP64 positions/momenta live in the
+//     registers of the owning threads.
+//   * The list is rebuilt on the device when any atom of the system moved more
+//     than skin/2 since the last build.
+//   * Small systems use 2..32 threads per atom (lanes split the list and reduce
+//     with warp shuffles).  Summation orders are fixed: results are
+//     deterministic and a system's trajectory does not depend on the batch.
+//   * Pair arithmetic FP32; positions, momenta and per-system energy FP64.
 #include <math.h>
 
 #include "tsb_pair.cuh"
@@ -35,13 +34,17 @@ namespace tsb {
 
 constexpr int kFusedThreads = 512;
 constexpr int kFusedMaxAtoms = 512;
-constexpr int kExtMax = 4096;   // atoms + ghost images per system
-constexpr int kListLen = 192;   // Verlet-list slots per thread
-constexpr int kMaxGrid = 296;   // upper bound on persistent CTAs (scratch sizing)
-constexpr size_t kFusedSmem = (size_t)kExtMax * sizeof(float4) +      // ext
-                              (size_t)kExtMax * sizeof(uint32_t) +    // ghost records
-                              (size_t)kFusedMaxAtoms * 3 * sizeof(double) +  // xd
-                              (size_t)kFusedMaxAtoms * sizeof(int4);  // wrap
+constexpr int kExtMax = 3328;        // atoms + ghost images per system
+constexpr int kListLen = 136;        // Verlet-list slots per thread (multiple of 4)
+constexpr int kListGroups = kListLen / 4;
+constexpr int kFusedMaxSpecies = 4;
+constexpr int kMaxGrid = 296;        // upper bound on persistent CTAs
+constexpr size_t kSmemList = (size_t)kListGroups * kFusedThreads * sizeof(uint2);
+constexpr size_t kSmemExt = (size_t)kExtMax * sizeof(float4);
+constexpr size_t kSmemGhost = (size_t)kExtMax * sizeof(uint32_t);
+constexpr size_t kSmemXd = (size_t)kFusedMaxAtoms * 3 * sizeof(double);
+constexpr size_t kSmemWrap = (size_t)kFusedMaxAtoms * sizeof(short4);
+constexpr size_t kFusedSmem = kSmemList + kSmemExt + kSmemGhost + kSmemXd + kSmemWrap;
 
 struct FusedArgs {
   int integrator, potential, n_species;
@@ -59,13 +62,35 @@ struct FusedArgs {
   uint64_t seed, counter;
   double *energy;
   int32_t *n_rebuilds;
-  uint16_t *lists;
   int32_t *queue;
   int32_t *status;
 };
 
-__device__ inline int64_t block_excl_scan_i(int v, int *total, int *sh) {
-  // sh: >= 32 ints
+// per-system geometry, computed once by thread 0 into shared memory
+struct FusedGeom {
+  double C[9];    // row-vector cell
+  double T[9];    // inv(C)^T: fractional coordinates u = T r
+  double ctr[3];  // cell centre
+  double h[3];    // (cutoff + skin) * |row k of T|
+  int rep[3];
+  int n, tpa, ok;
+  int64_t start;
+};
+
+struct Smem {
+  uint2 *list;
+  float4 *ext;
+  uint32_t *ghost;
+  double *xd;
+  short4 *wrap;
+};
+
+__device__ inline void report(int32_t *status, int code, int64_t sys) {
+  if (atomicCAS(status, 0, code) == 0) status[1] = (int32_t)sys;
+}
+
+// Block-wide exclusive scan of one int per thread (512 threads).
+__device__ inline int block_excl_scan_i(int v, int *total, int *sh) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int inc = v;
 #pragma unroll
@@ -76,7 +101,7 @@ __device__ inline int64_t block_excl_scan_i(int v, int *total, int *sh) {
   if (lane == 31) sh[warp] = inc;
   __syncthreads();
   if (warp == 0) {
-    const int nw = blockDim.x >> 5;
+    const int nw = kFusedThreads / 32;
     int w = lane < nw ? sh[lane] : 0;
     int wi = w;
 #pragma unroll
@@ -94,18 +119,66 @@ __device__ inline int64_t block_excl_scan_i(int v, int *total, int *sh) {
   return r;
 }
 
-__device__ inline void report(int32_t *status, int code, int64_t sys) {
-  if (atomicCAS(status, 0, code) == 0) status[1] = (int32_t)sys;
+// FP32 standard normals for the O-step (Philox4x32-10 + Box-Muller).
+__device__ inline void normal3f(uint64_t seed, uint64_t atom, uint64_t counter, float *z) {
+  U4 c{(uint32_t)atom, (uint32_t)(atom >> 32), (uint32_t)counter, (uint32_t)(counter >> 32)};
+  U4 r = philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+  const float k24 = 5.9604644775390625e-8f;  // 2^-24
+  const float u1 = (float)((r.x >> 8) + 1u) * k24;  // (0, 1]
+  const float u2 = (float)((r.z >> 8) + 1u) * k24;
+  const float r1 = sqrtf(-2.0f * logf(u1));
+  const float r2 = sqrtf(-2.0f * logf(u2));
+  float s1, c1, s2, c2;
+  sincospif((float)(r.y >> 8) * (2.0f * k24), &s1, &c1);
+  sincospif((float)(r.w >> 8) * (2.0f * k24), &s2, &c2);
+  z[0] = r1 * c1;
+  z[1] = r1 * s1;
+  z[2] = r2 * c2;
+  (void)s2;
 }
 
+__device__ __forceinline__ float4 make_ext(const FusedGeom &g, double x0, double x1, double x2,
+                                           int ex, int ey, int ez, int sp) {
+  // position x + (ex, ey, ez) @ C relative to the cell centre, rounded to FP32
+  float4 e;
+  e.x = (float)(x0 + (ex * g.C[0] + ey * g.C[3] + ez * g.C[6]) - g.ctr[0]);
+  e.y = (float)(x1 + (ex * g.C[1] + ey * g.C[4] + ez * g.C[7]) - g.ctr[1]);
+  e.z = (float)(x2 + (ex * g.C[2] + ey * g.C[5] + ez * g.C[8]) - g.ctr[2]);
+  e.w = __int_as_float(sp);
+  return e;
+}
+
+__device__ __forceinline__ bool in_margin(const FusedGeom &g, double f, int k) {
+  return f >= -g.h[k] && f < 1.0 + g.h[k];
+}
+
+// Fast FP32 pair evaluation for the fused kernel (exp via ex2.approx).
 template <int POT>
+__device__ __forceinline__ void pair_eval_fast(const PairPrm<float> &q, float r2, float &e,
+                                               float &fr) {
+  if (POT == TSB_POT_MORSE) {
+    const float ir = rsqrtf(r2);
+    const float r = r2 * ir;
+    const float ex = __expf(-q.a2 * (r - q.a0));
+    const float om = 1.0f - ex;
+    e = q.a1 * om * om - q.a1 - q.a4;
+    fr = -q.a5 * ex * om * ir;
+  } else {
+    pair_eval<POT, float>(q, r2, e, fr);
+  }
+}
+
+template <int POT, bool MULTI>
 __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
-  float4 *ext = (float4 *)smem;
-  uint32_t *ghost = (uint32_t *)(ext + kExtMax);
-  double *xd = (double *)(ghost + kExtMax);
-  int4 *wrapW = (int4 *)(xd + 3 * kFusedMaxAtoms);
-  __shared__ PairPrm<float> prm[kMaxSpecies * kMaxSpecies];
+  Smem S;
+  S.list = (uint2 *)smem;
+  S.ext = (float4 *)(smem + kSmemList);
+  S.ghost = (uint32_t *)(smem + kSmemList + kSmemExt);
+  S.xd = (double *)(smem + kSmemList + kSmemExt + kSmemGhost);
+  S.wrap = (short4 *)(smem + kSmemList + kSmemExt + kSmemGhost + kSmemXd);
+  __shared__ FusedGeom g;
+  __shared__ PairPrm<float> prm[kFusedMaxSpecies * kFusedMaxSpecies];
   __shared__ int s_scan[33];
   __shared__ int s_work;
   __shared__ double s_red[kFusedThreads / 32];
@@ -113,10 +186,12 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
   const int tid = threadIdx.x;
   for (int k = tid; k < A.n_species * A.n_species; k += blockDim.x)
     prm[k] = make_prm<float>(POT, A.table + 5 * k, A.cutoff);
-  uint16_t *mylist = A.lists + (size_t)blockIdx.x * kListLen * kFusedThreads;
+  __syncthreads();
+  const PairPrm<float> p0 = prm[0];  // single-species parameters in registers
   const double rcs = A.cutoff + A.skin;
   const float rcs2_build = (float)(rcs * rcs) * (1.0f + 1e-5f);
-  const double half_skin2 = 0.25 * A.skin * A.skin;
+  const float half_skin2 = (float)(0.25 * A.skin * A.skin);
+  uint16_t *list16 = (uint16_t *)S.list;
 
   for (;;) {
     __syncthreads();
@@ -125,27 +200,15 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     const int64_t w = s_work;
     if (w >= A.n_sys) break;
     const int64_t s = A.order ? A.order[w] : w;
-    const int64_t start = A.lo[s];
-    const int n = (int)(A.hi[s] - start);
-    if (n <= 0) {
-      if (tid == 0) {
-        A.energy[s] = 0.0;
-        if (A.n_rebuilds) A.n_rebuilds[s] = 0;
-      }
-      continue;
-    }
-    if (n > kFusedMaxAtoms) {
-      if (tid == 0) report(A.status, TSB_ERR_UNSUPPORTED, s);
-      continue;
-    }
-    // ---- per-system geometry (every thread, FP64) ----
-    double C[9], T[9], h[3], ctr[3];
-    for (int k = 0; k < 9; ++k) C[k] = A.cell_row[9 * s + k];
-    {
+    if (tid == 0) {
+      g.start = A.lo[s];
+      g.n = (int)(A.hi[s] - g.start);
+      g.ok = 1;
+      double *C = g.C, *T = g.T;
+      for (int k = 0; k < 9; ++k) C[k] = A.cell_row[9 * s + k];
       const double d = C[0] * (C[4] * C[8] - C[5] * C[7]) - C[1] * (C[3] * C[8] - C[5] * C[6]) +
                        C[2] * (C[3] * C[7] - C[4] * C[6]);
       const double id = 1.0 / d;
-      // T = inv(C)^T: fractional coordinates u = T r
       T[0] = (C[4] * C[8] - C[5] * C[7]) * id;
       T[3] = (C[2] * C[7] - C[1] * C[8]) * id;
       T[6] = (C[1] * C[5] - C[2] * C[4]) * id;
@@ -155,253 +218,282 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       T[2] = (C[3] * C[7] - C[4] * C[6]) * id;
       T[5] = (C[1] * C[6] - C[0] * C[7]) * id;
       T[8] = (C[0] * C[4] - C[1] * C[3]) * id;
+      for (int k = 0; k < 3; ++k) {
+        g.h[k] = rcs * sqrt(T[3 * k] * T[3 * k] + T[3 * k + 1] * T[3 * k + 1] +
+                            T[3 * k + 2] * T[3 * k + 2]) * (1.0 + 1e-9);
+        g.rep[k] = (int)ceil(g.h[k]);
+        g.ctr[k] = 0.5 * (C[k] + C[3 + k] + C[6 + k]);
+      }
+      int tpa = 1;
+      while (tpa < 32 && g.n * tpa * 2 <= kFusedThreads) tpa *= 2;
+      g.tpa = tpa;
+      if (g.n <= 0) {
+        g.ok = 0;
+        A.energy[s] = 0.0;
+        if (A.n_rebuilds) A.n_rebuilds[s] = 0;
+      } else if (g.n > kFusedMaxAtoms || g.rep[0] > 15 || g.rep[1] > 15 || g.rep[2] > 15 ||
+                 !isfinite(d)) {
+        g.ok = 0;
+        report(A.status, TSB_ERR_UNSUPPORTED, s);
+      }
     }
-    int rep[3];
-    for (int k = 0; k < 3; ++k) {
-      h[k] = rcs * sqrt(T[3 * k] * T[3 * k] + T[3 * k + 1] * T[3 * k + 1] +
-                        T[3 * k + 2] * T[3 * k + 2]) * (1.0 + 1e-9);
-      rep[k] = (int)ceil(h[k]);
-      ctr[k] = 0.5 * (C[k] + C[3 + k] + C[6 + k]);
-    }
-    if (rep[0] > 15 || rep[1] > 15 || rep[2] > 15) {
-      if (tid == 0) report(A.status, TSB_ERR_UNSUPPORTED, s);
-      continue;
-    }
-    int tpa = 1;
-    while (tpa < 32 && n * tpa * 2 <= kFusedThreads) tpa *= 2;
+    __syncthreads();
+    if (!g.ok) continue;
+    const int n = g.n, tpa = g.tpa;
     const int a = tid / tpa, lane = tid - a * tpa;
     const bool own = a < n;
     const bool lead = own && lane == 0;
-    const int64_t gi = start + a;
-    double x[3] = {0, 0, 0}, pm[3] = {0, 0, 0}, F[3] = {0, 0, 0}, xr[3] = {0, 0, 0};
-    double mass = 1.0;
+    const int64_t gi = g.start + a;
+    double x0 = 0, x1 = 0, x2 = 0, p0x = 0, p0y = 0, p0z = 0, inv_m = 1.0, c2m = 0.0;
+    float F0 = 0.f, F1 = 0.f, F2 = 0.f, xr0 = 0.f, xr1 = 0.f, xr2 = 0.f;
     int sp = 0;
     if (own) {
-      for (int k = 0; k < 3; ++k) {
-        x[k] = A.x[3 * gi + k];
-        pm[k] = A.p[3 * gi + k];
-        F[k] = A.f[3 * gi + k];
-      }
-      mass = A.m[gi];
+      x0 = A.x[3 * gi];
+      x1 = A.x[3 * gi + 1];
+      x2 = A.x[3 * gi + 2];
+      p0x = A.p[3 * gi];
+      p0y = A.p[3 * gi + 1];
+      p0z = A.p[3 * gi + 2];
+      F0 = (float)A.f[3 * gi];
+      F1 = (float)A.f[3 * gi + 1];
+      F2 = (float)A.f[3 * gi + 2];
+      const double mass = A.m[gi];
+      inv_m = 1.0 / mass;
       sp = A.species ? min(max(A.species[gi], 0), A.n_species - 1) : 0;
+      if (A.integrator == TSB_INT_LANGEVIN)
+        c2m = sqrt(A.kT[s] * (1.0 - exp(-2.0 * (A.gamma[s] * A.dt[s])))) * sqrt(mass);
     }
     const double dt = A.dt[s];
     const double half = dt / 2.0;
-    double c1 = 1.0, c2m = 0.0;
-    if (A.integrator == TSB_INT_LANGEVIN) {
-      c1 = exp(-(A.gamma[s] * dt));
-      c2m = sqrt(A.kT[s] * (1.0 - c1 * c1)) * sqrt(mass);
-    }
+    const double c1 = (A.integrator == TSB_INT_LANGEVIN) ? exp(-(A.gamma[s] * dt)) : 1.0;
     int Wx = 0, Wy = 0, Wz = 0;
     int n_ext = n, n_ghost = 0, cnt = 0, rebuilds = 0;
     bool failed = false;
     float ei = 0.0f;
 
-    // ---------------------------------------------------------------- rebuild
-    auto rebuild = [&]() {
-      int gcount = 0;
-      double f0 = 0, f1 = 0, f2 = 0;
-      if (own) {
-        const double u0 = T[0] * x[0] + T[1] * x[1] + T[2] * x[2];
-        const double u1 = T[3] * x[0] + T[4] * x[1] + T[5] * x[2];
-        const double u2 = T[6] * x[0] + T[7] * x[1] + T[8] * x[2];
-        const double w0 = floor(u0), w1 = floor(u1), w2 = floor(u2);
-        f0 = u0 - w0;
-        f1 = u1 - w1;
-        f2 = u2 - w2;
-        Wx = (int)w0;
-        Wy = (int)w1;
-        Wz = (int)w2;
-        for (int k = 0; k < 3; ++k) xr[k] = x[k];
-        if (lead) {
-          wrapW[a] = make_int4(Wx, Wy, Wz, 0);
-          for (int k = 0; k < 3; ++k) xd[3 * a + k] = x[k];
-          float4 e;
-          e.x = (float)(x[0] - (Wx * C[0] + Wy * C[3] + Wz * C[6]) - ctr[0]);
-          e.y = (float)(x[1] - (Wx * C[1] + Wy * C[4] + Wz * C[7]) - ctr[1]);
-          e.z = (float)(x[2] - (Wx * C[2] + Wy * C[5] + Wz * C[8]) - ctr[2]);
-          e.w = __int_as_float(sp);
-          ext[a] = e;
-          for (int sx = -rep[0]; sx <= rep[0]; ++sx) {
-            const double g0 = f0 + sx;
-            if (g0 < -h[0] || g0 >= 1.0 + h[0]) continue;
-            for (int sy = -rep[1]; sy <= rep[1]; ++sy) {
-              const double g1 = f1 + sy;
-              if (g1 < -h[1] || g1 >= 1.0 + h[1]) continue;
-              for (int sz = -rep[2]; sz <= rep[2]; ++sz) {
-                const double g2 = f2 + sz;
-                if (g2 < -h[2] || g2 >= 1.0 + h[2]) continue;
-                if ((sx | sy | sz) != 0) ++gcount;
-              }
-            }
-          }
-        }
-      }
-      int total;
-      int off = (int)block_excl_scan_i(gcount, &total, s_scan);
-      n_ghost = total;
-      n_ext = n + total;
-      if (n_ext > kExtMax) {
-        failed = true;
-        return;
-      }
-      if (lead && gcount) {
-        int g = n + off;
-        for (int sx = -rep[0]; sx <= rep[0]; ++sx) {
-          const double g0 = f0 + sx;
-          if (g0 < -h[0] || g0 >= 1.0 + h[0]) continue;
-          for (int sy = -rep[1]; sy <= rep[1]; ++sy) {
-            const double g1 = f1 + sy;
-            if (g1 < -h[1] || g1 >= 1.0 + h[1]) continue;
-            for (int sz = -rep[2]; sz <= rep[2]; ++sz) {
-              const double g2 = f2 + sz;
-              if (g2 < -h[2] || g2 >= 1.0 + h[2]) continue;
-              if ((sx | sy | sz) == 0) continue;
-              const int ex = sx - Wx, ey = sy - Wy, ez = sz - Wz;
-              float4 e;
-              e.x = (float)(x[0] + (ex * C[0] + ey * C[3] + ez * C[6]) - ctr[0]);
-              e.y = (float)(x[1] + (ex * C[1] + ey * C[4] + ez * C[7]) - ctr[1]);
-              e.z = (float)(x[2] + (ex * C[2] + ey * C[5] + ez * C[8]) - ctr[2]);
-              e.w = __int_as_float(sp);
-              ext[g] = e;
-              ghost[g - n] = (uint32_t)a | ((uint32_t)(sx & 31) << 16) |
-                             ((uint32_t)(sy & 31) << 21) | ((uint32_t)(sz & 31) << 26);
-              ++g;
-            }
-          }
-        }
-      }
-      __syncthreads();
-      cnt = 0;
-      if (own) {
-        const float4 xi = ext[a];
-        for (int e = lane; e < n_ext; e += tpa) {
-          const float4 q = ext[e];
-          const float dx = q.x - xi.x, dy = q.y - xi.y, dz = q.z - xi.z;
-          const float d2 = dx * dx + dy * dy + dz * dz;
-          if (d2 < rcs2_build && e != a) {
-            if (cnt < kListLen) mylist[(size_t)cnt * kFusedThreads + tid] = (uint16_t)e;
-            ++cnt;
-          }
-        }
-      }
-      if (__syncthreads_or(cnt > kListLen)) failed = true;
-      ++rebuilds;
-    };
+    // ------------------------------------------------------------- rebuild
+#define TSB_REBUILD()                                                                        \
+  {                                                                                          \
+    int gcount = 0;                                                                          \
+    double f0 = 0, f1 = 0, f2 = 0;                                                           \
+    if (own) {                                                                               \
+      const double u0 = g.T[0] * x0 + g.T[1] * x1 + g.T[2] * x2;                             \
+      const double u1 = g.T[3] * x0 + g.T[4] * x1 + g.T[5] * x2;                             \
+      const double u2 = g.T[6] * x0 + g.T[7] * x1 + g.T[8] * x2;                             \
+      const double w0 = floor(u0), w1 = floor(u1), w2 = floor(u2);                           \
+      f0 = u0 - w0;                                                                          \
+      f1 = u1 - w1;                                                                          \
+      f2 = u2 - w2;                                                                          \
+      Wx = (int)fmin(fmax(w0, -30000.0), 30000.0);                                           \
+      Wy = (int)fmin(fmax(w1, -30000.0), 30000.0);                                           \
+      Wz = (int)fmin(fmax(w2, -30000.0), 30000.0);                                           \
+      xr0 = (float)x0;                                                                       \
+      xr1 = (float)x1;                                                                       \
+      xr2 = (float)x2;                                                                       \
+      if (lead) {                                                                            \
+        S.wrap[a] = make_short4((short)Wx, (short)Wy, (short)Wz, 0);                         \
+        S.xd[3 * a] = x0;                                                                    \
+        S.xd[3 * a + 1] = x1;                                                                \
+        S.xd[3 * a + 2] = x2;                                                                \
+        S.ext[a] = make_ext(g, x0, x1, x2, -Wx, -Wy, -Wz, sp);                               \
+        for (int sx = -g.rep[0]; sx <= g.rep[0]; ++sx) {                                     \
+          if (!in_margin(g, f0 + sx, 0)) continue;                                           \
+          for (int sy = -g.rep[1]; sy <= g.rep[1]; ++sy) {                                   \
+            if (!in_margin(g, f1 + sy, 1)) continue;                                         \
+            for (int sz = -g.rep[2]; sz <= g.rep[2]; ++sz) {                                 \
+              if (!in_margin(g, f2 + sz, 2)) continue;                                       \
+              if ((sx | sy | sz) != 0) ++gcount;                                             \
+            }                                                                                \
+          }                                                                                  \
+        }                                                                                    \
+      }                                                                                      \
+    }                                                                                        \
+    int total;                                                                               \
+    const int goff = block_excl_scan_i(gcount, &total, s_scan);                              \
+    n_ghost = total;                                                                         \
+    n_ext = n + total;                                                                       \
+    if (n_ext > kExtMax) {                                                                   \
+      failed = true;                                                                         \
+    } else {                                                                                 \
+      if (lead && gcount) {                                                                  \
+        int gg = n + goff;                                                                   \
+        for (int sx = -g.rep[0]; sx <= g.rep[0]; ++sx) {                                     \
+          if (!in_margin(g, f0 + sx, 0)) continue;                                           \
+          for (int sy = -g.rep[1]; sy <= g.rep[1]; ++sy) {                                   \
+            if (!in_margin(g, f1 + sy, 1)) continue;                                         \
+            for (int sz = -g.rep[2]; sz <= g.rep[2]; ++sz) {                                 \
+              if (!in_margin(g, f2 + sz, 2)) continue;                                       \
+              if ((sx | sy | sz) == 0) continue;                                             \
+              S.ext[gg] = make_ext(g, x0, x1, x2, sx - Wx, sy - Wy, sz - Wz, sp);            \
+              S.ghost[gg - n] = (uint32_t)a | ((uint32_t)(sx & 31) << 16) |                  \
+                                ((uint32_t)(sy & 31) << 21) | ((uint32_t)(sz & 31) << 26);   \
+              ++gg;                                                                          \
+            }                                                                                \
+          }                                                                                  \
+        }                                                                                    \
+      }                                                                                      \
+      __syncthreads();                                                                       \
+      cnt = 0;                                                                               \
+      if (own) {                                                                             \
+        const float4 xi = S.ext[a];                                                          \
+        for (int e = lane; e < n_ext; e += tpa) {                                            \
+          const float4 q = S.ext[e];                                                         \
+          const float dx = q.x - xi.x, dy = q.y - xi.y, dz = q.z - xi.z;                     \
+          const float d2 = dx * dx + dy * dy + dz * dz;                                      \
+          if (d2 < rcs2_build && e != a) {                                                   \
+            if (cnt < kListLen)                                                              \
+              list16[((size_t)(cnt >> 2) * kFusedThreads + tid) * 4 + (cnt & 3)] =           \
+                  (uint16_t)e;                                                               \
+            ++cnt;                                                                           \
+          }                                                                                  \
+        }                                                                                    \
+      }                                                                                      \
+      if (__syncthreads_or(cnt > kListLen)) failed = true;                                   \
+      ++rebuilds;                                                                            \
+    }                                                                                        \
+  }
 
-    // ------------------------------------------------- refresh positions only
-    auto refresh = [&]() {
-      if (lead) {
-        for (int k = 0; k < 3; ++k) xd[3 * a + k] = x[k];
-        float4 e;
-        e.x = (float)(x[0] - (Wx * C[0] + Wy * C[3] + Wz * C[6]) - ctr[0]);
-        e.y = (float)(x[1] - (Wx * C[1] + Wy * C[4] + Wz * C[7]) - ctr[1]);
-        e.z = (float)(x[2] - (Wx * C[2] + Wy * C[5] + Wz * C[8]) - ctr[2]);
-        e.w = __int_as_float(sp);
-        ext[a] = e;
-      }
-      __syncthreads();
-      for (int g = tid; g < n_ghost; g += blockDim.x) {
-        const uint32_t r = ghost[g];
-        const int src = (int)(r & 0xFFFFu);
-        const int sx = ((int)(r << 11)) >> 27;
-        const int sy = ((int)(r << 6)) >> 27;
-        const int sz = ((int)(r << 1)) >> 27;
-        const int4 W = wrapW[src];
-        const int ex = sx - W.x, ey = sy - W.y, ez = sz - W.z;
-        const double *xs = xd + 3 * src;
-        float4 e;
-        e.x = (float)(xs[0] + (ex * C[0] + ey * C[3] + ez * C[6]) - ctr[0]);
-        e.y = (float)(xs[1] + (ex * C[1] + ey * C[4] + ez * C[7]) - ctr[1]);
-        e.z = (float)(xs[2] + (ex * C[2] + ey * C[5] + ez * C[8]) - ctr[2]);
-        e.w = ext[src].w;
-        ext[n + g] = e;
-      }
-      __syncthreads();
-    };
+    // ----------------------------------------------- refresh positions only
+#define TSB_REFRESH()                                                                        \
+  {                                                                                          \
+    if (lead) {                                                                              \
+      S.xd[3 * a] = x0;                                                                      \
+      S.xd[3 * a + 1] = x1;                                                                  \
+      S.xd[3 * a + 2] = x2;                                                                  \
+      S.ext[a] = make_ext(g, x0, x1, x2, -Wx, -Wy, -Wz, sp);                                 \
+    }                                                                                        \
+    __syncthreads();                                                                         \
+    for (int gg = tid; gg < n_ghost; gg += kFusedThreads) {                                  \
+      const uint32_t r = S.ghost[gg];                                                        \
+      const int src = (int)(r & 0xFFFFu);                                                    \
+      const int sx = ((int)(r << 11)) >> 27;                                                 \
+      const int sy = ((int)(r << 6)) >> 27;                                                  \
+      const int sz = ((int)(r << 1)) >> 27;                                                  \
+      const short4 W = S.wrap[src];                                                          \
+      const double *xs = S.xd + 3 * src;                                                     \
+      S.ext[n + gg] = make_ext(g, xs[0], xs[1], xs[2], sx - W.x, sy - W.y, sz - W.z,         \
+                               __float_as_int(S.ext[src].w));                                \
+    }                                                                                        \
+    __syncthreads();                                                                         \
+  }
 
-    // ------------------------------------------------------------------ force
-    auto forces = [&]() {
-      float fx = 0.f, fy = 0.f, fz = 0.f, en = 0.f;
-      if (own) {
-        const float4 xi = ext[a];
-        const PairPrm<float> *row = prm + sp * A.n_species;
-        for (int k = 0; k < cnt; ++k) {
-          const int e = mylist[(size_t)k * kFusedThreads + tid];
-          const float4 q = ext[e];
-          const float rx = q.x - xi.x, ry = q.y - xi.y, rz = q.z - xi.z;
-          const float r2 = rx * rx + ry * ry + rz * rz;
-          const PairPrm<float> &pq = row[__float_as_int(q.w)];
-          if (r2 < pq.a3) {
-            float ep, fr;
-            pair_eval<POT, float>(pq, r2, ep, fr);
-            fx -= fr * rx;
-            fy -= fr * ry;
-            fz -= fr * rz;
-            en += ep;
-          }
-        }
-      }
-      // reduce over the tpa lanes of this atom (lanes are aligned inside a warp)
-      for (int o = 1; o < tpa; o <<= 1) {
-        fx += __shfl_xor_sync(0xffffffffu, fx, o);
-        fy += __shfl_xor_sync(0xffffffffu, fy, o);
-        fz += __shfl_xor_sync(0xffffffffu, fz, o);
-        en += __shfl_xor_sync(0xffffffffu, en, o);
-      }
-      F[0] = fx;
-      F[1] = fy;
-      F[2] = fz;
-      ei = en;
-    };
+    // --------------------------------------------------------------- forces
+#define TSB_PAIR(E)                                                                          \
+  {                                                                                          \
+    const float4 q = S.ext[E];                                                               \
+    const float rx = q.x - xi.x, ry = q.y - xi.y, rz = q.z - xi.z;                           \
+    const float r2 = rx * rx + ry * ry + rz * rz;                                            \
+    const PairPrm<float> &pq = MULTI ? row[__float_as_int(q.w)] : p0;                        \
+    if (r2 < pq.a3) {                                                                        \
+      float ep, fr;                                                                          \
+      pair_eval_fast<POT>(pq, r2, ep, fr);                                                   \
+      fx -= fr * rx;                                                                         \
+      fy -= fr * ry;                                                                         \
+      fz -= fr * rz;                                                                         \
+      en += ep;                                                                              \
+    }                                                                                        \
+  }
+#define TSB_FORCES()                                                                         \
+  {                                                                                          \
+    float fx = 0.f, fy = 0.f, fz = 0.f, en = 0.f;                                            \
+    if (own) {                                                                               \
+      const float4 xi = S.ext[a];                                                            \
+      const PairPrm<float> *row = prm + sp * A.n_species;                                    \
+      (void)row;                                                                             \
+      const int full = cnt >> 2;                                                             \
+      for (int k4 = 0; k4 < full; ++k4) {                                                    \
+        const uint2 ge = S.list[k4 * kFusedThreads + tid];                                   \
+        TSB_PAIR(ge.x & 0xFFFFu)                                                             \
+        TSB_PAIR(ge.x >> 16)                                                                 \
+        TSB_PAIR(ge.y & 0xFFFFu)                                                             \
+        TSB_PAIR(ge.y >> 16)                                                                 \
+      }                                                                                      \
+      const int rem = cnt & 3;                                                               \
+      if (rem) {                                                                             \
+        const uint2 ge = S.list[full * kFusedThreads + tid];                                 \
+        TSB_PAIR(ge.x & 0xFFFFu)                                                             \
+        if (rem > 1) TSB_PAIR(ge.x >> 16)                                                    \
+        if (rem > 2) TSB_PAIR(ge.y & 0xFFFFu)                                                \
+      }                                                                                      \
+    }                                                                                        \
+    for (int o = 1; o < tpa; o <<= 1) {                                                      \
+      fx += __shfl_xor_sync(0xffffffffu, fx, o);                                             \
+      fy += __shfl_xor_sync(0xffffffffu, fy, o);                                             \
+      fz += __shfl_xor_sync(0xffffffffu, fz, o);                                             \
+      en += __shfl_xor_sync(0xffffffffu, en, o);                                             \
+    }                                                                                        \
+    F0 = fx;                                                                                 \
+    F1 = fy;                                                                                 \
+    F2 = fz;                                                                                 \
+    ei = en;                                                                                 \
+  }
 
-    rebuild();
+    TSB_REBUILD()
     if (failed) {
       if (tid == 0) report(A.status, TSB_ERR_CAPACITY, s);
       continue;
     }
     for (int64_t step = 0; step < A.n_steps; ++step) {
       if (own) {
-        for (int k = 0; k < 3; ++k) pm[k] = pm[k] + F[k] * half;
+        p0x += F0 * half;
+        p0y += F1 * half;
+        p0z += F2 * half;
         if (A.integrator == TSB_INT_LANGEVIN) {
-          for (int k = 0; k < 3; ++k) x[k] = x[k] + (pm[k] / mass) * half;
-          double z[4];
-          normal4(A.seed, (uint64_t)gi, A.counter + (uint64_t)step, z);
-          for (int k = 0; k < 3; ++k) {
-            pm[k] = c1 * pm[k] + c2m * z[k];
-            x[k] = x[k] + (pm[k] / mass) * half;
-          }
+          x0 += (p0x * inv_m) * half;
+          x1 += (p0y * inv_m) * half;
+          x2 += (p0z * inv_m) * half;
+          float z[3];
+          normal3f(A.seed, (uint64_t)gi, A.counter + (uint64_t)step, z);
+          p0x = c1 * p0x + c2m * z[0];
+          p0y = c1 * p0y + c2m * z[1];
+          p0z = c1 * p0z + c2m * z[2];
+          x0 += (p0x * inv_m) * half;
+          x1 += (p0y * inv_m) * half;
+          x2 += (p0z * inv_m) * half;
         } else {
-          for (int k = 0; k < 3; ++k) x[k] = x[k] + (pm[k] / mass) * dt;
+          x0 += (p0x * inv_m) * dt;
+          x1 += (p0y * inv_m) * dt;
+          x2 += (p0z * inv_m) * dt;
         }
       }
       bool moved = false;
       if (own) {
-        const double d0 = x[0] - xr[0], d1 = x[1] - xr[1], d2 = x[2] - xr[2];
+        const float d0 = (float)x0 - xr0, d1 = (float)x1 - xr1, d2 = (float)x2 - xr2;
         moved = d0 * d0 + d1 * d1 + d2 * d2 > half_skin2;
       }
       if (__syncthreads_or(moved)) {
-        rebuild();
+        TSB_REBUILD()
         if (failed) break;
       } else {
-        refresh();
+        TSB_REFRESH()
       }
-      forces();
-      if (own)
-        for (int k = 0; k < 3; ++k) pm[k] = pm[k] + F[k] * half;
+      TSB_FORCES()
+      if (own) {
+        p0x += F0 * half;
+        p0y += F1 * half;
+        p0z += F2 * half;
+      }
     }
     if (failed) {
       if (tid == 0) report(A.status, TSB_ERR_CAPACITY, s);
       continue;
     }
-    if (A.n_steps == 0) forces();
+    if (A.n_steps == 0) TSB_FORCES()
+#undef TSB_FORCES
+#undef TSB_PAIR
+#undef TSB_REFRESH
+#undef TSB_REBUILD
     // ---- write back + FP64 energy reduction (each pair seen from both ends)
     if (lead) {
-      for (int k = 0; k < 3; ++k) {
-        A.x[3 * gi + k] = x[k];
-        A.p[3 * gi + k] = pm[k];
-        A.f[3 * gi + k] = F[k];
-      }
+      A.x[3 * gi] = x0;
+      A.x[3 * gi + 1] = x1;
+      A.x[3 * gi + 2] = x2;
+      A.p[3 * gi] = p0x;
+      A.p[3 * gi + 1] = p0y;
+      A.p[3 * gi + 2] = p0z;
+      A.f[3 * gi] = F0;
+      A.f[3 * gi + 1] = F1;
+      A.f[3 * gi + 2] = F2;
     }
     double ev = lead ? 0.5 * (double)ei : 0.0;
     for (int o = 16; o > 0; o >>= 1) ev += __shfl_xor_sync(0xffffffffu, ev, o);
@@ -424,10 +516,9 @@ extern "C" int tsb_fused_max_atoms(void) { return kFusedMaxAtoms; }
 
 extern "C" size_t tsb_fused_workspace_size(int64_t n_atoms, int64_t n_systems) {
   Carver c(nullptr, (size_t)-1);
-  c.take<int64_t>(n_systems);      // lo
-  c.take<int64_t>(n_systems);      // hi
-  c.take<int32_t>(4);              // queue
-  c.take<uint16_t>((int64_t)kMaxGrid * kListLen * kFusedThreads);
+  c.take<int64_t>(n_systems);  // lo
+  c.take<int64_t>(n_systems);  // hi
+  c.take<int32_t>(4);          // queue
   (void)n_atoms;
   return c.off + 256;
 }
@@ -438,6 +529,13 @@ __global__ void k_bounds_fused(const int64_t *sys, int64_t n, int64_t *lo, int64
   int64_t s = sys[i];
   if (i == 0 || sys[i - 1] != s) lo[s] = i;
   if (i == n - 1 || sys[i + 1] != s) hi[s] = i + 1;
+}
+
+template <int POT, bool MULTI>
+static void launch_fused(const FusedArgs &A, int64_t grid, cudaStream_t st) {
+  cudaFuncSetAttribute(k_fused_md<POT, MULTI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)kFusedSmem);
+  k_fused_md<POT, MULTI><<<(unsigned)grid, kFusedThreads, kFusedSmem, st>>>(A);
 }
 
 extern "C" int tsb_fused_md(int integrator, int potential, const double *table,
@@ -452,8 +550,8 @@ extern "C" int tsb_fused_md(int integrator, int potential, const double *table,
                             void *workspace, size_t workspace_bytes, void *stream) {
   if (integrator != TSB_INT_NVE && integrator != TSB_INT_LANGEVIN) return TSB_ERR_INVALID_ARG;
   if (potential < TSB_POT_LJ || potential > TSB_POT_SOFT) return TSB_ERR_INVALID_ARG;
-  if (n_species < 1 || n_species > kMaxSpecies || !table || (n_species > 1 && !species))
-    return TSB_ERR_INVALID_ARG;
+  if (n_species < 1 || !table || (n_species > 1 && !species)) return TSB_ERR_INVALID_ARG;
+  if (n_species > kFusedMaxSpecies) return TSB_ERR_UNSUPPORTED;
   if (n_atoms < 1 || n_systems < 1 || !(cutoff > 0.0) || !(skin >= 0.0) || n_steps < 0)
     return TSB_ERR_INVALID_ARG;
   if (!positions || !momenta || !forces || !masses || !cell_row || !system_idx || !dt_sys ||
@@ -464,7 +562,6 @@ extern "C" int tsb_fused_md(int integrator, int potential, const double *table,
   int64_t *lo = c.take<int64_t>(n_systems);
   int64_t *hi = c.take<int64_t>(n_systems);
   int32_t *queue = c.take<int32_t>(4);
-  uint16_t *lists = c.take<uint16_t>((int64_t)kMaxGrid * kListLen * kFusedThreads);
   if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   int dev = 0, n_sm = 148;
@@ -480,20 +577,17 @@ extern "C" int tsb_fused_md(int integrator, int potential, const double *table,
   k_bounds_fused<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, lo, hi);
   FusedArgs A{integrator, potential, n_species, table, species, positions, momenta, forces,
               masses, cell_row, lo, hi, n_systems, order, cutoff, skin, n_steps, dt_sys,
-              kT_sys, gamma_sys, seed, counter, energy, n_rebuilds, lists, queue, status};
-  const size_t smem = kFusedSmem;
-#define TSB_FUSED(POT)                                                                   \
-  cudaFuncSetAttribute(k_fused_md<POT>, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
-                       (int)smem);                                                       \
-  k_fused_md<POT><<<(unsigned)grid, kFusedThreads, smem, st>>>(A);
+              kT_sys, gamma_sys, seed, counter, energy, n_rebuilds, queue, status};
+  const bool multi = n_species > 1;
   if (potential == TSB_POT_LJ) {
-    TSB_FUSED(TSB_POT_LJ)
+    multi ? launch_fused<TSB_POT_LJ, true>(A, grid, st) : launch_fused<TSB_POT_LJ, false>(A, grid, st);
   } else if (potential == TSB_POT_MORSE) {
-    TSB_FUSED(TSB_POT_MORSE)
+    multi ? launch_fused<TSB_POT_MORSE, true>(A, grid, st)
+          : launch_fused<TSB_POT_MORSE, false>(A, grid, st);
   } else {
-    TSB_FUSED(TSB_POT_SOFT)
+    multi ? launch_fused<TSB_POT_SOFT, true>(A, grid, st)
+          : launch_fused<TSB_POT_SOFT, false>(A, grid, st);
   }
-#undef TSB_FUSED
   TSB_CHECK_LAUNCH();
   return TSB_OK;
 }
