@@ -131,9 +131,13 @@ int tsb_md_baoab_boa(void *positions, void *momenta, const void *forces,
  * positions/momenta/forces are float64 [N,3] in/out; energy [S] float64 out
  * (potential energy after the last step); n_rebuilds [S] int32 out (optional).
  * `order` [S] int32 (optional) is the order in which CTAs pick systems
- * (largest first balances the tail).  `status` [2] int32 device out: status[0]
- * is TSB_OK or TSB_ERR_CAPACITY / TSB_ERR_UNSUPPORTED for a system that did
- * not fit (that system is left unchanged), status[1] its index.
+ * (largest first balances the tail).  A system whose images or neighbours do
+ * not fit the shared-memory tables at the requested skin is rebuilt with a
+ * smaller skin (results are unchanged; only the rebuild rate grows).
+ * `status` [4] int32 device out: status[0] is TSB_OK, or TSB_ERR_CAPACITY /
+ * TSB_ERR_UNSUPPORTED for a system that does not fit even with zero skin
+ * (that system is left unchanged); status[1] its index, status[2] which table
+ * (1 images, 2 neighbour slots), status[3] the size that did not fit.
  * Requirements: pbc all true, n_atoms per system <= tsb_fused_max_atoms(). */
 int tsb_fused_max_atoms(void);
 size_t tsb_fused_workspace_size(int64_t n_atoms, int64_t n_systems);

@@ -193,3 +193,16 @@ def test_fused_rejects_unsupported():
                             forces=torch.zeros_like(st.positions))
     with pytest.raises(integrators.FusedMDError):
         integrators.run_md(md, m, 1, integrator="nve", dt=0.1)
+
+
+def test_fused_adaptive_skin_same_physics():
+    """A skin too large for the shared-memory tables is shrunk per system on the
+    device; the trajectory matches a run at a small skin to FP32 rounding."""
+    from tsb import integrators, workloads
+
+    md, m = _cu_state(12, seed=13, kT=600.0)
+    dt = 0.002 * workloads.METAL_TIME
+    a = integrators.run_md(md.clone(), m, 30, integrator="nve", dt=dt, skin=2.5)
+    b = integrators.run_md(md.clone(), m, 30, integrator="nve", dt=dt, skin=0.3)
+    np.testing.assert_allclose(a.positions.cpu(), b.positions.cpu(), atol=1e-5)
+    np.testing.assert_allclose(a.energy.cpu(), b.energy.cpu(), rtol=1e-5)

@@ -71,11 +71,24 @@ struct FusedGeom {
   double C[9];    // row-vector cell
   double T[9];    // inv(C)^T: fractional coordinates u = T r
   double ctr[3];  // cell centre
+  double tn[3];   // |row k of T|
   double h[3];    // (cutoff + skin) * |row k of T|
+  double skin;    // this system's current Verlet skin
   int rep[3];
   int n, tpa, ok;
   int64_t start;
 };
+
+// margins of the ghost region for the current skin (thread 0 only)
+__device__ inline bool set_margins(FusedGeom &g, double cutoff) {
+  bool ok = true;
+  for (int k = 0; k < 3; ++k) {
+    g.h[k] = (cutoff + g.skin) * g.tn[k] * (1.0 + 1e-9);
+    g.rep[k] = (int)ceil(g.h[k]);
+    ok = ok && g.rep[k] <= 15;
+  }
+  return ok;
+}
 
 struct Smem {
   uint2 *list;
@@ -85,8 +98,13 @@ struct Smem {
   short4 *wrap;
 };
 
-__device__ inline void report(int32_t *status, int code, int64_t sys) {
-  if (atomicCAS(status, 0, code) == 0) status[1] = (int32_t)sys;
+// status[0] = code, [1] = system, [2] = what (1 image slots, 2 list slots), [3] = size
+__device__ inline void report(int32_t *status, int code, int64_t sys, int what, int size) {
+  if (atomicCAS(status, 0, code) == 0) {
+    status[1] = (int32_t)sys;
+    status[2] = what;
+    status[3] = size;
+  }
 }
 
 // Block-wide exclusive scan of one int per thread (512 threads).
@@ -188,9 +206,6 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     prm[k] = make_prm<float>(POT, A.table + 5 * k, A.cutoff);
   __syncthreads();
   const PairPrm<float> p0 = prm[0];  // single-species parameters in registers
-  const double rcs = A.cutoff + A.skin;
-  const float rcs2_build = (float)(rcs * rcs) * (1.0f + 1e-5f);
-  const float half_skin2 = (float)(0.25 * A.skin * A.skin);
   uint16_t *list16 = (uint16_t *)S.list;
 
   for (;;) {
@@ -219,11 +234,12 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       T[5] = (C[1] * C[6] - C[0] * C[7]) * id;
       T[8] = (C[0] * C[4] - C[1] * C[3]) * id;
       for (int k = 0; k < 3; ++k) {
-        g.h[k] = rcs * sqrt(T[3 * k] * T[3 * k] + T[3 * k + 1] * T[3 * k + 1] +
-                            T[3 * k + 2] * T[3 * k + 2]) * (1.0 + 1e-9);
-        g.rep[k] = (int)ceil(g.h[k]);
+        g.tn[k] = sqrt(T[3 * k] * T[3 * k] + T[3 * k + 1] * T[3 * k + 1] +
+                       T[3 * k + 2] * T[3 * k + 2]);
         g.ctr[k] = 0.5 * (C[k] + C[3 + k] + C[6 + k]);
       }
+      g.skin = A.skin;
+      const bool rep_ok = set_margins(g, A.cutoff);
       int tpa = 1;
       while (tpa < 32 && g.n * tpa * 2 <= kFusedThreads) tpa *= 2;
       g.tpa = tpa;
@@ -231,10 +247,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
         g.ok = 0;
         A.energy[s] = 0.0;
         if (A.n_rebuilds) A.n_rebuilds[s] = 0;
-      } else if (g.n > kFusedMaxAtoms || g.rep[0] > 15 || g.rep[1] > 15 || g.rep[2] > 15 ||
-                 !isfinite(d)) {
+      } else if (g.n > kFusedMaxAtoms || !rep_ok || !isfinite(d)) {
         g.ok = 0;
-        report(A.status, TSB_ERR_UNSUPPORTED, s);
+        report(A.status, TSB_ERR_UNSUPPORTED, s, 0, g.n);
       }
     }
     __syncthreads();
@@ -270,10 +285,15 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     int n_ext = n, n_ghost = 0, cnt = 0, rebuilds = 0;
     bool failed = false;
     float ei = 0.0f;
+    float half_skin2 = 0.f;
 
     // ------------------------------------------------------------- rebuild
 #define TSB_REBUILD()                                                                        \
-  {                                                                                          \
+  for (;;) {                                                                                 \
+    const double rcs_ = A.cutoff + g.skin;                                                   \
+    const float rcs2_build = (float)(rcs_ * rcs_) * (1.0f + 1e-5f);                          \
+    half_skin2 = (float)(0.25 * g.skin * g.skin);                                            \
+    int over = 0, over_size = 0;                                                             \
     int gcount = 0;                                                                          \
     double f0 = 0, f1 = 0, f2 = 0;                                                           \
     if (own) {                                                                               \
@@ -313,7 +333,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     n_ghost = total;                                                                         \
     n_ext = n + total;                                                                       \
     if (n_ext > kExtMax) {                                                                   \
-      failed = true;                                                                         \
+      over = 1;                                                                              \
+      over_size = n_ext;                                                                     \
     } else {                                                                                 \
       if (lead && gcount) {                                                                  \
         int gg = n + goff;                                                                   \
@@ -348,9 +369,27 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
           }                                                                                  \
         }                                                                                    \
       }                                                                                      \
-      if (__syncthreads_or(cnt > kListLen)) failed = true;                                   \
-      ++rebuilds;                                                                            \
+      if (__syncthreads_or(cnt > kListLen)) {                                                \
+        over = 2;                                                                            \
+        over_size = kListLen;                                                                \
+      }                                                                                      \
     }                                                                                        \
+    ++rebuilds;                                                                              \
+    if (!over) break;                                                                        \
+    /* too many images / neighbours for this skin: shrink it (results unchanged) */          \
+    __syncthreads();                                                                         \
+    const bool zero_skin_ = g.skin == 0.0;                                                   \
+    __syncthreads();                                                                         \
+    if (zero_skin_) {                                                                        \
+      failed = true;                                                                         \
+      if (tid == 0) report(A.status, TSB_ERR_CAPACITY, s, over, over_size);                  \
+      break;                                                                                 \
+    }                                                                                        \
+    if (tid == 0) {                                                                          \
+      g.skin = g.skin > 0.05 ? 0.5 * g.skin : 0.0;                                           \
+      set_margins(g, A.cutoff);                                                              \
+    }                                                                                        \
+    __syncthreads();                                                                         \
   }
 
     // ----------------------------------------------- refresh positions only
@@ -429,10 +468,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
   }
 
     TSB_REBUILD()
-    if (failed) {
-      if (tid == 0) report(A.status, TSB_ERR_CAPACITY, s);
-      continue;
-    }
+    if (failed) continue;
     for (int64_t step = 0; step < A.n_steps; ++step) {
       if (own) {
         p0x += F0 * half;
@@ -474,10 +510,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
         p0z += F2 * half;
       }
     }
-    if (failed) {
-      if (tid == 0) report(A.status, TSB_ERR_CAPACITY, s);
-      continue;
-    }
+    if (failed) continue;
     if (A.n_steps == 0) TSB_FORCES()
 #undef TSB_FORCES
 #undef TSB_PAIR
@@ -573,7 +606,7 @@ extern "C" int tsb_fused_md(int integrator, int potential, const double *table,
   cudaMemsetAsync(lo, 0, sizeof(int64_t) * n_systems, st);
   cudaMemsetAsync(hi, 0, sizeof(int64_t) * n_systems, st);
   cudaMemsetAsync(queue, 0, sizeof(int32_t) * 4, st);
-  cudaMemsetAsync(status, 0, sizeof(int32_t) * 2, st);
+  cudaMemsetAsync(status, 0, sizeof(int32_t) * 4, st);
   k_bounds_fused<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, lo, hi);
   FusedArgs A{integrator, potential, n_species, table, species, positions, momenta, forces,
               masses, cell_row, lo, hi, n_systems, order, cutoff, skin, n_steps, dt_sys,

@@ -180,7 +180,7 @@ class FusedMD:
     """
 
     def __init__(self, state, model, *, integrator: str = "nvt_langevin", dt, kT=None,
-                 gamma=None, skin: float = 1.0, seed: int | None = None):
+                 gamma=None, skin: float = 0.7, seed: int | None = None):
         from .models.pair_potential import PairTableModel
 
         if not isinstance(model, PairTableModel):
@@ -218,7 +218,7 @@ class FusedMD:
         self.table = model.table if model.table.device == dev else model.table.to(dev)
         self.energy = torch.zeros(self.n_sys, dtype=f64, device=dev)
         self.rebuilds = torch.zeros(self.n_sys, dtype=torch.int32, device=dev)
-        self.status = torch.zeros(2, dtype=torch.int32, device=dev)
+        self.status = torch.zeros(4, dtype=torch.int32, device=dev)
         self.ws = torch.empty(self.lib.tsb_fused_workspace_size(self.n, self.n_sys),
                               dtype=torch.uint8, device=dev)
         self.skin = float(skin)
@@ -240,7 +240,9 @@ class FusedMD:
     def check(self) -> None:
         st = self.status.tolist()
         if st[0] != 0:
-            raise FusedMDError(f"fused MD: system {st[1]}: {L.status_string(st[0])}")
+            what = {1: "periodic images", 2: "neighbour slots"}.get(st[2], "atoms")
+            raise FusedMDError(f"fused MD: system {st[1]}: {L.status_string(st[0])} "
+                               f"({what}: {st[3]})")
 
     def write_back(self):
         s = self.state
@@ -253,7 +255,7 @@ class FusedMD:
 
 
 def run_md(state, model, n_steps: int, *, integrator: str = "nvt_langevin", dt, kT=None,
-           gamma=None, skin: float = 1.0, seed: int | None = None, check: bool = True,
+           gamma=None, skin: float = 0.7, seed: int | None = None, check: bool = True,
            return_rebuilds: bool = False):
     """Advance every system ``n_steps`` in ONE persistent kernel launch.
 
