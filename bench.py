@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--md-steps", type=int, default=500)
     ap.add_argument("--n-systems", type=int, default=2048)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--skin", type=float, default=SKIN)
     return ap.parse_args()
 
 
@@ -237,7 +238,7 @@ def main():
 
     runner = integrators.FusedMD(md, model, integrator="nvt_langevin",
                                  dt=0.002 * W.METAL_TIME, kT=1000 * W.KB_EV,
-                                 gamma=10.0 / W.METAL_TIME, skin=SKIN, seed=1234 + rank)
+                                 gamma=10.0 / W.METAL_TIME, skin=args.skin, seed=1234 + rank)
     stream = torch.cuda.current_stream(device)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
 
@@ -323,7 +324,7 @@ def main():
             "data": "synthetic (seeded Cu supercells)",
             "config": {"workload": WORKLOAD, "n_systems": args.n_systems,
                        "atoms_per_gpu": n_atoms, "md_steps_per_step": args.md_steps,
-                       "verlet_skin_A": SKIN, "precision": "FP32 pair math, FP64 state",
+                       "verlet_skin_A": args.skin, "precision": "FP32 pair math, FP64 state",
                        "mean_steps_between_list_rebuilds": rebuild_interval,
                        "l2": "256 MB buffer written between timed launches",
                        "parallelism": f"replicas x{ws} (independent systems per rank)"},

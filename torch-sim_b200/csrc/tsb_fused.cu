@@ -35,16 +35,14 @@ namespace tsb {
 constexpr int kFusedThreads = 512;
 constexpr int kFusedMaxAtoms = 512;
 constexpr int kExtMax = 3328;        // atoms + ghost images per system
-constexpr int kListLen = 136;        // Verlet-list slots per thread (multiple of 4)
+constexpr int kListLen = 152;        // Verlet-list slots per thread (multiple of 4)
 constexpr int kListGroups = kListLen / 4;
 constexpr int kFusedMaxSpecies = 4;
 constexpr int kMaxGrid = 296;        // upper bound on persistent CTAs
 constexpr size_t kSmemList = (size_t)kListGroups * kFusedThreads * sizeof(uint2);
 constexpr size_t kSmemExt = (size_t)kExtMax * sizeof(float4);
 constexpr size_t kSmemGhost = (size_t)kExtMax * sizeof(uint32_t);
-constexpr size_t kSmemXd = (size_t)kFusedMaxAtoms * 3 * sizeof(double);
-constexpr size_t kSmemWrap = (size_t)kFusedMaxAtoms * sizeof(short4);
-constexpr size_t kFusedSmem = kSmemList + kSmemExt + kSmemGhost + kSmemXd + kSmemWrap;
+constexpr size_t kFusedSmem = kSmemList + kSmemExt + kSmemGhost;
 
 struct FusedArgs {
   int integrator, potential, n_species;
@@ -89,14 +87,6 @@ __device__ inline bool set_margins(FusedGeom &g, double cutoff) {
   }
   return ok;
 }
-
-struct Smem {
-  uint2 *list;
-  float4 *ext;
-  uint32_t *ghost;
-  double *xd;
-  short4 *wrap;
-};
 
 // status[0] = code, [1] = system, [2] = what (1 image slots, 2 list slots), [3] = size
 __device__ inline void report(int32_t *status, int code, int64_t sys, int what, int size) {
@@ -189,12 +179,10 @@ __device__ __forceinline__ void pair_eval_fast(const PairPrm<float> &q, float r2
 template <int POT, bool MULTI>
 __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
-  Smem S;
-  S.list = (uint2 *)smem;
-  S.ext = (float4 *)(smem + kSmemList);
-  S.ghost = (uint32_t *)(smem + kSmemList + kSmemExt);
-  S.xd = (double *)(smem + kSmemList + kSmemExt + kSmemGhost);
-  S.wrap = (short4 *)(smem + kSmemList + kSmemExt + kSmemGhost + kSmemXd);
+  uint2 *s_list = (uint2 *)smem;
+  float4 *s_ext = (float4 *)(smem + kSmemList);
+  uint32_t *s_gshift = (uint32_t *)(smem + kSmemList + kSmemExt);
+  uint16_t *list16 = (uint16_t *)s_list;
   __shared__ FusedGeom g;
   __shared__ PairPrm<float> prm[kFusedMaxSpecies * kFusedMaxSpecies];
   __shared__ int s_scan[33];
@@ -206,7 +194,6 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     prm[k] = make_prm<float>(POT, A.table + 5 * k, A.cutoff);
   __syncthreads();
   const PairPrm<float> p0 = prm[0];  // single-species parameters in registers
-  uint16_t *list16 = (uint16_t *)S.list;
 
   for (;;) {
     __syncthreads();
@@ -259,16 +246,17 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     const bool own = a < n;
     const bool lead = own && lane == 0;
     const int64_t gi = g.start + a;
-    double x0 = 0, x1 = 0, x2 = 0, p0x = 0, p0y = 0, p0z = 0, inv_m = 1.0, c2m = 0.0;
+    // owner state (every lane of the atom holds an identical copy)
+    double x0 = 0, x1 = 0, x2 = 0, px = 0, py = 0, pz = 0, inv_m = 1.0, c2m = 0.0;
     float F0 = 0.f, F1 = 0.f, F2 = 0.f, xr0 = 0.f, xr1 = 0.f, xr2 = 0.f;
     int sp = 0;
     if (own) {
       x0 = A.x[3 * gi];
       x1 = A.x[3 * gi + 1];
       x2 = A.x[3 * gi + 2];
-      p0x = A.p[3 * gi];
-      p0y = A.p[3 * gi + 1];
-      p0z = A.p[3 * gi + 2];
+      px = A.p[3 * gi];
+      py = A.p[3 * gi + 1];
+      pz = A.p[3 * gi + 2];
       F0 = (float)A.f[3 * gi];
       F1 = (float)A.f[3 * gi + 1];
       F2 = (float)A.f[3 * gi + 2];
@@ -281,13 +269,16 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     const double dt = A.dt[s];
     const double half = dt / 2.0;
     const double c1 = (A.integrator == TSB_INT_LANGEVIN) ? exp(-(A.gamma[s] * dt)) : 1.0;
-    int Wx = 0, Wy = 0, Wz = 0;
-    int n_ext = n, n_ghost = 0, cnt = 0, rebuilds = 0;
+    int Wx = 0, Wy = 0, Wz = 0;        // integer wrap of the owned atom at the last build
+    int gbeg = 0, gcnt = 0;            // the owned atom's ghost slots [gbeg, gbeg + gcnt)
+    int cnt = 0, rebuilds = 0;
     bool failed = false;
-    float ei = 0.0f;
-    float half_skin2 = 0.f;
+    float ei = 0.0f, half_skin2 = 0.f;
 
     // ------------------------------------------------------------- rebuild
+    // Wrap the owned atom, create its periodic images inside the cutoff+skin
+    // margin of the cell, then every atom scans all atoms + images.  If the
+    // shared-memory tables overflow, the skin of this system is halved.
 #define TSB_REBUILD()                                                                        \
   for (;;) {                                                                                 \
     const double rcs_ = A.cutoff + g.skin;                                                   \
@@ -304,18 +295,14 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       f0 = u0 - w0;                                                                          \
       f1 = u1 - w1;                                                                          \
       f2 = u2 - w2;                                                                          \
-      Wx = (int)fmin(fmax(w0, -30000.0), 30000.0);                                           \
-      Wy = (int)fmin(fmax(w1, -30000.0), 30000.0);                                           \
-      Wz = (int)fmin(fmax(w2, -30000.0), 30000.0);                                           \
+      Wx = (int)fmin(fmax(w0, -1e8), 1e8);                                                   \
+      Wy = (int)fmin(fmax(w1, -1e8), 1e8);                                                   \
+      Wz = (int)fmin(fmax(w2, -1e8), 1e8);                                                   \
       xr0 = (float)x0;                                                                       \
       xr1 = (float)x1;                                                                       \
       xr2 = (float)x2;                                                                       \
       if (lead) {                                                                            \
-        S.wrap[a] = make_short4((short)Wx, (short)Wy, (short)Wz, 0);                         \
-        S.xd[3 * a] = x0;                                                                    \
-        S.xd[3 * a + 1] = x1;                                                                \
-        S.xd[3 * a + 2] = x2;                                                                \
-        S.ext[a] = make_ext(g, x0, x1, x2, -Wx, -Wy, -Wz, sp);                               \
+        s_ext[a] = make_ext(g, x0, x1, x2, -Wx, -Wy, -Wz, sp);                               \
         for (int sx = -g.rep[0]; sx <= g.rep[0]; ++sx) {                                     \
           if (!in_margin(g, f0 + sx, 0)) continue;                                           \
           for (int sy = -g.rep[1]; sy <= g.rep[1]; ++sy) {                                   \
@@ -330,14 +317,16 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     }                                                                                        \
     int total;                                                                               \
     const int goff = block_excl_scan_i(gcount, &total, s_scan);                              \
-    n_ghost = total;                                                                         \
-    n_ext = n + total;                                                                       \
+    /* broadcast the lead's ghost range to the other lanes of its atom */                    \
+    gbeg = __shfl_sync(0xffffffffu, n + goff, (threadIdx.x & 31) & ~(tpa - 1));              \
+    gcnt = __shfl_sync(0xffffffffu, gcount, (threadIdx.x & 31) & ~(tpa - 1));                \
+    const int n_ext = n + total;                                                             \
     if (n_ext > kExtMax) {                                                                   \
       over = 1;                                                                              \
       over_size = n_ext;                                                                     \
     } else {                                                                                 \
       if (lead && gcount) {                                                                  \
-        int gg = n + goff;                                                                   \
+        int gg = gbeg;                                                                       \
         for (int sx = -g.rep[0]; sx <= g.rep[0]; ++sx) {                                     \
           if (!in_margin(g, f0 + sx, 0)) continue;                                           \
           for (int sy = -g.rep[1]; sy <= g.rep[1]; ++sy) {                                   \
@@ -345,9 +334,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
             for (int sz = -g.rep[2]; sz <= g.rep[2]; ++sz) {                                 \
               if (!in_margin(g, f2 + sz, 2)) continue;                                       \
               if ((sx | sy | sz) == 0) continue;                                             \
-              S.ext[gg] = make_ext(g, x0, x1, x2, sx - Wx, sy - Wy, sz - Wz, sp);            \
-              S.ghost[gg - n] = (uint32_t)a | ((uint32_t)(sx & 31) << 16) |                  \
-                                ((uint32_t)(sy & 31) << 21) | ((uint32_t)(sz & 31) << 26);   \
+              s_ext[gg] = make_ext(g, x0, x1, x2, sx - Wx, sy - Wy, sz - Wz, sp);            \
+              s_gshift[gg - n] = ((uint32_t)(sx & 1023)) | ((uint32_t)(sy & 1023) << 10) |   \
+                                 ((uint32_t)(sz & 1023) << 20);                              \
               ++gg;                                                                          \
             }                                                                                \
           }                                                                                  \
@@ -356,9 +345,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       __syncthreads();                                                                       \
       cnt = 0;                                                                               \
       if (own) {                                                                             \
-        const float4 xi = S.ext[a];                                                          \
+        const float4 xi = s_ext[a];                                                          \
         for (int e = lane; e < n_ext; e += tpa) {                                            \
-          const float4 q = S.ext[e];                                                         \
+          const float4 q = s_ext[e];                                                         \
           const float dx = q.x - xi.x, dy = q.y - xi.y, dz = q.z - xi.z;                     \
           const float d2 = dx * dx + dy * dy + dz * dz;                                      \
           if (d2 < rcs2_build && e != a) {                                                   \
@@ -392,104 +381,83 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     __syncthreads();                                                                         \
   }
 
-    // ----------------------------------------------- refresh positions only
-#define TSB_REFRESH()                                                                        \
+    // ------------------------------------------------------------ pair loop
+    // Four list entries per iteration, branch-free (out-of-range pairs are
+    // evaluated and masked), so the loads and the math of the four pairs
+    // overlap.
+#define TSB_PAIR(E, WITH_E)                                                                  \
   {                                                                                          \
-    if (lead) {                                                                              \
-      S.xd[3 * a] = x0;                                                                      \
-      S.xd[3 * a + 1] = x1;                                                                  \
-      S.xd[3 * a + 2] = x2;                                                                  \
-      S.ext[a] = make_ext(g, x0, x1, x2, -Wx, -Wy, -Wz, sp);                                 \
-    }                                                                                        \
-    __syncthreads();                                                                         \
-    for (int gg = tid; gg < n_ghost; gg += kFusedThreads) {                                  \
-      const uint32_t r = S.ghost[gg];                                                        \
-      const int src = (int)(r & 0xFFFFu);                                                    \
-      const int sx = ((int)(r << 11)) >> 27;                                                 \
-      const int sy = ((int)(r << 6)) >> 27;                                                  \
-      const int sz = ((int)(r << 1)) >> 27;                                                  \
-      const short4 W = S.wrap[src];                                                          \
-      const double *xs = S.xd + 3 * src;                                                     \
-      S.ext[n + gg] = make_ext(g, xs[0], xs[1], xs[2], sx - W.x, sy - W.y, sz - W.z,         \
-                               __float_as_int(S.ext[src].w));                                \
-    }                                                                                        \
-    __syncthreads();                                                                         \
-  }
-
-    // --------------------------------------------------------------- forces
-#define TSB_PAIR(E)                                                                          \
-  {                                                                                          \
-    const float4 q = S.ext[E];                                                               \
+    const float4 q = s_ext[E];                                                               \
     const float rx = q.x - xi.x, ry = q.y - xi.y, rz = q.z - xi.z;                           \
-    const float r2 = rx * rx + ry * ry + rz * rz;                                            \
+    const float r2 = fmaxf(rx * rx + ry * ry + rz * rz, 1e-30f);                             \
     const PairPrm<float> &pq = MULTI ? row[__float_as_int(q.w)] : p0;                        \
-    if (r2 < pq.a3) {                                                                        \
-      float ep, fr;                                                                          \
-      pair_eval_fast<POT>(pq, r2, ep, fr);                                                   \
-      fx -= fr * rx;                                                                         \
-      fy -= fr * ry;                                                                         \
-      fz -= fr * rz;                                                                         \
-      en += ep;                                                                              \
-    }                                                                                        \
+    float ep, fr;                                                                            \
+    pair_eval_fast<POT>(pq, r2, ep, fr);                                                     \
+    const bool in_ = r2 < pq.a3;                                                             \
+    fr = in_ ? fr : 0.f;                                                                     \
+    fx -= fr * rx;                                                                           \
+    fy -= fr * ry;                                                                           \
+    fz -= fr * rz;                                                                           \
+    if (WITH_E) en += in_ ? ep : 0.f;                                                        \
   }
-#define TSB_FORCES()                                                                         \
+#define TSB_FORCES(WITH_E)                                                                   \
   {                                                                                          \
     float fx = 0.f, fy = 0.f, fz = 0.f, en = 0.f;                                            \
     if (own) {                                                                               \
-      const float4 xi = S.ext[a];                                                            \
+      const float4 xi = s_ext[a];                                                            \
       const PairPrm<float> *row = prm + sp * A.n_species;                                    \
       (void)row;                                                                             \
       const int full = cnt >> 2;                                                             \
       for (int k4 = 0; k4 < full; ++k4) {                                                    \
-        const uint2 ge = S.list[k4 * kFusedThreads + tid];                                   \
-        TSB_PAIR(ge.x & 0xFFFFu)                                                             \
-        TSB_PAIR(ge.x >> 16)                                                                 \
-        TSB_PAIR(ge.y & 0xFFFFu)                                                             \
-        TSB_PAIR(ge.y >> 16)                                                                 \
+        const uint2 ge = s_list[k4 * kFusedThreads + tid];                                   \
+        TSB_PAIR(ge.x & 0xFFFFu, WITH_E)                                                     \
+        TSB_PAIR(ge.x >> 16, WITH_E)                                                         \
+        TSB_PAIR(ge.y & 0xFFFFu, WITH_E)                                                     \
+        TSB_PAIR(ge.y >> 16, WITH_E)                                                         \
       }                                                                                      \
       const int rem = cnt & 3;                                                               \
       if (rem) {                                                                             \
-        const uint2 ge = S.list[full * kFusedThreads + tid];                                 \
-        TSB_PAIR(ge.x & 0xFFFFu)                                                             \
-        if (rem > 1) TSB_PAIR(ge.x >> 16)                                                    \
-        if (rem > 2) TSB_PAIR(ge.y & 0xFFFFu)                                                \
+        const uint2 ge = s_list[full * kFusedThreads + tid];                                 \
+        TSB_PAIR(ge.x & 0xFFFFu, WITH_E)                                                     \
+        if (rem > 1) TSB_PAIR(ge.x >> 16, WITH_E)                                            \
+        if (rem > 2) TSB_PAIR(ge.y & 0xFFFFu, WITH_E)                                        \
       }                                                                                      \
     }                                                                                        \
     for (int o = 1; o < tpa; o <<= 1) {                                                      \
       fx += __shfl_xor_sync(0xffffffffu, fx, o);                                             \
       fy += __shfl_xor_sync(0xffffffffu, fy, o);                                             \
       fz += __shfl_xor_sync(0xffffffffu, fz, o);                                             \
-      en += __shfl_xor_sync(0xffffffffu, en, o);                                             \
+      if (WITH_E) en += __shfl_xor_sync(0xffffffffu, en, o);                                 \
     }                                                                                        \
     F0 = fx;                                                                                 \
     F1 = fy;                                                                                 \
     F2 = fz;                                                                                 \
-    ei = en;                                                                                 \
+    if (WITH_E) ei = en;                                                                     \
   }
 
     TSB_REBUILD()
     if (failed) continue;
     for (int64_t step = 0; step < A.n_steps; ++step) {
       if (own) {
-        p0x += F0 * half;
-        p0y += F1 * half;
-        p0z += F2 * half;
+        px += F0 * half;
+        py += F1 * half;
+        pz += F2 * half;
         if (A.integrator == TSB_INT_LANGEVIN) {
-          x0 += (p0x * inv_m) * half;
-          x1 += (p0y * inv_m) * half;
-          x2 += (p0z * inv_m) * half;
+          x0 += (px * inv_m) * half;
+          x1 += (py * inv_m) * half;
+          x2 += (pz * inv_m) * half;
           float z[3];
           normal3f(A.seed, (uint64_t)gi, A.counter + (uint64_t)step, z);
-          p0x = c1 * p0x + c2m * z[0];
-          p0y = c1 * p0y + c2m * z[1];
-          p0z = c1 * p0z + c2m * z[2];
-          x0 += (p0x * inv_m) * half;
-          x1 += (p0y * inv_m) * half;
-          x2 += (p0z * inv_m) * half;
+          px = c1 * px + c2m * z[0];
+          py = c1 * py + c2m * z[1];
+          pz = c1 * pz + c2m * z[2];
+          x0 += (px * inv_m) * half;
+          x1 += (py * inv_m) * half;
+          x2 += (pz * inv_m) * half;
         } else {
-          x0 += (p0x * inv_m) * dt;
-          x1 += (p0y * inv_m) * dt;
-          x2 += (p0z * inv_m) * dt;
+          x0 += (px * inv_m) * dt;
+          x1 += (py * inv_m) * dt;
+          x2 += (pz * inv_m) * dt;
         }
       }
       bool moved = false;
@@ -497,33 +465,51 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
         const float d0 = (float)x0 - xr0, d1 = (float)x1 - xr1, d2 = (float)x2 - xr2;
         moved = d0 * d0 + d1 * d1 + d2 * d2 > half_skin2;
       }
+      // all warps are done reading the previous positions
+      __syncthreads();
+      // refresh: the lanes of each atom rewrite the atom and its own images
+      if (own) {
+        for (int it = lane; it <= gcnt; it += tpa) {
+          if (it == 0) {
+            s_ext[a] = make_ext(g, x0, x1, x2, -Wx, -Wy, -Wz, sp);
+          } else {
+            const int gg = gbeg + it - 1;
+            const uint32_t r = s_gshift[gg - n];
+            const int sx = ((int)(r << 22)) >> 22;
+            const int sy = ((int)(r << 12)) >> 22;
+            const int sz = ((int)(r << 2)) >> 22;
+            s_ext[gg] = make_ext(g, x0, x1, x2, sx - Wx, sy - Wy, sz - Wz, sp);
+          }
+        }
+      }
       if (__syncthreads_or(moved)) {
         TSB_REBUILD()
         if (failed) break;
-      } else {
-        TSB_REFRESH()
       }
-      TSB_FORCES()
+      if (step + 1 == A.n_steps) {
+        TSB_FORCES(true)
+      } else {
+        TSB_FORCES(false)
+      }
       if (own) {
-        p0x += F0 * half;
-        p0y += F1 * half;
-        p0z += F2 * half;
+        px += F0 * half;
+        py += F1 * half;
+        pz += F2 * half;
       }
     }
     if (failed) continue;
-    if (A.n_steps == 0) TSB_FORCES()
+    if (A.n_steps == 0) TSB_FORCES(true)
 #undef TSB_FORCES
 #undef TSB_PAIR
-#undef TSB_REFRESH
 #undef TSB_REBUILD
     // ---- write back + FP64 energy reduction (each pair seen from both ends)
     if (lead) {
       A.x[3 * gi] = x0;
       A.x[3 * gi + 1] = x1;
       A.x[3 * gi + 2] = x2;
-      A.p[3 * gi] = p0x;
-      A.p[3 * gi + 1] = p0y;
-      A.p[3 * gi + 2] = p0z;
+      A.p[3 * gi] = px;
+      A.p[3 * gi + 1] = py;
+      A.p[3 * gi + 2] = pz;
       A.f[3 * gi] = F0;
       A.f[3 * gi + 1] = F1;
       A.f[3 * gi + 2] = F2;
