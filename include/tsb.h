@@ -151,6 +151,33 @@ int tsb_fused_md(int integrator, int potential, const double *table, int n_speci
                  int32_t *status, void *workspace, size_t workspace_bytes,
                  void *stream);
 
+/* ---- allocation-free fused MD -------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory -- hosts that own all device memory through their own pool and bar
+ * libraries from cudaMalloc, code that must not trigger the implicit
+ * device-wide synchronisation of cudaMalloc/cudaFree while other streams run,
+ * or runs with a fixed memory budget that cannot risk a failed allocation.
+ * Same arguments and results as tsb_fused_md, minus the workspace: the scratch
+ * (per-system atom ranges and the work counter, about 256 KB) is a fixed array
+ * inside the library that every GPU loading the library keeps until exit.
+ * At most TSB_FUSED_STATIC_MAX_SYSTEMS systems per call; more returns
+ * TSB_ERR_CAPACITY without launching anything.  The first call on each device
+ * looks up the array's device address (make that first call before any stream
+ * capture).  All calls share the one array: calls that overlap on the GPU
+ * (from different streams or host threads) race and must be serialised.
+ * Nothing here calls cudaMalloc, cudaFree or any allocating routine. */
+#define TSB_FUSED_STATIC_MAX_SYSTEMS 16384
+int tsb_fused_md_static(int integrator, int potential, const double *table,
+                        int n_species, const int32_t *species, double *positions,
+                        double *momenta, double *forces, const double *masses,
+                        const double *cell_row, const int64_t *system_idx,
+                        int64_t n_atoms, int64_t n_systems, const int32_t *order,
+                        double cutoff, double skin, int64_t n_steps,
+                        const double *dt_sys, const double *kT_sys,
+                        const double *gamma_sys, uint64_t seed, uint64_t counter,
+                        double *energy, int32_t *n_rebuilds, int32_t *status,
+                        void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,6 +27,8 @@
 //   * Pair arithmetic FP32; positions, momenta and per-system energy FP64.
 #include <math.h>
 
+#include <mutex>
+
 #include "tsb_pair.cuh"
 #include "tsb_rng.cuh"
 
@@ -589,6 +591,102 @@ extern "C" int tsb_fused_md(int integrator, int potential, const double *table,
   int64_t grid = n_sm;
   if (grid > kMaxGrid) grid = kMaxGrid;
   if (grid > n_systems) grid = n_systems;
+  cudaMemsetAsync(lo, 0, sizeof(int64_t) * n_systems, st);
+  cudaMemsetAsync(hi, 0, sizeof(int64_t) * n_systems, st);
+  cudaMemsetAsync(queue, 0, sizeof(int32_t) * 4, st);
+  cudaMemsetAsync(status, 0, sizeof(int32_t) * 4, st);
+  k_bounds_fused<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, lo, hi);
+  FusedArgs A{integrator, potential, n_species, table, species, positions, momenta, forces,
+              masses, cell_row, lo, hi, n_systems, order, cutoff, skin, n_steps, dt_sys,
+              kT_sys, gamma_sys, seed, counter, energy, n_rebuilds, queue, status};
+  const bool multi = n_species > 1;
+  if (potential == TSB_POT_LJ) {
+    multi ? launch_fused<TSB_POT_LJ, true>(A, grid, st) : launch_fused<TSB_POT_LJ, false>(A, grid, st);
+  } else if (potential == TSB_POT_MORSE) {
+    multi ? launch_fused<TSB_POT_MORSE, true>(A, grid, st)
+          : launch_fused<TSB_POT_MORSE, false>(A, grid, st);
+  } else {
+    multi ? launch_fused<TSB_POT_SOFT, true>(A, grid, st)
+          : launch_fused<TSB_POT_SOFT, false>(A, grid, st);
+  }
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of tsb_fused_md.
+//
+// Some callers cannot hand us a workspace: host programs that own every byte of
+// device memory through their own pool and do not let a library call
+// cudaMalloc, programs that must not trigger the implicit device-wide
+// synchronisation cudaMalloc/cudaFree can cause while other streams run, and
+// programs with a fixed memory budget that cannot risk an allocation failing
+// mid-run.  For them the scratch of the fused kernel (per-system atom ranges
+// and the work counter) lives in this fixed array, compiled into the library.
+// Every GPU that loads the library holds it until the process exits.
+// ---------------------------------------------------------------------------
+namespace tsb {
+constexpr int kStaticMaxSystems = TSB_FUSED_STATIC_MAX_SYSTEMS;
+constexpr size_t kStaticScratchBytes = 2 * sizeof(int64_t) * kStaticMaxSystems + 256;
+static __device__ __align__(256) unsigned char g_fused_static_scratch[kStaticScratchBytes];
+
+// Device address of the array on each device (host code may not use the
+// symbol itself as a pointer); looked up once per device, with it current.
+constexpr int kMaxDevices = 64;
+static void *g_fused_static_ptr[kMaxDevices];
+static std::mutex g_fused_static_mu;
+
+static int fused_static_scratch(void **out) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return TSB_ERR_CUDA;
+  std::lock_guard<std::mutex> lock(g_fused_static_mu);
+  if (!g_fused_static_ptr[dev]) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_fused_static_scratch) != cudaSuccess || !p)
+      return TSB_ERR_CUDA;
+    g_fused_static_ptr[dev] = p;
+  }
+  *out = g_fused_static_ptr[dev];
+  return TSB_OK;
+}
+}  // namespace tsb
+
+extern "C" int tsb_fused_md_static(int integrator, int potential, const double *table,
+                                   int n_species, const int32_t *species, double *positions,
+                                   double *momenta, double *forces, const double *masses,
+                                   const double *cell_row, const int64_t *system_idx,
+                                   int64_t n_atoms, int64_t n_systems, const int32_t *order,
+                                   double cutoff, double skin, int64_t n_steps,
+                                   const double *dt_sys, const double *kT_sys,
+                                   const double *gamma_sys, uint64_t seed, uint64_t counter,
+                                   double *energy, int32_t *n_rebuilds, int32_t *status,
+                                   void *stream) {
+  if (integrator != TSB_INT_NVE && integrator != TSB_INT_LANGEVIN) return TSB_ERR_INVALID_ARG;
+  if (potential < TSB_POT_LJ || potential > TSB_POT_SOFT) return TSB_ERR_INVALID_ARG;
+  if (n_species < 1 || !table || (n_species > 1 && !species)) return TSB_ERR_INVALID_ARG;
+  if (n_species > kFusedMaxSpecies) return TSB_ERR_UNSUPPORTED;
+  if (n_atoms < 1 || n_systems < 1 || !(cutoff > 0.0) || !(skin >= 0.0) || n_steps < 0)
+    return TSB_ERR_INVALID_ARG;
+  if (!positions || !momenta || !forces || !masses || !cell_row || !system_idx || !dt_sys ||
+      !energy || !status)
+    return TSB_ERR_INVALID_ARG;
+  if (integrator == TSB_INT_LANGEVIN && (!kT_sys || !gamma_sys)) return TSB_ERR_INVALID_ARG;
+  // the fixed scratch holds the atom ranges of at most kStaticMaxSystems systems
+  if (n_systems > kStaticMaxSystems) return TSB_ERR_CAPACITY;
+  void *scratch = nullptr;
+  TSB_TRY(fused_static_scratch(&scratch));
+  char *base = (char *)scratch;
+  int64_t *lo = (int64_t *)base;
+  int64_t *hi = lo + kStaticMaxSystems;
+  int32_t *queue = (int32_t *)(hi + kStaticMaxSystems);
+  cudaStream_t st = (cudaStream_t)stream;
+  int dev = 0, n_sm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  int64_t grid = n_sm;
+  if (grid > kMaxGrid) grid = kMaxGrid;
+  if (grid > n_systems) grid = n_systems;
+  // the array keeps the previous call's contents: clear what must start at zero
   cudaMemsetAsync(lo, 0, sizeof(int64_t) * n_systems, st);
   cudaMemsetAsync(hi, 0, sizeof(int64_t) * n_systems, st);
   cudaMemsetAsync(queue, 0, sizeof(int32_t) * 4, st);
