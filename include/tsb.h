@@ -92,7 +92,9 @@ int tsb_nl_build(const void *positions, const void *cell_row, const uint8_t *pbc
  * The neighbour search is fused with the force evaluation (no pair list is
  * stored).  energy [S], stress [S,3,3], forces [N,3], energies [N],
  * stresses [N,3,3] are written in `dtype`; outputs not requested by
- * `out_flags` may be NULL. */
+ * `out_flags` may be NULL.  `sys_active` [S] uint8 (optional): systems with 0
+ * are skipped and their outputs left untouched (converged systems of a batched
+ * relaxation). */
 size_t tsb_pair_workspace_size(int64_t n_atoms, int64_t n_systems);
 int tsb_pair_forward(int potential, const double *table, int n_species,
                      const int32_t *species, const void *positions,
@@ -100,7 +102,8 @@ int tsb_pair_forward(int potential, const double *table, int n_species,
                      const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
                      int dtype, double cutoff, int out_flags, void *energy,
                      void *forces, void *stress, void *energies, void *stresses,
-                     void *workspace, size_t workspace_bytes, void *stream);
+                     const uint8_t *sys_active, void *workspace,
+                     size_t workspace_bytes, void *stream);
 
 /* ---- integrator steps (elementwise, per-system parameters) ---------------
  * dt_sys, kT_sys, gamma_sys are device float64 arrays of length n_systems.
@@ -121,6 +124,44 @@ int tsb_md_baoab_boa(void *positions, void *momenta, const void *forces,
                      const double *dt_sys, const double *kT_sys,
                      const double *gamma_sys, const void *noise, uint64_t seed,
                      uint64_t counter, int64_t n_atoms, int dtype, void *stream);
+
+/* ---- FIRE + Frechet cell filter -----------------------------------------
+ * Per-system state arrays (dtype): dt [S], alpha [S], n_pos [S] int32; cell,
+ * reference_cell, cell_positions, cell_velocities, cell_forces [S,3,3] in the
+ * COLUMN-vector convention of SimState.cell (state.py:138-142); cell_factor
+ * [S]; cell_masses [S] (sum of atomic masses, cell_filters.py:97-101).
+ * cell_filter 0 = positions only, 1 = Frechet filter.  Systems whose `active`
+ * entry is 0 are skipped.  eps is 1e-8 (float32) / 1e-16 (float64) as in
+ * fire.py:154.
+ * tsb_fire_ase_pre: fire.py:288-485 (_ase_fire_step up to the model call).
+ * tsb_fire_vv_pre / tsb_fire_vv_post: fire.py:179-285 around the model call.
+ * tsb_frechet_cell_forces: cell_filters.py:353-391 (init=1: the initial cell
+ *   forces of frechet_cell_filter_init, cell_filters.py:230-284).
+ * tsb_fire_converged: max|F_i| < fmax (and cell-force row norms < fmax when
+ *   cell_forces is given) per system, runners.py:501-538; converged systems
+ *   get active = 0, *n_active (device int32) counts the rest. */
+size_t tsb_fire_workspace_size(int64_t n_systems);
+#define TSB_FIRE_ARGS_DECL                                                       \
+  int cell_filter, void *positions, void *velocities, const void *forces,       \
+      const void *masses, const int64_t *system_idx, int64_t n_atoms,           \
+      int64_t n_systems, void *dt, void *alpha, int32_t *n_pos, void *cell,     \
+      const void *reference_cell, const void *cell_factor,                      \
+      void *cell_positions, void *cell_velocities, const void *cell_forces,     \
+      const void *cell_masses, const uint8_t *active, double dt_max,            \
+      int n_min, double f_inc, double f_dec, double alpha_start,                \
+      double f_alpha, double max_step, double eps, int dtype, void *workspace,  \
+      size_t workspace_bytes, void *stream
+int tsb_fire_ase_pre(TSB_FIRE_ARGS_DECL);
+int tsb_fire_vv_pre(TSB_FIRE_ARGS_DECL);
+int tsb_fire_vv_post(TSB_FIRE_ARGS_DECL);
+int tsb_frechet_cell_forces(void *cell_forces, const void *stress, const void *cell,
+                            const void *reference_cell, const void *pressure,
+                            const void *cell_factor, int64_t n_systems, int init,
+                            const uint8_t *active, int dtype, void *stream);
+int tsb_fire_converged(const void *forces, const int64_t *system_idx, int64_t n_atoms,
+                       int64_t n_systems, const void *cell_forces, double fmax,
+                       uint8_t *active, int32_t *n_active, int dtype, void *workspace,
+                       size_t workspace_bytes, void *stream);
 
 /* ---- fused persistent batched MD ----------------------------------------
  * Advances every system by n_steps of velocity Verlet (TSB_INT_NVE,

@@ -17,7 +17,8 @@ template <int POT, class R, class P>
 __global__ void __launch_bounds__(128)
     k_pair_forces(BinData b, int64_t n, const double *__restrict__ table, int ns_species,
                   const int32_t *__restrict__ species, double cutoff, int flags, P *forces,
-                  P *energies, P *stresses, double *e_half, double *vir_half) {
+                  P *energies, P *stresses, double *e_half, double *vir_half,
+                  const uint8_t *__restrict__ sys_active) {
   __shared__ PairPrm<R> prm[kMaxSpecies * kMaxSpecies];
   for (int k = threadIdx.x; k < ns_species * ns_species; k += blockDim.x)
     prm[k] = make_prm<R>(POT, table + 5 * k, cutoff);
@@ -27,6 +28,7 @@ __global__ void __launch_bounds__(128)
   const double4 w = b.spos[p];
   const int i = (int)__double_as_longlong(w.w);
   const int s = b.sys_of[i];
+  if (sys_active && !sys_active[s]) return;
   const SysGeom &G = b.geom[s];
   const int si = species ? min(max(species[i], 0), ns_species - 1) : 0;
   const PairPrm<R> *row = prm + si * ns_species;
@@ -83,9 +85,10 @@ __global__ void __launch_bounds__(128)
 // One block per system, fixed-order tree reduction in FP64 (deterministic).
 template <class P>
 __global__ void k_sys_reduce(const SysGeom *g, const double *e_half, const double *vir_half,
-                             int flags, P *energy, P *stress) {
+                             int flags, P *energy, P *stress, const uint8_t *sys_active) {
   __shared__ double sh[7][kBlock / 32];
   const int s = blockIdx.x;
+  if (sys_active && !sys_active[s]) return;
   const SysGeom &G = g[s];
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
   for (int a = threadIdx.x; a < G.count; a += blockDim.x) {
@@ -129,28 +132,28 @@ static void carve_pair(Carver &c, PairWork &w, int64_t n, int64_t ns) {
 template <int POT, class R, class P>
 static void launch_forces(PairWork &w, int64_t n, const double *table, int nsp,
                           const int32_t *species, double cutoff, int flags, P *forces,
-                          P *energies, P *stresses, cudaStream_t st) {
+                          P *energies, P *stresses, const uint8_t *active, cudaStream_t st) {
   k_pair_forces<POT, R, P><<<grid_for(n, 128), 128, 0, st>>>(
       w.b, n, table, nsp, species, cutoff, flags, forces, energies, stresses, w.e_half,
-      w.vir_half);
+      w.vir_half, active);
 }
 
 template <class P>
 static int pair_forward(int pot, const double *table, int nsp, const int32_t *species,
                         const P *pos, const P *cell, const uint8_t *pbc, const int64_t *sys,
                         int64_t n, int64_t ns, double cutoff, int flags, P *energy,
-                        P *forces, P *stress, P *energies, P *stresses, PairWork &w,
-                        cudaStream_t st) {
+                        P *forces, P *stress, P *energies, P *stresses,
+                        const uint8_t *active, PairWork &w, cudaStream_t st) {
   TSB_TRY(prepare_bins<P>(pos, cell, pbc, sys, n, ns, cutoff, w.b, st));
   const bool f64 = flags & TSB_MATH_FP64;
   if (n > 0) {
 #define TSB_LAUNCH(POT)                                                                    \
   if (f64)                                                                                 \
     launch_forces<POT, double, P>(w, n, table, nsp, species, cutoff, flags, forces,       \
-                                  energies, stresses, st);                                 \
+                                  energies, stresses, active, st);                         \
   else                                                                                     \
     launch_forces<POT, float, P>(w, n, table, nsp, species, cutoff, flags, forces,        \
-                                 energies, stresses, st);
+                                 energies, stresses, active, st);
     if (pot == TSB_POT_LJ) {
       TSB_LAUNCH(TSB_POT_LJ)
     } else if (pot == TSB_POT_MORSE) {
@@ -161,7 +164,7 @@ static int pair_forward(int pot, const double *table, int nsp, const int32_t *sp
 #undef TSB_LAUNCH
   }
   k_sys_reduce<P><<<(unsigned)ns, kBlock, 0, st>>>(w.b.geom, w.e_half, w.vir_half, flags,
-                                                  energy, stress);
+                                                  energy, stress, active);
   TSB_CHECK_LAUNCH();
   return TSB_OK;
 }
@@ -183,8 +186,8 @@ extern "C" int tsb_pair_forward(int potential, const double *table, int n_specie
                                 const int64_t *system_idx, int64_t n_atoms,
                                 int64_t n_systems, int dtype, double cutoff, int out_flags,
                                 void *energy, void *forces, void *stress, void *energies,
-                                void *stresses, void *workspace, size_t workspace_bytes,
-                                void *stream) {
+                                void *stresses, const uint8_t *sys_active, void *workspace,
+                                size_t workspace_bytes, void *stream) {
   if (potential < TSB_POT_LJ || potential > TSB_POT_SOFT) return TSB_ERR_INVALID_ARG;
   if (n_species < 1 || n_species > kMaxSpecies || !table) return TSB_ERR_INVALID_ARG;
   if (n_species > 1 && !species) return TSB_ERR_INVALID_ARG;
@@ -207,9 +210,10 @@ extern "C" int tsb_pair_forward(int potential, const double *table, int n_specie
                                 (const double *)positions, (const double *)cell_row, pbc,
                                 system_idx, n_atoms, n_systems, cutoff, out_flags,
                                 (double *)energy, (double *)forces, (double *)stress,
-                                (double *)energies, (double *)stresses, w, st);
+                                (double *)energies, (double *)stresses, sys_active, w, st);
   return pair_forward<float>(potential, table, n_species, species, (const float *)positions,
                              (const float *)cell_row, pbc, system_idx, n_atoms, n_systems,
                              cutoff, out_flags, (float *)energy, (float *)forces,
-                             (float *)stress, (float *)energies, (float *)stresses, w, st);
+                             (float *)stress, (float *)energies, (float *)stresses, sys_active,
+                             w, st);
 }

@@ -33,6 +33,10 @@ INT_NVE, INT_LANGEVIN = 0, 1
 _vp, _i64, _u64, _i32, _dbl, _sz, _int = (C.c_void_p, C.c_int64, C.c_uint64, C.c_int32,
                                          C.c_double, C.c_size_t, C.c_int)
 
+_FIRE_ARGS = [_int, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+              _vp, _vp, _vp, _vp, _dbl, _int, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _int, _vp,
+              _sz, _vp]
+
 # name -> (restype, argtypes); mirrors include/tsb.h exactly
 PROTOTYPES = {
     "tsb_version": (C.c_char_p, []),
@@ -42,11 +46,19 @@ PROTOTYPES = {
                             _vp, _vp, _i64, _vp, _vp, _sz, _vp]),
     "tsb_pair_workspace_size": (_sz, [_i64, _i64]),
     "tsb_pair_forward": (_int, [_int, _vp, _int, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _int,
-                                _dbl, _int, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
+                                _dbl, _int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
     "tsb_md_kick": (_int, [_vp, _vp, _vp, _vp, _dbl, _i64, _int, _vp]),
     "tsb_md_drift": (_int, [_vp, _vp, _vp, _vp, _vp, _dbl, _i64, _int, _vp]),
     "tsb_md_baoab_boa": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _u64, _u64,
                                 _i64, _int, _vp]),
+    "tsb_fire_workspace_size": (_sz, [_i64]),
+    "tsb_fire_ase_pre": (_int, _FIRE_ARGS),
+    "tsb_fire_vv_pre": (_int, _FIRE_ARGS),
+    "tsb_fire_vv_post": (_int, _FIRE_ARGS),
+    "tsb_frechet_cell_forces": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _int, _vp, _int,
+                                       _vp]),
+    "tsb_fire_converged": (_int, [_vp, _vp, _i64, _i64, _vp, _dbl, _vp, _vp, _int, _vp, _sz,
+                                  _vp]),
     "tsb_fused_max_atoms": (_int, []),
     "tsb_fused_workspace_size": (_sz, [_i64, _i64]),
     "tsb_fused_md": (_int, [_int, _int, _vp, _int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64,

@@ -107,41 +107,14 @@ class PairTableModel(ModelInterface):
         pos = state.positions
         L.require_cuda(pos, "state.positions")
         dev, dt = pos.device, pos.dtype
-        n = pos.shape[0]
-        n_sys = state.n_systems
-        cell_row = state.cell.mT.contiguous()
-        pbc = state.pbc
-        if pbc.ndim == 1:
-            pbc = pbc.unsqueeze(0).expand(n_sys, 3)
-        pbc = pbc.to(torch.uint8).contiguous()
-        sys_idx = state.system_idx.contiguous()
-        species = self._species(state.atomic_numbers)
-        table = self.table if self.table.device == dev else self.table.to(dev)
-        flags = 0
-        if self._compute_forces:
-            flags |= L.OUT_FORCES
-        if self._compute_stress:
-            flags |= L.OUT_STRESS
-        if self.per_atom_energies:
-            flags |= L.OUT_ENERGIES
-        if self.per_atom_stresses:
-            flags |= L.OUT_STRESSES
-        if self.precision == "fp64":
-            flags |= L.MATH_FP64
+        n, n_sys = pos.shape[0], state.n_systems
         energy = torch.empty(n_sys, dtype=dt, device=dev)
         forces = torch.empty((n, 3), dtype=dt, device=dev) if self._compute_forces else None
         stress = torch.empty((n_sys, 3, 3), dtype=dt, device=dev) if self._compute_stress else None
         energies = torch.empty(n, dtype=dt, device=dev) if self.per_atom_energies else None
         stresses = (torch.empty((n, 3, 3), dtype=dt, device=dev)
                     if self.per_atom_stresses else None)
-        ws_bytes = L.load().tsb_pair_workspace_size(n, n_sys)
-        ws = L.Workspace.get(dev, ws_bytes)
-        pos = pos.contiguous()
-        L.call("tsb_pair_forward", self.kind, L.ptr(table), self.n_species, L.ptr(species),
-               L.ptr(pos), L.ptr(cell_row), L.ptr(pbc), L.ptr(sys_idx), n, n_sys,
-               L.dtype_code(dt), self.cutoff, flags, L.ptr(energy), L.ptr(forces),
-               L.ptr(stress), L.ptr(energies), L.ptr(stresses), L.ptr(ws), ws.numel(),
-               L.stream_ptr(dev))
+        self._launch(state, energy, forces, stress, energies, stresses, None)
         out = {"energy": energy}
         if forces is not None:
             out["forces"] = forces
@@ -152,6 +125,49 @@ class PairTableModel(ModelInterface):
         if stresses is not None:
             out["stresses"] = stresses
         return out
+
+    def forward_into(self, state, *, energy, forces, stress=None, sys_active=None):
+        """Write energy/forces(/stress) of the systems with ``sys_active`` != 0 into
+        existing contiguous buffers; the other systems' entries are left untouched."""
+        if state.dtype != self._dtype:
+            raise TypeError(
+                f"SimState dtype {state.dtype} does not match model dtype {self._dtype}.")
+        L.require_cuda(state.positions, "state.positions")
+        for t in (energy, forces, stress):
+            if t is not None and not t.is_contiguous():
+                raise ValueError("forward_into needs contiguous output buffers")
+        self._launch(state, energy, forces, stress if self._compute_stress else None, None,
+                     None, sys_active)
+
+    def _launch(self, state, energy, forces, stress, energies, stresses, sys_active):
+        pos = state.positions.contiguous()
+        dev, dt = pos.device, pos.dtype
+        n, n_sys = pos.shape[0], state.n_systems
+        cell_row = state.cell.mT.contiguous()
+        pbc = state.pbc
+        if pbc.ndim == 1:
+            pbc = pbc.unsqueeze(0).expand(n_sys, 3)
+        pbc = pbc.to(torch.uint8).contiguous()
+        sys_idx = state.system_idx.contiguous()
+        species = self._species(state.atomic_numbers)
+        table = self.table if self.table.device == dev else self.table.to(dev)
+        flags = 0
+        if forces is not None:
+            flags |= L.OUT_FORCES
+        if stress is not None:
+            flags |= L.OUT_STRESS
+        if energies is not None:
+            flags |= L.OUT_ENERGIES
+        if stresses is not None:
+            flags |= L.OUT_STRESSES
+        if self.precision == "fp64":
+            flags |= L.MATH_FP64
+        ws = L.Workspace.get(dev, L.load().tsb_pair_workspace_size(n, n_sys))
+        L.call("tsb_pair_forward", self.kind, L.ptr(table), self.n_species, L.ptr(species),
+               L.ptr(pos), L.ptr(cell_row), L.ptr(pbc), L.ptr(sys_idx), n, n_sys,
+               L.dtype_code(dt), self.cutoff, flags, L.ptr(energy), L.ptr(forces),
+               L.ptr(stress), L.ptr(energies), L.ptr(stresses), L.ptr(sys_active), L.ptr(ws),
+               ws.numel(), L.stream_ptr(dev))
 
 
 def single_species_table(sigma, epsilon, alpha=0.0, rc=np.inf, eshift=0.0):
