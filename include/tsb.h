@@ -125,6 +125,39 @@ int tsb_md_baoab_boa(void *positions, void *momenta, const void *forces,
                      const double *gamma_sys, const void *noise, uint64_t seed,
                      uint64_t counter, int64_t n_atoms, int dtype, void *stream);
 
+/* ---- Verlet-list forces for large periodic systems ----------------------
+ * One fully periodic system whose cell widths are all >= 2 (cutoff + skin)
+ * (e.g. 500,000 atoms).  The reference rebuilds its list in every model call
+ * (torch_sim/models/pair_potential.py:168-174); here the list holds all pairs
+ * within cutoff + skin and is reused until an atom moved more than skin/2,
+ * giving the same pairs and forces as PairPotentialModel.forward (:351-464).
+ * tsb_verlet_build: cell-list search, ELL list[k * N + i] = j << 5 | image code,
+ *   counts [N], reference positions [N,3] f64, integer wraps [N,3] i32;
+ *   *status > 0 if an atom had more than max_neighbors (regrow and rebuild);
+ *   cell_row in `dtype`.
+ * tsb_verlet_check: maps the current positions into the build frame (kept in
+ *   the workspace for tsb_verlet_forces) and sets *expired when any atom moved
+ *   more than skin/2 (then rebuild and check again).  cell_row float64.
+ * tsb_verlet_forces: energy [1], forces [N,3] (dtype), stress [1,3,3] with
+ *   TSB_OUT_STRESS; e_atom [N] and vir_atom [N,6] are float64 scratch.  Uses the
+ *   workspace filled by tsb_verlet_check.  cell_row float64. */
+size_t tsb_verlet_workspace_size(int64_t n_atoms);
+int tsb_verlet_build(const void *positions, const void *cell_row, int64_t n_atoms, int dtype,
+                     double cutoff, double skin, uint32_t *list, int32_t *counts,
+                     int max_neighbors, double *ref_positions, int32_t *wraps,
+                     int32_t *status, void *workspace, size_t workspace_bytes,
+                     void *stream);
+int tsb_verlet_check(const void *positions, const double *ref_positions,
+                     const int32_t *wraps, const double *cell_row, const int32_t *species,
+                     int64_t n_atoms, int dtype, double skin, int32_t *expired,
+                     void *workspace, size_t workspace_bytes, void *stream);
+int tsb_verlet_forces(int potential, const double *table, int n_species,
+                      const uint32_t *list, const int32_t *counts, int64_t n_atoms,
+                      const double *cell_row, int dtype, double cutoff, int out_flags,
+                      void *energy, void *forces, void *stress, double *e_atom,
+                      double *vir_atom, void *workspace, size_t workspace_bytes,
+                      void *stream);
+
 /* ---- FIRE + Frechet cell filter -----------------------------------------
  * Per-system state arrays (dtype): dt [S], alpha [S], n_pos [S] int32; cell,
  * reference_cell, cell_positions, cell_velocities, cell_forces [S,3,3] in the

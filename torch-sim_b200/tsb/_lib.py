@@ -51,6 +51,13 @@ PROTOTYPES = {
     "tsb_md_drift": (_int, [_vp, _vp, _vp, _vp, _vp, _dbl, _i64, _int, _vp]),
     "tsb_md_baoab_boa": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _u64, _u64,
                                 _i64, _int, _vp]),
+    "tsb_verlet_workspace_size": (_sz, [_i64]),
+    "tsb_verlet_build": (_int, [_vp, _vp, _i64, _int, _dbl, _dbl, _vp, _vp, _int, _vp, _vp,
+                                _vp, _vp, _sz, _vp]),
+    "tsb_verlet_check": (_int, [_vp, _vp, _vp, _vp, _vp, _i64, _int, _dbl, _vp, _vp, _sz,
+                                _vp]),
+    "tsb_verlet_forces": (_int, [_int, _vp, _int, _vp, _vp, _i64, _vp, _int, _dbl, _int, _vp,
+                                 _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
     "tsb_fire_workspace_size": (_sz, [_i64]),
     "tsb_fire_ase_pre": (_int, _FIRE_ARGS),
     "tsb_fire_vv_pre": (_int, _FIRE_ARGS),

@@ -6,7 +6,8 @@ from .lennard_jones import (LennardJonesModel, LennardJonesMultiModel,
 from .morse import MorseModel
 from .pair_potential import PairTableModel
 from .soft_sphere import SoftSphereModel, SoftSphereMultiModel
+from .verlet import VerletListModel
 
 __all__ = ["LennardJonesModel", "LennardJonesMultiModel", "ModelInterface", "MorseModel",
            "PairTableModel", "SoftSphereModel", "SoftSphereMultiModel",
-           "UnbatchedLennardJonesModel", "kob_andersen_model"]
+           "UnbatchedLennardJonesModel", "VerletListModel", "kob_andersen_model"]
