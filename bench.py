@@ -351,9 +351,9 @@ def main():
     torch.cuda.synchronize(device)
     runner.check()
 
-    def barrier():
-        if ws > 1:
-            torch.distributed.barrier()
+    from tsb import replicas
+
+    barrier = replicas.barrier
 
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -372,12 +372,8 @@ def main():
     rebuild_interval = args.md_steps / max(float(rebuilds.mean()), 1e-9)
     per_launch_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     t_rank = sum(per_launch_ms) / 1e3
-    t = torch.tensor([t_rank], dtype=torch.float64, device=device)
-    if ws > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    t_max = float(t)
-    total_atom_steps = n_atoms * args.md_steps * args.steps * ws
-    value = total_atom_steps / t_max
+    t_max = replicas.max_over_ranks(t_rank, device)
+    value = replicas.weak_scaling_value(n_atoms * args.md_steps * args.steps, t_max, ws)
     avg_launch_s = statistics.mean(per_launch_ms) / 1e3
 
     # ---- end to end through the C ABI with host buffers (pinned), copies timed
@@ -407,11 +403,8 @@ def main():
     torch.cuda.synchronize(device)
     barrier()
     runner.check()
-    te = torch.tensor([sum(s.elapsed_time(e) for s, e in zip(es, ee)) / 1e3],
-                      dtype=torch.float64, device=device)
-    if ws > 1:
-        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-    e2e_value = n_atoms * args.md_steps * e2e_steps * ws / float(te)
+    te = replicas.max_over_ranks(sum(s.elapsed_time(e) for s, e in zip(es, ee)) / 1e3, device)
+    e2e_value = replicas.weak_scaling_value(n_atoms * args.md_steps * e2e_steps, te, ws)
     h2d = 3 * hx.numel() * 8
     d2h = 2 * hx.numel() * 8 + oe.numel() * 8
 

@@ -126,7 +126,7 @@ int tsb_md_baoab_boa(void *positions, void *momenta, const void *forces,
                      uint64_t counter, int64_t n_atoms, int dtype, void *stream);
 
 /* ---- Verlet-list forces for large periodic systems ----------------------
- * One fully periodic system whose cell widths are all >= 2 (cutoff + skin)
+ * One fully periodic system whose cell widths are all >= cutoff + skin
  * (e.g. 500,000 atoms).  The reference rebuilds its list in every model call
  * (torch_sim/models/pair_potential.py:168-174); here the list holds all pairs
  * within cutoff + skin and is reused until an atom moved more than skin/2,

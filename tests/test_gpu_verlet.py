@@ -87,13 +87,19 @@ def test_verlet_unwrapped_positions():
     assert _rel(out["forces"], r["forces"]) < 1e-5
 
 
-def test_verlet_rejects_small_cells():
+def test_verlet_small_cell_two_images_and_rejection():
+    """A cell narrower than 2 (rc + skin) but wider than rc + skin is fine: the
+    list holds both images of a neighbour.  Narrower cells need shifts beyond
+    +-1 and are rejected."""
     from tsb import models, workloads
     from tsb.state import state_from_arrays
 
-    d = workloads.argon_fcc((3, 3, 3), seed=0)  # 15.8 A < 2 (8.5 + 1)
+    d = workloads.argon_fcc((3, 3, 3), jitter=0.1, seed=0)  # 15.8 A: 9.5 < L < 19
     st = state_from_arrays(d, device="cuda")
-    vm = models.VerletListModel(models.LennardJonesModel(sigma=3.405, epsilon=0.0104,
-                                                         cutoff=8.5), skin=1.0)
+    vm, ref = _models()
+    out, r = vm(st), ref(st)
+    assert _rel(out["forces"], r["forces"]) < 1e-5
+    d1 = workloads.argon_fcc((1, 1, 1), seed=0)  # 5.26 A < rc + skin
+    vm1, _ = _models()
     with pytest.raises(ValueError):
-        vm(st)
+        vm1(state_from_arrays(d1, device="cuda"))

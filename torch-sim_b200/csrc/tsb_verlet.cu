@@ -9,8 +9,8 @@
 //
 // Layout: ELL table list[k * N + i] (uint32: j << 5 | image code), code =
 // (sx+1)*9 + (sy+1)*3 + (sz+1) for lattice shifts in {-1,0,1}^3 relative to the
-// positions wrapped at build time (requires every periodic cell width >= 2 *
-// (cutoff + skin); the entry point checks).  At evaluation the current
+// positions wrapped at build time (requires every periodic cell width >= cutoff +
+// skin; the build kernel flags wider shifts).  At evaluation the current
 // positions are mapped with the build-time integer wraps into FP64 "build-frame"
 // coordinates, so displacements across the periodic boundary are exact.
 #include "tsb_pair.cuh"
@@ -44,7 +44,7 @@ __global__ void k_verlet_build(BinData b, int64_t n, double rcs2, uint32_t *list
   search_neighbors(G, b.spos, b.bin_start, i, w.x, w.y, w.z, rcs2, false,
                    [&](int j, int sx, int sy, int sz, double, double, double, double) {
                      if (sx < -1 || sx > 1 || sy < -1 || sy > 1 || sz < -1 || sz > 1) {
-                       atomicMax(status, 1 << 30);  // cell narrower than 2 (rc + skin)
+                       atomicMax(status, 1 << 30);  // cell narrower than rc + skin
                        return;
                      }
                      if (c < max_nb)

@@ -70,7 +70,7 @@ class VerletListModel(ModelInterface):
             if st == 0:
                 break
             if st >= (1 << 30):
-                raise ValueError("VerletListModel needs every cell width >= 2 (cutoff + skin)")
+                raise ValueError("VerletListModel needs every cell width >= cutoff + skin")
             self.cap = int(st * 1.2) + 8
             self.list = torch.empty(self.cap * state.n_atoms, dtype=torch.int32,
                                     device=state.device)
