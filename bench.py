@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skin", type=float, default=SKIN)
     ap.add_argument("--workload", default="batched_md",
-                    choices=["batched_md", "single_large", "relax"])
+                    choices=["batched_md", "single_large", "relax", "adjoint"])
     return ap.parse_args()
 
 
@@ -314,8 +314,57 @@ def run_relax(args):
     return 0
 
 
+def run_adjoint(args):
+    """256 two-species LJ systems of 108 atoms, 200 NVE steps (2 fs) from 80 K;
+    loss = squared error of the final-frame smeared pair-distance histogram;
+    one bench step = loss + adjoint gradients (sigma, epsilon, q0, p0), 20-step
+    checkpoints."""
+    import torch
+
+    from tsb import adjoint, integrators, workloads
+    from tsb.state import state_from_arrays
+
+    dev = torch.device("cuda", 0)
+    d = workloads.argon_species_batch(256, (3, 3, 3), seed=0)
+    st = state_from_arrays(d, device=dev)
+    g = torch.Generator(device=dev).manual_seed(5)
+    p0 = integrators.initialize_momenta(st.positions, st.masses, st.system_idx,
+                                        torch.tensor(80.0 * workloads.KB_EV, device=dev), g)
+    P = adjoint.make_problem(st, 200, 0.002 * workloads.METAL_TIME)
+    s0, e0 = adjoint.argon_pair_params(device=dev)
+    qT, _, _ = adjoint.integrate(st.positions, p0, adjoint.lj_table(s0, e0), P, False)
+    P.target = adjoint.histogram(qT, P)
+    s, e = adjoint.argon_pair_params(perturb=0.05, seed=1, device=dev)
+    for _ in range(max(1, args.warmup)):
+        adjoint.loss_and_grad(s, e, st.positions, p0, P)
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    with ClockSampler(0) as clocks:
+        for a, b in evs:
+            a.record()
+            loss, gs, ge, gq, gp = adjoint.loss_and_grad(s, e, st.positions, p0, P)
+            b.record()
+        torch.cuda.synchronize()
+    t = sum(a.elapsed_time(b) for a, b in evs) / 1e3 / args.steps
+    n = st.n_atoms
+    line = {"metric": "gradient evaluations/s (200-step NVE trajectory loss, adjoint)",
+            "value": 1.0 / t, "unit": "grad-evals/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (256 x fcc 3x3x3 argon, two species 50:50)",
+            "config": {"workload": "adjoint", "systems": 256, "atoms": n, "md_steps": 200,
+                       "checkpoint_every": 20, "forward_atom_steps_per_s": n * 200 / t,
+                       "loss": float(loss)},
+            "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "adjoint" and args.impl != "reference":
+        return run_adjoint(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "single_large":

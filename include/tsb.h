@@ -158,6 +158,33 @@ int tsb_verlet_forces(int potential, const double *table, int n_species,
                       double *vir_atom, void *workspace, size_t workspace_bytes,
                       void *stream);
 
+/* ---- adjoint of NVE trajectories (species-matrix LJ, FP64) ---------------
+ * No kernel of the reference corresponds: it differentiates trajectories with
+ * torch.autograd through PairPotentialModel (pair_potential.py:420-425), which
+ * omits the force-Jacobian terms.  These are the pieces of the exact discrete
+ * adjoint of velocity Verlet (nve.py:74-130):
+ * tsb_lj_hvp: lam_q += coef * J_F(q)^T v (J_F = -Hessian of the LJ energy) and
+ *   grad_params [S, ns, ns, 2] += coef * dF/d(sigma_ab, epsilon_ab)^T v per system.
+ * tsb_rdf_hist: hist [S, n_bins] = sum over pairs r < r_max of
+ *   exp(-(r - c_b)^2 / (2 width^2)), c_b = (b + 1/2) r_max / n_bins.
+ * tsb_rdf_hist_grad: grad_positions [N,3] = d(sum_sb dl_dhist_sb hist_sb)/dq.
+ * per_atom for tsb_adjoint_workspace_size: 2*ns*ns (hvp) or n_bins (rdf). */
+size_t tsb_adjoint_workspace_size(int64_t n_atoms, int64_t n_systems, int64_t per_atom);
+int tsb_lj_hvp(const double *table, int n_species, const int32_t *species,
+               const double *positions, const double *cell_row, const uint8_t *pbc,
+               const int64_t *system_idx, int64_t n_atoms, int64_t n_systems, double cutoff,
+               const double *v, double coef, double *lam_q, double *grad_params,
+               void *workspace, size_t workspace_bytes, void *stream);
+int tsb_rdf_hist(const double *positions, const double *cell_row, const uint8_t *pbc,
+                 const int64_t *system_idx, int64_t n_atoms, int64_t n_systems, double r_max,
+                 int n_bins, double width, double *hist, void *workspace,
+                 size_t workspace_bytes, void *stream);
+int tsb_rdf_hist_grad(const double *positions, const double *cell_row, const uint8_t *pbc,
+                      const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
+                      double r_max, int n_bins, double width, const double *dl_dhist,
+                      double *grad_positions, void *workspace, size_t workspace_bytes,
+                      void *stream);
+
 /* ---- FIRE + Frechet cell filter -----------------------------------------
  * Per-system state arrays (dtype): dt [S], alpha [S], n_pos [S] int32; cell,
  * reference_cell, cell_positions, cell_velocities, cell_forces [S,3,3] in the

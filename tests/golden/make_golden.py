@@ -20,6 +20,10 @@ Outputs (small ``.npz`` files beside this script):
 * ``md.npz``        NVE (velocity Verlet) and NVT-Langevin (BAOAB) trajectories,
                     with the Langevin noise recorded
 * ``fire.npz``      ASE-FIRE + Frechet cell filter and VV-FIRE trajectories
+* ``adjoint.npz``   gradients of a 20-step NVE histogram loss w.r.t. sigma,
+                    epsilon, q0, p0 by FP64 autograd with create_graph=True (the
+                    exact trajectory derivative), and the reference's own
+                    retain_graph=True route for comparison
 * ``math.npz``      expm / Frechet derivative / matrix log of 3x3 batches
 """
 
@@ -278,6 +282,116 @@ def main(ref_root):
     for k in ("masses", "system_idx", "atomic_numbers", "cell"):
         out[f"vv/{k}"] = ka2[k]
     np.savez_compressed(os.path.join(HERE, "fire.npz"), **out)
+
+    # ------------------------------------------------------------- adjoint
+    # FP64 restatement of an NVE trajectory with autograd through the forces
+    # (create_graph=True keeps the Hessian terms), on the reference's own LJ
+    # pair function and neighbour list; plus the reference's retain_graph route.
+    from torch_sim.models.pair_potential import full_to_half_list
+    from torch_sim.transforms import compute_cell_shifts
+
+    out = {}
+    ad = W.argon_species_batch(2, (2, 2, 2), jitter=0.05, seed=5)
+    n_steps, dt_ad, rc_ad = 20, 0.002 * W.METAL_TIME, 2.5 * 3.405
+    sp = T(ad["atomic_numbers"] - 1, torch.long)
+    row_cell = T(np.transpose(ad["cell"], (0, 2, 1)))
+    pbc2 = torch.ones((2, 3), dtype=torch.bool)
+    sysi = T(ad["system_idx"], torch.long)
+    masses = T(ad["masses"])
+    gen = torch.Generator().manual_seed(11)
+    p0 = torch.randn((len(masses), 3), generator=gen, dtype=torch.float64) * torch.sqrt(
+        masses * 80.0 * W.KB_EV).unsqueeze(-1)
+    q0 = T(ad["positions"])
+    rng_ad = np.random.default_rng(4)
+    sig0 = torch.full((2, 2), 3.405, dtype=torch.float64)
+    eps0 = torch.full((2, 2), 0.0104, dtype=torch.float64)
+    sig = sig0.clone()
+    eps_ = eps0.clone()
+    for a_ in range(2):
+        for b_ in range(a_, 2):
+            fs, fe = 1 + rng_ad.uniform(-0.05, 0.05, 2)
+            sig[a_, b_] = sig[b_, a_] = 3.405 * fs
+            eps_[a_, b_] = eps_[b_, a_] = 0.0104 * fe
+
+    def pairs_of(q, cut):
+        m, sm, sh = torch_nl_linked_cell(q.detach(), row_cell, pbc2, cut, sysi)
+        m, sm, sh = full_to_half_list(m, sm, sh)
+        cs = compute_cell_shifts(row_cell, sh, sm)
+        return m, sm, q[m[1]] - q[m[0]] + cs
+
+    def energy(q, sg, ep):
+        m, _, dr = pairs_of(q, rc_ad)
+        r = dr.norm(dim=1)
+        a_, b_ = sp[m[0]], sp[m[1]]
+        v = lennard_jones_pair(r, None, None, sg[a_, b_], ep[a_, b_])
+        return torch.where(r < rc_ad, v, torch.zeros_like(v)).sum()
+
+    def force(q, sg, ep, graph=True):
+        (g_,) = torch.autograd.grad(energy(q, sg, ep), q, create_graph=graph)
+        return -g_
+
+    centers = (torch.arange(64, dtype=torch.float64) + 0.5) * (8.0 / 64)
+
+    def hist(q):
+        m, sm, dr = pairs_of(q, 8.0)
+        r = dr.norm(dim=1)
+        w_ = torch.exp(-((r[:, None] - centers[None]) ** 2) / (2 * 0.05 ** 2))
+        w_ = torch.where((r < 8.0)[:, None], w_, torch.zeros_like(w_))
+        return torch.zeros((2, 64), dtype=torch.float64).index_add(0, sm, w_)
+
+    def run(q, p, sg, ep, graph=True):
+        f = force(q, sg, ep, graph)
+        for _ in range(n_steps):
+            p = p + f * (dt_ad / 2)
+            q = q + p / masses.unsqueeze(-1) * dt_ad
+            f = force(q, sg, ep, graph)
+            p = p + f * (dt_ad / 2)
+        return q
+
+    q_t = run(q0.clone().requires_grad_(True), p0, sig0, eps0, graph=False).detach()
+    target = hist(q_t).detach()
+    sg_ = sig.clone().requires_grad_(True)
+    ep_ = eps_.clone().requires_grad_(True)
+    qq = q0.clone().requires_grad_(True)
+    pp = p0.clone().requires_grad_(True)
+    loss = ((hist(run(qq, pp, sg_, ep_)) - target) ** 2).sum()
+    gs_, ge_, gq_, gp_ = torch.autograd.grad(loss, [sg_, ep_, qq, pp])
+    out["adj/positions"] = ad["positions"]
+    out["adj/cell"] = ad["cell"]
+    out["adj/masses"] = ad["masses"]
+    out["adj/system_idx"] = ad["system_idx"]
+    out["adj/atomic_numbers"] = ad["atomic_numbers"]
+    out["adj/p0"] = p0.numpy()
+    out["adj/sigma"] = sig.numpy()
+    out["adj/epsilon"] = eps_.numpy()
+    out["adj/target"] = target.numpy()
+    out["adj/loss"] = np.array(float(loss))
+    out["adj/n_steps"] = np.array(n_steps)
+    out["adj/dt"] = np.array(dt_ad)
+    sym = lambda g_: (g_ + g_.T - torch.diag(torch.diagonal(g_))).numpy()  # noqa: E731
+    out["adj/grad_sigma"] = sym(gs_)
+    out["adj/grad_epsilon"] = sym(ge_)
+    out["adj/grad_q0"] = gq_.numpy()
+    out["adj/grad_p0"] = gp_.numpy()
+    # the reference's route: PairPotentialModel(retain_graph=True) inside nve_step
+    def ka2(dr, zi, zj, sg=sg_, ep=ep_):
+        return lennard_jones_pair(dr, zi, zj, sg[zi - 1, zj - 1], ep[zi - 1, zj - 1])
+
+    model_rg = PairPotentialModel(pair_fn=ka2, cutoff=rc_ad, reduce_to_half_list=True,
+                                  retain_graph=True)
+    st = to_state(ad)
+    st.positions = q0.clone().requires_grad_(True)
+    q_leaf = st.positions
+    md = ts.nve_init(st, model_rg, kT=torch.tensor(80.0 * W.KB_EV))
+    md.momenta = p0.clone()
+    md.forces = model_rg(md)["forces"]
+    for _ in range(n_steps):
+        md = ts.nve_step(md, model_rg, dt=torch.tensor(dt_ad))
+    loss_rg = ((hist(md.positions) - target) ** 2).sum()
+    (gq_rg,) = torch.autograd.grad(loss_rg, [q_leaf], allow_unused=True)
+    out["adj/ref_retain_graph_grad_q0"] = gq_rg.numpy()
+    out["adj/ref_retain_graph_loss"] = np.array(float(loss_rg))
+    np.savez_compressed(os.path.join(HERE, "adjoint.npz"), **out)
 
     # ---------------------------------------------------------------- math
     import torch_sim.math as tsm

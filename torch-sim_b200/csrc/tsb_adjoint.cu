@@ -1,0 +1,232 @@
+// Kernels for the hand-written adjoint of NVE (velocity Verlet) trajectories
+// with species-matrix Lennard-Jones forces, in FP64 throughout.
+//
+// The reference differentiates trajectories with torch.autograd through
+// PairPotentialModel (pair_potential.py:420-425, create_graph=False), which
+// drops the force-Jacobian terms; here the discrete adjoint is exact:
+//   lam_p += (dt/m) lam_q ;  lam_q += c * J_F(q)^T lam_p ;  g_theta += c * dF/dtheta^T lam_p
+// with J_F = -Hessian(E).  For a pair (i, j) with d = r_j - r_i, r = |d|,
+// u = d / r, the Hessian block is K = V'' u u^T + (V'/r)(I - u u^T) and
+// (H v)_i = sum_j K (v_i - v_j); the force is F_i = sum_j V'(r) u, so
+// dF_i/dtheta = sum_j (dV'/dtheta) u.
+//
+// Also: the Gaussian-smeared pair-distance histogram of each system and its
+// gradient with respect to positions (the trajectory loss).
+#include "tsb_search.cuh"
+
+namespace tsb {
+
+constexpr int kAdjMaxSpecies = 4;
+
+struct AdjWork {
+  BinData b;
+  double *part;  // per-atom partials (parameter gradients or histogram bins)
+};
+
+static void carve_adj(Carver &c, AdjWork &w, int64_t n, int64_t ns, int64_t per_atom) {
+  carve_bins(c, w.b, n, ns);
+  w.part = c.take<double>(n * per_atom);
+}
+
+// LJ: V = 4 eps (s^12 - s^6), s = sigma / r (lennard_jones.py:23-47)
+//   V'  = -(24 eps / r)(2 s^12 - s^6)
+//   V'' = (24 eps / r^2)(26 s^12 - 7 s^6)
+//   dV'/deps = V' / eps ;  dV'/dsigma = -(144 eps / (r sigma))(4 s^12 - s^6)
+__global__ void __launch_bounds__(128)
+    k_lj_hvp(BinData b, int64_t n, const double *__restrict__ table, int nsp,
+             const int32_t *__restrict__ species, double cutoff, const double *__restrict__ v,
+             double coef, double *__restrict__ lam_q, double *__restrict__ gpart) {
+  __shared__ double sig[kAdjMaxSpecies * kAdjMaxSpecies], eps[kAdjMaxSpecies * kAdjMaxSpecies],
+      rc2[kAdjMaxSpecies * kAdjMaxSpecies];
+  for (int k = threadIdx.x; k < nsp * nsp; k += blockDim.x) {
+    sig[k] = table[5 * k];
+    eps[k] = table[5 * k + 1];
+    const double r = fmin(cutoff, table[5 * k + 3]);
+    rc2[k] = r * r;
+  }
+  __syncthreads();
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const double4 w = b.spos[p];
+  const int i = (int)__double_as_longlong(w.w);
+  const SysGeom &G = b.geom[b.sys_of[i]];
+  const int si = species ? min(max(species[i], 0), nsp - 1) : 0;
+  const double vi0 = v[3 * i], vi1 = v[3 * i + 1], vi2 = v[3 * i + 2];
+  double hx = 0, hy = 0, hz = 0;
+  double gs[kAdjMaxSpecies * kAdjMaxSpecies], ge[kAdjMaxSpecies * kAdjMaxSpecies];
+  for (int k = 0; k < nsp * nsp; ++k) gs[k] = ge[k] = 0.0;
+  search_neighbors(G, b.spos, b.bin_start, i, w.x, w.y, w.z, cutoff * cutoff, false,
+                   [&](int j, int, int, int, double dx, double dy, double dz, double d2) {
+                     const int sj = species ? min(max(species[j], 0), nsp - 1) : 0;
+                     const int k = si * nsp + sj;
+                     if (!(d2 < rc2[k]) || !(d2 > 0.0)) return;
+                     const double r = sqrt(d2), ir = 1.0 / r;
+                     const double ux = dx * ir, uy = dy * ir, uz = dz * ir;
+                     const double s2 = sig[k] * sig[k] / d2, s6 = s2 * s2 * s2, s12 = s6 * s6;
+                     const double e = eps[k];
+                     const double vp = -(24.0 * e * ir) * (2.0 * s12 - s6);
+                     const double vpp = (24.0 * e / d2) * (26.0 * s12 - 7.0 * s6);
+                     const double w0 = vi0 - v[3 * j], w1 = vi1 - v[3 * j + 1], w2 = vi2 - v[3 * j + 2];
+                     const double uw = ux * w0 + uy * w1 + uz * w2;
+                     const double a = vpp - vp * ir;  // K w = a (u.w) u + (V'/r) w
+                     hx += a * uw * ux + vp * ir * w0;
+                     hy += a * uw * uy + vp * ir * w1;
+                     hz += a * uw * uz + vp * ir * w2;
+                     const double uvi = ux * vi0 + uy * vi1 + uz * vi2;
+                     ge[k] += (vp / e) * uvi;
+                     gs[k] += (-(144.0 * e * ir / sig[k]) * (4.0 * s12 - s6)) * uvi;
+                   });
+  // J_F^T v = -H v
+  lam_q[3 * i] -= coef * hx;
+  lam_q[3 * i + 1] -= coef * hy;
+  lam_q[3 * i + 2] -= coef * hz;
+  double *g = gpart + (size_t)i * (2 * nsp * nsp);
+  for (int k = 0; k < nsp * nsp; ++k) {
+    g[2 * k] = coef * gs[k];
+    g[2 * k + 1] = coef * ge[k];
+  }
+}
+
+// Gaussian-smeared histogram of pair distances r < r_max (each unordered pair
+// once): h_b = sum_pairs exp(-(r - c_b)^2 / (2 w^2)), c_b = (b + 1/2) r_max / B.
+__global__ void __launch_bounds__(128)
+    k_rdf_part(BinData b, int64_t n, double r_max, int nb, double width, double *part) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const double4 w = b.spos[p];
+  const int i = (int)__double_as_longlong(w.w);
+  const SysGeom &G = b.geom[b.sys_of[i]];
+  double *h = part + (size_t)i * nb;
+  for (int k = 0; k < nb; ++k) h[k] = 0.0;
+  const double bw = r_max / nb, inv2w2 = 1.0 / (2.0 * width * width);
+  search_neighbors(G, b.spos, b.bin_start, i, w.x, w.y, w.z, r_max * r_max, false,
+                   [&](int, int, int, int, double, double, double, double d2) {
+                     const double r = sqrt(d2);
+                     for (int k = 0; k < nb; ++k) {
+                       const double x = r - (k + 0.5) * bw;
+                       h[k] += 0.5 * exp(-x * x * inv2w2);  // each pair is visited twice
+                     }
+                   });
+}
+
+// dL/dq_i = sum_j dL/dr_ij * (-u_ij), dL/dr = sum_b dL/dh_b * dg/dr
+__global__ void __launch_bounds__(128)
+    k_rdf_grad(BinData b, int64_t n, double r_max, int nb, double width,
+               const double *__restrict__ dl_dh, double *__restrict__ grad) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const double4 w = b.spos[p];
+  const int i = (int)__double_as_longlong(w.w);
+  const int s = b.sys_of[i];
+  const SysGeom &G = b.geom[s];
+  const double *dh = dl_dh + (size_t)s * nb;
+  const double bw = r_max / nb, inv2w2 = 1.0 / (2.0 * width * width), iw2 = 1.0 / (width * width);
+  double gx = 0, gy = 0, gz = 0;
+  search_neighbors(G, b.spos, b.bin_start, i, w.x, w.y, w.z, r_max * r_max, false,
+                   [&](int, int, int, int, double dx, double dy, double dz, double d2) {
+                     const double r = sqrt(d2);
+                     double dlr = 0.0;
+                     for (int k = 0; k < nb; ++k) {
+                       const double x = r - (k + 0.5) * bw;
+                       dlr += dh[k] * (-x * iw2) * exp(-x * x * inv2w2);
+                     }
+                     const double ir = 1.0 / r;
+                     gx -= dlr * dx * ir;
+                     gy -= dlr * dy * ir;
+                     gz -= dlr * dz * ir;
+                   });
+  grad[3 * i] = gx;
+  grad[3 * i + 1] = gy;
+  grad[3 * i + 2] = gz;
+}
+
+// out[s, k] = sum over atoms of system s of part[i, k]  (fixed order)
+__global__ void k_sum_parts(const SysGeom *g, const double *part, int width, double *out,
+                            int accumulate) {
+  const int s = blockIdx.x;
+  const SysGeom &G = g[s];
+  for (int k = threadIdx.x; k < width; k += blockDim.x) {
+    double t = 0.0;
+    for (int a = 0; a < G.count; ++a) t += part[(size_t)(G.start + a) * width + k];
+    out[(size_t)s * width + k] = accumulate ? out[(size_t)s * width + k] + t : t;
+  }
+}
+
+}  // namespace tsb
+
+using namespace tsb;
+
+extern "C" size_t tsb_adjoint_workspace_size(int64_t n_atoms, int64_t n_systems,
+                                             int64_t per_atom) {
+  Carver c(nullptr, (size_t)-1);
+  AdjWork w;
+  carve_adj(c, w, n_atoms, n_systems, per_atom);
+  return c.off + 256;
+}
+
+extern "C" int tsb_lj_hvp(const double *table, int n_species, const int32_t *species,
+                          const double *positions, const double *cell_row, const uint8_t *pbc,
+                          const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
+                          double cutoff, const double *v, double coef, double *lam_q,
+                          double *grad_params, void *workspace, size_t workspace_bytes,
+                          void *stream) {
+  if (n_species < 1 || n_species > kAdjMaxSpecies || !table || (n_species > 1 && !species) ||
+      n_atoms < 1 || n_systems < 1 || !positions || !cell_row || !pbc || !system_idx || !v ||
+      !lam_q || !grad_params || !(cutoff > 0.0))
+    return TSB_ERR_INVALID_ARG;
+  const int per_atom = 2 * n_species * n_species;
+  Carver c(workspace, workspace_bytes);
+  AdjWork w;
+  carve_adj(c, w, n_atoms, n_systems, per_atom);
+  if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  TSB_TRY(prepare_bins<double>(positions, cell_row, pbc, system_idx, n_atoms, n_systems, cutoff,
+                               w.b, st));
+  k_lj_hvp<<<grid_for(n_atoms, 128), 128, 0, st>>>(w.b, n_atoms, table, n_species, species,
+                                                   cutoff, v, coef, lam_q, w.part);
+  // per-system parameter gradients, accumulated into grad_params [S, ns, ns, 2]
+  k_sum_parts<<<(unsigned)n_systems, 64, 0, st>>>(w.b.geom, w.part, per_atom, grad_params, 1);
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
+
+extern "C" int tsb_rdf_hist(const double *positions, const double *cell_row, const uint8_t *pbc,
+                            const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
+                            double r_max, int n_bins, double width, double *hist,
+                            void *workspace, size_t workspace_bytes, void *stream) {
+  if (n_atoms < 1 || n_systems < 1 || !positions || !cell_row || !pbc || !system_idx || !hist ||
+      n_bins < 1 || !(r_max > 0.0) || !(width > 0.0))
+    return TSB_ERR_INVALID_ARG;
+  Carver c(workspace, workspace_bytes);
+  AdjWork w;
+  carve_adj(c, w, n_atoms, n_systems, n_bins);
+  if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  TSB_TRY(prepare_bins<double>(positions, cell_row, pbc, system_idx, n_atoms, n_systems, r_max,
+                               w.b, st));
+  k_rdf_part<<<grid_for(n_atoms, 128), 128, 0, st>>>(w.b, n_atoms, r_max, n_bins, width, w.part);
+  k_sum_parts<<<(unsigned)n_systems, 64, 0, st>>>(w.b.geom, w.part, n_bins, hist, 0);
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
+
+extern "C" int tsb_rdf_hist_grad(const double *positions, const double *cell_row,
+                                 const uint8_t *pbc, const int64_t *system_idx, int64_t n_atoms,
+                                 int64_t n_systems, double r_max, int n_bins, double width,
+                                 const double *dl_dhist, double *grad_positions,
+                                 void *workspace, size_t workspace_bytes, void *stream) {
+  if (n_atoms < 1 || n_systems < 1 || !positions || !cell_row || !pbc || !system_idx ||
+      !dl_dhist || !grad_positions || n_bins < 1 || !(r_max > 0.0) || !(width > 0.0))
+    return TSB_ERR_INVALID_ARG;
+  Carver c(workspace, workspace_bytes);
+  AdjWork w;
+  carve_adj(c, w, n_atoms, n_systems, n_bins);
+  if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  TSB_TRY(prepare_bins<double>(positions, cell_row, pbc, system_idx, n_atoms, n_systems, r_max,
+                               w.b, st));
+  k_rdf_grad<<<grid_for(n_atoms, 128), 128, 0, st>>>(w.b, n_atoms, r_max, n_bins, width,
+                                                     dl_dhist, grad_positions);
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
