@@ -457,6 +457,17 @@ def main():
     h2d = 3 * hx.numel() * 8
     d2h = 2 * hx.numel() * 8 + oe.numel() * 8
 
+    # force error of the fused kernel's FP32 pair arithmetic vs an FP64 evaluation
+    # of the same final configuration (the metric's "force err <= 1e-5 vs FP64")
+    from tsb import models as _models
+
+    md.positions, md.forces = runner.x, runner.f
+    ref64 = _models.MorseModel(sigma=2.866, epsilon=0.3429, alpha=1.3588, cutoff=6.0,
+                               precision="fp64", device=device)(md)["forces"]
+    df = (runner.f - ref64).abs()
+    force_err = {"max_abs_over_max_abs": float(df.max() / ref64.abs().max()),
+                 "rms_rel": float(df.pow(2).mean().sqrt() / ref64.pow(2).mean().sqrt())}
+
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
         alg_bytes = n_atoms * args.md_steps * ALG_BYTES_PER_ATOM_STEP
@@ -481,6 +492,7 @@ def main():
                          "kernel": "k_fused_md"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
+            "force_err_vs_fp64": force_err,
             "gpu_launches": 2 * args.steps,
             "clocks": clocks.summary(),
             "per_launch_ms": per_launch_ms,

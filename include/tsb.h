@@ -239,6 +239,10 @@ int tsb_fire_converged(const void *forces, const int64_t *system_idx, int64_t n_
  * TSB_ERR_UNSUPPORTED for a system that does not fit even with zero skin
  * (that system is left unchanged); status[1] its index, status[2] which table
  * (1 images, 2 neighbour slots), status[3] the size that did not fit.
+ * The Langevin noise of MD step t (0-based within the launch) is drawn with
+ * Philox counter `counter + t` (+ *counter_dev when counter_dev is not NULL; the
+ * call then advances *counter_dev by n_steps on the stream, so a captured CUDA
+ * graph draws fresh noise on every replay).
  * Requirements: pbc all true, n_atoms per system <= tsb_fused_max_atoms(). */
 int tsb_fused_max_atoms(void);
 size_t tsb_fused_workspace_size(int64_t n_atoms, int64_t n_systems);
@@ -248,9 +252,9 @@ int tsb_fused_md(int integrator, int potential, const double *table, int n_speci
                  const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
                  const int32_t *order, double cutoff, double skin, int64_t n_steps,
                  const double *dt_sys, const double *kT_sys, const double *gamma_sys,
-                 uint64_t seed, uint64_t counter, double *energy, int32_t *n_rebuilds,
-                 int32_t *status, void *workspace, size_t workspace_bytes,
-                 void *stream);
+                 uint64_t seed, uint64_t counter, uint64_t *counter_dev, double *energy,
+                 int32_t *n_rebuilds, int32_t *status, void *workspace,
+                 size_t workspace_bytes, void *stream);
 
 /* ---- allocation-free fused MD -------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device

@@ -206,3 +206,25 @@ def test_fused_adaptive_skin_same_physics():
     b = integrators.run_md(md.clone(), m, 30, integrator="nve", dt=dt, skin=0.3)
     np.testing.assert_allclose(a.positions.cpu(), b.positions.cpu(), atol=1e-5)
     np.testing.assert_allclose(a.energy.cpu(), b.energy.cpu(), rtol=1e-5)
+
+
+def test_fused_graph_replay_matches_direct_launches():
+    """The persistent kernel under a captured CUDA graph: two replays equal two
+    direct launches bitwise (the device Philox counter advances per replay)."""
+    from tsb import integrators, workloads
+
+    md, m = _cu_state(6, seed=17)
+    kw = dict(integrator="nvt_langevin", dt=0.002 * workloads.METAL_TIME,
+              kT=1000 * workloads.KB_EV, gamma=10.0 / workloads.METAL_TIME, seed=99)
+    a = integrators.FusedMD(md.clone(), m, **kw)
+    a.launch(25)
+    a.launch(25)
+    b = integrators.FusedMD(md.clone(), m, **kw)
+    g = b.graph(25)
+    g.replay()
+    g.replay()
+    torch.cuda.synchronize()
+    a.check()
+    b.check()
+    assert a.counter == b.counter == 50
+    assert torch.equal(a.x, b.x) and torch.equal(a.p, b.p) and torch.equal(a.energy, b.energy)

@@ -68,7 +68,9 @@ def test_static_entry_matches_workspace_entry_on_two_calls():
         for call, counter in ((0, 0), (1, 40)):  # two calls in a row, trajectory continues
             args, keep = _args(md, m, x, p, f, energy, rebuilds, status, 40, counter)
             if name == "tsb_fused_md":
-                rc = lib.tsb_fused_md(*args, L.ptr(ws), ws.numel(), stream)
+                a = list(args)
+                a.insert(22, None)  # counter_dev: none, the counter is passed by value
+                rc = lib.tsb_fused_md(*a, L.ptr(ws), ws.numel(), stream)
             else:
                 rc = lib.tsb_fused_md_static(*args, stream)
             assert rc == L.TSB_OK, (name, call, rc)

@@ -60,6 +60,7 @@ struct FusedArgs {
   int64_t n_steps;
   const double *dt, *kT, *gamma;
   uint64_t seed, counter;
+  const uint64_t *counter_dev;  // optional device-resident counter added to `counter`
   double *energy;
   int32_t *n_rebuilds;
   int32_t *queue;
@@ -196,6 +197,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     prm[k] = make_prm<float>(POT, A.table + 5 * k, A.cutoff);
   __syncthreads();
   const PairPrm<float> p0 = prm[0];  // single-species parameters in registers
+  const uint64_t counter0 = A.counter + (A.counter_dev ? *A.counter_dev : 0ull);
 
   for (;;) {
     __syncthreads();
@@ -449,7 +451,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
           x1 += (py * inv_m) * half;
           x2 += (pz * inv_m) * half;
           float z[3];
-          normal3f(A.seed, (uint64_t)gi, A.counter + (uint64_t)step, z);
+          normal3f(A.seed, (uint64_t)gi, counter0 + (uint64_t)step, z);
           px = c1 * px + c2m * z[0];
           py = c1 * py + c2m * z[1];
           pz = c1 * pz + c2m * z[2];
@@ -544,6 +546,10 @@ extern "C" size_t tsb_fused_workspace_size(int64_t n_atoms, int64_t n_systems) {
   return c.off + 256;
 }
 
+__global__ void k_advance_counter(uint64_t *counter_dev, int64_t n_steps) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *counter_dev += (uint64_t)n_steps;
+}
+
 __global__ void k_bounds_fused(const int64_t *sys, int64_t n, int64_t *lo, int64_t *hi) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -567,8 +573,9 @@ extern "C" int tsb_fused_md(int integrator, int potential, const double *table,
                             double cutoff, double skin, int64_t n_steps,
                             const double *dt_sys, const double *kT_sys,
                             const double *gamma_sys, uint64_t seed, uint64_t counter,
-                            double *energy, int32_t *n_rebuilds, int32_t *status,
-                            void *workspace, size_t workspace_bytes, void *stream) {
+                            uint64_t *counter_dev, double *energy, int32_t *n_rebuilds,
+                            int32_t *status, void *workspace, size_t workspace_bytes,
+                            void *stream) {
   if (integrator != TSB_INT_NVE && integrator != TSB_INT_LANGEVIN) return TSB_ERR_INVALID_ARG;
   if (potential < TSB_POT_LJ || potential > TSB_POT_SOFT) return TSB_ERR_INVALID_ARG;
   if (n_species < 1 || !table || (n_species > 1 && !species)) return TSB_ERR_INVALID_ARG;
@@ -598,7 +605,8 @@ extern "C" int tsb_fused_md(int integrator, int potential, const double *table,
   k_bounds_fused<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, lo, hi);
   FusedArgs A{integrator, potential, n_species, table, species, positions, momenta, forces,
               masses, cell_row, lo, hi, n_systems, order, cutoff, skin, n_steps, dt_sys,
-              kT_sys, gamma_sys, seed, counter, energy, n_rebuilds, queue, status};
+              kT_sys, gamma_sys, seed, counter, counter_dev, energy, n_rebuilds, queue,
+              status};
   const bool multi = n_species > 1;
   if (potential == TSB_POT_LJ) {
     multi ? launch_fused<TSB_POT_LJ, true>(A, grid, st) : launch_fused<TSB_POT_LJ, false>(A, grid, st);
@@ -609,6 +617,7 @@ extern "C" int tsb_fused_md(int integrator, int potential, const double *table,
     multi ? launch_fused<TSB_POT_SOFT, true>(A, grid, st)
           : launch_fused<TSB_POT_SOFT, false>(A, grid, st);
   }
+  if (counter_dev) k_advance_counter<<<1, 32, 0, st>>>(counter_dev, n_steps);
   TSB_CHECK_LAUNCH();
   return TSB_OK;
 }
@@ -694,7 +703,7 @@ extern "C" int tsb_fused_md_static(int integrator, int potential, const double *
   k_bounds_fused<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, lo, hi);
   FusedArgs A{integrator, potential, n_species, table, species, positions, momenta, forces,
               masses, cell_row, lo, hi, n_systems, order, cutoff, skin, n_steps, dt_sys,
-              kT_sys, gamma_sys, seed, counter, energy, n_rebuilds, queue, status};
+              kT_sys, gamma_sys, seed, counter, nullptr, energy, n_rebuilds, queue, status};
   const bool multi = n_species > 1;
   if (potential == TSB_POT_LJ) {
     multi ? launch_fused<TSB_POT_LJ, true>(A, grid, st) : launch_fused<TSB_POT_LJ, false>(A, grid, st);

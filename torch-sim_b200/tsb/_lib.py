@@ -76,7 +76,7 @@ PROTOTYPES = {
     "tsb_fused_max_atoms": (_int, []),
     "tsb_fused_workspace_size": (_sz, [_i64, _i64]),
     "tsb_fused_md": (_int, [_int, _int, _vp, _int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64,
-                            _i64, _vp, _dbl, _dbl, _i64, _vp, _vp, _vp, _u64, _u64, _vp,
+                            _i64, _vp, _dbl, _dbl, _i64, _vp, _vp, _vp, _u64, _u64, _vp, _vp,
                             _vp, _vp, _vp, _sz, _vp]),
     "tsb_fused_md_static": (_int, [_int, _int, _vp, _int, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                    _i64, _i64, _vp, _dbl, _dbl, _i64, _vp, _vp, _vp, _u64,

@@ -224,7 +224,14 @@ class FusedMD:
         self.skin = float(skin)
         self.seed = (seed if seed is not None
                      else getattr(state, "_philox_seed", _seed_of(state))) & (2**64 - 1)
-        self.counter = getattr(state, "_philox_counter", 0)
+        # Philox counter lives on the device so that graph replays advance it
+        self.counter_dev = torch.tensor([getattr(state, "_philox_counter", 0)],
+                                        dtype=torch.int64, device=dev)
+        self._graphs = {}
+
+    @property
+    def counter(self) -> int:
+        return int(self.counter_dev.item())
 
     def launch(self, n_steps: int, stream: int | None = None) -> None:
         m = self.model
@@ -232,10 +239,29 @@ class FusedMD:
                L.ptr(self.species), L.ptr(self.x), L.ptr(self.p), L.ptr(self.f), L.ptr(self.m),
                L.ptr(self.cell_row), L.ptr(self.sys_idx), self.n, self.n_sys,
                L.ptr(self.order), m.cutoff, self.skin, int(n_steps), L.ptr(self.dt_s),
-               L.ptr(self.kT_s), L.ptr(self.g_s), self.seed, self.counter, L.ptr(self.energy),
-               L.ptr(self.rebuilds), L.ptr(self.status), L.ptr(self.ws), self.ws.numel(),
-               stream if stream is not None else L.stream_ptr(self.dev))
-        self.counter += int(n_steps)
+               L.ptr(self.kT_s), L.ptr(self.g_s), self.seed, 0, L.ptr(self.counter_dev),
+               L.ptr(self.energy), L.ptr(self.rebuilds), L.ptr(self.status), L.ptr(self.ws),
+               self.ws.numel(), stream if stream is not None else L.stream_ptr(self.dev))
+
+    def graph(self, n_steps: int) -> "torch.cuda.CUDAGraph":
+        """CUDA graph of one ``launch(n_steps)``; ``g.replay()`` advances every system
+        by n_steps with fresh Langevin noise (the device counter moves on)."""
+        if n_steps not in self._graphs:
+            torch.cuda.synchronize(self.dev)
+            saved = [t.clone() for t in (self.x, self.p, self.f, self.counter_dev)]
+            s = torch.cuda.Stream(self.dev)
+            s.wait_stream(torch.cuda.current_stream(self.dev))
+            with torch.cuda.stream(s):  # warm-up outside capture (sets kernel attributes)
+                self.launch(n_steps)
+            torch.cuda.current_stream(self.dev).wait_stream(s)
+            torch.cuda.synchronize(self.dev)
+            for t, v in zip((self.x, self.p, self.f, self.counter_dev), saved):
+                t.copy_(v)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self.launch(n_steps)
+            self._graphs[n_steps] = g
+        return self._graphs[n_steps]
 
     def check(self) -> None:
         st = self.status.tolist()
