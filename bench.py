@@ -40,7 +40,7 @@ WORKLOAD = ("2048 Cu fcc systems (8-512 atoms, strain +-2%, shear +-3deg), Morse
             "(D=0.3429 eV, alpha=1.3588/A, r0=2.866 A, rc=6.0 A), NVT-Langevin BAOAB "
             "1000 K, dt=2 fs, gamma=0.01/fs")
 ALG_BYTES_PER_ATOM_STEP = 76  # streaming state r/w: 48 B FP64 pos + 24 B mom + 4 B type/mass
-SKIN = 1.4  # Verlet skin (A); shrunk per system on the device when tables overflow
+SKIN = 0.7  # Verlet skin (A); shrunk per system on the device when tables overflow
 
 
 def parse():

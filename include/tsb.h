@@ -237,8 +237,12 @@ int tsb_fire_converged(const void *forces, const int64_t *system_idx, int64_t n_
  * smaller skin (results are unchanged; only the rebuild rate grows).
  * `status` [4] int32 device out: status[0] is TSB_OK, or TSB_ERR_CAPACITY /
  * TSB_ERR_UNSUPPORTED for a system that does not fit even with zero skin
- * (that system is left unchanged); status[1] its index, status[2] which table
- * (1 images, 2 neighbour slots), status[3] the size that did not fit.
+ * (its positions and momenta are left unchanged, its forces are not);
+ * status[1] its index, status[2] which table (1 images, 2 neighbour slots),
+ * status[3] the size that did not fit.  While a system runs, its rows of
+ * `forces` hold FP64 positions (the kernel decides whether a pair is inside
+ * the cutoff on them when FP32 rounding could flip the decision); the final
+ * forces are written over them.
  * The Langevin noise of MD step t (0-based within the launch) is drawn with
  * Philox counter `counter + t` (+ *counter_dev when counter_dev is not NULL; the
  * call then advances *counter_dev by n_steps on the stream, so a captured CUDA

@@ -20,8 +20,11 @@ __global__ void __launch_bounds__(128)
                   P *energies, P *stresses, double *e_half, double *vir_half,
                   const uint8_t *__restrict__ sys_active) {
   __shared__ PairPrm<R> prm[kMaxSpecies * kMaxSpecies];
-  for (int k = threadIdx.x; k < ns_species * ns_species; k += blockDim.x)
+  __shared__ double prc2[kMaxSpecies * kMaxSpecies];
+  for (int k = threadIdx.x; k < ns_species * ns_species; k += blockDim.x) {
     prm[k] = make_prm<R>(POT, table + 5 * k, cutoff);
+    prc2[k] = pair_rc2(POT, table + 5 * k, cutoff);
+  }
   __syncthreads();
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
@@ -36,12 +39,12 @@ __global__ void __launch_bounds__(128)
   R fx = 0, fy = 0, fz = 0;
   double ei = 0, vxx = 0, vyy = 0, vzz = 0, vyz = 0, vxz = 0, vxy = 0;
   search_neighbors(G, b.spos, b.bin_start, i, w.x, w.y, w.z, cutoff * cutoff, false,
-                   [&](int j, int, int, int, double dx, double dy, double dz, double) {
+                   [&](int j, int, int, int, double dx, double dy, double dz, double d2) {
                      const int sj = species ? min(max(species[j], 0), ns_species - 1) : 0;
+                     if (!(d2 < prc2[si * ns_species + sj])) return;  // FP64 decision
                      const PairPrm<R> &q = row[sj];
                      const R rx = (R)dx, ry = (R)dy, rz = (R)dz;
                      const R r2 = rx * rx + ry * ry + rz * rz;
-                     if (!(r2 < q.a3)) return;
                      R e, fr;
                      pair_eval<POT, R>(q, r2, e, fr);
                      const R gx = fr * rx, gy = fr * ry, gz = fr * rz;  // force on j

@@ -14,17 +14,29 @@
 //     independent: no grid-wide synchronisation, no host round trips).
 //   * Everything the step loop touches lives in shared memory: the system's
 //     atoms and the periodic images ("ghosts") within cutoff+skin of the cell as
-//     float4 (x, y, z, species) in cell-centre-relative FP32 coordinates, FP64
-//     copies of the positions for refreshing the ghosts, and the Verlet list
-//     (cutoff + skin) as a uint16 ELL table [slot group][thread] that each thread
-//     reads four entries per 64-bit load.  FP64 positions/momenta live in the
-//     registers of the owning threads.
+//     float4 (x, y, z, species) in cell-centre-relative FP32 coordinates, and
+//     the Verlet list (cutoff + skin) as a uint16 ELL table [slot group][thread]
+//     that each thread reads four entries per 64-bit load.  FP64
+//     positions/momenta live in the registers of the owning threads.
 //   * The list is rebuilt on the device when any atom of the system moved more
-//     than skin/2 since the last build.
-//   * Small systems use 2..32 threads per atom (lanes split the list and reduce
-//     with warp shuffles).  Summation orders are fixed: results are
-//     deterministic and a system's trajectory does not depend on the batch.
+//     than skin/2 since the last build.  A rebuild sorts atoms + images into
+//     bins of half the list radius in fractional coordinates (counting sort in
+//     shared memory, entries ordered by index inside a bin) and each atom scans
+//     the 5 x 5 x 5 bins around its own, row by row over contiguous entries.
+//   * The list has two parts: "core" pairs (slots from the bottom), closer at
+//     the build than cutoff - skin, stay inside the cutoff for the list's whole
+//     life and are evaluated without any cutoff test; "shell" pairs (slots from
+//     the top) get the cutoff test.
+//   * Small systems use 2..32 threads per atom (lanes split the candidates and
+//     the list and reduce with warp shuffles).  Summation orders are fixed:
+//     results are deterministic and a system's trajectory does not depend on
+//     the batch.
 //   * Pair arithmetic FP32; positions, momenta and per-system energy FP64.
+//     Whether a pair is inside the cutoff is decided as in FP64: a shell pair
+//     whose FP32 r^2 lies within the proven FP32 rounding bound of the
+//     cutoff^2 is re-tested on FP64 positions.  Those live in the caller's
+//     force array while the system runs (wrapped, cell-centre relative; the
+//     forces are held in registers and written over them at the end).
 #include <math.h>
 
 #include <mutex>
@@ -37,14 +49,20 @@ namespace tsb {
 constexpr int kFusedThreads = 512;
 constexpr int kFusedMaxAtoms = 512;
 constexpr int kExtMax = 3328;        // atoms + ghost images per system
-constexpr int kListLen = 152;        // Verlet-list slots per thread (multiple of 4)
+constexpr int kListLen = 144;        // Verlet-list slots per thread (multiple of 4)
 constexpr int kListGroups = kListLen / 4;
+constexpr int kMaxBins = 2048;       // spatial bins over the image region
 constexpr int kFusedMaxSpecies = 4;
 constexpr int kMaxGrid = 296;        // upper bound on persistent CTAs
 constexpr size_t kSmemList = (size_t)kListGroups * kFusedThreads * sizeof(uint2);
 constexpr size_t kSmemExt = (size_t)kExtMax * sizeof(float4);
 constexpr size_t kSmemGhost = (size_t)kExtMax * sizeof(uint32_t);
-constexpr size_t kFusedSmem = kSmemList + kSmemExt + kSmemGhost;
+constexpr size_t kSmemSorted = (size_t)kExtMax * sizeof(uint16_t);
+constexpr size_t kSmemBins = (size_t)kMaxBins * sizeof(int);
+constexpr size_t kFusedSmem = kSmemList + kSmemExt + kSmemGhost + kSmemSorted + kSmemBins;
+// the bin of every entry is kept in the list area while the list is rebuilt
+static_assert(kExtMax * sizeof(uint16_t) <= kSmemList, "bin ids alias the list");
+static_assert(kMaxBins <= 4 * kFusedThreads, "bin scan: four bins per thread");
 
 struct FusedArgs {
   int integrator, potential, n_species;
@@ -67,28 +85,93 @@ struct FusedArgs {
   int32_t *status;
 };
 
-// per-system geometry, computed once by thread 0 into shared memory
+// per-system geometry, computed by thread 0 into shared memory
 struct FusedGeom {
   double C[9];    // row-vector cell
   double T[9];    // inv(C)^T: fractional coordinates u = T r
   double ctr[3];  // cell centre
   double tn[3];   // |row k of T|
-  double h[3];    // (cutoff + skin) * |row k of T|
+  double h[3];    // (cutoff + skin) * |row k of T|: image margin, fractional
+  double iw[3];   // 1 / bin width, fractional
   double skin;    // this system's current Verlet skin
+  double half_skin2;    // (skin / 2)^2: rebuild when an atom moved further
+  double dt, half, c1;  // time step, dt / 2, Langevin exp(-gamma dt)
+  float band;     // FP32 r^2 within +-band of cutoff^2: decide in FP64
+  float build2;   // list radius^2 used by the FP32 build test
+  float core2[kFusedMaxSpecies * kFusedMaxSpecies];  // core-pair bound^2 per pair type
   int rep[3];
+  int nb[3];
+  int nbins;
   int n, tpa, ok;
   int64_t start;
 };
 
-// margins of the ghost region for the current skin (thread 0 only)
-__device__ inline bool set_margins(FusedGeom &g, double cutoff) {
+// Margins of the image region, bins, FP32 error bounds and core radii for the
+// current skin (thread 0 only).
+//
+// Error bounds: every image y (FP64) is stored as fl32(y) with |y_m| <= Y (per
+// coordinate, Y = max_m sum_k (1/2 + h_k) |C_km|), so each coordinate carries
+// an error <= 2^-24 Y and a difference d_m one <= 2^-24 (2Y + |d_m|).
+//   * band: for |d| ~ rc the FP32 r^2 differs from the exact one by at most
+//     2^-24 (4 sqrt3 Y rc + 2 rc^2), plus 3 2^-24 rc^2 for the products and sums
+//     and 2^-24 rc^2 for the rounding of cutoff^2 itself; the band is twice it.
+//   * distances (list build) and displacements (rebuild test, against the FP32
+//     build position) are off by less than 1e-7 (4Y + R) together,
+//     R = cutoff + skin; `margin` = 10x that widens the build radius and
+//     narrows the core radius.
+// Bins: width >= R |T_k| / 2 in fractional coordinate k, so two points closer
+// than R differ by at most 2 bins per axis; coarsened until <= kMaxBins.
+__device__ inline bool set_margins(FusedGeom &g, double cutoff, const double *rc2d, int nsp2) {
   bool ok = true;
+  const double R = cutoff + g.skin;
+  g.half_skin2 = 0.25 * g.skin * g.skin;
   for (int k = 0; k < 3; ++k) {
-    g.h[k] = (cutoff + g.skin) * g.tn[k] * (1.0 + 1e-9);
+    g.h[k] = R * g.tn[k] * (1.0 + 1e-9);
     g.rep[k] = (int)ceil(g.h[k]);
     ok = ok && g.rep[k] <= 15;
   }
+  double ymax = 0.0;
+  for (int m = 0; m < 3; ++m) {
+    double y = 0.0;
+    for (int k = 0; k < 3; ++k) y += (0.5 + g.h[k]) * fabs(g.C[3 * k + m]);
+    ymax = fmax(ymax, y);
+  }
+  g.band = (float)(2.0 * 5.9604644775390625e-8 *
+                   (4.0 * 1.7320508075688772 * ymax * cutoff + 6.0 * cutoff * cutoff));
+  const double margin = 1e-6 * (4.0 * ymax + R);
+  g.build2 = (float)((R + margin) * (R + margin));
+  for (int k = 0; k < nsp2; ++k) {
+    const double cr = sqrt(rc2d[k]) - g.skin - margin;
+    g.core2[k] = cr > 0.0 ? (float)(cr * cr) : -1.0f;
+  }
+  // one bin of the whole region (always valid) unless a finer grid fits
+  g.nb[0] = g.nb[1] = g.nb[2] = 1;
+  g.nbins = 1;
+  for (int k = 0; k < 3; ++k) g.iw[k] = 0.0;
+  double c = 1.0;
+  for (int it = 0; it < 64; ++it, c *= 1.25) {
+    double tot = 1.0, nbd[3], iw[3];
+    for (int k = 0; k < 3; ++k) {
+      const double w = c * 0.5 * R * g.tn[k] * (1.0 + 1e-6);
+      nbd[k] = fmax(1.0, ceil((1.0 + 2.0 * g.h[k]) / w));
+      iw[k] = 1.0 / w;
+      tot *= nbd[k];
+    }
+    if (tot <= (double)kMaxBins) {
+      for (int k = 0; k < 3; ++k) {
+        g.nb[k] = (int)nbd[k];
+        g.iw[k] = iw[k];
+      }
+      g.nbins = (int)tot;
+      break;
+    }
+  }
   return ok;
+}
+
+__device__ __forceinline__ int bin_coord(const FusedGeom &g, double f, int k) {
+  const int b = (int)floor((f + g.h[k]) * g.iw[k]);
+  return min(max(b, 0), g.nb[k] - 1);
 }
 
 // status[0] = code, [1] = system, [2] = what (1 image slots, 2 list slots), [3] = size
@@ -148,13 +231,54 @@ __device__ inline void normal3f(uint64_t seed, uint64_t atom, uint64_t counter, 
   (void)s2;
 }
 
-__device__ __forceinline__ float4 make_ext(const FusedGeom &g, double x0, double x1, double x2,
-                                           int ex, int ey, int ez, int sp) {
-  // position x + (ex, ey, ez) @ C relative to the cell centre, rounded to FP32
+// ghost slot word: shift (sx, sy, sz) in [-15, 15] as 5-bit fields, owner atom above
+__device__ __forceinline__ uint32_t pack_ghost(int owner, int sx, int sy, int sz) {
+  return ((uint32_t)(sx & 31)) | ((uint32_t)(sy & 31) << 5) | ((uint32_t)(sz & 31) << 10) |
+         ((uint32_t)owner << 15);
+}
+__device__ __forceinline__ void unpack_ghost(uint32_t r, int &owner, int &sx, int &sy, int &sz) {
+  sx = ((int)(r << 27)) >> 27;
+  sy = ((int)(r << 22)) >> 27;
+  sz = ((int)(r << 17)) >> 27;
+  owner = (int)(r >> 15);
+}
+
+// Exact (FP64) squared distance between the home image of atom a and table
+// entry e (an atom, or a ghost = owner + shift @ C), from the FP64 wrapped
+// positions Y [n, 3] of the system.  Rarely called (pairs within the band).
+__device__ __noinline__ double exact_r2(const double *Y, const uint32_t *s_gshift,
+                                        const FusedGeom &g, int n, int a, int e) {
+  int j = e;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  if (e >= n) {
+    int sx, sy, sz;
+    unpack_ghost(s_gshift[e - n], j, sx, sy, sz);
+    s0 = sx * g.C[0] + sy * g.C[3] + sz * g.C[6];
+    s1 = sx * g.C[1] + sy * g.C[4] + sz * g.C[7];
+    s2 = sx * g.C[2] + sy * g.C[5] + sz * g.C[8];
+  }
+  const double dx = (Y[3 * j] + s0) - Y[3 * a];
+  const double dy = (Y[3 * j + 1] + s1) - Y[3 * a + 1];
+  const double dz = (Y[3 * j + 2] + s2) - Y[3 * a + 2];
+  return dx * dx + dy * dy + dz * dz;
+}
+
+// wrapped, cell-centre-relative FP64 position x - W @ C - ctr
+__device__ __forceinline__ void wrapped(const FusedGeom &g, double x0, double x1, double x2,
+                                        int wx, int wy, int wz, double &y0, double &y1,
+                                        double &y2) {
+  y0 = x0 - (wx * g.C[0] + wy * g.C[3] + wz * g.C[6]) - g.ctr[0];
+  y1 = x1 - (wx * g.C[1] + wy * g.C[4] + wz * g.C[7]) - g.ctr[1];
+  y2 = x2 - (wx * g.C[2] + wy * g.C[5] + wz * g.C[8]) - g.ctr[2];
+}
+
+// image y + s @ C rounded to FP32, species in w
+__device__ __forceinline__ float4 image_of(const FusedGeom &g, double y0, double y1, double y2,
+                                           int sx, int sy, int sz, int sp) {
   float4 e;
-  e.x = (float)(x0 + (ex * g.C[0] + ey * g.C[3] + ez * g.C[6]) - g.ctr[0]);
-  e.y = (float)(x1 + (ex * g.C[1] + ey * g.C[4] + ez * g.C[7]) - g.ctr[1]);
-  e.z = (float)(x2 + (ex * g.C[2] + ey * g.C[5] + ez * g.C[8]) - g.ctr[2]);
+  e.x = (float)(y0 + (sx * g.C[0] + sy * g.C[3] + sz * g.C[6]));
+  e.y = (float)(y1 + (sx * g.C[1] + sy * g.C[4] + sz * g.C[7]));
+  e.z = (float)(y2 + (sx * g.C[2] + sy * g.C[5] + sz * g.C[8]));
   e.w = __int_as_float(sp);
   return e;
 }
@@ -163,17 +287,54 @@ __device__ __forceinline__ bool in_margin(const FusedGeom &g, double f, int k) {
   return f >= -g.h[k] && f < 1.0 + g.h[k];
 }
 
-// Fast FP32 pair evaluation for the fused kernel (exp via ex2.approx).
+// PTX approximate instructions (relative error ~2^-22 .. 2^-23, denormals
+// flushed: r^2 > 1e-30 and the exponents here are far from the denormal range).
+__device__ __forceinline__ float ex2_ftz(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_ftz(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// Morse rows of the fused kernel also carry the exponent as one FMA in base 2:
+// a6 = -alpha log2(e), a7 = alpha r0 log2(e), so exp(-alpha (r - r0)) =
+// 2^(a6 r + a7).
+__device__ inline void fused_prm_extra(int pot, const double *t, PairPrm<float> &q) {
+  if (pot == TSB_POT_MORSE) {
+    const double log2e = 1.4426950408889634;
+    q.a6 = (float)(-t[2] * log2e);
+    q.a7 = (float)(t[2] * t[0] * log2e);
+  }
+}
+
+// Fast FP32 pair evaluation for the fused kernel (same e and fr = -V'(r)/r as
+// pair_eval, fewer instructions).
 template <int POT>
 __device__ __forceinline__ void pair_eval_fast(const PairPrm<float> &q, float r2, float &e,
                                                float &fr) {
   if (POT == TSB_POT_MORSE) {
-    const float ir = rsqrtf(r2);
+    // V = D (1 - x)^2 - D - shift = D x (x - 2) - shift, x = exp(-alpha (r - r0))
+    const float ir = rsqrt_ftz(r2);
     const float r = r2 * ir;
-    const float ex = __expf(-q.a2 * (r - q.a0));
-    const float om = 1.0f - ex;
-    e = q.a1 * om * om - q.a1 - q.a4;
-    fr = -q.a5 * ex * om * ir;
+    const float x = ex2_ftz(fmaf(q.a6, r, q.a7));
+    e = q.a1 * x * (x - 2.0f) - q.a4;
+    fr = -q.a5 * fmaf(-x, x, x) * ir;  // -2 alpha D x (1 - x) / r
+  } else if (POT == TSB_POT_LJ) {
+    // V = 4 eps (s6^2 - s6) - shift, s6 = (sigma^2 / r^2)^3
+    const float ir2 = rcp_ftz(r2);
+    const float s2 = q.a0 * ir2;
+    const float s6 = s2 * s2 * s2;
+    e = q.a1 * s6 * (s6 - 1.0f) - q.a4;
+    fr = q.a2 * s6 * fmaf(2.0f, s6, -1.0f) * ir2;
   } else {
     pair_eval<POT, float>(q, r2, e, fr);
   }
@@ -185,18 +346,27 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
   uint2 *s_list = (uint2 *)smem;
   float4 *s_ext = (float4 *)(smem + kSmemList);
   uint32_t *s_gshift = (uint32_t *)(smem + kSmemList + kSmemExt);
+  uint16_t *s_sorted = (uint16_t *)(smem + kSmemList + kSmemExt + kSmemGhost);
+  int *s_bin = (int *)(smem + kSmemList + kSmemExt + kSmemGhost + kSmemSorted);
   uint16_t *list16 = (uint16_t *)s_list;
+  uint16_t *s_ebin = (uint16_t *)s_list;  // bin of each entry, during a rebuild only
   __shared__ FusedGeom g;
   __shared__ PairPrm<float> prm[kFusedMaxSpecies * kFusedMaxSpecies];
+  __shared__ double rc2d[kFusedMaxSpecies * kFusedMaxSpecies];
   __shared__ int s_scan[33];
   __shared__ int s_work;
   __shared__ double s_red[kFusedThreads / 32];
 
   const int tid = threadIdx.x;
-  for (int k = tid; k < A.n_species * A.n_species; k += blockDim.x)
+  const int nsp2 = A.n_species * A.n_species;
+  for (int k = tid; k < nsp2; k += blockDim.x) {
     prm[k] = make_prm<float>(POT, A.table + 5 * k, A.cutoff);
+    fused_prm_extra(POT, A.table + 5 * k, prm[k]);
+    rc2d[k] = pair_rc2(POT, A.table + 5 * k, A.cutoff);
+  }
   __syncthreads();
   const PairPrm<float> p0 = prm[0];  // single-species parameters in registers
+  const double rc2d0 = rc2d[0];
   const uint64_t counter0 = A.counter + (A.counter_dev ? *A.counter_dev : 0ull);
 
   for (;;) {
@@ -230,7 +400,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
         g.ctr[k] = 0.5 * (C[k] + C[3 + k] + C[6 + k]);
       }
       g.skin = A.skin;
-      const bool rep_ok = set_margins(g, A.cutoff);
+      g.dt = A.dt[s];
+      g.half = g.dt / 2.0;
+      g.c1 = (A.integrator == TSB_INT_LANGEVIN) ? exp(-(A.gamma[s] * g.dt)) : 1.0;
+      const bool rep_ok = isfinite(d) && d != 0.0 && set_margins(g, A.cutoff, rc2d, nsp2);
       int tpa = 1;
       while (tpa < 32 && g.n * tpa * 2 <= kFusedThreads) tpa *= 2;
       g.tpa = tpa;
@@ -238,7 +411,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
         g.ok = 0;
         A.energy[s] = 0.0;
         if (A.n_rebuilds) A.n_rebuilds[s] = 0;
-      } else if (g.n > kFusedMaxAtoms || !rep_ok || !isfinite(d)) {
+      } else if (g.n > kFusedMaxAtoms || !rep_ok) {
         g.ok = 0;
         report(A.status, TSB_ERR_UNSUPPORTED, s, 0, g.n);
       }
@@ -250,9 +423,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     const bool own = a < n;
     const bool lead = own && lane == 0;
     const int64_t gi = g.start + a;
+    double *Y = A.f + 3 * g.start;  // FP64 wrapped positions of this system (see top)
     // owner state (every lane of the atom holds an identical copy)
     double x0 = 0, x1 = 0, x2 = 0, px = 0, py = 0, pz = 0, inv_m = 1.0, c2m = 0.0;
-    float F0 = 0.f, F1 = 0.f, F2 = 0.f, xr0 = 0.f, xr1 = 0.f, xr2 = 0.f;
+    float F0 = 0.f, F1 = 0.f, F2 = 0.f;
     int sp = 0;
     if (own) {
       x0 = A.x[3 * gi];
@@ -270,27 +444,43 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       if (A.integrator == TSB_INT_LANGEVIN)
         c2m = sqrt(A.kT[s] * (1.0 - exp(-2.0 * (A.gamma[s] * A.dt[s])))) * sqrt(mass);
     }
-    const double dt = A.dt[s];
-    const double half = dt / 2.0;
-    const double c1 = (A.integrator == TSB_INT_LANGEVIN) ? exp(-(A.gamma[s] * dt)) : 1.0;
     int Wx = 0, Wy = 0, Wz = 0;        // integer wrap of the owned atom at the last build
     int gbeg = 0, gcnt = 0;            // the owned atom's ghost slots [gbeg, gbeg + gcnt)
-    int cnt = 0, rebuilds = 0;
+    int ncore = 0, nshell = 0, rebuilds = 0;
     bool failed = false;
-    float ei = 0.0f, half_skin2 = 0.f;
+    float ei = 0.0f;
+    float yb0 = 0.f, yb1 = 0.f, yb2 = 0.f;  // wrapped position at the build (FP32)
 
     // ------------------------------------------------------------- rebuild
-    // Wrap the owned atom, create its periodic images inside the cutoff+skin
-    // margin of the cell, then every atom scans all atoms + images.  If the
-    // shared-memory tables overflow, the skin of this system is halved.
+    // Wrap the owned atom and create its periodic images inside the
+    // cutoff+skin margin of the cell; bin all entries (counting sort, index
+    // order inside a bin); every atom scans the 5x5x5 bins around its own and
+    // files each neighbour as core or shell.  If the shared-memory tables
+    // overflow, the skin of this system is halved.
+    //
+    // file a candidate E at Q as a core or shell neighbour of the owned atom
+#define TSB_FILE_PAIR(E, Q)                                                                  \
+  {                                                                                          \
+    const float dx = (Q).x - xi.x, dy = (Q).y - xi.y, dz = (Q).z - xi.z;                     \
+    const float d2 = dx * dx + dy * dy + dz * dz;                                            \
+    if (d2 < build2 && (E) != a) {                                                           \
+      const float cr2 = MULTI ? g.core2[sp * A.n_species + __float_as_int((Q).w)] : core0;   \
+      if (ncore + nshell < kListLen) {                                                       \
+        const int slot_ = d2 < cr2 ? ncore : kListLen - 1 - nshell;                          \
+        list16[((size_t)(slot_ >> 2) * kFusedThreads + tid) * 4 + (slot_ & 3)] =             \
+            (uint16_t)(E);                                                                   \
+      }                                                                                      \
+      if (d2 < cr2)                                                                          \
+        ++ncore;                                                                             \
+      else                                                                                   \
+        ++nshell;                                                                            \
+    }                                                                                        \
+  }
 #define TSB_REBUILD()                                                                        \
   for (;;) {                                                                                 \
-    const double rcs_ = A.cutoff + g.skin;                                                   \
-    const float rcs2_build = (float)(rcs_ * rcs_) * (1.0f + 1e-5f);                          \
-    half_skin2 = (float)(0.25 * g.skin * g.skin);                                            \
     int over = 0, over_size = 0;                                                             \
     int gcount = 0;                                                                          \
-    double f0 = 0, f1 = 0, f2 = 0;                                                           \
+    double f0 = 0, f1 = 0, f2 = 0, y0_ = 0, y1_ = 0, y2_ = 0;                                \
     if (own) {                                                                               \
       const double u0 = g.T[0] * x0 + g.T[1] * x1 + g.T[2] * x2;                             \
       const double u1 = g.T[3] * x0 + g.T[4] * x1 + g.T[5] * x2;                             \
@@ -302,11 +492,11 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       Wx = (int)fmin(fmax(w0, -1e8), 1e8);                                                   \
       Wy = (int)fmin(fmax(w1, -1e8), 1e8);                                                   \
       Wz = (int)fmin(fmax(w2, -1e8), 1e8);                                                   \
-      xr0 = (float)x0;                                                                       \
-      xr1 = (float)x1;                                                                       \
-      xr2 = (float)x2;                                                                       \
+      wrapped(g, x0, x1, x2, Wx, Wy, Wz, y0_, y1_, y2_);                                     \
+      yb0 = (float)y0_;                                                                      \
+      yb1 = (float)y1_;                                                                      \
+      yb2 = (float)y2_;                                                                      \
       if (lead) {                                                                            \
-        s_ext[a] = make_ext(g, x0, x1, x2, -Wx, -Wy, -Wz, sp);                               \
         for (int sx = -g.rep[0]; sx <= g.rep[0]; ++sx) {                                     \
           if (!in_margin(g, f0 + sx, 0)) continue;                                           \
           for (int sy = -g.rep[1]; sy <= g.rep[1]; ++sy) {                                   \
@@ -329,40 +519,101 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       over = 1;                                                                              \
       over_size = n_ext;                                                                     \
     } else {                                                                                 \
-      if (lead && gcount) {                                                                  \
+      const int nbins = g.nbins;                                                             \
+      for (int b = tid; b < nbins; b += kFusedThreads) s_bin[b] = 0;                         \
+      /* the initial force reads of all lanes precede the scan's barriers */                 \
+      if (lead) {                                                                            \
+        s_ext[a] = make_float4(yb0, yb1, yb2, __int_as_float(sp));                           \
+        Y[3 * a] = y0_;                                                                      \
+        Y[3 * a + 1] = y1_;                                                                  \
+        Y[3 * a + 2] = y2_;                                                                  \
+        s_ebin[a] = (uint16_t)((bin_coord(g, f0, 0) * g.nb[1] + bin_coord(g, f1, 1)) *       \
+                                   g.nb[2] +                                                 \
+                               bin_coord(g, f2, 2));                                         \
         int gg = gbeg;                                                                       \
-        for (int sx = -g.rep[0]; sx <= g.rep[0]; ++sx) {                                     \
+        for (int sx = -g.rep[0]; gcount && sx <= g.rep[0]; ++sx) {                           \
           if (!in_margin(g, f0 + sx, 0)) continue;                                           \
+          const int bx = bin_coord(g, f0 + sx, 0);                                           \
           for (int sy = -g.rep[1]; sy <= g.rep[1]; ++sy) {                                   \
             if (!in_margin(g, f1 + sy, 1)) continue;                                         \
+            const int bxy = bx * g.nb[1] + bin_coord(g, f1 + sy, 1);                         \
             for (int sz = -g.rep[2]; sz <= g.rep[2]; ++sz) {                                 \
               if (!in_margin(g, f2 + sz, 2)) continue;                                       \
               if ((sx | sy | sz) == 0) continue;                                             \
-              s_ext[gg] = make_ext(g, x0, x1, x2, sx - Wx, sy - Wy, sz - Wz, sp);            \
-              s_gshift[gg - n] = ((uint32_t)(sx & 1023)) | ((uint32_t)(sy & 1023) << 10) |   \
-                                 ((uint32_t)(sz & 1023) << 20);                              \
+              s_ext[gg] = image_of(g, y0_, y1_, y2_, sx, sy, sz, sp);                        \
+              s_gshift[gg - n] = pack_ghost(a, sx, sy, sz);                                  \
+              s_ebin[gg] = (uint16_t)(bxy * g.nb[2] + bin_coord(g, f2 + sz, 2));             \
               ++gg;                                                                          \
             }                                                                                \
           }                                                                                  \
         }                                                                                    \
       }                                                                                      \
       __syncthreads();                                                                       \
-      cnt = 0;                                                                               \
+      for (int e = tid; e < n_ext; e += kFusedThreads) atomicAdd(&s_bin[s_ebin[e]], 1);      \
+      __syncthreads();                                                                       \
+      {                                                                                      \
+        const int b0 = 4 * tid;                                                              \
+        int c4[4], sum = 0;                                                                  \
+        for (int q = 0; q < 4; ++q) {                                                        \
+          c4[q] = b0 + q < nbins ? s_bin[b0 + q] : 0;                                        \
+          sum += c4[q];                                                                      \
+        }                                                                                    \
+        int tot_;                                                                            \
+        int off = block_excl_scan_i(sum, &tot_, s_scan);                                     \
+        for (int q = 0; q < 4; ++q) {                                                        \
+          if (b0 + q < nbins) s_bin[b0 + q] = off;                                           \
+          off += c4[q];                                                                      \
+        }                                                                                    \
+      }                                                                                      \
+      __syncthreads();                                                                       \
+      for (int e = tid; e < n_ext; e += kFusedThreads)                                       \
+        s_sorted[atomicAdd(&s_bin[s_ebin[e]], 1)] = (uint16_t)e;                             \
+      __syncthreads();                                                                       \
+      /* s_bin[b] is now the end of bin b; order each bin by entry index */                  \
+      for (int b = tid; b < nbins; b += kFusedThreads) {                                     \
+        const int lo_ = b ? s_bin[b - 1] : 0, hi_ = s_bin[b];                                \
+        for (int i_ = lo_ + 1; i_ < hi_; ++i_) {                                             \
+          const uint16_t v_ = s_sorted[i_];                                                  \
+          int j_ = i_ - 1;                                                                   \
+          while (j_ >= lo_ && s_sorted[j_] > v_) {                                           \
+            s_sorted[j_ + 1] = s_sorted[j_];                                                 \
+            --j_;                                                                            \
+          }                                                                                  \
+          s_sorted[j_ + 1] = v_;                                                             \
+        }                                                                                    \
+      }                                                                                      \
+      __syncthreads();                                                                       \
+      ncore = 0;                                                                             \
+      nshell = 0;                                                                            \
       if (own) {                                                                             \
         const float4 xi = s_ext[a];                                                          \
-        for (int e = lane; e < n_ext; e += tpa) {                                            \
-          const float4 q = s_ext[e];                                                         \
-          const float dx = q.x - xi.x, dy = q.y - xi.y, dz = q.z - xi.z;                     \
-          const float d2 = dx * dx + dy * dy + dz * dz;                                      \
-          if (d2 < rcs2_build && e != a) {                                                   \
-            if (cnt < kListLen)                                                              \
-              list16[((size_t)(cnt >> 2) * kFusedThreads + tid) * 4 + (cnt & 3)] =           \
-                  (uint16_t)e;                                                               \
-            ++cnt;                                                                           \
+        const float build2 = g.build2;                                                       \
+        const float core0 = g.core2[0];                                                      \
+        const int bx = bin_coord(g, f0, 0), by = bin_coord(g, f1, 1);                        \
+        const int bz = bin_coord(g, f2, 2);                                                  \
+        const int zlo = max(bz - 2, 0), zhi = min(bz + 2, g.nb[2] - 1);                      \
+        for (int cx = max(bx - 2, 0); cx <= min(bx + 2, g.nb[0] - 1); ++cx) {                \
+          for (int cy = max(by - 2, 0); cy <= min(by + 2, g.nb[1] - 1); ++cy) {              \
+            const int row = (cx * g.nb[1] + cy) * g.nb[2];                                   \
+            const int plo = (row + zlo) ? s_bin[row + zlo - 1] : 0;                          \
+            const int phi = s_bin[row + zhi];                                                \
+            /* two candidates per iteration (independent loads), kept in order */            \
+            int p_ = plo + lane;                                                             \
+            for (; p_ + tpa < phi; p_ += 2 * tpa) {                                          \
+              const int e0 = s_sorted[p_], e1 = s_sorted[p_ + tpa];                          \
+              const float4 q0 = s_ext[e0], q1 = s_ext[e1];                                   \
+              TSB_FILE_PAIR(e0, q0)                                                          \
+              TSB_FILE_PAIR(e1, q1)                                                          \
+            }                                                                                \
+            if (p_ < phi) {                                                                  \
+              const int e0 = s_sorted[p_];                                                   \
+              const float4 q0 = s_ext[e0];                                                   \
+              TSB_FILE_PAIR(e0, q0)                                                          \
+            }                                                                                \
           }                                                                                  \
         }                                                                                    \
       }                                                                                      \
-      if (__syncthreads_or(cnt > kListLen)) {                                                \
+      if (__syncthreads_or(ncore + nshell > kListLen)) {                                     \
         over = 2;                                                                            \
         over_size = kListLen;                                                                \
       }                                                                                      \
@@ -380,7 +631,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     }                                                                                        \
     if (tid == 0) {                                                                          \
       g.skin = g.skin > 0.05 ? 0.5 * g.skin : 0.0;                                           \
-      set_margins(g, A.cutoff);                                                              \
+      set_margins(g, A.cutoff, rc2d, nsp2);                                                  \
     }                                                                                        \
     __syncthreads();                                                                         \
   }
@@ -388,16 +639,32 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     // ------------------------------------------------------------ pair loop
     // Four list entries per iteration, branch-free (out-of-range pairs are
     // evaluated and masked), so the loads and the math of the four pairs
-    // overlap.
-#define TSB_PAIR(E, WITH_E)                                                                  \
+    // overlap.  Core pairs need no cutoff test.
+#define TSB_PAIR_CORE(Q, WITH_E)                                                             \
   {                                                                                          \
-    const float4 q = s_ext[E];                                                               \
+    const float4 q = (Q);                                                                    \
     const float rx = q.x - xi.x, ry = q.y - xi.y, rz = q.z - xi.z;                           \
     const float r2 = fmaxf(rx * rx + ry * ry + rz * rz, 1e-30f);                             \
     const PairPrm<float> &pq = MULTI ? row[__float_as_int(q.w)] : p0;                        \
     float ep, fr;                                                                            \
     pair_eval_fast<POT>(pq, r2, ep, fr);                                                     \
-    const bool in_ = r2 < pq.a3;                                                             \
+    fx -= fr * rx;                                                                           \
+    fy -= fr * ry;                                                                           \
+    fz -= fr * rz;                                                                           \
+    if (WITH_E) en += ep;                                                                    \
+  }
+#define TSB_PAIR_SHELL(Q, E, WITH_E)                                                         \
+  {                                                                                          \
+    const float4 q = (Q);                                                                    \
+    const float rx = q.x - xi.x, ry = q.y - xi.y, rz = q.z - xi.z;                           \
+    const float r2 = fmaxf(rx * rx + ry * ry + rz * rz, 1e-30f);                             \
+    const PairPrm<float> &pq = MULTI ? row[__float_as_int(q.w)] : p0;                        \
+    float ep, fr;                                                                            \
+    pair_eval_fast<POT>(pq, r2, ep, fr);                                                     \
+    bool in_ = r2 < pq.a3;                                                                   \
+    if (fabsf(r2 - pq.a3) < band_)                                                           \
+      in_ = exact_r2(Y, s_gshift, g, n, a, (int)(E)) <                                       \
+            (MULTI ? rc2d[sp * A.n_species + __float_as_int(q.w)] : rc2d0);                  \
     fr = in_ ? fr : 0.f;                                                                     \
     fx -= fr * rx;                                                                           \
     fy -= fr * ry;                                                                           \
@@ -409,22 +676,39 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     float fx = 0.f, fy = 0.f, fz = 0.f, en = 0.f;                                            \
     if (own) {                                                                               \
       const float4 xi = s_ext[a];                                                            \
+      const float band_ = g.band;                                                            \
       const PairPrm<float> *row = prm + sp * A.n_species;                                    \
       (void)row;                                                                             \
-      const int full = cnt >> 2;                                                             \
+      const int full = ncore >> 2;                                                           \
       for (int k4 = 0; k4 < full; ++k4) {                                                    \
         const uint2 ge = s_list[k4 * kFusedThreads + tid];                                   \
-        TSB_PAIR(ge.x & 0xFFFFu, WITH_E)                                                     \
-        TSB_PAIR(ge.x >> 16, WITH_E)                                                         \
-        TSB_PAIR(ge.y & 0xFFFFu, WITH_E)                                                     \
-        TSB_PAIR(ge.y >> 16, WITH_E)                                                         \
+        TSB_PAIR_CORE(s_ext[ge.x & 0xFFFFu], WITH_E)                                         \
+        TSB_PAIR_CORE(s_ext[ge.x >> 16], WITH_E)                                             \
+        TSB_PAIR_CORE(s_ext[ge.y & 0xFFFFu], WITH_E)                                         \
+        TSB_PAIR_CORE(s_ext[ge.y >> 16], WITH_E)                                             \
       }                                                                                      \
-      const int rem = cnt & 3;                                                               \
+      const int rem = ncore & 3;                                                             \
       if (rem) {                                                                             \
         const uint2 ge = s_list[full * kFusedThreads + tid];                                 \
-        TSB_PAIR(ge.x & 0xFFFFu, WITH_E)                                                     \
-        if (rem > 1) TSB_PAIR(ge.x >> 16, WITH_E)                                            \
-        if (rem > 2) TSB_PAIR(ge.y & 0xFFFFu, WITH_E)                                        \
+        TSB_PAIR_CORE(s_ext[ge.x & 0xFFFFu], WITH_E)                                         \
+        if (rem > 1) TSB_PAIR_CORE(s_ext[ge.x >> 16], WITH_E)                                \
+        if (rem > 2) TSB_PAIR_CORE(s_ext[ge.y & 0xFFFFu], WITH_E)                            \
+      }                                                                                      \
+      /* shell entry k sits in slot kListLen - 1 - k */                                      \
+      const int sfull = nshell >> 2;                                                         \
+      for (int k4 = 0; k4 < sfull; ++k4) {                                                   \
+        const uint2 ge = s_list[(kListGroups - 1 - k4) * kFusedThreads + tid];               \
+        TSB_PAIR_SHELL(s_ext[ge.y >> 16], ge.y >> 16, WITH_E)                                \
+        TSB_PAIR_SHELL(s_ext[ge.y & 0xFFFFu], ge.y & 0xFFFFu, WITH_E)                        \
+        TSB_PAIR_SHELL(s_ext[ge.x >> 16], ge.x >> 16, WITH_E)                                \
+        TSB_PAIR_SHELL(s_ext[ge.x & 0xFFFFu], ge.x & 0xFFFFu, WITH_E)                        \
+      }                                                                                      \
+      const int srem = nshell & 3;                                                           \
+      if (srem) {                                                                            \
+        const uint2 ge = s_list[(kListGroups - 1 - sfull) * kFusedThreads + tid];            \
+        TSB_PAIR_SHELL(s_ext[ge.y >> 16], ge.y >> 16, WITH_E)                                \
+        if (srem > 1) TSB_PAIR_SHELL(s_ext[ge.y & 0xFFFFu], ge.y & 0xFFFFu, WITH_E)          \
+        if (srem > 2) TSB_PAIR_SHELL(s_ext[ge.x >> 16], ge.x >> 16, WITH_E)                  \
       }                                                                                      \
     }                                                                                        \
     for (int o = 1; o < tpa; o <<= 1) {                                                      \
@@ -442,6 +726,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     TSB_REBUILD()
     if (failed) continue;
     for (int64_t step = 0; step < A.n_steps; ++step) {
+      const double dt = g.dt, half = g.half, c1 = g.c1;
       if (own) {
         px += F0 * half;
         py += F1 * half;
@@ -464,10 +749,13 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
           x2 += (pz * inv_m) * dt;
         }
       }
+      // displacement since the build, in FP64 on the wrapped position
+      double y0 = 0.0, y1 = 0.0, y2 = 0.0;
       bool moved = false;
       if (own) {
-        const float d0 = (float)x0 - xr0, d1 = (float)x1 - xr1, d2 = (float)x2 - xr2;
-        moved = d0 * d0 + d1 * d1 + d2 * d2 > half_skin2;
+        wrapped(g, x0, x1, x2, Wx, Wy, Wz, y0, y1, y2);
+        const double d0 = y0 - yb0, d1 = y1 - yb1, d2 = y2 - yb2;
+        moved = d0 * d0 + d1 * d1 + d2 * d2 > g.half_skin2;
       }
       // all warps are done reading the previous positions
       __syncthreads();
@@ -475,14 +763,15 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       if (own) {
         for (int it = lane; it <= gcnt; it += tpa) {
           if (it == 0) {
-            s_ext[a] = make_ext(g, x0, x1, x2, -Wx, -Wy, -Wz, sp);
+            s_ext[a] = image_of(g, y0, y1, y2, 0, 0, 0, sp);
+            Y[3 * a] = y0;
+            Y[3 * a + 1] = y1;
+            Y[3 * a + 2] = y2;
           } else {
             const int gg = gbeg + it - 1;
-            const uint32_t r = s_gshift[gg - n];
-            const int sx = ((int)(r << 22)) >> 22;
-            const int sy = ((int)(r << 12)) >> 22;
-            const int sz = ((int)(r << 2)) >> 22;
-            s_ext[gg] = make_ext(g, x0, x1, x2, sx - Wx, sy - Wy, sz - Wz, sp);
+            int owner, sx, sy, sz;
+            unpack_ghost(s_gshift[gg - n], owner, sx, sy, sz);
+            s_ext[gg] = image_of(g, y0, y1, y2, sx, sy, sz, sp);
           }
         }
       }
@@ -496,17 +785,20 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
         TSB_FORCES(false)
       }
       if (own) {
-        px += F0 * half;
-        py += F1 * half;
-        pz += F2 * half;
+        px += F0 * g.half;
+        py += F1 * g.half;
+        pz += F2 * g.half;
       }
     }
     if (failed) continue;
     if (A.n_steps == 0) TSB_FORCES(true)
 #undef TSB_FORCES
-#undef TSB_PAIR
+#undef TSB_PAIR_CORE
+#undef TSB_PAIR_SHELL
 #undef TSB_REBUILD
+#undef TSB_FILE_PAIR
     // ---- write back + FP64 energy reduction (each pair seen from both ends)
+    __syncthreads();  // every lane is done reading Y before forces overwrite it
     if (lead) {
       A.x[3 * gi] = x0;
       A.x[3 * gi + 1] = x1;
@@ -532,6 +824,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
 }
 
 }  // namespace tsb
+
 
 using namespace tsb;
 

@@ -49,6 +49,14 @@ __device__ inline PairPrm<R> make_prm(int pot, const double *t, double cutoff) {
   return q;
 }
 
+// FP64 effective cutoff^2 of a parameter row (the in/out decision of a pair is
+// made on the FP64 squared distance against this, as the FP64 reference does).
+__device__ inline double pair_rc2(int pot, const double *t, double cutoff) {
+  double rc = fmin(cutoff, t[3]);
+  if (pot == TSB_POT_SOFT) rc = fmin(rc, t[0]);
+  return rc * rc;
+}
+
 __device__ inline float rsqrt_r(float x) { return rsqrtf(x); }
 __device__ inline double rsqrt_r(double x) { return rsqrt(x); }
 __device__ inline float exp_r(float x) { return expf(x); }

@@ -85,9 +85,12 @@ __global__ void __launch_bounds__(256)
                     const double *__restrict__ table, int ns_species, double cutoff,
                     int flags, P *forces, double *e_atom, double *vir_atom) {
   __shared__ PairPrm<float> prm[kMaxSpecies * kMaxSpecies];
+  __shared__ double prc2[kMaxSpecies * kMaxSpecies];
   __shared__ double sv[27 * 3];
-  for (int k = threadIdx.x; k < ns_species * ns_species; k += blockDim.x)
+  for (int k = threadIdx.x; k < ns_species * ns_species; k += blockDim.x) {
     prm[k] = make_prm<float>(POT, table + 5 * k, cutoff);
+    prc2[k] = pair_rc2(POT, table + 5 * k, cutoff);
+  }
   for (int k = threadIdx.x; k < 27; k += blockDim.x) {
     const int sx = k / 9 - 1, sy = (k / 3) % 3 - 1, sz = k % 3 - 1;
     for (int m = 0; m < 3; ++m) sv[3 * k + m] = sx * cell[m] + sy * cell[3 + m] + sz * cell[6 + m];
@@ -107,12 +110,14 @@ __global__ void __launch_bounds__(256)
     const int j = (int)(e >> 5);
     const int code = (int)(e & 31u);
     const double4 wj = wpos[j];
-    const float rx = (float)(wj.x - wi.x + sv[3 * code]);
-    const float ry = (float)(wj.y - wi.y + sv[3 * code + 1]);
-    const float rz = (float)(wj.z - wi.z + sv[3 * code + 2]);
+    const double dx = wj.x - wi.x + sv[3 * code];
+    const double dy = wj.y - wi.y + sv[3 * code + 1];
+    const double dz = wj.z - wi.z + sv[3 * code + 2];
+    const int sj = (int)__double_as_longlong(wj.w);
+    const float rx = (float)dx, ry = (float)dy, rz = (float)dz;
     const float r2 = rx * rx + ry * ry + rz * rz;
-    const PairPrm<float> &q = row[(int)__double_as_longlong(wj.w)];
-    if (r2 < q.a3) {
+    const PairPrm<float> &q = row[sj];
+    if (dx * dx + dy * dy + dz * dz < prc2[si * ns_species + sj]) {  // FP64 decision
       float ep, fr;
       pair_eval<POT, float>(q, r2, ep, fr);
       const float gx = fr * rx, gy = fr * ry, gz = fr * rz;
