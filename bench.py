@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--n-systems", type=int, default=2048)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skin", type=float, default=SKIN)
+    ap.add_argument("--plain-steps", type=int, default=20,
+                    help="MD steps of the plain per-call path timed beside the fused kernel")
     ap.add_argument("--workload", default="batched_md",
                     choices=["batched_md", "single_large", "relax", "adjoint"])
     return ap.parse_args()
@@ -468,6 +470,24 @@ def main():
     force_err = {"max_abs_over_max_abs": float(df.max() / ref64.abs().max()),
                  "rms_rel": float(df.pow(2).mean().sqrt() / ref64.pow(2).mean().sqrt())}
 
+    # the plain per-call GPU path on the same systems: one nvt_langevin_step per MD
+    # step (cell list rebuilt, pair forces, BAOAB kernels, launched from Python)
+    ps = md.clone()
+    ps.momenta = runner.p.clone()
+    step_kw = dict(dt=0.002 * W.METAL_TIME, kT=1000 * W.KB_EV, gamma=10.0 / W.METAL_TIME)
+    for _ in range(3):
+        ps = integrators.nvt_langevin_step(ps, model, **step_kw)
+    pa, pb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize(device)
+    pa.record(stream)
+    for _ in range(args.plain_steps):
+        ps = integrators.nvt_langevin_step(ps, model, **step_kw)
+    pb.record(stream)
+    torch.cuda.synchronize(device)
+    t_plain = replicas.max_over_ranks(pa.elapsed_time(pb) / 1e3, device)
+    plain_value = replicas.weak_scaling_value(n_atoms * args.plain_steps, t_plain, ws)
+
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
         alg_bytes = n_atoms * args.md_steps * ALG_BYTES_PER_ATOM_STEP
@@ -493,6 +513,10 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "force_err_vs_fp64": force_err,
+            "plain_path": {"value": plain_value, "unit": UNIT, "md_steps": args.plain_steps,
+                           "what": "tsb.integrators.nvt_langevin_step per MD step (cell "
+                                   "list + FP32 pair forces + BAOAB kernels each call)",
+                           "fused_over_plain": value / plain_value},
             "gpu_launches": 2 * args.steps,
             "clocks": clocks.summary(),
             "per_launch_ms": per_launch_ms,
