@@ -40,7 +40,6 @@ WORKLOAD = ("2048 Cu fcc systems (8-512 atoms, strain +-2%, shear +-3deg), Morse
             "(D=0.3429 eV, alpha=1.3588/A, r0=2.866 A, rc=6.0 A), NVT-Langevin BAOAB "
             "1000 K, dt=2 fs, gamma=0.01/fs")
 ALG_BYTES_PER_ATOM_STEP = 76  # streaming state r/w: 48 B FP64 pos + 24 B mom + 4 B type/mass
-SKIN = 0.7  # Verlet skin (A); shrunk per system on the device when tables overflow
 
 
 def parse():
@@ -52,7 +51,8 @@ def parse():
     ap.add_argument("--md-steps", type=int, default=500)
     ap.add_argument("--n-systems", type=int, default=2048)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--skin", type=float, default=SKIN)
+    ap.add_argument("--skin", default="auto",
+                    help="Verlet skin in A, or 'auto' (project autotuner, cached per workload)")
     ap.add_argument("--plain-steps", type=int, default=20,
                     help="MD steps of the plain per-call path timed beside the fused kernel")
     ap.add_argument("--workload", default="batched_md",
@@ -393,7 +393,9 @@ def main():
 
     runner = integrators.FusedMD(md, model, integrator="nvt_langevin",
                                  dt=0.002 * W.METAL_TIME, kT=1000 * W.KB_EV,
-                                 gamma=10.0 / W.METAL_TIME, skin=args.skin, seed=1234 + rank)
+                                 gamma=10.0 / W.METAL_TIME,
+                                 skin=args.skin if args.skin == "auto" else float(args.skin),
+                                 seed=1234 + rank)
     stream = torch.cuda.current_stream(device)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
 
@@ -501,7 +503,8 @@ def main():
             "data": "synthetic (seeded Cu supercells)",
             "config": {"workload": WORKLOAD, "n_systems": args.n_systems,
                        "atoms_per_gpu": n_atoms, "md_steps_per_step": args.md_steps,
-                       "verlet_skin_A": args.skin, "precision": "FP32 pair math, FP64 state",
+                       "verlet_skin_A": runner.skin,
+                       "skin_source": "autotuner" if args.skin == "auto" else "argument", "precision": "FP32 pair math, FP64 state",
                        "mean_steps_between_list_rebuilds": rebuild_interval,
                        "l2": "256 MB buffer written between timed launches",
                        "parallelism": f"replicas x{ws} (independent systems per rank)"},

@@ -180,7 +180,7 @@ class FusedMD:
     """
 
     def __init__(self, state, model, *, integrator: str = "nvt_langevin", dt, kT=None,
-                 gamma=None, skin: float = 0.7, seed: int | None = None):
+                 gamma=None, skin: float | str = 0.7, seed: int | None = None):
         from .models.pair_potential import PairTableModel
 
         if not isinstance(model, PairTableModel):
@@ -221,6 +221,13 @@ class FusedMD:
         self.status = torch.zeros(4, dtype=torch.int32, device=dev)
         self.ws = torch.empty(self.lib.tsb_fused_workspace_size(self.n, self.n_sys),
                               dtype=torch.uint8, device=dev)
+        if isinstance(skin, str):
+            if skin != "auto":
+                raise ValueError(f"skin must be a number or 'auto', got {skin!r}")
+            from .autotune import tune_fused_skin
+
+            skin = tune_fused_skin(state, model, integrator=integrator, dt=dt, kT=kT,
+                                   gamma=gamma)
         self.skin = float(skin)
         self.seed = (seed if seed is not None
                      else getattr(state, "_philox_seed", _seed_of(state))) & (2**64 - 1)
@@ -281,7 +288,7 @@ class FusedMD:
 
 
 def run_md(state, model, n_steps: int, *, integrator: str = "nvt_langevin", dt, kT=None,
-           gamma=None, skin: float = 0.7, seed: int | None = None, check: bool = True,
+           gamma=None, skin: float | str = 0.7, seed: int | None = None, check: bool = True,
            return_rebuilds: bool = False):
     """Advance every system ``n_steps`` in ONE persistent kernel launch.
 

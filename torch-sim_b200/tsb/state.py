@@ -185,3 +185,41 @@ def state_from_arrays(d: dict, device="cuda", dtype=torch.float64) -> SimState:
                     pbc=torch.as_tensor(d["pbc"], dtype=torch.bool, device=device),
                     atomic_numbers=t(d["atomic_numbers"], torch.int64),
                     system_idx=t(d["system_idx"], torch.int64))
+
+
+# per-atom fields of the state classes above (first dimension n_atoms)
+_ATOM_FIELDS = {"positions", "masses", "atomic_numbers", "system_idx", "momenta", "forces",
+                "velocities"}
+
+
+def select_systems(state, systems):
+    """The systems ``systems`` (indices, any order) of a batched state, as a new
+    state of the same class with systems renumbered 0..k-1 in ascending order of
+    their old index (as ``SimState.__getitem__`` in torch_sim/state.py selects
+    systems).  Per-atom fields are masked, per-system fields indexed, the rest
+    copied by reference."""
+    dev = state.device
+    n_sys = state.n_systems
+    sel = torch.unique(torch.as_tensor(systems, dtype=torch.long, device=dev))
+    if sel.numel() == 0 or int(sel.min()) < 0 or int(sel.max()) >= n_sys:
+        raise IndexError(f"system indices must lie in [0, {n_sys})")
+    keep = torch.zeros(n_sys, dtype=torch.bool, device=dev)
+    keep[sel] = True
+    atom_mask = keep[state.system_idx]
+    renum = torch.full((n_sys,), -1, dtype=torch.long, device=dev)
+    renum[sel] = torch.arange(sel.numel(), device=dev)
+    n_atoms = state.n_atoms
+    kw = {}
+    for f in dataclasses.fields(state):
+        v = getattr(state, f.name)
+        if f.name == "system_idx":
+            v = renum[v[atom_mask]]
+        elif f.name == "_n_systems":
+            v = None
+        elif isinstance(v, torch.Tensor) and v.ndim > 0:
+            if f.name in _ATOM_FIELDS or (v.shape[0] == n_atoms and n_atoms != n_sys):
+                v = v[atom_mask]
+            elif v.shape[0] == n_sys and not (f.name == "pbc" and v.ndim == 1):
+                v = v[sel]
+        kw[f.name] = v
+    return type(state)(**kw)
