@@ -261,6 +261,13 @@ def run_single_large(args):
     alg = 4 * entries + n * (32 + 12 + 56)
     peak, kind = measured_peak_hbm()
     achieved = alg * evals / t / 1e9
+    # FP32 list forces of the final configuration vs an FP64 evaluation of it
+    f32 = vm(md)["forces"].double()
+    ref = models.LennardJonesModel(sigma=3.405, epsilon=0.0104, cutoff=8.5, precision="fp64",
+                                   dtype=torch.float64, device=dev)(md.to(dtype=torch.float64))
+    df = (f32 - ref["forces"]).abs()
+    force_err = {"max_abs_over_max_abs": float(df.max() / ref["forces"].abs().max()),
+                 "rms_rel": float(df.pow(2).mean().sqrt() / ref["forces"].pow(2).mean().sqrt())}
     line = {"metric": "force evaluations x atoms / s (single 500k-atom system, Verlet list)",
             "value": n * evals / t, "unit": "atom-evals/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
@@ -273,6 +280,7 @@ def run_single_large(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "peak_source": kind,
                          "kernel": "k_verlet_forces (+ integrator kernels)"},
+            "force_err_vs_fp64": force_err,
             "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
     return 0
@@ -303,6 +311,9 @@ def run_relax(args):
         torch.cuda.synchronize()
     t = a.elapsed_time(b) / 1e3
     n = st.n_atoms
+    # forces of the relaxed states: FP32 pair math vs FP64, against the fmax criterion
+    ref = models.kob_andersen_model(compute_stress=True, device=dev, precision="fp64")(st)
+    err = float((m(st)["forces"] - ref["forces"]).abs().max())
     line = {"metric": "FIRE+Frechet relaxation: atom-steps/s (all systems, until converged)",
             "value": n * steps / t, "unit": "atom-steps/s", "n_gpus": 1, "steps": steps,
             "warmup": 0, "ms_per_step": 1e3 * t / steps, "higher_is_better": True,
@@ -311,6 +322,7 @@ def run_relax(args):
             "config": {"workload": "relax", "systems": st.n_systems, "atoms": n,
                        "fire_steps": steps, "converged": int(conv.sum()),
                        "time_to_all_converged_s": t, "fmax": 1e-3},
+            "force_err_vs_fp64": {"max_abs_eV_per_A": err, "over_fmax": err / 1e-3},
             "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
     return 0

@@ -18,11 +18,14 @@
 
 namespace tsb {
 
+constexpr int kVerletBlock = 256;  // threads per block of the force kernel
+
 struct VerletWork {
   BinData b;
   double4 *wpos;  // [N] current positions in the build frame (FP64), .w = species bits
   uint8_t *pbc;   // [3] all periodic
   int64_t *sys;   // [N] single system
+  double *part;   // [7 * blocks] per-block energy / virial sums of the force kernel
 };
 
 static void carve_verlet(Carver &c, VerletWork &w, int64_t n) {
@@ -30,6 +33,7 @@ static void carve_verlet(Carver &c, VerletWork &w, int64_t n) {
   w.wpos = c.take<double4>(n);
   w.pbc = c.take<uint8_t>(16);
   w.sys = c.take<int64_t>(n);
+  w.part = c.take<double>(7 * ((n + kVerletBlock - 1) / kVerletBlock));
 }
 
 // build: thread per atom (bin order), ELL write, overflow flag
@@ -83,7 +87,7 @@ __global__ void __launch_bounds__(256)
     k_verlet_forces(const double4 *__restrict__ wpos, const uint32_t *__restrict__ list,
                     const int32_t *__restrict__ cnt, int64_t n, const double *__restrict__ cell,
                     const double *__restrict__ table, int ns_species, double cutoff,
-                    int flags, P *forces, double *e_atom, double *vir_atom) {
+                    int flags, P *forces, double *e_atom, double *vir_atom, double *part) {
   __shared__ PairPrm<float> prm[kMaxSpecies * kMaxSpecies];
   __shared__ double prc2[kMaxSpecies * kMaxSpecies];
   __shared__ double sv[27 * 3];
@@ -97,71 +101,82 @@ __global__ void __launch_bounds__(256)
   }
   __syncthreads();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double4 wi = wpos[i];
-  const int si = (int)__double_as_longlong(wi.w);
-  const PairPrm<float> *row = prm + si * ns_species;
-  const int c = cnt[i];
-  float fx = 0.f, fy = 0.f, fz = 0.f;
   double ei = 0.0, vxx = 0, vyy = 0, vzz = 0, vyz = 0, vxz = 0, vxy = 0;
   const bool want_vir = flags & TSB_OUT_STRESS;
-  for (int k = 0; k < c; ++k) {
-    const uint32_t e = list[(size_t)k * n + i];
-    const int j = (int)(e >> 5);
-    const int code = (int)(e & 31u);
-    const double4 wj = wpos[j];
-    const double dx = wj.x - wi.x + sv[3 * code];
-    const double dy = wj.y - wi.y + sv[3 * code + 1];
-    const double dz = wj.z - wi.z + sv[3 * code + 2];
-    const int sj = (int)__double_as_longlong(wj.w);
-    const float rx = (float)dx, ry = (float)dy, rz = (float)dz;
-    const float r2 = rx * rx + ry * ry + rz * rz;
-    const PairPrm<float> &q = row[sj];
-    if (dx * dx + dy * dy + dz * dz < prc2[si * ns_species + sj]) {  // FP64 decision
-      float ep, fr;
-      pair_eval<POT, float>(q, r2, ep, fr);
-      const float gx = fr * rx, gy = fr * ry, gz = fr * rz;
-      fx -= gx;
-      fy -= gy;
-      fz -= gz;
-      ei += (double)ep;
-      if (want_vir) {
-        vxx += (double)(rx * gx);
-        vyy += (double)(ry * gy);
-        vzz += (double)(rz * gz);
-        vyz += (double)(ry * gz);
-        vxz += (double)(rx * gz);
-        vxy += (double)(rx * gy);
+  if (i < n) {
+    const double4 wi = wpos[i];
+    const int si = (int)__double_as_longlong(wi.w);
+    const PairPrm<float> *row = prm + si * ns_species;
+    const int c = cnt[i];
+    float fx = 0.f, fy = 0.f, fz = 0.f;
+    for (int k = 0; k < c; ++k) {
+      const uint32_t e = list[(size_t)k * n + i];
+      const int j = (int)(e >> 5);
+      const int code = (int)(e & 31u);
+      const double4 wj = wpos[j];
+      const double dx = wj.x - wi.x + sv[3 * code];
+      const double dy = wj.y - wi.y + sv[3 * code + 1];
+      const double dz = wj.z - wi.z + sv[3 * code + 2];
+      const int sj = (int)__double_as_longlong(wj.w);
+      const float rx = (float)dx, ry = (float)dy, rz = (float)dz;
+      const float r2 = rx * rx + ry * ry + rz * rz;
+      const PairPrm<float> &q = row[sj];
+      if (dx * dx + dy * dy + dz * dz < prc2[si * ns_species + sj]) {  // FP64 decision
+        float ep, fr;
+        pair_eval<POT, float>(q, r2, ep, fr);
+        const float gx = fr * rx, gy = fr * ry, gz = fr * rz;
+        fx -= gx;
+        fy -= gy;
+        fz -= gz;
+        ei += (double)ep;
+        if (want_vir) {
+          vxx += (double)(rx * gx);
+          vyy += (double)(ry * gy);
+          vzz += (double)(rz * gz);
+          vyz += (double)(ry * gz);
+          vxz += (double)(rx * gz);
+          vxy += (double)(rx * gy);
+        }
       }
     }
+    forces[3 * i] = (P)fx;
+    forces[3 * i + 1] = (P)fy;
+    forces[3 * i + 2] = (P)fz;
+    e_atom[i] = 0.5 * ei;
+    if (want_vir) {
+      double *v = vir_atom + 6 * i;
+      v[0] = 0.5 * vxx;
+      v[1] = 0.5 * vyy;
+      v[2] = 0.5 * vzz;
+      v[3] = 0.5 * vyz;
+      v[4] = 0.5 * vxz;
+      v[5] = 0.5 * vxy;
+    }
   }
-  forces[3 * i] = (P)fx;
-  forces[3 * i + 1] = (P)fy;
-  forces[3 * i + 2] = (P)fz;
-  e_atom[i] = 0.5 * ei;
-  if (want_vir) {
-    double *v = vir_atom + 6 * i;
-    v[0] = 0.5 * vxx;
-    v[1] = 0.5 * vyy;
-    v[2] = 0.5 * vzz;
-    v[3] = 0.5 * vyz;
-    v[4] = 0.5 * vxz;
-    v[5] = 0.5 * vxy;
+  // per-block sums of the half pair energies / virials in a fixed order (FP64):
+  // shuffles inside each warp, then the warps in order; the last kernel adds blocks
+  __shared__ double sh[7][kVerletBlock / 32];
+  double acc[7] = {0.5 * ei, 0.5 * vxx, 0.5 * vyy, 0.5 * vzz, 0.5 * vyz, 0.5 * vxz, 0.5 * vxy};
+  for (int k = 0; k < 7; ++k) {
+    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+    if ((threadIdx.x & 31) == 0) sh[k][threadIdx.x >> 5] = acc[k];
+  }
+  __syncthreads();
+  if (threadIdx.x < 7) {
+    double t = 0.0;
+    for (int w = 0; w < kVerletBlock / 32; ++w) t += sh[threadIdx.x][w];
+    part[7 * blockIdx.x + threadIdx.x] = t;
   }
 }
 
-// fixed-order FP64 reduction over all atoms of the single system
+// sum of the force kernel's block partials in a fixed order (FP64)
 template <class P>
-__global__ void k_verlet_reduce(const double *e_atom, const double *vir_atom, int64_t n,
-                                int flags, const double *cell, P *energy, P *stress) {
+__global__ void k_verlet_final(const double *part, int64_t n_blocks, int flags,
+                               const double *cell, P *energy, P *stress) {
   __shared__ double sh[7][32];
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-  const bool want_vir = flags & TSB_OUT_STRESS;
-  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
-    acc[0] += e_atom[i];
-    if (want_vir)
-      for (int k = 0; k < 6; ++k) acc[1 + k] += vir_atom[6 * i + k];
-  }
+  for (int64_t b = threadIdx.x; b < n_blocks; b += blockDim.x)
+    for (int k = 0; k < 7; ++k) acc[k] += part[7 * b + k];
   for (int k = 0; k < 7; ++k) {
     for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
     if ((threadIdx.x & 31) == 0) sh[k][threadIdx.x >> 5] = acc[k];
@@ -174,7 +189,7 @@ __global__ void k_verlet_reduce(const double *e_atom, const double *vir_atom, in
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t[k] += sh[k][w];
   }
   energy[0] = (P)t[0];
-  if (want_vir) {
+  if (flags & TSB_OUT_STRESS) {
     const double *a = cell;
     const double vol = fabs(a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
                             a[2] * (a[3] * a[7] - a[4] * a[6]));
@@ -285,11 +300,11 @@ extern "C" int tsb_verlet_forces(int potential, const double *table, int n_speci
   if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
 #define TSB_VF(POT, P)                                                                      \
-  k_verlet_forces<POT, P><<<grid_for(n_atoms), 256, 0, st>>>(                              \
+  k_verlet_forces<POT, P><<<grid_for(n_atoms, kVerletBlock), kVerletBlock, 0, st>>>(      \
       w.wpos, list, counts, n_atoms, cell_row, table, n_species, cutoff, out_flags,       \
-      (P *)forces, e_atom, vir_atom);                                                      \
-  k_verlet_reduce<P><<<1, 1024, 0, st>>>(e_atom, vir_atom, n_atoms, out_flags, cell_row,  \
-                                         (P *)energy, (P *)stress);
+      (P *)forces, e_atom, vir_atom, w.part);                                              \
+  k_verlet_final<P><<<1, 256, 0, st>>>(w.part, grid_for(n_atoms, kVerletBlock), out_flags, \
+                                       cell_row, (P *)energy, (P *)stress);
   if (dtype == TSB_F64) {
     if (potential == TSB_POT_LJ) { TSB_VF(TSB_POT_LJ, double) }
     else if (potential == TSB_POT_MORSE) { TSB_VF(TSB_POT_MORSE, double) }
