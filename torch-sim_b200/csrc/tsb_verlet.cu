@@ -109,36 +109,53 @@ __global__ void __launch_bounds__(256)
     const PairPrm<float> *row = prm + si * ns_species;
     const int c = cnt[i];
     float fx = 0.f, fy = 0.f, fz = 0.f;
-    for (int k = 0; k < c; ++k) {
-      const uint32_t e = list[(size_t)k * n + i];
-      const int j = (int)(e >> 5);
-      const int code = (int)(e & 31u);
-      const double4 wj = wpos[j];
-      const double dx = wj.x - wi.x + sv[3 * code];
-      const double dy = wj.y - wi.y + sv[3 * code + 1];
-      const double dz = wj.z - wi.z + sv[3 * code + 2];
-      const int sj = (int)__double_as_longlong(wj.w);
-      const float rx = (float)dx, ry = (float)dy, rz = (float)dz;
-      const float r2 = rx * rx + ry * ry + rz * rz;
-      const PairPrm<float> &q = row[sj];
-      if (dx * dx + dy * dy + dz * dz < prc2[si * ns_species + sj]) {  // FP64 decision
-        float ep, fr;
-        pair_eval<POT, float>(q, r2, ep, fr);
-        const float gx = fr * rx, gy = fr * ry, gz = fr * rz;
-        fx -= gx;
-        fy -= gy;
-        fz -= gz;
-        ei += (double)ep;
-        if (want_vir) {
-          vxx += (double)(rx * gx);
-          vyy += (double)(ry * gy);
-          vzz += (double)(rz * gz);
-          vyz += (double)(ry * gz);
-          vxz += (double)(rx * gz);
-          vxy += (double)(rx * gy);
-        }
-      }
+    // one pair (entry E, neighbour position WJ); the displacement and the
+    // cutoff test are FP64, the pair function FP32
+#define TSB_VPAIR(E, WJ)                                                                     \
+  {                                                                                          \
+    const int code = (int)((E) & 31u);                                                       \
+    const double dx = (WJ).x - wi.x + sv[3 * code];                                          \
+    const double dy = (WJ).y - wi.y + sv[3 * code + 1];                                      \
+    const double dz = (WJ).z - wi.z + sv[3 * code + 2];                                      \
+    const int sj = (int)__double_as_longlong((WJ).w);                                        \
+    if (dx * dx + dy * dy + dz * dz < prc2[si * ns_species + sj]) {                          \
+      const float rx = (float)dx, ry = (float)dy, rz = (float)dz;                            \
+      const float r2 = rx * rx + ry * ry + rz * rz;                                          \
+      float ep, fr;                                                                          \
+      pair_eval<POT, float>(row[sj], r2, ep, fr);                                            \
+      const float gx = fr * rx, gy = fr * ry, gz = fr * rz;                                  \
+      fx -= gx;                                                                              \
+      fy -= gy;                                                                              \
+      fz -= gz;                                                                              \
+      ei += (double)ep;                                                                      \
+      if (want_vir) {                                                                        \
+        vxx += (double)(rx * gx);                                                            \
+        vyy += (double)(ry * gy);                                                            \
+        vzz += (double)(rz * gz);                                                            \
+        vyz += (double)(ry * gz);                                                            \
+        vxz += (double)(rx * gz);                                                            \
+        vxy += (double)(rx * gy);                                                            \
+      }                                                                                      \
+    }                                                                                        \
+  }
+    // four entries per iteration: their list words and positions load together
+    int k = 0;
+    for (; k + 4 <= c; k += 4) {
+      const uint32_t e0 = list[(size_t)k * n + i], e1 = list[(size_t)(k + 1) * n + i];
+      const uint32_t e2 = list[(size_t)(k + 2) * n + i], e3 = list[(size_t)(k + 3) * n + i];
+      const double4 w0 = wpos[e0 >> 5], w1 = wpos[e1 >> 5];
+      const double4 w2 = wpos[e2 >> 5], w3 = wpos[e3 >> 5];
+      TSB_VPAIR(e0, w0)
+      TSB_VPAIR(e1, w1)
+      TSB_VPAIR(e2, w2)
+      TSB_VPAIR(e3, w3)
     }
+    for (; k < c; ++k) {
+      const uint32_t e0 = list[(size_t)k * n + i];
+      const double4 w0 = wpos[e0 >> 5];
+      TSB_VPAIR(e0, w0)
+    }
+#undef TSB_VPAIR
     forces[3 * i] = (P)fx;
     forces[3 * i + 1] = (P)fy;
     forces[3 * i + 2] = (P)fz;
