@@ -340,8 +340,60 @@ __device__ __forceinline__ void pair_eval_fast(const PairPrm<float> &q, float r2
   }
 }
 
+// Two pairs at once in FP32x2 arithmetic (sm_100 FFMA2 / FMUL2 / FADD2): the
+// constants of one single-species parameter row duplicated into both halves.
+struct Prm2 {
+  float2 c0, c1, c2, c3;
+};
+
+template <int POT>
+__device__ inline Prm2 make_prm2(const PairPrm<float> &q) {
+  Prm2 k;
+  if (POT == TSB_POT_MORSE) {
+    k.c0 = make_float2(q.a6, q.a6);  // exponent slope (base 2)
+    k.c1 = make_float2(q.a7, q.a7);  // exponent offset
+    k.c2 = make_float2(q.a5, q.a5);  // 2 alpha D
+  } else {
+    k.c0 = make_float2(q.a0, q.a0);  // sigma^2
+    k.c1 = make_float2(q.a2, q.a2);  // 24 eps
+    k.c2 = make_float2(2.0f, 2.0f);
+  }
+  k.c3 = make_float2(-1.0f, -1.0f);
+  return k;
+}
+
+// fr = -V'(r)/r of two pairs (LJ or Morse); energies only when WITH_E
+template <int POT, bool WITH_E>
+__device__ __forceinline__ float2 pair_fr2(const Prm2 &k, const PairPrm<float> &q, float2 r2,
+                                           float2 &e) {
+  if (POT == TSB_POT_MORSE) {
+    const float2 ir = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+    const float2 r = __fmul2_rn(r2, ir);
+    const float2 arg = __ffma2_rn(k.c0, r, k.c1);
+    const float2 x = make_float2(ex2_ftz(arg.x), ex2_ftz(arg.y));
+    if (WITH_E) {
+      e.x = q.a1 * x.x * (x.x - 2.0f) - q.a4;
+      e.y = q.a1 * x.y * (x.y - 2.0f) - q.a4;
+    }
+    // -2 alpha D x (1 - x) / r = x (x - 1) (2 alpha D / r)
+    return __fmul2_rn(__fmul2_rn(x, __fadd2_rn(x, k.c3)), __fmul2_rn(k.c2, ir));
+  } else {
+    const float2 ir2 = make_float2(rcp_ftz(r2.x), rcp_ftz(r2.y));
+    const float2 s2 = __fmul2_rn(k.c0, ir2);
+    const float2 s6 = __fmul2_rn(__fmul2_rn(s2, s2), s2);
+    if (WITH_E) {
+      e.x = q.a1 * s6.x * (s6.x - 1.0f) - q.a4;
+      e.y = q.a1 * s6.y * (s6.y - 1.0f) - q.a4;
+    }
+    // 24 eps s6 (2 s6 - 1) / r^2
+    return __fmul2_rn(__fmul2_rn(k.c1, s6), __fmul2_rn(__ffma2_rn(k.c2, s6, k.c3), ir2));
+  }
+}
+
 template <int POT, bool MULTI>
 __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
+  // single-species LJ / Morse: pairs evaluated two at a time in FP32x2
+  constexpr bool kPaired = !MULTI && POT != TSB_POT_SOFT;
   extern __shared__ __align__(16) unsigned char smem[];
   uint2 *s_list = (uint2 *)smem;
   float4 *s_ext = (float4 *)(smem + kSmemList);
@@ -366,6 +418,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
   }
   __syncthreads();
   const PairPrm<float> p0 = prm[0];  // single-species parameters in registers
+  const Prm2 k2 = make_prm2<POT>(p0);
   const double rc2d0 = rc2d[0];
   const uint64_t counter0 = A.counter + (A.counter_dev ? *A.counter_dev : 0ull);
 
@@ -671,6 +724,32 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     fz -= fr * rz;                                                                           \
     if (WITH_E) en += in_ ? ep : 0.f;                                                        \
   }
+  // two list entries at once (FP32x2); displacement xi - q so that the force
+  // accumulates as f += fr * d
+#define TSB_PAIR2(QA, QB, EA, EB, SHELL, WITH_E)                                             \
+  {                                                                                          \
+    const float4 qa = (QA), qb = (QB);                                                       \
+    const float2 dx = make_float2(xi.x - qa.x, xi.x - qb.x);                                 \
+    const float2 dy = make_float2(xi.y - qa.y, xi.y - qb.y);                                 \
+    const float2 dz = make_float2(xi.z - qa.z, xi.z - qb.z);                                 \
+    float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));                  \
+    r2 = make_float2(fmaxf(r2.x, 1e-30f), fmaxf(r2.y, 1e-30f));                              \
+    float2 e2;                                                                               \
+    float2 fr = pair_fr2<POT, WITH_E>(k2, p0, r2, e2);                                       \
+    if (SHELL) {                                                                             \
+      bool ina = r2.x < p0.a3, inb = r2.y < p0.a3;                                           \
+      if (fabsf(r2.x - p0.a3) < band_)                                                       \
+        ina = exact_r2(Y, s_gshift, g, n, a, (int)(EA)) < rc2d0;                             \
+      if (fabsf(r2.y - p0.a3) < band_)                                                       \
+        inb = exact_r2(Y, s_gshift, g, n, a, (int)(EB)) < rc2d0;                             \
+      fr = make_float2(ina ? fr.x : 0.f, inb ? fr.y : 0.f);                                  \
+      if (WITH_E) e2 = make_float2(ina ? e2.x : 0.f, inb ? e2.y : 0.f);                      \
+    }                                                                                        \
+    f2x = __ffma2_rn(fr, dx, f2x);                                                           \
+    f2y = __ffma2_rn(fr, dy, f2y);                                                           \
+    f2z = __ffma2_rn(fr, dz, f2z);                                                           \
+    if (WITH_E) en += e2.x + e2.y;                                                           \
+  }
 #define TSB_FORCES(WITH_E)                                                                   \
   {                                                                                          \
     float fx = 0.f, fy = 0.f, fz = 0.f, en = 0.f;                                            \
@@ -679,36 +758,73 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       const float band_ = g.band;                                                            \
       const PairPrm<float> *row = prm + sp * A.n_species;                                    \
       (void)row;                                                                             \
-      const int full = ncore >> 2;                                                           \
-      for (int k4 = 0; k4 < full; ++k4) {                                                    \
-        const uint2 ge = s_list[k4 * kFusedThreads + tid];                                   \
-        TSB_PAIR_CORE(s_ext[ge.x & 0xFFFFu], WITH_E)                                         \
-        TSB_PAIR_CORE(s_ext[ge.x >> 16], WITH_E)                                             \
-        TSB_PAIR_CORE(s_ext[ge.y & 0xFFFFu], WITH_E)                                         \
-        TSB_PAIR_CORE(s_ext[ge.y >> 16], WITH_E)                                             \
-      }                                                                                      \
-      const int rem = ncore & 3;                                                             \
-      if (rem) {                                                                             \
-        const uint2 ge = s_list[full * kFusedThreads + tid];                                 \
-        TSB_PAIR_CORE(s_ext[ge.x & 0xFFFFu], WITH_E)                                         \
-        if (rem > 1) TSB_PAIR_CORE(s_ext[ge.x >> 16], WITH_E)                                \
-        if (rem > 2) TSB_PAIR_CORE(s_ext[ge.y & 0xFFFFu], WITH_E)                            \
-      }                                                                                      \
-      /* shell entry k sits in slot kListLen - 1 - k */                                      \
-      const int sfull = nshell >> 2;                                                         \
-      for (int k4 = 0; k4 < sfull; ++k4) {                                                   \
-        const uint2 ge = s_list[(kListGroups - 1 - k4) * kFusedThreads + tid];               \
-        TSB_PAIR_SHELL(s_ext[ge.y >> 16], ge.y >> 16, WITH_E)                                \
-        TSB_PAIR_SHELL(s_ext[ge.y & 0xFFFFu], ge.y & 0xFFFFu, WITH_E)                        \
-        TSB_PAIR_SHELL(s_ext[ge.x >> 16], ge.x >> 16, WITH_E)                                \
-        TSB_PAIR_SHELL(s_ext[ge.x & 0xFFFFu], ge.x & 0xFFFFu, WITH_E)                        \
-      }                                                                                      \
-      const int srem = nshell & 3;                                                           \
-      if (srem) {                                                                            \
-        const uint2 ge = s_list[(kListGroups - 1 - sfull) * kFusedThreads + tid];            \
-        TSB_PAIR_SHELL(s_ext[ge.y >> 16], ge.y >> 16, WITH_E)                                \
-        if (srem > 1) TSB_PAIR_SHELL(s_ext[ge.y & 0xFFFFu], ge.y & 0xFFFFu, WITH_E)          \
-        if (srem > 2) TSB_PAIR_SHELL(s_ext[ge.x >> 16], ge.x >> 16, WITH_E)                  \
+      const int full = ncore >> 2, rem = ncore & 3;                                          \
+      const int sfull = nshell >> 2, srem = nshell & 3;                                      \
+      if constexpr (kPaired) {                                                               \
+        float2 f2x = make_float2(0.f, 0.f), f2y = f2x, f2z = f2x;                            \
+        for (int k4 = 0; k4 < full; ++k4) {                                                  \
+          const uint2 ge = s_list[k4 * kFusedThreads + tid];                                 \
+          TSB_PAIR2(s_ext[ge.x & 0xFFFFu], s_ext[ge.x >> 16], 0, 0, false, WITH_E)           \
+          TSB_PAIR2(s_ext[ge.y & 0xFFFFu], s_ext[ge.y >> 16], 0, 0, false, WITH_E)           \
+        }                                                                                    \
+        if (rem) {                                                                           \
+          const uint2 ge = s_list[full * kFusedThreads + tid];                               \
+          if (rem > 1) {                                                                     \
+            TSB_PAIR2(s_ext[ge.x & 0xFFFFu], s_ext[ge.x >> 16], 0, 0, false, WITH_E)         \
+            if (rem > 2) TSB_PAIR_CORE(s_ext[ge.y & 0xFFFFu], WITH_E)                        \
+          } else {                                                                           \
+            TSB_PAIR_CORE(s_ext[ge.x & 0xFFFFu], WITH_E)                                     \
+          }                                                                                  \
+        }                                                                                    \
+        /* shell entry k sits in slot kListLen - 1 - k */                                    \
+        for (int k4 = 0; k4 < sfull; ++k4) {                                                 \
+          const uint2 ge = s_list[(kListGroups - 1 - k4) * kFusedThreads + tid];             \
+          TSB_PAIR2(s_ext[ge.y >> 16], s_ext[ge.y & 0xFFFFu], ge.y >> 16, ge.y & 0xFFFFu,    \
+                    true, WITH_E)                                                            \
+          TSB_PAIR2(s_ext[ge.x >> 16], s_ext[ge.x & 0xFFFFu], ge.x >> 16, ge.x & 0xFFFFu,    \
+                    true, WITH_E)                                                            \
+        }                                                                                    \
+        if (srem) {                                                                          \
+          const uint2 ge = s_list[(kListGroups - 1 - sfull) * kFusedThreads + tid];          \
+          if (srem > 1) {                                                                    \
+            TSB_PAIR2(s_ext[ge.y >> 16], s_ext[ge.y & 0xFFFFu], ge.y >> 16, ge.y & 0xFFFFu,  \
+                      true, WITH_E)                                                          \
+            if (srem > 2) TSB_PAIR_SHELL(s_ext[ge.x >> 16], ge.x >> 16, WITH_E)              \
+          } else {                                                                           \
+            TSB_PAIR_SHELL(s_ext[ge.y >> 16], ge.y >> 16, WITH_E)                            \
+          }                                                                                  \
+        }                                                                                    \
+        fx += f2x.x + f2x.y;                                                                 \
+        fy += f2y.x + f2y.y;                                                                 \
+        fz += f2z.x + f2z.y;                                                                 \
+      } else {                                                                               \
+        for (int k4 = 0; k4 < full; ++k4) {                                                  \
+          const uint2 ge = s_list[k4 * kFusedThreads + tid];                                 \
+          TSB_PAIR_CORE(s_ext[ge.x & 0xFFFFu], WITH_E)                                       \
+          TSB_PAIR_CORE(s_ext[ge.x >> 16], WITH_E)                                           \
+          TSB_PAIR_CORE(s_ext[ge.y & 0xFFFFu], WITH_E)                                       \
+          TSB_PAIR_CORE(s_ext[ge.y >> 16], WITH_E)                                           \
+        }                                                                                    \
+        if (rem) {                                                                           \
+          const uint2 ge = s_list[full * kFusedThreads + tid];                               \
+          TSB_PAIR_CORE(s_ext[ge.x & 0xFFFFu], WITH_E)                                       \
+          if (rem > 1) TSB_PAIR_CORE(s_ext[ge.x >> 16], WITH_E)                              \
+          if (rem > 2) TSB_PAIR_CORE(s_ext[ge.y & 0xFFFFu], WITH_E)                          \
+        }                                                                                    \
+        /* shell entry k sits in slot kListLen - 1 - k */                                    \
+        for (int k4 = 0; k4 < sfull; ++k4) {                                                 \
+          const uint2 ge = s_list[(kListGroups - 1 - k4) * kFusedThreads + tid];             \
+          TSB_PAIR_SHELL(s_ext[ge.y >> 16], ge.y >> 16, WITH_E)                              \
+          TSB_PAIR_SHELL(s_ext[ge.y & 0xFFFFu], ge.y & 0xFFFFu, WITH_E)                      \
+          TSB_PAIR_SHELL(s_ext[ge.x >> 16], ge.x >> 16, WITH_E)                              \
+          TSB_PAIR_SHELL(s_ext[ge.x & 0xFFFFu], ge.x & 0xFFFFu, WITH_E)                      \
+        }                                                                                    \
+        if (srem) {                                                                          \
+          const uint2 ge = s_list[(kListGroups - 1 - sfull) * kFusedThreads + tid];          \
+          TSB_PAIR_SHELL(s_ext[ge.y >> 16], ge.y >> 16, WITH_E)                              \
+          if (srem > 1) TSB_PAIR_SHELL(s_ext[ge.y & 0xFFFFu], ge.y & 0xFFFFu, WITH_E)        \
+          if (srem > 2) TSB_PAIR_SHELL(s_ext[ge.x >> 16], ge.x >> 16, WITH_E)                \
+        }                                                                                    \
       }                                                                                      \
     }                                                                                        \
     for (int o = 1; o < tpa; o <<= 1) {                                                      \
@@ -795,6 +911,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
 #undef TSB_FORCES
 #undef TSB_PAIR_CORE
 #undef TSB_PAIR_SHELL
+#undef TSB_PAIR2
 #undef TSB_REBUILD
 #undef TSB_FILE_PAIR
     // ---- write back + FP64 energy reduction (each pair seen from both ends)
