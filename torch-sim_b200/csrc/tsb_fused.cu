@@ -16,7 +16,8 @@
 //     atoms and the periodic images ("ghosts") within cutoff+skin of the cell as
 //     float4 (x, y, z, species) in cell-centre-relative FP32 coordinates, and
 //     the Verlet list (cutoff + skin) as a uint16 ELL table [slot group][thread]
-//     that each thread reads four entries per 64-bit load.  FP64
+//     of byte offsets into the image table, which each thread reads four
+//     entries per 64-bit load.  FP64
 //     positions/momenta live in the registers of the owning threads.
 //   * The list is rebuilt on the device when any atom of the system moved more
 //     than skin/2 since the last build.  A rebuild sorts atoms + images into
@@ -63,6 +64,7 @@ constexpr size_t kFusedSmem = kSmemList + kSmemExt + kSmemGhost + kSmemSorted + 
 // the bin of every entry is kept in the list area while the list is rebuilt
 static_assert(kExtMax * sizeof(uint16_t) <= kSmemList, "bin ids alias the list");
 static_assert(kMaxBins <= 4 * kFusedThreads, "bin scan: four bins per thread");
+static_assert((kExtMax - 1) * sizeof(float4) <= 0xFFFF, "list entries are 16-bit byte offsets");
 
 struct FusedArgs {
   int integrator, potential, n_species;
@@ -520,8 +522,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       const float cr2 = MULTI ? g.core2[sp * A.n_species + __float_as_int((Q).w)] : core0;   \
       if (ncore + nshell < kListLen) {                                                       \
         const int slot_ = d2 < cr2 ? ncore : kListLen - 1 - nshell;                          \
-        list16[((size_t)(slot_ >> 2) * kFusedThreads + tid) * 4 + (slot_ & 3)] =             \
-            (uint16_t)(E);                                                                   \
+        list16[(((slot_ >> 2) * kFusedThreads + tid) << 2) | (slot_ & 3)] =                  \
+            (uint16_t)((E) << 4);                                                            \
       }                                                                                      \
       if (d2 < cr2)                                                                          \
         ++ncore;                                                                             \
@@ -690,6 +692,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
   }
 
     // ------------------------------------------------------------ pair loop
+    // list entries are byte offsets (entry * 16) into the image table
+#define EXT(OFF) (*(const float4 *)((const unsigned char *)s_ext + (OFF)))
     // Four list entries per iteration, branch-free (out-of-range pairs are
     // evaluated and masked), so the loads and the math of the four pairs
     // overlap.  Core pairs need no cutoff test.
@@ -716,7 +720,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     pair_eval_fast<POT>(pq, r2, ep, fr);                                                     \
     bool in_ = r2 < pq.a3;                                                                   \
     if (fabsf(r2 - pq.a3) < band_)                                                           \
-      in_ = exact_r2(Y, s_gshift, g, n, a, (int)(E)) <                                       \
+      in_ = exact_r2(Y, s_gshift, g, n, a, (int)((E) >> 4)) <                                \
             (MULTI ? rc2d[sp * A.n_species + __float_as_int(q.w)] : rc2d0);                  \
     fr = in_ ? fr : 0.f;                                                                     \
     fx -= fr * rx;                                                                           \
@@ -738,10 +742,12 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     float2 fr = pair_fr2<POT, WITH_E>(k2, p0, r2, e2);                                       \
     if (SHELL) {                                                                             \
       bool ina = r2.x < p0.a3, inb = r2.y < p0.a3;                                           \
-      if (fabsf(r2.x - p0.a3) < band_)                                                       \
-        ina = exact_r2(Y, s_gshift, g, n, a, (int)(EA)) < rc2d0;                             \
-      if (fabsf(r2.y - p0.a3) < band_)                                                       \
-        inb = exact_r2(Y, s_gshift, g, n, a, (int)(EB)) < rc2d0;                             \
+      const bool near_a = fabsf(r2.x - p0.a3) < band_;                                       \
+      const bool near_b = fabsf(r2.y - p0.a3) < band_;                                       \
+      if (near_a || near_b) { /* rare: one branch for both pairs */                          \
+        if (near_a) ina = exact_r2(Y, s_gshift, g, n, a, (int)((EA) >> 4)) < rc2d0;          \
+        if (near_b) inb = exact_r2(Y, s_gshift, g, n, a, (int)((EB) >> 4)) < rc2d0;          \
+      }                                                                                      \
       fr = make_float2(ina ? fr.x : 0.f, inb ? fr.y : 0.f);                                  \
       if (WITH_E) e2 = make_float2(ina ? e2.x : 0.f, inb ? e2.y : 0.f);                      \
     }                                                                                        \
@@ -764,34 +770,34 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
         float2 f2x = make_float2(0.f, 0.f), f2y = f2x, f2z = f2x;                            \
         for (int k4 = 0; k4 < full; ++k4) {                                                  \
           const uint2 ge = s_list[k4 * kFusedThreads + tid];                                 \
-          TSB_PAIR2(s_ext[ge.x & 0xFFFFu], s_ext[ge.x >> 16], 0, 0, false, WITH_E)           \
-          TSB_PAIR2(s_ext[ge.y & 0xFFFFu], s_ext[ge.y >> 16], 0, 0, false, WITH_E)           \
+          TSB_PAIR2(EXT(ge.x & 0xFFFFu), EXT(ge.x >> 16), 0, 0, false, WITH_E)           \
+          TSB_PAIR2(EXT(ge.y & 0xFFFFu), EXT(ge.y >> 16), 0, 0, false, WITH_E)           \
         }                                                                                    \
         if (rem) {                                                                           \
           const uint2 ge = s_list[full * kFusedThreads + tid];                               \
           if (rem > 1) {                                                                     \
-            TSB_PAIR2(s_ext[ge.x & 0xFFFFu], s_ext[ge.x >> 16], 0, 0, false, WITH_E)         \
-            if (rem > 2) TSB_PAIR_CORE(s_ext[ge.y & 0xFFFFu], WITH_E)                        \
+            TSB_PAIR2(EXT(ge.x & 0xFFFFu), EXT(ge.x >> 16), 0, 0, false, WITH_E)         \
+            if (rem > 2) TSB_PAIR_CORE(EXT(ge.y & 0xFFFFu), WITH_E)                        \
           } else {                                                                           \
-            TSB_PAIR_CORE(s_ext[ge.x & 0xFFFFu], WITH_E)                                     \
+            TSB_PAIR_CORE(EXT(ge.x & 0xFFFFu), WITH_E)                                     \
           }                                                                                  \
         }                                                                                    \
         /* shell entry k sits in slot kListLen - 1 - k */                                    \
         for (int k4 = 0; k4 < sfull; ++k4) {                                                 \
           const uint2 ge = s_list[(kListGroups - 1 - k4) * kFusedThreads + tid];             \
-          TSB_PAIR2(s_ext[ge.y >> 16], s_ext[ge.y & 0xFFFFu], ge.y >> 16, ge.y & 0xFFFFu,    \
+          TSB_PAIR2(EXT(ge.y >> 16), EXT(ge.y & 0xFFFFu), ge.y >> 16, ge.y & 0xFFFFu,    \
                     true, WITH_E)                                                            \
-          TSB_PAIR2(s_ext[ge.x >> 16], s_ext[ge.x & 0xFFFFu], ge.x >> 16, ge.x & 0xFFFFu,    \
+          TSB_PAIR2(EXT(ge.x >> 16), EXT(ge.x & 0xFFFFu), ge.x >> 16, ge.x & 0xFFFFu,    \
                     true, WITH_E)                                                            \
         }                                                                                    \
         if (srem) {                                                                          \
           const uint2 ge = s_list[(kListGroups - 1 - sfull) * kFusedThreads + tid];          \
           if (srem > 1) {                                                                    \
-            TSB_PAIR2(s_ext[ge.y >> 16], s_ext[ge.y & 0xFFFFu], ge.y >> 16, ge.y & 0xFFFFu,  \
+            TSB_PAIR2(EXT(ge.y >> 16), EXT(ge.y & 0xFFFFu), ge.y >> 16, ge.y & 0xFFFFu,  \
                       true, WITH_E)                                                          \
-            if (srem > 2) TSB_PAIR_SHELL(s_ext[ge.x >> 16], ge.x >> 16, WITH_E)              \
+            if (srem > 2) TSB_PAIR_SHELL(EXT(ge.x >> 16), ge.x >> 16, WITH_E)              \
           } else {                                                                           \
-            TSB_PAIR_SHELL(s_ext[ge.y >> 16], ge.y >> 16, WITH_E)                            \
+            TSB_PAIR_SHELL(EXT(ge.y >> 16), ge.y >> 16, WITH_E)                            \
           }                                                                                  \
         }                                                                                    \
         fx += f2x.x + f2x.y;                                                                 \
@@ -800,30 +806,30 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       } else {                                                                               \
         for (int k4 = 0; k4 < full; ++k4) {                                                  \
           const uint2 ge = s_list[k4 * kFusedThreads + tid];                                 \
-          TSB_PAIR_CORE(s_ext[ge.x & 0xFFFFu], WITH_E)                                       \
-          TSB_PAIR_CORE(s_ext[ge.x >> 16], WITH_E)                                           \
-          TSB_PAIR_CORE(s_ext[ge.y & 0xFFFFu], WITH_E)                                       \
-          TSB_PAIR_CORE(s_ext[ge.y >> 16], WITH_E)                                           \
+          TSB_PAIR_CORE(EXT(ge.x & 0xFFFFu), WITH_E)                                       \
+          TSB_PAIR_CORE(EXT(ge.x >> 16), WITH_E)                                           \
+          TSB_PAIR_CORE(EXT(ge.y & 0xFFFFu), WITH_E)                                       \
+          TSB_PAIR_CORE(EXT(ge.y >> 16), WITH_E)                                           \
         }                                                                                    \
         if (rem) {                                                                           \
           const uint2 ge = s_list[full * kFusedThreads + tid];                               \
-          TSB_PAIR_CORE(s_ext[ge.x & 0xFFFFu], WITH_E)                                       \
-          if (rem > 1) TSB_PAIR_CORE(s_ext[ge.x >> 16], WITH_E)                              \
-          if (rem > 2) TSB_PAIR_CORE(s_ext[ge.y & 0xFFFFu], WITH_E)                          \
+          TSB_PAIR_CORE(EXT(ge.x & 0xFFFFu), WITH_E)                                       \
+          if (rem > 1) TSB_PAIR_CORE(EXT(ge.x >> 16), WITH_E)                              \
+          if (rem > 2) TSB_PAIR_CORE(EXT(ge.y & 0xFFFFu), WITH_E)                          \
         }                                                                                    \
         /* shell entry k sits in slot kListLen - 1 - k */                                    \
         for (int k4 = 0; k4 < sfull; ++k4) {                                                 \
           const uint2 ge = s_list[(kListGroups - 1 - k4) * kFusedThreads + tid];             \
-          TSB_PAIR_SHELL(s_ext[ge.y >> 16], ge.y >> 16, WITH_E)                              \
-          TSB_PAIR_SHELL(s_ext[ge.y & 0xFFFFu], ge.y & 0xFFFFu, WITH_E)                      \
-          TSB_PAIR_SHELL(s_ext[ge.x >> 16], ge.x >> 16, WITH_E)                              \
-          TSB_PAIR_SHELL(s_ext[ge.x & 0xFFFFu], ge.x & 0xFFFFu, WITH_E)                      \
+          TSB_PAIR_SHELL(EXT(ge.y >> 16), ge.y >> 16, WITH_E)                              \
+          TSB_PAIR_SHELL(EXT(ge.y & 0xFFFFu), ge.y & 0xFFFFu, WITH_E)                      \
+          TSB_PAIR_SHELL(EXT(ge.x >> 16), ge.x >> 16, WITH_E)                              \
+          TSB_PAIR_SHELL(EXT(ge.x & 0xFFFFu), ge.x & 0xFFFFu, WITH_E)                      \
         }                                                                                    \
         if (srem) {                                                                          \
           const uint2 ge = s_list[(kListGroups - 1 - sfull) * kFusedThreads + tid];          \
-          TSB_PAIR_SHELL(s_ext[ge.y >> 16], ge.y >> 16, WITH_E)                              \
-          if (srem > 1) TSB_PAIR_SHELL(s_ext[ge.y & 0xFFFFu], ge.y & 0xFFFFu, WITH_E)        \
-          if (srem > 2) TSB_PAIR_SHELL(s_ext[ge.x >> 16], ge.x >> 16, WITH_E)                \
+          TSB_PAIR_SHELL(EXT(ge.y >> 16), ge.y >> 16, WITH_E)                              \
+          if (srem > 1) TSB_PAIR_SHELL(EXT(ge.y & 0xFFFFu), ge.y & 0xFFFFu, WITH_E)        \
+          if (srem > 2) TSB_PAIR_SHELL(EXT(ge.x >> 16), ge.x >> 16, WITH_E)                \
         }                                                                                    \
       }                                                                                      \
     }                                                                                        \
@@ -912,6 +918,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
 #undef TSB_PAIR_CORE
 #undef TSB_PAIR_SHELL
 #undef TSB_PAIR2
+#undef EXT
 #undef TSB_REBUILD
 #undef TSB_FILE_PAIR
     // ---- write back + FP64 energy reduction (each pair seen from both ends)
