@@ -513,17 +513,20 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     // files each neighbour as core or shell.  If the shared-memory tables
     // overflow, the skin of this system is halved.
     //
-    // file a candidate E at Q as a core or shell neighbour of the owned atom
+    // list entries and the bin-sorted entry order hold byte offsets (entry * 16)
+    // into the image table
+#define EXT(OFF) (*(const float4 *)((const unsigned char *)s_ext + (OFF)))
+    // file a candidate at byte offset E (position Q) as a core or shell
+    // neighbour of the owned atom
 #define TSB_FILE_PAIR(E, Q)                                                                  \
   {                                                                                          \
     const float dx = (Q).x - xi.x, dy = (Q).y - xi.y, dz = (Q).z - xi.z;                     \
     const float d2 = dx * dx + dy * dy + dz * dz;                                            \
-    if (d2 < build2 && (E) != a) {                                                           \
+    if (d2 < build2 && (E) != a16) {                                                         \
       const float cr2 = MULTI ? g.core2[sp * A.n_species + __float_as_int((Q).w)] : core0;   \
       if (ncore + nshell < kListLen) {                                                       \
         const int slot_ = d2 < cr2 ? ncore : kListLen - 1 - nshell;                          \
-        list16[(((slot_ >> 2) * kFusedThreads + tid) << 2) | (slot_ & 3)] =                  \
-            (uint16_t)((E) << 4);                                                            \
+        list16[(((slot_ >> 2) * kFusedThreads + tid) << 2) | (slot_ & 3)] = (uint16_t)(E);   \
       }                                                                                      \
       if (d2 < cr2)                                                                          \
         ++ncore;                                                                             \
@@ -622,9 +625,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       }                                                                                      \
       __syncthreads();                                                                       \
       for (int e = tid; e < n_ext; e += kFusedThreads)                                       \
-        s_sorted[atomicAdd(&s_bin[s_ebin[e]], 1)] = (uint16_t)e;                             \
+        s_sorted[atomicAdd(&s_bin[s_ebin[e]], 1)] = (uint16_t)(e << 4);                      \
       __syncthreads();                                                                       \
-      /* s_bin[b] is now the end of bin b; order each bin by entry index */                  \
+      /* s_bin[b] is now the end of bin b; order each bin by entry */                        \
       for (int b = tid; b < nbins; b += kFusedThreads) {                                     \
         const int lo_ = b ? s_bin[b - 1] : 0, hi_ = s_bin[b];                                \
         for (int i_ = lo_ + 1; i_ < hi_; ++i_) {                                             \
@@ -644,6 +647,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
         const float4 xi = s_ext[a];                                                          \
         const float build2 = g.build2;                                                       \
         const float core0 = g.core2[0];                                                      \
+        const int a16 = a << 4;                                                              \
         const int bx = bin_coord(g, f0, 0), by = bin_coord(g, f1, 1);                        \
         const int bz = bin_coord(g, f2, 2);                                                  \
         const int zlo = max(bz - 2, 0), zhi = min(bz + 2, g.nb[2] - 1);                      \
@@ -656,13 +660,13 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
             int p_ = plo + lane;                                                             \
             for (; p_ + tpa < phi; p_ += 2 * tpa) {                                          \
               const int e0 = s_sorted[p_], e1 = s_sorted[p_ + tpa];                          \
-              const float4 q0 = s_ext[e0], q1 = s_ext[e1];                                   \
+              const float4 q0 = EXT(e0), q1 = EXT(e1);                                       \
               TSB_FILE_PAIR(e0, q0)                                                          \
               TSB_FILE_PAIR(e1, q1)                                                          \
             }                                                                                \
             if (p_ < phi) {                                                                  \
               const int e0 = s_sorted[p_];                                                   \
-              const float4 q0 = s_ext[e0];                                                   \
+              const float4 q0 = EXT(e0);                                                     \
               TSB_FILE_PAIR(e0, q0)                                                          \
             }                                                                                \
           }                                                                                  \
@@ -692,8 +696,6 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
   }
 
     // ------------------------------------------------------------ pair loop
-    // list entries are byte offsets (entry * 16) into the image table
-#define EXT(OFF) (*(const float4 *)((const unsigned char *)s_ext + (OFF)))
     // Four list entries per iteration, branch-free (out-of-range pairs are
     // evaluated and masked), so the loads and the math of the four pairs
     // overlap.  Core pairs need no cutoff test.

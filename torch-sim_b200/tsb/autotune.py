@@ -112,9 +112,10 @@ def tune_fused_skin(state, model, *, integrator: str = "nvt_langevin", dt, kT=No
                     force: bool = False, timer=_time_launch) -> float:
     """Verlet skin for ``FusedMD`` on this workload (cached; see module doc).
 
-    Each candidate runs the fused kernel ``n_steps`` steps (after a short
-    warm-up launch) from the same starting point on a sample of the batch: two
-    systems per SM by default, spread over the batch.
+    Each candidate runs the fused kernel on a sample of the batch (two systems
+    per SM by default, spread over the batch) from the same starting point:
+    ``n_steps`` steps of warm-up (the atoms leave their starting positions and
+    the list rebuild rate settles), then ``n_steps`` timed steps.
     """
     from .integrators import FusedMD
 
@@ -144,7 +145,7 @@ def tune_fused_skin(state, model, *, integrator: str = "nvt_langevin", dt, kT=No
     for skin in candidates:
         r = FusedMD(sample.clone(), model, integrator=integrator, dt=per_sys(dt),
                     kT=per_sys(kT), gamma=per_sys(gamma), skin=float(skin), seed=0)
-        r.launch(max(1, n_steps // 10))
+        r.launch(n_steps)
         timings[float(skin)] = float(timer(r, n_steps))
         r.check()
     best = select_best(timings)
