@@ -40,6 +40,22 @@ WORKLOAD = ("2048 Cu fcc systems (8-512 atoms, strain +-2%, shear +-3deg), Morse
             "(D=0.3429 eV, alpha=1.3588/A, r0=2.866 A, rc=6.0 A), NVT-Langevin BAOAB "
             "1000 K, dt=2 fs, gamma=0.01/fs")
 ALG_BYTES_PER_ATOM_STEP = 76  # streaming state r/w: 48 B FP64 pos + 24 B mom + 4 B type/mass
+# algorithmic compute per atom-step of the Morse workload (rho = 0.0850 / A^3, rc = 6 A):
+# 38.5 half-list pairs, ~45 FP32 flops and one exp per pair
+HALF_PAIRS_PER_ATOM = 38.5
+FLOPS_PER_PAIR = 45
+
+
+def sm_peaks(device):
+    """Nominal FP32 (FMA = 2 flops, 128 lanes/SM) and MUFU (16 lanes/SM) peaks at
+    the maximum SM clock."""
+    import torch
+
+    props = torch.cuda.get_device_properties(device)
+    ghz = ClockSampler.max_sm_mhz(device.index or 0) / 1e3
+    fp32 = props.multi_processor_count * 128 * 2 * ghz / 1e3  # TFLOP/s
+    sfu = props.multi_processor_count * 16 * ghz  # G ops/s
+    return fp32, sfu
 
 
 def parse():
@@ -92,6 +108,17 @@ class ClockSampler:
             except Exception:  # noqa: BLE001
                 pass
             self._stop.wait(0.2)
+
+    @staticmethod
+    def max_sm_mhz(index: int) -> float:
+        """clocks.max.sm of GPU `index` (B200 specification value if unreadable)."""
+        try:
+            out = subprocess.run(["nvidia-smi", f"--id={index}", "--query-gpu=clocks.max.sm",
+                                  "--format=csv,noheader,nounits"], capture_output=True,
+                                 text=True, timeout=5).stdout.strip()
+            return float(out.splitlines()[0])
+        except Exception:  # noqa: BLE001
+            return 1965.0
 
     def __enter__(self):
         self._t = threading.Thread(target=self._run, daemon=True)
@@ -504,6 +531,7 @@ def main():
 
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
+        fp32_peak, sfu_peak = sm_peaks(device)
         alg_bytes = n_atoms * args.md_steps * ALG_BYTES_PER_ATOM_STEP
         achieved = alg_bytes / avg_launch_s / 1e9
         traffic = profiled_traffic()
@@ -525,6 +553,19 @@ def main():
                          "peak_source": peak_kind,
                          "algorithmic_bytes_per_atom_step": ALG_BYTES_PER_ATOM_STEP,
                          "kernel": "k_fused_md"},
+            # the binding bound of this shared-memory-resident kernel is inside the SM
+            "roofline_sm": {"bound": "fp32 issue", "kernel": "k_fused_md",
+                            "achieved": value * HALF_PAIRS_PER_ATOM * FLOPS_PER_PAIR / 1e12,
+                            "peak": fp32_peak, "unit": "TFLOP/s",
+                            "frac": value * HALF_PAIRS_PER_ATOM * FLOPS_PER_PAIR / 1e12
+                            / fp32_peak,
+                            "exp_per_s": value * HALF_PAIRS_PER_ATOM,
+                            "sfu_peak_per_s": sfu_peak * 1e9,
+                            "sfu_frac": value * HALF_PAIRS_PER_ATOM / (sfu_peak * 1e9),
+                            "algorithm": f"{HALF_PAIRS_PER_ATOM} half-list pairs x "
+                                         f"{FLOPS_PER_PAIR} FP32 flops + 1 exp per atom-step",
+                            "peak_source": "nominal: SMs x 128 FP32 lanes x 2 x max SM clock; "
+                                           "MUFU 16 lanes/SM"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "force_err_vs_fp64": force_err,
