@@ -100,4 +100,57 @@ __device__ __forceinline__ void pair_eval(const PairPrm<R> &q, R r2, R &e, R &fr
   }
 }
 
+// PTX approximate instructions (relative error ~2^-22 .. 2^-23, denormals
+// flushed: r^2 > 1e-30 and the exponents here are far from the denormal range).
+__device__ __forceinline__ float ex2_ftz(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_ftz(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// Morse rows used with pair_eval_fast also carry the exponent as one FMA in base 2:
+// a6 = -alpha log2(e), a7 = alpha r0 log2(e), so exp(-alpha (r - r0)) =
+// 2^(a6 r + a7).
+__device__ inline void prm_fast_extra(int pot, const double *t, PairPrm<float> &q) {
+  if (pot == TSB_POT_MORSE) {
+    const double log2e = 1.4426950408889634;
+    q.a6 = (float)(-t[2] * log2e);
+    q.a7 = (float)(t[2] * t[0] * log2e);
+  }
+}
+
+// Fast FP32 pair evaluation (same e and fr = -V'(r)/r as pair_eval, fewer
+// instructions; rows need prm_fast_extra).
+template <int POT>
+__device__ __forceinline__ void pair_eval_fast(const PairPrm<float> &q, float r2, float &e,
+                                               float &fr) {
+  if (POT == TSB_POT_MORSE) {
+    // V = D (1 - x)^2 - D - shift = D x (x - 2) - shift, x = exp(-alpha (r - r0))
+    const float ir = rsqrt_ftz(r2);
+    const float r = r2 * ir;
+    const float x = ex2_ftz(fmaf(q.a6, r, q.a7));
+    e = q.a1 * x * (x - 2.0f) - q.a4;
+    fr = -q.a5 * fmaf(-x, x, x) * ir;  // -2 alpha D x (1 - x) / r
+  } else if (POT == TSB_POT_LJ) {
+    // V = 4 eps (s6^2 - s6) - shift, s6 = (sigma^2 / r^2)^3
+    const float ir2 = rcp_ftz(r2);
+    const float s2 = q.a0 * ir2;
+    const float s6 = s2 * s2 * s2;
+    e = q.a1 * s6 * (s6 - 1.0f) - q.a4;
+    fr = q.a2 * s6 * fmaf(2.0f, s6, -1.0f) * ir2;
+  } else {
+    pair_eval<POT, float>(q, r2, e, fr);
+  }
+}
+
 }  // namespace tsb

@@ -93,6 +93,7 @@ __global__ void __launch_bounds__(256)
   __shared__ double sv[27 * 3];
   for (int k = threadIdx.x; k < ns_species * ns_species; k += blockDim.x) {
     prm[k] = make_prm<float>(POT, table + 5 * k, cutoff);
+    prm_fast_extra(POT, table + 5 * k, prm[k]);
     prc2[k] = pair_rc2(POT, table + 5 * k, cutoff);
   }
   for (int k = threadIdx.x; k < 27; k += blockDim.x) {
@@ -108,9 +109,9 @@ __global__ void __launch_bounds__(256)
     const int si = (int)__double_as_longlong(wi.w);
     const PairPrm<float> *row = prm + si * ns_species;
     const int c = cnt[i];
-    float fx = 0.f, fy = 0.f, fz = 0.f;
-    // one pair (entry E, neighbour position WJ); the displacement and the
-    // cutoff test are FP64, the pair function FP32
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    // one pair (entry E, neighbour position WJ): FP64 displacement, cutoff test,
+    // force and virial accumulation; FP32 pair function of r^2
 #define TSB_VPAIR(E, WJ)                                                                     \
   {                                                                                          \
     const int code = (int)((E) & 31u);                                                       \
@@ -118,23 +119,23 @@ __global__ void __launch_bounds__(256)
     const double dy = (WJ).y - wi.y + sv[3 * code + 1];                                      \
     const double dz = (WJ).z - wi.z + sv[3 * code + 2];                                      \
     const int sj = (int)__double_as_longlong((WJ).w);                                        \
-    if (dx * dx + dy * dy + dz * dz < prc2[si * ns_species + sj]) {                          \
-      const float rx = (float)dx, ry = (float)dy, rz = (float)dz;                            \
-      const float r2 = rx * rx + ry * ry + rz * rz;                                          \
+    const double d2 = dx * dx + dy * dy + dz * dz;                                           \
+    if (d2 < prc2[si * ns_species + sj]) {                                                   \
       float ep, fr;                                                                          \
-      pair_eval<POT, float>(row[sj], r2, ep, fr);                                            \
-      const float gx = fr * rx, gy = fr * ry, gz = fr * rz;                                  \
+      pair_eval_fast<POT>(row[sj], (float)d2, ep, fr);                                       \
+      const double gr = (double)fr;                                                          \
+      const double gx = gr * dx, gy = gr * dy, gz = gr * dz;                                 \
       fx -= gx;                                                                              \
       fy -= gy;                                                                              \
       fz -= gz;                                                                              \
       ei += (double)ep;                                                                      \
       if (want_vir) {                                                                        \
-        vxx += (double)(rx * gx);                                                            \
-        vyy += (double)(ry * gy);                                                            \
-        vzz += (double)(rz * gz);                                                            \
-        vyz += (double)(ry * gz);                                                            \
-        vxz += (double)(rx * gz);                                                            \
-        vxy += (double)(rx * gy);                                                            \
+        vxx += dx * gx;                                                                      \
+        vyy += dy * gy;                                                                      \
+        vzz += dz * gz;                                                                      \
+        vyz += dy * gz;                                                                      \
+        vxz += dx * gz;                                                                      \
+        vxy += dx * gy;                                                                      \
       }                                                                                      \
     }                                                                                        \
   }
