@@ -223,6 +223,40 @@ int tsb_fire_converged(const void *forces, const int64_t *system_idx, int64_t n_
                        uint8_t *active, int32_t *n_active, int dtype, void *workspace,
                        size_t workspace_bytes, void *stream);
 
+/* ---- NVT thermostats: Nose-Hoover chains and V-rescale (CSVR) -------------
+ * One block per system; per-system arrays are float64 [S] (chain arrays [S,M]).
+ * tsb_kinetic_energy: ke[s] = 1/2 sum p^2/m over system s (quantities.py:104-139).
+ * tsb_nhc_half_step: the chain half step of nvt_nose_hoover_step
+ *   (torch_sim/integrators/md.py:388-514, nvt.py:381-488): chain_steps x sy_steps
+ *   Suzuki-Yoshida sub-steps (sy_steps 1, 3, 5 or 7) of the chain positions xi and
+ *   momenta p_xi (in/out), chain masses Q (out) recomputed from kT, tau and dof
+ *   (Q_j = kT tau^2, Q_1 = dof kT tau^2, md.py:534-559), momenta rescaled in place.
+ *   ke (in/out) is the kinetic energy the chain sees: with recompute_ke it is
+ *   first summed from the momenta, else the value carried from the last call is
+ *   used (as the reference carries chain.kinetic_energy).  dt is the chain's
+ *   time step (the one the chain was constructed with, md.py:495-508).
+ *   chain_length 1..16.
+ * tsb_vrescale: momenta *= lambda per system, lambda^2 = c1 + c2 (r1^2 + 2 g) +
+ *   2 r1 sqrt(c1 c2), c1 = exp(-dt/tau), c2 = (1 - c1) (dof kT / 2) / KE / dof
+ *   (nvt.py:594-654).  noise [S,2] = (r1, g) with g ~ Gamma((dof-1)/2, 1) when
+ *   non-NULL; else both are drawn on the device from Philox4x32-10 keyed by
+ *   (seed, system, counter).  lam [S] (optional) receives lambda. */
+size_t tsb_thermostat_workspace_size(int64_t n_systems);
+int tsb_kinetic_energy(const void *momenta, const void *masses, const int64_t *system_idx,
+                       int64_t n_atoms, int64_t n_systems, int dtype, double *ke,
+                       void *workspace, size_t workspace_bytes, void *stream);
+int tsb_nhc_half_step(void *momenta, const void *masses, const int64_t *system_idx,
+                      int64_t n_atoms, int64_t n_systems, int dtype, double *xi,
+                      double *p_xi, double *Q, double *ke, const double *dof,
+                      const double *kT, const double *tau, const double *dt,
+                      int chain_length, int chain_steps, int sy_steps, int recompute_ke,
+                      void *workspace, size_t workspace_bytes, void *stream);
+int tsb_vrescale(void *momenta, const void *masses, const int64_t *system_idx,
+                 int64_t n_atoms, int64_t n_systems, int dtype, const double *dof,
+                 const double *kT, const double *tau, const double *dt, const double *noise,
+                 uint64_t seed, uint64_t counter, double *lam, void *workspace,
+                 size_t workspace_bytes, void *stream);
+
 /* ---- fused persistent batched MD ----------------------------------------
  * Advances every system by n_steps of velocity Verlet (TSB_INT_NVE,
  * nve.py:74-130) or BAOAB Langevin (TSB_INT_LANGEVIN, nvt.py:144-240) in one

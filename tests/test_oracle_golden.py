@@ -196,3 +196,57 @@ def test_math_oracle_matches_reference(golden):
     np.testing.assert_allclose(linalg3.expm(m["A"]), m["expm_torch"], rtol=1e-13,
                                atol=1e-14)
     np.testing.assert_allclose(linalg3.logm(m["T"]), m["logT"], rtol=1e-10, atol=1e-13)
+
+
+def _morse_fn(cell, sysi):
+    tab = opair.single_table(opair.MORSE, 2.866, 0.3429, 1.3588)
+
+    def fn(q):
+        o = opair.pair_forward(opair.MORSE, tab, np.zeros(len(q), int), q,
+                               np.transpose(cell, (0, 2, 1)), np.array([True] * 3), sysi, 6.0)
+        return o["energy"], o["forces"]
+    return fn
+
+
+def test_nose_hoover_oracle_matches_reference(golden):
+    from oracle import thermostats as oth
+
+    s, g = golden["thermostats"]["sys"], golden["thermostats"]["nhc"]
+    sysi = s["system_idx"].astype(np.int64)
+    fn = _morse_fn(s["cell"], sysi)
+    dt, kT = float(s["dt"]), float(s["kT"])
+    np.testing.assert_allclose(oth.chain_masses(g["dof"], kT, g["tau"], 3), g["Q"][0],
+                               rtol=1e-14)
+    e0, f0 = fn(g["positions"][0])
+    st = {"positions": g["positions"][0], "momenta": g["momenta"][0], "masses": s["masses"],
+          "forces": f0, "energy": e0}
+    ch = {"xi": g["xi"][0], "p_xi": g["p_xi"][0], "ke": g["KE"][0], "dof": g["dof"],
+          "tau": g["tau"]}
+    for k in range(1, g["positions"].shape[0]):
+        st, ch = oth.nvt_nose_hoover_step(st, ch, fn, dt, kT, 3, 3, sysi)
+        np.testing.assert_allclose(st["positions"], g["positions"][k], rtol=1e-12, atol=1e-12)
+        np.testing.assert_allclose(st["momenta"], g["momenta"][k], rtol=1e-9, atol=1e-12)
+        np.testing.assert_allclose(ch["xi"], g["xi"][k], rtol=1e-9, atol=1e-14)
+        np.testing.assert_allclose(ch["p_xi"], g["p_xi"][k], rtol=1e-9, atol=1e-14)
+        np.testing.assert_allclose(ch["ke"], g["KE"][k], rtol=1e-10)
+        inv = oth.nose_hoover_invariant(st["energy"], s["masses"], st["momenta"], sysi,
+                                        ch["xi"], ch["p_xi"], ch["q"], g["dof"], kT)
+        np.testing.assert_allclose(inv, g["invariant"][k], rtol=1e-11)
+
+
+def test_vrescale_oracle_matches_reference(golden):
+    from oracle import thermostats as oth
+
+    s, g = golden["thermostats"]["sys"], golden["thermostats"]["vr"]
+    sysi = s["system_idx"].astype(np.int64)
+    fn = _morse_fn(s["cell"], sysi)
+    dt, kT = float(s["dt"]), float(s["kT"])
+    e0, f0 = fn(g["positions"][0])
+    st = {"positions": g["positions"][0], "momenta": g["momenta"][0], "masses": s["masses"],
+          "forces": f0, "energy": e0}
+    for k in range(1, g["positions"].shape[0]):
+        st = oth.nvt_vrescale_step(st, fn, dt, kT, float(g["tau"]), g["r1"][k - 1],
+                                   g["gamma"][k - 1], sysi)
+        np.testing.assert_allclose(st["positions"], g["positions"][k], rtol=1e-12, atol=1e-12)
+        np.testing.assert_allclose(st["momenta"], g["momenta"][k], rtol=1e-9, atol=1e-12)
+        np.testing.assert_allclose(st["energy"], g["energy"][k], rtol=1e-10)

@@ -9,6 +9,9 @@ converts user units, torch_sim/integrators/__init__.py:193-255):
   ``nvt_langevin_step(state, model, *, dt, kT, gamma=None)``
   <- torch_sim/integrators/nvt.py:89-240 (BAOAB, gamma default 1/(100 dt))
 * ``initialize_momenta`` <- md.py:113-166
+* ``nvt_nose_hoover_init/step/invariant`` <- nvt.py:244-562 (Nose-Hoover chains,
+  md.py:249-563)
+* ``nvt_vrescale_init/step`` <- nvt.py:565-741 (CSVR; ``step(model, state, ...)``)
 
 Steps mutate ``state`` in place and return it (md.py:184-187).  ``dt``, ``kT``
 and ``gamma`` may be scalars or per-system tensors.
@@ -141,6 +144,153 @@ def nvt_langevin_step(state, model, *, dt, kT, gamma=None, noise=None, **_kw):
            L.ptr(kT_s), L.ptr(g_s), L.ptr(noise), seed & (2**64 - 1), counter,
            state.n_atoms, L.dtype_code(state.dtype), L.stream_ptr(state.device))
     state._philox_seed, state._philox_counter = seed, counter + 1
+    _apply_model(state, model)
+    _kick(state, dt_s, 0.5)
+    return state
+
+
+# ---------------------------------------------------------------------------
+# NVT Nose-Hoover chains and V-rescale (CSVR)
+# ---------------------------------------------------------------------------
+def _dof(state) -> torch.Tensor:
+    """3N - 3 per system (the COM motion removed, nvt.py:287-290, 355-357)."""
+    counts = torch.bincount(state.system_idx, minlength=state.n_systems)
+    dof = 3 * counts - 3
+    if bool((dof <= 0).any()):
+        raise ValueError("Degrees of freedom cannot be zero or negative")
+    return dof.to(torch.float64)
+
+
+def _thermo_ws(state):
+    return L.Workspace.get(state.device,
+                           L.load().tsb_thermostat_workspace_size(state.n_systems))
+
+
+def kinetic_energy(state) -> torch.Tensor:
+    """Per-system 1/2 sum p^2/m in FP64 on the device (quantities.py:104-139)."""
+    ke = torch.empty(state.n_systems, dtype=torch.float64, device=state.device)
+    ws = _thermo_ws(state)
+    L.call("tsb_kinetic_energy", L.ptr(state.momenta), L.ptr(state.masses),
+           L.ptr(state.system_idx), state.n_atoms, state.n_systems,
+           L.dtype_code(state.dtype), L.ptr(ke), L.ptr(ws), ws.numel(),
+           L.stream_ptr(state.device))
+    return ke
+
+
+def nvt_nose_hoover_init(state, model, *, kT, dt, tau=None, chain_length: int = 3,
+                         chain_steps: int = 3, sy_steps: int = 3, **kwargs):
+    """NVT Nose-Hoover-chain state (nvt.py:293-378): tau defaults to 10 dt, chain
+    positions and momenta start at zero, Q_j = kT tau^2, Q_1 = dof kT tau^2."""
+    from .state import NoseHooverChain, NVTNoseHooverState
+
+    if not 1 <= chain_length <= 16:
+        raise ValueError("chain_length must lie in 1..16")
+    if sy_steps not in (1, 3, 5, 7):
+        raise ValueError("sy_steps must be 1, 3, 5 or 7")
+    if kwargs.get("momenta") is not None:
+        state = MDState.from_state(state, momenta=kwargs["momenta"],
+                                   energy=torch.zeros(state.n_systems, dtype=state.dtype,
+                                                      device=state.device),
+                                   forces=torch.zeros_like(state.positions))
+    md = _md_init(state, model, kT)
+    _prepare(md)
+    n_sys, dev = md.n_systems, md.device
+    dt_s = _per_system(dt, n_sys, dev)
+    kT_s = _per_system(kT, n_sys, dev)
+    tau_s = _per_system(10.0 * dt_s if tau is None else tau, n_sys, dev)
+    dof = _dof(md)
+    q = (kT_s * tau_s * tau_s).unsqueeze(-1).repeat(1, chain_length)
+    q[:, 0] *= dof
+    zeros = torch.zeros((n_sys, chain_length), dtype=torch.float64, device=dev)
+    chain = NoseHooverChain(positions=zeros.clone(), momenta=zeros.clone(),
+                            masses=q.contiguous(), tau=tau_s.clone(),
+                            kinetic_energy=kinetic_energy(md), degrees_of_freedom=dof)
+    out = NVTNoseHooverState.from_state(md, chain=chain, chain_steps=int(chain_steps),
+                                        sy_steps=int(sy_steps), chain_dt=dt_s.clone())
+    out._philox_seed, out._philox_counter = md._philox_seed, 0
+    return out
+
+
+def _nhc_half(state, kT_s, recompute: bool):
+    c = state.chain
+    ws = _thermo_ws(state)
+    L.call("tsb_nhc_half_step", L.ptr(state.momenta), L.ptr(state.masses),
+           L.ptr(state.system_idx), state.n_atoms, state.n_systems,
+           L.dtype_code(state.dtype), L.ptr(c.positions), L.ptr(c.momenta), L.ptr(c.masses),
+           L.ptr(c.kinetic_energy), L.ptr(c.degrees_of_freedom), L.ptr(kT_s), L.ptr(c.tau),
+           L.ptr(state.chain_dt), c.positions.shape[1], state.chain_steps, state.sy_steps,
+           int(recompute), L.ptr(ws), ws.numel(), L.stream_ptr(state.device))
+
+
+def nvt_nose_hoover_step(state, model, *, dt, kT, **_kw):
+    """NHC(dt/2) . velocity Verlet . NHC(dt/2) (nvt.py:381-488).  The chain
+    masses follow kT on every step; the chain's own time step is the one it was
+    initialised with."""
+    _prepare(state)
+    c = state.chain
+    for name in ("positions", "momenta", "masses", "tau", "kinetic_energy",
+                 "degrees_of_freedom"):
+        t = getattr(c, name)
+        if t.dtype != torch.float64 or not t.is_contiguous():
+            setattr(c, name, t.to(torch.float64).contiguous())
+    dt_s = _per_system(dt, state.n_systems, state.device)
+    kT_s = _per_system(kT, state.n_systems, state.device)
+    _nhc_half(state, kT_s, recompute=False)
+    _kick(state, dt_s, 0.5)
+    _drift(state, dt_s, 1.0)
+    _apply_model(state, model)
+    _kick(state, dt_s, 0.5)
+    _nhc_half(state, kT_s, recompute=True)
+    return state
+
+
+def nvt_nose_hoover_invariant(state, kT) -> torch.Tensor:
+    """Extended-system energy: E_pot + E_kin + sum_j p_xi_j^2 / (2 Q_j) + dof kT xi_1
+    + kT sum_{j>1} xi_j (nvt.py:491-562)."""
+    c = state.chain
+    kT_s = _per_system(kT, state.n_systems, state.device)
+    e = state.energy.to(torch.float64) + kinetic_energy(state)
+    e = e + c.momenta[:, 0] ** 2 / (2 * c.masses[:, 0]) + c.degrees_of_freedom * kT_s * c.positions[:, 0]
+    for j in range(1, c.positions.shape[1]):
+        e = e + c.momenta[:, j] ** 2 / (2 * c.masses[:, j]) + kT_s * c.positions[:, j]
+    return e
+
+
+def nvt_vrescale_init(state, model, *, kT, **_kw):
+    """V-rescale (CSVR) state (nvt.py:657-712)."""
+    from .state import NVTVRescaleState
+
+    md = _md_init(state, model, kT)
+    out = NVTVRescaleState.from_state(md)
+    out._philox_seed, out._philox_counter = md._philox_seed, 0
+    return out
+
+
+def nvt_vrescale_step(model, state, *, dt, kT, tau=None, noise=None, **_kw):
+    """Rescale the momenta by the CSVR factor, then velocity Verlet
+    (nvt.py:715-741; note the reference's argument order, model first).  tau
+    defaults to 10 dt.  The normal r1 and the Gamma((dof - 1)/2) deviate are drawn
+    on the device from the Philox stream (seed, system, step); ``noise`` [S, 2]
+    = (r1, gamma deviate) supplies them instead, e.g. the reference's own draws."""
+    _prepare(state)
+    n_sys, dev = state.n_systems, state.device
+    dt_s = _per_system(dt, n_sys, dev)
+    kT_s = _per_system(kT, n_sys, dev)
+    tau_s = _per_system(10.0 * dt_s if tau is None else tau, n_sys, dev)
+    dof = _dof(state)
+    if noise is not None:
+        noise = torch.as_tensor(noise, dtype=torch.float64, device=dev).reshape(n_sys, 2)
+        noise = noise.contiguous()
+    seed = getattr(state, "_philox_seed", _seed_of(state))
+    counter = getattr(state, "_philox_counter", 0)
+    ws = _thermo_ws(state)
+    L.call("tsb_vrescale", L.ptr(state.momenta), L.ptr(state.masses), L.ptr(state.system_idx),
+           state.n_atoms, n_sys, L.dtype_code(state.dtype), L.ptr(dof), L.ptr(kT_s),
+           L.ptr(tau_s), L.ptr(dt_s), L.ptr(noise), seed & (2**64 - 1), counter, None,
+           L.ptr(ws), ws.numel(), L.stream_ptr(dev))
+    state._philox_seed, state._philox_counter = seed, counter + 1
+    _kick(state, dt_s, 0.5)
+    _drift(state, dt_s, 1.0)
     _apply_model(state, model)
     _kick(state, dt_s, 0.5)
     return state

@@ -150,6 +150,47 @@ class MDState(SimState):
         self.momenta = new_momenta
 
 
+@dataclass
+class NoseHooverChain:
+    """Per-system Nose-Hoover chain variables (torch_sim/integrators/md.py:249-273):
+    positions / momenta / masses [S, M], tau, kinetic_energy, degrees_of_freedom [S]."""
+
+    positions: torch.Tensor
+    momenta: torch.Tensor
+    masses: torch.Tensor
+    tau: torch.Tensor
+    kinetic_energy: torch.Tensor
+    degrees_of_freedom: torch.Tensor
+
+    def clone(self) -> "NoseHooverChain":
+        return NoseHooverChain(*(getattr(self, f.name).clone()
+                                 for f in dataclasses.fields(self)))
+
+
+@dataclass(kw_only=True)
+class NVTNoseHooverState(MDState):
+    """MDState + Nose-Hoover chain (torch_sim/integrators/nvt.py:244-290).  The
+    chain integrates with ``chain_dt`` [S], the time step it was set up with."""
+
+    chain: NoseHooverChain
+    chain_steps: int = 3
+    sy_steps: int = 3
+    chain_dt: torch.Tensor | None = None
+
+    def clone(self):
+        c = super().clone()
+        c.chain = self.chain.clone()
+        return c
+
+    def get_number_of_degrees_of_freedom(self) -> torch.Tensor:
+        return self.chain.degrees_of_freedom
+
+
+@dataclass(kw_only=True)
+class NVTVRescaleState(MDState):
+    """MDState for the V-rescale thermostat (torch_sim/integrators/nvt.py:565-591)."""
+
+
 @dataclass(kw_only=True)
 class FireState(SimState):
     forces: torch.Tensor
