@@ -61,6 +61,8 @@ extern "C" {
 
 #define TSB_INT_NVE 0
 #define TSB_INT_LANGEVIN 1
+#define TSB_INT_NOSE_HOOVER 2 /* tsb_fused_md_nvt only */
+#define TSB_INT_VRESCALE 3    /* tsb_fused_md_nvt only */
 
 const char *tsb_version(void);
 const char *tsb_status_string(int status);
@@ -293,6 +295,29 @@ int tsb_fused_md(int integrator, int potential, const double *table, int n_speci
                  uint64_t seed, uint64_t counter, uint64_t *counter_dev, double *energy,
                  int32_t *n_rebuilds, int32_t *status, void *workspace,
                  size_t workspace_bytes, void *stream);
+
+/* ---- fused persistent batched MD with a Nose-Hoover chain or V-rescale ----
+ * tsb_fused_md with thermostat TSB_INT_NOSE_HOOVER (nvt_nose_hoover_step,
+ * torch_sim/integrators/nvt.py:381-488: chain half step, velocity Verlet, chain
+ * half step, per system) or TSB_INT_VRESCALE (nvt_vrescale_step, nvt.py:715-741:
+ * CSVR rescale, then velocity Verlet).  The thermostat arithmetic is that of
+ * tsb_nhc_half_step / tsb_vrescale (shared code), degrees of freedom 3N - 3.
+ * tau_sys [S]: thermostat time constant.  Nose-Hoover: chain_xi, chain_pxi,
+ * chain_Q [S, chain_length] and chain_ke [S] in/out (the state's chain; Q is
+ * recomputed from kT, tau, dof), chain_dt [S] the chain's time step.
+ * V-rescale draws (r1, Gamma) from the Philox stream (seed, system,
+ * counter + step), the same stream tsb_vrescale uses with that counter. */
+int tsb_fused_md_nvt(int thermostat, int potential, const double *table, int n_species,
+                     const int32_t *species, double *positions, double *momenta,
+                     double *forces, const double *masses, const double *cell_row,
+                     const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
+                     const int32_t *order, double cutoff, double skin, int64_t n_steps,
+                     const double *dt_sys, const double *kT_sys, const double *tau_sys,
+                     double *chain_xi, double *chain_pxi, double *chain_Q, double *chain_ke,
+                     const double *chain_dt, int chain_length, int chain_steps, int sy_steps,
+                     uint64_t seed, uint64_t counter, uint64_t *counter_dev, double *energy,
+                     int32_t *n_rebuilds, int32_t *status, void *workspace,
+                     size_t workspace_bytes, void *stream);
 
 /* ---- allocation-free fused MD -------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device

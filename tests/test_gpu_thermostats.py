@@ -144,3 +144,58 @@ def test_thermostat_holds_temperature(thermostat):
             temps.append(float((t * n_at).sum() / n_at.sum()) / workloads.KB_EV)
     # calc_kT divides by 3N; the thermostats target kT on 3N - 3 degrees of freedom
     assert abs(np.mean(temps) - 600.0) < 45.0, temps
+
+
+def _cu_batch(n_sys=10, seed=8):
+    from tsb import models, workloads
+    from tsb.state import state_from_arrays
+
+    d = workloads.copper_batch(n_sys, 16, 300, seed=seed)
+    st = state_from_arrays(d, device="cuda")
+    st.rng = seed
+    m = models.MorseModel(sigma=2.866, epsilon=0.3429, alpha=1.3588, cutoff=6.0)
+    return st, m
+
+
+def test_fused_nose_hoover_matches_step_function():
+    """Persistent kernel with the chain inside == nvt_nose_hoover_step loop (FP32
+    pair math on both paths; chain arithmetic shared)."""
+    from tsb import integrators as I
+    from tsb import workloads
+
+    st, m = _cu_batch()
+    kT, dt = 800.0 * workloads.KB_EV, 0.002 * workloads.METAL_TIME
+    md = I.nvt_nose_hoover_init(st, m, kT=kT, dt=dt)
+    a = md.clone()
+    for _ in range(20):
+        a = I.nvt_nose_hoover_step(a, m, dt=dt, kT=kT)
+    b = I.run_md(md.clone(), m, 20, integrator="nvt_nose_hoover", dt=dt, kT=kT, skin=0.5)
+    np.testing.assert_allclose(b.positions.cpu(), a.positions.cpu(), atol=2e-6)
+    np.testing.assert_allclose(b.momenta.cpu(), a.momenta.cpu(), atol=1e-4, rtol=1e-4)
+    np.testing.assert_allclose(b.chain.momenta.cpu(), a.chain.momenta.cpu(), rtol=1e-4,
+                               atol=1e-7)
+    np.testing.assert_allclose(b.chain.positions.cpu(), a.chain.positions.cpu(), rtol=1e-4,
+                               atol=1e-8)
+    np.testing.assert_allclose(b.chain.kinetic_energy.cpu(), a.chain.kinetic_energy.cpu(),
+                               rtol=1e-5)
+    np.testing.assert_allclose(I.nvt_nose_hoover_invariant(b, kT).cpu(),
+                               I.nvt_nose_hoover_invariant(a, kT).cpu(), rtol=1e-6)
+
+
+def test_fused_vrescale_matches_step_function():
+    """Same Philox draws (seed, system, step) in the kernel and the step function."""
+    from tsb import integrators as I
+    from tsb import workloads
+
+    st, m = _cu_batch(seed=9)
+    kT, dt = 800.0 * workloads.KB_EV, 0.002 * workloads.METAL_TIME
+    md = I.nvt_vrescale_init(st, m, kT=kT)
+    a = md.clone()
+    a._philox_seed, a._philox_counter = 77, 0
+    for _ in range(20):
+        a = I.nvt_vrescale_step(m, a, dt=dt, kT=kT)
+    b = md.clone()
+    b._philox_seed, b._philox_counter = 77, 0
+    b = I.run_md(b, m, 20, integrator="nvt_vrescale", dt=dt, kT=kT, skin=0.5)
+    np.testing.assert_allclose(b.positions.cpu(), a.positions.cpu(), atol=2e-6)
+    np.testing.assert_allclose(b.momenta.cpu(), a.momenta.cpu(), atol=1e-4, rtol=1e-4)

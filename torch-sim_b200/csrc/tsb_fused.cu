@@ -44,6 +44,7 @@
 
 #include "tsb_pair.cuh"
 #include "tsb_rng.cuh"
+#include "tsb_thermostat.cuh"
 
 namespace tsb {
 
@@ -85,6 +86,10 @@ struct FusedArgs {
   int32_t *n_rebuilds;
   int32_t *queue;
   int32_t *status;
+  // Nose-Hoover chain / V-rescale (integrator TSB_INT_NOSE_HOOVER / TSB_INT_VRESCALE)
+  double *cxi, *cpxi, *cQ, *cke;  // chain positions, momenta, masses [S, M]; carried KE [S]
+  const double *tau, *cdt;        // thermostat time constant [S]; chain time step [S]
+  int M, nc, nsy;                 // chain length, chain steps, Suzuki-Yoshida steps
 };
 
 // per-system geometry, computed by thread 0 into shared memory
@@ -98,6 +103,10 @@ struct FusedGeom {
   double skin;    // this system's current Verlet skin
   double half_skin2;    // (skin / 2)^2: rebuild when an atom moved further
   double dt, half, c1;  // time step, dt / 2, Langevin exp(-gamma dt)
+  // thermostat scalars of this system (thread 0), and the momentum factor it
+  // hands to all threads
+  double cx[kMaxChain], cv[kMaxChain], cq[kMaxChain];
+  double cke, nf, kt, tau, cdt, th_scale;
   float band;     // FP32 r^2 within +-band of cutoff^2: decide in FP64
   float build2;   // list radius^2 used by the FP32 build test
   float core2[kFusedMaxSpecies * kFusedMaxSpecies];  // core-pair bound^2 per pair type
@@ -213,6 +222,18 @@ __device__ inline int block_excl_scan_i(int v, int *total, int *sh) {
   *total = sh[32];
   __syncthreads();
   return r;
+}
+
+// FP64 sum over the block in a fixed order (shuffles inside each warp, then the
+// warps in order); the result is valid in thread 0 only
+__device__ inline double block_sum_to0(double v, double *sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < kFusedThreads / 32; ++w) t += sh[w];
+  return t;
 }
 
 // FP32 standard normals for the O-step (Philox4x32-10 + Box-Muller).
@@ -405,6 +426,20 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       g.dt = A.dt[s];
       g.half = g.dt / 2.0;
       g.c1 = (A.integrator == TSB_INT_LANGEVIN) ? exp(-(A.gamma[s] * g.dt)) : 1.0;
+      if (A.integrator == TSB_INT_NOSE_HOOVER || A.integrator == TSB_INT_VRESCALE) {
+        g.nf = 3.0 * (double)g.n - 3.0;  // COM motion removed (nvt.py:287-290)
+        g.kt = A.kT[s];
+        g.tau = A.tau[s];
+        if (A.integrator == TSB_INT_NOSE_HOOVER) {
+          g.cdt = A.cdt[s];
+          g.cke = A.cke[s];
+          for (int j = 0; j < A.M; ++j) {
+            g.cq[j] = g.kt * (g.tau * g.tau) * (j == 0 ? g.nf : 1.0);
+            g.cx[j] = A.cxi[s * A.M + j];
+            g.cv[j] = A.cpxi[s * A.M + j];
+          }
+        }
+      }
       const bool rep_ok = isfinite(d) && d != 0.0 && set_margins(g, A.cutoff, rc2d, nsp2);
       int tpa = 1;
       while (tpa < 32 && g.n * tpa * 2 <= kFusedThreads) tpa *= 2;
@@ -798,6 +833,29 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     if (failed) continue;
     for (int64_t step = 0; step < A.n_steps; ++step) {
       const double dt = g.dt, half = g.half, c1 = g.c1;
+      // thermostat before the step: V-rescale factor from the current kinetic
+      // energy (nvt.py:715-741), or the first Nose-Hoover half step with the
+      // kinetic energy carried from the last one (nvt.py:462-470)
+      if (A.integrator == TSB_INT_VRESCALE) {
+        const double k2 = block_sum_to0(lead ? (px * px + py * py + pz * pz) * inv_m : 0.0,
+                                        s_red);
+        if (tid == 0)
+          g.th_scale = vrescale_lambda(k2, g.nf, g.kt, dt, g.tau, nullptr, A.seed, s,
+                                       counter0 + (uint64_t)step);
+        __syncthreads();
+        const double sc = g.th_scale;
+        px *= sc;
+        py *= sc;
+        pz *= sc;
+      } else if (A.integrator == TSB_INT_NOSE_HOOVER) {
+        if (tid == 0)
+          g.th_scale = nhc_half(g.cdt, A.M, A.nc, A.nsy, g.cq, g.cx, g.cv, g.cke, g.nf, g.kt);
+        __syncthreads();
+        const double sc = g.th_scale;
+        px *= sc;
+        py *= sc;
+        pz *= sc;
+      }
       if (own) {
         px += F0 * half;
         py += F1 * half;
@@ -860,6 +918,20 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
         py += F1 * g.half;
         pz += F2 * g.half;
       }
+      if (A.integrator == TSB_INT_NOSE_HOOVER) {
+        // second half step with the kinetic energy after velocity Verlet
+        const double k2 = block_sum_to0(lead ? (px * px + py * py + pz * pz) * inv_m : 0.0,
+                                        s_red);
+        if (tid == 0) {
+          g.cke = 0.5 * k2;
+          g.th_scale = nhc_half(g.cdt, A.M, A.nc, A.nsy, g.cq, g.cx, g.cv, g.cke, g.nf, g.kt);
+        }
+        __syncthreads();
+        const double sc = g.th_scale;
+        px *= sc;
+        py *= sc;
+        pz *= sc;
+      }
     }
     if (failed) continue;
     if (A.n_steps == 0) TSB_FORCES(true)
@@ -892,6 +964,14 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       for (int k = 0; k < kFusedThreads / 32; ++k) t += s_red[k];
       A.energy[s] = t;
       if (A.n_rebuilds) A.n_rebuilds[s] = rebuilds;
+      if (A.integrator == TSB_INT_NOSE_HOOVER) {
+        for (int j = 0; j < A.M; ++j) {
+          A.cxi[s * A.M + j] = g.cx[j];
+          A.cpxi[s * A.M + j] = g.cv[j];
+          A.cQ[s * A.M + j] = g.cq[j];
+        }
+        A.cke[s] = g.cke;
+      }
     }
   }
 }
@@ -973,6 +1053,72 @@ extern "C" int tsb_fused_md(int integrator, int potential, const double *table,
               masses, cell_row, lo, hi, n_systems, order, cutoff, skin, n_steps, dt_sys,
               kT_sys, gamma_sys, seed, counter, counter_dev, energy, n_rebuilds, queue,
               status};
+  const bool multi = n_species > 1;
+  if (potential == TSB_POT_LJ) {
+    multi ? launch_fused<TSB_POT_LJ, true>(A, grid, st) : launch_fused<TSB_POT_LJ, false>(A, grid, st);
+  } else if (potential == TSB_POT_MORSE) {
+    multi ? launch_fused<TSB_POT_MORSE, true>(A, grid, st)
+          : launch_fused<TSB_POT_MORSE, false>(A, grid, st);
+  } else {
+    multi ? launch_fused<TSB_POT_SOFT, true>(A, grid, st)
+          : launch_fused<TSB_POT_SOFT, false>(A, grid, st);
+  }
+  if (counter_dev) k_advance_counter<<<1, 32, 0, st>>>(counter_dev, n_steps);
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
+
+extern "C" int tsb_fused_md_nvt(int thermostat, int potential, const double *table,
+                                int n_species, const int32_t *species, double *positions,
+                                double *momenta, double *forces, const double *masses,
+                                const double *cell_row, const int64_t *system_idx,
+                                int64_t n_atoms, int64_t n_systems, const int32_t *order,
+                                double cutoff, double skin, int64_t n_steps,
+                                const double *dt_sys, const double *kT_sys,
+                                const double *tau_sys, double *chain_xi, double *chain_pxi,
+                                double *chain_Q, double *chain_ke, const double *chain_dt,
+                                int chain_length, int chain_steps, int sy_steps, uint64_t seed,
+                                uint64_t counter, uint64_t *counter_dev, double *energy,
+                                int32_t *n_rebuilds, int32_t *status, void *workspace,
+                                size_t workspace_bytes, void *stream) {
+  if (thermostat != TSB_INT_NOSE_HOOVER && thermostat != TSB_INT_VRESCALE)
+    return TSB_ERR_INVALID_ARG;
+  if (potential < TSB_POT_LJ || potential > TSB_POT_SOFT) return TSB_ERR_INVALID_ARG;
+  if (n_species < 1 || !table || (n_species > 1 && !species)) return TSB_ERR_INVALID_ARG;
+  if (n_species > kFusedMaxSpecies) return TSB_ERR_UNSUPPORTED;
+  if (n_atoms < 1 || n_systems < 1 || !(cutoff > 0.0) || !(skin >= 0.0) || n_steps < 0)
+    return TSB_ERR_INVALID_ARG;
+  if (!positions || !momenta || !forces || !masses || !cell_row || !system_idx || !dt_sys ||
+      !kT_sys || !tau_sys || !energy || !status)
+    return TSB_ERR_INVALID_ARG;
+  if (thermostat == TSB_INT_NOSE_HOOVER) {
+    if (!chain_xi || !chain_pxi || !chain_Q || !chain_ke || !chain_dt) return TSB_ERR_INVALID_ARG;
+    if (chain_length < 1 || chain_length > kMaxChain || chain_steps < 1) return TSB_ERR_INVALID_ARG;
+    if (sy_steps != 1 && sy_steps != 3 && sy_steps != 5 && sy_steps != 7)
+      return TSB_ERR_INVALID_ARG;
+  }
+  Carver c(workspace, workspace_bytes);
+  int64_t *lo = c.take<int64_t>(n_systems);
+  int64_t *hi = c.take<int64_t>(n_systems);
+  int32_t *queue = c.take<int32_t>(4);
+  if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  int dev = 0, n_sm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  int64_t grid = n_sm;
+  if (grid > kMaxGrid) grid = kMaxGrid;
+  if (grid > n_systems) grid = n_systems;
+  cudaMemsetAsync(lo, 0, sizeof(int64_t) * n_systems, st);
+  cudaMemsetAsync(hi, 0, sizeof(int64_t) * n_systems, st);
+  cudaMemsetAsync(queue, 0, sizeof(int32_t) * 4, st);
+  cudaMemsetAsync(status, 0, sizeof(int32_t) * 4, st);
+  k_bounds_fused<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, lo, hi);
+  FusedArgs A{thermostat, potential, n_species, table, species, positions, momenta, forces,
+              masses, cell_row, lo, hi, n_systems, order, cutoff, skin, n_steps, dt_sys,
+              kT_sys, nullptr, seed, counter, counter_dev, energy, n_rebuilds, queue,
+              status, chain_xi, chain_pxi, chain_Q, chain_ke, tau_sys, chain_dt,
+              chain_length, chain_steps, sy_steps};
   const bool multi = n_species > 1;
   if (potential == TSB_POT_LJ) {
     multi ? launch_fused<TSB_POT_LJ, true>(A, grid, st) : launch_fused<TSB_POT_LJ, false>(A, grid, st);

@@ -15,12 +15,11 @@
 #include <math.h>
 
 #include "tsb_common.cuh"
-#include "tsb_rng.cuh"
+#include "tsb_thermostat.cuh"
 
 namespace tsb {
 
 constexpr int kThBlock = 256;
-constexpr int kMaxChain = 16;
 
 struct ThermoWork {
   int64_t *lo, *hi;  // [S] atom range of each system
@@ -63,59 +62,6 @@ __device__ void scale_momenta(P *p, int64_t a0, int64_t a1, double s) {
     for (int c = 0; c < 3; ++c) p[3 * i + c] = (P)((double)p[3 * i + c] * s);
 }
 
-__device__ inline double sy_weight(int n, int k) {
-  // Suzuki-Yoshida composition weights (Yoshida 1990, Suzuki 1993)
-  switch (n) {
-    case 3: {
-      const double w[3] = {0.828981543588751, -0.657963087177502, 0.828981543588751};
-      return w[k];
-    }
-    case 5: {
-      const double w[5] = {0.2967324292201065, 0.2967324292201065, -0.186929716880426,
-                           0.2967324292201065, 0.2967324292201065};
-      return w[k];
-    }
-    case 7: {
-      const double w[7] = {0.784513610477560, 0.235573213359357, -1.17767998417887,
-                           1.31518632068391, -1.17767998417887, 0.235573213359357,
-                           0.784513610477560};
-      return w[k];
-    }
-    default:
-      return 1.0;
-  }
-}
-
-// One chain sub-step of length `delta` (chain masses q, positions x, momenta v,
-// M = chain length); returns the particle-momentum factor and updates ke.
-__device__ double nhc_substep(double delta, int M, const double *q, double *x, double *v,
-                              double &ke, double nf, double kt) {
-  const double d2 = delta / 2.0, d4 = d2 / 2.0, d8 = d4 / 2.0;
-  const int m = M - 1;
-  if (m > 0) v[m] += d4 * (v[m - 1] * v[m - 1] / q[m - 1] - kt);
-  for (int j = m - 1; j > 0; --j) {
-    const double g = v[j - 1] * v[j - 1] / q[j - 1] - kt;
-    const double s = exp(-d8 * v[j + 1] / q[j + 1]);
-    v[j] = s * (s * v[j] + d4 * g);
-  }
-  {
-    const double g = 2.0 * ke - nf * kt;
-    const double s = m > 0 ? exp(-d8 * v[1] / q[1]) : 1.0;
-    v[0] = s * (s * v[0] + d4 * g);
-  }
-  const double scale = exp(-d2 * v[0] / q[0]);
-  ke = ke * (scale * scale);
-  for (int j = 0; j < M; ++j) x[j] = x[j] + d2 * v[j] / q[j];
-  double g = 2.0 * ke - nf * kt;
-  for (int j = 0; j < m; ++j) {
-    const double s = exp(-d8 * v[j + 1] / q[j + 1]);
-    v[j] = s * (s * v[j] + d4 * g);
-    g = v[j] * v[j] / q[j] - kt;
-  }
-  v[m] += d4 * g;
-  return scale;
-}
-
 template <class P>
 __global__ void __launch_bounds__(kThBlock)
     k_nhc_half(P *p, const P *m, const int64_t *lo, const int64_t *hi, double *xi,
@@ -137,14 +83,7 @@ __global__ void __launch_bounds__(kThBlock)
     }
     q[0] *= nf;
     double k = recompute ? 0.5 * k2 : ke[s];
-    double tot = 1.0;
-    if (nc == 1 && nsy == 1) {
-      tot = nhc_substep(h, M, q, x, v, k, nf, kt);
-    } else {
-      const double delta = h / nc;
-      for (int sub = 0; sub < nc * nsy; ++sub)
-        tot *= nhc_substep(delta * sy_weight(nsy, sub % nsy), M, q, x, v, k, nf, kt);
-    }
+    const double tot = nhc_half(h, M, nc, nsy, q, x, v, k, nf, kt);
     for (int j = 0; j < M; ++j) {
       xi[s * M + j] = x[j];
       p_xi[s * M + j] = v[j];
@@ -166,50 +105,6 @@ __global__ void __launch_bounds__(kThBlock)
   if (threadIdx.x == 0) ke[s] = 0.5 * t;
 }
 
-// uniform in (0, 1] with 53 random bits from two 32-bit words
-__device__ inline double u53(uint32_t a, uint32_t b) {
-  return ((double)((uint64_t)(a >> 5) * 67108864ull + (b >> 6)) + 1.0) *
-         1.1102230246251565e-16;
-}
-
-// Philox words for (seed, system, counter, slot): the slot separates the draws
-// of one step; the tag word keeps these streams apart from the Langevin ones
-__device__ inline U4 thermo_words(uint64_t seed, int64_t s, uint64_t counter, uint32_t slot) {
-  U4 c{(uint32_t)s, 0xC5A00000u ^ slot, (uint32_t)counter, (uint32_t)(counter >> 32)};
-  return philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
-}
-
-__device__ inline double thermo_normal(uint64_t seed, int64_t s, uint64_t counter,
-                                       uint32_t slot) {
-  const U4 r = thermo_words(seed, s, counter, slot);
-  return sqrt(-2.0 * log(u53(r.x, r.y))) * cospi(2.0 * u53(r.z, r.w));
-}
-
-// Gamma(a, 1) deviate, a > 0 (Marsaglia & Tsang, ACM TOMS 26:363, 2000; a < 1
-// through Gamma(a + 1) U^(1/a)); at most 64 proposals (acceptance > 95 % for
-// a >= 1), after which the mode-like value d is returned
-__device__ double gamma_deviate(double a, uint64_t seed, int64_t s, uint64_t counter) {
-  double boost = 1.0;
-  if (a < 1.0) {
-    const U4 r = thermo_words(seed, s, counter, 1u);
-    boost = pow(u53(r.x, r.y), 1.0 / a);
-    a += 1.0;
-  }
-  const double d = a - 1.0 / 3.0, c = 1.0 / sqrt(9.0 * d);
-  for (uint32_t k = 0; k < 64; ++k) {
-    const double xn = thermo_normal(seed, s, counter, 16u + 2u * k);
-    const double v0 = 1.0 + c * xn;
-    if (v0 <= 0.0) continue;
-    const double v = v0 * v0 * v0;
-    const U4 r = thermo_words(seed, s, counter, 17u + 2u * k);
-    const double u = u53(r.x, r.y);
-    if (u < 1.0 - 0.0331 * (xn * xn) * (xn * xn) ||
-        log(u) < 0.5 * xn * xn + d * (1.0 - v + log(v)))
-      return d * v * boost;
-  }
-  return d * boost;
-}
-
 template <class P>
 __global__ void __launch_bounds__(kThBlock)
     k_vrescale(P *p, const P *m, const int64_t *lo, const int64_t *hi, const double *dof,
@@ -221,21 +116,8 @@ __global__ void __launch_bounds__(kThBlock)
   const int64_t a0 = lo[s], a1 = hi[s];
   const double sum = sys_p2m(p, m, a0, a1, sh);
   if (threadIdx.x == 0) {
-    const double nf = dof[s];
-    const double ke_old = nf * (sum / nf) / 2.0;  // dof * current kT / 2
-    const double ke_new = nf * kT[s] / 2.0;
-    double r1, g;
-    if (noise) {
-      r1 = noise[2 * s];
-      g = noise[2 * s + 1];
-    } else {
-      r1 = thermo_normal(seed, s, counter, 0u);
-      g = gamma_deviate((nf - 1.0) / 2.0, seed, s, counter);
-    }
-    const double c1 = exp(-dt[s] / tau[s]);
-    const double c2 = (1.0 - c1) * ke_new / ke_old / nf;
-    const double sc = c1 + c2 * (r1 * r1 + 2.0 * g) + 2.0 * r1 * sqrt(c1 * c2);
-    s_lam = sqrt(sc);
+    s_lam = vrescale_lambda(sum, dof[s], kT[s], dt[s], tau[s], noise ? noise + 2 * s : nullptr,
+                            seed, s, counter);
     if (lam_out) lam_out[s] = s_lam;
   }
   __syncthreads();

@@ -28,7 +28,7 @@ F32, F64 = 0, 1
 POT_LJ, POT_MORSE, POT_SOFT = 0, 1, 2
 NL_SELF_INTERACTION, NL_HALF = 1, 2
 OUT_FORCES, OUT_STRESS, OUT_ENERGIES, OUT_STRESSES, MATH_FP64 = 1, 2, 4, 8, 16
-INT_NVE, INT_LANGEVIN = 0, 1
+INT_NVE, INT_LANGEVIN, INT_NOSE_HOOVER, INT_VRESCALE = 0, 1, 2, 3
 
 _vp, _i64, _u64, _i32, _dbl, _sz, _int = (C.c_void_p, C.c_int64, C.c_uint64, C.c_int32,
                                          C.c_double, C.c_size_t, C.c_int)
@@ -81,6 +81,10 @@ PROTOTYPES = {
     "tsb_fused_md_static": (_int, [_int, _int, _vp, _int, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                    _i64, _i64, _vp, _dbl, _dbl, _i64, _vp, _vp, _vp, _u64,
                                    _u64, _vp, _vp, _vp, _vp]),
+    "tsb_fused_md_nvt": (_int, [_int, _int, _vp, _int, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                _i64, _i64, _vp, _dbl, _dbl, _i64, _vp, _vp, _vp, _vp, _vp,
+                                _vp, _vp, _vp, _int, _int, _int, _u64, _u64, _vp, _vp, _vp,
+                                _vp, _vp, _sz, _vp]),
     "tsb_thermostat_workspace_size": (_sz, [_i64]),
     "tsb_kinetic_energy": (_int, [_vp, _vp, _vp, _i64, _i64, _int, _vp, _vp, _sz, _vp]),
     "tsb_nhc_half_step": (_int, [_vp, _vp, _vp, _i64, _i64, _int, _vp, _vp, _vp, _vp, _vp,

@@ -330,12 +330,14 @@ class FusedMD:
     """
 
     def __init__(self, state, model, *, integrator: str = "nvt_langevin", dt, kT=None,
-                 gamma=None, skin: float | str = 0.7, seed: int | None = None):
+                 gamma=None, skin: float | str = 0.7, seed: int | None = None, tau=None):
         from .models.pair_potential import PairTableModel
 
         if not isinstance(model, PairTableModel):
             raise TypeError("the fused path needs a tsb PairTableModel (LJ / Morse / soft sphere)")
-        self.integ = {"nve": L.INT_NVE, "nvt_langevin": L.INT_LANGEVIN}[integrator]
+        self.integ = {"nve": L.INT_NVE, "nvt_langevin": L.INT_LANGEVIN,
+                      "nvt_nose_hoover": L.INT_NOSE_HOOVER,
+                      "nvt_vrescale": L.INT_VRESCALE}[integrator]
         L.require_cuda(state.positions, "state.positions")
         if not bool(torch.as_tensor(state.pbc).all()):
             raise FusedMDError("the fused path requires periodic boundaries on all axes")
@@ -348,7 +350,26 @@ class FusedMD:
             raise FusedMDError(f"systems with {max_atoms} atoms exceed the fused-kernel "
                                f"limit of {self.lib.tsb_fused_max_atoms()}")
         self.dt_s = _per_system(dt, self.n_sys, dev)
-        if self.integ == L.INT_LANGEVIN:
+        if self.integ in (L.INT_NOSE_HOOVER, L.INT_VRESCALE):
+            if kT is None:
+                raise ValueError(f"kT is required for {integrator}")
+            _dof(state)  # every system needs >= 2 atoms (3N - 3 > 0)
+            self.kT_s = _per_system(kT, self.n_sys, dev)
+            self.g_s = None
+            if self.integ == L.INT_NOSE_HOOVER:
+                c = getattr(state, "chain", None)
+                if c is None:
+                    raise TypeError("nvt_nose_hoover needs a state from nvt_nose_hoover_init")
+                f64c = lambda t: t.to(torch.float64).contiguous().clone()  # noqa: E731
+                self.cxi, self.cpxi = f64c(c.positions), f64c(c.momenta)
+                self.cQ, self.cke = f64c(c.masses), f64c(c.kinetic_energy)
+                self.tau_s = f64c(c.tau)
+                self.cdt = f64c(state.chain_dt)
+                self.M, self.nc, self.nsy = c.positions.shape[1], state.chain_steps, state.sy_steps
+            else:
+                self.tau_s = _per_system(10.0 * self.dt_s if tau is None else tau,
+                                         self.n_sys, dev)
+        elif self.integ == L.INT_LANGEVIN:
             if kT is None:
                 raise ValueError("kT is required for nvt_langevin")
             self.kT_s = _per_system(kT, self.n_sys, dev)
@@ -392,27 +413,44 @@ class FusedMD:
 
     def launch(self, n_steps: int, stream: int | None = None) -> None:
         m = self.model
+        st = stream if stream is not None else L.stream_ptr(self.dev)
+        if self.integ in (L.INT_NOSE_HOOVER, L.INT_VRESCALE):
+            nh = self.integ == L.INT_NOSE_HOOVER
+            g = (lambda name: L.ptr(getattr(self, name)) if nh else None)  # noqa: E731
+            L.call("tsb_fused_md_nvt", self.integ, m.kind, L.ptr(self.table), m.n_species,
+                   L.ptr(self.species), L.ptr(self.x), L.ptr(self.p), L.ptr(self.f),
+                   L.ptr(self.m), L.ptr(self.cell_row), L.ptr(self.sys_idx), self.n, self.n_sys,
+                   L.ptr(self.order), m.cutoff, self.skin, int(n_steps), L.ptr(self.dt_s),
+                   L.ptr(self.kT_s), L.ptr(self.tau_s), g("cxi"), g("cpxi"), g("cQ"), g("cke"),
+                   g("cdt"), self.M if nh else 0, self.nc if nh else 0, self.nsy if nh else 0,
+                   self.seed, 0, L.ptr(self.counter_dev), L.ptr(self.energy),
+                   L.ptr(self.rebuilds), L.ptr(self.status), L.ptr(self.ws), self.ws.numel(),
+                   st)
+            return
         L.call("tsb_fused_md", self.integ, m.kind, L.ptr(self.table), m.n_species,
                L.ptr(self.species), L.ptr(self.x), L.ptr(self.p), L.ptr(self.f), L.ptr(self.m),
                L.ptr(self.cell_row), L.ptr(self.sys_idx), self.n, self.n_sys,
                L.ptr(self.order), m.cutoff, self.skin, int(n_steps), L.ptr(self.dt_s),
                L.ptr(self.kT_s), L.ptr(self.g_s), self.seed, 0, L.ptr(self.counter_dev),
                L.ptr(self.energy), L.ptr(self.rebuilds), L.ptr(self.status), L.ptr(self.ws),
-               self.ws.numel(), stream if stream is not None else L.stream_ptr(self.dev))
+               self.ws.numel(), st)
 
     def graph(self, n_steps: int) -> "torch.cuda.CUDAGraph":
         """CUDA graph of one ``launch(n_steps)``; ``g.replay()`` advances every system
         by n_steps with fresh Langevin noise (the device counter moves on)."""
         if n_steps not in self._graphs:
             torch.cuda.synchronize(self.dev)
-            saved = [t.clone() for t in (self.x, self.p, self.f, self.counter_dev)]
+            keep = [self.x, self.p, self.f, self.counter_dev]
+            if self.integ == L.INT_NOSE_HOOVER:
+                keep += [self.cxi, self.cpxi, self.cQ, self.cke]
+            saved = [t.clone() for t in keep]
             s = torch.cuda.Stream(self.dev)
             s.wait_stream(torch.cuda.current_stream(self.dev))
             with torch.cuda.stream(s):  # warm-up outside capture (sets kernel attributes)
                 self.launch(n_steps)
             torch.cuda.current_stream(self.dev).wait_stream(s)
             torch.cuda.synchronize(self.dev)
-            for t, v in zip((self.x, self.p, self.f, self.counter_dev), saved):
+            for t, v in zip(keep, saved):
                 t.copy_(v)
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g):
@@ -434,16 +472,23 @@ class FusedMD:
         s.positions, s.momenta, s.forces = cast(self.x), cast(self.p), cast(self.f)
         s.energy = cast(self.energy)
         s._philox_seed, s._philox_counter = self.seed, self.counter
+        if self.integ == L.INT_NOSE_HOOVER:
+            c = s.chain
+            c.positions, c.momenta = self.cxi.clone(), self.cpxi.clone()
+            c.masses, c.kinetic_energy = self.cQ.clone(), self.cke.clone()
         return s
 
 
 def run_md(state, model, n_steps: int, *, integrator: str = "nvt_langevin", dt, kT=None,
            gamma=None, skin: float | str = 0.7, seed: int | None = None, check: bool = True,
-           return_rebuilds: bool = False):
+           return_rebuilds: bool = False, tau=None):
     """Advance every system ``n_steps`` in ONE persistent kernel launch.
 
     Same update rules as ``nve_step`` / ``nvt_langevin_step`` (Langevin noise
-    from the Philox stream), with a device-side Verlet list (cutoff + skin)
+    from the Philox stream) / ``nvt_nose_hoover_step`` (state from
+    ``nvt_nose_hoover_init``; its chain is updated) / ``nvt_vrescale_step`` (``tau``,
+    default 10 dt; same Philox draws as the step function), with a device-side
+    Verlet list (cutoff + skin)
     rebuilt when any atom of a system moved more than skin/2.  ``model`` must be
     a :class:`tsb.models.PairTableModel` (LJ / Morse / soft sphere, any species
     table); all axes must be periodic and systems may have up to
@@ -451,7 +496,7 @@ def run_md(state, model, n_steps: int, *, integrator: str = "nvt_langevin", dt, 
     (positions, momenta, forces, energy).
     """
     r = FusedMD(state, model, integrator=integrator, dt=dt, kT=kT, gamma=gamma, skin=skin,
-                seed=seed)
+                seed=seed, tau=tau)
     r.launch(n_steps)
     if check:
         r.check()
