@@ -39,6 +39,8 @@ UNIT = "atom-steps/s"
 WORKLOAD = ("2048 Cu fcc systems (8-512 atoms, strain +-2%, shear +-3deg), Morse "
             "(D=0.3429 eV, alpha=1.3588/A, r0=2.866 A, rc=6.0 A), NVT-Langevin BAOAB "
             "1000 K, dt=2 fs, gamma=0.01/fs")
+INTEGRATOR_NAMES = {"nvt_nose_hoover": "NVT Nose-Hoover chain (3 x 3 x 3)",
+                    "nvt_vrescale": "NVT V-rescale (tau 10 dt)", "nve": "NVE velocity Verlet"}
 ALG_BYTES_PER_ATOM_STEP = 76  # streaming state r/w: 48 B FP64 pos + 24 B mom + 4 B type/mass
 # algorithmic compute per atom-step of the Morse workload (rho = 0.0850 / A^3, rc = 6 A):
 # 38.5 half-list pairs, ~45 FP32 flops and one exp per pair
@@ -71,6 +73,9 @@ def parse():
                     help="Verlet skin in A, or 'auto' (project autotuner, cached per workload)")
     ap.add_argument("--plain-steps", type=int, default=20,
                     help="MD steps of the plain per-call path timed beside the fused kernel")
+    ap.add_argument("--integrator", default="nvt_langevin",
+                    choices=["nvt_langevin", "nvt_nose_hoover", "nvt_vrescale", "nve"],
+                    help="batched_md: integrator inside the fused kernel and the plain path")
     ap.add_argument("--workload", default="batched_md",
                     choices=["batched_md", "single_large", "relax", "adjoint"])
     return ap.parse_args()
@@ -430,9 +435,13 @@ def main():
     n_atoms = md.n_atoms
     from tsb import workloads as W
 
-    runner = integrators.FusedMD(md, model, integrator="nvt_langevin",
-                                 dt=0.002 * W.METAL_TIME, kT=1000 * W.KB_EV,
-                                 gamma=10.0 / W.METAL_TIME,
+    dt_md, kT_md = 0.002 * W.METAL_TIME, 1000 * W.KB_EV
+    if args.integrator == "nvt_nose_hoover":
+        md = integrators.nvt_nose_hoover_init(md, model, kT=kT_md, dt=dt_md)
+    runner = integrators.FusedMD(md, model, integrator=args.integrator,
+                                 dt=dt_md, kT=kT_md if args.integrator != "nve" else None,
+                                 gamma=10.0 / W.METAL_TIME if args.integrator == "nvt_langevin"
+                                 else None,
                                  skin=args.skin if args.skin == "auto" else float(args.skin),
                                  seed=1234 + rank)
     stream = torch.cuda.current_stream(device)
@@ -515,15 +524,27 @@ def main():
     # step (cell list rebuilt, pair forces, BAOAB kernels, launched from Python)
     ps = md.clone()
     ps.momenta = runner.p.clone()
-    step_kw = dict(dt=0.002 * W.METAL_TIME, kT=1000 * W.KB_EV, gamma=10.0 / W.METAL_TIME)
+    if args.integrator == "nvt_langevin":
+        def plain_step(st):
+            return integrators.nvt_langevin_step(st, model, dt=dt_md, kT=kT_md,
+                                                 gamma=10.0 / W.METAL_TIME)
+    elif args.integrator == "nvt_nose_hoover":
+        def plain_step(st):
+            return integrators.nvt_nose_hoover_step(st, model, dt=dt_md, kT=kT_md)
+    elif args.integrator == "nvt_vrescale":
+        def plain_step(st):
+            return integrators.nvt_vrescale_step(model, st, dt=dt_md, kT=kT_md)
+    else:
+        def plain_step(st):
+            return integrators.nve_step(st, model, dt=dt_md)
     for _ in range(3):
-        ps = integrators.nvt_langevin_step(ps, model, **step_kw)
+        ps = plain_step(ps)
     pa, pb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     torch.cuda.synchronize(device)
     pa.record(stream)
     for _ in range(args.plain_steps):
-        ps = integrators.nvt_langevin_step(ps, model, **step_kw)
+        ps = plain_step(ps)
     pb.record(stream)
     torch.cuda.synchronize(device)
     t_plain = replicas.max_over_ranks(pa.elapsed_time(pb) / 1e3, device)
@@ -541,7 +562,9 @@ def main():
             "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded Cu supercells)",
-            "config": {"workload": WORKLOAD, "n_systems": args.n_systems,
+            "config": {"workload": WORKLOAD if args.integrator == "nvt_langevin" else
+                       WORKLOAD.replace("NVT-Langevin BAOAB", INTEGRATOR_NAMES[args.integrator]),
+                       "n_systems": args.n_systems,
                        "atoms_per_gpu": n_atoms, "md_steps_per_step": args.md_steps,
                        "verlet_skin_A": runner.skin,
                        "skin_source": "autotuner" if args.skin == "auto" else "argument", "precision": "FP32 pair math, FP64 state",
@@ -570,8 +593,9 @@ def main():
                     "d2h_bytes_per_step": d2h},
             "force_err_vs_fp64": force_err,
             "plain_path": {"value": plain_value, "unit": UNIT, "md_steps": args.plain_steps,
-                           "what": "tsb.integrators.nvt_langevin_step per MD step (cell "
-                                   "list + FP32 pair forces + BAOAB kernels each call)",
+                           "what": f"tsb.integrators step function ({args.integrator}) per MD "
+                                   "step (cell list + FP32 pair forces + integrator kernels "
+                                   "each call)",
                            "fused_over_plain": value / plain_value},
             "gpu_launches": 2 * args.steps,
             "clocks": clocks.summary(),

@@ -40,31 +40,38 @@ __device__ inline double sy_weight(int n, int k) {
   }
 }
 
-// One chain sub-step of length `delta` (chain masses q, positions x, momenta v,
-// M = chain length); returns the particle-momentum factor and updates ke.
-__device__ inline double nhc_substep(double delta, int M, const double *q, double *x, double *v,
-                              double &ke, double nf, double kt) {
+// One chain sub-step of length `delta` (chain masses q with reciprocals iq,
+// positions x, momenta v, M = chain length); returns the particle-momentum
+// factor and updates ke.  The forward pass reuses the backward pass's factors
+// exp(-delta/8 v_{j+1}/q_{j+1}): v_{j+1} does not change in between, so the
+// values are identical.  Divisions by q are multiplications by 1/q (one
+// thread runs these sub-steps serially).
+__device__ inline double nhc_substep(double delta, int M, const double *iq, double *x,
+                                     double *v, double &ke, double nf, double kt) {
   const double d2 = delta / 2.0, d4 = d2 / 2.0, d8 = d4 / 2.0;
   const int m = M - 1;
-  if (m > 0) v[m] += d4 * (v[m - 1] * v[m - 1] / q[m - 1] - kt);
+  double sj[kMaxChain];
+  if (m > 0) v[m] += d4 * (v[m - 1] * v[m - 1] * iq[m - 1] - kt);
   for (int j = m - 1; j > 0; --j) {
-    const double g = v[j - 1] * v[j - 1] / q[j - 1] - kt;
-    const double s = exp(-d8 * v[j + 1] / q[j + 1]);
+    const double g = v[j - 1] * v[j - 1] * iq[j - 1] - kt;
+    const double s = exp(-d8 * v[j + 1] * iq[j + 1]);
+    sj[j] = s;
     v[j] = s * (s * v[j] + d4 * g);
   }
   {
     const double g = 2.0 * ke - nf * kt;
-    const double s = m > 0 ? exp(-d8 * v[1] / q[1]) : 1.0;
+    const double s = m > 0 ? exp(-d8 * v[1] * iq[1]) : 1.0;
+    sj[0] = s;
     v[0] = s * (s * v[0] + d4 * g);
   }
-  const double scale = exp(-d2 * v[0] / q[0]);
+  const double scale = exp(-d2 * v[0] * iq[0]);
   ke = ke * (scale * scale);
-  for (int j = 0; j < M; ++j) x[j] = x[j] + d2 * v[j] / q[j];
+  for (int j = 0; j < M; ++j) x[j] = x[j] + d2 * v[j] * iq[j];
   double g = 2.0 * ke - nf * kt;
   for (int j = 0; j < m; ++j) {
-    const double s = exp(-d8 * v[j + 1] / q[j + 1]);
+    const double s = sj[j];
     v[j] = s * (s * v[j] + d4 * g);
-    g = v[j] * v[j] / q[j] - kt;
+    g = v[j] * v[j] * iq[j] - kt;
   }
   v[m] += d4 * g;
   return scale;
@@ -75,11 +82,13 @@ __device__ inline double nhc_substep(double delta, int M, const double *q, doubl
 // the momentum factors
 __device__ inline double nhc_half(double h, int M, int nc, int nsy, const double *q, double *x,
                                   double *v, double &ke, double nf, double kt) {
-  if (nc == 1 && nsy == 1) return nhc_substep(h, M, q, x, v, ke, nf, kt);
+  double iq[kMaxChain];
+  for (int j = 0; j < M; ++j) iq[j] = 1.0 / q[j];
+  if (nc == 1 && nsy == 1) return nhc_substep(h, M, iq, x, v, ke, nf, kt);
   double tot = 1.0;
   const double delta = h / nc;
   for (int sub = 0; sub < nc * nsy; ++sub)
-    tot *= nhc_substep(delta * sy_weight(nsy, sub % nsy), M, q, x, v, ke, nf, kt);
+    tot *= nhc_substep(delta * sy_weight(nsy, sub % nsy), M, iq, x, v, ke, nf, kt);
   return tot;
 }
 
