@@ -752,13 +752,16 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       const int sfull = nshell >> 2, srem = nshell & 3;                                      \
       if constexpr (kPaired) {                                                               \
         float2 f2x = make_float2(0.f, 0.f), f2y = f2x, f2z = f2x;                            \
+        /* the next group's list word loads one iteration ahead (in-bounds index) */         \
+        uint2 gn = s_list[tid];                                                              \
         for (int k4 = 0; k4 < full; ++k4) {                                                  \
-          const uint2 ge = s_list[k4 * kFusedThreads + tid];                                 \
+          const uint2 ge = gn;                                                               \
+          gn = s_list[min(k4 + 1, kListGroups - 1) * kFusedThreads + tid];                   \
           TSB_PAIR2(EXT(ge.x & 0xFFFFu), EXT(ge.x >> 16), 0, 0, false, WITH_E)           \
           TSB_PAIR2(EXT(ge.y & 0xFFFFu), EXT(ge.y >> 16), 0, 0, false, WITH_E)           \
         }                                                                                    \
         if (rem) {                                                                           \
-          const uint2 ge = s_list[full * kFusedThreads + tid];                               \
+          const uint2 ge = gn; /* group `full` */                                            \
           if (rem > 1) {                                                                     \
             TSB_PAIR2(EXT(ge.x & 0xFFFFu), EXT(ge.x >> 16), 0, 0, false, WITH_E)         \
             if (rem > 2) TSB_PAIR_CORE(EXT(ge.y & 0xFFFFu), WITH_E)                        \
@@ -767,15 +770,17 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
           }                                                                                  \
         }                                                                                    \
         /* shell entry k sits in slot kListLen - 1 - k */                                    \
+        uint2 gs = s_list[(kListGroups - 1) * kFusedThreads + tid];                          \
         for (int k4 = 0; k4 < sfull; ++k4) {                                                 \
-          const uint2 ge = s_list[(kListGroups - 1 - k4) * kFusedThreads + tid];             \
+          const uint2 ge = gs;                                                               \
+          gs = s_list[max(kListGroups - 2 - k4, 0) * kFusedThreads + tid];                   \
           TSB_PAIR2(EXT(ge.y >> 16), EXT(ge.y & 0xFFFFu), ge.y >> 16, ge.y & 0xFFFFu,    \
                     true, WITH_E)                                                            \
           TSB_PAIR2(EXT(ge.x >> 16), EXT(ge.x & 0xFFFFu), ge.x >> 16, ge.x & 0xFFFFu,    \
                     true, WITH_E)                                                            \
         }                                                                                    \
         if (srem) {                                                                          \
-          const uint2 ge = s_list[(kListGroups - 1 - sfull) * kFusedThreads + tid];          \
+          const uint2 ge = gs; /* group kListGroups - 1 - sfull */                           \
           if (srem > 1) {                                                                    \
             TSB_PAIR2(EXT(ge.y >> 16), EXT(ge.y & 0xFFFFu), ge.y >> 16, ge.y & 0xFFFFu,  \
                       true, WITH_E)                                                          \
