@@ -18,6 +18,9 @@
  *              LJ:    p0=sigma p1=epsilon
  *              MORSE: p0=sigma p1=epsilon p2=alpha
  *              SOFT:  p0=sigma p1=epsilon p2=alpha
+ *              PLIFE: p0=sigma p1=A p2=beta (particle life; the row of species pair
+ *                     (a, b) is the force of a's neighbour b on a, so tables may be
+ *                     asymmetric; no energy)
  *              rc = per-pair truncation radius, eshift subtracted inside rc.
  *   species    [n_atoms] int32 species index (NULL = all species 0)
  */
@@ -48,6 +51,7 @@ extern "C" {
 #define TSB_POT_LJ 0
 #define TSB_POT_MORSE 1
 #define TSB_POT_SOFT 2
+#define TSB_POT_PLIFE 3 /* particle life (force-defined): tsb_pair_forward only */
 
 #define TSB_NL_SELF_INTERACTION 1 /* also emit (i, i, 0) pairs                     */
 #define TSB_NL_HALF 2             /* emit each unordered pair once (half list)      */

@@ -137,3 +137,50 @@ def kob_andersen_table(sigma_aa=3.4, eps_aa=0.0104, trunc=2.5, shift=True):
             tab[a, b] = [sig[a, b], eps[a, b], 0.0, rc,
                          lj_shift(sig[a, b], eps[a, b], rc) if shift else 0.0]
     return tab
+
+
+def particle_life_force(r, A=1.0, beta=0.3, sigma=1.0):
+    """Particle-life force magnitude (torch_sim/models/particle_life.py:24-54):
+    r/beta - 1 for r < beta; A (1 - |2r - 1 - beta| / (1 - beta)) for beta <= r < sigma."""
+    r = np.asarray(r, dtype=np.float64)
+    inner = np.where(r < beta, r / beta - 1.0, 0.0)
+    outer = np.where((r >= beta) & (r < sigma),
+                     A * (1.0 - np.abs(2.0 * r - 1.0 - beta) / (1.0 - beta)), 0.0)
+    return inner + outer
+
+
+def pair_forces_forward(force_fn, positions, cell_row, pbc, system_idx, atomic_numbers, cutoff,
+                        *, half=False):
+    """PairForcesModel.forward (torch_sim/models/pair_potential.py:467-612): forces from
+    a scalar pair force f(r, zi, zj); F_i -= f r_hat, F_j += f r_hat per listed pair;
+    stress -1/V sum r (x) f_vec times 1 (half list) or 1/2 (full list); per-atom
+    stresses w = 1/2 or 1/4 of each pair virial on both endpoints; energy zero."""
+    positions = np.asarray(positions, dtype=np.float64)
+    system_idx = np.asarray(system_idx, dtype=np.int64)
+    z = np.asarray(atomic_numbers)
+    n = positions.shape[0]
+    n_sys = int(system_idx.max()) + 1
+    cell_row, pbc = onl.normalize_inputs(cell_row, pbc, n_sys)
+    mapping, sysm, shifts = onl.neighbor_list(positions, cell_row, pbc, cutoff, system_idx)
+    if half:
+        mapping, sysm, shifts = onl.full_to_half_list(mapping, sysm, shifts)
+    i, j = mapping
+    dr = positions[j] - positions[i] + np.einsum("pk,pkm->pm", shifts, cell_row[sysm])
+    r = np.linalg.norm(dr, axis=1)
+    f = np.where(r < cutoff, force_fn(r, z[i], z[j]), 0.0)
+    safe = np.where(r > 0, r, 1.0)
+    fv = (f / safe)[:, None] * dr
+    forces = np.zeros((n, 3))
+    np.add.at(forces, i, -fv)
+    np.add.at(forces, j, fv)
+    vol = np.abs(np.linalg.det(cell_row))
+    spp = np.einsum("pi,pj->pij", dr, fv)
+    stress = np.zeros((n_sys, 3, 3))
+    np.add.at(stress, sysm, -spp)
+    stress = stress / vol[:, None, None] * (1.0 if half else 0.5)
+    w = 0.5 if half else 0.25
+    sa = np.zeros((n, 3, 3))
+    np.add.at(sa, i, -w * spp)
+    np.add.at(sa, j, -w * spp)
+    return {"energy": np.zeros(n_sys), "forces": forces, "stress": stress,
+            "stresses": sa / vol[system_idx][:, None, None]}

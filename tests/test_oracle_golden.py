@@ -250,3 +250,22 @@ def test_vrescale_oracle_matches_reference(golden):
         np.testing.assert_allclose(st["positions"], g["positions"][k], rtol=1e-12, atol=1e-12)
         np.testing.assert_allclose(st["momenta"], g["momenta"][k], rtol=1e-9, atol=1e-12)
         np.testing.assert_allclose(st["energy"], g["energy"][k], rtol=1e-10)
+
+
+def _asym_force(r, zi, zj):
+    return (1.0 + zi - 0.5 * zj) * (1.1 - r)
+
+
+@pytest.mark.parametrize("case", ["plife", "asym"])
+def test_pair_forces_oracle_matches_reference(golden, case):
+    s, g = golden["pairforces"]["sys"], golden["pairforces"][case]
+    if case == "plife":
+        fn = lambda r, zi, zj: opair.particle_life_force(r, 1.0, 0.3, 1.0)  # noqa: E731
+        cutoff = 1.2
+    else:
+        fn, cutoff = _asym_force, 1.1
+    o = opair.pair_forces_forward(fn, s["positions"], np.transpose(s["cell"], (0, 2, 1)),
+                                  np.array([True] * 3), s["system_idx"].astype(np.int64),
+                                  s["atomic_numbers"].astype(np.float64), cutoff)
+    for k in ("energy", "forces", "stress", "stresses"):
+        np.testing.assert_allclose(o[k], g[k], rtol=1e-11, atol=1e-13)

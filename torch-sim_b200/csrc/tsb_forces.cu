@@ -47,17 +47,28 @@ __global__ void __launch_bounds__(128)
                      const R r2 = rx * rx + ry * ry + rz * rz;
                      R e, fr;
                      pair_eval<POT, R>(q, r2, e, fr);
+                     // force-defined pairs: i's thread sees both directed pairs
+                     // (i, j) and (j, i) of the reference's full list, so the force
+                     // adds f_ij and f_ji and the virial takes half of it
+                     // (pair_potential.py:567-600, stress scale 1/2 for a full list)
+                     double vw = 1.0;
+                     if constexpr (POT == TSB_POT_PLIFE) {
+                       R e2, fr2;
+                       pair_eval<POT, R>(prm[sj * ns_species + si], r2, e2, fr2);
+                       fr += fr2;
+                       vw = 0.5;
+                     }
                      const R gx = fr * rx, gy = fr * ry, gz = fr * rz;  // force on j
                      fx -= gx;
                      fy -= gy;
                      fz -= gz;
                      ei += (double)e;
-                     vxx += (double)(rx * gx);
-                     vyy += (double)(ry * gy);
-                     vzz += (double)(rz * gz);
-                     vyz += (double)(ry * gz);
-                     vxz += (double)(rx * gz);
-                     vxy += (double)(rx * gy);
+                     vxx += vw * (double)(rx * gx);
+                     vyy += vw * (double)(ry * gy);
+                     vzz += vw * (double)(rz * gz);
+                     vyz += vw * (double)(ry * gz);
+                     vxz += vw * (double)(rx * gz);
+                     vxy += vw * (double)(rx * gy);
                    });
   if (flags & TSB_OUT_FORCES) {
     forces[3 * i] = (P)fx;
@@ -204,8 +215,10 @@ static int pair_forward(int pot, const double *table, int nsp, const int32_t *sp
       TSB_LAUNCH(TSB_POT_LJ)
     } else if (pot == TSB_POT_MORSE) {
       TSB_LAUNCH(TSB_POT_MORSE)
-    } else {
+    } else if (pot == TSB_POT_SOFT) {
       TSB_LAUNCH(TSB_POT_SOFT)
+    } else {
+      TSB_LAUNCH(TSB_POT_PLIFE)
     }
 #undef TSB_LAUNCH
   }
@@ -237,7 +250,7 @@ extern "C" int tsb_pair_forward(int potential, const double *table, int n_specie
                                 void *energy, void *forces, void *stress, void *energies,
                                 void *stresses, const uint8_t *sys_active, void *workspace,
                                 size_t workspace_bytes, void *stream) {
-  if (potential < TSB_POT_LJ || potential > TSB_POT_SOFT) return TSB_ERR_INVALID_ARG;
+  if (potential < TSB_POT_LJ || potential > TSB_POT_PLIFE) return TSB_ERR_INVALID_ARG;
   if (n_species < 1 || n_species > kMaxSpecies || !table) return TSB_ERR_INVALID_ARG;
   if (n_species > 1 && !species) return TSB_ERR_INVALID_ARG;
   if (n_atoms < 0 || n_systems < 1 || !(cutoff > 0.0) || !cell_row || !pbc || !energy)

@@ -5,6 +5,7 @@
 //   LJ    (lennard_jones.py:23-47):  a0=sigma^2 a1=4eps a2=24eps
 //   MORSE (morse.py:23-47):          a0=sigma  a1=eps  a2=alpha a5=2*alpha*eps
 //   SOFT  (soft_sphere.py:35-59):    a0=sigma  a1=1/sigma a2=alpha a5=eps/alpha a6=eps/sigma
+//   PLIFE (particle_life.py:24-54):  a0=beta a1=A a5=1-beta a6=sigma a7=1+beta (force only)
 //   a3 = effective cutoff^2 = min(cutoff, rc)^2 (SOFT also min with sigma), a4 = eshift
 #pragma once
 
@@ -37,6 +38,13 @@ __device__ inline PairPrm<R> make_prm(int pot, const double *t, double cutoff) {
     q.a2 = (R)t[2];
     q.a5 = (R)(2.0 * t[2] * t[1]);
     q.a6 = (R)0;
+  } else if (pot == TSB_POT_PLIFE) {
+    q.a0 = (R)t[2];
+    q.a1 = (R)t[1];
+    q.a2 = (R)0;
+    q.a5 = (R)(1.0 - t[2]);
+    q.a6 = (R)t[0];
+    q.a7 = (R)(1.0 + t[2]);
   } else {
     rc = fmin(rc, t[0]);
     q.a0 = (R)t[0];
@@ -91,6 +99,14 @@ __device__ __forceinline__ void pair_eval(const PairPrm<R> &q, R r2, R &e, R &fr
       e = R(0) - q.a4;
       fr = R(0);
     }
+  } else if (POT == TSB_POT_PLIFE) {
+    // force-defined: magnitude f(r) = r/beta - 1 (r < beta), A (1 - |2r - 1 - beta| /
+    // (1 - beta)) (beta <= r < sigma); fr = f / r, no energy
+    const R r = sqrt(r2);
+    const R f = r < q.a0 ? r / q.a0 - R(1)
+                         : (r < q.a6 ? q.a1 * (R(1) - fabs(R(2) * r - q.a7) / q.a5) : R(0));
+    e = R(0);
+    fr = r > R(0) ? f / r : R(0);
   } else {  // SOFT: V = eps/alpha (1 - r/sigma)^alpha for r < sigma
     R r = (r2 > R(0)) ? r2 * rsqrt_r(r2) : R(0);
     R base = R(1) - r * q.a1;

@@ -25,7 +25,7 @@ TSB_ERR_UNSUPPORTED = 6
 TSB_ERR_WORKSPACE = 7
 
 F32, F64 = 0, 1
-POT_LJ, POT_MORSE, POT_SOFT = 0, 1, 2
+POT_LJ, POT_MORSE, POT_SOFT, POT_PLIFE = 0, 1, 2, 3
 NL_SELF_INTERACTION, NL_HALF = 1, 2
 OUT_FORCES, OUT_STRESS, OUT_ENERGIES, OUT_STRESSES, MATH_FP64 = 1, 2, 4, 8, 16
 INT_NVE, INT_LANGEVIN, INT_NOSE_HOOVER, INT_VRESCALE = 0, 1, 2, 3

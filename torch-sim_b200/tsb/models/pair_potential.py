@@ -25,7 +25,8 @@ import torch
 from .. import _lib as L
 from .interface import ModelInterface
 
-KIND = {"lj": L.POT_LJ, "morse": L.POT_MORSE, "soft_sphere": L.POT_SOFT}
+KIND = {"lj": L.POT_LJ, "morse": L.POT_MORSE, "soft_sphere": L.POT_SOFT,
+        "particle_life": L.POT_PLIFE}
 
 
 class PairTableModel(ModelInterface):
