@@ -323,6 +323,28 @@ int tsb_fused_md_nvt(int thermostat, int potential, const double *table, int n_s
                      int32_t *n_rebuilds, int32_t *status, void *workspace,
                      size_t workspace_bytes, void *stream);
 
+/* ---- fused persistent batched MD, every integrator, with trajectory frames ----
+ * Superset of tsb_fused_md and tsb_fused_md_nvt (integrator TSB_INT_NVE ..
+ * TSB_INT_VRESCALE; arguments a thermostat does not use may be NULL).  With
+ * report_every > 0, after every report_every-th step the kernel writes frame
+ * f = step / report_every - 1 (f < n_frames): positions as float32 into
+ * frame_x [n_frames, N, 3] and each system's potential energy into
+ * frame_e [n_frames, S] -- the device side of the reference's
+ * TrajectoryReporter (torch_sim/trajectory.py:267-340, coerce_to_float32). */
+int tsb_fused_md_ex(int integrator, int potential, const double *table, int n_species,
+                    const int32_t *species, double *positions, double *momenta,
+                    double *forces, const double *masses, const double *cell_row,
+                    const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
+                    const int32_t *order, double cutoff, double skin, int64_t n_steps,
+                    const double *dt_sys, const double *kT_sys, const double *gamma_sys,
+                    const double *tau_sys, double *chain_xi, double *chain_pxi,
+                    double *chain_Q, double *chain_ke, const double *chain_dt,
+                    int chain_length, int chain_steps, int sy_steps, uint64_t seed,
+                    uint64_t counter, uint64_t *counter_dev, float *frame_x, double *frame_e,
+                    int64_t report_every, int64_t n_frames, double *energy,
+                    int32_t *n_rebuilds, int32_t *status, void *workspace,
+                    size_t workspace_bytes, void *stream);
+
 /* ---- allocation-free fused MD -------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory -- hosts that own all device memory through their own pool and bar

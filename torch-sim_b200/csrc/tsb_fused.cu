@@ -90,6 +90,11 @@ struct FusedArgs {
   double *cxi, *cpxi, *cQ, *cke;  // chain positions, momenta, masses [S, M]; carried KE [S]
   const double *tau, *cdt;        // thermostat time constant [S]; chain time step [S]
   int M, nc, nsy;                 // chain length, chain steps, Suzuki-Yoshida steps
+  // trajectory frames (tsb_fused_md_ex): every rep_every steps, positions [N, 3]
+  // (FP32) into frame_x and the potential energy of each system into frame_e
+  float *frame_x;
+  double *frame_e;
+  int64_t rep_every, n_frames, n_atoms_total;
 };
 
 // per-system geometry, computed by thread 0 into shared memory
@@ -913,7 +918,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
         TSB_REBUILD()
         if (failed) break;
       }
-      if (step + 1 == A.n_steps) {
+      const bool report = A.rep_every > 0 && (step + 1) % A.rep_every == 0 &&
+                          (step + 1) / A.rep_every <= A.n_frames;
+      if (step + 1 == A.n_steps || report) {
         TSB_FORCES(true)
       } else {
         TSB_FORCES(false)
@@ -936,6 +943,20 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
         px *= sc;
         py *= sc;
         pz *= sc;
+      }
+      if (report) {
+        // frame f: FP32 positions (as the reference's trajectories store them by
+        // default) and the system's potential energy at this step
+        const int64_t f = (step + 1) / A.rep_every - 1;
+        if (lead) {
+          float *o = A.frame_x + 3 * (f * A.n_atoms_total + gi);
+          o[0] = (float)x0;
+          o[1] = (float)x1;
+          o[2] = (float)x2;
+        }
+        const double e_sys = block_sum_to0(lead ? 0.5 * (double)ei : 0.0, s_red);
+        if (tid == 0) A.frame_e[f * A.n_sys + s] = e_sys;
+        __syncthreads();
       }
     }
     if (failed) continue;
@@ -1124,6 +1145,78 @@ extern "C" int tsb_fused_md_nvt(int thermostat, int potential, const double *tab
               kT_sys, nullptr, seed, counter, counter_dev, energy, n_rebuilds, queue,
               status, chain_xi, chain_pxi, chain_Q, chain_ke, tau_sys, chain_dt,
               chain_length, chain_steps, sy_steps};
+  const bool multi = n_species > 1;
+  if (potential == TSB_POT_LJ) {
+    multi ? launch_fused<TSB_POT_LJ, true>(A, grid, st) : launch_fused<TSB_POT_LJ, false>(A, grid, st);
+  } else if (potential == TSB_POT_MORSE) {
+    multi ? launch_fused<TSB_POT_MORSE, true>(A, grid, st)
+          : launch_fused<TSB_POT_MORSE, false>(A, grid, st);
+  } else {
+    multi ? launch_fused<TSB_POT_SOFT, true>(A, grid, st)
+          : launch_fused<TSB_POT_SOFT, false>(A, grid, st);
+  }
+  if (counter_dev) k_advance_counter<<<1, 32, 0, st>>>(counter_dev, n_steps);
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
+
+extern "C" int tsb_fused_md_ex(int integrator, int potential, const double *table,
+                               int n_species, const int32_t *species, double *positions,
+                               double *momenta, double *forces, const double *masses,
+                               const double *cell_row, const int64_t *system_idx,
+                               int64_t n_atoms, int64_t n_systems, const int32_t *order,
+                               double cutoff, double skin, int64_t n_steps,
+                               const double *dt_sys, const double *kT_sys,
+                               const double *gamma_sys, const double *tau_sys,
+                               double *chain_xi, double *chain_pxi, double *chain_Q,
+                               double *chain_ke, const double *chain_dt, int chain_length,
+                               int chain_steps, int sy_steps, uint64_t seed, uint64_t counter,
+                               uint64_t *counter_dev, float *frame_x, double *frame_e,
+                               int64_t report_every, int64_t n_frames, double *energy,
+                               int32_t *n_rebuilds, int32_t *status, void *workspace,
+                               size_t workspace_bytes, void *stream) {
+  if (integrator < TSB_INT_NVE || integrator > TSB_INT_VRESCALE) return TSB_ERR_INVALID_ARG;
+  if (potential < TSB_POT_LJ || potential > TSB_POT_SOFT) return TSB_ERR_INVALID_ARG;
+  if (n_species < 1 || !table || (n_species > 1 && !species)) return TSB_ERR_INVALID_ARG;
+  if (n_species > kFusedMaxSpecies) return TSB_ERR_UNSUPPORTED;
+  if (n_atoms < 1 || n_systems < 1 || !(cutoff > 0.0) || !(skin >= 0.0) || n_steps < 0)
+    return TSB_ERR_INVALID_ARG;
+  if (!positions || !momenta || !forces || !masses || !cell_row || !system_idx || !dt_sys ||
+      !energy || !status)
+    return TSB_ERR_INVALID_ARG;
+  if (integrator == TSB_INT_LANGEVIN && (!kT_sys || !gamma_sys)) return TSB_ERR_INVALID_ARG;
+  if (integrator >= TSB_INT_NOSE_HOOVER && (!kT_sys || !tau_sys)) return TSB_ERR_INVALID_ARG;
+  if (integrator == TSB_INT_NOSE_HOOVER) {
+    if (!chain_xi || !chain_pxi || !chain_Q || !chain_ke || !chain_dt) return TSB_ERR_INVALID_ARG;
+    if (chain_length < 1 || chain_length > kMaxChain || chain_steps < 1) return TSB_ERR_INVALID_ARG;
+    if (sy_steps != 1 && sy_steps != 3 && sy_steps != 5 && sy_steps != 7)
+      return TSB_ERR_INVALID_ARG;
+  }
+  if (report_every < 0 || n_frames < 0) return TSB_ERR_INVALID_ARG;
+  if (report_every > 0 && n_frames > 0 && (!frame_x || !frame_e)) return TSB_ERR_INVALID_ARG;
+  Carver c(workspace, workspace_bytes);
+  int64_t *lo = c.take<int64_t>(n_systems);
+  int64_t *hi = c.take<int64_t>(n_systems);
+  int32_t *queue = c.take<int32_t>(4);
+  if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  int dev = 0, n_sm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  int64_t grid = n_sm;
+  if (grid > kMaxGrid) grid = kMaxGrid;
+  if (grid > n_systems) grid = n_systems;
+  cudaMemsetAsync(lo, 0, sizeof(int64_t) * n_systems, st);
+  cudaMemsetAsync(hi, 0, sizeof(int64_t) * n_systems, st);
+  cudaMemsetAsync(queue, 0, sizeof(int32_t) * 4, st);
+  cudaMemsetAsync(status, 0, sizeof(int32_t) * 4, st);
+  k_bounds_fused<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, lo, hi);
+  FusedArgs A{integrator, potential, n_species, table, species, positions, momenta, forces,
+              masses, cell_row, lo, hi, n_systems, order, cutoff, skin, n_steps, dt_sys,
+              kT_sys, gamma_sys, seed, counter, counter_dev, energy, n_rebuilds, queue,
+              status, chain_xi, chain_pxi, chain_Q, chain_ke, tau_sys, chain_dt,
+              chain_length, chain_steps, sy_steps, frame_x, frame_e,
+              report_every > 0 && n_frames > 0 ? report_every : 0, n_frames, n_atoms};
   const bool multi = n_species > 1;
   if (potential == TSB_POT_LJ) {
     multi ? launch_fused<TSB_POT_LJ, true>(A, grid, st) : launch_fused<TSB_POT_LJ, false>(A, grid, st);

@@ -411,9 +411,28 @@ class FusedMD:
     def counter(self) -> int:
         return int(self.counter_dev.item())
 
-    def launch(self, n_steps: int, stream: int | None = None) -> None:
+    def launch(self, n_steps: int, stream: int | None = None, frames=None) -> None:
+        """Advance every system by n_steps in one persistent launch.  ``frames`` =
+        (frame_x float32 [F, N, 3], frame_e float64 [F, S], report_every) makes the
+        kernel write positions and potential energies every report_every steps
+        (F frames at most)."""
         m = self.model
         st = stream if stream is not None else L.stream_ptr(self.dev)
+        if frames is not None:
+            fx, fe, every = frames
+            nh = self.integ == L.INT_NOSE_HOOVER
+            g = (lambda name: L.ptr(getattr(self, name, None)) if nh else None)  # noqa: E731
+            L.call("tsb_fused_md_ex", self.integ, m.kind, L.ptr(self.table), m.n_species,
+                   L.ptr(self.species), L.ptr(self.x), L.ptr(self.p), L.ptr(self.f),
+                   L.ptr(self.m), L.ptr(self.cell_row), L.ptr(self.sys_idx), self.n, self.n_sys,
+                   L.ptr(self.order), m.cutoff, self.skin, int(n_steps), L.ptr(self.dt_s),
+                   L.ptr(self.kT_s), L.ptr(self.g_s), L.ptr(getattr(self, "tau_s", None)),
+                   g("cxi"), g("cpxi"), g("cQ"), g("cke"), g("cdt"),
+                   self.M if nh else 0, self.nc if nh else 0, self.nsy if nh else 0,
+                   self.seed, 0, L.ptr(self.counter_dev), L.ptr(fx), L.ptr(fe), int(every),
+                   int(fx.shape[0]), L.ptr(self.energy), L.ptr(self.rebuilds),
+                   L.ptr(self.status), L.ptr(self.ws), self.ws.numel(), st)
+            return
         if self.integ in (L.INT_NOSE_HOOVER, L.INT_VRESCALE):
             nh = self.integ == L.INT_NOSE_HOOVER
             g = (lambda name: L.ptr(getattr(self, name)) if nh else None)  # noqa: E731
