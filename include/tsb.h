@@ -263,6 +263,40 @@ int tsb_vrescale(void *momenta, const void *masses, const int64_t *system_idx,
                  uint64_t seed, uint64_t counter, double *lam, void *workspace,
                  size_t workspace_bytes, void *stream);
 
+/* ---- isotropic NPT Langevin (strain-based GJF) ----------------------------
+ * npt_langevin_isotropic_step (torch_sim/integrators/npt.py:988-1107), split
+ * around the force/stress call.  Atom arrays (positions, momenta, forces,
+ * masses) and stress [S,3,3] / cell [S,3,3] have dtype `dtype`; per-system
+ * scalars are float64 [S]: eps (strain, in/out), eps_dot (strain velocity),
+ * cell_masses (Q = (N + 1) kT b_tau^2, written by _pre), f_eps (strain force
+ * before the step, written by _pre, read by _post), alpha / cell_alpha (particle /
+ * cell friction), b_tau, kT, p_ext, dt.  reference_cell [S,3,3] float64; _pre
+ * writes cell = exp(eps) reference_cell.  Noise: cell_noise [S] and
+ * particle_noise [N,3] standard normals, or NULL to draw them from Philox4x32-10
+ * keyed by (seed, system/atom, counter); _pre and _post must see the same noise
+ * (same arrays or the same seed and counter). */
+size_t tsb_npt_workspace_size(int64_t n_systems);
+int tsb_npt_langevin_iso_pre(void *positions, const void *momenta, const void *forces,
+                             const void *masses, const int64_t *system_idx, int64_t n_atoms,
+                             int64_t n_systems, int dtype, const void *stress,
+                             const double *reference_cell, void *cell, double *eps,
+                             const double *eps_dot, double *cell_masses, double *f_eps,
+                             const double *alpha, const double *cell_alpha,
+                             const double *b_tau, const double *kT, const double *p_ext,
+                             const double *dt, const double *cell_noise,
+                             const double *particle_noise, uint64_t seed, uint64_t counter,
+                             void *workspace, size_t workspace_bytes, void *stream);
+int tsb_npt_langevin_iso_post(void *momenta, const void *masses, const void *forces_old,
+                              const void *forces, const int64_t *system_idx, int64_t n_atoms,
+                              int64_t n_systems, int dtype, const void *stress,
+                              const double *reference_cell, const double *eps,
+                              double *eps_dot, const double *cell_masses,
+                              const double *f_eps, const double *alpha,
+                              const double *cell_alpha, const double *kT,
+                              const double *p_ext, const double *dt, const double *cell_noise,
+                              const double *particle_noise, uint64_t seed, uint64_t counter,
+                              void *workspace, size_t workspace_bytes, void *stream);
+
 /* ---- fused persistent batched MD ----------------------------------------
  * Advances every system by n_steps of velocity Verlet (TSB_INT_NVE,
  * nve.py:74-130) or BAOAB Langevin (TSB_INT_LANGEVIN, nvt.py:144-240) in one

@@ -1,0 +1,68 @@
+"""Isotropic NPT Langevin oracle (TEST INFRASTRUCTURE ONLY; never the product path).
+
+FP64 numpy restatement of the reference's strain-based isotropic NPT Langevin
+step (Gronbech-Jensen & Farago GJF scheme), noise passed in:
+
+* ``cell_force``          <- torch_sim/integrators/npt.py:704-749
+                             F_eps = 3 V (P_avg - P_ext), P_avg = -tr(sigma)/3 + N kT / V
+* ``npt_langevin_isotropic_step`` <- npt.py:988-1107 with the helpers
+  ``_npt_langevin_isotropic_cell_position_step`` (:769-798),
+  ``_npt_langevin_isotropic_position_step`` (:838-885),
+  ``_npt_langevin_isotropic_cell_velocity_step`` (:801-835),
+  ``_npt_langevin_particle_velocity_step`` (:316-367),
+  cell = exp(eps) reference_cell, V = det(reference_cell) exp(3 eps) (:690-703)
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+
+def cell_force(stress, vol, n_atoms, kT, p_ext):
+    p_avg = -np.einsum("sii->s", stress) / 3.0 + n_atoms * kT / vol
+    return 3.0 * vol * (p_avg - p_ext)
+
+
+def npt_langevin_isotropic_step(st, force_fn, dt, kT, p_ext, cell_noise, particle_noise,
+                                system_idx):
+    """st: dict positions, momenta, masses, forces, stress, cell_positions (eps),
+    cell_velocities, alpha, cell_alpha, b_tau, reference_cell.  force_fn(q, cell)
+    -> (energy, forces, stress)."""
+    st = dict(st)
+    n_sys = len(st["cell_positions"])
+    n_at = np.bincount(system_idx, minlength=n_sys).astype(np.float64)
+    q_mass = (n_at + 1) * kT * st["b_tau"] ** 2
+    v0 = np.linalg.det(st["reference_cell"])
+    eps_old = st["cell_positions"].copy()
+    vol = v0 * np.exp(3 * eps_old)
+    f_n = cell_force(st["stress"], vol, n_at, kT, p_ext)
+    beta_c = np.sqrt(2.0 * st["cell_alpha"] * kT * dt) * cell_noise
+    a_at = st["alpha"][system_idx]
+    beta_p = np.sqrt(2 * a_at * kT * dt)[:, None] * particle_noise
+    # strain position step
+    q2 = 2 * q_mass
+    cb = 1 / (1 + st["cell_alpha"] * dt / q2)
+    eps = eps_old + cb * dt * st["cell_velocities"] + cb * dt * dt * f_n / q2 + cb * dt * beta_c / q2
+    cell = np.exp(eps)[:, None, None] * st["reference_cell"]
+    # particle position step with box scaling
+    m = st["masses"]
+    scale = np.exp(eps - eps_old)[system_idx]
+    b = 1 / (1 + a_at * dt / (2 * m))
+    vel = st["momenta"] / m[:, None]
+    c3 = vel + dt * st["forces"] / (2 * m[:, None]) + beta_p / (2 * m[:, None])
+    q = scale[:, None] * st["positions"] + ((2 * scale / (scale + 1)) * b * dt)[:, None] * c3
+    forces_old = st["forces"]
+    e, f, s = force_fn(q, cell)
+    vol = v0 * np.exp(3 * eps)
+    f_new = cell_force(s, vol, n_at, kT, p_ext)
+    qm = q_mass
+    ac = (1 - st["cell_alpha"] * dt / (2 * qm)) / (1 + st["cell_alpha"] * dt / (2 * qm))
+    bc = 1 / (1 + st["cell_alpha"] * dt / (2 * qm))
+    eps_dot = ac * st["cell_velocities"] + dt * (ac * f_n + f_new) / (2 * qm) + bc * beta_c / qm
+    m2 = 2 * m
+    ap = ((1 - a_at * dt / m2) / (1 + a_at * dt / m2))[:, None]
+    bp = (1 / (1 + a_at * dt / m2))[:, None]
+    v_new = ap * vel + dt * (ap * forces_old + f) / m2[:, None] + bp * beta_p / m[:, None]
+    st.update(positions=q, momenta=v_new * m[:, None], forces=f, energy=e, stress=s, cell=cell,
+              cell_positions=eps, cell_velocities=eps_dot, cell_masses=q_mass)
+    return st

@@ -269,3 +269,31 @@ def test_pair_forces_oracle_matches_reference(golden, case):
                                   s["atomic_numbers"].astype(np.float64), cutoff)
     for k in ("energy", "forces", "stress", "stresses"):
         np.testing.assert_allclose(o[k], g[k], rtol=1e-11, atol=1e-13)
+
+
+def test_npt_langevin_isotropic_oracle_matches_reference(golden):
+    from oracle import npt as onpt
+
+    s, g = golden["npt"]["sys"], golden["npt"]["npt"]
+    sysi = s["system_idx"].astype(np.int64)
+    tab = opair.single_table(opair.MORSE, 2.866, 0.3429, 1.3588)
+
+    def fn(q, cell_col):
+        o = opair.pair_forward(opair.MORSE, tab, np.zeros(len(q), int), q,
+                               np.transpose(cell_col, (0, 2, 1)), np.array([True] * 3), sysi,
+                               6.0)
+        return o["energy"], o["forces"], o["stress"]
+
+    dt, kT, p_ext = float(g["dt"]), float(g["kT"]), float(g["p_ext"])
+    st = {"positions": g["positions"][0], "momenta": g["momenta"][0], "masses": s["masses"],
+          "forces": g["forces"][0], "stress": g["stress"][0],
+          "cell_positions": g["cell_positions"][0], "cell_velocities": g["cell_velocities"][0],
+          "alpha": g["alpha"], "cell_alpha": g["cell_alpha"], "b_tau": g["b_tau"],
+          "reference_cell": g["reference_cell"]}
+    for k in range(1, g["positions"].shape[0]):
+        st = onpt.npt_langevin_isotropic_step(st, fn, dt, kT, p_ext, g["cell_noise"][k - 1],
+                                              g["particle_noise"][k - 1], sysi)
+        for key, rt in (("positions", 1e-12), ("momenta", 1e-9), ("cell", 1e-12),
+                        ("cell_positions", 1e-9), ("cell_velocities", 1e-9),
+                        ("cell_masses", 1e-14), ("stress", 1e-9)):
+            np.testing.assert_allclose(st[key], g[key][k], rtol=rt, atol=1e-14, err_msg=key)

@@ -1,0 +1,248 @@
+// Isotropic NPT Langevin step (torch_sim/integrators/npt.py:653-1107): the cell
+// degree of freedom is the logarithmic strain eps = ln(V/V0)/3, integrated with
+// particle and strain positions/velocities by the Gronbech-Jensen-Farago
+// Langevin scheme.  The step is split around the force call:
+//
+//   pre:  per system, strain force F_eps = 3 V (P_avg - P_ext) with
+//         P_avg = -tr(stress)/3 + N kT / V (npt.py:704-749), barostat mass
+//         Q = (N + 1) kT b_tau^2, strain position step (:769-798), new cell
+//         exp(eps) h0 (:690-697); per atom, the GJF position step with the box
+//         scaled by exp(eps_new - eps_old) (:838-885)
+//   post: per system, the strain velocity step with the new strain force
+//         (:801-835); per atom, the GJF velocity step (:316-367)
+//
+// The same noise realisation enters both halves: it is read from the caller's
+// arrays, or drawn twice from the same counter-based Philox4x32-10 streams
+// (particle: key seed, counter (atom, step); strain: (system, step)).
+#include <math.h>
+
+#include "tsb_common.cuh"
+#include "tsb_rng.cuh"
+#include "tsb_thermostat.cuh"
+
+namespace tsb {
+
+struct NptWork {
+  int64_t *lo, *hi;  // [S] atom range of each system
+  double *scale;     // [S] exp(eps_new - eps_old)
+};
+
+static void carve_npt(Carver &c, NptWork &w, int64_t ns) {
+  w.lo = c.take<int64_t>(ns);
+  w.hi = c.take<int64_t>(ns);
+  w.scale = c.take<double>(ns);
+}
+
+__global__ void k_npt_bounds(const int64_t *sys, int64_t n, int64_t *lo, int64_t *hi) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t s = sys[i];
+  if (i == 0 || sys[i - 1] != s) lo[s] = i;
+  if (i == n - 1 || sys[i + 1] != s) hi[s] = i + 1;
+}
+
+__device__ inline double det3(const double *a) {
+  return a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+         a[2] * (a[3] * a[7] - a[4] * a[6]);
+}
+
+template <class P>
+__device__ inline double strain_force(const P *stress, double vol, double n_at, double kt,
+                                      double p_ext) {
+  const double tr = (double)stress[0] + (double)stress[4] + (double)stress[8];
+  const double p_avg = -tr / 3.0 + n_at * kt / vol;
+  return 3.0 * vol * (p_avg - p_ext);
+}
+
+__device__ inline double cell_noise_of(const double *cell_noise, uint64_t seed, int64_t s,
+                                       uint64_t counter) {
+  return cell_noise ? cell_noise[s] : thermo_normal(seed, s, counter, 2u);
+}
+
+__device__ inline void particle_noise_of(const double *pn, uint64_t seed, int64_t i,
+                                         uint64_t counter, double *z) {
+  if (pn) {
+    z[0] = pn[3 * i];
+    z[1] = pn[3 * i + 1];
+    z[2] = pn[3 * i + 2];
+  } else {
+    normal4(seed, (uint64_t)i, counter, z);
+  }
+}
+
+template <class P>
+__global__ void k_npt_cell_pre(int64_t ns, const int64_t *lo, const int64_t *hi,
+                               const P *stress, const double *ref_cell, P *cell, double *eps,
+                               const double *eps_dot, double *Q, double *f_eps, double *scale,
+                               const double *cell_alpha, const double *b_tau, const double *kT,
+                               const double *p_ext, const double *dt, const double *cell_noise,
+                               uint64_t seed, uint64_t counter) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  const double n_at = (double)(hi[s] - lo[s]), kt = kT[s], h = dt[s], ac = cell_alpha[s];
+  const double q = (n_at + 1.0) * kt * (b_tau[s] * b_tau[s]);
+  const double v0 = det3(ref_cell + 9 * s);
+  const double e0 = eps[s];
+  const double f = strain_force(stress + 9 * s, v0 * exp(3.0 * e0), n_at, kt, p_ext[s]);
+  const double beta = sqrt(2.0 * ac * kt * h) * cell_noise_of(cell_noise, seed, s, counter);
+  const double q2 = 2.0 * q;
+  const double cb = 1.0 / (1.0 + (ac * h) / q2);
+  const double e1 = e0 + cb * h * eps_dot[s] + cb * h * h * f / q2 + cb * h * beta / q2;
+  Q[s] = q;
+  f_eps[s] = f;
+  eps[s] = e1;
+  scale[s] = exp(e1 - e0);
+  const double g = exp(e1);
+  for (int k = 0; k < 9; ++k) cell[9 * s + k] = (P)(g * ref_cell[9 * s + k]);
+}
+
+template <class P>
+__global__ void k_npt_atom_pre(int64_t n, P *x, const P *p, const P *f, const P *m,
+                               const int64_t *sys, const double *scale, const double *alpha,
+                               const double *kT, const double *dt, const double *pn,
+                               uint64_t seed, uint64_t counter) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t s = sys[i];
+  double z[4];
+  particle_noise_of(pn, seed, i, counter, z);
+  const double a = alpha[s], h = dt[s], mi = m[i], sc = scale[s];
+  const double pre = sqrt(2.0 * a * kT[s] * h);
+  const double b = 1.0 / (1.0 + (a * h) / (2.0 * mi));
+  const double c2 = (2.0 * sc / (sc + 1.0)) * b * h;
+  for (int c = 0; c < 3; ++c) {
+    const double c3 = (double)p[3 * i + c] / mi + h * (double)f[3 * i + c] / (2.0 * mi) +
+                      pre * z[c] / (2.0 * mi);
+    x[3 * i + c] = (P)(sc * (double)x[3 * i + c] + c2 * c3);
+  }
+}
+
+template <class P>
+__global__ void k_npt_cell_post(int64_t ns, const int64_t *lo, const int64_t *hi,
+                                const P *stress, const double *ref_cell, const double *eps,
+                                double *eps_dot, const double *Q, const double *f_eps,
+                                const double *cell_alpha, const double *kT,
+                                const double *p_ext, const double *dt, const double *cell_noise,
+                                uint64_t seed, uint64_t counter) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  const double n_at = (double)(hi[s] - lo[s]), kt = kT[s], h = dt[s], ac = cell_alpha[s];
+  const double q = Q[s];
+  const double v = det3(ref_cell + 9 * s) * exp(3.0 * eps[s]);
+  const double f1 = strain_force(stress + 9 * s, v, n_at, kt, p_ext[s]);
+  const double beta = sqrt(2.0 * ac * kt * h) * cell_noise_of(cell_noise, seed, s, counter);
+  const double a = (1.0 - (ac * h) / (2.0 * q)) / (1.0 + (ac * h) / (2.0 * q));
+  const double b = 1.0 / (1.0 + (ac * h) / (2.0 * q));
+  eps_dot[s] = a * eps_dot[s] + h * ((a * f_eps[s]) + f1) / (2.0 * q) + b * beta / q;
+}
+
+template <class P>
+__global__ void k_npt_atom_post(int64_t n, P *p, const P *m, const P *f_old, const P *f_new,
+                                const int64_t *sys, const double *alpha, const double *kT,
+                                const double *dt, const double *pn, uint64_t seed,
+                                uint64_t counter) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t s = sys[i];
+  double z[4];
+  particle_noise_of(pn, seed, i, counter, z);
+  const double al = alpha[s], h = dt[s], mi = m[i];
+  const double pre = sqrt(2.0 * al * kT[s] * h);
+  const double m2 = 2.0 * mi;
+  const double a = (1.0 - (al * h) / m2) / (1.0 + (al * h) / m2);
+  const double b = 1.0 / (1.0 + (al * h) / m2);
+  for (int c = 0; c < 3; ++c) {
+    const double v = (double)p[3 * i + c] / mi;
+    const double vn = a * v + h * ((a * (double)f_old[3 * i + c]) + (double)f_new[3 * i + c]) / m2 +
+                      b * (pre * z[c]) / mi;
+    p[3 * i + c] = (P)(vn * mi);
+  }
+}
+
+}  // namespace tsb
+
+using namespace tsb;
+
+extern "C" size_t tsb_npt_workspace_size(int64_t n_systems) {
+  Carver c(nullptr, (size_t)-1);
+  NptWork w;
+  carve_npt(c, w, n_systems);
+  return c.off + 256;
+}
+
+extern "C" int tsb_npt_langevin_iso_pre(
+    void *positions, const void *momenta, const void *forces, const void *masses,
+    const int64_t *system_idx, int64_t n_atoms, int64_t n_systems, int dtype,
+    const void *stress, const double *reference_cell, void *cell, double *eps,
+    const double *eps_dot, double *cell_masses, double *f_eps, const double *alpha,
+    const double *cell_alpha, const double *b_tau, const double *kT, const double *p_ext,
+    const double *dt, const double *cell_noise, const double *particle_noise, uint64_t seed,
+    uint64_t counter, void *workspace, size_t workspace_bytes, void *stream) {
+  if (n_atoms < 1 || n_systems < 1 || !positions || !momenta || !forces || !masses ||
+      !system_idx || !stress || !reference_cell || !cell || !eps || !eps_dot || !cell_masses ||
+      !f_eps || !alpha || !cell_alpha || !b_tau || !kT || !p_ext || !dt)
+    return TSB_ERR_INVALID_ARG;
+  if (dtype != TSB_F32 && dtype != TSB_F64) return TSB_ERR_INVALID_ARG;
+  Carver c(workspace, workspace_bytes);
+  NptWork w;
+  carve_npt(c, w, n_systems);
+  if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaMemsetAsync(w.lo, 0, sizeof(int64_t) * n_systems, st);
+  cudaMemsetAsync(w.hi, 0, sizeof(int64_t) * n_systems, st);
+  k_npt_bounds<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, w.lo, w.hi);
+#define TSB_NPT_PRE(P)                                                                        \
+  k_npt_cell_pre<P><<<grid_for(n_systems), kBlock, 0, st>>>(                                 \
+      n_systems, w.lo, w.hi, (const P *)stress, reference_cell, (P *)cell, eps, eps_dot,      \
+      cell_masses, f_eps, w.scale, cell_alpha, b_tau, kT, p_ext, dt, cell_noise, seed,         \
+      counter);                                                                              \
+  k_npt_atom_pre<P><<<grid_for(n_atoms), kBlock, 0, st>>>(                                   \
+      n_atoms, (P *)positions, (const P *)momenta, (const P *)forces, (const P *)masses,     \
+      system_idx, w.scale, alpha, kT, dt, particle_noise, seed, counter);
+  if (dtype == TSB_F64) {
+    TSB_NPT_PRE(double)
+  } else {
+    TSB_NPT_PRE(float)
+  }
+#undef TSB_NPT_PRE
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
+
+extern "C" int tsb_npt_langevin_iso_post(
+    void *momenta, const void *masses, const void *forces_old, const void *forces,
+    const int64_t *system_idx, int64_t n_atoms, int64_t n_systems, int dtype,
+    const void *stress, const double *reference_cell, const double *eps, double *eps_dot,
+    const double *cell_masses, const double *f_eps, const double *alpha,
+    const double *cell_alpha, const double *kT, const double *p_ext, const double *dt,
+    const double *cell_noise, const double *particle_noise, uint64_t seed, uint64_t counter,
+    void *workspace, size_t workspace_bytes, void *stream) {
+  if (n_atoms < 1 || n_systems < 1 || !momenta || !masses || !forces_old || !forces ||
+      !system_idx || !stress || !reference_cell || !eps || !eps_dot || !cell_masses ||
+      !f_eps || !alpha || !cell_alpha || !kT || !p_ext || !dt)
+    return TSB_ERR_INVALID_ARG;
+  if (dtype != TSB_F32 && dtype != TSB_F64) return TSB_ERR_INVALID_ARG;
+  Carver c(workspace, workspace_bytes);
+  NptWork w;
+  carve_npt(c, w, n_systems);
+  if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaMemsetAsync(w.lo, 0, sizeof(int64_t) * n_systems, st);
+  cudaMemsetAsync(w.hi, 0, sizeof(int64_t) * n_systems, st);
+  k_npt_bounds<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, w.lo, w.hi);
+#define TSB_NPT_POST(P)                                                                       \
+  k_npt_cell_post<P><<<grid_for(n_systems), kBlock, 0, st>>>(                                \
+      n_systems, w.lo, w.hi, (const P *)stress, reference_cell, eps, eps_dot, cell_masses,    \
+      f_eps, cell_alpha, kT, p_ext, dt, cell_noise, seed, counter);                          \
+  k_npt_atom_post<P><<<grid_for(n_atoms), kBlock, 0, st>>>(                                  \
+      n_atoms, (P *)momenta, (const P *)masses, (const P *)forces_old, (const P *)forces,    \
+      system_idx, alpha, kT, dt, particle_noise, seed, counter);
+  if (dtype == TSB_F64) {
+    TSB_NPT_POST(double)
+  } else {
+    TSB_NPT_POST(float)
+  }
+#undef TSB_NPT_POST
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}

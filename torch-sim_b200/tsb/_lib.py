@@ -89,6 +89,13 @@ PROTOTYPES = {
                                _i64, _vp, _dbl, _dbl, _i64, _vp, _vp, _vp, _vp, _vp, _vp,
                                _vp, _vp, _vp, _int, _int, _int, _u64, _u64, _vp, _vp, _vp,
                                _i64, _i64, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "tsb_npt_workspace_size": (_sz, [_i64]),
+    "tsb_npt_langevin_iso_pre": (_int, [_vp, _vp, _vp, _vp, _vp, _i64, _i64, _int, _vp, _vp,
+                                        _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                        _vp, _vp, _vp, _u64, _u64, _vp, _sz, _vp]),
+    "tsb_npt_langevin_iso_post": (_int, [_vp, _vp, _vp, _vp, _vp, _i64, _i64, _int, _vp, _vp,
+                                         _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                         _vp, _u64, _u64, _vp, _sz, _vp]),
     "tsb_thermostat_workspace_size": (_sz, [_i64]),
     "tsb_kinetic_energy": (_int, [_vp, _vp, _vp, _i64, _i64, _int, _vp, _vp, _sz, _vp]),
     "tsb_nhc_half_step": (_int, [_vp, _vp, _vp, _i64, _i64, _int, _vp, _vp, _vp, _vp, _vp,

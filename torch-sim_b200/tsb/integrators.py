@@ -12,6 +12,7 @@ converts user units, torch_sim/integrators/__init__.py:193-255):
 * ``nvt_nose_hoover_init/step/invariant`` <- nvt.py:244-562 (Nose-Hoover chains,
   md.py:249-563)
 * ``nvt_vrescale_init/step`` <- nvt.py:565-741 (CSVR; ``step(model, state, ...)``)
+* ``npt_langevin_isotropic_init/step`` <- npt.py:653-1107 (strain-based GJF barostat)
 
 Steps mutate ``state`` in place and return it (md.py:184-187).  ``dt``, ``kT``
 and ``gamma`` may be scalars or per-system tensors.
@@ -50,8 +51,12 @@ def initialize_momenta(positions, masses, system_idx, kT, generator=None):
                     generator=generator) * torch.sqrt(masses * kT).unsqueeze(-1)
     n_sys = int(system_idx[-1]) + 1
     counts = torch.bincount(system_idx, minlength=n_sys)
-    mean = torch.zeros((n_sys, 3), device=p.device, dtype=p.dtype).index_add_(
-        0, system_idx, p) / counts.view(-1, 1)
+    # per-system sums from an FP64 prefix sum over the contiguous systems: a fixed
+    # summation order (index_add_ on the GPU sums in a run-dependent order)
+    cs = torch.cat([torch.zeros((1, 3), dtype=torch.float64, device=p.device),
+                    p.to(torch.float64).cumsum(0)])
+    ends = counts.cumsum(0)
+    mean = ((cs[ends] - cs[ends - counts]) / counts.view(-1, 1)).to(p.dtype)
     return torch.where((counts > 1)[system_idx].view(-1, 1), p - mean[system_idx], p)
 
 
@@ -293,6 +298,84 @@ def nvt_vrescale_step(model, state, *, dt, kT, tau=None, noise=None, **_kw):
     _drift(state, dt_s, 1.0)
     _apply_model(state, model)
     _kick(state, dt_s, 0.5)
+    return state
+
+
+# ---------------------------------------------------------------------------
+# Isotropic NPT Langevin
+# ---------------------------------------------------------------------------
+def npt_langevin_isotropic_init(state, model, *, kT, dt, alpha=None, cell_alpha=None,
+                                b_tau=None, **_kw):
+    """Strain-based isotropic NPT Langevin state (npt.py:888-985): eps = 0,
+    alpha = 1/(5 dt), cell_alpha = 1/(30 dt), b_tau = 300 dt by default,
+    Q = (N + 1) kT b_tau^2.  ``model`` must compute the stress."""
+    from .state import NPTLangevinIsotropicState
+
+    md = _md_init(state, model, kT)
+    out = model(md)
+    if "stress" not in out:
+        raise ValueError("NPT needs a model with compute_stress=True")
+    n_sys, dev = md.n_systems, md.device
+    dt_s = _per_system(dt, n_sys, dev)
+    kT_s = _per_system(kT, n_sys, dev)
+    alpha = _per_system(1.0 / (5 * dt_s) if alpha is None else alpha, n_sys, dev).clone()
+    cell_alpha = _per_system(1.0 / (30 * dt_s) if cell_alpha is None else cell_alpha,
+                             n_sys, dev).clone()
+    b_tau = _per_system(300 * dt_s if b_tau is None else b_tau, n_sys, dev).clone()
+    n_at = torch.bincount(md.system_idx, minlength=n_sys).to(torch.float64)
+    z = torch.zeros(n_sys, dtype=torch.float64, device=dev)
+    st = NPTLangevinIsotropicState.from_state(
+        md, stress=out["stress"], alpha=alpha, cell_alpha=cell_alpha, b_tau=b_tau,
+        reference_cell=md.cell.to(torch.float64).clone(), cell_positions=z.clone(),
+        cell_velocities=z.clone(), cell_masses=(n_at + 1) * kT_s * b_tau * b_tau)
+    st._philox_seed, st._philox_counter = md._philox_seed, 0
+    return st
+
+
+def npt_langevin_isotropic_step(state, model, *, dt, kT, external_pressure, noise=None, **_kw):
+    """One isotropic NPT Langevin step (npt.py:988-1107).  The cell noise [S] and the
+    particle noise [N, 3] are drawn on the device from the Philox stream (seed,
+    system / atom, step); ``noise = (cell_noise, particle_noise)`` supplies them
+    instead, e.g. the reference's own draws."""
+    _prepare(state)
+    n_sys, n, dev = state.n_systems, state.n_atoms, state.device
+    dt_s = _per_system(dt, n_sys, dev)
+    kT_s = _per_system(kT, n_sys, dev)
+    p_s = _per_system(external_pressure, n_sys, dev)
+    for name in ("alpha", "cell_alpha", "b_tau", "reference_cell", "cell_positions",
+                 "cell_velocities", "cell_masses"):
+        v = getattr(state, name)
+        if v.dtype != torch.float64 or not v.is_contiguous():
+            setattr(state, name, v.to(torch.float64).contiguous())
+    state.cell = state.cell.to(state.dtype).contiguous()
+    state.stress = state.stress.to(state.dtype).contiguous()
+    cn = pn = None
+    if noise is not None:
+        cn = torch.as_tensor(noise[0], dtype=torch.float64, device=dev).reshape(n_sys)
+        pn = torch.as_tensor(noise[1], dtype=torch.float64, device=dev).reshape(n, 3)
+        cn, pn = cn.contiguous(), pn.contiguous()
+    seed = getattr(state, "_philox_seed", _seed_of(state)) & (2**64 - 1)
+    counter = getattr(state, "_philox_counter", 0)
+    f_eps = torch.empty(n_sys, dtype=torch.float64, device=dev)
+    ws = L.Workspace.get(dev, L.load().tsb_npt_workspace_size(n_sys))
+    dtc, stp = L.dtype_code(state.dtype), L.stream_ptr(dev)
+    L.call("tsb_npt_langevin_iso_pre", L.ptr(state.positions), L.ptr(state.momenta),
+           L.ptr(state.forces), L.ptr(state.masses), L.ptr(state.system_idx), n, n_sys, dtc,
+           L.ptr(state.stress), L.ptr(state.reference_cell), L.ptr(state.cell),
+           L.ptr(state.cell_positions), L.ptr(state.cell_velocities), L.ptr(state.cell_masses),
+           L.ptr(f_eps), L.ptr(state.alpha), L.ptr(state.cell_alpha), L.ptr(state.b_tau),
+           L.ptr(kT_s), L.ptr(p_s), L.ptr(dt_s), L.ptr(cn), L.ptr(pn), seed, counter,
+           L.ptr(ws), ws.numel(), stp)
+    forces_old = state.forces
+    out = _apply_model(state, model)
+    state.stress = out["stress"].to(state.dtype).contiguous()
+    L.call("tsb_npt_langevin_iso_post", L.ptr(state.momenta), L.ptr(state.masses),
+           L.ptr(forces_old), L.ptr(state.forces), L.ptr(state.system_idx), n, n_sys, dtc,
+           L.ptr(state.stress), L.ptr(state.reference_cell), L.ptr(state.cell_positions),
+           L.ptr(state.cell_velocities), L.ptr(state.cell_masses), L.ptr(f_eps),
+           L.ptr(state.alpha), L.ptr(state.cell_alpha), L.ptr(kT_s), L.ptr(p_s), L.ptr(dt_s),
+           L.ptr(cn), L.ptr(pn), seed, counter, L.ptr(ws), ws.numel(), stp)
+    state._philox_seed, state._philox_counter = seed, counter + 1
     return state
 
 

@@ -192,6 +192,31 @@ class NVTVRescaleState(MDState):
 
 
 @dataclass(kw_only=True)
+class NPTLangevinIsotropicState(MDState):
+    """MDState + strain-based isotropic barostat (torch_sim/integrators/npt.py:653-703):
+    stress [S,3,3]; per system alpha, cell_alpha, b_tau, strain ``cell_positions``
+    (eps = ln(V/V0)/3), ``cell_velocities`` (d eps/dt), ``cell_masses``;
+    ``reference_cell`` [S,3,3] (cell = exp(eps) reference_cell)."""
+
+    stress: torch.Tensor
+    alpha: torch.Tensor
+    cell_alpha: torch.Tensor
+    b_tau: torch.Tensor
+    reference_cell: torch.Tensor
+    cell_positions: torch.Tensor
+    cell_velocities: torch.Tensor
+    cell_masses: torch.Tensor
+
+    @property
+    def current_cell(self) -> torch.Tensor:
+        return torch.exp(self.cell_positions)[:, None, None] * self.reference_cell
+
+    @property
+    def volume(self) -> torch.Tensor:
+        return torch.linalg.det(self.reference_cell) * torch.exp(3 * self.cell_positions)
+
+
+@dataclass(kw_only=True)
 class FireState(SimState):
     forces: torch.Tensor
     energy: torch.Tensor
