@@ -221,7 +221,10 @@ __global__ void k_geom_bins(const P *pos, SysGeom *g, int32_t *sys_nbins) {
       G.org[k] = a;
       len[k] = fmax(b - a, 1e-9);
     }
-    double q = floor(len[k] / G.h[k]);
+    // bins at least half the search half-width wide: the search window spans at
+    // most 5 bins per axis and tests ~3.7x the sphere's volume instead of the
+    // ~6.4x (27 bins of one cutoff) that cutoff-wide bins give
+    double q = floor(2.0 * len[k] / G.h[k]);
     nbd[k] = fmin(fmax(q, 1.0), 1048576.0);
   }
   double cap = fmax(1.0, 2.0 * (double)G.count);
