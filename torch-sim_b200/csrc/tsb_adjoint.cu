@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(128)
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   const double4 w = b.spos[p];
-  const int i = (int)__double_as_longlong(w.w);
+  const int i = tag_atom(w.w);
   const SysGeom &G = b.geom[b.sys_of[i]];
   const int si = species ? min(max(species[i], 0), nsp - 1) : 0;
   const double vi0 = v[3 * i], vi1 = v[3 * i + 1], vi2 = v[3 * i + 2];
@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(128)
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   const double4 w = b.spos[p];
-  const int i = (int)__double_as_longlong(w.w);
+  const int i = tag_atom(w.w);
   const SysGeom &G = b.geom[b.sys_of[i]];
   double *h = part + (size_t)i * nb;
   for (int k = 0; k < nb; ++k) h[k] = 0.0;
@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(128)
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   const double4 w = b.spos[p];
-  const int i = (int)__double_as_longlong(w.w);
+  const int i = tag_atom(w.w);
   const int s = b.sys_of[i];
   const SysGeom &G = b.geom[s];
   const double *dh = dl_dh + (size_t)s * nb;

@@ -295,7 +295,7 @@ __global__ void k_bin_scatter(const int32_t *bin_of, const int64_t *bin_start,
 // Deterministic order inside each bin (ascending atom index), then gather the
 // wrapped positions into bin order.
 __global__ void k_bin_sort(const int64_t *bin_start, int64_t nbins_total, int32_t *sidx,
-                           const double4 *wpos, double4 *spos) {
+                           const double4 *wpos, const int32_t *species, double4 *spos) {
   int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nbins_total) return;
   int64_t s0 = bin_start[b], s1 = bin_start[b + 1];
@@ -311,7 +311,8 @@ __global__ void k_bin_sort(const int64_t *bin_start, int64_t nbins_total, int32_
   for (int64_t p = s0; p < s1; ++p) {
     int32_t j = sidx[p];
     double4 w = wpos[j];
-    w.w = __longlong_as_double((long long)j);
+    const unsigned long long hi = species ? (unsigned long long)(uint32_t)species[j] : 0ull;
+    w.w = __longlong_as_double((long long)((hi << 32) | (uint32_t)j));
     spos[p] = w;
   }
 }
@@ -343,7 +344,7 @@ void carve_bins(Carver &c, BinData &b, int64_t n, int64_t ns) {
 template <class P>
 int prepare_bins(const P *positions, const P *cell_row, const uint8_t *pbc,
                  const int64_t *system_idx, int64_t n, int64_t ns, double cutoff,
-                 BinData &b, cudaStream_t st) {
+                 BinData &b, cudaStream_t st, const int32_t *species) {
   cudaMemsetAsync(b.sys_lo, 0, sizeof(int64_t) * ns, st);
   cudaMemsetAsync(b.sys_hi, 0, sizeof(int64_t) * ns, st);
   cudaMemsetAsync(b.bin_count, 0, sizeof(int32_t) * b.bcap, st);
@@ -362,7 +363,7 @@ int prepare_bins(const P *positions, const P *cell_row, const uint8_t *pbc,
     k_bin_scatter<<<grid_for(n), kBlock, 0, st>>>(b.bin_of, b.bin_start, b.bin_fill, n,
                                                   b.sidx);
     k_bin_sort<<<grid_for(b.bcap), kBlock, 0, st>>>(b.bin_start, b.bcap, b.sidx, b.wpos,
-                                                    b.spos);
+                                                    species, b.spos);
   }
   TSB_CHECK_LAUNCH();
   return TSB_OK;
@@ -370,9 +371,9 @@ int prepare_bins(const P *positions, const P *cell_row, const uint8_t *pbc,
 
 template int prepare_bins<float>(const float *, const float *, const uint8_t *,
                                  const int64_t *, int64_t, int64_t, double, BinData &,
-                                 cudaStream_t);
+                                 cudaStream_t, const int32_t *);
 template int prepare_bins<double>(const double *, const double *, const uint8_t *,
                                   const int64_t *, int64_t, int64_t, double, BinData &,
-                                  cudaStream_t);
+                                  cudaStream_t, const int32_t *);
 
 }  // namespace tsb

@@ -64,6 +64,13 @@ struct SysGeom {
   int32_t nbins;
 };
 
+// A bin-ordered position's .w carries the atom index in its low 32 bits and
+// the atom's species (0 when the caller gave none) in its high 32 bits.
+__device__ inline int tag_atom(double w) {
+  return (int)(uint32_t)(unsigned long long)__double_as_longlong(w);
+}
+__device__ inline int tag_species(double w) { return (int)(__double_as_longlong(w) >> 32); }
+
 struct Vec3 {
   double x, y, z;
 };
@@ -110,10 +117,12 @@ struct BinData {
 int64_t bin_capacity(int64_t n_atoms, int64_t n_systems);
 void carve_bins(Carver &c, BinData &b, int64_t n_atoms, int64_t n_systems);
 
-// dtype-generic preparation.  `search_cutoff` sets the bin size.
+// dtype-generic preparation.  `search_cutoff` sets the bin size; `species`
+// (optional) is tagged into the bin-ordered positions.
 template <class P>
 int prepare_bins(const P *positions, const P *cell_row, const uint8_t *pbc,
                  const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
-                 double search_cutoff, BinData &b, cudaStream_t st);
+                 double search_cutoff, BinData &b, cudaStream_t st,
+                 const int32_t *species = nullptr);
 
 }  // namespace tsb

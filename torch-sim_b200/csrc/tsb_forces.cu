@@ -29,18 +29,19 @@ __global__ void __launch_bounds__(128)
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   const double4 w = b.spos[p];
-  const int i = (int)__double_as_longlong(w.w);
+  const int i = tag_atom(w.w);
   const int s = b.sys_of[i];
   if (sys_active && !sys_active[s]) return;
   const SysGeom &G = b.geom[s];
-  const int si = species ? min(max(species[i], 0), ns_species - 1) : 0;
+  const int si = min(max(tag_species(w.w), 0), ns_species - 1);
   const PairPrm<R> *row = prm + si * ns_species;
   // forces accumulate in R; energy and virial in FP64 (per-system sums in FP64)
   R fx = 0, fy = 0, fz = 0;
   double ei = 0, vxx = 0, vyy = 0, vzz = 0, vyz = 0, vxz = 0, vxy = 0;
   search_neighbors(G, b.spos, b.bin_start, i, w.x, w.y, w.z, cutoff * cutoff, false,
-                   [&](int j, int, int, int, double dx, double dy, double dz, double d2) {
-                     const int sj = species ? min(max(species[j], 0), ns_species - 1) : 0;
+                   [&](int, int, int, int, double dx, double dy, double dz, double d2,
+                       int sp) {
+                     const int sj = min(max(sp, 0), ns_species - 1);
                      if (!(d2 < prc2[si * ns_species + sj])) return;  // FP64 decision
                      const PairPrm<R> &q = row[sj];
                      const R rx = (R)dx, ry = (R)dy, rz = (R)dz;
@@ -201,7 +202,7 @@ static int pair_forward(int pot, const double *table, int nsp, const int32_t *sp
                         int64_t n, int64_t ns, double cutoff, int flags, P *energy,
                         P *forces, P *stress, P *energies, P *stresses,
                         const uint8_t *active, PairWork &w, cudaStream_t st) {
-  TSB_TRY(prepare_bins<P>(pos, cell, pbc, sys, n, ns, cutoff, w.b, st));
+  TSB_TRY(prepare_bins<P>(pos, cell, pbc, sys, n, ns, cutoff, w.b, st, species));
   const bool f64 = flags & TSB_MATH_FP64;
   if (n > 0) {
 #define TSB_LAUNCH(POT)                                                                    \

@@ -18,7 +18,7 @@ __global__ void k_nl_count(BinData b, int64_t n, double rc2, int flags, int32_t 
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   const double4 w = b.spos[p];
-  const int i = (int)__double_as_longlong(w.w);
+  const int i = tag_atom(w.w);
   const SysGeom &G = b.geom[b.sys_of[i]];
   const bool self = flags & TSB_NL_SELF_INTERACTION;
   const bool half = flags & TSB_NL_HALF;
@@ -44,7 +44,7 @@ __global__ void k_nl_fill(BinData b, int64_t n, double rc2, int flags, const int
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   const double4 w = b.spos[p];
-  const int i = (int)__double_as_longlong(w.w);
+  const int i = tag_atom(w.w);
   int64_t o = off[i];
   if (o >= cap) return;
   const int s = b.sys_of[i];

@@ -1,6 +1,8 @@
 // Cell-list neighbour search over the binned, wrapped positions.
 #pragma once
 
+#include <type_traits>
+
 #include "tsb_common.cuh"
 
 namespace tsb {
@@ -19,7 +21,8 @@ __device__ inline int floordiv_dev(int a, int b) {
 
 // Visit every image (j, S) with |w_j + S @ cell - w_i|^2 < rc2 (FP64), where w
 // are the wrapped positions.  The unshifted self image is skipped unless
-// `self_pairs`.  Callback: f(j, Sx, Sy, Sz, dx, dy, dz, d2) with d = w_j + S@cell - w_i.
+// `self_pairs`.  Callback: f(j, Sx, Sy, Sz, dx, dy, dz, d2) with d = w_j + S@cell - w_i,
+// or f(..., d2, species_j) when it takes the species tag as a ninth argument.
 template <class F>
 __device__ inline void search_neighbors(const SysGeom &G, const double4 *__restrict__ spos,
                                         const int64_t *__restrict__ bin_start, int i,
@@ -61,9 +64,13 @@ __device__ inline void search_neighbors(const SysGeom &G, const double4 *__restr
           const double dz = (q.z + sz) - wz;
           const double d2 = dx * dx + dy * dy + dz * dz;
           if (d2 < rc2) {
-            const int j = (int)__double_as_longlong(q.w);
+            const int j = tag_atom(q.w);
             if (j == i && zero_shift && !self_pairs) continue;
-            f(j, ix, iy, iz, dx, dy, dz, d2);
+            if constexpr (std::is_invocable_v<F, int, int, int, int, double, double, double,
+                                              double, int>)
+              f(j, ix, iy, iz, dx, dy, dz, d2, tag_species(q.w));
+            else
+              f(j, ix, iy, iz, dx, dy, dz, d2);
           }
         }
       }

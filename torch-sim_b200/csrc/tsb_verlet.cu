@@ -42,7 +42,7 @@ __global__ void k_verlet_build(BinData b, int64_t n, double rcs2, uint32_t *list
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   const double4 w = b.spos[p];
-  const int i = (int)__double_as_longlong(w.w);
+  const int i = tag_atom(w.w);
   const SysGeom &G = b.geom[0];
   int c = 0;
   search_neighbors(G, b.spos, b.bin_start, i, w.x, w.y, w.z, rcs2, false,
