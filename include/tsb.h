@@ -164,6 +164,46 @@ int tsb_verlet_forces(int potential, const double *table, int n_species,
                       double *vir_atom, void *workspace, size_t workspace_bytes,
                       void *stream);
 
+/* ---- batched Verlet lists (many systems, moving atoms and cells) ----------
+ * Replaces the per-call neighbour search inside PairPotentialModel.forward
+ * (torch_sim/models/pair_potential.py:168-174, 351-464) for a batch whose atoms
+ * and cells change between calls (FIRE with a cell filter, NPT, MD).  Each
+ * system's list holds every pair within cutoff + skin (image shifts in
+ * {-1,0,1}^3 of the cell at its build) and is rebuilt, per system, when
+ * 2 D + c > skin or 2 D + 2 c > w_min - cutoff (D: largest drift of an atom in
+ * the build frame, c: sum of the norms of the periodic cell rows' change since
+ * the build, w_min: smallest periodic plane spacing at the build).  The pairs
+ * inside the cutoff, hence energy, forces and stresses, equal the per-call path.
+ * The workspace (tsb_vlist_workspace_size) holds the list frame and must be kept
+ * by the caller between calls; tsb_vlist_reset marks every system unbuilt.
+ * tsb_vlist_check: flags[0] = 1 when any active system must be rebuilt.
+ * tsb_vlist_build: rebins the batch and rebuilds the expired systems' lists
+ *   (list[k * N + slot] = slot of j << 5 | image code, counts [N] by slot);
+ *   flags[1] = 1 << 30 when a periodic cell is narrower than cutoff + skin, else
+ *   the largest neighbour count when it exceeded max_neighbors (regrow, reset and
+ *   build again), else 0.
+ * tsb_vlist_forces: energy [S], forces [N,3], stress [S,3,3], per-atom energies
+ *   [N] and stresses [N,3,3] per out_flags (TSB_MATH_FP64: FP64 pair function),
+ *   for the systems with sys_active != 0 (NULL: all).  LJ, Morse, soft sphere. */
+size_t tsb_vlist_workspace_size(int64_t n_atoms, int64_t n_systems);
+int tsb_vlist_reset(int64_t n_atoms, int64_t n_systems, void *workspace,
+                    size_t workspace_bytes, void *stream);
+int tsb_vlist_check(const void *positions, const void *cell_row, const int64_t *system_idx,
+                    const uint8_t *sys_active, int64_t n_atoms, int64_t n_systems, int dtype,
+                    double cutoff, double skin, int32_t *flags, void *workspace,
+                    size_t workspace_bytes, void *stream);
+int tsb_vlist_build(const void *positions, const void *cell_row, const uint8_t *pbc,
+                    const int64_t *system_idx, const int32_t *species, int64_t n_atoms,
+                    int64_t n_systems, int dtype, double cutoff, double skin, uint32_t *list,
+                    int32_t *counts, int max_neighbors, int32_t *flags, void *workspace,
+                    size_t workspace_bytes, void *stream);
+int tsb_vlist_forces(int potential, const double *table, int n_species, const int32_t *species,
+                     const uint32_t *list, const int32_t *counts, const void *positions,
+                     const void *cell_row, const int64_t *system_idx, const uint8_t *sys_active,
+                     int64_t n_atoms, int64_t n_systems, int dtype, double cutoff,
+                     int out_flags, void *energy, void *forces, void *stress, void *energies,
+                     void *stresses, void *workspace, size_t workspace_bytes, void *stream);
+
 /* ---- adjoint of NVE trajectories (species-matrix LJ, FP64) ---------------
  * No kernel of the reference corresponds: it differentiates trajectories with
  * torch.autograd through PairPotentialModel (pair_potential.py:420-425), which

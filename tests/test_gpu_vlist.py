@@ -1,0 +1,177 @@
+"""Batched Verlet lists (VerletListModel over many systems whose atoms and cells
+move) against the per-call cell-list search and the reference FIRE trajectory.
+
+Tolerances: FP64 pair arithmetic on both paths -> max|d|/max|ref| <= 1e-10 (same
+pairs, different summation order); FP32 pair arithmetic -> 1e-5; the reference
+FIRE + Frechet trajectory to rtol 1e-7, as for the per-call path.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _ka(n_systems=12, n_min=64, n_max=400, seed=0, dtype=torch.float64):
+    from tsb import workloads
+    from tsb.state import state_from_arrays
+
+    d = workloads.kob_andersen_batch(n_systems, n_min, n_max, seed=seed)
+    return state_from_arrays(d, device="cuda", dtype=dtype)
+
+
+def _models(precision="fp64", dtype=torch.float64, skin=1.0, **kw):
+    from tsb import models
+
+    mk = lambda: models.kob_andersen_model(compute_stress=True, precision=precision,  # noqa
+                                           dtype=dtype, **kw)
+    return models.VerletListModel(mk(), skin=skin), mk()
+
+
+def _cmp(a, b, rtol, keys=("energy", "forces", "stress")):
+    for k in keys:
+        x, y = a[k].double().cpu().numpy(), b[k].double().cpu().numpy()
+        err = np.abs(x - y).max() / max(np.abs(y).max(), 1e-300)
+        assert err <= rtol, (k, err)
+
+
+def test_vlist_matches_cell_list_per_atom_outputs():
+    st = _ka()
+    vm, ref = _models(per_atom_energies=True, per_atom_stresses=True)
+    _cmp(vm(st), ref(st), 1e-10, ("energy", "forces", "stress", "energies", "stresses"))
+    assert vm.n_builds == 1
+
+
+def test_vlist_moving_atoms_and_cells_rebuild_only_when_needed():
+    st = _ka(seed=3)
+    vm, ref = _models()
+    _cmp(vm(st), ref(st), 1e-10)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    eye = torch.eye(3, dtype=st.dtype, device="cuda")
+    # small moves and strains: lists kept, pairs still exact
+    for _ in range(4):
+        eps = 2e-4 * torch.randn((st.n_systems, 3, 3), device="cuda", dtype=st.dtype,
+                                 generator=g)
+        F = eye + 0.5 * (eps + eps.mT)
+        st.positions = torch.einsum("nij,nj->ni", F[st.system_idx], st.positions) + \
+            0.01 * torch.randn(st.positions.shape, device="cuda", dtype=st.dtype, generator=g)
+        st.cell = torch.einsum("nij,njk->nik", F, st.cell).contiguous()
+        _cmp(vm(st), ref(st), 1e-10)
+    assert vm.n_builds == 1
+    # a 3 % strain of one system: its list expires (and only it is rebuilt)
+    F = eye.repeat(st.n_systems, 1, 1)
+    F[4] += 0.03 * torch.tensor([[1.0, 0.2, 0.0], [0.2, -0.5, 0.0], [0.0, 0.0, 0.4]],
+                                device="cuda", dtype=st.dtype)
+    st.positions = torch.einsum("nij,nj->ni", F[st.system_idx], st.positions).contiguous()
+    st.cell = torch.einsum("nij,njk->nik", F, st.cell).contiguous()
+    _cmp(vm(st), ref(st), 1e-10)
+    assert vm.n_builds == 2
+    # atoms moved by lattice vectors (unwrapped) and one atom jumping by 0.7 A
+    k = torch.randint(-3, 4, st.positions.shape, device="cuda", generator=g).to(st.dtype)
+    st.positions = (st.positions +
+                    torch.einsum("ni,nij->nj", k, st.cell.mT[st.system_idx])).contiguous()
+    st.positions[17] += torch.tensor([0.7, 0.0, 0.0], device="cuda", dtype=st.dtype)
+    _cmp(vm(st), ref(st), 1e-10)
+
+
+def test_vlist_triclinic_copper_and_open_axis():
+    from tsb import models, workloads
+    from tsb.state import state_from_arrays
+
+    d = workloads.copper_batch(6, 256, 500, seed=0, jitter=0.02)
+    # every plane spacing (10.6 A at least) exceeds cutoff + skin = 6.8 A
+    widths = [1.0 / np.linalg.norm(np.linalg.inv(c.T), axis=0) for c in d["cell"]]
+    assert min(w.min() for w in widths) > 6.8
+    for pbc in (True, [True, False, True]):
+        st = state_from_arrays(d, device="cuda")
+        st.pbc = torch.as_tensor(pbc, dtype=torch.bool, device="cuda")
+        mk = lambda: models.MorseModel(sigma=2.866, epsilon=0.3429, alpha=1.3588,  # noqa
+                                       cutoff=6.0, compute_stress=True, precision="fp64")
+        vm, ref = models.VerletListModel(mk(), skin=0.8), mk()
+        _cmp(vm(st), ref(st), 1e-10)
+        st.positions = (st.positions + 0.05).contiguous()
+        _cmp(vm(st), ref(st), 1e-10)
+
+
+def test_vlist_float32_mixed_precision():
+    st32 = _ka(seed=7, dtype=torch.float32)
+    vm, _ = _models(precision="mixed", dtype=torch.float32)
+    _, ref = _models()
+    st64 = _ka(seed=7)
+    st64.positions = st32.positions.double()
+    st64.cell = st32.cell.double()
+    out = vm(st32)
+    assert out["forces"].dtype == torch.float32
+    _cmp(out, ref(st64), 1e-5, ("forces",))
+
+
+def test_vlist_list_overflow_regrows():
+    st = _ka(n_systems=4, seed=9)
+    vm, ref = _models()
+    vm(st)
+    n = st.n_atoms
+    vm.cap = 8
+    vm.list = torch.empty(vm.cap * n, dtype=torch.int32, device="cuda")
+    vm._reset(n, st.n_systems, torch.device("cuda"))
+    _cmp(vm(st), ref(st), 1e-10)
+    assert vm.cap > 8
+
+
+def test_vlist_narrow_cell_rejected():
+    st = _ka(n_systems=2, n_min=64, n_max=64)  # 12.8 A boxes
+    vm, _ = _models(skin=5.0)  # cutoff + skin = 13.5 A
+    with pytest.raises(ValueError):
+        vm(st)
+
+
+def test_vlist_forward_into_inactive_systems_untouched():
+    st = _ka(n_systems=6, seed=11)
+    vm, ref = _models()
+    r = ref(st)
+    active = torch.tensor([1, 0, 1, 0, 0, 1], dtype=torch.uint8, device="cuda")
+    e = torch.full((6,), 7.0, dtype=torch.float64, device="cuda")
+    f = torch.full((st.n_atoms, 3), 7.0, dtype=torch.float64, device="cuda")
+    s = torch.full((6, 3, 3), 7.0, dtype=torch.float64, device="cuda")
+    vm.forward_into(st, energy=e, forces=f, stress=s, sys_active=active)
+    act_atoms = active.bool()[st.system_idx]
+    assert bool((f[~act_atoms] == 7.0).all()) and bool((e[~active.bool()] == 7.0).all())
+    np.testing.assert_allclose(f[act_atoms].cpu(), r["forces"][act_atoms].cpu(), rtol=0,
+                               atol=1e-10 * float(r["forces"].abs().max()))
+    np.testing.assert_allclose(s[active.bool()].cpu(), r["stress"][active.bool()].cpu(),
+                               rtol=1e-10, atol=1e-16)
+
+
+def test_vlist_fire_frechet_matches_reference(golden):
+    from tsb import models, optimizers
+    from tsb.state import SimState
+
+    g = golden["fire"]["ase_frechet"]
+    dev = torch.device("cuda")
+    T = lambda x, dt=torch.float64: torch.as_tensor(np.asarray(x), dtype=dt, device=dev)  # noqa
+    st = SimState(positions=T(g["positions"][0]), masses=T(g["masses"]), cell=T(g["cell"][0]),
+                  pbc=True, atomic_numbers=T(g["atomic_numbers"], torch.int64),
+                  system_idx=T(g["system_idx"], torch.int64))
+    m = models.VerletListModel(models.kob_andersen_model(compute_stress=True,
+                                                         precision="fp64"), skin=1.0)
+    st = optimizers.fire_init(st, m, cell_filter="frechet")
+    for k in range(1, g["positions"].shape[0]):
+        st = optimizers.fire_step(st, m)
+        for key in ("positions", "cell", "energy", "forces", "cell_forces", "velocities"):
+            np.testing.assert_allclose(getattr(st, key).cpu().numpy(), g[key][k], rtol=1e-7,
+                                       atol=1e-10, err_msg=f"step {k} {key}")
+
+
+def test_vlist_optimize_converges_like_cell_list():
+    from tsb import optimizers
+
+    st = _ka(n_systems=8, n_max=300, seed=13)
+    vm, ref = _models()
+    st, steps, conv = optimizers.optimize(st, vm, fmax=1e-3, max_steps=6000,
+                                          cell_filter="frechet")
+    assert bool(conv.all()), (steps, conv)
+    out = ref(st)
+    fmax = torch.zeros(st.n_systems, dtype=torch.float64, device="cuda").scatter_reduce(
+        0, st.system_idx, out["forces"].norm(dim=1), reduce="amax")
+    assert float(fmax.max()) < 1e-3
+    assert vm.n_builds < steps

@@ -70,3 +70,22 @@ def test_units_match_reference_constants():
 
     assert abs(workloads.METAL_TIME - 98.22694788464062) < 1e-9
     assert abs(workloads.KB_EV - 8.617330337217213e-05) < 1e-18
+
+
+def test_pbc_rows_accepts_every_reference_form():
+    """SimState.pbc may be a bool, a 0-d or [3] tensor, or per-system rows."""
+    import pytest
+    import torch
+
+    from tsb import _lib as L
+
+    want = torch.tensor([[1, 0, 1]] * 4, dtype=torch.uint8)
+    assert torch.equal(L.pbc_rows(torch.tensor([True, False, True]), 4, "cpu"), want)
+    assert torch.equal(L.pbc_rows(want.bool(), 4, "cpu"), want)
+    assert torch.equal(L.pbc_rows(want.reshape(-1), 4, "cpu"), want)
+    assert torch.equal(L.pbc_rows(True, 4, "cpu"), torch.ones(4, 3, dtype=torch.uint8))
+    assert torch.equal(L.pbc_rows(torch.tensor(False), 2, "cpu"),
+                       torch.zeros(2, 3, dtype=torch.uint8))
+    assert L.pbc_rows(True, 4, "cpu").is_contiguous()
+    with pytest.raises(ValueError):
+        L.pbc_rows(torch.ones(5, dtype=torch.bool), 4, "cpu")

@@ -21,6 +21,7 @@
 namespace tsb {
 
 constexpr int kFireThreads = 256;
+constexpr int kFireScr = 21;  // per-system scratch: drs, sc, fac, Finv[9], Fa[9]
 
 struct FireHyper {
   double dt_max, f_inc, f_dec, alpha_start, f_alpha, max_step, eps;
@@ -103,13 +104,18 @@ __global__ void k_count_finite_v(const P *v, int64_t n, int32_t *count) {
   if ((threadIdx.x & 31) == 0 && b) atomicAdd(count, __popc(b));
 }
 
+// ASE-FIRE step in three launches: (a) one block per system for the power,
+// mixing and velocity step with its FP64 sums, (b) one thread per system for the
+// cell velocity, the max_step factor and the Frechet cell update (3x3 algebra,
+// kept out of (a) so that the per-system blocks stay light on registers), (c) one
+// thread per atom for the position update.
 template <class P>
-__global__ void __launch_bounds__(kFireThreads) k_fire_ase_pre(FireArgs<P> A,
-                                                               const int32_t *n_finite) {
+__global__ void __launch_bounds__(kFireThreads) k_fire_ase_vel(FireArgs<P> A,
+                                                               const int32_t *n_finite,
+                                                               double *scr) {
   __shared__ double sh[100];
-  __shared__ double s_alpha, s_vs, s_fs, s_dt, s_fac, s_sc;
+  __shared__ double s_alpha, s_vs, s_fs;
   __shared__ int s_pos;
-  __shared__ double s_Finv[9], s_Fa[9];
   const int s = blockIdx.x;
   if (A.active && !A.active[s]) return;
   const int64_t a0 = A.lo[s], a1 = A.hi[s];
@@ -195,7 +201,19 @@ __global__ void __launch_bounds__(kFireThreads) k_fire_ase_pre(FireArgs<P> A,
     }
   __syncthreads();
   block_sum3(drs, dummy1, dummy2, sh);
-  if (tid == 0) {
+  if (tid == 0) scr[kFireScr * s] = drs;
+}
+
+template <class P>
+__global__ void k_fire_ase_cell(FireArgs<P> A, int64_t ns, double *scr) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns || (A.active && !A.active[s])) return;
+  const bool cellf = A.cell_filter != 0;
+  const FireHyper &h = A.h;
+  const double dts = (double)A.dt[s];
+  double drs = scr[kFireScr * s];
+  double *o = scr + kFireScr * s;
+  {
     double dc[9];
     if (cellf)
       for (int k = 0; k < 9; ++k) {
@@ -206,9 +224,8 @@ __global__ void __launch_bounds__(kFireThreads) k_fire_ase_pre(FireArgs<P> A,
         drs += dc[k] * dc[k];
       }
     const double sc = sqrt(drs);
-    s_sc = sc;
-    s_dt = dts;
-    s_fac = sc > h.max_step ? h.max_step / (sc + h.eps) : 1.0;
+    o[1] = sc;
+    o[2] = sc > h.max_step ? h.max_step / (sc + h.eps) : 1.0;
     if (cellf) {
       // Frechet cell update (fire.py:400-470)
       const M3 ref = load_m3(A.ref_cell + 9 * s);
@@ -236,15 +253,28 @@ __global__ void __launch_bounds__(kFireThreads) k_fire_ase_pre(FireArgs<P> A,
       const M3 Fa = m3_mul(load_m3(A.cell + 9 * s), refi);
       store_m3(A.cell_pos + 9 * s, m3_scale(m3_logm(Fa), cf));
       for (int k = 0; k < 9; ++k) {
-        s_Finv[k] = Finv.a[k];
-        s_Fa[k] = Fa.a[k];
+        o[3 + k] = Finv.a[k];
+        o[12 + k] = Fa.a[k];
       }
     }
   }
-  __syncthreads();
-  const double fac = s_fac;
-  const double dtu = s_dt;
-  for (int64_t i = a0 + tid; i < a1; i += blockDim.x) {
+}
+
+template <class P>
+__global__ void k_fire_ase_pos(FireArgs<P> A, int64_t n, const int64_t *system_idx,
+                               const double *scr) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t s = system_idx[i];
+  if (A.active && !A.active[s]) return;
+  const bool cellf = A.cell_filter != 0;
+  const FireHyper &h = A.h;
+  const double *o = scr + kFireScr * s;
+  const double fac = o[2];
+  const double dtu = (double)A.dt[s];
+  const double *s_Finv = o + 3, *s_Fa = o + 12;
+  const double s_sc = o[1];
+  {
     double d[3], x[3];
     for (int k = 0; k < 3; ++k) {
       const double dk = (double)(P)((double)A.v[3 * i + k] * dtu);
@@ -439,12 +469,14 @@ __global__ void k_bounds(const int64_t *sys, int64_t n, int64_t *lo, int64_t *hi
 struct FireWork {
   int64_t *lo, *hi;
   int32_t *counter;
+  double *scr;  // [kFireScr * S] per-system values passed between the ASE launches
 };
 
 static void carve_fire(Carver &c, FireWork &w, int64_t ns) {
   w.lo = c.take<int64_t>(ns);
   w.hi = c.take<int64_t>(ns);
   w.counter = c.take<int32_t>(4);
+  w.scr = c.take<double>(kFireScr * ns);
 }
 
 static int prep_bounds(FireWork &w, const int64_t *sys, int64_t n, int64_t ns,
@@ -490,7 +522,10 @@ static int fire_call(int which, int cell_filter, void *positions, void *velociti
     if (n_atoms > 0)
       k_count_finite_v<P><<<grid_for(n_atoms), kBlock, 0, st>>>((const P *)velocities, n_atoms,
                                                                  w.counter);
-    k_fire_ase_pre<P><<<(unsigned)n_systems, kFireThreads, 0, st>>>(A, w.counter);
+    k_fire_ase_vel<P><<<(unsigned)n_systems, kFireThreads, 0, st>>>(A, w.counter, w.scr);
+    k_fire_ase_cell<P><<<grid_for(n_systems, 128), 128, 0, st>>>(A, n_systems, w.scr);
+    if (n_atoms > 0)
+      k_fire_ase_pos<P><<<grid_for(n_atoms), kBlock, 0, st>>>(A, n_atoms, system_idx, w.scr);
   } else if (which == 1) {
     if (n_atoms > 0)
       k_fire_vv_pre<P><<<grid_for(n_atoms), kBlock, 0, st>>>(A, n_atoms, system_idx);

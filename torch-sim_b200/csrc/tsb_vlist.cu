@@ -1,0 +1,657 @@
+// Batched Verlet lists: many systems, moving atoms and changing cells (FIRE with
+// a cell filter, NPT, plain MD on a batch).  Drop-in for the neighbour search
+// inside PairPotentialModel.forward (torch_sim/models/pair_potential.py:351-464),
+// which rebuilds its list in every call (pair_potential.py:168-174).  Here each
+// system's list holds every pair within cutoff + skin, is kept between calls and
+// is rebuilt, per system, only when the bound below allows a pair to have moved
+// from beyond cutoff + skin to inside the cutoff.  The pairs inside the cutoff,
+// and so energies, forces and stresses, are those of the per-call search.
+//
+// Validity.  A system's list is built at cell C0 from positions wrapped into it,
+// w0_i = x0_i - W_i C0 (W_i integer, zero on open axes), with entries (i, j, S),
+// S in {-1,0,1}^3 (code (Sx+1)*9 + (Sy+1)*3 + (Sz+1)).  At a later call with
+// positions x and cell C the frame positions are w_i = x_i - W_i C and an entry's
+// vector w_j + S C - w_i differs from its build value by at most 2 D + |S dC|,
+// D = max_i |w_i - w0_i|, dC = C - C0.  With c = sum over periodic k of |row k of
+// dC|, every pair with |S|_inf <= 1 is covered while 2 D + c <= skin.  A pair
+// with |S_k| = m >= 2 was at least (m - 1) w_min apart at build (w_min the
+// smallest periodic plane spacing of C0; the build checks that no such pair lies
+// within cutoff + skin), so it stays beyond the cutoff while
+// 2 D + 2 c <= w_min - cutoff and c <= w_min / 2.  Each call sets per system
+// dmax = min(skin - c, w_min - cutoff - 2 c) / 2 (negative when c > w_min / 2)
+// and expires the system when an atom's |w_i - w0_i| exceeds dmax.
+//
+// Layout by slot: a system's atoms occupy the slots of its atom range, ordered
+// by the bins of its last build (perm[slot] = atom), so neighbouring threads and
+// their neighbours sit close in memory.  ELL list[k * N + slot] (uint32: slot of
+// j << 5 | image code), counts per slot, frame positions per slot as double4 with
+// the species in the high word of .w.  Force kernel: one thread per slot over its
+// list, FP64 displacements and cutoff test, pair function in R, FP64
+// accumulation, per-system sums in a fixed order (deterministic).
+#include "tsb_pair.cuh"
+#include "tsb_search.cuh"
+#include "tsb_sysreduce.cuh"
+
+namespace tsb {
+
+constexpr int kVlBlock = 256;
+constexpr int kVlSmemSys = 16;  // systems of a force block whose shifts sit in shared memory
+
+struct VlWork {
+  BinData b;           // bins of the last rebuild (sys_of / sys_lo / sys_hi persist)
+  double4 *ref;        // [N] w0 at the atom's last build
+  int32_t *rwrap;      // [3N] W at the last build
+  double *rcell;       // [9S] C0
+  double *slack;       // [S] w_min - cutoff at build (+inf without periodic axes)
+  int32_t *permask;    // [S] periodic axes of the build frame (bit k)
+  double *dmax;        // [S] allowed drift for this call
+  int32_t *sys_exp;    // [S] rebuild this system
+  int32_t *sys_built;  // [S]
+  int32_t *perm;       // [N] atom of each slot (identity until a system is built)
+  int32_t *islot;      // [N] slot of each atom in the fresh bins of a build
+  int32_t *ecount;     // [S] atoms to rebuild per system
+  int64_t *eoff;       // [S+1] their exclusive prefix (work list of the build)
+  double4 *wpos;       // [N] current frame positions by slot, species in the high word
+  double *sv;          // [81 S] S C per image code
+  SysGeom *cur;        // [S] start / count / vol of the current cells
+  double *e_half;      // [N]
+  double *vir_half;    // [6N]
+  double *part;        // [7 S chunks]
+  int chunks;
+};
+
+static void carve_vl(Carver &c, VlWork &w, int64_t n, int64_t ns) {
+  w.sys_built = c.take<int32_t>(ns);
+  w.sys_exp = c.take<int32_t>(ns);
+  carve_bins(c, w.b, n, ns);
+  w.ref = c.take<double4>(n);
+  w.rwrap = c.take<int32_t>(3 * n);
+  w.rcell = c.take<double>(9 * ns);
+  w.slack = c.take<double>(ns);
+  w.permask = c.take<int32_t>(ns);
+  w.dmax = c.take<double>(ns);
+  w.perm = c.take<int32_t>(n);
+  w.islot = c.take<int32_t>(n);
+  w.ecount = c.take<int32_t>(ns);
+  w.eoff = c.take<int64_t>(ns + 1);
+  w.wpos = c.take<double4>(n);
+  w.sv = c.take<double>(81 * ns);
+  w.cur = c.take<SysGeom>(ns);
+  w.e_half = c.take<double>(n);
+  w.vir_half = c.take<double>(6 * n);
+  w.chunks = reduce_chunks(n, ns);
+  w.part = w.chunks > 1 ? c.take<double>(7 * ns * w.chunks) : nullptr;
+}
+
+__device__ inline double row_norm(const double *a) {
+  return sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+}
+
+// per system: deformation since the build -> allowed drift (or expiry)
+template <class P>
+__global__ void k_vl_sys_check(const P *cell_row, const uint8_t *active, int64_t ns,
+                               double cutoff, double skin, const double *rcell,
+                               const double *slack, const int32_t *permask,
+                               const int32_t *built, double *dmax, int32_t *sys_exp,
+                               int32_t *flags) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  if (active && !active[s]) {
+    dmax[s] = INFINITY;
+    sys_exp[s] = 0;
+    return;
+  }
+  if (!built[s]) {
+    dmax[s] = -1.0;
+    sys_exp[s] = 1;
+    flags[0] = 1;
+    return;
+  }
+  double c = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    if (!((permask[s] >> k) & 1)) continue;
+    double d[3];
+    for (int m = 0; m < 3; ++m)
+      d[m] = (double)cell_row[9 * s + 3 * k + m] - rcell[9 * s + 3 * k + m];
+    c += row_norm(d);
+  }
+  const double wmin = slack[s] + cutoff;
+  double d = 0.5 * fmin(skin - c, slack[s] - 2.0 * c);
+  if (c > 0.5 * wmin) d = -1.0;
+  dmax[s] = d;
+  sys_exp[s] = d < 0.0;
+  if (d < 0.0) flags[0] = 1;
+}
+
+// per atom: drift in the build frame against the system's allowance
+template <class P>
+__global__ void k_vl_atom_check(const P *pos, const P *cell_row, const int64_t *sys,
+                                int64_t n, const int32_t *rwrap, const double4 *ref,
+                                const double *dmax, int32_t *sys_exp, int32_t *flags) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t s = sys[i];
+  const double dm = dmax[s];
+  if (!(dm >= 0.0) || isinf(dm)) return;  // expired already, or inactive
+  const P *C = cell_row + 9 * s;
+  const int W0 = rwrap[3 * i], W1 = rwrap[3 * i + 1], W2 = rwrap[3 * i + 2];
+  const double4 r = ref[i];
+  double d2 = 0.0;
+  for (int m = 0; m < 3; ++m) {
+    const double w = (double)pos[3 * i + m] -
+                     (W0 * (double)C[m] + W1 * (double)C[3 + m] + W2 * (double)C[6 + m]);
+    const double d = w - (m == 0 ? r.x : (m == 1 ? r.y : r.z));
+    d2 += d * d;
+  }
+  if (d2 > dm * dm) {
+    sys_exp[s] = 1;
+    flags[0] = 1;
+  }
+}
+
+__global__ void k_vl_iota(int32_t *perm, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) perm[i] = (int32_t)i;
+}
+
+// slot of each atom in the fresh bin order
+__global__ void k_vl_islot(const int32_t *sidx, int64_t n, int32_t *islot) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) islot[sidx[p]] = (int32_t)p;
+}
+
+// atoms of expired systems, for the work list of the build
+__global__ void k_vl_exp_counts(const int32_t *sys_exp, const int64_t *lo, const int64_t *hi,
+                                int64_t ns, int32_t *ecount) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < ns) ecount[s] = sys_exp[s] ? (int32_t)(hi[s] - lo[s]) : 0;
+}
+
+// List search for the atoms of expired systems over fresh bins (cutoff + skin),
+// one warp per atom.  Work item t (< eoff[ns]) is atom t - eoff[s] of system s,
+// the last system with eoff[s] <= t (bisection; empty systems are skipped); a
+// fixed grid of warps strides over the items.  The warp walks the atom's search
+// window row by row: bins of a row and image are adjacent in bin order, so each
+// span of candidates is contiguous and the lanes test 32 of them at a time; hits
+// are compacted with a ballot, so the list order (row, span, candidate) is fixed
+// and the writes of a span are coalesced.
+__global__ void __launch_bounds__(256)
+    k_vl_build(BinData b, int64_t n, int64_t ns, double rcs2, const int64_t *eoff,
+               const int32_t *islot, uint32_t *list, int32_t *cnt, int max_nb, int32_t *flags,
+               int32_t *perm, double4 *ref, int32_t *rwrap) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  const int64_t n_work = eoff[ns];
+  const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < n_work;
+       t += warps) {
+    int64_t a = 0, z = ns - 1;
+    while (a < z) {
+      const int64_t m = (a + z + 1) >> 1;
+      if (eoff[m] <= t) a = m; else z = m - 1;
+    }
+    const int64_t s = a;
+    const int64_t p = b.sys_lo[s] + (t - eoff[s]);
+    const double4 w = b.spos[p];
+    const int i = tag_atom(w.w);
+    const SysGeom &G = b.geom[s];
+    double u[3];
+    frame_coords(G, w.x, w.y, w.z, u);
+    int lo[3], hi[3];
+    for (int k = 0; k < 3; ++k) {
+      double f0 = floor((u[k] - G.h[k] - G.org[k]) * G.scale[k]);
+      double f1 = floor((u[k] + G.h[k] - G.org[k]) * G.scale[k]);
+      if (!G.per[k]) {
+        f0 = fmax(f0, 0.0);
+        f1 = fmin(f1, (double)(G.nb[k] - 1));
+      }
+      lo[k] = (int)f0;
+      hi[k] = (int)f1;
+    }
+    const int nb1 = G.nb[1], nb2 = G.nb[2];
+    int c = 0;
+    for (int cx = lo[0]; cx <= hi[0]; ++cx) {
+      const int ix = G.per[0] ? floordiv_dev(cx, G.nb[0]) : 0;
+      const int bx = cx - ix * G.nb[0];
+      for (int cy = lo[1]; cy <= hi[1]; ++cy) {
+        const int iy = G.per[1] ? floordiv_dev(cy, nb1) : 0;
+        const int by = cy - iy * nb1;
+        const int row = G.bin_base + (bx * nb1 + by) * nb2;
+        for (int cz = lo[2]; cz <= hi[2];) {
+          const int iz = G.per[2] ? floordiv_dev(cz, nb2) : 0;
+          const int bz = cz - iz * nb2;
+          const int bz_end = min(nb2 - 1, bz + (hi[2] - cz));  // last bin of this image
+          cz += bz_end - bz + 1;
+          const double sx = ix * G.cell[0] + iy * G.cell[3] + iz * G.cell[6];
+          const double sy = ix * G.cell[1] + iy * G.cell[4] + iz * G.cell[7];
+          const double sz = ix * G.cell[2] + iy * G.cell[5] + iz * G.cell[8];
+          const bool zero_shift = (ix | iy | iz) == 0;
+          const bool in_range =
+              ix >= -1 && ix <= 1 && iy >= -1 && iy <= 1 && iz >= -1 && iz <= 1;
+          const uint32_t code = (uint32_t)((ix + 1) * 9 + (iy + 1) * 3 + (iz + 1));
+          const int64_t q1 = b.bin_start[row + bz_end + 1];
+          for (int64_t q0 = b.bin_start[row + bz]; q0 < q1; q0 += 32) {
+            const int64_t q = q0 + lane;
+            bool hit = false;
+            int j = 0;
+            if (q < q1) {
+              const double4 o = b.spos[q];
+              const double dx = (o.x + sx) - w.x;
+              const double dy = (o.y + sy) - w.y;
+              const double dz = (o.z + sz) - w.z;
+              j = tag_atom(o.w);
+              hit = dx * dx + dy * dy + dz * dz < rcs2 && !(j == i && zero_shift);
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (m == 0u) continue;
+            if (!in_range) {  // a hit beyond the first images: cell narrower than rc + skin
+              if (lane == 0) atomicMax(&flags[1], 1 << 30);
+              continue;
+            }
+            if (hit) {
+              const int k = c + __popc(m & lt_mask);
+              if (k < max_nb) list[(size_t)k * n + p] = ((uint32_t)islot[j] << 5) | code;
+            }
+            c += __popc(m);
+          }
+        }
+      }
+    }
+    if (lane == 0) {
+      cnt[p] = c < max_nb ? c : max_nb;
+      if (c > max_nb) atomicMax(&flags[1], c);
+      perm[p] = i;
+      const double4 w0 = b.wpos[i];
+      ref[i] = make_double4(w0.x, w0.y, w0.z, 0.0);
+      rwrap[3 * i] = b.wrap[3 * i];
+      rwrap[3 * i + 1] = b.wrap[3 * i + 1];
+      rwrap[3 * i + 2] = b.wrap[3 * i + 2];
+    }
+  }
+}
+
+// per rebuilt system: record the build cell, its slack and periodic axes
+__global__ void k_vl_sys_built(const SysGeom *g, int64_t ns, double cutoff, int32_t *sys_exp,
+                               int32_t *built, double *rcell, double *slack,
+                               int32_t *permask) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns || !sys_exp[s]) return;
+  const SysGeom &G = g[s];
+  double wmin = INFINITY;
+  int mask = 0;
+  for (int k = 0; k < 3; ++k) {
+    if (!G.per[k]) continue;
+    mask |= 1 << k;
+    // plane spacing of lattice planes k = 1 / |reciprocal vector k| (row k of T)
+    wmin = fmin(wmin, 1.0 / row_norm(G.T + 3 * k));
+  }
+  for (int k = 0; k < 9; ++k) rcell[9 * s + k] = G.cell[k];
+  slack[s] = wmin - cutoff;
+  permask[s] = mask;
+  built[s] = 1;
+  sys_exp[s] = 0;
+}
+
+// per system for the force call: shift vectors, start / count, volume
+template <class P>
+__global__ void k_vl_sys_geom(const P *cell_row, int64_t ns, const int64_t *lo,
+                              const int64_t *hi, double *sv, SysGeom *cur) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  double C[9];
+  for (int k = 0; k < 9; ++k) C[k] = (double)cell_row[9 * s + k];
+  for (int code = 0; code < 27; ++code) {
+    const int sx = code / 9 - 1, sy = (code / 3) % 3 - 1, sz = code % 3 - 1;
+    for (int m = 0; m < 3; ++m)
+      sv[81 * s + 3 * code + m] = sx * C[m] + sy * C[3 + m] + sz * C[6 + m];
+  }
+  SysGeom &G = cur[s];
+  G.start = lo[s];
+  G.count = (int32_t)(hi[s] - lo[s]);
+  G.vol = fabs(C[0] * (C[4] * C[8] - C[5] * C[7]) - C[1] * (C[3] * C[8] - C[5] * C[6]) +
+               C[2] * (C[3] * C[7] - C[4] * C[6]));
+}
+
+// current positions -> frame of the atom's build (FP64) by slot, species in .w
+template <class P>
+__global__ void k_vl_frame(const P *pos, const P *cell_row, const int64_t *sys,
+                           const int32_t *species, int64_t n, const int32_t *perm,
+                           const int32_t *rwrap, double4 *wpos) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int64_t i = perm[p];
+  const P *C = cell_row + 9 * sys[i];
+  const int W0 = rwrap[3 * i], W1 = rwrap[3 * i + 1], W2 = rwrap[3 * i + 2];
+  double w[3];
+  for (int m = 0; m < 3; ++m)
+    w[m] = (double)pos[3 * i + m] -
+           (W0 * (double)C[m] + W1 * (double)C[3 + m] + W2 * (double)C[6 + m]);
+  const unsigned long long hi = species ? (unsigned long long)(uint32_t)species[i] : 0ull;
+  wpos[p] = make_double4(w[0], w[1], w[2], __longlong_as_double((long long)(hi << 32)));
+}
+
+template <int POT, class R, class P>
+__global__ void __launch_bounds__(kVlBlock)
+    k_vl_forces(const double4 *__restrict__ wpos, const uint32_t *__restrict__ list,
+                const int32_t *__restrict__ cnt, int64_t n, const int32_t *__restrict__ perm,
+                const int64_t *__restrict__ sys, const double *__restrict__ sv,
+                const double *__restrict__ table, int ns_species, double cutoff, int flags,
+                P *forces, P *energies, P *stresses, const SysGeom *__restrict__ cur,
+                double *e_half, double *vir_half, const uint8_t *__restrict__ active) {
+  __shared__ PairPrm<R> prm[kMaxSpecies * kMaxSpecies];
+  __shared__ double prc2[kMaxSpecies * kMaxSpecies];
+  __shared__ double ssv[kVlSmemSys * 81];
+  for (int k = threadIdx.x; k < ns_species * ns_species; k += blockDim.x) {
+    prm[k] = make_prm<R>(POT, table + 5 * k, cutoff);
+    if constexpr (sizeof(R) == 4) prm_fast_extra(POT, table + 5 * k, prm[k]);
+    prc2[k] = pair_rc2(POT, table + 5 * k, cutoff);
+  }
+  // slots are grouped by system, so a block spans systems s_lo..s_hi; the shift
+  // vectors of the first kVlSmemSys of them are staged in shared memory
+  const int64_t p0 = (int64_t)blockIdx.x * blockDim.x;
+  const int64_t s_lo = sys[perm[p0]];
+  const int64_t s_hi = sys[perm[min(p0 + (int64_t)blockDim.x, n) - 1]];
+  const int n_st = (int)min(s_hi - s_lo + 1, (int64_t)kVlSmemSys);
+  for (int k = threadIdx.x; k < 81 * n_st; k += blockDim.x) ssv[k] = sv[81 * s_lo + k];
+  __syncthreads();
+  const int64_t p = p0 + threadIdx.x;
+  if (p >= n) return;
+  const int64_t i = perm[p];
+  const int64_t s = sys[i];
+  if (active && !active[s]) return;
+  const double4 wi = wpos[p];
+  const int si = min(max(tag_species(wi.w), 0), ns_species - 1);
+  const PairPrm<R> *row = prm + si * ns_species;
+  const double *rc2row = prc2 + si * ns_species;
+  const double *svs = s - s_lo < n_st ? ssv + 81 * (s - s_lo) : sv + 81 * s;
+  const bool want_vir = flags & (TSB_OUT_STRESS | TSB_OUT_STRESSES);
+  const int c = cnt[p];
+  double fx = 0.0, fy = 0.0, fz = 0.0, ei = 0.0;
+  double vxx = 0, vyy = 0, vzz = 0, vyz = 0, vxz = 0, vxy = 0;
+  // one entry E with neighbour frame position WJ: FP64 displacement and cutoff
+  // test, pair function in R, FP64 accumulation
+#define TSB_VLPAIR(E, WJ)                                                                    \
+  {                                                                                          \
+    const int code = (int)((E) & 31u);                                                       \
+    const double dx = (WJ).x - wi.x + svs[3 * code];                                         \
+    const double dy = (WJ).y - wi.y + svs[3 * code + 1];                                     \
+    const double dz = (WJ).z - wi.z + svs[3 * code + 2];                                     \
+    const int sj = min(max(tag_species((WJ).w), 0), ns_species - 1);                        \
+    const double d2 = dx * dx + dy * dy + dz * dz;                                           \
+    if (d2 < rc2row[sj]) {                                                                   \
+      R ep, fr;                                                                              \
+      if constexpr (sizeof(R) == 4)                                                          \
+        pair_eval_fast<POT>(row[sj], (float)d2, ep, fr);                                     \
+      else                                                                                   \
+        pair_eval<POT, R>(row[sj], (R)d2, ep, fr);                                           \
+      const double gr = (double)fr;                                                          \
+      const double gx = gr * dx, gy = gr * dy, gz = gr * dz;                                 \
+      fx -= gx;                                                                              \
+      fy -= gy;                                                                              \
+      fz -= gz;                                                                              \
+      ei += (double)ep;                                                                      \
+      if (want_vir) {                                                                        \
+        vxx += dx * gx;                                                                      \
+        vyy += dy * gy;                                                                      \
+        vzz += dz * gz;                                                                      \
+        vyz += dy * gz;                                                                      \
+        vxz += dx * gz;                                                                      \
+        vxy += dx * gy;                                                                      \
+      }                                                                                      \
+    }                                                                                        \
+  }
+  // four entries per iteration; the next four list words are loaded one
+  // iteration ahead so their DRAM latency overlaps the current gathers and math
+  int k = 0;
+  const uint32_t *lp = list + p;
+  uint32_t e0 = 0, e1 = 0, e2 = 0, e3 = 0;
+  if (c >= 4) {
+    e0 = lp[0];
+    e1 = lp[(size_t)n];
+    e2 = lp[(size_t)2 * n];
+    e3 = lp[(size_t)3 * n];
+  }
+  for (; k + 4 <= c; k += 4) {
+    uint32_t f0 = 0, f1 = 0, f2 = 0, f3 = 0;
+    if (k + 8 <= c) {
+      const uint32_t *q = lp + (size_t)(k + 4) * n;
+      f0 = q[0];
+      f1 = q[(size_t)n];
+      f2 = q[(size_t)2 * n];
+      f3 = q[(size_t)3 * n];
+    }
+    const double4 w0 = wpos[e0 >> 5], w1 = wpos[e1 >> 5];
+    const double4 w2 = wpos[e2 >> 5], w3 = wpos[e3 >> 5];
+    TSB_VLPAIR(e0, w0)
+    TSB_VLPAIR(e1, w1)
+    TSB_VLPAIR(e2, w2)
+    TSB_VLPAIR(e3, w3)
+    e0 = f0;
+    e1 = f1;
+    e2 = f2;
+    e3 = f3;
+  }
+  for (; k < c; ++k) {
+    const uint32_t e = lp[(size_t)k * n];
+    const double4 wj = wpos[e >> 5];
+    TSB_VLPAIR(e, wj)
+  }
+#undef TSB_VLPAIR
+  if (flags & TSB_OUT_FORCES) {
+    forces[3 * i] = (P)fx;
+    forces[3 * i + 1] = (P)fy;
+    forces[3 * i + 2] = (P)fz;
+  }
+  // per-atom energies and stresses as the per-call search path writes them
+  if (flags & TSB_OUT_ENERGIES) energies[i] = (P)ei;
+  if (flags & TSB_OUT_STRESSES) {
+    const double cf = -0.5 / cur[s].vol;
+    P *o = stresses + 9 * i;
+    o[0] = (P)(cf * vxx); o[1] = (P)(cf * vxy); o[2] = (P)(cf * vxz);
+    o[3] = (P)(cf * vxy); o[4] = (P)(cf * vyy); o[5] = (P)(cf * vyz);
+    o[6] = (P)(cf * vxz); o[7] = (P)(cf * vyz); o[8] = (P)(cf * vzz);
+  }
+  e_half[i] = 0.5 * ei;
+  double *v = vir_half + 6 * i;
+  v[0] = 0.5 * vxx;
+  v[1] = 0.5 * vyy;
+  v[2] = 0.5 * vzz;
+  v[3] = 0.5 * vyz;
+  v[4] = 0.5 * vxz;
+  v[5] = 0.5 * vxy;
+}
+
+template <class P>
+static int vl_check(const P *pos, const P *cell, const int64_t *sys, const uint8_t *active,
+                    int64_t n, int64_t ns, double cutoff, double skin, int32_t *flags,
+                    VlWork &w, cudaStream_t st) {
+  cudaMemsetAsync(flags, 0, 2 * sizeof(int32_t), st);
+  k_vl_sys_check<P><<<grid_for(ns), kBlock, 0, st>>>(cell, active, ns, cutoff, skin, w.rcell,
+                                                     w.slack, w.permask, w.sys_built, w.dmax,
+                                                     w.sys_exp, flags);
+  k_vl_atom_check<P><<<grid_for(n), kBlock, 0, st>>>(pos, cell, sys, n, w.rwrap, w.ref, w.dmax,
+                                                     w.sys_exp, flags);
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
+
+template <class P>
+static int vl_build(const P *pos, const P *cell, const uint8_t *pbc, const int64_t *sys,
+                    const int32_t *species, int64_t n, int64_t ns, double cutoff, double skin,
+                    uint32_t *list, int32_t *counts, int max_nb, int32_t *flags, VlWork &w,
+                    cudaStream_t st) {
+  cudaMemsetAsync(flags + 1, 0, sizeof(int32_t), st);
+  const double rcs = cutoff + skin;
+  TSB_TRY(prepare_bins<P>(pos, cell, pbc, sys, n, ns, rcs, w.b, st, species));
+  k_vl_islot<<<grid_for(n), kBlock, 0, st>>>(w.b.sidx, n, w.islot);
+  k_vl_exp_counts<<<grid_for(ns), kBlock, 0, st>>>(w.sys_exp, w.b.sys_lo, w.b.sys_hi, ns,
+                                                   w.ecount);
+  TSB_TRY(exclusive_scan(w.ecount, w.eoff, ns, w.b.scan_tmp, st));
+  // a fixed grid of warps (8 blocks of 256 threads per SM) strides over the work
+  int dev = 0, n_sm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  k_vl_build<<<(unsigned)(n_sm * 8), 256, 0, st>>>(w.b, n, ns, rcs * rcs, w.eoff, w.islot, list,
+                                                    counts, max_nb, flags, w.perm, w.ref,
+                                                    w.rwrap);
+  k_vl_sys_built<<<grid_for(ns), kBlock, 0, st>>>(w.b.geom, ns, cutoff, w.sys_exp, w.sys_built,
+                                                  w.rcell, w.slack, w.permask);
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
+
+template <int POT, class R, class P>
+static void vl_launch(VlWork &w, const uint32_t *list, const int32_t *counts, int64_t n,
+                      const int64_t *sys, const double *table, int nsp, double cutoff,
+                      int flags, P *forces, P *energies, P *stresses, const uint8_t *active,
+                      cudaStream_t st) {
+  k_vl_forces<POT, R, P><<<grid_for(n, kVlBlock), kVlBlock, 0, st>>>(
+      w.wpos, list, counts, n, w.perm, sys, w.sv, table, nsp, cutoff, flags, forces, energies,
+      stresses, w.cur, w.e_half, w.vir_half, active);
+}
+
+template <class P>
+static int vl_forces(int pot, const double *table, int nsp, const int32_t *species,
+                     const uint32_t *list, const int32_t *counts, const P *pos, const P *cell,
+                     const int64_t *sys, const uint8_t *active, int64_t n, int64_t ns,
+                     double cutoff, int flags, P *energy, P *forces, P *stress, P *energies,
+                     P *stresses, VlWork &w, cudaStream_t st) {
+  k_vl_sys_geom<P><<<grid_for(ns), kBlock, 0, st>>>(cell, ns, w.b.sys_lo, w.b.sys_hi, w.sv,
+                                                    w.cur);
+  k_vl_frame<P><<<grid_for(n), kBlock, 0, st>>>(pos, cell, sys, species, n, w.perm, w.rwrap,
+                                                w.wpos);
+  const bool f64 = flags & TSB_MATH_FP64;
+#define TSB_VLL(POT)                                                                        \
+  if (f64)                                                                                  \
+    vl_launch<POT, double, P>(w, list, counts, n, sys, table, nsp, cutoff, flags, forces,  \
+                              energies, stresses, active, st);                              \
+  else                                                                                      \
+    vl_launch<POT, float, P>(w, list, counts, n, sys, table, nsp, cutoff, flags, forces,   \
+                             energies, stresses, active, st);
+  if (pot == TSB_POT_LJ) {
+    TSB_VLL(TSB_POT_LJ)
+  } else if (pot == TSB_POT_MORSE) {
+    TSB_VLL(TSB_POT_MORSE)
+  } else {
+    TSB_VLL(TSB_POT_SOFT)
+  }
+#undef TSB_VLL
+  k_sys_reduce<P><<<dim3((unsigned)ns, (unsigned)w.chunks), kBlock, 0, st>>>(
+      w.cur, w.e_half, w.vir_half, flags, energy, stress, active, w.chunks, w.part);
+  if (w.chunks > 1)
+    k_sys_final<P><<<grid_for(ns), kBlock, 0, st>>>(w.cur, w.part, ns, w.chunks, flags, energy,
+                                                     stress, active);
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
+
+}  // namespace tsb
+
+using namespace tsb;
+
+extern "C" size_t tsb_vlist_workspace_size(int64_t n_atoms, int64_t n_systems) {
+  Carver c(nullptr, (size_t)-1);
+  VlWork w;
+  carve_vl(c, w, n_atoms, n_systems);
+  return c.off + 256;
+}
+
+extern "C" int tsb_vlist_reset(int64_t n_atoms, int64_t n_systems, void *workspace,
+                               size_t workspace_bytes, void *stream) {
+  if (n_atoms < 1 || n_systems < 1 || !workspace) return TSB_ERR_INVALID_ARG;
+  Carver c(workspace, workspace_bytes);
+  VlWork w;
+  carve_vl(c, w, n_atoms, n_systems);
+  if (!c.ok) return TSB_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaMemsetAsync(w.sys_built, 0, sizeof(int32_t) * n_systems, st);
+  cudaMemsetAsync(w.sys_exp, 0, sizeof(int32_t) * n_systems, st);
+  k_vl_iota<<<grid_for(n_atoms), kBlock, 0, st>>>(w.perm, n_atoms);
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
+
+extern "C" int tsb_vlist_check(const void *positions, const void *cell_row,
+                               const int64_t *system_idx, const uint8_t *sys_active,
+                               int64_t n_atoms, int64_t n_systems, int dtype, double cutoff,
+                               double skin, int32_t *flags, void *workspace,
+                               size_t workspace_bytes, void *stream) {
+  if (n_atoms < 1 || n_systems < 1 || !positions || !cell_row || !system_idx || !flags ||
+      !(cutoff > 0.0) || !(skin >= 0.0))
+    return TSB_ERR_INVALID_ARG;
+  Carver c(workspace, workspace_bytes);
+  VlWork w;
+  carve_vl(c, w, n_atoms, n_systems);
+  if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == TSB_F64)
+    return vl_check<double>((const double *)positions, (const double *)cell_row, system_idx,
+                            sys_active, n_atoms, n_systems, cutoff, skin, flags, w, st);
+  if (dtype == TSB_F32)
+    return vl_check<float>((const float *)positions, (const float *)cell_row, system_idx,
+                           sys_active, n_atoms, n_systems, cutoff, skin, flags, w, st);
+  return TSB_ERR_INVALID_ARG;
+}
+
+extern "C" int tsb_vlist_build(const void *positions, const void *cell_row, const uint8_t *pbc,
+                               const int64_t *system_idx, const int32_t *species,
+                               int64_t n_atoms, int64_t n_systems, int dtype, double cutoff,
+                               double skin, uint32_t *list, int32_t *counts, int max_neighbors,
+                               int32_t *flags, void *workspace, size_t workspace_bytes,
+                               void *stream) {
+  if (n_atoms < 1 || n_systems < 1 || !positions || !cell_row || !pbc || !system_idx ||
+      !list || !counts || !flags || max_neighbors < 1 || !(cutoff > 0.0) || !(skin >= 0.0))
+    return TSB_ERR_INVALID_ARG;
+  if (n_atoms >= ((int64_t)1 << 27)) return TSB_ERR_UNSUPPORTED;
+  Carver c(workspace, workspace_bytes);
+  VlWork w;
+  carve_vl(c, w, n_atoms, n_systems);
+  if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == TSB_F64)
+    return vl_build<double>((const double *)positions, (const double *)cell_row, pbc,
+                            system_idx, species, n_atoms, n_systems, cutoff, skin, list,
+                            counts, max_neighbors, flags, w, st);
+  if (dtype == TSB_F32)
+    return vl_build<float>((const float *)positions, (const float *)cell_row, pbc, system_idx,
+                           species, n_atoms, n_systems, cutoff, skin, list, counts,
+                           max_neighbors, flags, w, st);
+  return TSB_ERR_INVALID_ARG;
+}
+
+extern "C" int tsb_vlist_forces(int potential, const double *table, int n_species,
+                                const int32_t *species, const uint32_t *list,
+                                const int32_t *counts, const void *positions,
+                                const void *cell_row, const int64_t *system_idx,
+                                const uint8_t *sys_active, int64_t n_atoms, int64_t n_systems,
+                                int dtype, double cutoff, int out_flags, void *energy,
+                                void *forces, void *stress, void *energies, void *stresses,
+                                void *workspace, size_t workspace_bytes, void *stream) {
+  if (potential < TSB_POT_LJ || potential > TSB_POT_SOFT || n_species < 1 ||
+      n_species > kMaxSpecies || !table || n_atoms < 1 || n_systems < 1 || !list || !counts ||
+      !positions || !cell_row || !system_idx || !energy)
+    return TSB_ERR_INVALID_ARG;
+  if (n_species > 1 && !species) return TSB_ERR_INVALID_ARG;
+  if (((out_flags & TSB_OUT_FORCES) && !forces) || ((out_flags & TSB_OUT_STRESS) && !stress) ||
+      ((out_flags & TSB_OUT_ENERGIES) && !energies) ||
+      ((out_flags & TSB_OUT_STRESSES) && !stresses))
+    return TSB_ERR_INVALID_ARG;
+  Carver c(workspace, workspace_bytes);
+  VlWork w;
+  carve_vl(c, w, n_atoms, n_systems);
+  if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == TSB_F64)
+    return vl_forces<double>(potential, table, n_species, species, list, counts,
+                             (const double *)positions, (const double *)cell_row, system_idx,
+                             sys_active, n_atoms, n_systems, cutoff, out_flags,
+                             (double *)energy, (double *)forces, (double *)stress,
+                             (double *)energies, (double *)stresses, w, st);
+  if (dtype == TSB_F32)
+    return vl_forces<float>(potential, table, n_species, species, list, counts,
+                            (const float *)positions, (const float *)cell_row, system_idx,
+                            sys_active, n_atoms, n_systems, cutoff, out_flags, (float *)energy,
+                            (float *)forces, (float *)stress, (float *)energies,
+                            (float *)stresses, w, st);
+  return TSB_ERR_INVALID_ARG;
+}

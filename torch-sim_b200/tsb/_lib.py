@@ -65,6 +65,14 @@ PROTOTYPES = {
                                 _vp]),
     "tsb_verlet_forces": (_int, [_int, _vp, _int, _vp, _vp, _i64, _vp, _int, _dbl, _int, _vp,
                                  _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "tsb_vlist_workspace_size": (_sz, [_i64, _i64]),
+    "tsb_vlist_reset": (_int, [_i64, _i64, _vp, _sz, _vp]),
+    "tsb_vlist_check": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _int, _dbl, _dbl, _vp, _vp, _sz,
+                               _vp]),
+    "tsb_vlist_build": (_int, [_vp, _vp, _vp, _vp, _vp, _i64, _i64, _int, _dbl, _dbl, _vp, _vp,
+                               _int, _vp, _vp, _sz, _vp]),
+    "tsb_vlist_forces": (_int, [_int, _vp, _int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64,
+                                _int, _dbl, _int, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
     "tsb_fire_workspace_size": (_sz, [_i64]),
     "tsb_fire_ase_pre": (_int, _FIRE_ARGS),
     "tsb_fire_vv_pre": (_int, _FIRE_ARGS),
@@ -168,6 +176,21 @@ def dtype_code(dtype: torch.dtype) -> int:
     if dtype == torch.float32:
         return F32
     raise TypeError(f"tsb kernels support float32/float64, got {dtype}")
+
+
+def pbc_rows(pbc, n_systems: int, device) -> torch.Tensor:
+    """Periodic flags as a contiguous uint8 [S, 3] tensor from a bool, a 0-d or
+    [3] tensor (every system alike), an [S, 3] tensor or a flat [3 S] one."""
+    p = torch.as_tensor(pbc, device=device)
+    if p.ndim == 0:
+        p = p.reshape(1).expand(3)
+    if p.ndim == 1 and p.shape[0] == 3:
+        p = p.unsqueeze(0).expand(n_systems, 3)
+    elif p.ndim == 1 and p.shape[0] == 3 * n_systems:
+        p = p.reshape(n_systems, 3)
+    if tuple(p.shape) != (n_systems, 3):
+        raise ValueError(f"pbc of shape {tuple(p.shape)} does not fit {n_systems} systems")
+    return p.to(torch.uint8).contiguous()
 
 
 def require_cuda(t: torch.Tensor, what: str = "tensor") -> None:

@@ -196,7 +196,7 @@ def make_problem(state, n_steps, dt, *, cutoff=8.5125, checkpoint_every=20, targ
     lut = torch.full((int(z.max()) + 1,), -1, dtype=torch.int32, device=state.device)
     lut[z] = torch.arange(len(z), dtype=torch.int32, device=state.device)
     n_sys = state.n_systems
-    pbc = state.pbc if state.pbc.ndim == 2 else state.pbc.unsqueeze(0).expand(n_sys, 3)
+    pbc = L.pbc_rows(state.pbc, n_sys, state.positions.device).bool()
     return TrajectoryProblem(cell_row=state.cell.mT.double().contiguous(),
                              pbc=pbc.to(torch.uint8).contiguous(),
                              system_idx=state.system_idx.contiguous(),

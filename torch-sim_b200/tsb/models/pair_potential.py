@@ -145,10 +145,7 @@ class PairTableModel(ModelInterface):
         dev, dt = pos.device, pos.dtype
         n, n_sys = pos.shape[0], state.n_systems
         cell_row = state.cell.mT.contiguous()
-        pbc = state.pbc
-        if pbc.ndim == 1:
-            pbc = pbc.unsqueeze(0).expand(n_sys, 3)
-        pbc = pbc.to(torch.uint8).contiguous()
+        pbc = L.pbc_rows(state.pbc, n_sys, dev)
         sys_idx = state.system_idx.contiguous()
         species = self._species(state.atomic_numbers)
         table = self.table if self.table.device == dev else self.table.to(dev)

@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import torch
 
+from .. import _lib as L
 from ..neighbors import full_to_half_list, torchsim_nl
 from .interface import ModelInterface
 from .pair_potential import PairTableModel
@@ -89,7 +90,7 @@ class PairForcesModel(ModelInterface):
         pos = state.positions
         n_sys = state.n_systems
         row_cell = state.cell.mT
-        pbc = state.pbc if state.pbc.ndim == 2 else state.pbc.unsqueeze(0).expand(n_sys, 3)
+        pbc = L.pbc_rows(state.pbc, n_sys, pos.device).bool()
         mapping, sysm, shifts = self.neighbor_list_fn(
             positions=pos, cell=row_cell, pbc=pbc, cutoff=self.cutoff,
             system_idx=state.system_idx)

@@ -1,11 +1,18 @@
-"""Verlet-list model wrapper for large periodic systems.
+"""Verlet-list model wrapper: neighbour lists kept between calls.
 
-``VerletListModel(model, skin=1.0)`` keeps the neighbour list (cutoff + skin) of
-one large fully periodic system between calls and rebuilds it only when an atom
-moved more than skin/2 (C ABI: tsb_verlet_build / tsb_verlet_check /
-tsb_verlet_forces).  The reference rebuilds its list in every call
-(torch_sim/models/pair_potential.py:168-174); the pairs within the cutoff, and
-therefore energy, forces and stress, are the same.
+``VerletListModel(model, skin=1.0)`` wraps a tsb ``PairTableModel`` (LJ, Morse,
+soft sphere).  Each system's list holds every pair within cutoff + skin and is
+rebuilt, per system, only when its atoms' drift and its cell's deformation since
+the build could have brought a pair from beyond cutoff + skin to inside the
+cutoff (C ABI: tsb_vlist_check / tsb_vlist_build / tsb_vlist_forces).  The
+reference rebuilds its list in every call (torch_sim/models/pair_potential.py:
+168-174); the pairs inside the cutoff, and therefore energy, forces and stress,
+are the same.  Works for one large system (500,000 atoms) and for batches of
+small ones whose atoms and cells move (FIRE with a cell filter, NPT, MD).
+
+Every periodic cell must be at least cutoff + skin wide (image shifts in
+{-1,0,1}^3); narrower cells raise ValueError.  The wrapper keeps its own device
+workspace (the list frame) and reads two flags from the device per call.
 """
 
 from __future__ import annotations
@@ -22,93 +29,131 @@ class VerletListModel(ModelInterface):
         super().__init__()
         if not isinstance(model, PairTableModel):
             raise TypeError("VerletListModel wraps a tsb PairTableModel")
+        if model.kind not in (L.POT_LJ, L.POT_MORSE, L.POT_SOFT):
+            raise TypeError("VerletListModel supports LJ, Morse and soft-sphere tables")
         self.model = model
         self._device, self._dtype = model.device, model.dtype
         self._compute_forces, self._compute_stress = True, model.compute_stress
+        self.per_atom_energies = getattr(model, "per_atom_energies", False)
+        self.per_atom_stresses = getattr(model, "per_atom_stresses", False)
         self.skin = float(skin)
         self.max_neighbors = int(max_neighbors)
         self.n_builds = 0
         self._key = None
 
-    def _ensure(self, state):
-        n = state.n_atoms
-        key = (n, state.positions.dtype, state.positions.device)
-        if self._key != key:
-            dev = state.device
-            rcs = self.model.cutoff + self.skin
-            vol = float(torch.det(state.cell[0].double()).abs())
-            est = int(4.2 * rcs ** 3 * n / vol * 1.35) + 16
-            self.cap = max(self.max_neighbors, est)
-            self.list = torch.empty(self.cap * n, dtype=torch.int32, device=dev)
-            self.counts = torch.empty(n, dtype=torch.int32, device=dev)
-            self.ref = torch.empty((n, 3), dtype=torch.float64, device=dev)
-            self.wraps = torch.empty((n, 3), dtype=torch.int32, device=dev)
-            self.status = torch.zeros(1, dtype=torch.int32, device=dev)
-            self.expired = torch.zeros(1, dtype=torch.int32, device=dev)
-            self.e_atom = torch.empty(n, dtype=torch.float64, device=dev)
-            self.vir_atom = torch.empty((n, 6), dtype=torch.float64, device=dev)
-            self.ws = torch.empty(L.load().tsb_verlet_workspace_size(n), dtype=torch.uint8,
-                                  device=dev)
-            self._key = key
-            self._built = False
+    # -------------------------------------------------------------- buffers
+    def _ensure(self, state, pos, cell_row):
+        n, ns = state.n_atoms, state.n_systems
+        sysi, z = state.system_idx, state.atomic_numbers
+        key = (n, ns, pos.dtype, pos.device, sysi.data_ptr(), sysi._version, z.data_ptr(),
+               z._version)
+        if self._key == key:
+            return
+        dev = pos.device
+        rcs = self.model.cutoff + self.skin
+        counts = torch.bincount(sysi, minlength=ns).double()
+        vol = torch.linalg.det(cell_row.double()).abs().clamp_min(1e-30)
+        dens = float((counts / vol).max())
+        est = int(4.19 * rcs ** 3 * dens * 1.35) + 16
+        if not (est < 4096):
+            est = 4096
+        self.cap = max(self.max_neighbors, est)
+        self.list = torch.empty(self.cap * n, dtype=torch.int32, device=dev)
+        self.counts = torch.empty(n, dtype=torch.int32, device=dev)
+        self.flags = torch.zeros(2, dtype=torch.int32, device=dev)
+        self.ws = torch.empty(L.load().tsb_vlist_workspace_size(n, ns), dtype=torch.uint8,
+                              device=dev)
+        self._reset(n, ns, dev)
+        self._key = key
 
-    def _check(self, state, pos, cell64):
-        L.call("tsb_verlet_check", L.ptr(pos), L.ptr(self.ref), L.ptr(self.wraps),
-               L.ptr(cell64), L.ptr(self.model._species(state.atomic_numbers)), state.n_atoms,
-               L.dtype_code(pos.dtype), self.skin, L.ptr(self.expired), L.ptr(self.ws),
-               self.ws.numel(), L.stream_ptr(state.device))
+    def _reset(self, n, ns, dev):
+        L.call("tsb_vlist_reset", n, ns, L.ptr(self.ws), self.ws.numel(), L.stream_ptr(dev))
 
-    def _build(self, state, pos):
-        cell = state.cell[0].mT.to(pos.dtype).contiguous()
+    # ---------------------------------------------------------------- lists
+    def _update_lists(self, state, pos, cell_row, pbc, sysi, species, active):
+        n, ns, dev = state.n_atoms, state.n_systems, pos.device
+        dt = L.dtype_code(pos.dtype)
+        cutoff = self.model.cutoff
         while True:
-            L.call("tsb_verlet_build", L.ptr(pos), L.ptr(cell), state.n_atoms,
-                   L.dtype_code(pos.dtype), self.model.cutoff, self.skin, L.ptr(self.list),
-                   L.ptr(self.counts), self.cap, L.ptr(self.ref), L.ptr(self.wraps),
-                   L.ptr(self.status), L.ptr(self.ws), self.ws.numel(),
-                   L.stream_ptr(state.device))
-            st = int(self.status.item())
+            L.call("tsb_vlist_check", L.ptr(pos), L.ptr(cell_row), L.ptr(sysi), L.ptr(active),
+                   n, ns, dt, cutoff, self.skin, L.ptr(self.flags), L.ptr(self.ws),
+                   self.ws.numel(), L.stream_ptr(dev))
+            if not int(self.flags[0].item()):
+                return
+            L.call("tsb_vlist_build", L.ptr(pos), L.ptr(cell_row), L.ptr(pbc), L.ptr(sysi),
+                   L.ptr(species), n, ns, dt, cutoff, self.skin, L.ptr(self.list),
+                   L.ptr(self.counts), self.cap, L.ptr(self.flags), L.ptr(self.ws),
+                   self.ws.numel(), L.stream_ptr(dev))
+            self.n_builds += 1
+            st = int(self.flags[1].item())
             if st == 0:
-                break
+                return
             if st >= (1 << 30):
-                raise ValueError("VerletListModel needs every cell width >= cutoff + skin")
+                raise ValueError("VerletListModel needs every periodic cell width >= "
+                                 "cutoff + skin")
+            # a list overflowed: regrow and rebuild every system
             self.cap = int(st * 1.2) + 8
-            self.list = torch.empty(self.cap * state.n_atoms, dtype=torch.int32,
-                                    device=state.device)
-        self.n_builds += 1
-        self._built = True
+            self.list = torch.empty(self.cap * n, dtype=torch.int32, device=dev)
+            self._reset(n, ns, dev)
 
-    def forward(self, state, **_kw):
-        if state.n_systems != 1:
-            raise ValueError("VerletListModel handles one large system")
-        if not bool(torch.as_tensor(state.pbc).all()):
-            raise ValueError("VerletListModel needs periodic boundaries on all axes")
+    def _run(self, state, energy, forces, stress, energies, stresses, active):
         if state.dtype != self._dtype:
             raise TypeError(f"SimState dtype {state.dtype} does not match model dtype "
                             f"{self._dtype}.")
-        self._ensure(state)
         pos = state.positions.contiguous()
-        cell64 = state.cell[0].mT.double().contiguous()
-        if not self._built:
-            self._build(state, pos)
-            self._check(state, pos, cell64)
-        else:
-            self._check(state, pos, cell64)
-            if int(self.expired.item()):
-                self._build(state, pos)
-                self._check(state, pos, cell64)
-        dt = pos.dtype
-        energy = torch.empty(1, dtype=dt, device=state.device)
-        forces = torch.empty_like(pos)
-        stress = (torch.empty((1, 3, 3), dtype=dt, device=state.device)
+        L.require_cuda(pos, "state.positions")
+        n_sys = state.n_systems
+        cell_row = state.cell.mT.contiguous()
+        pbc = L.pbc_rows(state.pbc, n_sys, pos.device)
+        sysi = state.system_idx.contiguous()
+        species = self.model._species(state.atomic_numbers)
+        self._ensure(state, pos, cell_row)
+        self._update_lists(state, pos, cell_row, pbc, sysi, species, active)
+        m = self.model
+        table = m.table if m.table.device == pos.device else m.table.to(pos.device)
+        flags = 0
+        if forces is not None:
+            flags |= L.OUT_FORCES
+        if stress is not None:
+            flags |= L.OUT_STRESS
+        if energies is not None:
+            flags |= L.OUT_ENERGIES
+        if stresses is not None:
+            flags |= L.OUT_STRESSES
+        if m.precision == "fp64":
+            flags |= L.MATH_FP64
+        L.call("tsb_vlist_forces", m.kind, L.ptr(table), m.n_species, L.ptr(species),
+               L.ptr(self.list), L.ptr(self.counts), L.ptr(pos), L.ptr(cell_row), L.ptr(sysi),
+               L.ptr(active), state.n_atoms, n_sys, L.dtype_code(pos.dtype), m.cutoff, flags,
+               L.ptr(energy), L.ptr(forces), L.ptr(stress), L.ptr(energies), L.ptr(stresses),
+               L.ptr(self.ws), self.ws.numel(), L.stream_ptr(pos.device))
+
+    # ------------------------------------------------------------------ API
+    def forward(self, state, **_kw) -> dict[str, torch.Tensor]:
+        dev, dt = state.positions.device, state.positions.dtype
+        n, n_sys = state.n_atoms, state.n_systems
+        energy = torch.empty(n_sys, dtype=dt, device=dev)
+        forces = torch.empty((n, 3), dtype=dt, device=dev)
+        stress = (torch.empty((n_sys, 3, 3), dtype=dt, device=dev)
                   if self._compute_stress else None)
-        flags = L.OUT_FORCES | (L.OUT_STRESS if stress is not None else 0)
-        table = self.model.table
-        L.call("tsb_verlet_forces", self.model.kind, L.ptr(table), self.model.n_species,
-               L.ptr(self.list), L.ptr(self.counts), state.n_atoms, L.ptr(cell64),
-               L.dtype_code(dt), self.model.cutoff, flags, L.ptr(energy), L.ptr(forces),
-               L.ptr(stress), L.ptr(self.e_atom), L.ptr(self.vir_atom), L.ptr(self.ws),
-               self.ws.numel(), L.stream_ptr(state.device))
+        energies = torch.empty(n, dtype=dt, device=dev) if self.per_atom_energies else None
+        stresses = (torch.empty((n, 3, 3), dtype=dt, device=dev)
+                    if self.per_atom_stresses else None)
+        self._run(state, energy, forces, stress, energies, stresses, None)
         out = {"energy": energy, "forces": forces}
         if stress is not None:
             out["stress"] = stress
+        if energies is not None:
+            out["energies"] = energies
+        if stresses is not None:
+            out["stresses"] = stresses
         return out
+
+    def forward_into(self, state, *, energy, forces, stress=None, sys_active=None):
+        """Write energy/forces(/stress) of the systems with ``sys_active`` != 0 into
+        existing contiguous buffers; the other systems' entries are left untouched."""
+        for t in (energy, forces, stress):
+            if t is not None and not t.is_contiguous():
+                raise ValueError("forward_into needs contiguous output buffers")
+        self._run(state, energy, forces, stress if self._compute_stress else None, None, None,
+                  sys_active)

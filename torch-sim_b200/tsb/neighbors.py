@@ -29,6 +29,8 @@ def _normalize(cell: torch.Tensor, pbc: torch.Tensor, n_systems: int):
         cell = (cell.unsqueeze(0).expand(n_systems, 3, 3) if cell.shape[0] == 3
                 else cell.reshape(n_systems, 3, 3))
     pbc = torch.as_tensor(pbc, device=cell.device)
+    if pbc.ndim == 0:
+        pbc = pbc.reshape(1).expand(3)
     if pbc.ndim == 1:
         pbc = (pbc.unsqueeze(0).expand(n_systems, 3) if pbc.shape[0] == 3
                else pbc.reshape(n_systems, 3))

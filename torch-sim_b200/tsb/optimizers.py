@@ -44,9 +44,7 @@ def _counts(state):
 def _eval_model(state, model, active=None):
     """Model forward writing into the state's buffers; systems with active == 0
     keep their previous forces/energy/stress."""
-    from .models.pair_potential import PairTableModel
-
-    if active is None or not isinstance(model, PairTableModel):
+    if active is None or not hasattr(model, "forward_into"):
         out = model(state)
         state.forces = out["forces"].contiguous()
         state.energy = out["energy"]
