@@ -76,7 +76,7 @@ def parse():
     ap.add_argument("--integrator", default="nvt_langevin",
                     choices=["nvt_langevin", "nvt_nose_hoover", "nvt_vrescale", "nve"],
                     help="batched_md: integrator inside the fused kernel and the plain path")
-    ap.add_argument("--list-skin", type=float, default=1.0,
+    ap.add_argument("--list-skin", type=float, default=1.5,
                     help="relax workload: Verlet-list skin in A (0 = cell-list search per call)")
     ap.add_argument("--workload", default="batched_md",
                     choices=["batched_md", "single_large", "relax", "adjoint"])
@@ -289,7 +289,7 @@ def run_single_large(args):
     t = sum(a.elapsed_time(b) for a, b in ev) / 1e3
     evals = n_steps * args.steps
     n = md.n_atoms
-    entries = int(vm.counts.sum())
+    entries = int(vm.list_counts.sum())
     # algorithmic bytes per evaluation: list (4 B/entry) + build-frame positions
     # (32 B) + forces (12 B) + per-atom energy/virial scratch (56 B)
     alg = 4 * entries + n * (32 + 12 + 56)

@@ -143,7 +143,8 @@ int tsb_md_baoab_boa(void *positions, void *momenta, const void *forces,
  *   cell_row in `dtype`.
  * tsb_verlet_check: maps the current positions into the build frame (kept in
  *   the workspace for tsb_verlet_forces) and sets *expired when any atom moved
- *   more than skin/2 (then rebuild and check again).  cell_row float64.
+ *   more than skin/2 or the cell differs from the build's (then rebuild and check
+ *   again).  cell_row float64.
  * tsb_verlet_forces: energy [1], forces [N,3] (dtype), stress [1,3,3] with
  *   TSB_OUT_STRESS; e_atom [N] and vir_atom [N,6] are float64 scratch.  Uses the
  *   workspace filled by tsb_verlet_check.  cell_row float64. */

@@ -175,3 +175,22 @@ def test_vlist_optimize_converges_like_cell_list():
         0, st.system_idx, out["forces"].norm(dim=1), reduce="amax")
     assert float(fmax.max()) < 1e-3
     assert vm.n_builds < steps
+
+
+def test_single_system_engine_expires_on_cell_change():
+    """One large periodic system takes the single-system kernels; a changed cell
+    (or a moved atom) rebuilds its list and the forces stay exact."""
+    from tsb import models, workloads
+    from tsb.state import state_from_arrays
+
+    st = state_from_arrays(workloads.argon_fcc((8, 8, 8), jitter=0.1, seed=2), device="cuda")
+    mk = lambda p: models.LennardJonesModel(sigma=3.405, epsilon=0.0104, cutoff=8.5,  # noqa
+                                            compute_stress=True, precision=p)
+    vm, ref = models.VerletListModel(mk("mixed"), skin=1.0), mk("fp64")
+    _cmp(vm(st), ref(st), 1e-5, ("forces", "stress"))
+    assert vm.n_builds == 1 and getattr(vm, "_s_built", False)
+    F = torch.eye(3, dtype=st.dtype, device="cuda") * 1.002
+    st.positions = (st.positions @ F.T).contiguous()
+    st.cell = (F @ st.cell[0]).unsqueeze(0).contiguous()
+    _cmp(vm(st), ref(st), 1e-5, ("forces", "stress"))
+    assert vm.n_builds == 2

@@ -24,6 +24,7 @@ struct VerletWork {
   BinData b;
   double4 *wpos;  // [N] current positions in the build frame (FP64), .w = species bits
   uint8_t *pbc;   // [3] all periodic
+  double *cell0;  // [9] cell of the last build (a changed cell expires the list)
   int64_t *sys;   // [N] single system
   double *part;   // [7 * blocks] per-block energy / virial sums of the force kernel
 };
@@ -32,6 +33,7 @@ static void carve_verlet(Carver &c, VerletWork &w, int64_t n) {
   carve_bins(c, w.b, n, 1);
   w.wpos = c.take<double4>(n);
   w.pbc = c.take<uint8_t>(16);
+  w.cell0 = c.take<double>(9);
   w.sys = c.take<int64_t>(n);
   w.part = c.take<double>(7 * ((n + kVerletBlock - 1) / kVerletBlock));
 }
@@ -67,7 +69,8 @@ __global__ void k_verlet_build(BinData b, int64_t n, double rcs2, uint32_t *list
 template <class P>
 __global__ void k_verlet_frame(const P *pos, const double *ref, const int32_t *wrap,
                                const double *cell, const int32_t *species, int64_t n,
-                               double half_skin2, double4 *wpos, int32_t *expired) {
+                               double half_skin2, const double *cell0, double4 *wpos,
+                               int32_t *expired) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double x0 = (double)pos[3 * i], x1 = (double)pos[3 * i + 1], x2 = (double)pos[3 * i + 2];
@@ -80,6 +83,10 @@ __global__ void k_verlet_frame(const P *pos, const double *ref, const int32_t *w
   wpos[i] = w;
   const double d0 = x0 - ref[3 * i], d1 = x1 - ref[3 * i + 1], d2 = x2 - ref[3 * i + 2];
   if (d0 * d0 + d1 * d1 + d2 * d2 > half_skin2) atomicOr(expired, 1);
+  // the list's images belong to the build cell: any change of the cell expires it
+  if (i == 0)
+    for (int k = 0; k < 9; ++k)
+      if (cell[k] != cell0[k]) atomicOr(expired, 1);
 }
 
 template <int POT, class P>
@@ -219,9 +226,10 @@ __global__ void k_verlet_final(const double *part, int64_t n_blocks, int flags,
 }
 
 template <class P>
-__global__ void k_copy_ref(const P *pos, double *ref, int64_t n) {
+__global__ void k_copy_ref(const P *pos, double *ref, int64_t n, const P *cell, double *cell0) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < 3 * n) ref[i] = (double)pos[i];
+  if (i < 9) cell0[i] = (double)cell[i];
 }
 
 }  // namespace tsb
@@ -260,12 +268,16 @@ extern "C" int tsb_verlet_build(const void *positions, const void *cell_row, int
     TSB_TRY(prepare_bins<double>((const double *)positions, (const double *)cell_row, pbc, sys,
                                  n_atoms, 1, rcs, w.b, st));
     k_copy_ref<double><<<grid_for(3 * n_atoms), kBlock, 0, st>>>((const double *)positions,
-                                                                 ref_positions, n_atoms);
+                                                                 ref_positions, n_atoms,
+                                                                 (const double *)cell_row,
+                                                                 w.cell0);
   } else {
     TSB_TRY(prepare_bins<float>((const float *)positions, (const float *)cell_row, pbc, sys,
                                 n_atoms, 1, rcs, w.b, st));
     k_copy_ref<float><<<grid_for(3 * n_atoms), kBlock, 0, st>>>((const float *)positions,
-                                                                ref_positions, n_atoms);
+                                                                ref_positions, n_atoms,
+                                                                (const float *)cell_row,
+                                                                w.cell0);
   }
   k_verlet_build<<<grid_for(n_atoms, 128), 128, 0, st>>>(w.b, n_atoms, rcs * rcs, list, counts,
                                                          max_neighbors, status, wraps);
@@ -290,11 +302,11 @@ extern "C" int tsb_verlet_check(const void *positions, const double *ref_positio
   if (dtype == TSB_F64)
     k_verlet_frame<double><<<grid_for(n_atoms), kBlock, 0, st>>>(
         (const double *)positions, ref_positions, wraps, cell_row, species, n_atoms, hs2,
-        w.wpos, expired);
+        w.cell0, w.wpos, expired);
   else if (dtype == TSB_F32)
     k_verlet_frame<float><<<grid_for(n_atoms), kBlock, 0, st>>>(
         (const float *)positions, ref_positions, wraps, cell_row, species, n_atoms, hs2,
-        w.wpos, expired);
+        w.cell0, w.wpos, expired);
   else
     return TSB_ERR_INVALID_ARG;
   TSB_CHECK_LAUNCH();

@@ -13,6 +13,12 @@ small ones whose atoms and cells move (FIRE with a cell filter, NPT, MD).
 Every periodic cell must be at least cutoff + skin wide (image shifts in
 {-1,0,1}^3); narrower cells raise ValueError.  The wrapper keeps its own device
 workspace (the list frame) and reads two flags from the device per call.
+
+One fully periodic system with FP32 pair arithmetic and no per-atom outputs (the
+500,000-atom workload) takes the single-system kernels (tsb_verlet_build /
+tsb_verlet_check / tsb_verlet_forces: atom order, per-block sums fused into the
+force kernel), about 10 % faster there; its list expires when an atom moved more
+than skin/2 or the cell changed.
 """
 
 from __future__ import annotations
@@ -40,6 +46,7 @@ class VerletListModel(ModelInterface):
         self.max_neighbors = int(max_neighbors)
         self.n_builds = 0
         self._key = None
+        self._last_single = False
 
     # -------------------------------------------------------------- buffers
     def _ensure(self, state, pos, cell_row):
@@ -128,8 +135,111 @@ class VerletListModel(ModelInterface):
                L.ptr(energy), L.ptr(forces), L.ptr(stress), L.ptr(energies), L.ptr(stresses),
                L.ptr(self.ws), self.ws.numel(), L.stream_ptr(pos.device))
 
+    # ------------------------------------------------- one large system
+    def _single_ok(self, state):
+        if (state.n_systems != 1 or self.model.precision == "fp64" or self.per_atom_energies
+                or self.per_atom_stresses):
+            return False
+        pbc = state.pbc
+        key = (pbc.data_ptr(), pbc._version) if isinstance(pbc, torch.Tensor) else bool(pbc)
+        if getattr(self, "_pbc_key", None) != key:  # one device read per pbc tensor
+            self._pbc_key = key
+            self._pbc_all = bool(L.pbc_rows(pbc, 1, state.positions.device).all())
+        return self._pbc_all
+
+    def _s_ensure(self, state):
+        n = state.n_atoms
+        key = (n, state.positions.dtype, state.positions.device)
+        if getattr(self, "_s_key", None) == key:
+            return
+        dev = state.device
+        rcs = self.model.cutoff + self.skin
+        vol = float(torch.det(state.cell[0].double()).abs())
+        est = int(4.2 * rcs ** 3 * n / vol * 1.35) + 16
+        self.s_cap = max(self.max_neighbors, est)
+        self.s_list = torch.empty(self.s_cap * n, dtype=torch.int32, device=dev)
+        self.s_counts = torch.empty(n, dtype=torch.int32, device=dev)
+        self.s_ref = torch.empty((n, 3), dtype=torch.float64, device=dev)
+        self.s_wraps = torch.empty((n, 3), dtype=torch.int32, device=dev)
+        self.s_status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.s_expired = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.s_e_atom = torch.empty(n, dtype=torch.float64, device=dev)
+        self.s_vir_atom = torch.empty((n, 6), dtype=torch.float64, device=dev)
+        self.s_ws = torch.empty(L.load().tsb_verlet_workspace_size(n), dtype=torch.uint8,
+                                device=dev)
+        self._s_key = key
+        self._s_built = False
+
+    def _s_check(self, state, pos, cell64):
+        L.call("tsb_verlet_check", L.ptr(pos), L.ptr(self.s_ref), L.ptr(self.s_wraps),
+               L.ptr(cell64), L.ptr(self.model._species(state.atomic_numbers)), state.n_atoms,
+               L.dtype_code(pos.dtype), self.skin, L.ptr(self.s_expired), L.ptr(self.s_ws),
+               self.s_ws.numel(), L.stream_ptr(state.device))
+
+    def _s_build(self, state, pos):
+        cell = state.cell[0].mT.to(pos.dtype).contiguous()
+        while True:
+            L.call("tsb_verlet_build", L.ptr(pos), L.ptr(cell), state.n_atoms,
+                   L.dtype_code(pos.dtype), self.model.cutoff, self.skin, L.ptr(self.s_list),
+                   L.ptr(self.s_counts), self.s_cap, L.ptr(self.s_ref), L.ptr(self.s_wraps),
+                   L.ptr(self.s_status), L.ptr(self.s_ws), self.s_ws.numel(),
+                   L.stream_ptr(state.device))
+            st = int(self.s_status.item())
+            if st == 0:
+                break
+            if st >= (1 << 30):
+                raise ValueError("VerletListModel needs every periodic cell width >= "
+                                 "cutoff + skin")
+            self.s_cap = int(st * 1.2) + 8
+            self.s_list = torch.empty(self.s_cap * state.n_atoms, dtype=torch.int32,
+                                      device=state.device)
+        self.n_builds += 1
+        self._s_built = True
+
+    def _single_forward(self, state):
+        if state.dtype != self._dtype:
+            raise TypeError(f"SimState dtype {state.dtype} does not match model dtype "
+                            f"{self._dtype}.")
+        L.require_cuda(state.positions, "state.positions")
+        self._s_ensure(state)
+        pos = state.positions.contiguous()
+        cell64 = state.cell[0].mT.double().contiguous()
+        if not self._s_built:
+            self._s_build(state, pos)
+            self._s_check(state, pos, cell64)
+        else:
+            self._s_check(state, pos, cell64)
+            if int(self.s_expired.item()):
+                self._s_build(state, pos)
+                self._s_check(state, pos, cell64)
+        dt = pos.dtype
+        energy = torch.empty(1, dtype=dt, device=state.device)
+        forces = torch.empty_like(pos)
+        stress = (torch.empty((1, 3, 3), dtype=dt, device=state.device)
+                  if self._compute_stress else None)
+        flags = L.OUT_FORCES | (L.OUT_STRESS if stress is not None else 0)
+        m = self.model
+        L.call("tsb_verlet_forces", m.kind, L.ptr(m.table), m.n_species, L.ptr(self.s_list),
+               L.ptr(self.s_counts), state.n_atoms, L.ptr(cell64), L.dtype_code(dt), m.cutoff,
+               flags, L.ptr(energy), L.ptr(forces), L.ptr(stress), L.ptr(self.s_e_atom),
+               L.ptr(self.s_vir_atom), L.ptr(self.s_ws), self.s_ws.numel(),
+               L.stream_ptr(state.device))
+        out = {"energy": energy, "forces": forces}
+        if stress is not None:
+            out["stress"] = stress
+        return out
+
     # ------------------------------------------------------------------ API
+    @property
+    def list_counts(self) -> torch.Tensor:
+        """Neighbour-list entries per atom (slot order on the batched path) of the
+        engine used by the last call."""
+        return self.s_counts if self._last_single else self.counts
+
     def forward(self, state, **_kw) -> dict[str, torch.Tensor]:
+        self._last_single = self._single_ok(state)
+        if self._last_single:
+            return self._single_forward(state)
         dev, dt = state.positions.device, state.positions.dtype
         n, n_sys = state.n_atoms, state.n_systems
         energy = torch.empty(n_sys, dtype=dt, device=dev)
@@ -155,5 +265,6 @@ class VerletListModel(ModelInterface):
         for t in (energy, forces, stress):
             if t is not None and not t.is_contiguous():
                 raise ValueError("forward_into needs contiguous output buffers")
+        self._last_single = False
         self._run(state, energy, forces, stress if self._compute_stress else None, None, None,
                   sys_active)
