@@ -407,7 +407,7 @@ def run_adjoint(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (256 x fcc 3x3x3 argon, two species 50:50)",
             "config": {"workload": "adjoint", "systems": 256, "atoms": n, "md_steps": 200,
-                       "checkpoint_every": 20, "forward_atom_steps_per_s": n * 200 / t,
+                       "checkpoint_every": 20, "atom_steps_per_s_incl_adjoint": n * 200 / t,
                        "loss": float(loss)},
             "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)

@@ -32,6 +32,9 @@ static void carve_adj(Carver &c, AdjWork &w, int64_t n, int64_t ns, int64_t per_
 //   V'  = -(24 eps / r)(2 s^12 - s^6)
 //   V'' = (24 eps / r^2)(26 s^12 - 7 s^6)
 //   dV'/deps = V' / eps ;  dV'/dsigma = -(144 eps / (r sigma))(4 s^12 - s^6)
+// LANES > 1: LANES lanes per atom (small batches; fixed-order reduction of the lanes'
+// partial sums), LANES = 1: one thread per atom.
+template <int LANES>
 __global__ void __launch_bounds__(128)
     k_lj_hvp(BinData b, int64_t n, const double *__restrict__ table, int nsp,
              const int32_t *__restrict__ species, double cutoff, const double *__restrict__ v,
@@ -45,7 +48,8 @@ __global__ void __launch_bounds__(128)
     rc2[k] = r * r;
   }
   __syncthreads();
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t p = t / LANES;
   if (p >= n) return;
   const double4 w = b.spos[p];
   const int i = tag_atom(w.w);
@@ -55,8 +59,7 @@ __global__ void __launch_bounds__(128)
   double hx = 0, hy = 0, hz = 0;
   double gs[kAdjMaxSpecies * kAdjMaxSpecies], ge[kAdjMaxSpecies * kAdjMaxSpecies];
   for (int k = 0; k < nsp * nsp; ++k) gs[k] = ge[k] = 0.0;
-  search_neighbors(G, b.spos, b.bin_start, i, w.x, w.y, w.z, cutoff * cutoff, false,
-                   [&](int j, int, int, int, double dx, double dy, double dz, double d2) {
+  auto pair = [&](int j, int, int, int, double dx, double dy, double dz, double d2, int) {
                      const int sj = species ? min(max(species[j], 0), nsp - 1) : 0;
                      const int k = si * nsp + sj;
                      if (!(d2 < rc2[k]) || !(d2 > 0.0)) return;
@@ -75,7 +78,22 @@ __global__ void __launch_bounds__(128)
                      const double uvi = ux * vi0 + uy * vi1 + uz * vi2;
                      ge[k] += (vp / e) * uvi;
                      gs[k] += (-(144.0 * e * ir / sig[k]) * (4.0 * s12 - s6)) * uvi;
-                   });
+                   };
+  if constexpr (LANES > 1) {
+    group_search_neighbors<LANES>(G, b.spos, b.bin_start, i, w.x, w.y, w.z, cutoff * cutoff, false,
+                          pair);
+    hx = group_sum<LANES>(hx);
+    hy = group_sum<LANES>(hy);
+    hz = group_sum<LANES>(hz);
+    for (int k = 0; k < kAdjMaxSpecies * kAdjMaxSpecies; ++k) {
+      if (k >= nsp * nsp) break;
+      gs[k] = group_sum<LANES>(gs[k]);
+      ge[k] = group_sum<LANES>(ge[k]);
+    }
+    if ((threadIdx.x & (LANES - 1)) != 0) return;
+  } else {
+    search_neighbors(G, b.spos, b.bin_start, i, w.x, w.y, w.z, cutoff * cutoff, false, pair);
+  }
   // J_F^T v = -H v
   lam_q[3 * i] -= coef * hx;
   lam_q[3 * i + 1] -= coef * hy;
@@ -182,8 +200,12 @@ extern "C" int tsb_lj_hvp(const double *table, int n_species, const int32_t *spe
   cudaStream_t st = (cudaStream_t)stream;
   TSB_TRY(prepare_bins<double>(positions, cell_row, pbc, system_idx, n_atoms, n_systems, cutoff,
                                w.b, st));
-  k_lj_hvp<<<grid_for(n_atoms, 128), 128, 0, st>>>(w.b, n_atoms, table, n_species, species,
-                                                   cutoff, v, coef, lam_q, w.part);
+  if (n_atoms <= kGroupSearchMaxAtoms)
+    k_lj_hvp<kSearchGroup><<<grid_for(kSearchGroup * n_atoms, 128), 128, 0, st>>>(
+        w.b, n_atoms, table, n_species, species, cutoff, v, coef, lam_q, w.part);
+  else
+    k_lj_hvp<1><<<grid_for(n_atoms, 128), 128, 0, st>>>(
+        w.b, n_atoms, table, n_species, species, cutoff, v, coef, lam_q, w.part);
   // per-system parameter gradients, accumulated into grad_params [S, ns, ns, 2]
   k_sum_parts<<<(unsigned)n_systems, 64, 0, st>>>(w.b.geom, w.part, per_atom, grad_params, 1);
   TSB_CHECK_LAUNCH();

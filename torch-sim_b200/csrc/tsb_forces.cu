@@ -14,7 +14,9 @@
 
 namespace tsb {
 
-template <int POT, class R, class P>
+// LANES > 1: LANES lanes per atom (small batches; lanes split the candidates and the
+// partial sums are reduced in a fixed order), LANES = 1: one thread per atom.
+template <int POT, class R, class P, int LANES>
 __global__ void __launch_bounds__(128)
     k_pair_forces(BinData b, int64_t n, const double *__restrict__ table, int ns_species,
                   const int32_t *__restrict__ species, double cutoff, int flags, P *forces,
@@ -27,7 +29,8 @@ __global__ void __launch_bounds__(128)
     prc2[k] = pair_rc2(POT, table + 5 * k, cutoff);
   }
   __syncthreads();
-  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t p = t / LANES;
   if (p >= n) return;
   const double4 w = b.spos[p];
   const int i = tag_atom(w.w);
@@ -39,8 +42,7 @@ __global__ void __launch_bounds__(128)
   // forces accumulate in R; energy and virial in FP64 (per-system sums in FP64)
   R fx = 0, fy = 0, fz = 0;
   double ei = 0, vxx = 0, vyy = 0, vzz = 0, vyz = 0, vxz = 0, vxy = 0;
-  search_neighbors(G, b.spos, b.bin_start, i, w.x, w.y, w.z, cutoff * cutoff, false,
-                   [&](int, int, int, int, double dx, double dy, double dz, double d2,
+  auto pair = [&](int, int, int, int, double dx, double dy, double dz, double d2,
                        int sp) {
                      const int sj = min(max(sp, 0), ns_species - 1);
                      if (!(d2 < prc2[si * ns_species + sj])) return;  // FP64 decision
@@ -71,7 +73,24 @@ __global__ void __launch_bounds__(128)
                      vyz += vw * (double)(ry * gz);
                      vxz += vw * (double)(rx * gz);
                      vxy += vw * (double)(rx * gy);
-                   });
+                   };
+  if constexpr (LANES > 1) {
+    group_search_neighbors<LANES>(G, b.spos, b.bin_start, i, w.x, w.y, w.z, cutoff * cutoff, false,
+                          pair);
+    fx = group_sum<LANES>(fx);
+    fy = group_sum<LANES>(fy);
+    fz = group_sum<LANES>(fz);
+    ei = group_sum<LANES>(ei);
+    vxx = group_sum<LANES>(vxx);
+    vyy = group_sum<LANES>(vyy);
+    vzz = group_sum<LANES>(vzz);
+    vyz = group_sum<LANES>(vyz);
+    vxz = group_sum<LANES>(vxz);
+    vxy = group_sum<LANES>(vxy);
+    if ((threadIdx.x & (LANES - 1)) != 0) return;
+  } else {
+    search_neighbors(G, b.spos, b.bin_start, i, w.x, w.y, w.z, cutoff * cutoff, false, pair);
+  }
   if (flags & TSB_OUT_FORCES) {
     forces[3 * i] = (P)fx;
     forces[3 * i + 1] = (P)fy;
@@ -118,9 +137,14 @@ template <int POT, class R, class P>
 static void launch_forces(PairWork &w, int64_t n, const double *table, int nsp,
                           const int32_t *species, double cutoff, int flags, P *forces,
                           P *energies, P *stresses, const uint8_t *active, cudaStream_t st) {
-  k_pair_forces<POT, R, P><<<grid_for(n, 128), 128, 0, st>>>(
-      w.b, n, table, nsp, species, cutoff, flags, forces, energies, stresses, w.e_half,
-      w.vir_half, active);
+  if (n <= kGroupSearchMaxAtoms)
+    k_pair_forces<POT, R, P, kSearchGroup><<<grid_for(kSearchGroup * n, 128), 128, 0, st>>>(
+        w.b, n, table, nsp, species, cutoff, flags, forces, energies, stresses, w.e_half,
+        w.vir_half, active);
+  else
+    k_pair_forces<POT, R, P, 1><<<grid_for(n, 128), 128, 0, st>>>(
+        w.b, n, table, nsp, species, cutoff, flags, forces, energies, stresses, w.e_half,
+        w.vir_half, active);
 }
 
 template <class P>

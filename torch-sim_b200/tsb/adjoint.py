@@ -70,13 +70,14 @@ def _ws(dev, n, s, per_atom):
     return L.Workspace.get(dev, L.load().tsb_adjoint_workspace_size(n, s, per_atom))
 
 
-def forces(q, table, P: TrajectoryProblem):
+def forces(q, table, P: TrajectoryProblem, ws=None):
     """FP64 LJ energy [S] and forces [N,3] (tsb_pair_forward, FP64 pair math)."""
     dev = q.device
     n, s = P.n_atoms, P.n_systems
     e = torch.empty(s, dtype=torch.float64, device=dev)
     f = torch.empty((n, 3), dtype=torch.float64, device=dev)
-    ws = L.Workspace.get(dev, L.load().tsb_pair_workspace_size(n, s))
+    if ws is None:
+        ws = L.Workspace.get(dev, L.load().tsb_pair_workspace_size(n, s))
     L.call("tsb_pair_forward", L.POT_LJ, L.ptr(table), P.n_species, L.ptr(P.species), L.ptr(q),
            L.ptr(P.cell_row), L.ptr(P.pbc), L.ptr(P.system_idx), n, s, L.F64, P.cutoff,
            L.OUT_FORCES | L.MATH_FP64, L.ptr(e), L.ptr(f), None, None, None, None, L.ptr(ws),
@@ -102,25 +103,144 @@ def _hist_grad(q, dl_dh, P):
     return g
 
 
-def _hvp(q, table, v, coef, lam_q, gparams, P):
-    ws = _ws(q.device, P.n_atoms, P.n_systems, 2 * P.n_species ** 2)
+def _hvp(q, table, v, coef, lam_q, gparams, P, ws=None):
+    if ws is None:
+        ws = _ws(q.device, P.n_atoms, P.n_systems, 2 * P.n_species ** 2)
     L.call("tsb_lj_hvp", L.ptr(table), P.n_species, L.ptr(P.species), L.ptr(q),
            L.ptr(P.cell_row), L.ptr(P.pbc), L.ptr(P.system_idx), P.n_atoms, P.n_systems,
            P.cutoff, L.ptr(v), float(coef), L.ptr(lam_q), L.ptr(gparams), L.ptr(ws),
            ws.numel(), L.stream_ptr(q.device))
 
 
-def _vv_step(q, p, f, table, P, inv_m):
+def _vv_step(q, p, f, table, P, inv_m, ws=None):
     """One velocity-Verlet step (same floating-point order as nve.py:118-130)."""
     dt = P.dt
     p = p + f * (dt / 2)
     q = q + (p * inv_m) * dt
-    _, f = forces(q, table, P)
+    _, f = forces(q, table, P, ws)
     p = p + f * (dt / 2)
     return q, p, f
 
 
-def integrate(q0, p0, table, P: TrajectoryProblem, keep_checkpoints=True):
+class _Graphs:
+    """CUDA graphs of the checkpoint segments of one problem.
+
+    A segment of ``length`` steps is (a) forces at its first positions, then
+    ``length`` velocity-Verlet steps keeping the positions of each step, and (b)
+    the adjoint sweep back over those positions.  Every call in them (the C-ABI
+    force / HVP launches and torch element-wise ops) is stream-ordered and
+    allocates nothing once its workspace exists, so each part is captured once
+    and replayed: one graph launch per segment instead of some forty host calls
+    per step.  The graphs read and write the static buffers below; results are
+    bitwise those of the step-by-step path (forces are recomputed at a segment
+    start, from the same positions, by the same deterministic kernels)."""
+
+    def __init__(self, P: TrajectoryProblem, table: torch.Tensor):
+        dev = P.cell_row.device
+        n, f64 = P.n_atoms, torch.float64
+        self.P = P
+        self.table = table.clone().contiguous()
+        self.q0 = torch.zeros((n, 3), dtype=f64, device=dev)
+        self.p0 = torch.zeros_like(self.q0)
+        self.lam_q = torch.zeros_like(self.q0)
+        self.lam_p = torch.zeros_like(self.q0)
+        self.gpar = torch.zeros((P.n_systems, P.n_species, P.n_species, 2), dtype=f64,
+                                device=dev)
+        self.inv_m = (1.0 / P.masses).unsqueeze(-1)
+        lib = L.load()
+        self.ws_pair = torch.empty(lib.tsb_pair_workspace_size(n, P.n_systems),
+                                   dtype=torch.uint8, device=dev)
+        self.ws_adj = torch.empty(
+            lib.tsb_adjoint_workspace_size(n, P.n_systems, 2 * P.n_species ** 2),
+            dtype=torch.uint8, device=dev)
+        self.fwd, self.bwd, self.out = {}, {}, {}
+
+    @staticmethod
+    def _capture(body, keep=()):
+        """Warm ``body`` up once, then capture it.  The warm-up really runs, so the
+        buffers in ``keep`` (state that ``body`` updates in place) are restored
+        after it."""
+        saved = [t.clone() for t in keep]
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            body()  # warm-up outside the capture
+        torch.cuda.current_stream().wait_stream(side)
+        for t, v in zip(keep, saved):
+            t.copy_(v)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            body()
+        return g
+
+    def forward(self, length):
+        """Replay: (q0, p0) -> positions of each step and (q, p) after ``length``."""
+        if length not in self.fwd:
+            P = self.P
+
+            def body():
+                q, p = self.q0, self.p0
+                _, f = forces(q, self.table, P, self.ws_pair)
+                seg = [q]
+                for k in range(length):
+                    q, p, f = _vv_step(q, p, f, self.table, P, self.inv_m, self.ws_pair)
+                    if k < length - 1:
+                        seg.append(q)
+                self.out[length] = (seg, q, p)
+
+            self.fwd[length] = self._capture(body)
+        self.fwd[length].replay()
+        return self.out[length]
+
+    def backward(self, length, first):
+        """Replay the adjoint sweep over the positions of the last ``forward(length)``
+        (``first``: the segment holds step 0, whose coefficient is dt / 2)."""
+        key = (length, first)
+        if key not in self.bwd:
+            P = self.P
+            seg = self.out[length][0]
+
+            def body():
+                for k in range(length - 1, -1, -1):
+                    self.lam_p.add_(self.lam_q * (P.dt * self.inv_m))
+                    coef = P.dt / 2 if (first and k == 0) else P.dt
+                    _hvp(seg[k], self.table, self.lam_p, coef, self.lam_q, self.gpar, P,
+                         self.ws_adj)
+
+            self.bwd[key] = self._capture(body, keep=(self.lam_q, self.lam_p, self.gpar))
+        self.bwd[key].replay()
+
+
+def _graphs_for(P: TrajectoryProblem, table: torch.Tensor) -> _Graphs:
+    G = P.__dict__.get("_graphs")
+    if G is None:
+        G = _Graphs(P, table)
+        P.__dict__["_graphs"] = G
+    else:
+        G.table.copy_(table)
+    return G
+
+
+def _integrate_graphs(q0, p0, table, P, keep_checkpoints):
+    G = _graphs_for(P, table)
+    G.q0.copy_(q0)
+    G.p0.copy_(p0)
+    ckpt = {}
+    for c in range(0, P.n_steps, P.checkpoint_every):
+        if keep_checkpoints:
+            ckpt[c] = (G.q0.clone(), G.p0.clone())
+        _, q, p = G.forward(min(P.checkpoint_every, P.n_steps - c))
+        G.q0.copy_(q)
+        G.p0.copy_(p)
+    return G.q0.clone(), G.p0.clone(), ckpt
+
+
+def integrate(q0, p0, table, P: TrajectoryProblem, keep_checkpoints=True, use_graphs=True):
+    """Velocity Verlet for ``P.n_steps`` steps from (q0, p0); returns (q_T, p_T, and
+    the checkpoints {step: (q, p)} every ``P.checkpoint_every`` steps).  With
+    ``use_graphs`` each checkpoint segment replays one CUDA graph."""
+    if use_graphs and q0.is_cuda and P.n_steps > 0:
+        return _integrate_graphs(q0, p0, table, P, keep_checkpoints)
     inv_m = (1.0 / P.masses).unsqueeze(-1)
     q, p = q0.contiguous(), p0.contiguous()
     _, f = forces(q, table, P)
@@ -137,12 +257,33 @@ def loss_of(q_T, P):
     return ((h - P.target) ** 2).sum(), h
 
 
-def loss_and_grad(sigma, epsilon, q0, p0, P: TrajectoryProblem):
+def _adjoint_graphs(table, ckpt, lam_q, P):
+    """The backward sweep with one forward and one adjoint graph replay per segment."""
+    G = _graphs_for(P, table)
+    G.lam_q.copy_(lam_q)
+    G.lam_p.zero_()
+    G.gpar.zero_()
+    for c in sorted(ckpt, reverse=True):
+        length = min(P.checkpoint_every, P.n_steps - c)
+        G.q0.copy_(ckpt[c][0])
+        G.p0.copy_(ckpt[c][1])
+        G.forward(length)
+        G.backward(length, c == 0)
+    return G.lam_q.clone(), G.lam_p.clone(), G.gpar.clone()
+
+
+def loss_and_grad(sigma, epsilon, q0, p0, P: TrajectoryProblem, use_graphs=True):
     """Loss and its gradients w.r.t. sigma [ns,ns], epsilon [ns,ns], q0, p0."""
     table = lj_table(sigma, epsilon)
-    qT, pT, ckpt = integrate(q0, p0, table, P)
+    qT, pT, ckpt = integrate(q0, p0, table, P, use_graphs=use_graphs)
     loss, h = loss_of(qT, P)
     lam_q = _hist_grad(qT, 2.0 * (h - P.target), P)
+    if use_graphs and q0.is_cuda and P.n_steps > 0:
+        lam_q, lam_p, gpar = _adjoint_graphs(table, ckpt, lam_q, P)
+        g = gpar.sum(0)
+        gs = g[..., 0] + g[..., 0].T - torch.diag(torch.diagonal(g[..., 0]))
+        ge = g[..., 1] + g[..., 1].T - torch.diag(torch.diagonal(g[..., 1]))
+        return loss, gs, ge, lam_q, lam_p
     lam_p = torch.zeros_like(lam_q)
     gpar = torch.zeros((P.n_systems, P.n_species, P.n_species, 2), dtype=torch.float64,
                        device=q0.device)
