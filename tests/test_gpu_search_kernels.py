@@ -1,6 +1,6 @@
-"""The cell-list kernels come in two shapes: one warp per atom for batches of at
-most 65,536 atoms (enough warps to hide the search latency) and one thread per
-atom above that.  The same systems computed once as a large batch and once as
+"""The cell-list kernels come in two shapes: a group of lanes per atom for
+batches of at most 65,536 atoms (enough warps to hide the search latency) and
+one thread per atom above that.  The same systems computed once as a large batch and once as
 two small ones must agree to FP64 rounding (max|d|/max|ref| <= 1e-10)."""
 
 import numpy as np
@@ -34,7 +34,7 @@ def test_pair_forces_warp_and_thread_kernels_agree():
     big = m(st)  # one thread per atom
     a, b = _split(st, 150)
     assert a.n_atoms <= 65536 and b.n_atoms <= 65536
-    oa, ob = m(a), m(b)  # one warp per atom
+    oa, ob = m(a), m(b)  # a group of lanes per atom
     for k in ("forces", "energies"):
         assert _rel(torch.cat([oa[k], ob[k]]), big[k]) < 1e-10, k
     for k in ("energy", "stress"):
