@@ -171,10 +171,10 @@ int tsb_verlet_forces(int potential, const double *table, int n_species,
  * and cells change between calls (FIRE with a cell filter, NPT, MD).  Each
  * system's list holds every pair within cutoff + skin (image shifts in
  * {-1,0,1}^3 of the cell at its build) and is rebuilt, per system, when
- * 2 D + c > skin or 2 D + 2 c > w_min - cutoff (D: largest drift of an atom in
- * the build frame, c: sum of the norms of the periodic cell rows' change since
- * the build, w_min: smallest periodic plane spacing at the build).  The pairs
- * inside the cutoff, hence energy, forces and stresses, equal the per-call path.
+ * 2 max|u| + (cutoff + skin) |F - I| > skin (F = C0^-1 C the cell deformation
+ * since the build, u_i = w_i - w0_i F an atom's non-affine drift in the build
+ * frame).  The pairs inside the cutoff, hence energy, forces and stresses, equal
+ * the per-call path.
  * The workspace (tsb_vlist_workspace_size) holds the list frame and must be kept
  * by the caller between calls; tsb_vlist_reset marks every system unbuilt.
  * tsb_vlist_check: flags[0] = 1 when any active system must be rebuilt.

@@ -59,14 +59,18 @@ def test_vlist_moving_atoms_and_cells_rebuild_only_when_needed():
         st.cell = torch.einsum("nij,njk->nik", F, st.cell).contiguous()
         _cmp(vm(st), ref(st), 1e-10)
     assert vm.n_builds == 1
-    # a 3 % strain of one system: its list expires (and only it is rebuilt)
-    F = eye.repeat(st.n_systems, 1, 1)
-    F[4] += 0.03 * torch.tensor([[1.0, 0.2, 0.0], [0.2, -0.5, 0.0], [0.0, 0.0, 0.4]],
-                                device="cuda", dtype=st.dtype)
-    st.positions = torch.einsum("nij,nj->ni", F[st.system_idx], st.positions).contiguous()
-    st.cell = torch.einsum("nij,njk->nik", F, st.cell).contiguous()
-    _cmp(vm(st), ref(st), 1e-10)
-    assert vm.n_builds == 2
+    # a uniform 3 % strain of one system moves no atom off its affine image: the
+    # list stays valid ((cutoff + skin) |F - I| < skin); a 12 % strain expires it
+    shape = torch.tensor([[1.0, 0.2, 0.0], [0.2, -0.5, 0.0], [0.0, 0.0, 0.4]],
+                         device="cuda", dtype=st.dtype)
+    for amp, builds in ((0.03, 1), (0.12, 2)):
+        F = eye.repeat(st.n_systems, 1, 1)
+        F[4] += amp * shape
+        st.positions = torch.einsum("nij,nj->ni", F[st.system_idx],
+                                    st.positions).contiguous()
+        st.cell = torch.einsum("nij,njk->nik", F, st.cell).contiguous()
+        _cmp(vm(st), ref(st), 1e-10)
+        assert vm.n_builds == builds
     # atoms moved by lattice vectors (unwrapped) and one atom jumping by 0.7 A
     k = torch.randint(-3, 4, st.positions.shape, device="cuda", generator=g).to(st.dtype)
     st.positions = (st.positions +

@@ -7,19 +7,20 @@
 // from beyond cutoff + skin to inside the cutoff.  The pairs inside the cutoff,
 // and so energies, forces and stresses, are those of the per-call search.
 //
-// Validity.  A system's list is built at cell C0 from positions wrapped into it,
-// w0_i = x0_i - W_i C0 (W_i integer, zero on open axes), with entries (i, j, S),
-// S in {-1,0,1}^3 (code (Sx+1)*9 + (Sy+1)*3 + (Sz+1)).  At a later call with
-// positions x and cell C the frame positions are w_i = x_i - W_i C and an entry's
-// vector w_j + S C - w_i differs from its build value by at most 2 D + |S dC|,
-// D = max_i |w_i - w0_i|, dC = C - C0.  With c = sum over periodic k of |row k of
-// dC|, every pair with |S|_inf <= 1 is covered while 2 D + c <= skin.  A pair
-// with |S_k| = m >= 2 was at least (m - 1) w_min apart at build (w_min the
-// smallest periodic plane spacing of C0; the build checks that no such pair lies
-// within cutoff + skin), so it stays beyond the cutoff while
-// 2 D + 2 c <= w_min - cutoff and c <= w_min / 2.  Each call sets per system
-// dmax = min(skin - c, w_min - cutoff - 2 c) / 2 (negative when c > w_min / 2)
-// and expires the system when an atom's |w_i - w0_i| exceeds dmax.
+// Validity.  A system's list is built at cell C0 (rows = lattice vectors) from
+// positions wrapped into it, w0_i = x0_i - W_i C0 (W_i integer, zero on open
+// axes), with entries (i, j, S), S in {-1,0,1}^3 (code (Sx+1)*9 + (Sy+1)*3 +
+// (Sz+1)); the search covers every image, and the build fails when a pair with
+// |S|_inf >= 2 lies within cutoff + skin, so every pair left out of the list was
+// at least cutoff + skin apart.  At a later call with positions x and cell C the
+// frame positions are w_i = x_i - W_i C.  With the deformation F = C0^-1 C (the
+// identity for a system without a fractional frame) and the non-affine drift
+// u_i = w_i - w0_i F, any pair's vector is exactly r = r0 F + u_j - u_i (the
+// image term S C - S C0 F vanishes), so |r| >= |r0| (1 - |F - I|) - 2 max|u|.
+// A system's list therefore stays valid while 2 max|u| + (cutoff + skin) e <=
+// skin, e = |F - I|_Frobenius (< 1): each call sets dmax = (skin - (cutoff +
+// skin) e) / 2 per system and expires the system when an atom's |u_i| exceeds it.
+// A uniform strain costs (cutoff + skin) e, not the atoms' affine displacement.
 //
 // Layout by slot: a system's atoms occupy the slots of its atom range, ordered
 // by the bins of its last build (perm[slot] = atom), so neighbouring threads and
@@ -41,10 +42,10 @@ struct VlWork {
   BinData b;           // bins of the last rebuild (sys_of / sys_lo / sys_hi persist)
   double4 *ref;        // [N] w0 at the atom's last build
   int32_t *rwrap;      // [3N] W at the last build
-  double *rcell;       // [9S] C0
-  double *slack;       // [S] w_min - cutoff at build (+inf without periodic axes)
-  int32_t *permask;    // [S] periodic axes of the build frame (bit k)
-  double *dmax;        // [S] allowed drift for this call
+  double *rinv;        // [9S] C0^-1 (rows), or the identity without a fractional frame
+  int32_t *rframe;     // [S] the build had a fractional frame
+  double *fdef;        // [9S] F = C0^-1 C of this call
+  double *dmax;        // [S] allowed non-affine drift for this call
   int32_t *sys_exp;    // [S] rebuild this system
   int32_t *sys_built;  // [S]
   int32_t *perm;       // [N] atom of each slot (identity until a system is built)
@@ -66,9 +67,9 @@ static void carve_vl(Carver &c, VlWork &w, int64_t n, int64_t ns) {
   carve_bins(c, w.b, n, ns);
   w.ref = c.take<double4>(n);
   w.rwrap = c.take<int32_t>(3 * n);
-  w.rcell = c.take<double>(9 * ns);
-  w.slack = c.take<double>(ns);
-  w.permask = c.take<int32_t>(ns);
+  w.rinv = c.take<double>(9 * ns);
+  w.rframe = c.take<int32_t>(ns);
+  w.fdef = c.take<double>(9 * ns);
   w.dmax = c.take<double>(ns);
   w.perm = c.take<int32_t>(n);
   w.islot = c.take<int32_t>(n);
@@ -83,17 +84,12 @@ static void carve_vl(Carver &c, VlWork &w, int64_t n, int64_t ns) {
   w.part = w.chunks > 1 ? c.take<double>(7 * ns * w.chunks) : nullptr;
 }
 
-__device__ inline double row_norm(const double *a) {
-  return sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
-}
-
-// per system: deformation since the build -> allowed drift (or expiry)
+// per system: deformation F = C0^-1 C since the build -> allowed drift (or expiry)
 template <class P>
 __global__ void k_vl_sys_check(const P *cell_row, const uint8_t *active, int64_t ns,
-                               double cutoff, double skin, const double *rcell,
-                               const double *slack, const int32_t *permask,
-                               const int32_t *built, double *dmax, int32_t *sys_exp,
-                               int32_t *flags) {
+                               double cutoff, double skin, const double *rinv,
+                               const int32_t *rframe, const int32_t *built, double *fdef,
+                               double *dmax, int32_t *sys_exp, int32_t *flags) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= ns) return;
   if (active && !active[s]) {
@@ -107,40 +103,47 @@ __global__ void k_vl_sys_check(const P *cell_row, const uint8_t *active, int64_t
     flags[0] = 1;
     return;
   }
-  double c = 0.0;
-  for (int k = 0; k < 3; ++k) {
-    if (!((permask[s] >> k) & 1)) continue;
-    double d[3];
-    for (int m = 0; m < 3; ++m)
-      d[m] = (double)cell_row[9 * s + 3 * k + m] - rcell[9 * s + 3 * k + m];
-    c += row_norm(d);
-  }
-  const double wmin = slack[s] + cutoff;
-  double d = 0.5 * fmin(skin - c, slack[s] - 2.0 * c);
-  if (c > 0.5 * wmin) d = -1.0;
+  double F[9];
+  double e2 = 0.0;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      double f = r == c ? 1.0 : 0.0;
+      if (rframe[s]) {
+        f = 0.0;
+        for (int k = 0; k < 3; ++k) f += rinv[9 * s + 3 * r + k] * (double)cell_row[9 * s + 3 * k + c];
+      }
+      F[3 * r + c] = f;
+      const double d = f - (r == c ? 1.0 : 0.0);
+      e2 += d * d;
+    }
+  for (int k = 0; k < 9; ++k) fdef[9 * s + k] = F[k];
+  const double e = sqrt(e2);
+  const double d = e < 1.0 ? 0.5 * (skin - (cutoff + skin) * e) : -1.0;
   dmax[s] = d;
   sys_exp[s] = d < 0.0;
   if (d < 0.0) flags[0] = 1;
 }
 
-// per atom: drift in the build frame against the system's allowance
+// per atom: non-affine drift u_i = w_i - w0_i F against the system's allowance
 template <class P>
 __global__ void k_vl_atom_check(const P *pos, const P *cell_row, const int64_t *sys,
                                 int64_t n, const int32_t *rwrap, const double4 *ref,
-                                const double *dmax, int32_t *sys_exp, int32_t *flags) {
+                                const double *fdef, const double *dmax, int32_t *sys_exp,
+                                int32_t *flags) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int64_t s = sys[i];
   const double dm = dmax[s];
   if (!(dm >= 0.0) || isinf(dm)) return;  // expired already, or inactive
   const P *C = cell_row + 9 * s;
+  const double *F = fdef + 9 * s;
   const int W0 = rwrap[3 * i], W1 = rwrap[3 * i + 1], W2 = rwrap[3 * i + 2];
   const double4 r = ref[i];
   double d2 = 0.0;
   for (int m = 0; m < 3; ++m) {
     const double w = (double)pos[3 * i + m] -
                      (W0 * (double)C[m] + W1 * (double)C[3 + m] + W2 * (double)C[6 + m]);
-    const double d = w - (m == 0 ? r.x : (m == 1 ? r.y : r.z));
+    const double d = w - (r.x * F[m] + r.y * F[3 + m] + r.z * F[6 + m]);
     d2 += d * d;
   }
   if (d2 > dm * dm) {
@@ -270,24 +273,15 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// per rebuilt system: record the build cell, its slack and periodic axes
-__global__ void k_vl_sys_built(const SysGeom *g, int64_t ns, double cutoff, int32_t *sys_exp,
-                               int32_t *built, double *rcell, double *slack,
-                               int32_t *permask) {
+// per rebuilt system: record C0^-1 (the transpose of the frame matrix T)
+__global__ void k_vl_sys_built(const SysGeom *g, int64_t ns, int32_t *sys_exp, int32_t *built,
+                               double *rinv, int32_t *rframe) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= ns || !sys_exp[s]) return;
   const SysGeom &G = g[s];
-  double wmin = INFINITY;
-  int mask = 0;
-  for (int k = 0; k < 3; ++k) {
-    if (!G.per[k]) continue;
-    mask |= 1 << k;
-    // plane spacing of lattice planes k = 1 / |reciprocal vector k| (row k of T)
-    wmin = fmin(wmin, 1.0 / row_norm(G.T + 3 * k));
-  }
-  for (int k = 0; k < 9; ++k) rcell[9 * s + k] = G.cell[k];
-  slack[s] = wmin - cutoff;
-  permask[s] = mask;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) rinv[9 * s + 3 * r + c] = G.active ? G.T[3 * c + r] : (r == c);
+  rframe[s] = G.active;
   built[s] = 1;
   sys_exp[s] = 0;
 }
@@ -466,11 +460,11 @@ static int vl_check(const P *pos, const P *cell, const int64_t *sys, const uint8
                     int64_t n, int64_t ns, double cutoff, double skin, int32_t *flags,
                     VlWork &w, cudaStream_t st) {
   cudaMemsetAsync(flags, 0, 2 * sizeof(int32_t), st);
-  k_vl_sys_check<P><<<grid_for(ns), kBlock, 0, st>>>(cell, active, ns, cutoff, skin, w.rcell,
-                                                     w.slack, w.permask, w.sys_built, w.dmax,
+  k_vl_sys_check<P><<<grid_for(ns), kBlock, 0, st>>>(cell, active, ns, cutoff, skin, w.rinv,
+                                                     w.rframe, w.sys_built, w.fdef, w.dmax,
                                                      w.sys_exp, flags);
-  k_vl_atom_check<P><<<grid_for(n), kBlock, 0, st>>>(pos, cell, sys, n, w.rwrap, w.ref, w.dmax,
-                                                     w.sys_exp, flags);
+  k_vl_atom_check<P><<<grid_for(n), kBlock, 0, st>>>(pos, cell, sys, n, w.rwrap, w.ref, w.fdef,
+                                                     w.dmax, w.sys_exp, flags);
   TSB_CHECK_LAUNCH();
   return TSB_OK;
 }
@@ -494,8 +488,8 @@ static int vl_build(const P *pos, const P *cell, const uint8_t *pbc, const int64
   k_vl_build<<<(unsigned)(n_sm * 8), 256, 0, st>>>(w.b, n, ns, rcs * rcs, w.eoff, w.islot, list,
                                                     counts, max_nb, flags, w.perm, w.ref,
                                                     w.rwrap);
-  k_vl_sys_built<<<grid_for(ns), kBlock, 0, st>>>(w.b.geom, ns, cutoff, w.sys_exp, w.sys_built,
-                                                  w.rcell, w.slack, w.permask);
+  k_vl_sys_built<<<grid_for(ns), kBlock, 0, st>>>(w.b.geom, ns, w.sys_exp, w.sys_built, w.rinv,
+                                                  w.rframe);
   TSB_CHECK_LAUNCH();
   return TSB_OK;
 }
