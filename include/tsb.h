@@ -165,6 +165,23 @@ int tsb_verlet_forces(int potential, const double *table, int n_species,
                       double *vir_atom, void *workspace, size_t workspace_bytes,
                       void *stream);
 
+/* ---- isotropic C-rescale barostat -----------------------------------------
+ * The barostat step of npt_crescale_isotropic_step (torch_sim/integrators/
+ * npt.py:2455-2492, 2797-2901; Bernetti & Bussi 2020): per system, the trace of
+ * the instantaneous pressure (quantities.py:156-198), the stochastic update of
+ * sqrt(V), mu = (V'/V)^(1/3), cell *= mu; per atom r <- mu r + (mu + 1/mu) p dt /
+ * (2 m), p <- p / mu.  cell is the state's [S,3,3] cell (either convention: only
+ * its determinant and a scale enter).  Per-system parameters are float64 [S];
+ * noise [S] (standard normal) or NULL for the counter-based Philox draw (seed,
+ * system, counter).  Workspace: tsb_npt_workspace_size. */
+int tsb_npt_crescale_iso(void *positions, void *momenta, const void *masses,
+                         const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
+                         int dtype, const void *stress, void *cell,
+                         const double *compressibility, const double *tau_p, const double *kT,
+                         const double *p_ext, const double *dt, const double *noise,
+                         uint64_t seed, uint64_t counter, void *workspace,
+                         size_t workspace_bytes, void *stream);
+
 /* ---- batched Verlet lists (many systems, moving atoms and cells) ----------
  * Replaces the per-call neighbour search inside PairPotentialModel.forward
  * (torch_sim/models/pair_potential.py:168-174, 351-464) for a batch whose atoms

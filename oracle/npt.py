@@ -11,11 +11,17 @@ step (Gronbech-Jensen & Farago GJF scheme), noise passed in:
   ``_npt_langevin_isotropic_cell_velocity_step`` (:801-835),
   ``_npt_langevin_particle_velocity_step`` (:316-367),
   cell = exp(eps) reference_cell, V = det(reference_cell) exp(3 eps) (:690-703)
+* ``npt_crescale_isotropic_step`` <- npt.py:2797-2901 (V-rescale half steps of
+  nvt.py:594-654, momentum half steps, ``_crescale_isotropic_barostat_step``
+  :2455-2492 with the instantaneous pressure of quantities.py:156-198)
 """
 
 from __future__ import annotations
 
 import numpy as np
+
+from . import md as omd
+from . import thermostats as oth
 
 
 def cell_force(stress, vol, n_atoms, kT, p_ext):
@@ -65,4 +71,45 @@ def npt_langevin_isotropic_step(st, force_fn, dt, kT, p_ext, cell_noise, particl
     v_new = ap * vel + dt * (ap * forces_old + f) / m2[:, None] + bp * beta_p / m[:, None]
     st.update(positions=q, momenta=v_new * m[:, None], forces=f, energy=e, stress=s, cell=cell,
               cell_positions=eps, cell_velocities=eps_dot, cell_masses=q_mass)
+    return st
+
+
+def _vrescale(st, kT, tau, dt, r1, gamma_sample, system_idx):
+    n_sys = int(system_idx.max()) + 1
+    dof = 3 * np.bincount(system_idx, minlength=n_sys) - 3
+    kt_now = omd.calc_kT(st["masses"], st["momenta"], system_idx, dof)
+    lam = oth.vrescale_factor(dof * kt_now / 2.0, dof, kT, tau, dt, r1, gamma_sample)
+    return st["momenta"] * lam[system_idx][:, None]
+
+
+def npt_crescale_isotropic_step(st, force_fn, dt, kT, p_ext, tau, noise, system_idx):
+    """st: dict positions, momenta, masses, forces, stress, cell [S,3,3] (either
+    convention), isothermal_compressibility [S], tau_p [S].  noise = (r1_a [S],
+    gamma_a [S], cell [S], r1_b [S], gamma_b [S]) in the order the reference draws
+    them.  force_fn(q, cell) -> (energy, forces, stress)."""
+    st = dict(st)
+    r1a, ga, zc, r1b, gb = noise
+    m = st["masses"]
+    st["momenta"] = _vrescale(st, kT, tau, dt / 2, r1a, ga, system_idx)
+    st["momenta"] = st["momenta"] + st["forces"] * (dt / 2)
+    vol = np.linalg.det(st["cell"])
+    p = st["momenta"]
+    n_sys = len(vol)
+    two_k = np.zeros(n_sys)
+    np.add.at(two_k, system_idx, (p * p / m[:, None]).sum(1))
+    tr_p = two_k / vol - np.einsum("sii->s", st["stress"])
+    bt, tp = st["isothermal_compressibility"], st["tau_p"]
+    sqrt_vol = np.sqrt(vol)
+    pre_random = np.sqrt(kT * bt * dt / (4 * tp))
+    pre = bt * sqrt_vol / (2 * tp)
+    change = -pre * (p_ext - tr_p / 3 - kT / (2 * vol)) * dt + np.sqrt(2.0) * pre_random * zc
+    mu = ((sqrt_vol + change) / sqrt_vol) ** (2.0 / 3.0)
+    mu_a = mu[system_idx][:, None]
+    q = mu_a * st["positions"] + (mu_a + 1 / mu_a) * p * (0.5 * dt) / m[:, None]
+    p = p / mu_a
+    cell = mu[:, None, None] * st["cell"]
+    e, f, s = force_fn(q, cell)
+    st.update(positions=q, momenta=p, cell=cell, forces=f, energy=e, stress=s)
+    st["momenta"] = st["momenta"] + st["forces"] * (dt / 2)
+    st["momenta"] = _vrescale(st, kT, tau, dt / 2, r1b, gb, system_idx)
     return st

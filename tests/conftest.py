@@ -35,4 +35,5 @@ def load_golden(name):
 @pytest.fixture(scope="session")
 def golden():
     return {n: load_golden(f"{n}.npz") for n in ("nl", "models", "md", "fire", "math",
-                                                  "thermostats", "pairforces", "npt")}
+                                                  "thermostats", "pairforces", "npt",
+                                                  "crescale")}

@@ -1,0 +1,101 @@
+"""Golden fixtures for the isotropic C-rescale NPT step, generated by running the
+reference TorchSim itself.
+
+Run in a container where the reference source tree is present::
+
+    python tests/golden/make_crescale.py /path/to/torch-sim
+
+Writes ``crescale.npz`` beside this script: 8 steps of
+``npt_crescale_isotropic_step`` on three Morse Cu systems (compute_stress=True)
+at 600 K and 1 GPa (internal units), tau = 5 dt, tau_p = 50 dt, compressibility
+1e-4 bar^-1, with the reference's random numbers recorded per step in the order
+drawn: V-rescale (r1, Gamma deviate), barostat normal, V-rescale (r1, Gamma).
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, HERE)
+
+from make_golden import _install_shims  # noqa: E402
+
+
+def main(ref_root):
+    _install_shims(ref_root)
+    sys.path.insert(0, os.path.join(REPO, "torch-sim_b200"))
+    import torch
+
+    torch.set_default_dtype(torch.float64)
+    import torch_sim as ts
+    from torch_sim.integrators import npt as ref_npt
+    from torch_sim.models.morse import MorseModel
+    from torch_sim.units import MetalUnits
+
+    from tsb import workloads as W
+
+    cu3 = W.copper_batch(3, 8, 40, seed=29, jitter=0.03)
+    T = lambda x, dt=torch.float64: torch.as_tensor(x, dtype=dt)  # noqa: E731
+    st = ts.SimState(positions=T(cu3["positions"]), masses=T(cu3["masses"]),
+                     cell=T(cu3["cell"]), pbc=True,
+                     atomic_numbers=T(cu3["atomic_numbers"], torch.int64),
+                     system_idx=T(cu3["system_idx"], torch.int64))
+    st.rng = 37
+    morse = MorseModel(sigma=2.866, epsilon=0.3429, alpha=1.3588, cutoff=6.0,
+                       compute_stress=True)
+    kT = 600.0 * W.KB_EV
+    dt = 0.002 * W.METAL_TIME
+    p_ext = 1.0 * 0.006241509074460764  # 1 GPa in eV/A^3
+    beta = 1e-4 / float(MetalUnits.pressure)
+    md = ref_npt.npt_crescale_init(st, morse, kT=torch.tensor(kT), dt=torch.tensor(dt),
+                                   tau_p=torch.tensor(50 * dt),
+                                   isothermal_compressibility=torch.tensor(beta))
+    normals, gammas = [], []
+    real_randn, real_gamma = torch.randn, torch._standard_gamma
+
+    def rec_randn(*a, **k):
+        x = real_randn(*a, **k)
+        normals.append(x.clone())
+        return x
+
+    def rec_gamma(*a, **k):
+        x = real_gamma(*a, **k)
+        gammas.append(x.clone())
+        return x
+
+    keys = ("positions", "momenta", "energy", "forces", "stress", "cell")
+    traj = [[getattr(md, k).clone().numpy() for k in keys]]
+    torch.randn, torch._standard_gamma = rec_randn, rec_gamma
+    try:
+        for _ in range(8):
+            md = ref_npt.npt_crescale_isotropic_step(md, morse, dt=torch.tensor(dt),
+                                                     kT=torch.tensor(kT),
+                                                     external_pressure=torch.tensor(p_ext),
+                                                     tau=torch.tensor(5 * dt))
+            traj.append([getattr(md, k).clone().numpy() for k in keys])
+    finally:
+        torch.randn, torch._standard_gamma = real_randn, real_gamma
+    assert len(normals) == 24 and len(gammas) == 16, (len(normals), len(gammas))
+    out = {f"sys/{k}": cu3[k] for k in ("masses", "cell", "system_idx", "atomic_numbers")}
+    for i, k in enumerate(keys):
+        out[f"crescale/{k}"] = np.stack([t[i] for t in traj])
+    out["crescale/r1_a"] = np.stack([n.numpy() for n in normals[0::3]])
+    out["crescale/cell_noise"] = np.stack([n.numpy() for n in normals[1::3]])
+    out["crescale/r1_b"] = np.stack([n.numpy() for n in normals[2::3]])
+    out["crescale/gamma_a"] = np.stack([g.numpy() for g in gammas[0::2]])
+    out["crescale/gamma_b"] = np.stack([g.numpy() for g in gammas[1::2]])
+    for k in ("isothermal_compressibility", "tau_p"):
+        out[f"crescale/{k}"] = getattr(md, k).clone().numpy()
+    out["crescale/dt"], out["crescale/kT"] = np.array(dt), np.array(kT)
+    out["crescale/p_ext"], out["crescale/tau"] = np.array(p_ext), np.array(5 * dt)
+    np.savez_compressed(os.path.join(HERE, "crescale.npz"), **out)
+    print("C-rescale fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("TORCH_SIM_REF", ""))

@@ -1,4 +1,4 @@
-"""Isotropic NPT Langevin on the GPU.
+"""Isotropic NPT Langevin and isotropic C-rescale on the GPU.
 
 * 8 steps vs the reference (golden/npt.npz) with the reference's cell and
   particle noise injected; FP64 model: positions, cell and strain to 1e-12,
@@ -68,6 +68,68 @@ def test_npt_device_noise_reproducible_and_barostat_responds():
     b = _run(0.0)
     assert torch.equal(a.positions, b.positions) and torch.equal(a.cell, b.cell)
     c = _run(20.0)
+    va = torch.linalg.det(a.cell).abs()
+    vc = torch.linalg.det(c.cell).abs()
+    assert bool((vc < va).all()), (va, vc)
+    assert torch.isfinite(a.positions).all() and torch.isfinite(c.momenta).all()
+
+
+def test_npt_crescale_isotropic_matches_reference(golden):
+    """8 isotropic C-rescale steps vs the reference (golden/crescale.npz) with its
+    V-rescale and barostat draws injected; FP64 model, rtol 1e-9."""
+    from tsb import integrators as I
+    from tsb import models
+    from tsb.state import MDState
+
+    s, g = golden["crescale"]["sys"], golden["crescale"]["crescale"]
+    dev = torch.device("cuda")
+    T = lambda x, dt=torch.float64: torch.as_tensor(x, dtype=dt, device=dev)  # noqa: E731
+    n = len(s["masses"])
+    st = MDState(positions=T(g["positions"][0]), masses=T(s["masses"]), cell=T(s["cell"]),
+                 pbc=True, atomic_numbers=T(s["atomic_numbers"], torch.int64),
+                 system_idx=T(s["system_idx"], torch.int64), momenta=T(g["momenta"][0]),
+                 energy=T(np.zeros(3)), forces=T(np.zeros((n, 3))))
+    m = models.MorseModel(sigma=2.866, epsilon=0.3429, alpha=1.3588, cutoff=6.0,
+                          compute_stress=True, precision="fp64")
+    dt, kT, p, tau = (float(g[k]) for k in ("dt", "kT", "p_ext", "tau"))
+    st = I.npt_crescale_init(st, m, kT=kT, dt=dt, tau_p=g["tau_p"],
+                             isothermal_compressibility=g["isothermal_compressibility"])
+    np.testing.assert_allclose(st.stress.cpu(), g["stress"][0], rtol=1e-9, atol=1e-14)
+    for k in range(1, g["positions"].shape[0]):
+        noise = (np.stack([g["r1_a"][k - 1], g["gamma_a"][k - 1]], axis=1),
+                 g["cell_noise"][k - 1],
+                 np.stack([g["r1_b"][k - 1], g["gamma_b"][k - 1]], axis=1))
+        st = I.npt_crescale_isotropic_step(st, m, dt=dt, kT=kT, external_pressure=p, tau=tau,
+                                           noise=noise)
+        for key in ("positions", "momenta", "cell", "stress", "energy"):
+            np.testing.assert_allclose(getattr(st, key).cpu(), g[key][k], rtol=1e-9,
+                                       atol=1e-12, err_msg=f"step {k} {key}")
+
+
+def _run_crescale(p_gpa, seed=3, steps=300):
+    from tsb import integrators as I
+    from tsb import models, workloads
+    from tsb.state import state_from_arrays
+
+    d = workloads.copper_batch(6, 100, 250, seed=4)
+    st = state_from_arrays(d, device="cuda")
+    st.rng = seed
+    m = models.MorseModel(sigma=2.866, epsilon=0.3429, alpha=1.3588, cutoff=6.0,
+                          compute_stress=True)
+    kT, dt = 300 * workloads.KB_EV, 0.002 * workloads.METAL_TIME
+    # the default compressibility, 1e-6 / bar (copper: about 7e-7 / bar)
+    md = I.npt_crescale_init(st, m, kT=kT, dt=dt, tau_p=100 * dt)
+    for _ in range(steps):
+        md = I.npt_crescale_isotropic_step(md, m, dt=dt, kT=kT, external_pressure=p_gpa * GPA,
+                                           tau=10 * dt)
+    return md
+
+
+def test_npt_crescale_device_noise_reproducible_and_barostat_responds():
+    a = _run_crescale(0.0)
+    b = _run_crescale(0.0)
+    assert torch.equal(a.positions, b.positions) and torch.equal(a.cell, b.cell)
+    c = _run_crescale(20.0)
     va = torch.linalg.det(a.cell).abs()
     vc = torch.linalg.det(c.cell).abs()
     assert bool((vc < va).all()), (va, vc)

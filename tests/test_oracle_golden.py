@@ -297,3 +297,29 @@ def test_npt_langevin_isotropic_oracle_matches_reference(golden):
                         ("cell_positions", 1e-9), ("cell_velocities", 1e-9),
                         ("cell_masses", 1e-14), ("stress", 1e-9)):
             np.testing.assert_allclose(st[key], g[key][k], rtol=rt, atol=1e-14, err_msg=key)
+
+
+def test_npt_crescale_isotropic_oracle_matches_reference(golden):
+    from oracle import npt as onpt
+
+    s, g = golden["crescale"]["sys"], golden["crescale"]["crescale"]
+    sysi = s["system_idx"].astype(np.int64)
+    tab = opair.single_table(opair.MORSE, 2.866, 0.3429, 1.3588)
+
+    def fn(q, cell_col):
+        o = opair.pair_forward(opair.MORSE, tab, np.zeros(len(q), int), q,
+                               np.transpose(cell_col, (0, 2, 1)), np.array([True] * 3), sysi,
+                               6.0)
+        return o["energy"], o["forces"], o["stress"]
+
+    dt, kT, p_ext, tau = (float(g[k]) for k in ("dt", "kT", "p_ext", "tau"))
+    st = {"positions": g["positions"][0], "momenta": g["momenta"][0], "masses": s["masses"],
+          "forces": g["forces"][0], "stress": g["stress"][0], "cell": g["cell"][0],
+          "isothermal_compressibility": g["isothermal_compressibility"],
+          "tau_p": g["tau_p"]}
+    for k in range(1, g["positions"].shape[0]):
+        noise = (g["r1_a"][k - 1], g["gamma_a"][k - 1], g["cell_noise"][k - 1],
+                 g["r1_b"][k - 1], g["gamma_b"][k - 1])
+        st = onpt.npt_crescale_isotropic_step(st, fn, dt, kT, p_ext, tau, noise, sysi)
+        for key in ("positions", "momenta", "cell", "stress", "energy"):
+            np.testing.assert_allclose(st[key], g[key][k], rtol=1e-9, atol=1e-12, err_msg=key)

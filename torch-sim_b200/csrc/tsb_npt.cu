@@ -159,6 +159,68 @@ __global__ void k_npt_atom_post(int64_t n, P *p, const P *m, const P *f_old, con
   }
 }
 
+// Isotropic stochastic cell rescaling (C-rescale, Bernetti & Bussi 2020;
+// torch_sim/integrators/npt.py:2455-2492).  One block per system: the trace of
+// the instantaneous pressure tensor P = (sum_i p_i p_i^T / m_i) / V - stress
+// (quantities.py:156-198), summed in FP64 in a fixed order, then the Euler step
+// of lambda = sqrt(V):
+//   d lambda = -(beta_T lambda / (2 tau_p)) (P0 - tr P / 3 - kT / (2 V)) dt
+//              + sqrt(2) sqrt(kT beta_T dt / (4 tau_p)) z,
+// the factor mu = (lambda' / lambda)^(2/3) and the cell scaled by mu.
+template <class P>
+__global__ void __launch_bounds__(256)
+    k_crescale_iso_cell(const int64_t *lo, const int64_t *hi, const P *p, const P *m,
+                        const P *stress, P *cell, const double *beta_t, const double *tau_p,
+                        const double *kT, const double *p_ext, const double *dt,
+                        const double *noise, uint64_t seed, uint64_t counter, double *mu) {
+  __shared__ double sh[256 / 32];
+  const int64_t s = blockIdx.x;
+  double acc = 0.0;
+  for (int64_t i = lo[s] + threadIdx.x; i < hi[s]; i += blockDim.x) {
+    const double mi = (double)m[i];
+    for (int c = 0; c < 3; ++c) {
+      const double pc = (double)p[3 * i + c];
+      acc += pc * pc / mi;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  double two_k = 0.0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) two_k += sh[w];
+  double C[9];
+  for (int k = 0; k < 9; ++k) C[k] = (double)cell[9 * s + k];
+  const double vol = det3(C);
+  const P *st = stress + 9 * s;
+  const double tr_p = two_k / vol - ((double)st[0] + (double)st[4] + (double)st[8]);
+  const double kt = kT[s], h = dt[s], bt = beta_t[s], tp = tau_p[s];
+  const double sqrt_vol = sqrt(vol);
+  const double pre_random = sqrt(kt * bt * h / (4.0 * tp));
+  const double pre = bt * sqrt_vol / (2.0 * tp);
+  const double z = noise ? noise[s] : thermo_normal(seed, s, counter, 3u);
+  const double change =
+      -pre * (p_ext[s] - tr_p / 3.0 - kt / (2.0 * vol)) * h + sqrt(2.0) * pre_random * z;
+  const double f = pow((sqrt_vol + change) / sqrt_vol, 2.0 / 3.0);
+  mu[s] = f;
+  for (int k = 0; k < 9; ++k) cell[9 * s + k] = (P)(f * C[k]);
+}
+
+// per atom: r <- mu r + (mu + 1/mu) p dt / (2 m), p <- p / mu
+template <class P>
+__global__ void k_crescale_iso_atoms(int64_t n, P *x, P *p, const P *m, const int64_t *sys,
+                                     const double *dt, const double *mu) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t s = sys[i];
+  const double f = mu[s], fi = 1.0 / f, h = dt[s], mi = (double)m[i];
+  for (int c = 0; c < 3; ++c) {
+    const double pc = (double)p[3 * i + c];
+    x[3 * i + c] = (P)(f * (double)x[3 * i + c] + (f + fi) * pc * (0.5 * h) / mi);
+    p[3 * i + c] = (P)(fi * pc);
+  }
+}
+
 }  // namespace tsb
 
 using namespace tsb;
@@ -243,6 +305,42 @@ extern "C" int tsb_npt_langevin_iso_post(
     TSB_NPT_POST(float)
   }
 #undef TSB_NPT_POST
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
+
+extern "C" int tsb_npt_crescale_iso(void *positions, void *momenta, const void *masses,
+                                    const int64_t *system_idx, int64_t n_atoms,
+                                    int64_t n_systems, int dtype, const void *stress,
+                                    void *cell, const double *compressibility,
+                                    const double *tau_p, const double *kT, const double *p_ext,
+                                    const double *dt, const double *noise, uint64_t seed,
+                                    uint64_t counter, void *workspace, size_t workspace_bytes,
+                                    void *stream) {
+  if (n_atoms < 1 || n_systems < 1 || !positions || !momenta || !masses || !system_idx ||
+      !stress || !cell || !compressibility || !tau_p || !kT || !p_ext || !dt)
+    return TSB_ERR_INVALID_ARG;
+  if (dtype != TSB_F32 && dtype != TSB_F64) return TSB_ERR_INVALID_ARG;
+  Carver c(workspace, workspace_bytes);
+  NptWork w;
+  carve_npt(c, w, n_systems);
+  if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaMemsetAsync(w.lo, 0, sizeof(int64_t) * n_systems, st);
+  cudaMemsetAsync(w.hi, 0, sizeof(int64_t) * n_systems, st);
+  k_npt_bounds<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, w.lo, w.hi);
+#define TSB_CRESCALE(P)                                                                      \
+  k_crescale_iso_cell<P><<<(unsigned)n_systems, 256, 0, st>>>(                               \
+      w.lo, w.hi, (const P *)momenta, (const P *)masses, (const P *)stress, (P *)cell,       \
+      compressibility, tau_p, kT, p_ext, dt, noise, seed, counter, w.scale);                 \
+  k_crescale_iso_atoms<P><<<grid_for(n_atoms), kBlock, 0, st>>>(                             \
+      n_atoms, (P *)positions, (P *)momenta, (const P *)masses, system_idx, dt, w.scale);
+  if (dtype == TSB_F64) {
+    TSB_CRESCALE(double)
+  } else {
+    TSB_CRESCALE(float)
+  }
+#undef TSB_CRESCALE
   TSB_CHECK_LAUNCH();
   return TSB_OK;
 }

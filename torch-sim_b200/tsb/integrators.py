@@ -304,6 +304,93 @@ def nvt_vrescale_step(model, state, *, dt, kT, tau=None, noise=None, **_kw):
 # ---------------------------------------------------------------------------
 # Isotropic NPT Langevin
 # ---------------------------------------------------------------------------
+# ---------------------------------------------------------------------------
+# Isotropic stochastic cell rescaling (C-rescale)
+# ---------------------------------------------------------------------------
+# eV / A^3 per bar (MetalUnits.pressure, torch_sim/units.py:100-113)
+METAL_PRESSURE_BAR = 1e5 * 1e-30 / 1.6021766208e-19
+
+
+def npt_crescale_init(state, model, *, kT, dt, tau_p=None, isothermal_compressibility=None,
+                      **_kw):
+    """C-rescale state (npt.py:2904-2986): tau_p = 3 dt and the isothermal
+    compressibility 1e-6 bar^-1 by default; ``model`` must compute the stress."""
+    from .state import NPTCRescaleState
+
+    md = _md_init(state, model, kT)
+    out = model(md)
+    if "stress" not in out:
+        raise ValueError("NPT needs a model with compute_stress=True")
+    n_sys, dev = md.n_systems, md.device
+    dt_s = _per_system(dt, n_sys, dev)
+    tau_p = _per_system(3 * dt_s if tau_p is None else tau_p, n_sys, dev).clone()
+    beta = _per_system(1e-6 / METAL_PRESSURE_BAR if isothermal_compressibility is None
+                       else isothermal_compressibility, n_sys, dev).clone()
+    cell0 = md.cell.clone()
+    st = NPTCRescaleState.from_state(
+        md, stress=out["stress"], isothermal_compressibility=beta, tau_p=tau_p,
+        initial_cell=cell0, initial_cell_inv=torch.linalg.inv(cell0),
+        initial_volume=torch.linalg.det(cell0))
+    st._philox_seed, st._philox_counter = md._philox_seed, 0
+    return st
+
+
+def _vrescale(state, kT_s, tau_s, dt_s, noise, seed, counter):
+    dev, n_sys = state.device, state.n_systems
+    if noise is not None:
+        noise = torch.as_tensor(noise, dtype=torch.float64, device=dev).reshape(n_sys, 2)
+        noise = noise.contiguous()
+    ws = _thermo_ws(state)
+    L.call("tsb_vrescale", L.ptr(state.momenta), L.ptr(state.masses), L.ptr(state.system_idx),
+           state.n_atoms, n_sys, L.dtype_code(state.dtype), L.ptr(_dof(state)), L.ptr(kT_s),
+           L.ptr(tau_s), L.ptr(dt_s), L.ptr(noise), seed, counter, None, L.ptr(ws),
+           ws.numel(), L.stream_ptr(dev))
+
+
+def npt_crescale_isotropic_step(state, model, *, dt, kT, external_pressure, tau=None,
+                                noise=None, **_kw):
+    """One isotropic C-rescale step (npt.py:2797-2901; Bernetti & Bussi 2020):
+    V-rescale(dt/2), kick(dt/2), barostat(dt), forces, kick(dt/2), V-rescale(dt/2).
+    The thermostat's tau defaults to dt, as the reference's code does.  The draws
+    (two V-rescale pairs (r1, Gamma deviate) and the barostat normal) come from
+    the device Philox stream (seed, system, step); ``noise = (vrescale_1 [S, 2],
+    cell [S], vrescale_2 [S, 2])`` supplies them instead."""
+    _prepare(state)
+    n_sys, n, dev = state.n_systems, state.n_atoms, state.device
+    dt_s = _per_system(dt, n_sys, dev)
+    kT_s = _per_system(kT, n_sys, dev)
+    p_s = _per_system(external_pressure, n_sys, dev)
+    tau_s = _per_system(dt_s if tau is None else tau, n_sys, dev)
+    half = (dt_s / 2).contiguous()
+    for name in ("isothermal_compressibility", "tau_p"):
+        v = getattr(state, name)
+        if v.dtype != torch.float64 or not v.is_contiguous():
+            setattr(state, name, v.to(torch.float64).contiguous())
+    state.cell = state.cell.to(state.dtype).contiguous()
+    state.stress = state.stress.to(state.dtype).contiguous()
+    v1 = cn = v2 = None
+    if noise is not None:
+        v1, v2 = noise[0], noise[2]
+        cn = torch.as_tensor(noise[1], dtype=torch.float64, device=dev).reshape(n_sys)
+        cn = cn.contiguous()
+    seed = getattr(state, "_philox_seed", _seed_of(state)) & (2**64 - 1)
+    counter = getattr(state, "_philox_counter", 0)
+    _vrescale(state, kT_s, tau_s, half, v1, seed, counter)
+    _kick(state, dt_s, 0.5)
+    ws = L.Workspace.get(dev, L.load().tsb_npt_workspace_size(n_sys))
+    L.call("tsb_npt_crescale_iso", L.ptr(state.positions), L.ptr(state.momenta),
+           L.ptr(state.masses), L.ptr(state.system_idx), n, n_sys, L.dtype_code(state.dtype),
+           L.ptr(state.stress), L.ptr(state.cell), L.ptr(state.isothermal_compressibility),
+           L.ptr(state.tau_p), L.ptr(kT_s), L.ptr(p_s), L.ptr(dt_s), L.ptr(cn), seed, counter,
+           L.ptr(ws), ws.numel(), L.stream_ptr(dev))
+    out = _apply_model(state, model)
+    state.stress = out["stress"].to(state.dtype).contiguous()
+    _kick(state, dt_s, 0.5)
+    _vrescale(state, kT_s, tau_s, half, v2, seed, counter + 1)
+    state._philox_seed, state._philox_counter = seed, counter + 2
+    return state
+
+
 def npt_langevin_isotropic_init(state, model, *, kT, dt, alpha=None, cell_alpha=None,
                                 b_tau=None, **_kw):
     """Strain-based isotropic NPT Langevin state (npt.py:888-985): eps = 0,

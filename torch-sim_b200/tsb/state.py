@@ -217,6 +217,20 @@ class NPTLangevinIsotropicState(MDState):
 
 
 @dataclass(kw_only=True)
+class NPTCRescaleState(MDState):
+    """MDState + stochastic cell rescaling (torch_sim/integrators/npt.py:2062-2090):
+    stress [S,3,3]; per system isothermal_compressibility and tau_p; the initial cell
+    [S,3,3], its inverse and volume."""
+
+    stress: torch.Tensor
+    isothermal_compressibility: torch.Tensor
+    tau_p: torch.Tensor
+    initial_cell: torch.Tensor
+    initial_cell_inv: torch.Tensor
+    initial_volume: torch.Tensor
+
+
+@dataclass(kw_only=True)
 class FireState(SimState):
     forces: torch.Tensor
     energy: torch.Tensor
