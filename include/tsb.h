@@ -182,6 +182,21 @@ int tsb_npt_crescale_iso(void *positions, void *momenta, const void *masses,
                          uint64_t seed, uint64_t counter, void *workspace,
                          size_t workspace_bytes, void *stream);
 
+/* tsb_npt_crescale_aniso: the anisotropic barostat step of
+ * npt_crescale_anisotropic_step (npt.py:2282-2343, 2645-2720): two half steps of
+ * sqrt(V) around a traceless random per-axis deformation, per-axis factors mu_k,
+ * cell row k *= mu_k (rows of the state's column-convention cell), r_k <- mu_k r_k
+ * + (mu_k + 1/mu_k) p_k dt / (2 m), p_k <- p_k / mu_k.  noise [S, 5] = (volume
+ * normal, z_x, z_y, z_z, volume normal) or NULL for Philox draws.  Workspace:
+ * tsb_npt_workspace_size. */
+int tsb_npt_crescale_aniso(void *positions, void *momenta, const void *masses,
+                           const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
+                           int dtype, const void *stress, void *cell,
+                           const double *compressibility, const double *tau_p, const double *kT,
+                           const double *p_ext, const double *dt, const double *noise,
+                           uint64_t seed, uint64_t counter, void *workspace,
+                           size_t workspace_bytes, void *stream);
+
 /* ---- batched Verlet lists (many systems, moving atoms and cells) ----------
  * Replaces the per-call neighbour search inside PairPotentialModel.forward
  * (torch_sim/models/pair_potential.py:168-174, 351-464) for a batch whose atoms

@@ -14,6 +14,8 @@ step (Gronbech-Jensen & Farago GJF scheme), noise passed in:
 * ``npt_crescale_isotropic_step`` <- npt.py:2797-2901 (V-rescale half steps of
   nvt.py:594-654, momentum half steps, ``_crescale_isotropic_barostat_step``
   :2455-2492 with the instantaneous pressure of quantities.py:156-198)
+* ``npt_crescale_anisotropic_step`` <- npt.py:2645-2720 with
+  ``_crescale_anisotropic_barostat_step`` (:2282-2343)
 """
 
 from __future__ import annotations
@@ -108,6 +110,44 @@ def npt_crescale_isotropic_step(st, force_fn, dt, kT, p_ext, tau, noise, system_
     q = mu_a * st["positions"] + (mu_a + 1 / mu_a) * p * (0.5 * dt) / m[:, None]
     p = p / mu_a
     cell = mu[:, None, None] * st["cell"]
+    e, f, s = force_fn(q, cell)
+    st.update(positions=q, momenta=p, cell=cell, forces=f, energy=e, stress=s)
+    st["momenta"] = st["momenta"] + st["forces"] * (dt / 2)
+    st["momenta"] = _vrescale(st, kT, tau, dt / 2, r1b, gb, system_idx)
+    return st
+
+
+def npt_crescale_anisotropic_step(st, force_fn, dt, kT, p_ext, tau, noise, system_idx):
+    """As npt_crescale_isotropic_step with per-axis factors; noise = (r1_a, gamma_a,
+    baro [S, 5] = (volume normal, z_x, z_y, z_z, volume normal), r1_b, gamma_b)."""
+    st = dict(st)
+    r1a, ga, zb, r1b, gb = noise
+    m = st["masses"]
+    st["momenta"] = _vrescale(st, kT, tau, dt / 2, r1a, ga, system_idx)
+    st["momenta"] = st["momenta"] + st["forces"] * (dt / 2)
+    vol = np.linalg.det(st["cell"])
+    p = st["momenta"]
+    n_sys = len(vol)
+    two_k = np.zeros((n_sys, 3))
+    np.add.at(two_k, system_idx, p * p / m[:, None])
+    p_diag = two_k / vol[:, None] - np.einsum("sii->si", st["stress"])
+    tr_p = p_diag.sum(1)
+    bt, tp = st["isothermal_compressibility"], st["tau_p"]
+    sqrt_vol = np.sqrt(vol)
+    pre_random = np.sqrt(kT * bt * dt / (4 * tp))
+    pre = bt * sqrt_vol / (2 * tp)
+    lam = sqrt_vol + (-pre * (p_ext - tr_p / 3 - kT / (2 * vol)) * dt / 2 + pre_random * zb[:, 0])
+    c_rand = np.sqrt(2 * bt * kT * dt / (3 * tp)) / lam
+    a_t = (bt / (3 * tp))[:, None] * (p_diag - tr_p[:, None] / 3)
+    z = zb[:, 1:4]
+    z = z - z.mean(1, keepdims=True)
+    d = np.exp(a_t * dt + c_rand[:, None] * z)
+    lam = lam + (-pre * (p_ext - tr_p / 3 - kT / (2 * vol)) * dt / 2 + pre_random * zb[:, 4])
+    mu = d * ((lam / sqrt_vol) ** (2.0 / 3.0))[:, None]
+    mu_a = mu[system_idx]
+    q = mu_a * st["positions"] + (mu_a + 1 / mu_a) * p * dt / (2 * m[:, None])
+    p = p / mu_a
+    cell = mu[:, :, None] * st["cell"]
     e, f, s = force_fn(q, cell)
     st.update(positions=q, momenta=p, cell=cell, forces=f, energy=e, stress=s)
     st["momenta"] = st["momenta"] + st["forces"] * (dt / 2)

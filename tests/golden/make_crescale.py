@@ -5,11 +5,14 @@ Run in a container where the reference source tree is present::
 
     python tests/golden/make_crescale.py /path/to/torch-sim
 
-Writes ``crescale.npz`` beside this script: 8 steps of
-``npt_crescale_isotropic_step`` on three Morse Cu systems (compute_stress=True)
-at 600 K and 1 GPa (internal units), tau = 5 dt, tau_p = 50 dt, compressibility
-1e-4 bar^-1, with the reference's random numbers recorded per step in the order
-drawn: V-rescale (r1, Gamma deviate), barostat normal, V-rescale (r1, Gamma).
+Writes ``crescale.npz`` beside this script: 8 steps each of
+``npt_crescale_isotropic_step`` (group ``crescale``) and
+``npt_crescale_anisotropic_step`` (group ``crescale_aniso``) on three Morse Cu
+systems (compute_stress=True) at 600 K and 1 GPa (internal units), tau = 5 dt,
+tau_p = 50 dt, compressibility 1e-4 bar^-1, with the reference's random numbers
+recorded per step in the order drawn: V-rescale (r1, Gamma deviate), the
+barostat normals (isotropic: one [S]; anisotropic: [S], [S, 3], [S]), V-rescale
+(r1, Gamma deviate).
 """
 
 from __future__ import annotations
@@ -52,47 +55,55 @@ def main(ref_root):
     dt = 0.002 * W.METAL_TIME
     p_ext = 1.0 * 0.006241509074460764  # 1 GPa in eV/A^3
     beta = 1e-4 / float(MetalUnits.pressure)
-    md = ref_npt.npt_crescale_init(st, morse, kT=torch.tensor(kT), dt=torch.tensor(dt),
-                                   tau_p=torch.tensor(50 * dt),
-                                   isothermal_compressibility=torch.tensor(beta))
-    normals, gammas = [], []
-    real_randn, real_gamma = torch.randn, torch._standard_gamma
-
-    def rec_randn(*a, **k):
-        x = real_randn(*a, **k)
-        normals.append(x.clone())
-        return x
-
-    def rec_gamma(*a, **k):
-        x = real_gamma(*a, **k)
-        gammas.append(x.clone())
-        return x
-
-    keys = ("positions", "momenta", "energy", "forces", "stress", "cell")
-    traj = [[getattr(md, k).clone().numpy() for k in keys]]
-    torch.randn, torch._standard_gamma = rec_randn, rec_gamma
-    try:
-        for _ in range(8):
-            md = ref_npt.npt_crescale_isotropic_step(md, morse, dt=torch.tensor(dt),
-                                                     kT=torch.tensor(kT),
-                                                     external_pressure=torch.tensor(p_ext),
-                                                     tau=torch.tensor(5 * dt))
-            traj.append([getattr(md, k).clone().numpy() for k in keys])
-    finally:
-        torch.randn, torch._standard_gamma = real_randn, real_gamma
-    assert len(normals) == 24 and len(gammas) == 16, (len(normals), len(gammas))
     out = {f"sys/{k}": cu3[k] for k in ("masses", "cell", "system_idx", "atomic_numbers")}
-    for i, k in enumerate(keys):
-        out[f"crescale/{k}"] = np.stack([t[i] for t in traj])
-    out["crescale/r1_a"] = np.stack([n.numpy() for n in normals[0::3]])
-    out["crescale/cell_noise"] = np.stack([n.numpy() for n in normals[1::3]])
-    out["crescale/r1_b"] = np.stack([n.numpy() for n in normals[2::3]])
-    out["crescale/gamma_a"] = np.stack([g.numpy() for g in gammas[0::2]])
-    out["crescale/gamma_b"] = np.stack([g.numpy() for g in gammas[1::2]])
-    for k in ("isothermal_compressibility", "tau_p"):
-        out[f"crescale/{k}"] = getattr(md, k).clone().numpy()
-    out["crescale/dt"], out["crescale/kT"] = np.array(dt), np.array(kT)
-    out["crescale/p_ext"], out["crescale/tau"] = np.array(p_ext), np.array(5 * dt)
+    real_randn, real_gamma = torch.randn, torch._standard_gamma
+    keys = ("positions", "momenta", "energy", "forces", "stress", "cell")
+    for grp, step_fn, n_normal in (("crescale", ref_npt.npt_crescale_isotropic_step, 3),
+                                   ("crescale_aniso", ref_npt.npt_crescale_anisotropic_step,
+                                    5)):
+        st.rng = 37
+        md = ref_npt.npt_crescale_init(st, morse, kT=torch.tensor(kT), dt=torch.tensor(dt),
+                                       tau_p=torch.tensor(50 * dt),
+                                       isothermal_compressibility=torch.tensor(beta))
+        normals, gammas = [], []
+
+        def rec_randn(*a, **k):
+            x = real_randn(*a, **k)
+            normals.append(x.clone())
+            return x
+
+        def rec_gamma(*a, **k):
+            x = real_gamma(*a, **k)
+            gammas.append(x.clone())
+            return x
+
+        traj = [[getattr(md, k).clone().numpy() for k in keys]]
+        torch.randn, torch._standard_gamma = rec_randn, rec_gamma
+        try:
+            for _ in range(8):
+                md = step_fn(md, morse, dt=torch.tensor(dt), kT=torch.tensor(kT),
+                             external_pressure=torch.tensor(p_ext), tau=torch.tensor(5 * dt))
+                traj.append([getattr(md, k).clone().numpy() for k in keys])
+        finally:
+            torch.randn, torch._standard_gamma = real_randn, real_gamma
+        assert len(normals) == 8 * n_normal and len(gammas) == 16, (len(normals), len(gammas))
+        for i, k in enumerate(keys):
+            out[f"{grp}/{k}"] = np.stack([t[i] for t in traj])
+        per = [normals[j::n_normal] for j in range(n_normal)]
+        out[f"{grp}/r1_a"] = np.stack([n.numpy() for n in per[0]])
+        out[f"{grp}/r1_b"] = np.stack([n.numpy() for n in per[-1]])
+        if n_normal == 3:
+            out[f"{grp}/cell_noise"] = np.stack([n.numpy() for n in per[1]])
+        else:  # (volume normal, z [S, 3], volume normal) -> [S, 5]
+            out[f"{grp}/cell_noise"] = np.stack([
+                np.concatenate([a.numpy()[:, None], b.numpy(), c.numpy()[:, None]], axis=1)
+                for a, b, c in zip(per[1], per[2], per[3])])
+        out[f"{grp}/gamma_a"] = np.stack([g.numpy() for g in gammas[0::2]])
+        out[f"{grp}/gamma_b"] = np.stack([g.numpy() for g in gammas[1::2]])
+        for k in ("isothermal_compressibility", "tau_p"):
+            out[f"{grp}/{k}"] = getattr(md, k).clone().numpy()
+        out[f"{grp}/dt"], out[f"{grp}/kT"] = np.array(dt), np.array(kT)
+        out[f"{grp}/p_ext"], out[f"{grp}/tau"] = np.array(p_ext), np.array(5 * dt)
     np.savez_compressed(os.path.join(HERE, "crescale.npz"), **out)
     print("C-rescale fixtures written to", HERE)
 

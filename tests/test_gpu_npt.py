@@ -74,14 +74,18 @@ def test_npt_device_noise_reproducible_and_barostat_responds():
     assert torch.isfinite(a.positions).all() and torch.isfinite(c.momenta).all()
 
 
-def test_npt_crescale_isotropic_matches_reference(golden):
-    """8 isotropic C-rescale steps vs the reference (golden/crescale.npz) with its
-    V-rescale and barostat draws injected; FP64 model, rtol 1e-9."""
+@pytest.mark.parametrize("grp", ["crescale", "crescale_aniso"])
+def test_npt_crescale_matches_reference(golden, grp):
+    """8 isotropic / anisotropic C-rescale steps vs the reference
+    (golden/crescale.npz) with its V-rescale and barostat draws injected; FP64
+    model, rtol 1e-9."""
     from tsb import integrators as I
     from tsb import models
     from tsb.state import MDState
 
-    s, g = golden["crescale"]["sys"], golden["crescale"]["crescale"]
+    s, g = golden["crescale"]["sys"], golden["crescale"][grp]
+    step = (I.npt_crescale_isotropic_step if grp == "crescale"
+            else I.npt_crescale_anisotropic_step)
     dev = torch.device("cuda")
     T = lambda x, dt=torch.float64: torch.as_tensor(x, dtype=dt, device=dev)  # noqa: E731
     n = len(s["masses"])
@@ -99,8 +103,7 @@ def test_npt_crescale_isotropic_matches_reference(golden):
         noise = (np.stack([g["r1_a"][k - 1], g["gamma_a"][k - 1]], axis=1),
                  g["cell_noise"][k - 1],
                  np.stack([g["r1_b"][k - 1], g["gamma_b"][k - 1]], axis=1))
-        st = I.npt_crescale_isotropic_step(st, m, dt=dt, kT=kT, external_pressure=p, tau=tau,
-                                           noise=noise)
+        st = step(st, m, dt=dt, kT=kT, external_pressure=p, tau=tau, noise=noise)
         for key in ("positions", "momenta", "cell", "stress", "energy"):
             np.testing.assert_allclose(getattr(st, key).cpu(), g[key][k], rtol=1e-9,
                                        atol=1e-12, err_msg=f"step {k} {key}")

@@ -299,10 +299,13 @@ def test_npt_langevin_isotropic_oracle_matches_reference(golden):
             np.testing.assert_allclose(st[key], g[key][k], rtol=rt, atol=1e-14, err_msg=key)
 
 
-def test_npt_crescale_isotropic_oracle_matches_reference(golden):
+@pytest.mark.parametrize("grp", ["crescale", "crescale_aniso"])
+def test_npt_crescale_oracle_matches_reference(golden, grp):
     from oracle import npt as onpt
 
-    s, g = golden["crescale"]["sys"], golden["crescale"]["crescale"]
+    s, g = golden["crescale"]["sys"], golden["crescale"][grp]
+    step = (onpt.npt_crescale_isotropic_step if grp == "crescale"
+            else onpt.npt_crescale_anisotropic_step)
     sysi = s["system_idx"].astype(np.int64)
     tab = opair.single_table(opair.MORSE, 2.866, 0.3429, 1.3588)
 
@@ -320,6 +323,6 @@ def test_npt_crescale_isotropic_oracle_matches_reference(golden):
     for k in range(1, g["positions"].shape[0]):
         noise = (g["r1_a"][k - 1], g["gamma_a"][k - 1], g["cell_noise"][k - 1],
                  g["r1_b"][k - 1], g["gamma_b"][k - 1])
-        st = onpt.npt_crescale_isotropic_step(st, fn, dt, kT, p_ext, tau, noise, sysi)
+        st = step(st, fn, dt, kT, p_ext, tau, noise, sysi)
         for key in ("positions", "momenta", "cell", "stress", "energy"):
             np.testing.assert_allclose(st[key], g[key][k], rtol=1e-9, atol=1e-12, err_msg=key)

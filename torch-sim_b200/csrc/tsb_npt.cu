@@ -24,13 +24,15 @@ namespace tsb {
 
 struct NptWork {
   int64_t *lo, *hi;  // [S] atom range of each system
-  double *scale;     // [S] exp(eps_new - eps_old)
+  double *scale;     // [S] exp(eps_new - eps_old), or the isotropic C-rescale factor
+  double *scale3;    // [3S] per-axis C-rescale factors
 };
 
 static void carve_npt(Carver &c, NptWork &w, int64_t ns) {
   w.lo = c.take<int64_t>(ns);
   w.hi = c.take<int64_t>(ns);
   w.scale = c.take<double>(ns);
+  w.scale3 = c.take<double>(3 * ns);
 }
 
 __global__ void k_npt_bounds(const int64_t *sys, int64_t n, int64_t *lo, int64_t *hi) {
@@ -221,6 +223,83 @@ __global__ void k_crescale_iso_atoms(int64_t n, P *x, P *p, const P *m, const in
   }
 }
 
+// Anisotropic C-rescale (npt.py:2282-2343): the volume half step, a traceless
+// random per-axis deformation exp(a~ dt + c z~) with a~_k = beta_T / (3 tau_p)
+// (P_kk - tr P / 3) and c = sqrt(2 beta_T kT dt / (3 tau_p)) / lambda', a second
+// volume half step, and per-axis factors mu_k = d_k (lambda'' / lambda)^(2/3).
+// noise [S, 5] = (volume normal, z_x, z_y, z_z, volume normal) in the reference's
+// order of draws, or Philox slots 3..7.
+template <class P>
+__global__ void __launch_bounds__(256)
+    k_crescale_aniso_cell(const int64_t *lo, const int64_t *hi, const P *p, const P *m,
+                          const P *stress, P *cell, const double *beta_t, const double *tau_p,
+                          const double *kT, const double *p_ext, const double *dt,
+                          const double *noise, uint64_t seed, uint64_t counter, double *mu3) {
+  __shared__ double sh[3][256 / 32];
+  const int64_t s = blockIdx.x;
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int64_t i = lo[s] + threadIdx.x; i < hi[s]; i += blockDim.x) {
+    const double mi = (double)m[i];
+    for (int c = 0; c < 3; ++c) {
+      const double pc = (double)p[3 * i + c];
+      acc[c] += pc * pc / mi;
+    }
+  }
+  for (int c = 0; c < 3; ++c) {
+    for (int o = 16; o > 0; o >>= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+    if ((threadIdx.x & 31) == 0) sh[c][threadIdx.x >> 5] = acc[c];
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  double two_k[3] = {0.0, 0.0, 0.0};
+  for (int c = 0; c < 3; ++c)
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) two_k[c] += sh[c][w];
+  double C[9];
+  for (int k = 0; k < 9; ++k) C[k] = (double)cell[9 * s + k];
+  const double vol = det3(C);
+  const P *st = stress + 9 * s;
+  double pd[3];
+  for (int c = 0; c < 3; ++c) pd[c] = two_k[c] / vol - (double)st[4 * c];
+  const double tr_p = pd[0] + pd[1] + pd[2];
+  const double kt = kT[s], h = dt[s], bt = beta_t[s], tp = tau_p[s];
+  double z[5];
+  for (int k = 0; k < 5; ++k)
+    z[k] = noise ? noise[5 * s + k] : thermo_normal(seed, s, counter, 3u + (uint32_t)k);
+  const double sqrt_vol = sqrt(vol);
+  const double pre_random = sqrt(kt * bt * h / (4.0 * tp));
+  const double pre = bt * sqrt_vol / (2.0 * tp);
+  const double drift = -pre * (p_ext[s] - tr_p / 3.0 - kt / (2.0 * vol)) * h / 2.0;
+  double lam = sqrt_vol + (drift + pre_random * z[0]);
+  const double c_rand = sqrt(2.0 * bt * kt * h / (3.0 * tp)) / lam;
+  const double zm = (z[1] + z[2] + z[3]) / 3.0;
+  double d[3];
+  for (int c = 0; c < 3; ++c)
+    d[c] = exp((bt / (3.0 * tp)) * (pd[c] - tr_p / 3.0) * h + c_rand * (z[1 + c] - zm));
+  lam += drift + pre_random * z[4];
+  const double f = pow(lam / sqrt_vol, 2.0 / 3.0);
+  for (int c = 0; c < 3; ++c) {
+    const double mu = d[c] * f;
+    mu3[3 * s + c] = mu;
+    for (int k = 0; k < 3; ++k) cell[9 * s + 3 * c + k] = (P)(mu * C[3 * c + k]);
+  }
+}
+
+// per atom and axis: r_k <- mu_k r_k + (mu_k + 1/mu_k) p_k dt / (2 m), p_k <- p_k / mu_k
+template <class P>
+__global__ void k_crescale_aniso_atoms(int64_t n, P *x, P *p, const P *m, const int64_t *sys,
+                                       const double *dt, const double *mu3) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t s = sys[i];
+  const double h = dt[s], mi = (double)m[i];
+  for (int c = 0; c < 3; ++c) {
+    const double f = mu3[3 * s + c], fi = 1.0 / f;
+    const double pc = (double)p[3 * i + c];
+    x[3 * i + c] = (P)(f * (double)x[3 * i + c] + (f + fi) * pc * h / (2.0 * mi));
+    p[3 * i + c] = (P)(fi * pc);
+  }
+}
+
 }  // namespace tsb
 
 using namespace tsb;
@@ -341,6 +420,42 @@ extern "C" int tsb_npt_crescale_iso(void *positions, void *momenta, const void *
     TSB_CRESCALE(float)
   }
 #undef TSB_CRESCALE
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
+
+extern "C" int tsb_npt_crescale_aniso(void *positions, void *momenta, const void *masses,
+                                      const int64_t *system_idx, int64_t n_atoms,
+                                      int64_t n_systems, int dtype, const void *stress,
+                                      void *cell, const double *compressibility,
+                                      const double *tau_p, const double *kT,
+                                      const double *p_ext, const double *dt, const double *noise,
+                                      uint64_t seed, uint64_t counter, void *workspace,
+                                      size_t workspace_bytes, void *stream) {
+  if (n_atoms < 1 || n_systems < 1 || !positions || !momenta || !masses || !system_idx ||
+      !stress || !cell || !compressibility || !tau_p || !kT || !p_ext || !dt)
+    return TSB_ERR_INVALID_ARG;
+  if (dtype != TSB_F32 && dtype != TSB_F64) return TSB_ERR_INVALID_ARG;
+  Carver c(workspace, workspace_bytes);
+  NptWork w;
+  carve_npt(c, w, n_systems);
+  if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaMemsetAsync(w.lo, 0, sizeof(int64_t) * n_systems, st);
+  cudaMemsetAsync(w.hi, 0, sizeof(int64_t) * n_systems, st);
+  k_npt_bounds<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, w.lo, w.hi);
+#define TSB_CRESCALE_A(P)                                                                    \
+  k_crescale_aniso_cell<P><<<(unsigned)n_systems, 256, 0, st>>>(                             \
+      w.lo, w.hi, (const P *)momenta, (const P *)masses, (const P *)stress, (P *)cell,       \
+      compressibility, tau_p, kT, p_ext, dt, noise, seed, counter, w.scale3);                \
+  k_crescale_aniso_atoms<P><<<grid_for(n_atoms), kBlock, 0, st>>>(                           \
+      n_atoms, (P *)positions, (P *)momenta, (const P *)masses, system_idx, dt, w.scale3);
+  if (dtype == TSB_F64) {
+    TSB_CRESCALE_A(double)
+  } else {
+    TSB_CRESCALE_A(float)
+  }
+#undef TSB_CRESCALE_A
   TSB_CHECK_LAUNCH();
   return TSB_OK;
 }

@@ -347,20 +347,13 @@ def _vrescale(state, kT_s, tau_s, dt_s, noise, seed, counter):
            ws.numel(), L.stream_ptr(dev))
 
 
-def npt_crescale_isotropic_step(state, model, *, dt, kT, external_pressure, tau=None,
-                                noise=None, **_kw):
-    """One isotropic C-rescale step (npt.py:2797-2901; Bernetti & Bussi 2020):
-    V-rescale(dt/2), kick(dt/2), barostat(dt), forces, kick(dt/2), V-rescale(dt/2).
-    The thermostat's tau defaults to dt, as the reference's code does.  The draws
-    (two V-rescale pairs (r1, Gamma deviate) and the barostat normal) come from
-    the device Philox stream (seed, system, step); ``noise = (vrescale_1 [S, 2],
-    cell [S], vrescale_2 [S, 2])`` supplies them instead."""
+def _crescale_step(state, model, *, dt, kT, external_pressure, tau, noise, entry, n_baro):
     _prepare(state)
     n_sys, n, dev = state.n_systems, state.n_atoms, state.device
     dt_s = _per_system(dt, n_sys, dev)
     kT_s = _per_system(kT, n_sys, dev)
     p_s = _per_system(external_pressure, n_sys, dev)
-    tau_s = _per_system(dt_s if tau is None else tau, n_sys, dev)
+    tau_s = _per_system(tau, n_sys, dev)
     half = (dt_s / 2).contiguous()
     for name in ("isothermal_compressibility", "tau_p"):
         v = getattr(state, name)
@@ -371,24 +364,50 @@ def npt_crescale_isotropic_step(state, model, *, dt, kT, external_pressure, tau=
     v1 = cn = v2 = None
     if noise is not None:
         v1, v2 = noise[0], noise[2]
-        cn = torch.as_tensor(noise[1], dtype=torch.float64, device=dev).reshape(n_sys)
-        cn = cn.contiguous()
+        cn = torch.as_tensor(noise[1], dtype=torch.float64, device=dev)
+        cn = cn.reshape(n_sys, n_baro).contiguous()
     seed = getattr(state, "_philox_seed", _seed_of(state)) & (2**64 - 1)
     counter = getattr(state, "_philox_counter", 0)
     _vrescale(state, kT_s, tau_s, half, v1, seed, counter)
     _kick(state, dt_s, 0.5)
     ws = L.Workspace.get(dev, L.load().tsb_npt_workspace_size(n_sys))
-    L.call("tsb_npt_crescale_iso", L.ptr(state.positions), L.ptr(state.momenta),
-           L.ptr(state.masses), L.ptr(state.system_idx), n, n_sys, L.dtype_code(state.dtype),
-           L.ptr(state.stress), L.ptr(state.cell), L.ptr(state.isothermal_compressibility),
-           L.ptr(state.tau_p), L.ptr(kT_s), L.ptr(p_s), L.ptr(dt_s), L.ptr(cn), seed, counter,
-           L.ptr(ws), ws.numel(), L.stream_ptr(dev))
+    L.call(entry, L.ptr(state.positions), L.ptr(state.momenta), L.ptr(state.masses),
+           L.ptr(state.system_idx), n, n_sys, L.dtype_code(state.dtype), L.ptr(state.stress),
+           L.ptr(state.cell), L.ptr(state.isothermal_compressibility), L.ptr(state.tau_p),
+           L.ptr(kT_s), L.ptr(p_s), L.ptr(dt_s), L.ptr(cn), seed, counter, L.ptr(ws),
+           ws.numel(), L.stream_ptr(dev))
     out = _apply_model(state, model)
     state.stress = out["stress"].to(state.dtype).contiguous()
     _kick(state, dt_s, 0.5)
     _vrescale(state, kT_s, tau_s, half, v2, seed, counter + 1)
     state._philox_seed, state._philox_counter = seed, counter + 2
     return state
+
+
+def npt_crescale_anisotropic_step(state, model, *, dt, kT, external_pressure, tau=None,
+                                  noise=None, **_kw):
+    """One anisotropic C-rescale step (npt.py:2645-2720): as the isotropic step with
+    per-axis cell factors; the thermostat's tau defaults to 100 dt, as the reference's
+    code does.  ``noise = (vrescale_1 [S, 2], barostat [S, 5], vrescale_2 [S, 2])``,
+    barostat = (volume normal, z_x, z_y, z_z, volume normal)."""
+    dt_s = _per_system(dt, state.n_systems, state.device)
+    return _crescale_step(state, model, dt=dt, kT=kT, external_pressure=external_pressure,
+                          tau=100 * dt_s if tau is None else tau, noise=noise,
+                          entry="tsb_npt_crescale_aniso", n_baro=5)
+
+
+def npt_crescale_isotropic_step(state, model, *, dt, kT, external_pressure, tau=None,
+                                noise=None, **_kw):
+    """One isotropic C-rescale step (npt.py:2797-2901; Bernetti & Bussi 2020):
+    V-rescale(dt/2), kick(dt/2), barostat(dt), forces, kick(dt/2), V-rescale(dt/2).
+    The thermostat's tau defaults to dt, as the reference's code does.  The draws
+    (two V-rescale pairs (r1, Gamma deviate) and the barostat normal) come from
+    the device Philox stream (seed, system, step); ``noise = (vrescale_1 [S, 2],
+    cell [S], vrescale_2 [S, 2])`` supplies them instead."""
+    dt_s = _per_system(dt, state.n_systems, state.device)
+    return _crescale_step(state, model, dt=dt, kT=kT, external_pressure=external_pressure,
+                          tau=dt_s if tau is None else tau, noise=noise,
+                          entry="tsb_npt_crescale_iso", n_baro=1)
 
 
 def npt_langevin_isotropic_init(state, model, *, kT, dt, alpha=None, cell_alpha=None,
