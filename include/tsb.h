@@ -197,6 +197,27 @@ int tsb_npt_crescale_aniso(void *positions, void *momenta, const void *masses,
                            uint64_t seed, uint64_t counter, void *workspace,
                            size_t workspace_bytes, void *stream);
 
+/* tsb_npt_crescale_tri: the triclinic barostat step of npt_crescale_triclinic_step
+ * (npt.py:2186-2280, 2517-2644) or, with average != 0, of
+ * npt_crescale_triclinic_average_step (:2376-2452, 2721-2796; average kinetic
+ * pressure (3N - 3)/3 kT / V, momenta unscaled).  Per system: the pressure tensor,
+ * for a tensor external pressure p_ext_tensor [S, 9] (NULL: scalar p_ext [S]) the
+ * deviatoric correction through initial_cell_inv [S, 9] and initial_volume [S],
+ * two half steps of sqrt(V), R = GramSchmidt(expm(a~ dt + c Z~)) (V''/V)^(1/3),
+ * cell <- cell R^T; per atom r <- R r + (M + R) p dt / (2 m), p <- M p with
+ * M = inv(R)^T (I for the average variant).  noise [S, 11] = (volume normal, 3x3
+ * normals row-major, volume normal) or NULL for Philox draws.  Workspace:
+ * tsb_npt_workspace_size. */
+int tsb_npt_crescale_tri(void *positions, void *momenta, const void *masses,
+                         const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
+                         int dtype, const void *stress, void *cell,
+                         const double *compressibility, const double *tau_p, const double *kT,
+                         const double *p_ext, const double *p_ext_tensor,
+                         const double *initial_cell_inv, const double *initial_volume,
+                         const double *dt, int average, const double *noise, uint64_t seed,
+                         uint64_t counter, void *workspace, size_t workspace_bytes,
+                         void *stream);
+
 /* ---- batched Verlet lists (many systems, moving atoms and cells) ----------
  * Replaces the per-call neighbour search inside PairPotentialModel.forward
  * (torch_sim/models/pair_potential.py:168-174, 351-464) for a batch whose atoms

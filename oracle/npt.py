@@ -16,6 +16,10 @@ step (Gronbech-Jensen & Farago GJF scheme), noise passed in:
   :2455-2492 with the instantaneous pressure of quantities.py:156-198)
 * ``npt_crescale_anisotropic_step`` <- npt.py:2645-2720 with
   ``_crescale_anisotropic_barostat_step`` (:2282-2343)
+* ``npt_crescale_triclinic_step`` <- npt.py:2517-2644 with
+  ``_crescale_triclinic_barostat_step`` (:2186-2280), ``_compute_deviatoric_correction``
+  (:2145-2183), ``rotate_gram_schmidt`` (:2093-2126); ``average=True`` gives
+  ``npt_crescale_triclinic_average_step`` (:2721-2796, barostat :2376-2452)
 """
 
 from __future__ import annotations
@@ -148,6 +152,85 @@ def npt_crescale_anisotropic_step(st, force_fn, dt, kT, p_ext, tau, noise, syste
     q = mu_a * st["positions"] + (mu_a + 1 / mu_a) * p * dt / (2 * m[:, None])
     p = p / mu_a
     cell = mu[:, :, None] * st["cell"]
+    e, f, s = force_fn(q, cell)
+    st.update(positions=q, momenta=p, cell=cell, forces=f, energy=e, stress=s)
+    st["momenta"] = st["momenta"] + st["forces"] * (dt / 2)
+    st["momenta"] = _vrescale(st, kT, tau, dt / 2, r1b, gb, system_idx)
+    return st
+
+
+def _gram_schmidt_lower(box):
+    out = np.zeros_like(box)
+    a, b, c = box[:, :, 0], box[:, :, 1], box[:, :, 2]
+    out[:, 0, 0] = np.linalg.norm(a, axis=1)
+    out[:, 1, 0] = (a * b).sum(1) / out[:, 0, 0]
+    out[:, 1, 1] = np.sqrt((b * b).sum(1) - out[:, 1, 0] ** 2)
+    out[:, 2, 0] = (a * c).sum(1) / out[:, 0, 0]
+    out[:, 2, 1] = ((b * c).sum(1) - out[:, 2, 0] * out[:, 1, 0]) / out[:, 1, 1]
+    out[:, 2, 2] = np.sqrt((c * c).sum(1) - out[:, 2, 0] ** 2 - out[:, 2, 1] ** 2)
+    return out
+
+
+def npt_crescale_triclinic_step(st, force_fn, dt, kT, p_ext, tau, noise, system_idx,
+                                average=False):
+    """noise = (r1_a, gamma_a, baro [S, 11] = (volume normal, 3x3 normals row-major,
+    volume normal), r1_b, gamma_b).  p_ext: scalar, or [3, 3] for the deviatoric
+    correction (st then holds initial_cell_inv [S,3,3] and initial_volume [S])."""
+    from scipy.linalg import expm
+
+    st = dict(st)
+    r1a, ga, zb, r1b, gb = noise
+    m = st["masses"]
+    st["momenta"] = _vrescale(st, kT, tau, dt / 2, r1a, ga, system_idx)
+    st["momenta"] = st["momenta"] + st["forces"] * (dt / 2)
+    cell = st["cell"]
+    vol = np.linalg.det(cell)
+    p = st["momenta"]
+    n_sys = len(vol)
+    eye = np.eye(3)
+    if average:
+        nat = np.bincount(system_idx, minlength=n_sys)
+        pint = ((3 * nat - 3) / 3 * kT / vol)[:, None, None] * eye - st["stress"]
+    else:
+        kin = np.zeros((n_sys, 3, 3))
+        np.add.at(kin, system_idx, np.einsum("ni,nj->nij", p, p) / m[:, None, None])
+        pint = kin / vol[:, None, None] - st["stress"]
+    tr_p = np.einsum("sii->s", pint)
+    bt, tp = st["isothermal_compressibility"], st["tau_p"]
+    sqrt_vol = np.sqrt(vol)
+    pre_random = np.sqrt(kT * bt * dt / (4 * tp))
+    pre = bt * sqrt_vol / (2 * tp)
+    p_ext = np.asarray(p_ext, dtype=np.float64)
+    pdrive = pint
+    if p_ext.ndim >= 2:
+        T = np.broadcast_to(p_ext, (n_sys, 3, 3))
+        hydro = np.einsum("sii->s", T) / 3
+        sdev = T - hydro[:, None, None] * eye
+        ci = st["initial_cell_inv"]
+        sig = st["initial_volume"][:, None, None] * (np.transpose(ci, (0, 2, 1)) @ sdev @ ci)
+        sym = 0.5 * (sig + np.transpose(sig, (0, 2, 1)))
+        pdev = np.transpose(cell, (0, 2, 1)) @ sym @ cell / vol[:, None, None]
+        eff = hydro + np.einsum("sii->s", pdev) / 3
+        pdrive = pint - pdev
+    else:
+        eff = p_ext
+    drift = -pre * (eff - tr_p / 3 - kT / (2 * vol)) * dt / 2
+    lam = sqrt_vol + (drift + pre_random * zb[:, 0])
+    prm = np.sqrt(2 * bt * kT * dt / (3 * tp)) / lam
+    tr_d = np.einsum("sii->s", pdrive)
+    a_t = (bt / (3 * tp))[:, None, None] * (pdrive - (tr_d / 3)[:, None, None] * eye)
+    Z = zb[:, 1:10].reshape(n_sys, 3, 3)
+    Zt = Z - (np.einsum("sii->s", Z) / 3)[:, None, None] * eye
+    D = np.stack([expm(x) for x in a_t * dt + prm[:, None, None] * Zt])
+    D = _gram_schmidt_lower(D)
+    lam = lam + (drift + pre_random * zb[:, 10])
+    R = D * ((lam / sqrt_vol) ** (2.0 / 3.0))[:, None, None]
+    M = np.broadcast_to(eye, R.shape) if average else np.transpose(np.linalg.inv(R), (0, 2, 1))
+    Ra, Ma = R[system_idx], M[system_idx]
+    q = np.einsum("nij,nj->ni", Ra, st["positions"]) + \
+        np.einsum("nij,nj->ni", Ma + Ra, p) * dt / (2 * m[:, None])
+    p = np.einsum("nij,nj->ni", Ma, p)
+    cell = cell @ np.transpose(R, (0, 2, 1))
     e, f, s = force_fn(q, cell)
     st.update(positions=q, momenta=p, cell=cell, forces=f, energy=e, stress=s)
     st["momenta"] = st["momenta"] + st["forces"] * (dt / 2)

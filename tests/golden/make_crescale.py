@@ -6,13 +6,16 @@ Run in a container where the reference source tree is present::
     python tests/golden/make_crescale.py /path/to/torch-sim
 
 Writes ``crescale.npz`` beside this script: 8 steps each of
-``npt_crescale_isotropic_step`` (group ``crescale``) and
-``npt_crescale_anisotropic_step`` (group ``crescale_aniso``) on three Morse Cu
+``npt_crescale_isotropic_step`` (group ``crescale``),
+``npt_crescale_anisotropic_step`` (``crescale_aniso``),
+``npt_crescale_triclinic_step`` with a scalar and with a non-hydrostatic tensor
+pressure (``crescale_tri``, ``crescale_tri_dev``) and
+``npt_crescale_triclinic_average_step`` (``crescale_tri_avg``) on three Morse Cu
 systems (compute_stress=True) at 600 K and 1 GPa (internal units), tau = 5 dt,
 tau_p = 50 dt, compressibility 1e-4 bar^-1, with the reference's random numbers
 recorded per step in the order drawn: V-rescale (r1, Gamma deviate), the
-barostat normals (isotropic: one [S]; anisotropic: [S], [S, 3], [S]), V-rescale
-(r1, Gamma deviate).
+barostat normals (isotropic: one [S]; anisotropic: [S], [S, 3], [S]; triclinic:
+[S], [S, 3, 3], [S]), V-rescale (r1, Gamma deviate).
 """
 
 from __future__ import annotations
@@ -58,9 +61,14 @@ def main(ref_root):
     out = {f"sys/{k}": cu3[k] for k in ("masses", "cell", "system_idx", "atomic_numbers")}
     real_randn, real_gamma = torch.randn, torch._standard_gamma
     keys = ("positions", "momenta", "energy", "forces", "stress", "cell")
-    for grp, step_fn, n_normal in (("crescale", ref_npt.npt_crescale_isotropic_step, 3),
-                                   ("crescale_aniso", ref_npt.npt_crescale_anisotropic_step,
-                                    5)):
+    # a non-hydrostatic external pressure for the deviatoric correction
+    p_tensor = torch.tensor([[1.2, 0.1, 0.0], [0.1, 0.9, -0.05], [0.0, -0.05, 1.0]]) * p_ext
+    runs = (("crescale", ref_npt.npt_crescale_isotropic_step, 3, p_ext),
+            ("crescale_aniso", ref_npt.npt_crescale_anisotropic_step, 5, p_ext),
+            ("crescale_tri", ref_npt.npt_crescale_triclinic_step, 5, p_ext),
+            ("crescale_tri_dev", ref_npt.npt_crescale_triclinic_step, 5, p_tensor),
+            ("crescale_tri_avg", ref_npt.npt_crescale_triclinic_average_step, 5, p_ext))
+    for grp, step_fn, n_normal, pe in runs:
         st.rng = 37
         md = ref_npt.npt_crescale_init(st, morse, kT=torch.tensor(kT), dt=torch.tensor(dt),
                                        tau_p=torch.tensor(50 * dt),
@@ -82,7 +90,7 @@ def main(ref_root):
         try:
             for _ in range(8):
                 md = step_fn(md, morse, dt=torch.tensor(dt), kT=torch.tensor(kT),
-                             external_pressure=torch.tensor(p_ext), tau=torch.tensor(5 * dt))
+                             external_pressure=torch.as_tensor(pe), tau=torch.tensor(5 * dt))
                 traj.append([getattr(md, k).clone().numpy() for k in keys])
         finally:
             torch.randn, torch._standard_gamma = real_randn, real_gamma
@@ -94,16 +102,17 @@ def main(ref_root):
         out[f"{grp}/r1_b"] = np.stack([n.numpy() for n in per[-1]])
         if n_normal == 3:
             out[f"{grp}/cell_noise"] = np.stack([n.numpy() for n in per[1]])
-        else:  # (volume normal, z [S, 3], volume normal) -> [S, 5]
+        else:  # (volume normal, z [S, 3] or Z [S, 3, 3], volume normal) -> [S, 5 | 11]
             out[f"{grp}/cell_noise"] = np.stack([
-                np.concatenate([a.numpy()[:, None], b.numpy(), c.numpy()[:, None]], axis=1)
+                np.concatenate([a.numpy()[:, None], b.numpy().reshape(len(a), -1),
+                                c.numpy()[:, None]], axis=1)
                 for a, b, c in zip(per[1], per[2], per[3])])
         out[f"{grp}/gamma_a"] = np.stack([g.numpy() for g in gammas[0::2]])
         out[f"{grp}/gamma_b"] = np.stack([g.numpy() for g in gammas[1::2]])
         for k in ("isothermal_compressibility", "tau_p"):
             out[f"{grp}/{k}"] = getattr(md, k).clone().numpy()
         out[f"{grp}/dt"], out[f"{grp}/kT"] = np.array(dt), np.array(kT)
-        out[f"{grp}/p_ext"], out[f"{grp}/tau"] = np.array(p_ext), np.array(5 * dt)
+        out[f"{grp}/p_ext"], out[f"{grp}/tau"] = np.asarray(pe), np.array(5 * dt)
     np.savez_compressed(os.path.join(HERE, "crescale.npz"), **out)
     print("C-rescale fixtures written to", HERE)
 

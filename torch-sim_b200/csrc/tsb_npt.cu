@@ -19,6 +19,7 @@
 #include "tsb_common.cuh"
 #include "tsb_rng.cuh"
 #include "tsb_thermostat.cuh"
+#include "tsb_mat3.cuh"
 
 namespace tsb {
 
@@ -26,6 +27,8 @@ struct NptWork {
   int64_t *lo, *hi;  // [S] atom range of each system
   double *scale;     // [S] exp(eps_new - eps_old), or the isotropic C-rescale factor
   double *scale3;    // [3S] per-axis C-rescale factors
+  double *kin6;      // [6S] sum_i p p^T / m per system (xx, yy, zz, xy, xz, yz)
+  double *rv;        // [18S] triclinic C-rescale: R and the momentum matrix per system
 };
 
 static void carve_npt(Carver &c, NptWork &w, int64_t ns) {
@@ -33,6 +36,8 @@ static void carve_npt(Carver &c, NptWork &w, int64_t ns) {
   w.hi = c.take<int64_t>(ns);
   w.scale = c.take<double>(ns);
   w.scale3 = c.take<double>(3 * ns);
+  w.kin6 = c.take<double>(6 * ns);
+  w.rv = c.take<double>(18 * ns);
 }
 
 __global__ void k_npt_bounds(const int64_t *sys, int64_t n, int64_t *lo, int64_t *hi) {
@@ -300,6 +305,161 @@ __global__ void k_crescale_aniso_atoms(int64_t n, P *x, P *p, const P *m, const 
   }
 }
 
+// Triclinic C-rescale (npt.py:2186-2280; average variant :2376-2452) in three
+// launches: (a) one block per system sums the kinetic tensor sum_i p p^T / m in
+// FP64 in a fixed order; (b) one thread per system does the 3x3 algebra
+// (pressure tensor, deviatoric correction for a tensor external pressure,
+// sqrt(V) half steps, matrix exponential of the traceless drive plus noise,
+// Gram-Schmidt rotation to lower-triangular form, R and the momentum matrix
+// inv(R)^T, cell <- cell R^T); (c) one thread per atom applies
+// r <- R r + (M + R) p dt / (2 m), p <- M p.  The average variant uses the
+// average kinetic pressure (3N - 3)/3 kT / V and M = I (momenta unscaled).
+// noise [S, 11] = (volume normal, 3x3 normals row-major, volume normal) in the
+// reference's order of draws, or Philox slots 3..13.
+template <class P>
+__global__ void __launch_bounds__(256)
+    k_crescale_kinetic(const int64_t *lo, const int64_t *hi, const P *p, const P *m,
+                       double *kin6) {
+  __shared__ double sh[6][256 / 32];
+  const int64_t s = blockIdx.x;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int64_t i = lo[s] + threadIdx.x; i < hi[s]; i += blockDim.x) {
+    const double mi = (double)m[i];
+    const double px = (double)p[3 * i], py = (double)p[3 * i + 1], pz = (double)p[3 * i + 2];
+    acc[0] += px * px / mi;
+    acc[1] += py * py / mi;
+    acc[2] += pz * pz / mi;
+    acc[3] += px * py / mi;
+    acc[4] += px * pz / mi;
+    acc[5] += py * pz / mi;
+  }
+  for (int c = 0; c < 6; ++c) {
+    for (int o = 16; o > 0; o >>= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+    if ((threadIdx.x & 31) == 0) sh[c][threadIdx.x >> 5] = acc[c];
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[threadIdx.x][w];
+    kin6[6 * s + threadIdx.x] = t;
+  }
+}
+
+__device__ inline M3 gram_schmidt_lower(const M3 &D) {
+  // columns a, b, c of D -> lower-triangular box (npt.py:2093-2126)
+  double a[3], b[3], c[3];
+  for (int r = 0; r < 3; ++r) {
+    a[r] = D(r, 0);
+    b[r] = D(r, 1);
+    c[r] = D(r, 2);
+  }
+  auto dot = [](const double *x, const double *y) { return x[0] * y[0] + x[1] * y[1] + x[2] * y[2]; };
+  M3 o = m3_zero();
+  o(0, 0) = sqrt(dot(a, a));
+  o(1, 0) = dot(a, b) / o(0, 0);
+  o(1, 1) = sqrt(dot(b, b) - o(1, 0) * o(1, 0));
+  o(2, 0) = dot(a, c) / o(0, 0);
+  o(2, 1) = (dot(b, c) - o(2, 0) * o(1, 0)) / o(1, 1);
+  o(2, 2) = sqrt(dot(c, c) - o(2, 0) * o(2, 0) - o(2, 1) * o(2, 1));
+  return o;
+}
+
+template <class P>
+__global__ void k_crescale_tri_cell(int64_t ns, const int64_t *lo, const int64_t *hi,
+                                    const double *kin6, const P *stress, P *cell,
+                                    const double *beta_t, const double *tau_p, const double *kT,
+                                    const double *p_ext, const double *p_ext_t,
+                                    const double *cell0_inv, const double *vol0, const double *dt,
+                                    int average, const double *noise, uint64_t seed,
+                                    uint64_t counter, double *rv) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  M3 C;
+  for (int k = 0; k < 9; ++k) C.a[k] = (double)cell[9 * s + k];
+  const double vol = m3_det(C);
+  const double kt = kT[s], h = dt[s], bt = beta_t[s], tp = tau_p[s];
+  M3 Pint;
+  if (average) {
+    const double pref = ((3.0 * (double)(hi[s] - lo[s]) - 3.0) / 3.0) * kt / vol;
+    for (int k = 0; k < 9; ++k) Pint.a[k] = (k % 4 == 0 ? pref : 0.0) - (double)stress[9 * s + k];
+  } else {
+    const double *q = kin6 + 6 * s;
+    const double K[9] = {q[0], q[3], q[4], q[3], q[1], q[5], q[4], q[5], q[2]};
+    for (int k = 0; k < 9; ++k) Pint.a[k] = K[k] / vol - (double)stress[9 * s + k];
+  }
+  const double trP = Pint.a[0] + Pint.a[4] + Pint.a[8];
+  const double sqrt_vol = sqrt(vol);
+  const double pre_random = sqrt(kt * bt * h / (4.0 * tp));
+  const double pre = bt * sqrt_vol / (2.0 * tp);
+  double eff = average || !p_ext_t ? p_ext[s] : 0.0;
+  M3 Pdrive = Pint;
+  if (!average && p_ext_t) {
+    // deviatoric correction (npt.py:2145-2183)
+    M3 T;
+    for (int k = 0; k < 9; ++k) T.a[k] = p_ext_t[9 * s + k];
+    const double hydro = (T.a[0] + T.a[4] + T.a[8]) / 3.0;
+    M3 Sd = T;
+    Sd.a[0] -= hydro;
+    Sd.a[4] -= hydro;
+    Sd.a[8] -= hydro;
+    M3 Ci;
+    for (int k = 0; k < 9; ++k) Ci.a[k] = cell0_inv[9 * s + k];
+    const M3 sig = m3_scale(m3_mul(m3_mul(m3_T(Ci), Sd), Ci), vol0[s]);
+    const M3 sym = m3_scale(m3_add(sig, m3_T(sig)), 0.5);
+    const M3 Pdev = m3_scale(m3_mul(m3_mul(m3_T(C), sym), C), 1.0 / vol);
+    eff = hydro + (Pdev.a[0] + Pdev.a[4] + Pdev.a[8]) / 3.0;
+    Pdrive = m3_add(Pint, Pdev, 1.0, -1.0);
+  }
+  double z[11];
+  for (int k = 0; k < 11; ++k)
+    z[k] = noise ? noise[11 * s + k] : thermo_normal(seed, s, counter, 3u + (uint32_t)k);
+  const double drift = -pre * (eff - trP / 3.0 - kt / (2.0 * vol)) * h / 2.0;
+  double lam = sqrt_vol + (drift + pre_random * z[0]);
+  const double prm = sqrt(2.0 * bt * kt * h / (3.0 * tp)) / lam;
+  const double trD = Pdrive.a[0] + Pdrive.a[4] + Pdrive.a[8];
+  const double trZ = z[1] + z[5] + z[9];
+  M3 X;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      const double a_t = (bt / (3.0 * tp)) * (Pdrive(r, c) - (r == c ? trD / 3.0 : 0.0));
+      const double zt = z[1 + 3 * r + c] - (r == c ? trZ / 3.0 : 0.0);
+      X(r, c) = a_t * h + prm * zt;
+    }
+  const M3 D = gram_schmidt_lower(m3_expm(X));
+  lam += drift + pre_random * z[10];
+  const double f = pow(lam / sqrt_vol, 2.0 / 3.0);
+  const M3 R = m3_scale(D, f);
+  const M3 Mp = average ? m3_eye() : m3_T(m3_inv(R));
+  for (int k = 0; k < 9; ++k) {
+    rv[18 * s + k] = R.a[k];
+    rv[18 * s + 9 + k] = Mp.a[k];
+  }
+  const M3 Cn = m3_mul(C, m3_T(R));
+  for (int k = 0; k < 9; ++k) cell[9 * s + k] = (P)Cn.a[k];
+}
+
+template <class P>
+__global__ void k_crescale_tri_atoms(int64_t n, P *x, P *p, const P *m, const int64_t *sys,
+                                     const double *dt, const double *rv) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t s = sys[i];
+  const double *R = rv + 18 * s, *M = rv + 18 * s + 9;
+  const double h = dt[s], mi = (double)m[i];
+  const double r0[3] = {(double)x[3 * i], (double)x[3 * i + 1], (double)x[3 * i + 2]};
+  const double p0[3] = {(double)p[3 * i], (double)p[3 * i + 1], (double)p[3 * i + 2]};
+  for (int a = 0; a < 3; ++a) {
+    double rr = 0.0, mp = 0.0, np = 0.0;
+    for (int b = 0; b < 3; ++b) {
+      rr += R[3 * a + b] * r0[b];
+      mp += (M[3 * a + b] + R[3 * a + b]) * p0[b];
+      np += M[3 * a + b] * p0[b];
+    }
+    x[3 * i + a] = (P)(rr + mp * h / (2.0 * mi));
+    p[3 * i + a] = (P)np;
+  }
+}
+
 }  // namespace tsb
 
 using namespace tsb;
@@ -456,6 +616,49 @@ extern "C" int tsb_npt_crescale_aniso(void *positions, void *momenta, const void
     TSB_CRESCALE_A(float)
   }
 #undef TSB_CRESCALE_A
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
+
+extern "C" int tsb_npt_crescale_tri(void *positions, void *momenta, const void *masses,
+                                    const int64_t *system_idx, int64_t n_atoms,
+                                    int64_t n_systems, int dtype, const void *stress,
+                                    void *cell, const double *compressibility,
+                                    const double *tau_p, const double *kT, const double *p_ext,
+                                    const double *p_ext_tensor, const double *initial_cell_inv,
+                                    const double *initial_volume, const double *dt, int average,
+                                    const double *noise, uint64_t seed, uint64_t counter,
+                                    void *workspace, size_t workspace_bytes, void *stream) {
+  if (n_atoms < 1 || n_systems < 1 || !positions || !momenta || !masses || !system_idx ||
+      !stress || !cell || !compressibility || !tau_p || !kT || !p_ext || !dt)
+    return TSB_ERR_INVALID_ARG;
+  if (p_ext_tensor && (average || !initial_cell_inv || !initial_volume))
+    return TSB_ERR_INVALID_ARG;
+  if (dtype != TSB_F32 && dtype != TSB_F64) return TSB_ERR_INVALID_ARG;
+  Carver c(workspace, workspace_bytes);
+  NptWork w;
+  carve_npt(c, w, n_systems);
+  if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaMemsetAsync(w.lo, 0, sizeof(int64_t) * n_systems, st);
+  cudaMemsetAsync(w.hi, 0, sizeof(int64_t) * n_systems, st);
+  k_npt_bounds<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, w.lo, w.hi);
+#define TSB_CRESCALE_T(P)                                                                    \
+  if (!average)                                                                              \
+    k_crescale_kinetic<P><<<(unsigned)n_systems, 256, 0, st>>>(                              \
+        w.lo, w.hi, (const P *)momenta, (const P *)masses, w.kin6);                          \
+  k_crescale_tri_cell<P><<<grid_for(n_systems, 64), 64, 0, st>>>(                            \
+      n_systems, w.lo, w.hi, w.kin6, (const P *)stress, (P *)cell, compressibility, tau_p,   \
+      kT, p_ext, p_ext_tensor, initial_cell_inv, initial_volume, dt, average, noise, seed,   \
+      counter, w.rv);                                                                        \
+  k_crescale_tri_atoms<P><<<grid_for(n_atoms), kBlock, 0, st>>>(                             \
+      n_atoms, (P *)positions, (P *)momenta, (const P *)masses, system_idx, dt, w.rv);
+  if (dtype == TSB_F64) {
+    TSB_CRESCALE_T(double)
+  } else {
+    TSB_CRESCALE_T(float)
+  }
+#undef TSB_CRESCALE_T
   TSB_CHECK_LAUNCH();
   return TSB_OK;
 }

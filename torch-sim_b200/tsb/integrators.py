@@ -347,12 +347,12 @@ def _vrescale(state, kT_s, tau_s, dt_s, noise, seed, counter):
            ws.numel(), L.stream_ptr(dev))
 
 
-def _crescale_step(state, model, *, dt, kT, external_pressure, tau, noise, entry, n_baro):
+def _crescale_step(state, model, *, dt, kT, external_pressure, tau, noise, n_baro, barostat):
+    """V-rescale(dt/2), kick(dt/2), ``barostat``, forces, kick(dt/2), V-rescale(dt/2)."""
     _prepare(state)
-    n_sys, n, dev = state.n_systems, state.n_atoms, state.device
+    n_sys, dev = state.n_systems, state.device
     dt_s = _per_system(dt, n_sys, dev)
     kT_s = _per_system(kT, n_sys, dev)
-    p_s = _per_system(external_pressure, n_sys, dev)
     tau_s = _per_system(tau, n_sys, dev)
     half = (dt_s / 2).contiguous()
     for name in ("isothermal_compressibility", "tau_p"):
@@ -371,17 +371,80 @@ def _crescale_step(state, model, *, dt, kT, external_pressure, tau, noise, entry
     _vrescale(state, kT_s, tau_s, half, v1, seed, counter)
     _kick(state, dt_s, 0.5)
     ws = L.Workspace.get(dev, L.load().tsb_npt_workspace_size(n_sys))
-    L.call(entry, L.ptr(state.positions), L.ptr(state.momenta), L.ptr(state.masses),
-           L.ptr(state.system_idx), n, n_sys, L.dtype_code(state.dtype), L.ptr(state.stress),
-           L.ptr(state.cell), L.ptr(state.isothermal_compressibility), L.ptr(state.tau_p),
-           L.ptr(kT_s), L.ptr(p_s), L.ptr(dt_s), L.ptr(cn), seed, counter, L.ptr(ws),
-           ws.numel(), L.stream_ptr(dev))
+    barostat(state, kT_s, dt_s, cn, seed, counter, ws)
     out = _apply_model(state, model)
     state.stress = out["stress"].to(state.dtype).contiguous()
     _kick(state, dt_s, 0.5)
     _vrescale(state, kT_s, tau_s, half, v2, seed, counter + 1)
     state._philox_seed, state._philox_counter = seed, counter + 2
     return state
+
+
+def _crescale_simple(entry, external_pressure):
+    """Barostat call of the isotropic / anisotropic C-rescale entry points."""
+
+    def call(state, kT_s, dt_s, cn, seed, counter, ws):
+        p_s = _per_system(external_pressure, state.n_systems, state.device)
+        L.call(entry, L.ptr(state.positions), L.ptr(state.momenta), L.ptr(state.masses),
+               L.ptr(state.system_idx), state.n_atoms, state.n_systems,
+               L.dtype_code(state.dtype), L.ptr(state.stress), L.ptr(state.cell),
+               L.ptr(state.isothermal_compressibility), L.ptr(state.tau_p), L.ptr(kT_s),
+               L.ptr(p_s), L.ptr(dt_s), L.ptr(cn), seed, counter, L.ptr(ws), ws.numel(),
+               L.stream_ptr(state.device))
+
+    return call
+
+
+def _crescale_triclinic(external_pressure, average):
+    """Barostat call of tsb_npt_crescale_tri; a [3, 3] or [S, 3, 3] external pressure
+    takes the deviatoric correction (npt.py:2145-2183)."""
+
+    def call(state, kT_s, dt_s, cn, seed, counter, ws):
+        n_sys, dev = state.n_systems, state.device
+        pe = torch.as_tensor(external_pressure, dtype=torch.float64, device=dev)
+        pt = None
+        if pe.ndim >= 2:
+            if average:
+                raise ValueError("the average-pressure variant takes a scalar pressure")
+            pt = pe.expand(n_sys, 3, 3).reshape(n_sys, 9).contiguous()
+            p_s = torch.zeros(n_sys, dtype=torch.float64, device=dev)
+        else:
+            p_s = _per_system(pe, n_sys, dev)
+        ci = state.initial_cell_inv.to(torch.float64).reshape(n_sys, 9).contiguous()
+        v0 = state.initial_volume.to(torch.float64).contiguous()
+        L.call("tsb_npt_crescale_tri", L.ptr(state.positions), L.ptr(state.momenta),
+               L.ptr(state.masses), L.ptr(state.system_idx), state.n_atoms, n_sys,
+               L.dtype_code(state.dtype), L.ptr(state.stress), L.ptr(state.cell),
+               L.ptr(state.isothermal_compressibility), L.ptr(state.tau_p), L.ptr(kT_s),
+               L.ptr(p_s), L.ptr(pt), L.ptr(ci), L.ptr(v0), L.ptr(dt_s), int(average),
+               L.ptr(cn), seed, counter, L.ptr(ws), ws.numel(), L.stream_ptr(dev))
+
+    return call
+
+
+def npt_crescale_triclinic_step(state, model, *, dt, kT, external_pressure, tau=None,
+                                noise=None, **_kw):
+    """One triclinic C-rescale step (npt.py:2517-2644; Del Tatto et al. 2022):
+    matrix deformation from the traceless pressure tensor, Gram-Schmidt rotated to
+    lower-triangular form; a tensor ``external_pressure`` takes the deviatoric
+    correction.  tau defaults to dt.  ``noise = (vrescale_1 [S, 2], barostat
+    [S, 11], vrescale_2 [S, 2])``, barostat = (volume normal, 3x3 normals
+    row-major, volume normal)."""
+    dt_s = _per_system(dt, state.n_systems, state.device)
+    return _crescale_step(state, model, dt=dt, kT=kT, external_pressure=external_pressure,
+                          tau=dt_s if tau is None else tau, noise=noise, n_baro=11,
+                          barostat=_crescale_triclinic(external_pressure, False))
+
+
+def npt_crescale_triclinic_average_step(state, model, *, dt, kT, external_pressure,
+                                        tau=None, noise=None, **_kw):
+    """One triclinic C-rescale step with the average kinetic pressure
+    (3N - 3)/3 kT / V in place of the instantaneous one and unscaled momenta
+    (npt.py:2376-2452, 2721-2796).  Arguments as npt_crescale_triclinic_step."""
+    dt_s = _per_system(dt, state.n_systems, state.device)
+    return _crescale_step(state, model, dt=dt, kT=kT, external_pressure=external_pressure,
+                          tau=dt_s if tau is None else tau, noise=noise, n_baro=11,
+                          barostat=_crescale_triclinic(external_pressure, True))
 
 
 def npt_crescale_anisotropic_step(state, model, *, dt, kT, external_pressure, tau=None,
@@ -392,8 +455,9 @@ def npt_crescale_anisotropic_step(state, model, *, dt, kT, external_pressure, ta
     barostat = (volume normal, z_x, z_y, z_z, volume normal)."""
     dt_s = _per_system(dt, state.n_systems, state.device)
     return _crescale_step(state, model, dt=dt, kT=kT, external_pressure=external_pressure,
-                          tau=100 * dt_s if tau is None else tau, noise=noise,
-                          entry="tsb_npt_crescale_aniso", n_baro=5)
+                          tau=100 * dt_s if tau is None else tau, noise=noise, n_baro=5,
+                          barostat=_crescale_simple("tsb_npt_crescale_aniso",
+                                                    external_pressure))
 
 
 def npt_crescale_isotropic_step(state, model, *, dt, kT, external_pressure, tau=None,
@@ -406,8 +470,8 @@ def npt_crescale_isotropic_step(state, model, *, dt, kT, external_pressure, tau=
     cell [S], vrescale_2 [S, 2])`` supplies them instead."""
     dt_s = _per_system(dt, state.n_systems, state.device)
     return _crescale_step(state, model, dt=dt, kT=kT, external_pressure=external_pressure,
-                          tau=dt_s if tau is None else tau, noise=noise,
-                          entry="tsb_npt_crescale_iso", n_baro=1)
+                          tau=dt_s if tau is None else tau, noise=noise, n_baro=1,
+                          barostat=_crescale_simple("tsb_npt_crescale_iso", external_pressure))
 
 
 def npt_langevin_isotropic_init(state, model, *, kT, dt, alpha=None, cell_alpha=None,
