@@ -165,6 +165,33 @@ int tsb_verlet_forces(int potential, const double *table, int n_species,
                       double *vir_atom, void *workspace, size_t workspace_bytes,
                       void *stream);
 
+/* ---- anisotropic NPT Langevin (per-axis strains) ---------------------------
+ * npt_langevin_anisotropic_step (torch_sim/integrators/npt.py:513-650): strains
+ * eps [S,3], cell row k = exp(eps_k) * row k of reference_cell [S,9] (float64),
+ * strain forces F_k = V (-stress_kk + N kT / V - p_ext_k) with V = det(cell),
+ * GJF strain and particle steps as the isotropic pair; p_ext [S,3]; f_eps [S,3];
+ * cell noise [S,3] (or NULL: Philox) shared by both halves, particle noise [N,3]
+ * likewise.  Workspace: tsb_npt_workspace_size. */
+int tsb_npt_langevin_aniso_pre(void *positions, const void *momenta, const void *forces,
+                               const void *masses, const int64_t *system_idx, int64_t n_atoms,
+                               int64_t n_systems, int dtype, const void *stress,
+                               const double *reference_cell, void *cell, double *eps,
+                               const double *eps_dot, double *cell_masses, double *f_eps,
+                               const double *alpha, const double *cell_alpha,
+                               const double *b_tau, const double *kT, const double *p_ext,
+                               const double *dt, const double *cell_noise,
+                               const double *particle_noise, uint64_t seed, uint64_t counter,
+                               void *workspace, size_t workspace_bytes, void *stream);
+int tsb_npt_langevin_aniso_post(void *momenta, const void *masses, const void *forces_old,
+                                const void *forces, const int64_t *system_idx, int64_t n_atoms,
+                                int64_t n_systems, int dtype, const void *stress,
+                                const void *cell, double *eps_dot, const double *cell_masses,
+                                const double *f_eps, const double *alpha,
+                                const double *cell_alpha, const double *kT, const double *p_ext,
+                                const double *dt, const double *cell_noise,
+                                const double *particle_noise, uint64_t seed, uint64_t counter,
+                                void *workspace, size_t workspace_bytes, void *stream);
+
 /* ---- isotropic C-rescale barostat -----------------------------------------
  * The barostat step of npt_crescale_isotropic_step (torch_sim/integrators/
  * npt.py:2455-2492, 2797-2901; Bernetti & Bussi 2020): per system, the trace of

@@ -11,6 +11,8 @@ step (Gronbech-Jensen & Farago GJF scheme), noise passed in:
   ``_npt_langevin_isotropic_cell_velocity_step`` (:801-835),
   ``_npt_langevin_particle_velocity_step`` (:316-367),
   cell = exp(eps) reference_cell, V = det(reference_cell) exp(3 eps) (:690-703)
+* ``npt_langevin_anisotropic_step`` <- npt.py:513-650 (per-axis strains; cell
+  force :370-406, strain steps :201-264, position step :267-313)
 * ``npt_crescale_isotropic_step`` <- npt.py:2797-2901 (V-rescale half steps of
   nvt.py:594-654, momentum half steps, ``_crescale_isotropic_barostat_step``
   :2455-2492 with the instantaneous pressure of quantities.py:156-198)
@@ -235,4 +237,52 @@ def npt_crescale_triclinic_step(st, force_fn, dt, kT, p_ext, tau, noise, system_
     st.update(positions=q, momenta=p, cell=cell, forces=f, energy=e, stress=s)
     st["momenta"] = st["momenta"] + st["forces"] * (dt / 2)
     st["momenta"] = _vrescale(st, kT, tau, dt / 2, r1b, gb, system_idx)
+    return st
+
+
+def npt_langevin_anisotropic_step(st, force_fn, dt, kT, p_ext, cell_noise, particle_noise,
+                                  system_idx):
+    """st: dict positions, momenta, masses, forces, stress, cell, cell_positions
+    [S,3], cell_velocities [S,3], alpha, cell_alpha, b_tau, reference_cell; p_ext
+    [3] or [S, 3]; cell_noise [S, 3]."""
+    st = dict(st)
+    n_sys = len(st["cell_positions"])
+    n_at = np.bincount(system_idx, minlength=n_sys).astype(np.float64)
+    q_mass = (n_at + 1) * kT * st["b_tau"] ** 2
+    p3 = np.broadcast_to(np.asarray(p_ext, dtype=np.float64), (n_sys, 3))
+
+    def force(stress, cell):
+        vol = np.linalg.det(cell)
+        p_diag = -np.einsum("sii->si", stress) + (n_at * kT / vol)[:, None]
+        return vol[:, None] * (p_diag - p3)
+
+    eps_old = st["cell_positions"].copy()
+    f_n = force(st["stress"], st["cell"])
+    beta_c = np.sqrt(2.0 * st["cell_alpha"] * kT * dt)[:, None] * cell_noise
+    a_at = st["alpha"][system_idx]
+    beta_p = np.sqrt(2 * a_at * kT * dt)[:, None] * particle_noise
+    q2 = (2 * q_mass)[:, None]
+    cb = 1 / (1 + st["cell_alpha"][:, None] * dt / q2)
+    eps = eps_old + cb * dt * st["cell_velocities"] + cb * dt * dt * f_n / q2 + cb * dt * beta_c / q2
+    cell = np.exp(eps)[:, :, None] * st["reference_cell"]
+    m = st["masses"]
+    scale = np.exp(eps - eps_old)[system_idx]
+    b = 1 / (1 + a_at * dt / (2 * m))
+    vel = st["momenta"] / m[:, None]
+    c3 = vel + dt * st["forces"] / (2 * m[:, None]) + beta_p / (2 * m[:, None])
+    q = scale * st["positions"] + (2 * scale / (scale + 1)) * (b * dt)[:, None] * c3
+    forces_old = st["forces"]
+    e, f, s = force_fn(q, cell)
+    f_new = force(s, cell)
+    qm = q_mass[:, None]
+    ca = st["cell_alpha"][:, None]
+    ac = (1 - ca * dt / (2 * qm)) / (1 + ca * dt / (2 * qm))
+    bc = 1 / (1 + ca * dt / (2 * qm))
+    eps_dot = ac * st["cell_velocities"] + dt * (ac * f_n + f_new) / (2 * qm) + bc * beta_c / qm
+    m2 = 2 * m
+    ap = ((1 - a_at * dt / m2) / (1 + a_at * dt / m2))[:, None]
+    bp = (1 / (1 + a_at * dt / m2))[:, None]
+    v_new = ap * vel + dt * (ap * forces_old + f) / m2[:, None] + bp * beta_p / m[:, None]
+    st.update(positions=q, momenta=v_new * m[:, None], forces=f, energy=e, stress=s, cell=cell,
+              cell_positions=eps, cell_velocities=eps_dot, cell_masses=q_mass)
     return st

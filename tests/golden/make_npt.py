@@ -6,9 +6,11 @@ Run in a container where the reference source tree is present::
     python tests/golden/make_npt.py /path/to/torch-sim
 
 Writes ``npt.npz`` beside this script: 8 steps of ``npt_langevin_isotropic_step``
-on three Morse Cu systems (compute_stress=True) at 1000 K and 1 GPa (internal
-units), with the reference's random numbers recorded (per step: the cell noise
-[S], then the particle noise [N, 3]).
+(group ``npt``) on three Morse Cu systems (compute_stress=True) at 1000 K and
+1 GPa (internal units), and 8 steps of ``npt_langevin_anisotropic_step`` (group
+``npt_aniso``) at (1.0, 1.3, 0.7) GPa per axis, with the reference's random
+numbers recorded (per step: the cell noise [S] or [S, 3], then the particle
+noise [N, 3]).
 """
 
 from __future__ import annotations
@@ -79,6 +81,30 @@ def main(ref_root):
     for k in ("alpha", "cell_alpha", "b_tau", "reference_cell"):
         out[f"npt/{k}"] = getattr(md, k).clone().numpy()
     out["npt/dt"], out["npt/kT"], out["npt/p_ext"] = np.array(dt), np.array(kT), np.array(p_ext)
+
+    # per-axis strains with a different target pressure on each axis
+    p3 = torch.tensor([1.0, 1.3, 0.7]) * p_ext
+    st.rng = 31
+    md = ref_npt.npt_langevin_anisotropic_init(st, morse, kT=torch.tensor(kT),
+                                               dt=torch.tensor(dt))
+    noises = []
+    traj = [[getattr(md, k).clone().numpy() for k in keys]]
+    torch.randn = rec
+    try:
+        for _ in range(8):
+            md = ref_npt.npt_langevin_anisotropic_step(md, morse, dt=torch.tensor(dt),
+                                                       kT=torch.tensor(kT), external_pressure=p3)
+            traj.append([getattr(md, k).clone().numpy() for k in keys])
+    finally:
+        torch.randn = real_randn
+    for i, k in enumerate(keys):
+        out[f"npt_aniso/{k}"] = np.stack([t[i] for t in traj])
+    out["npt_aniso/cell_noise"] = np.stack([n.numpy() for n in noises[0::2]])
+    out["npt_aniso/particle_noise"] = np.stack([n.numpy() for n in noises[1::2]])
+    for k in ("alpha", "cell_alpha", "b_tau", "reference_cell"):
+        out[f"npt_aniso/{k}"] = getattr(md, k).clone().numpy()
+    out["npt_aniso/dt"], out["npt_aniso/kT"] = np.array(dt), np.array(kT)
+    out["npt_aniso/p_ext"] = p3.numpy()
     np.savez_compressed(os.path.join(HERE, "npt.npz"), **out)
     print("NPT fixtures written to", HERE)
 

@@ -1,4 +1,4 @@
-"""Isotropic NPT Langevin and isotropic C-rescale on the GPU.
+"""NPT Langevin (isotropic, anisotropic) and C-rescale (all variants) on the GPU.
 
 * 8 steps vs the reference (golden/npt.npz) with the reference's cell and
   particle noise injected; FP64 model: positions, cell and strain to 1e-12,
@@ -144,3 +144,34 @@ def test_npt_crescale_device_noise_reproducible_and_barostat_responds():
     vc = torch.linalg.det(c.cell).abs()
     assert bool((vc < va).all()), (va, vc)
     assert torch.isfinite(a.positions).all() and torch.isfinite(c.momenta).all()
+
+
+def test_npt_langevin_anisotropic_matches_reference(golden):
+    """8 per-axis NPT Langevin steps at (1.0, 1.3, 0.7) GPa vs the reference
+    (golden/npt.npz, npt_aniso) with its cell and particle noise injected; FP64
+    model, max|d| / max|ref| <= 1e-9."""
+    from tsb import integrators as I
+    from tsb import models
+    from tsb.state import MDState
+
+    s, g = golden["npt"]["sys"], golden["npt"]["npt_aniso"]
+    dev = torch.device("cuda")
+    T = lambda x, dt=torch.float64: torch.as_tensor(x, dtype=dt, device=dev)  # noqa: E731
+    n = len(s["masses"])
+    st = MDState(positions=T(g["positions"][0]), masses=T(s["masses"]), cell=T(s["cell"]),
+                 pbc=True, atomic_numbers=T(s["atomic_numbers"], torch.int64),
+                 system_idx=T(s["system_idx"], torch.int64), momenta=T(g["momenta"][0]),
+                 energy=T(np.zeros(3)), forces=T(np.zeros((n, 3))))
+    m = models.MorseModel(sigma=2.866, epsilon=0.3429, alpha=1.3588, cutoff=6.0,
+                          compute_stress=True, precision="fp64")
+    dt, kT = float(g["dt"]), float(g["kT"])
+    st = I.npt_langevin_anisotropic_init(st, m, kT=kT, dt=dt)
+    for k in range(1, g["positions"].shape[0]):
+        st = I.npt_langevin_anisotropic_step(st, m, dt=dt, kT=kT, external_pressure=g["p_ext"],
+                                             noise=(g["cell_noise"][k - 1],
+                                                    g["particle_noise"][k - 1]))
+        for key in ("positions", "momenta", "cell", "cell_positions", "cell_velocities",
+                    "stress"):
+            np.testing.assert_allclose(getattr(st, key).cpu(), g[key][k], rtol=0,
+                                       atol=1e-9 * np.abs(g[key][k]).max(),
+                                       err_msg=f"step {k} {key}")

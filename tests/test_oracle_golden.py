@@ -338,3 +338,31 @@ def test_npt_crescale_oracle_matches_reference(golden, grp):
             # of the matrix exponential to ~2e-10 over 8 steps
             np.testing.assert_allclose(st[key], g[key][k], rtol=0,
                                        atol=1e-9 * np.abs(g[key][k]).max(), err_msg=key)
+
+
+def test_npt_langevin_anisotropic_oracle_matches_reference(golden):
+    from oracle import npt as onpt
+
+    s, g = golden["npt"]["sys"], golden["npt"]["npt_aniso"]
+    sysi = s["system_idx"].astype(np.int64)
+    tab = opair.single_table(opair.MORSE, 2.866, 0.3429, 1.3588)
+
+    def fn(q, cell_col):
+        o = opair.pair_forward(opair.MORSE, tab, np.zeros(len(q), int), q,
+                               np.transpose(cell_col, (0, 2, 1)), np.array([True] * 3), sysi,
+                               6.0)
+        return o["energy"], o["forces"], o["stress"]
+
+    dt, kT = float(g["dt"]), float(g["kT"])
+    st = {"positions": g["positions"][0], "momenta": g["momenta"][0], "masses": s["masses"],
+          "forces": g["forces"][0], "stress": g["stress"][0], "cell": g["cell"][0],
+          "cell_positions": g["cell_positions"][0], "cell_velocities": g["cell_velocities"][0],
+          "alpha": g["alpha"], "cell_alpha": g["cell_alpha"], "b_tau": g["b_tau"],
+          "reference_cell": g["reference_cell"]}
+    for k in range(1, g["positions"].shape[0]):
+        st = onpt.npt_langevin_anisotropic_step(st, fn, dt, kT, g["p_ext"], g["cell_noise"][k - 1],
+                                                g["particle_noise"][k - 1], sysi)
+        for key in ("positions", "momenta", "cell", "cell_positions", "cell_velocities",
+                    "stress"):
+            np.testing.assert_allclose(st[key], g[key][k], rtol=0,
+                                       atol=1e-9 * np.abs(g[key][k]).max(), err_msg=key)

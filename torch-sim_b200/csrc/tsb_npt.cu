@@ -166,6 +166,106 @@ __global__ void k_npt_atom_post(int64_t n, P *p, const P *m, const P *f_old, con
   }
 }
 
+// Anisotropic NPT Langevin (npt.py:62-650): per-axis strains eps_k = ln(L_k/L0_k),
+// cell row k = exp(eps_k) row k of the reference cell (:123-127), strain forces
+// F_k = V (-sigma_kk + N kT / V - P_k) with V = det(cell) (:370-406), the GJF
+// strain steps per axis with the shared mass Q = (N + 1) kT b_tau^2 (:201-264),
+// positions scaled per component by exp(eps_new_k - eps_old_k) (:267-313); the
+// particle velocity step is the isotropic one.  Cell noise [S, 3] (Philox slots
+// 3..5 by default) and particle noise are shared by both halves.
+template <class P>
+__device__ inline void aniso_strain_force(const P *stress, const double *C, double n_at,
+                                          double kt, const double *p_ext, double *f) {
+  const double vol = det3(C);
+  for (int k = 0; k < 3; ++k)
+    f[k] = vol * ((-(double)stress[4 * k] + n_at * kt / vol) - p_ext[k]);
+}
+
+__device__ inline double aniso_cell_noise(const double *cn, uint64_t seed, int64_t s, int k,
+                                          uint64_t counter) {
+  return cn ? cn[3 * s + k] : thermo_normal(seed, s, counter, 3u + (uint32_t)k);
+}
+
+template <class P>
+__global__ void k_npt_aniso_cell_pre(int64_t ns, const int64_t *lo, const int64_t *hi,
+                                     const P *stress, const double *ref_cell, P *cell,
+                                     double *eps, const double *eps_dot, double *Q,
+                                     double *f_eps, double *scale3, const double *cell_alpha,
+                                     const double *b_tau, const double *kT, const double *p_ext,
+                                     const double *dt, const double *cell_noise, uint64_t seed,
+                                     uint64_t counter) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  const double n_at = (double)(hi[s] - lo[s]), kt = kT[s], h = dt[s], ac = cell_alpha[s];
+  const double q = (n_at + 1.0) * kt * (b_tau[s] * b_tau[s]);
+  double C[9];
+  for (int k = 0; k < 9; ++k) C[k] = (double)cell[9 * s + k];
+  double f[3];
+  aniso_strain_force(stress + 9 * s, C, n_at, kt, p_ext + 3 * s, f);
+  const double q2 = 2.0 * q;
+  const double cb = 1.0 / (1.0 + (ac * h) / q2);
+  const double sc = sqrt(2.0 * ac * kt * h);
+  for (int k = 0; k < 3; ++k) {
+    const double beta = sc * aniso_cell_noise(cell_noise, seed, s, k, counter);
+    const double e0 = eps[3 * s + k];
+    const double e1 = e0 + cb * h * eps_dot[3 * s + k] + cb * h * h * f[k] / q2 + cb * h * beta / q2;
+    eps[3 * s + k] = e1;
+    f_eps[3 * s + k] = f[k];
+    scale3[3 * s + k] = exp(e1 - e0);
+    const double g = exp(e1);
+    for (int m = 0; m < 3; ++m) cell[9 * s + 3 * k + m] = (P)(g * ref_cell[9 * s + 3 * k + m]);
+  }
+  Q[s] = q;
+}
+
+template <class P>
+__global__ void k_npt_aniso_atom_pre(int64_t n, P *x, const P *p, const P *f, const P *m,
+                                     const int64_t *sys, const double *scale3,
+                                     const double *alpha, const double *kT, const double *dt,
+                                     const double *pn, uint64_t seed, uint64_t counter) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t s = sys[i];
+  double z[4];
+  particle_noise_of(pn, seed, i, counter, z);
+  const double a = alpha[s], h = dt[s], mi = m[i];
+  const double pre = sqrt(2.0 * a * kT[s] * h);
+  const double b = 1.0 / (1.0 + (a * h) / (2.0 * mi));
+  for (int c = 0; c < 3; ++c) {
+    const double sc = scale3[3 * s + c];
+    const double c2 = (2.0 * sc / (sc + 1.0)) * b * h;
+    const double c3 = (double)p[3 * i + c] / mi + h * (double)f[3 * i + c] / (2.0 * mi) +
+                      pre * z[c] / (2.0 * mi);
+    x[3 * i + c] = (P)(sc * (double)x[3 * i + c] + c2 * c3);
+  }
+}
+
+template <class P>
+__global__ void k_npt_aniso_cell_post(int64_t ns, const int64_t *lo, const int64_t *hi,
+                                      const P *stress, const P *cell, double *eps_dot,
+                                      const double *Q, const double *f_eps,
+                                      const double *cell_alpha, const double *kT,
+                                      const double *p_ext, const double *dt,
+                                      const double *cell_noise, uint64_t seed,
+                                      uint64_t counter) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  const double n_at = (double)(hi[s] - lo[s]), kt = kT[s], h = dt[s], ac = cell_alpha[s];
+  const double q = Q[s];
+  double C[9];
+  for (int k = 0; k < 9; ++k) C[k] = (double)cell[9 * s + k];
+  double f1[3];
+  aniso_strain_force(stress + 9 * s, C, n_at, kt, p_ext + 3 * s, f1);
+  const double a = (1.0 - (ac * h) / (2.0 * q)) / (1.0 + (ac * h) / (2.0 * q));
+  const double b = 1.0 / (1.0 + (ac * h) / (2.0 * q));
+  const double sc = sqrt(2.0 * ac * kt * h);
+  for (int k = 0; k < 3; ++k) {
+    const double beta = sc * aniso_cell_noise(cell_noise, seed, s, k, counter);
+    eps_dot[3 * s + k] = a * eps_dot[3 * s + k] + h * ((a * f_eps[3 * s + k]) + f1[k]) / (2.0 * q) +
+                         b * beta / q;
+  }
+}
+
 // Isotropic stochastic cell rescaling (C-rescale, Bernetti & Bussi 2020;
 // torch_sim/integrators/npt.py:2455-2492).  One block per system: the trace of
 // the instantaneous pressure tensor P = (sum_i p_i p_i^T / m_i) / V - stress
@@ -659,6 +759,83 @@ extern "C" int tsb_npt_crescale_tri(void *positions, void *momenta, const void *
     TSB_CRESCALE_T(float)
   }
 #undef TSB_CRESCALE_T
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
+
+extern "C" int tsb_npt_langevin_aniso_pre(
+    void *positions, const void *momenta, const void *forces, const void *masses,
+    const int64_t *system_idx, int64_t n_atoms, int64_t n_systems, int dtype,
+    const void *stress, const double *reference_cell, void *cell, double *eps,
+    const double *eps_dot, double *cell_masses, double *f_eps, const double *alpha,
+    const double *cell_alpha, const double *b_tau, const double *kT, const double *p_ext,
+    const double *dt, const double *cell_noise, const double *particle_noise, uint64_t seed,
+    uint64_t counter, void *workspace, size_t workspace_bytes, void *stream) {
+  if (n_atoms < 1 || n_systems < 1 || !positions || !momenta || !forces || !masses ||
+      !system_idx || !stress || !reference_cell || !cell || !eps || !eps_dot || !cell_masses ||
+      !f_eps || !alpha || !cell_alpha || !b_tau || !kT || !p_ext || !dt)
+    return TSB_ERR_INVALID_ARG;
+  if (dtype != TSB_F32 && dtype != TSB_F64) return TSB_ERR_INVALID_ARG;
+  Carver c(workspace, workspace_bytes);
+  NptWork w;
+  carve_npt(c, w, n_systems);
+  if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaMemsetAsync(w.lo, 0, sizeof(int64_t) * n_systems, st);
+  cudaMemsetAsync(w.hi, 0, sizeof(int64_t) * n_systems, st);
+  k_npt_bounds<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, w.lo, w.hi);
+#define TSB_NPTA_PRE(P)                                                                       \
+  k_npt_aniso_cell_pre<P><<<grid_for(n_systems), kBlock, 0, st>>>(                           \
+      n_systems, w.lo, w.hi, (const P *)stress, reference_cell, (P *)cell, eps, eps_dot,      \
+      cell_masses, f_eps, w.scale3, cell_alpha, b_tau, kT, p_ext, dt, cell_noise, seed,       \
+      counter);                                                                              \
+  k_npt_aniso_atom_pre<P><<<grid_for(n_atoms), kBlock, 0, st>>>(                             \
+      n_atoms, (P *)positions, (const P *)momenta, (const P *)forces, (const P *)masses,     \
+      system_idx, w.scale3, alpha, kT, dt, particle_noise, seed, counter);
+  if (dtype == TSB_F64) {
+    TSB_NPTA_PRE(double)
+  } else {
+    TSB_NPTA_PRE(float)
+  }
+#undef TSB_NPTA_PRE
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
+
+extern "C" int tsb_npt_langevin_aniso_post(
+    void *momenta, const void *masses, const void *forces_old, const void *forces,
+    const int64_t *system_idx, int64_t n_atoms, int64_t n_systems, int dtype,
+    const void *stress, const void *cell, double *eps_dot, const double *cell_masses,
+    const double *f_eps, const double *alpha, const double *cell_alpha, const double *kT,
+    const double *p_ext, const double *dt, const double *cell_noise,
+    const double *particle_noise, uint64_t seed, uint64_t counter, void *workspace,
+    size_t workspace_bytes, void *stream) {
+  if (n_atoms < 1 || n_systems < 1 || !momenta || !masses || !forces_old || !forces ||
+      !system_idx || !stress || !cell || !eps_dot || !cell_masses || !f_eps || !alpha ||
+      !cell_alpha || !kT || !p_ext || !dt)
+    return TSB_ERR_INVALID_ARG;
+  if (dtype != TSB_F32 && dtype != TSB_F64) return TSB_ERR_INVALID_ARG;
+  Carver c(workspace, workspace_bytes);
+  NptWork w;
+  carve_npt(c, w, n_systems);
+  if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaMemsetAsync(w.lo, 0, sizeof(int64_t) * n_systems, st);
+  cudaMemsetAsync(w.hi, 0, sizeof(int64_t) * n_systems, st);
+  k_npt_bounds<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, w.lo, w.hi);
+#define TSB_NPTA_POST(P)                                                                      \
+  k_npt_aniso_cell_post<P><<<grid_for(n_systems), kBlock, 0, st>>>(                          \
+      n_systems, w.lo, w.hi, (const P *)stress, (const P *)cell, eps_dot, cell_masses, f_eps, \
+      cell_alpha, kT, p_ext, dt, cell_noise, seed, counter);                                 \
+  k_npt_atom_post<P><<<grid_for(n_atoms), kBlock, 0, st>>>(                                  \
+      n_atoms, (P *)momenta, (const P *)masses, (const P *)forces_old, (const P *)forces,    \
+      system_idx, alpha, kT, dt, particle_noise, seed, counter);
+  if (dtype == TSB_F64) {
+    TSB_NPTA_POST(double)
+  } else {
+    TSB_NPTA_POST(float)
+  }
+#undef TSB_NPTA_POST
   TSB_CHECK_LAUNCH();
   return TSB_OK;
 }

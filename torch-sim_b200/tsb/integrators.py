@@ -474,6 +474,84 @@ def npt_crescale_isotropic_step(state, model, *, dt, kT, external_pressure, tau=
                           barostat=_crescale_simple("tsb_npt_crescale_iso", external_pressure))
 
 
+def npt_langevin_anisotropic_init(state, model, *, kT, dt, alpha=None, cell_alpha=None,
+                                  b_tau=None, **_kw):
+    """Per-axis strain NPT Langevin state (npt.py:409-510): eps = 0 [S,3], alpha =
+    1/(5 dt), cell_alpha = 1/(30 dt), b_tau = 300 dt by default.  ``model`` must
+    compute the stress."""
+    from .state import NPTLangevinAnisotropicState
+
+    md = _md_init(state, model, kT)
+    out = model(md)
+    if "stress" not in out:
+        raise ValueError("NPT needs a model with compute_stress=True")
+    n_sys, dev = md.n_systems, md.device
+    dt_s = _per_system(dt, n_sys, dev)
+    kT_s = _per_system(kT, n_sys, dev)
+    alpha = _per_system(1.0 / (5 * dt_s) if alpha is None else alpha, n_sys, dev).clone()
+    cell_alpha = _per_system(1.0 / (30 * dt_s) if cell_alpha is None else cell_alpha,
+                             n_sys, dev).clone()
+    b_tau = _per_system(300 * dt_s if b_tau is None else b_tau, n_sys, dev).clone()
+    n_at = torch.bincount(md.system_idx, minlength=n_sys).to(torch.float64)
+    z = torch.zeros((n_sys, 3), dtype=torch.float64, device=dev)
+    st = NPTLangevinAnisotropicState.from_state(
+        md, stress=out["stress"], alpha=alpha, cell_alpha=cell_alpha, b_tau=b_tau,
+        reference_cell=md.cell.to(torch.float64).clone(), cell_positions=z.clone(),
+        cell_velocities=z.clone(), cell_masses=(n_at + 1) * kT_s * b_tau * b_tau)
+    st._philox_seed, st._philox_counter = md._philox_seed, 0
+    return st
+
+
+def npt_langevin_anisotropic_step(state, model, *, dt, kT, external_pressure, noise=None,
+                                  **_kw):
+    """One per-axis NPT Langevin step (npt.py:513-650).  ``external_pressure`` is a
+    scalar, a [3] vector or [S, 3]; the cell noise [S, 3] and particle noise [N, 3]
+    come from the device Philox stream, or from ``noise = (cell_noise,
+    particle_noise)``, e.g. the reference's own draws."""
+    _prepare(state)
+    n_sys, n, dev = state.n_systems, state.n_atoms, state.device
+    dt_s = _per_system(dt, n_sys, dev)
+    kT_s = _per_system(kT, n_sys, dev)
+    pe = torch.as_tensor(external_pressure, dtype=torch.float64, device=dev)
+    p3 = pe.reshape(1, 1).expand(n_sys, 3) if pe.ndim == 0 else pe.reshape(-1, 3).expand(n_sys, 3)
+    p3 = p3.contiguous()
+    for name in ("alpha", "cell_alpha", "b_tau", "reference_cell", "cell_positions",
+                 "cell_velocities", "cell_masses"):
+        v = getattr(state, name)
+        if v.dtype != torch.float64 or not v.is_contiguous():
+            setattr(state, name, v.to(torch.float64).contiguous())
+    state.cell = state.cell.to(state.dtype).contiguous()
+    state.stress = state.stress.to(state.dtype).contiguous()
+    cn = pn = None
+    if noise is not None:
+        cn = torch.as_tensor(noise[0], dtype=torch.float64, device=dev).reshape(n_sys, 3)
+        pn = torch.as_tensor(noise[1], dtype=torch.float64, device=dev).reshape(n, 3)
+        cn, pn = cn.contiguous(), pn.contiguous()
+    seed = getattr(state, "_philox_seed", _seed_of(state)) & (2**64 - 1)
+    counter = getattr(state, "_philox_counter", 0)
+    f_eps = torch.empty((n_sys, 3), dtype=torch.float64, device=dev)
+    ws = L.Workspace.get(dev, L.load().tsb_npt_workspace_size(n_sys))
+    dtc, stp = L.dtype_code(state.dtype), L.stream_ptr(dev)
+    L.call("tsb_npt_langevin_aniso_pre", L.ptr(state.positions), L.ptr(state.momenta),
+           L.ptr(state.forces), L.ptr(state.masses), L.ptr(state.system_idx), n, n_sys, dtc,
+           L.ptr(state.stress), L.ptr(state.reference_cell), L.ptr(state.cell),
+           L.ptr(state.cell_positions), L.ptr(state.cell_velocities), L.ptr(state.cell_masses),
+           L.ptr(f_eps), L.ptr(state.alpha), L.ptr(state.cell_alpha), L.ptr(state.b_tau),
+           L.ptr(kT_s), L.ptr(p3), L.ptr(dt_s), L.ptr(cn), L.ptr(pn), seed, counter,
+           L.ptr(ws), ws.numel(), stp)
+    forces_old = state.forces
+    out = _apply_model(state, model)
+    state.stress = out["stress"].to(state.dtype).contiguous()
+    L.call("tsb_npt_langevin_aniso_post", L.ptr(state.momenta), L.ptr(state.masses),
+           L.ptr(forces_old), L.ptr(state.forces), L.ptr(state.system_idx), n, n_sys, dtc,
+           L.ptr(state.stress), L.ptr(state.cell), L.ptr(state.cell_velocities),
+           L.ptr(state.cell_masses), L.ptr(f_eps), L.ptr(state.alpha), L.ptr(state.cell_alpha),
+           L.ptr(kT_s), L.ptr(p3), L.ptr(dt_s), L.ptr(cn), L.ptr(pn), seed, counter,
+           L.ptr(ws), ws.numel(), stp)
+    state._philox_seed, state._philox_counter = seed, counter + 1
+    return state
+
+
 def npt_langevin_isotropic_init(state, model, *, kT, dt, alpha=None, cell_alpha=None,
                                 b_tau=None, **_kw):
     """Strain-based isotropic NPT Langevin state (npt.py:888-985): eps = 0,

@@ -217,6 +217,31 @@ class NPTLangevinIsotropicState(MDState):
 
 
 @dataclass(kw_only=True)
+class NPTLangevinAnisotropicState(MDState):
+    """MDState + per-axis strain barostat (torch_sim/integrators/npt.py:62-131):
+    stress [S,3,3]; per system alpha, cell_alpha, b_tau, cell_masses; per-axis
+    strains ``cell_positions`` [S,3] (eps_k = ln(L_k/L0_k)) and ``cell_velocities``
+    [S,3]; ``reference_cell`` [S,3,3] (cell row k = exp(eps_k) reference row k)."""
+
+    stress: torch.Tensor
+    alpha: torch.Tensor
+    cell_alpha: torch.Tensor
+    b_tau: torch.Tensor
+    reference_cell: torch.Tensor
+    cell_positions: torch.Tensor
+    cell_velocities: torch.Tensor
+    cell_masses: torch.Tensor
+
+    @property
+    def current_cell(self) -> torch.Tensor:
+        return torch.exp(self.cell_positions).unsqueeze(-1) * self.reference_cell
+
+    @property
+    def volume(self) -> torch.Tensor:
+        return torch.linalg.det(self.cell)
+
+
+@dataclass(kw_only=True)
 class NPTCRescaleState(MDState):
     """MDState + stochastic cell rescaling (torch_sim/integrators/npt.py:2062-2090):
     stress [S,3,3]; per system isothermal_compressibility and tau_p; the initial cell
