@@ -192,6 +192,29 @@ int tsb_npt_langevin_aniso_post(void *momenta, const void *masses, const void *f
                                 const double *particle_noise, uint64_t seed, uint64_t counter,
                                 void *workspace, size_t workspace_bytes, void *stream);
 
+/* ---- isotropic NPT Nose-Hoover (MTK) inner step -------------------------------
+ * The part of npt_nose_hoover_isotropic_step (torch_sim/integrators/npt.py:
+ * 1532-1639, 1812-1963) between the chain half steps (those run on
+ * tsb_nhc_half_step).  eps [S] = ln(V/V0)/3, p_eps [S] cell momentum, cell_mass
+ * [S] W, reference_cell [S,9] float64, v_eps [S] out (pre) / in (post).
+ * pre: p_eps += F dt/2 with F = alpha 2 KE - tr(stress) V - 3 P V, alpha =
+ *   1 + 3/(3N - 3); v = p_eps/W; momenta by exp(iL2), eps += v dt, cell =
+ *   (V/V0)^(1/3) ref, positions by exp(iL1).
+ * post (after the force call): momenta by exp(iL2) with the new forces, p_eps +=
+ *   F(new stress, new volume) dt/2.  Workspace: tsb_npt_workspace_size. */
+int tsb_npt_nh_iso_pre(void *positions, void *momenta, const void *forces, const void *masses,
+                       const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
+                       int dtype, const void *stress, const double *reference_cell, void *cell,
+                       double *eps, double *p_eps, const double *cell_mass,
+                       const double *p_ext, const double *dt, double *v_eps, void *workspace,
+                       size_t workspace_bytes, void *stream);
+int tsb_npt_nh_iso_post(void *momenta, const void *forces, const void *masses,
+                        const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
+                        int dtype, const void *stress, const double *reference_cell,
+                        const double *eps, double *p_eps, const double *p_ext,
+                        const double *dt, const double *v_eps, void *workspace,
+                        size_t workspace_bytes, void *stream);
+
 /* ---- isotropic C-rescale barostat -----------------------------------------
  * The barostat step of npt_crescale_isotropic_step (torch_sim/integrators/
  * npt.py:2455-2492, 2797-2901; Bernetti & Bussi 2020): per system, the trace of

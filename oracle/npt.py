@@ -13,6 +13,9 @@ step (Gronbech-Jensen & Farago GJF scheme), noise passed in:
   cell = exp(eps) reference_cell, V = det(reference_cell) exp(3 eps) (:690-703)
 * ``npt_langevin_anisotropic_step`` <- npt.py:513-650 (per-axis strains; cell
   force :370-406, strain steps :201-264, position step :267-313)
+* ``npt_nose_hoover_isotropic_step`` <- npt.py:1812-1963 (MTK: chain half steps of
+  md.py:388-514, inner step :1532-1639 with exp_iL1 :1346-1399, exp_iL2 :1402-1457,
+  cell force :1460-1529, sinh(x)/x series :1312-1343)
 * ``npt_crescale_isotropic_step`` <- npt.py:2797-2901 (V-rescale half steps of
   nvt.py:594-654, momentum half steps, ``_crescale_isotropic_barostat_step``
   :2455-2492 with the instantaneous pressure of quantities.py:156-198)
@@ -285,4 +288,69 @@ def npt_langevin_anisotropic_step(st, force_fn, dt, kT, p_ext, cell_noise, parti
     v_new = ap * vel + dt * (ap * forces_old + f) / m2[:, None] + bp * beta_p / m[:, None]
     st.update(positions=q, momenta=v_new * m[:, None], forces=f, energy=e, stress=s, cell=cell,
               cell_positions=eps, cell_velocities=eps_dot, cell_masses=q_mass)
+    return st
+
+
+def _sinhx_x(x):
+    return 1 + x ** 2 / 6 + x ** 4 / 120 + x ** 6 / 5040 + x ** 8 / 362_880 + x ** 10 / 39_916_800
+
+
+def npt_nose_hoover_isotropic_step(st, force_fn, dt, kT, p_ext, system_idx):
+    """st: dict positions, momenta, masses, forces, stress, reference_cell,
+    cell_position [S], cell_momentum [S], and per chain ("t" particles, "b" cell)
+    xi / p_xi [S, M], ke [S], tau [S], chain_steps, sy_steps.  Returns the updated
+    dict (cell, cell_mass and the chains' masses included)."""
+    st = dict(st)
+    n_sys = len(st["cell_position"])
+    nat = np.bincount(system_idx, minlength=n_sys).astype(np.float64)
+    dof_t, dof_b = 3 * nat - 3, np.ones(n_sys)
+    m = st["masses"]
+    M = st["t_xi"].shape[1]
+    qt = oth.chain_masses(dof_t, kT, st["t_tau"], M)
+    qb = oth.chain_masses(dof_b, kT, st["b_tau"], M)
+    w = 3 * (nat + 1) * kT * st["b_tau"] ** 2
+    cs, ss = st["chain_steps"], st["sy_steps"]
+    sidx = np.arange(n_sys)
+    pc, b_xi, b_pxi, b_ke = oth.nhc_half_step(st["cell_momentum"][:, None], st["b_xi"],
+                                              st["b_pxi"], qb, st["b_ke"], dof_b, kT, dt, cs,
+                                              ss, sidx)
+    p, t_xi, t_pxi, t_ke = oth.nhc_half_step(st["momenta"], st["t_xi"], st["t_pxi"], qt,
+                                             st["t_ke"], dof_t, kT, dt, cs, ss, system_idx)
+    pc = pc[:, 0]
+    alpha = 1 + 3 / dof_t
+    v0 = np.linalg.det(st["reference_cell"])
+
+    def cell_force(p, stress, vol):
+        ke = omd.kinetic_energy(m, p, system_idx)
+        return alpha * 2 * ke - np.einsum("sii->s", stress) * vol - p_ext * vol * 3
+
+    vol = v0 * np.exp(3 * st["cell_position"])
+    pc = pc + dt / 2 * cell_force(p, st["stress"], vol)
+    v = pc / w
+    dt2 = dt / 2
+
+    def il2(p, f):
+        x = (alpha * v)[system_idx] * dt2
+        return p * np.exp(-x)[:, None] + dt2 * f * _sinhx_x(x / 2)[:, None] * np.exp(-x / 2)[:, None]
+
+    p = il2(p, st["forces"])
+    eps = st["cell_position"] + v * dt
+    vol = v0 * np.exp(3 * eps)
+    cell = ((vol / v0) ** (1.0 / 3.0))[:, None, None] * st["reference_cell"]
+    x = (v * dt)[system_idx]
+    q = st["positions"]
+    q = q + (q * (np.exp(x) - 1)[:, None] + dt * (p / m[:, None]) * np.exp(x / 2)[:, None] *
+             _sinhx_x(x / 2)[:, None])
+    e, f, s = force_fn(q, cell)
+    p = il2(p, f)
+    pc = pc + dt / 2 * cell_force(p, s, vol)
+    t_ke = omd.kinetic_energy(m, p, system_idx)
+    p, t_xi, t_pxi, t_ke = oth.nhc_half_step(p, t_xi, t_pxi, qt, t_ke, dof_t, kT, dt, cs, ss,
+                                             system_idx)
+    b_ke = pc ** 2 / (2 * w)
+    pc, b_xi, b_pxi, b_ke = oth.nhc_half_step(pc[:, None], b_xi, b_pxi, qb, b_ke, dof_b, kT,
+                                              dt, cs, ss, sidx)
+    st.update(positions=q, momenta=p, forces=f, energy=e, stress=s, cell=cell,
+              cell_position=eps, cell_momentum=pc[:, 0], cell_mass=w, t_xi=t_xi, t_pxi=t_pxi,
+              t_ke=t_ke, t_q=qt, b_xi=b_xi, b_pxi=b_pxi, b_ke=b_ke, b_q=qb)
     return st

@@ -10,7 +10,9 @@ Writes ``npt.npz`` beside this script: 8 steps of ``npt_langevin_isotropic_step`
 1 GPa (internal units), and 8 steps of ``npt_langevin_anisotropic_step`` (group
 ``npt_aniso``) at (1.0, 1.3, 0.7) GPa per axis, with the reference's random
 numbers recorded (per step: the cell noise [S] or [S, 3], then the particle
-noise [N, 3]).
+noise [N, 3]); and 8 deterministic steps of ``npt_nose_hoover_isotropic_step``
+(group ``npt_nh``, MTK barostat with Nose-Hoover chains) with both chains and the
+conserved quantity recorded.
 """
 
 from __future__ import annotations
@@ -105,6 +107,36 @@ def main(ref_root):
         out[f"npt_aniso/{k}"] = getattr(md, k).clone().numpy()
     out["npt_aniso/dt"], out["npt_aniso/kT"] = np.array(dt), np.array(kT)
     out["npt_aniso/p_ext"] = p3.numpy()
+
+    # MTK isotropic NPT with Nose-Hoover chains (deterministic)
+    st.rng = 31
+    md = ref_npt.npt_nose_hoover_isotropic_init(st, morse, kT=torch.tensor(kT),
+                                                dt=torch.tensor(dt))
+    nh_keys = ("positions", "momenta", "energy", "forces", "stress", "cell", "cell_position",
+               "cell_momentum", "cell_mass")
+
+    def snap(md):
+        row = [getattr(md, k).clone().numpy() for k in nh_keys]
+        for ch in (md.thermostat, md.barostat):
+            row += [ch.positions.clone().numpy(), ch.momenta.clone().numpy(),
+                    ch.masses.clone().numpy(), ch.kinetic_energy.clone().numpy()]
+        row.append(ref_npt.npt_nose_hoover_isotropic_invariant(
+            md, torch.tensor(kT), torch.tensor(p_ext)).clone().numpy())
+        return row
+
+    traj = [snap(md)]
+    for _ in range(8):
+        md = ref_npt.npt_nose_hoover_isotropic_step(md, morse, dt=torch.tensor(dt),
+                                                    kT=torch.tensor(kT),
+                                                    external_pressure=torch.tensor(p_ext))
+        traj.append(snap(md))
+    names = list(nh_keys) + [f"{c}_{v}" for c in ("thermostat", "barostat")
+                             for v in ("positions", "momenta", "masses", "kinetic_energy")]
+    names.append("invariant")
+    for i, k in enumerate(names):
+        out[f"npt_nh/{k}"] = np.stack([t[i] for t in traj])
+    out["npt_nh/dt"], out["npt_nh/kT"], out["npt_nh/p_ext"] = (np.array(dt), np.array(kT),
+                                                               np.array(p_ext))
     np.savez_compressed(os.path.join(HERE, "npt.npz"), **out)
     print("NPT fixtures written to", HERE)
 

@@ -175,3 +175,42 @@ def test_npt_langevin_anisotropic_matches_reference(golden):
             np.testing.assert_allclose(getattr(st, key).cpu(), g[key][k], rtol=0,
                                        atol=1e-9 * np.abs(g[key][k]).max(),
                                        err_msg=f"step {k} {key}")
+
+
+def test_npt_nose_hoover_isotropic_matches_reference(golden):
+    """8 MTK isotropic NPT steps with Nose-Hoover chains vs the reference
+    (golden/npt.npz, npt_nh; deterministic): positions, momenta, cell, log volume,
+    cell momentum, both chains and the conserved quantity; FP64 model,
+    max|d| / max|ref| <= 1e-9."""
+    from tsb import integrators as I
+    from tsb import models
+    from tsb.state import MDState
+
+    s, g = golden["npt"]["sys"], golden["npt"]["npt_nh"]
+    dev = torch.device("cuda")
+    T = lambda x, dt=torch.float64: torch.as_tensor(x, dtype=dt, device=dev)  # noqa: E731
+    n = len(s["masses"])
+    st = MDState(positions=T(g["positions"][0]), masses=T(s["masses"]), cell=T(g["cell"][0]),
+                 pbc=True, atomic_numbers=T(s["atomic_numbers"], torch.int64),
+                 system_idx=T(s["system_idx"], torch.int64), momenta=T(g["momenta"][0]),
+                 energy=T(np.zeros(3)), forces=T(np.zeros((n, 3))))
+    m = models.MorseModel(sigma=2.866, epsilon=0.3429, alpha=1.3588, cutoff=6.0,
+                          compute_stress=True, precision="fp64")
+    dt, kT, p = float(g["dt"]), float(g["kT"]), float(g["p_ext"])
+    st = I.npt_nose_hoover_isotropic_init(st, m, kT=kT, dt=dt)
+
+    def close(got, ref, what):
+        np.testing.assert_allclose(got.detach().cpu().numpy().reshape(ref.shape), ref, rtol=0,
+                                   atol=1e-9 * max(np.abs(ref).max(), 1e-30), err_msg=what)
+
+    close(I.npt_nose_hoover_isotropic_invariant(st, kT, p), g["invariant"][0], "invariant 0")
+    for k in range(1, g["positions"].shape[0]):
+        st = I.npt_nose_hoover_isotropic_step(st, m, dt=dt, kT=kT, external_pressure=p)
+        for key in ("positions", "momenta", "cell", "cell_position", "cell_momentum",
+                    "stress"):
+            close(getattr(st, key), g[key][k], f"step {k} {key}")
+        for ch, name in ((st.thermostat, "thermostat"), (st.barostat, "barostat")):
+            close(ch.positions, g[f"{name}_positions"][k], f"step {k} {name} xi")
+            close(ch.momenta, g[f"{name}_momenta"][k], f"step {k} {name} p_xi")
+        close(I.npt_nose_hoover_isotropic_invariant(st, kT, p), g["invariant"][k],
+              f"step {k} invariant")

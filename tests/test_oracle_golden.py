@@ -366,3 +366,38 @@ def test_npt_langevin_anisotropic_oracle_matches_reference(golden):
                     "stress"):
             np.testing.assert_allclose(st[key], g[key][k], rtol=0,
                                        atol=1e-9 * np.abs(g[key][k]).max(), err_msg=key)
+
+
+def test_npt_nose_hoover_isotropic_oracle_matches_reference(golden):
+    from oracle import npt as onpt
+
+    s, g = golden["npt"]["sys"], golden["npt"]["npt_nh"]
+    sysi = s["system_idx"].astype(np.int64)
+    tab = opair.single_table(opair.MORSE, 2.866, 0.3429, 1.3588)
+
+    def fn(q, cell_col):
+        o = opair.pair_forward(opair.MORSE, tab, np.zeros(len(q), int), q,
+                               np.transpose(cell_col, (0, 2, 1)), np.array([True] * 3), sysi,
+                               6.0)
+        return o["energy"], o["forces"], o["stress"]
+
+    dt, kT, p_ext = float(g["dt"]), float(g["kT"]), float(g["p_ext"])
+    st = {"positions": g["positions"][0], "momenta": g["momenta"][0], "masses": s["masses"],
+          "forces": g["forces"][0], "stress": g["stress"][0], "reference_cell": g["cell"][0],
+          "cell_position": g["cell_position"][0], "cell_momentum": g["cell_momentum"][0][:, 0],
+          "t_xi": g["thermostat_positions"][0], "t_pxi": g["thermostat_momenta"][0],
+          "t_ke": g["thermostat_kinetic_energy"][0], "t_tau": np.full(3, 10 * dt),
+          "b_xi": g["barostat_positions"][0], "b_pxi": g["barostat_momenta"][0],
+          "b_ke": g["barostat_kinetic_energy"][0], "b_tau": np.full(3, 100 * dt),
+          "chain_steps": 2, "sy_steps": 3}
+    for k in range(1, g["positions"].shape[0]):
+        st = onpt.npt_nose_hoover_isotropic_step(st, fn, dt, kT, p_ext, sysi)
+        for key, ref in (("positions", "positions"), ("momenta", "momenta"), ("cell", "cell"),
+                         ("cell_position", "cell_position"), ("stress", "stress"),
+                         ("t_xi", "thermostat_positions"), ("t_pxi", "thermostat_momenta"),
+                         ("b_xi", "barostat_positions"), ("b_pxi", "barostat_momenta"),
+                         ("t_q", "thermostat_masses"), ("b_q", "barostat_masses")):
+            np.testing.assert_allclose(st[key], g[ref][k], rtol=0,
+                                       atol=1e-9 * np.abs(g[ref][k]).max(), err_msg=key)
+        np.testing.assert_allclose(st["cell_momentum"], g["cell_momentum"][k][:, 0], rtol=1e-9,
+                                   atol=1e-12)

@@ -266,6 +266,125 @@ __global__ void k_npt_aniso_cell_post(int64_t ns, const int64_t *lo, const int64
   }
 }
 
+// Isotropic NPT Nose-Hoover (Martyna-Tuckerman-Klein; npt.py:1110-1965): the
+// inner step around the force call, between the chain half steps (which run on
+// the thermostat kernel).  Log-volume coordinate eps = ln(V/V0)/3, cell momentum
+// p_eps with mass W; alpha = 1 + 3/(3N - 3); cell force
+// F = alpha 2 KE - tr(stress) V - 3 P V (:1460-1529).  pre: p_eps += F dt/2,
+// v = p_eps / W, momenta by exp(iL2) (:1402-1457), eps += v dt, cell =
+// (V/V0)^(1/3) ref, positions by exp(iL1) (:1346-1399); post: momenta by exp(iL2)
+// with the new forces, p_eps += F(new stress, new V) dt/2 (:1532-1639).
+__device__ inline double mtk_sinhx_x(double x) {
+  const double x2 = x * x, x4 = x2 * x2, x6 = x4 * x2, x8 = x4 * x4, x10 = x8 * x2;
+  return 1.0 + x2 / 6.0 + x4 / 120.0 + x6 / 5040.0 + x8 / 362880.0 + x10 / 39916800.0;
+}
+
+// per system: 2 KE = sum p^2 / m over the block, fixed order (thread 0 gets it)
+template <class P>
+__device__ inline double block_two_ke(int64_t lo, int64_t hi, const P *p, const P *m,
+                                      double *sh) {
+  double acc = 0.0;
+  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const double mi = (double)m[i];
+    for (int c = 0; c < 3; ++c) {
+      const double pc = (double)p[3 * i + c];
+      acc += pc * pc / mi;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+  return t;
+}
+
+__device__ inline double mtk_alpha(int64_t lo, int64_t hi) {
+  return 1.0 + 3.0 / (3.0 * (double)(hi - lo) - 3.0);
+}
+
+template <class P>
+__global__ void __launch_bounds__(256)
+    k_mtk_pre_cell(const int64_t *lo, const int64_t *hi, const P *p, const P *m,
+                   const P *stress, const double *ref_cell, P *cell, double *eps,
+                   double *p_eps, const double *W, const double *p_ext, const double *dt,
+                   double *v_eps) {
+  __shared__ double sh[256 / 32];
+  const int64_t s = blockIdx.x;
+  const double two_ke = block_two_ke(lo[s], hi[s], p, m, sh);
+  if (threadIdx.x != 0) return;
+  const double ke = 0.5 * two_ke;
+  const double al = mtk_alpha(lo[s], hi[s]), h = dt[s];
+  const double v0 = det3(ref_cell + 9 * s);
+  const double vol = v0 * exp(3.0 * eps[s]);
+  const P *st = stress + 9 * s;
+  const double tr = (double)st[0] + (double)st[4] + (double)st[8];
+  const double f = (al * 2.0 * ke) - (tr * vol) - (p_ext[s] * vol * 3.0);
+  const double pe = p_eps[s] + (h / 2.0) * f;
+  const double v = pe / W[s];
+  const double e1 = eps[s] + v * h;
+  const double vol1 = v0 * exp(3.0 * e1);
+  const double sc = pow(vol1 / v0, 1.0 / 3.0);
+  for (int k = 0; k < 9; ++k) cell[9 * s + k] = (P)(sc * ref_cell[9 * s + k]);
+  p_eps[s] = pe;
+  eps[s] = e1;
+  v_eps[s] = v;
+}
+
+template <class P>
+__global__ void k_mtk_pre_atoms(int64_t n, P *x, P *p, const P *f, const P *m,
+                                const int64_t *sys, const int64_t *lo, const int64_t *hi,
+                                const double *v_eps, const double *dt) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t s = sys[i];
+  const double h = dt[s], h2 = h / 2.0, v = v_eps[s], mi = (double)m[i];
+  const double x2 = mtk_alpha(lo[s], hi[s]) * v * h2, x2h = x2 / 2.0;
+  const double e2 = exp(-x2), e2h = exp(-x2h), s2 = mtk_sinhx_x(x2h);
+  const double x1 = v * h, x1h = x1 / 2.0;
+  const double e1m = exp(x1) - 1.0, e1h = exp(x1h), s1 = mtk_sinhx_x(x1h);
+  for (int c = 0; c < 3; ++c) {
+    const double pn = (double)p[3 * i + c] * e2 + h2 * (double)f[3 * i + c] * s2 * e2h;
+    p[3 * i + c] = (P)pn;
+    const double r = (double)x[3 * i + c];
+    const double vel = (double)(P)pn / mi;
+    x[3 * i + c] = (P)(r + (r * e1m + h * vel * e1h * s1));
+  }
+}
+
+template <class P>
+__global__ void k_mtk_post_atoms(int64_t n, P *p, const P *f, const int64_t *sys,
+                                 const int64_t *lo, const int64_t *hi, const double *v_eps,
+                                 const double *dt) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t s = sys[i];
+  const double h2 = dt[s] / 2.0;
+  const double x2 = mtk_alpha(lo[s], hi[s]) * v_eps[s] * h2, x2h = x2 / 2.0;
+  const double e2 = exp(-x2), e2h = exp(-x2h), s2 = mtk_sinhx_x(x2h);
+  for (int c = 0; c < 3; ++c)
+    p[3 * i + c] = (P)((double)p[3 * i + c] * e2 + h2 * (double)f[3 * i + c] * s2 * e2h);
+}
+
+template <class P>
+__global__ void __launch_bounds__(256)
+    k_mtk_post_cell(const int64_t *lo, const int64_t *hi, const P *p, const P *m,
+                    const P *stress, const double *ref_cell, const double *eps, double *p_eps,
+                    const double *p_ext, const double *dt) {
+  __shared__ double sh[256 / 32];
+  const int64_t s = blockIdx.x;
+  const double two_ke = block_two_ke(lo[s], hi[s], p, m, sh);
+  if (threadIdx.x != 0) return;
+  const double ke = 0.5 * two_ke;
+  const double al = mtk_alpha(lo[s], hi[s]), h = dt[s];
+  const double vol = det3(ref_cell + 9 * s) * exp(3.0 * eps[s]);
+  const P *st = stress + 9 * s;
+  const double tr = (double)st[0] + (double)st[4] + (double)st[8];
+  const double f = (al * 2.0 * ke) - (tr * vol) - (p_ext[s] * vol * 3.0);
+  p_eps[s] = p_eps[s] + (h / 2.0) * f;
+}
+
 // Isotropic stochastic cell rescaling (C-rescale, Bernetti & Bussi 2020;
 // torch_sim/integrators/npt.py:2455-2492).  One block per system: the trace of
 // the instantaneous pressure tensor P = (sum_i p_i p_i^T / m_i) / V - stress
@@ -836,6 +955,78 @@ extern "C" int tsb_npt_langevin_aniso_post(
     TSB_NPTA_POST(float)
   }
 #undef TSB_NPTA_POST
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
+
+extern "C" int tsb_npt_nh_iso_pre(void *positions, void *momenta, const void *forces,
+                                  const void *masses, const int64_t *system_idx,
+                                  int64_t n_atoms, int64_t n_systems, int dtype,
+                                  const void *stress, const double *reference_cell, void *cell,
+                                  double *eps, double *p_eps, const double *cell_mass,
+                                  const double *p_ext, const double *dt, double *v_eps,
+                                  void *workspace, size_t workspace_bytes, void *stream) {
+  if (n_atoms < 1 || n_systems < 1 || !positions || !momenta || !forces || !masses ||
+      !system_idx || !stress || !reference_cell || !cell || !eps || !p_eps || !cell_mass ||
+      !p_ext || !dt || !v_eps)
+    return TSB_ERR_INVALID_ARG;
+  if (dtype != TSB_F32 && dtype != TSB_F64) return TSB_ERR_INVALID_ARG;
+  Carver c(workspace, workspace_bytes);
+  NptWork w;
+  carve_npt(c, w, n_systems);
+  if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaMemsetAsync(w.lo, 0, sizeof(int64_t) * n_systems, st);
+  cudaMemsetAsync(w.hi, 0, sizeof(int64_t) * n_systems, st);
+  k_npt_bounds<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, w.lo, w.hi);
+#define TSB_MTK_PRE(P)                                                                       \
+  k_mtk_pre_cell<P><<<(unsigned)n_systems, 256, 0, st>>>(                                    \
+      w.lo, w.hi, (const P *)momenta, (const P *)masses, (const P *)stress, reference_cell,  \
+      (P *)cell, eps, p_eps, cell_mass, p_ext, dt, v_eps);                                   \
+  k_mtk_pre_atoms<P><<<grid_for(n_atoms), kBlock, 0, st>>>(                                  \
+      n_atoms, (P *)positions, (P *)momenta, (const P *)forces, (const P *)masses,           \
+      system_idx, w.lo, w.hi, v_eps, dt);
+  if (dtype == TSB_F64) {
+    TSB_MTK_PRE(double)
+  } else {
+    TSB_MTK_PRE(float)
+  }
+#undef TSB_MTK_PRE
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
+
+extern "C" int tsb_npt_nh_iso_post(void *momenta, const void *forces, const void *masses,
+                                   const int64_t *system_idx, int64_t n_atoms,
+                                   int64_t n_systems, int dtype, const void *stress,
+                                   const double *reference_cell, const double *eps,
+                                   double *p_eps, const double *p_ext, const double *dt,
+                                   const double *v_eps, void *workspace,
+                                   size_t workspace_bytes, void *stream) {
+  if (n_atoms < 1 || n_systems < 1 || !momenta || !forces || !masses || !system_idx ||
+      !stress || !reference_cell || !eps || !p_eps || !p_ext || !dt || !v_eps)
+    return TSB_ERR_INVALID_ARG;
+  if (dtype != TSB_F32 && dtype != TSB_F64) return TSB_ERR_INVALID_ARG;
+  Carver c(workspace, workspace_bytes);
+  NptWork w;
+  carve_npt(c, w, n_systems);
+  if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaMemsetAsync(w.lo, 0, sizeof(int64_t) * n_systems, st);
+  cudaMemsetAsync(w.hi, 0, sizeof(int64_t) * n_systems, st);
+  k_npt_bounds<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, w.lo, w.hi);
+#define TSB_MTK_POST(P)                                                                      \
+  k_mtk_post_atoms<P><<<grid_for(n_atoms), kBlock, 0, st>>>(                                 \
+      n_atoms, (P *)momenta, (const P *)forces, system_idx, w.lo, w.hi, v_eps, dt);          \
+  k_mtk_post_cell<P><<<(unsigned)n_systems, 256, 0, st>>>(                                   \
+      w.lo, w.hi, (const P *)momenta, (const P *)masses, (const P *)stress, reference_cell,  \
+      eps, p_eps, p_ext, dt);
+  if (dtype == TSB_F64) {
+    TSB_MTK_POST(double)
+  } else {
+    TSB_MTK_POST(float)
+  }
+#undef TSB_MTK_POST
   TSB_CHECK_LAUNCH();
   return TSB_OK;
 }

@@ -78,6 +78,10 @@ PROTOTYPES = {
     "tsb_npt_langevin_aniso_post": (_int, [_vp, _vp, _vp, _vp, _vp, _i64, _i64, _int, _vp, _vp,
                                            _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                            _u64, _u64, _vp, _sz, _vp]),
+    "tsb_npt_nh_iso_pre": (_int, [_vp, _vp, _vp, _vp, _vp, _i64, _i64, _int, _vp, _vp, _vp,
+                                  _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "tsb_npt_nh_iso_post": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _int, _vp, _vp, _vp, _vp,
+                                   _vp, _vp, _vp, _vp, _sz, _vp]),
     "tsb_vlist_workspace_size": (_sz, [_i64, _i64]),
     "tsb_vlist_reset": (_int, [_i64, _i64, _vp, _sz, _vp]),
     "tsb_vlist_check": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _int, _dbl, _dbl, _vp, _vp, _sz,

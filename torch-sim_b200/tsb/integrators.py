@@ -474,6 +474,146 @@ def npt_crescale_isotropic_step(state, model, *, dt, kT, external_pressure, tau=
                           barostat=_crescale_simple("tsb_npt_crescale_iso", external_pressure))
 
 
+# ---------------------------------------------------------------------------
+# Isotropic NPT Nose-Hoover (MTK)
+# ---------------------------------------------------------------------------
+def _new_chain(n_sys, chain_length, dof, kT_s, tau_s, ke, dev):
+    from .state import NoseHooverChain
+
+    q = (kT_s * tau_s * tau_s).unsqueeze(-1).repeat(1, chain_length)
+    q[:, 0] *= dof
+    z = torch.zeros((n_sys, chain_length), dtype=torch.float64, device=dev)
+    return NoseHooverChain(positions=z.clone(), momenta=z.clone(), masses=q.contiguous(),
+                           tau=tau_s.clone(), kinetic_energy=ke.to(torch.float64).clone(),
+                           degrees_of_freedom=dof.to(torch.float64).clone())
+
+
+def npt_nose_hoover_isotropic_init(state, model, *, kT, dt, chain_length: int = 3,
+                                   chain_steps: int = 2, sy_steps: int = 3, t_tau=None,
+                                   b_tau=None, **kwargs):
+    """MTK isotropic NPT state (npt.py:1642-1809): t_tau = 10 dt, b_tau = 100 dt,
+    cell mass W = 3 (N + 1) kT b_tau^2, log volume and cell momentum zero; the
+    particle chain sees 3N - 3 degrees of freedom, the cell chain 1."""
+    from .state import NPTNoseHooverIsotropicState
+
+    if not 1 <= chain_length <= 16:
+        raise ValueError("chain_length must lie in 1..16")
+    if sy_steps not in (1, 3, 5, 7):
+        raise ValueError("sy_steps must be 1, 3, 5 or 7")
+    if kwargs.get("momenta") is not None:
+        state = MDState.from_state(state, momenta=kwargs["momenta"],
+                                   energy=torch.zeros(state.n_systems, dtype=state.dtype,
+                                                      device=state.device),
+                                   forces=torch.zeros_like(state.positions))
+    md = _md_init(state, model, kT)
+    out = model(md)
+    if "stress" not in out:
+        raise ValueError("NPT needs a model with compute_stress=True")
+    _prepare(md)
+    n_sys, dev = md.n_systems, md.device
+    dt_s = _per_system(dt, n_sys, dev)
+    kT_s = _per_system(kT, n_sys, dev)
+    t_tau_s = _per_system(10 * dt_s if t_tau is None else t_tau, n_sys, dev)
+    b_tau_s = _per_system(100 * dt_s if b_tau is None else b_tau, n_sys, dev)
+    n_at = torch.bincount(md.system_idx, minlength=n_sys).to(torch.float64)
+    zs = torch.zeros(n_sys, dtype=torch.float64, device=dev)
+    thermo = _new_chain(n_sys, chain_length, _dof(md), kT_s, t_tau_s, kinetic_energy(md), dev)
+    baro = _new_chain(n_sys, chain_length, torch.ones_like(zs), kT_s, b_tau_s, zs, dev)
+    st = NPTNoseHooverIsotropicState.from_state(
+        md, stress=out["stress"], reference_cell=md.cell.to(torch.float64).clone(),
+        cell_position=zs.clone(), cell_momentum=zs.clone().unsqueeze(-1),
+        cell_mass=3 * (n_at + 1) * kT_s * b_tau_s * b_tau_s, thermostat=thermo,
+        barostat=baro, chain_steps=int(chain_steps), sy_steps=int(sy_steps),
+        chain_dt=dt_s.clone())
+    return st
+
+
+def _chain_half(c, momenta, masses, system_idx, n_items, n_sys, dtype, kT_s, chain_dt,
+                chain_steps, sy_steps, recompute, dev):
+    ws = L.Workspace.get(dev, L.load().tsb_thermostat_workspace_size(n_sys))
+    L.call("tsb_nhc_half_step", L.ptr(momenta), L.ptr(masses), L.ptr(system_idx), n_items,
+           n_sys, L.dtype_code(dtype), L.ptr(c.positions), L.ptr(c.momenta), L.ptr(c.masses),
+           L.ptr(c.kinetic_energy), L.ptr(c.degrees_of_freedom), L.ptr(kT_s), L.ptr(c.tau),
+           L.ptr(chain_dt), c.positions.shape[1], chain_steps, sy_steps, int(recompute),
+           L.ptr(ws), ws.numel(), L.stream_ptr(dev))
+
+
+def npt_nose_hoover_isotropic_step(state, model, *, dt, kT, external_pressure, **_kw):
+    """One MTK isotropic NPT step (npt.py:1812-1963): cell chain and particle chain
+    half steps, the inner step (cell-momentum half kick, exp(iL2) momenta, log-volume
+    and exp(iL1) position updates, forces, exp(iL2), half kick), then the particle
+    and cell chain half steps with freshly summed kinetic energies."""
+    _prepare(state)
+    n_sys, n, dev = state.n_systems, state.n_atoms, state.device
+    dt_s = _per_system(dt, n_sys, dev)
+    kT_s = _per_system(kT, n_sys, dev)
+    p_s = _per_system(external_pressure, n_sys, dev)
+    for c in (state.thermostat, state.barostat):
+        for name in ("positions", "momenta", "masses", "tau", "kinetic_energy",
+                     "degrees_of_freedom"):
+            t = getattr(c, name)
+            if t.dtype != torch.float64 or not t.is_contiguous():
+                setattr(c, name, t.to(torch.float64).contiguous())
+    for name in ("reference_cell", "cell_position"):
+        setattr(state, name, getattr(state, name).to(torch.float64).contiguous())
+    state.cell = state.cell.to(state.dtype).contiguous()
+    state.stress = state.stress.to(state.dtype).contiguous()
+    n_at = torch.bincount(state.system_idx, minlength=n_sys).to(torch.float64)
+    b_tau = state.barostat.tau
+    state.cell_mass = (3 * (n_at + 1) * kT_s * b_tau * b_tau).contiguous()
+    # the cell momentum as a [S, 3] momentum array (p_eps, 0, 0) with mass W, one
+    # item per system, for the chain kernel
+    p3 = torch.zeros((n_sys, 3), dtype=state.dtype, device=dev)
+    p3[:, 0] = state.cell_momentum.reshape(n_sys).to(state.dtype)
+    w_mass = state.cell_mass.to(state.dtype).contiguous()
+    sys_items = torch.arange(n_sys, dtype=torch.int64, device=dev)
+    cd = state.chain_dt if state.chain_dt is not None else dt_s
+    _chain_half(state.barostat, p3, w_mass, sys_items, n_sys, n_sys, state.dtype, kT_s, cd,
+                state.chain_steps, state.sy_steps, False, dev)
+    _chain_half(state.thermostat, state.momenta, state.masses, state.system_idx, n, n_sys,
+                state.dtype, kT_s, cd, state.chain_steps, state.sy_steps, False, dev)
+    p_eps = p3[:, 0].to(torch.float64).contiguous()
+    v_eps = torch.empty(n_sys, dtype=torch.float64, device=dev)
+    ws = L.Workspace.get(dev, L.load().tsb_npt_workspace_size(n_sys))
+    dtc, stp = L.dtype_code(state.dtype), L.stream_ptr(dev)
+    L.call("tsb_npt_nh_iso_pre", L.ptr(state.positions), L.ptr(state.momenta),
+           L.ptr(state.forces), L.ptr(state.masses), L.ptr(state.system_idx), n, n_sys, dtc,
+           L.ptr(state.stress), L.ptr(state.reference_cell), L.ptr(state.cell),
+           L.ptr(state.cell_position), L.ptr(p_eps), L.ptr(state.cell_mass), L.ptr(p_s),
+           L.ptr(dt_s), L.ptr(v_eps), L.ptr(ws), ws.numel(), stp)
+    out = _apply_model(state, model)
+    state.stress = out["stress"].to(state.dtype).contiguous()
+    L.call("tsb_npt_nh_iso_post", L.ptr(state.momenta), L.ptr(state.forces),
+           L.ptr(state.masses), L.ptr(state.system_idx), n, n_sys, dtc, L.ptr(state.stress),
+           L.ptr(state.reference_cell), L.ptr(state.cell_position), L.ptr(p_eps), L.ptr(p_s),
+           L.ptr(dt_s), L.ptr(v_eps), L.ptr(ws), ws.numel(), stp)
+    _chain_half(state.thermostat, state.momenta, state.masses, state.system_idx, n, n_sys,
+                state.dtype, kT_s, cd, state.chain_steps, state.sy_steps, True, dev)
+    p3 = torch.zeros((n_sys, 3), dtype=state.dtype, device=dev)
+    p3[:, 0] = p_eps.to(state.dtype)
+    _chain_half(state.barostat, p3, w_mass, sys_items, n_sys, n_sys, state.dtype, kT_s, cd,
+                state.chain_steps, state.sy_steps, True, dev)
+    state.cell_momentum = p3[:, :1].to(torch.float64).clone()
+    return state
+
+
+def npt_nose_hoover_isotropic_invariant(state, kT, external_pressure) -> torch.Tensor:
+    """Extended energy (npt.py:1966-2059): E_pot + E_kin + both chains' energies
+    (particle chain with 3N - 3 degrees of freedom, cell chain with 1) + P V +
+    p_eps^2 / (2 W)."""
+    n_sys, dev = state.n_systems, state.device
+    kT_s = _per_system(kT, n_sys, dev)
+    p_s = _per_system(external_pressure, n_sys, dev)
+    e = state.energy.to(torch.float64) + kinetic_energy(state)
+    for c, dof in ((state.thermostat, _dof(state)),
+                   (state.barostat, torch.ones(n_sys, dtype=torch.float64, device=dev))):
+        e = e + c.momenta[:, 0] ** 2 / (2 * c.masses[:, 0]) + dof * kT_s * c.positions[:, 0]
+        for j in range(1, c.positions.shape[1]):
+            e = e + c.momenta[:, j] ** 2 / (2 * c.masses[:, j]) + kT_s * c.positions[:, j]
+    e = e + p_s * torch.linalg.det(state.cell.to(torch.float64))
+    return e + state.cell_momentum.reshape(n_sys) ** 2 / (2 * state.cell_mass)
+
+
 def npt_langevin_anisotropic_init(state, model, *, kT, dt, alpha=None, cell_alpha=None,
                                   b_tau=None, **_kw):
     """Per-axis strain NPT Langevin state (npt.py:409-510): eps = 0 [S,3], alpha =

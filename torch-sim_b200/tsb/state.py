@@ -242,6 +242,38 @@ class NPTLangevinAnisotropicState(MDState):
 
 
 @dataclass(kw_only=True)
+class NPTNoseHooverIsotropicState(MDState):
+    """MDState + MTK isotropic barostat with Nose-Hoover chains
+    (torch_sim/integrators/npt.py:1110-1219): stress [S,3,3]; reference_cell
+    [S,3,3]; log-volume ``cell_position`` [S] (ln(V/V0)/3), ``cell_momentum`` [S,1],
+    ``cell_mass`` [S]; particle ``thermostat`` and cell ``barostat`` chains; the
+    chains integrate with ``chain_dt`` [S]."""
+
+    stress: torch.Tensor
+    reference_cell: torch.Tensor
+    cell_position: torch.Tensor
+    cell_momentum: torch.Tensor
+    cell_mass: torch.Tensor
+    thermostat: NoseHooverChain
+    barostat: NoseHooverChain
+    chain_steps: int = 2
+    sy_steps: int = 3
+    chain_dt: torch.Tensor | None = None
+
+    @property
+    def current_cell(self) -> torch.Tensor:
+        v0 = torch.linalg.det(self.reference_cell)
+        v = v0 * torch.exp(3 * self.cell_position)
+        return torch.pow(v / v0, 1.0 / 3.0)[:, None, None] * self.reference_cell
+
+    def clone(self):
+        c = super().clone()
+        c.thermostat = self.thermostat.clone()
+        c.barostat = self.barostat.clone()
+        return c
+
+
+@dataclass(kw_only=True)
 class NPTCRescaleState(MDState):
     """MDState + stochastic cell rescaling (torch_sim/integrators/npt.py:2062-2090):
     stress [S,3,3]; per system isothermal_compressibility and tau_p; the initial cell
