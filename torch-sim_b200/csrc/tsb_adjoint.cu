@@ -39,11 +39,17 @@ __global__ void __launch_bounds__(128)
     k_lj_hvp(BinData b, int64_t n, const double *__restrict__ table, int nsp,
              const int32_t *__restrict__ species, double cutoff, const double *__restrict__ v,
              double coef, double *__restrict__ lam_q, double *__restrict__ gpart) {
-  __shared__ double sig[kAdjMaxSpecies * kAdjMaxSpecies], eps[kAdjMaxSpecies * kAdjMaxSpecies],
+  // per species pair: sigma^2, 1/sigma, epsilon, 1/epsilon, cutoff^2 (one FP64
+  // division per neighbour pair remains, 1/r)
+  __shared__ double sig2[kAdjMaxSpecies * kAdjMaxSpecies], isig[kAdjMaxSpecies * kAdjMaxSpecies],
+      eps[kAdjMaxSpecies * kAdjMaxSpecies], ieps[kAdjMaxSpecies * kAdjMaxSpecies],
       rc2[kAdjMaxSpecies * kAdjMaxSpecies];
   for (int k = threadIdx.x; k < nsp * nsp; k += blockDim.x) {
-    sig[k] = table[5 * k];
-    eps[k] = table[5 * k + 1];
+    const double sg = table[5 * k], ep = table[5 * k + 1];
+    sig2[k] = sg * sg;
+    isig[k] = 1.0 / sg;
+    eps[k] = ep;
+    ieps[k] = 1.0 / ep;
     const double r = fmin(cutoff, table[5 * k + 3]);
     rc2[k] = r * r;
   }
@@ -57,18 +63,21 @@ __global__ void __launch_bounds__(128)
   const int si = species ? min(max(species[i], 0), nsp - 1) : 0;
   const double vi0 = v[3 * i], vi1 = v[3 * i + 1], vi2 = v[3 * i + 2];
   double hx = 0, hy = 0, hz = 0;
-  double gs[kAdjMaxSpecies * kAdjMaxSpecies], ge[kAdjMaxSpecies * kAdjMaxSpecies];
-  for (int k = 0; k < nsp * nsp; ++k) gs[k] = ge[k] = 0.0;
-  auto pair = [&](int j, int, int, int, double dx, double dy, double dz, double d2, int) {
-                     const int sj = species ? min(max(species[j], 0), nsp - 1) : 0;
+  // parameter gradients of the pairs (si, t) by neighbour species t, in registers
+  // (a static select below keeps them out of local memory)
+  double gs[kAdjMaxSpecies], ge[kAdjMaxSpecies];
+#pragma unroll
+  for (int t2 = 0; t2 < kAdjMaxSpecies; ++t2) gs[t2] = ge[t2] = 0.0;
+  auto pair = [&](int j, int, int, int, double dx, double dy, double dz, double d2, int sp) {
+                     const int sj = min(max(sp, 0), nsp - 1);
                      const int k = si * nsp + sj;
                      if (!(d2 < rc2[k]) || !(d2 > 0.0)) return;
-                     const double r = sqrt(d2), ir = 1.0 / r;
+                     const double r = sqrt(d2), ir = 1.0 / r, ir2 = ir * ir;
                      const double ux = dx * ir, uy = dy * ir, uz = dz * ir;
-                     const double s2 = sig[k] * sig[k] / d2, s6 = s2 * s2 * s2, s12 = s6 * s6;
+                     const double s2 = sig2[k] * ir2, s6 = s2 * s2 * s2, s12 = s6 * s6;
                      const double e = eps[k];
                      const double vp = -(24.0 * e * ir) * (2.0 * s12 - s6);
-                     const double vpp = (24.0 * e / d2) * (26.0 * s12 - 7.0 * s6);
+                     const double vpp = (24.0 * e * ir2) * (26.0 * s12 - 7.0 * s6);
                      const double w0 = vi0 - v[3 * j], w1 = vi1 - v[3 * j + 1], w2 = vi2 - v[3 * j + 2];
                      const double uw = ux * w0 + uy * w1 + uz * w2;
                      const double a = vpp - vp * ir;  // K w = a (u.w) u + (V'/r) w
@@ -76,8 +85,14 @@ __global__ void __launch_bounds__(128)
                      hy += a * uw * uy + vp * ir * w1;
                      hz += a * uw * uz + vp * ir * w2;
                      const double uvi = ux * vi0 + uy * vi1 + uz * vi2;
-                     ge[k] += (vp / e) * uvi;
-                     gs[k] += (-(144.0 * e * ir / sig[k]) * (4.0 * s12 - s6)) * uvi;
+                     const double dge = (vp * ieps[k]) * uvi;
+                     const double dgs = (-(144.0 * e * ir * isig[k]) * (4.0 * s12 - s6)) * uvi;
+#pragma unroll
+                     for (int t2 = 0; t2 < kAdjMaxSpecies; ++t2)
+                       if (t2 == sj) {
+                         ge[t2] += dge;
+                         gs[t2] += dgs;
+                       }
                    };
   if constexpr (LANES > 1) {
     group_search_neighbors<LANES>(G, b.spos, b.bin_start, i, w.x, w.y, w.z, cutoff * cutoff, false,
@@ -85,10 +100,10 @@ __global__ void __launch_bounds__(128)
     hx = group_sum<LANES>(hx);
     hy = group_sum<LANES>(hy);
     hz = group_sum<LANES>(hz);
-    for (int k = 0; k < kAdjMaxSpecies * kAdjMaxSpecies; ++k) {
-      if (k >= nsp * nsp) break;
-      gs[k] = group_sum<LANES>(gs[k]);
-      ge[k] = group_sum<LANES>(ge[k]);
+#pragma unroll
+    for (int t2 = 0; t2 < kAdjMaxSpecies; ++t2) {
+      gs[t2] = group_sum<LANES>(gs[t2]);
+      ge[t2] = group_sum<LANES>(ge[t2]);
     }
     if ((threadIdx.x & (LANES - 1)) != 0) return;
   } else {
@@ -100,9 +115,15 @@ __global__ void __launch_bounds__(128)
   lam_q[3 * i + 2] -= coef * hz;
   double *g = gpart + (size_t)i * (2 * nsp * nsp);
   for (int k = 0; k < nsp * nsp; ++k) {
-    g[2 * k] = coef * gs[k];
-    g[2 * k + 1] = coef * ge[k];
+    g[2 * k] = 0.0;
+    g[2 * k + 1] = 0.0;
   }
+#pragma unroll
+  for (int t2 = 0; t2 < kAdjMaxSpecies; ++t2)
+    if (t2 < nsp) {
+      g[2 * (si * nsp + t2)] = coef * gs[t2];
+      g[2 * (si * nsp + t2) + 1] = coef * ge[t2];
+    }
 }
 
 // Gaussian-smeared histogram of pair distances r < r_max (each unordered pair
@@ -199,7 +220,7 @@ extern "C" int tsb_lj_hvp(const double *table, int n_species, const int32_t *spe
   if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   TSB_TRY(prepare_bins<double>(positions, cell_row, pbc, system_idx, n_atoms, n_systems, cutoff,
-                               w.b, st));
+                               w.b, st, species));
   if (n_atoms <= kGroupSearchMaxAtoms)
     k_lj_hvp<kSearchGroup><<<grid_for(kSearchGroup * n_atoms, 128), 128, 0, st>>>(
         w.b, n_atoms, table, n_species, species, cutoff, v, coef, lam_q, w.part);
