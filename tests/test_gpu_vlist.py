@@ -198,3 +198,45 @@ def test_single_system_engine_expires_on_cell_change():
     st.cell = (F @ st.cell[0]).unsqueeze(0).contiguous()
     _cmp(vm(st), ref(st), 1e-5, ("forces", "stress"))
     assert vm.n_builds == 2
+
+
+@pytest.mark.parametrize("rel", [1e-7, -1e-7])
+def test_vlist_fp32_path_decides_near_cutoff_pairs_in_fp64(rel):
+    """Perfect fcc lattices with the cutoff 1e-7 (relative) beyond or short of the
+    third neighbour shell: FP32 r^2 cannot tell these pairs apart from the cutoff
+    (its rounding is ~1e-6 relative here), so the mixed-precision path must
+    re-decide them from the FP64 positions, as the per-call search does.  One
+    wrong decision moves a system's energy by |V(r_c)| and its stress by
+    r_c |V'(r_c)| / volume; the paths must agree to a tenth of that."""
+    from tsb import models, workloads
+    from tsb.state import state_from_arrays
+
+    a, sig, eps = 5.26, 3.405, 0.0104
+    d = workloads.argon_fcc((4, 4, 4), a=a, jitter=0.0, n_systems=3)
+    st = state_from_arrays(d, device="cuda")
+    g = torch.Generator(device="cuda").manual_seed(1)
+    st.positions = (st.positions + 3.0 * torch.rand((st.n_systems, 3), device="cuda",
+                                                    dtype=st.dtype, generator=g)
+                    [st.system_idx]).contiguous()
+    rc = a * np.sqrt(1.5) * (1.0 + rel)
+    mk = lambda p: models.LennardJonesModel(sigma=sig, epsilon=eps, cutoff=rc,  # noqa
+                                            compute_stress=True, precision=p)
+    vm, ref = models.VerletListModel(mk("mixed"), skin=1.0), mk("mixed")
+    s6 = (sig / rc) ** 6
+    v_rc = abs(4 * eps * (s6 * s6 - s6))
+    w_rc = abs(4 * eps * (-12 * s6 * s6 + 6 * s6)) / (4 * a) ** 3
+
+    def check():
+        out, r = vm(st), ref(st)
+        assert not vm._last_single
+        de = (out["energy"] - r["energy"]).abs().max().item()
+        ds = (out["stress"] - r["stress"]).abs().max().item()
+        assert de < 0.1 * v_rc and ds < 0.1 * w_rc, (de / v_rc, ds / w_rc)
+
+    check()
+    # a uniform 0.5 % strain keeps the lists (bands from the strained cells)
+    F = torch.eye(3, dtype=st.dtype, device="cuda") * 1.005
+    st.positions = (st.positions @ F.T).contiguous()
+    st.cell = torch.einsum("ij,njk->nik", F, st.cell).contiguous()
+    check()
+    assert vm.n_builds == 1

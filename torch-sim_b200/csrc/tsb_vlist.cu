@@ -26,9 +26,17 @@
 // by the bins of its last build (perm[slot] = atom), so neighbouring threads and
 // their neighbours sit close in memory.  ELL list[k * N + slot] (uint32: slot of
 // j << 5 | image code), counts per slot, frame positions per slot as double4 with
-// the species in the high word of .w.  Force kernel: one thread per slot over its
-// list, FP64 displacements and cutoff test, pair function in R, FP64
-// accumulation, per-system sums in a fixed order (deterministic).
+// the species in the high word of .w (and as float4 for the FP32 path).  Force
+// kernel: one thread per slot over its list, pair function in R, FP64
+// accumulation, per-system sums in a fixed order (deterministic).  The FP64 path
+// forms displacements and the cutoff test in FP64.  The FP32 path gathers float4
+// positions and decides in FP32 outside a band around each cutoff that bounds
+// the FP32 rounding of r^2: with |coordinates|, |shifts| <= B, the FP32 r^2 of a
+// pair near the cutoff r_c is within 2^-24 (17.3 B r_c + 6.5 r_c^2) of the FP64
+// one; pairs inside twice that band are re-decided (and evaluated) from the FP64
+// positions, so the pair set is the FP64 one.  B = sum of the cell rows' norms +
+// skin/2 for a fully periodic system (frame positions stay within the cell plus
+// the allowed drift); systems with an open axis always take the FP64 test.
 #include "tsb_pair.cuh"
 #include "tsb_search.cuh"
 #include "tsb_sysreduce.cuh"
@@ -44,6 +52,8 @@ struct VlWork {
   int32_t *rwrap;      // [3N] W at the last build
   double *rinv;        // [9S] C0^-1 (rows), or the identity without a fractional frame
   int32_t *rframe;     // [S] the build had a fractional frame
+  double *rslack;      // [S] skin / 2 when every axis is periodic (bound on the drift
+                       // of a frame position from its affine image), else -1
   double *fdef;        // [9S] F = C0^-1 C of this call
   double *dmax;        // [S] allowed non-affine drift for this call
   int32_t *sys_exp;    // [S] rebuild this system
@@ -53,6 +63,9 @@ struct VlWork {
   int32_t *ecount;     // [S] atoms to rebuild per system
   int64_t *eoff;       // [S+1] their exclusive prefix (work list of the build)
   double4 *wpos;       // [N] current frame positions by slot, species in the high word
+  float4 *wpos32;      // [N] the same in FP32, species bits in .w
+  float *svf;          // [81 S] FP32 shift vectors
+  float *band;         // [S] FP32 decision band of r^2 (+inf: always FP64)
   double *sv;          // [81 S] S C per image code
   SysGeom *cur;        // [S] start / count / vol of the current cells
   double *e_half;      // [N]
@@ -69,6 +82,7 @@ static void carve_vl(Carver &c, VlWork &w, int64_t n, int64_t ns) {
   w.rwrap = c.take<int32_t>(3 * n);
   w.rinv = c.take<double>(9 * ns);
   w.rframe = c.take<int32_t>(ns);
+  w.rslack = c.take<double>(ns);
   w.fdef = c.take<double>(9 * ns);
   w.dmax = c.take<double>(ns);
   w.perm = c.take<int32_t>(n);
@@ -76,6 +90,9 @@ static void carve_vl(Carver &c, VlWork &w, int64_t n, int64_t ns) {
   w.ecount = c.take<int32_t>(ns);
   w.eoff = c.take<int64_t>(ns + 1);
   w.wpos = c.take<double4>(n);
+  w.wpos32 = c.take<float4>(n);
+  w.svf = c.take<float>(81 * ns);
+  w.band = c.take<float>(ns);
   w.sv = c.take<double>(81 * ns);
   w.cur = c.take<SysGeom>(ns);
   w.e_half = c.take<double>(n);
@@ -275,13 +292,14 @@ __global__ void __launch_bounds__(256)
 
 // per rebuilt system: record C0^-1 (the transpose of the frame matrix T)
 __global__ void k_vl_sys_built(const SysGeom *g, int64_t ns, int32_t *sys_exp, int32_t *built,
-                               double *rinv, int32_t *rframe) {
+                               double skin, double *rinv, int32_t *rframe, double *rslack) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= ns || !sys_exp[s]) return;
   const SysGeom &G = g[s];
   for (int r = 0; r < 3; ++r)
     for (int c = 0; c < 3; ++c) rinv[9 * s + 3 * r + c] = G.active ? G.T[3 * c + r] : (r == c);
   rframe[s] = G.active;
+  rslack[s] = G.active && G.per[0] && G.per[1] && G.per[2] ? 0.5 * skin : -1.0;
   built[s] = 1;
   sys_exp[s] = 0;
 }
@@ -289,16 +307,31 @@ __global__ void k_vl_sys_built(const SysGeom *g, int64_t ns, int32_t *sys_exp, i
 // per system for the force call: shift vectors, start / count, volume
 template <class P>
 __global__ void k_vl_sys_geom(const P *cell_row, int64_t ns, const int64_t *lo,
-                              const int64_t *hi, double *sv, SysGeom *cur) {
+                              const int64_t *hi, const double *rslack, double cutoff,
+                              double *sv, float *svf, float *band, SysGeom *cur) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= ns) return;
   double C[9];
   for (int k = 0; k < 9; ++k) C[k] = (double)cell_row[9 * s + k];
   for (int code = 0; code < 27; ++code) {
     const int sx = code / 9 - 1, sy = (code / 3) % 3 - 1, sz = code % 3 - 1;
-    for (int m = 0; m < 3; ++m)
-      sv[81 * s + 3 * code + m] = sx * C[m] + sy * C[3 + m] + sz * C[6 + m];
+    for (int m = 0; m < 3; ++m) {
+      const double v = sx * C[m] + sy * C[3 + m] + sz * C[6 + m];
+      sv[81 * s + 3 * code + m] = v;
+      svf[81 * s + 3 * code + m] = (float)v;
+    }
   }
+  double bsum = 0.0;
+  for (int k = 0; k < 3; ++k)
+    bsum += sqrt(C[3 * k] * C[3 * k] + C[3 * k + 1] * C[3 * k + 1] + C[3 * k + 2] * C[3 * k + 2]);
+  // |frame position| <= sum of row norms + drift, |shift| <= sum of row norms:
+  // FP32 rounding of the inputs, the difference, the shift sum and the square
+  // sum puts r^2 within 2^-24 (17.3 B r + 6.5 r^2) of the FP64 value near
+  // r = r_c, plus 2^-24 r_c^2 for the rounding of r_c^2; the band is twice it
+  const double B = bsum + rslack[s];
+  band[s] = rslack[s] >= 0.0
+                ? (float)(2.0 * ldexp(1.0, -24) * (17.4 * B * cutoff + 7.6 * cutoff * cutoff))
+                : INFINITY;
   SysGeom &G = cur[s];
   G.start = lo[s];
   G.count = (int32_t)(hi[s] - lo[s]);
@@ -310,7 +343,7 @@ __global__ void k_vl_sys_geom(const P *cell_row, int64_t ns, const int64_t *lo,
 template <class P>
 __global__ void k_vl_frame(const P *pos, const P *cell_row, const int64_t *sys,
                            const int32_t *species, int64_t n, const int32_t *perm,
-                           const int32_t *rwrap, double4 *wpos) {
+                           const int32_t *rwrap, double4 *wpos, float4 *wpos32) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   const int64_t i = perm[p];
@@ -322,62 +355,117 @@ __global__ void k_vl_frame(const P *pos, const P *cell_row, const int64_t *sys,
            (W0 * (double)C[m] + W1 * (double)C[3 + m] + W2 * (double)C[6 + m]);
   const unsigned long long hi = species ? (unsigned long long)(uint32_t)species[i] : 0ull;
   wpos[p] = make_double4(w[0], w[1], w[2], __longlong_as_double((long long)(hi << 32)));
+  wpos32[p] = make_float4((float)w[0], (float)w[1], (float)w[2], __int_as_float((int)hi));
 }
+
+__device__ __forceinline__ int vl_species(double w) { return tag_species(w); }
+__device__ __forceinline__ int vl_species(float w) { return __float_as_int(w); }
 
 template <int POT, class R, class P>
 __global__ void __launch_bounds__(kVlBlock)
-    k_vl_forces(const double4 *__restrict__ wpos, const uint32_t *__restrict__ list,
-                const int32_t *__restrict__ cnt, int64_t n, const int32_t *__restrict__ perm,
-                const int64_t *__restrict__ sys, const double *__restrict__ sv,
-                const double *__restrict__ table, int ns_species, double cutoff, int flags,
-                P *forces, P *energies, P *stresses, const SysGeom *__restrict__ cur,
-                double *e_half, double *vir_half, const uint8_t *__restrict__ active) {
+    k_vl_forces(const double4 *__restrict__ wpos, const float4 *__restrict__ wpos32,
+                const uint32_t *__restrict__ list, const int32_t *__restrict__ cnt, int64_t n,
+                const int32_t *__restrict__ perm, const int64_t *__restrict__ sys,
+                const double *__restrict__ sv, const float *__restrict__ svf,
+                const float *__restrict__ band, const double *__restrict__ table,
+                int ns_species, double cutoff, int flags, P *forces, P *energies, P *stresses,
+                const SysGeom *__restrict__ cur, double *e_half, double *vir_half,
+                const uint8_t *__restrict__ active) {
+  constexpr bool F32 = sizeof(R) == 4;
+  using Pos4 = std::conditional_t<F32, float4, double4>;
+  using Sh = std::conditional_t<F32, float, double>;
   __shared__ PairPrm<R> prm[kMaxSpecies * kMaxSpecies];
   __shared__ double prc2[kMaxSpecies * kMaxSpecies];
-  __shared__ double ssv[kVlSmemSys * 81];
+  __shared__ float prc2f[kMaxSpecies * kMaxSpecies];
+  __shared__ Sh ssv[kVlSmemSys * 81];
+  __shared__ float sband[kVlSmemSys];
   for (int k = threadIdx.x; k < ns_species * ns_species; k += blockDim.x) {
     prm[k] = make_prm<R>(POT, table + 5 * k, cutoff);
-    if constexpr (sizeof(R) == 4) prm_fast_extra(POT, table + 5 * k, prm[k]);
+    if constexpr (F32) prm_fast_extra(POT, table + 5 * k, prm[k]);
     prc2[k] = pair_rc2(POT, table + 5 * k, cutoff);
+    prc2f[k] = (float)prc2[k];
   }
   // slots are grouped by system, so a block spans systems s_lo..s_hi; the shift
-  // vectors of the first kVlSmemSys of them are staged in shared memory
+  // vectors (FP32 ones and the bands on the FP32 path) of the first kVlSmemSys of
+  // them are staged in shared memory
+  const Sh *shifts;
+  const Pos4 *__restrict__ wg;
+  if constexpr (F32) {
+    shifts = svf;
+    wg = wpos32;
+  } else {
+    shifts = sv;
+    wg = wpos;
+  }
   const int64_t p0 = (int64_t)blockIdx.x * blockDim.x;
   const int64_t s_lo = sys[perm[p0]];
   const int64_t s_hi = sys[perm[min(p0 + (int64_t)blockDim.x, n) - 1]];
   const int n_st = (int)min(s_hi - s_lo + 1, (int64_t)kVlSmemSys);
-  for (int k = threadIdx.x; k < 81 * n_st; k += blockDim.x) ssv[k] = sv[81 * s_lo + k];
+  for (int k = threadIdx.x; k < 81 * n_st; k += blockDim.x) ssv[k] = shifts[81 * s_lo + k];
+  if constexpr (F32)
+    for (int k = threadIdx.x; k < n_st; k += blockDim.x) sband[k] = band[s_lo + k];
   __syncthreads();
   const int64_t p = p0 + threadIdx.x;
   if (p >= n) return;
   const int64_t i = perm[p];
   const int64_t s = sys[i];
   if (active && !active[s]) return;
-  const double4 wi = wpos[p];
-  const int si = min(max(tag_species(wi.w), 0), ns_species - 1);
+  const Pos4 wi = wg[p];
+  const int si = min(max(vl_species(wi.w), 0), ns_species - 1);
   const PairPrm<R> *row = prm + si * ns_species;
   const double *rc2row = prc2 + si * ns_species;
-  const double *svs = s - s_lo < n_st ? ssv + 81 * (s - s_lo) : sv + 81 * s;
+  const float *rc2frow = prc2f + si * ns_species;
+  const bool staged = s - s_lo < n_st;
+  const Sh *svs = staged ? ssv + 81 * (s - s_lo) : shifts + 81 * s;
+  float bnd = 0.f;
+  if constexpr (F32) bnd = staged ? sband[s - s_lo] : band[s];
   const bool want_vir = flags & (TSB_OUT_STRESS | TSB_OUT_STRESSES);
   const int c = cnt[p];
   double fx = 0.0, fy = 0.0, fz = 0.0, ei = 0.0;
   double vxx = 0, vyy = 0, vzz = 0, vyz = 0, vxz = 0, vxy = 0;
-  // one entry E with neighbour frame position WJ: FP64 displacement and cutoff
-  // test, pair function in R, FP64 accumulation
+  // one entry E with neighbour frame position WJ.  FP64 path: FP64 displacement
+  // and cutoff test.  FP32 path: FP32 displacement and test, except within the
+  // band around the cutoff, where both come from the FP64 positions.  Pair
+  // function in R, FP64 accumulation.
 #define TSB_VLPAIR(E, WJ)                                                                    \
   {                                                                                          \
     const int code = (int)((E) & 31u);                                                       \
-    const double dx = (WJ).x - wi.x + svs[3 * code];                                         \
-    const double dy = (WJ).y - wi.y + svs[3 * code + 1];                                     \
-    const double dz = (WJ).z - wi.z + svs[3 * code + 2];                                     \
-    const int sj = min(max(tag_species((WJ).w), 0), ns_species - 1);                        \
-    const double d2 = dx * dx + dy * dy + dz * dz;                                           \
-    if (d2 < rc2row[sj]) {                                                                   \
+    const int sj = min(max(vl_species((WJ).w), 0), ns_species - 1);                         \
+    double dx, dy, dz;                                                                       \
+    bool in_;                                                                                \
+    R r2;                                                                                    \
+    if constexpr (F32) {                                                                     \
+      const float ax = (WJ).x - wi.x + svs[3 * code];                                        \
+      const float ay = (WJ).y - wi.y + svs[3 * code + 1];                                    \
+      const float az = (WJ).z - wi.z + svs[3 * code + 2];                                    \
+      r2 = ax * ax + ay * ay + az * az;                                                      \
+      in_ = r2 < rc2frow[sj];                                                                \
+      dx = ax;                                                                               \
+      dy = ay;                                                                               \
+      dz = az;                                                                               \
+      if (!(fabsf(r2 - rc2frow[sj]) >= bnd)) {                                               \
+        const double4 di = wpos[p], dj = wpos[(E) >> 5];                                     \
+        const double *sd = sv + 81 * s + 3 * code;                                           \
+        dx = dj.x - di.x + sd[0];                                                            \
+        dy = dj.y - di.y + sd[1];                                                            \
+        dz = dj.z - di.z + sd[2];                                                            \
+        const double d2 = dx * dx + dy * dy + dz * dz;                                       \
+        in_ = d2 < rc2row[sj];                                                               \
+        r2 = (float)d2;                                                                      \
+      }                                                                                      \
+    } else {                                                                                 \
+      dx = (WJ).x - wi.x + svs[3 * code];                                                    \
+      dy = (WJ).y - wi.y + svs[3 * code + 1];                                                \
+      dz = (WJ).z - wi.z + svs[3 * code + 2];                                                \
+      r2 = dx * dx + dy * dy + dz * dz;                                                      \
+      in_ = r2 < rc2row[sj];                                                                 \
+    }                                                                                        \
+    if (in_) {                                                                               \
       R ep, fr;                                                                              \
-      if constexpr (sizeof(R) == 4)                                                          \
-        pair_eval_fast<POT>(row[sj], (float)d2, ep, fr);                                     \
+      if constexpr (F32)                                                                     \
+        pair_eval_fast<POT>(row[sj], r2, ep, fr);                                            \
       else                                                                                   \
-        pair_eval<POT, R>(row[sj], (R)d2, ep, fr);                                           \
+        pair_eval<POT, R>(row[sj], r2, ep, fr);                                              \
       const double gr = (double)fr;                                                          \
       const double gx = gr * dx, gy = gr * dy, gz = gr * dz;                                 \
       fx -= gx;                                                                              \
@@ -414,8 +502,8 @@ __global__ void __launch_bounds__(kVlBlock)
       f2 = q[(size_t)2 * n];
       f3 = q[(size_t)3 * n];
     }
-    const double4 w0 = wpos[e0 >> 5], w1 = wpos[e1 >> 5];
-    const double4 w2 = wpos[e2 >> 5], w3 = wpos[e3 >> 5];
+    const Pos4 w0 = wg[e0 >> 5], w1 = wg[e1 >> 5];
+    const Pos4 w2 = wg[e2 >> 5], w3 = wg[e3 >> 5];
     TSB_VLPAIR(e0, w0)
     TSB_VLPAIR(e1, w1)
     TSB_VLPAIR(e2, w2)
@@ -427,7 +515,7 @@ __global__ void __launch_bounds__(kVlBlock)
   }
   for (; k < c; ++k) {
     const uint32_t e = lp[(size_t)k * n];
-    const double4 wj = wpos[e >> 5];
+    const Pos4 wj = wg[e >> 5];
     TSB_VLPAIR(e, wj)
   }
 #undef TSB_VLPAIR
@@ -488,8 +576,8 @@ static int vl_build(const P *pos, const P *cell, const uint8_t *pbc, const int64
   k_vl_build<<<(unsigned)(n_sm * 8), 256, 0, st>>>(w.b, n, ns, rcs * rcs, w.eoff, w.islot, list,
                                                     counts, max_nb, flags, w.perm, w.ref,
                                                     w.rwrap);
-  k_vl_sys_built<<<grid_for(ns), kBlock, 0, st>>>(w.b.geom, ns, w.sys_exp, w.sys_built, w.rinv,
-                                                  w.rframe);
+  k_vl_sys_built<<<grid_for(ns), kBlock, 0, st>>>(w.b.geom, ns, w.sys_exp, w.sys_built, skin,
+                                                  w.rinv, w.rframe, w.rslack);
   TSB_CHECK_LAUNCH();
   return TSB_OK;
 }
@@ -500,8 +588,8 @@ static void vl_launch(VlWork &w, const uint32_t *list, const int32_t *counts, in
                       int flags, P *forces, P *energies, P *stresses, const uint8_t *active,
                       cudaStream_t st) {
   k_vl_forces<POT, R, P><<<grid_for(n, kVlBlock), kVlBlock, 0, st>>>(
-      w.wpos, list, counts, n, w.perm, sys, w.sv, table, nsp, cutoff, flags, forces, energies,
-      stresses, w.cur, w.e_half, w.vir_half, active);
+      w.wpos, w.wpos32, list, counts, n, w.perm, sys, w.sv, w.svf, w.band, table, nsp, cutoff,
+      flags, forces, energies, stresses, w.cur, w.e_half, w.vir_half, active);
 }
 
 template <class P>
@@ -510,10 +598,10 @@ static int vl_forces(int pot, const double *table, int nsp, const int32_t *speci
                      const int64_t *sys, const uint8_t *active, int64_t n, int64_t ns,
                      double cutoff, int flags, P *energy, P *forces, P *stress, P *energies,
                      P *stresses, VlWork &w, cudaStream_t st) {
-  k_vl_sys_geom<P><<<grid_for(ns), kBlock, 0, st>>>(cell, ns, w.b.sys_lo, w.b.sys_hi, w.sv,
-                                                    w.cur);
+  k_vl_sys_geom<P><<<grid_for(ns), kBlock, 0, st>>>(cell, ns, w.b.sys_lo, w.b.sys_hi, w.rslack,
+                                                    cutoff, w.sv, w.svf, w.band, w.cur);
   k_vl_frame<P><<<grid_for(n), kBlock, 0, st>>>(pos, cell, sys, species, n, w.perm, w.rwrap,
-                                                w.wpos);
+                                                w.wpos, w.wpos32);
   const bool f64 = flags & TSB_MATH_FP64;
 #define TSB_VLL(POT)                                                                        \
   if (f64)                                                                                  \
@@ -560,6 +648,7 @@ extern "C" int tsb_vlist_reset(int64_t n_atoms, int64_t n_systems, void *workspa
   cudaStream_t st = (cudaStream_t)stream;
   cudaMemsetAsync(w.sys_built, 0, sizeof(int32_t) * n_systems, st);
   cudaMemsetAsync(w.sys_exp, 0, sizeof(int32_t) * n_systems, st);
+  cudaMemsetAsync(w.rslack, 0xff, sizeof(double) * n_systems, st);  // NaN: FP64 test
   k_vl_iota<<<grid_for(n_atoms), kBlock, 0, st>>>(w.perm, n_atoms);
   TSB_CHECK_LAUNCH();
   return TSB_OK;
