@@ -304,23 +304,25 @@ __global__ void k_vl_sys_built(const SysGeom *g, int64_t ns, int32_t *sys_exp, i
   sys_exp[s] = 0;
 }
 
-// per system for the force call: shift vectors, start / count, volume
+// per system for the force call: shift vectors (one thread per system and image
+// code), and from the code-0 thread the FP32 band, start / count and volume
 template <class P>
 __global__ void k_vl_sys_geom(const P *cell_row, int64_t ns, const int64_t *lo,
                               const int64_t *hi, const double *rslack, double cutoff,
                               double *sv, float *svf, float *band, SysGeom *cur) {
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= ns) return;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 27 * ns) return;
+  const int64_t s = t / 27;
+  const int code = (int)(t - 27 * s);
   double C[9];
   for (int k = 0; k < 9; ++k) C[k] = (double)cell_row[9 * s + k];
-  for (int code = 0; code < 27; ++code) {
-    const int sx = code / 9 - 1, sy = (code / 3) % 3 - 1, sz = code % 3 - 1;
-    for (int m = 0; m < 3; ++m) {
-      const double v = sx * C[m] + sy * C[3 + m] + sz * C[6 + m];
-      sv[81 * s + 3 * code + m] = v;
-      svf[81 * s + 3 * code + m] = (float)v;
-    }
+  const int sx = code / 9 - 1, sy = (code / 3) % 3 - 1, sz = code % 3 - 1;
+  for (int m = 0; m < 3; ++m) {
+    const double v = sx * C[m] + sy * C[3 + m] + sz * C[6 + m];
+    sv[81 * s + 3 * code + m] = v;
+    svf[81 * s + 3 * code + m] = (float)v;
   }
+  if (code) return;
   double bsum = 0.0;
   for (int k = 0; k < 3; ++k)
     bsum += sqrt(C[3 * k] * C[3 * k] + C[3 * k + 1] * C[3 * k + 1] + C[3 * k + 2] * C[3 * k + 2]);
@@ -460,12 +462,15 @@ __global__ void __launch_bounds__(kVlBlock)
       r2 = dx * dx + dy * dy + dz * dz;                                                      \
       in_ = r2 < rc2row[sj];                                                                 \
     }                                                                                        \
-    if (in_) {                                                                               \
+    if (F32 || in_) {                                                                        \
       R ep, fr;                                                                              \
-      if constexpr (F32)                                                                     \
+      if constexpr (F32) {                                                                   \
         pair_eval_fast<POT>(row[sj], r2, ep, fr);                                            \
-      else                                                                                   \
+        fr = in_ ? fr : 0.f;                                                                 \
+        ep = in_ ? ep : 0.f;                                                                 \
+      } else {                                                                               \
         pair_eval<POT, R>(row[sj], r2, ep, fr);                                              \
+      }                                                                                      \
       const double gr = (double)fr;                                                          \
       const double gx = gr * dx, gy = gr * dy, gz = gr * dz;                                 \
       fx -= gx;                                                                              \
@@ -598,8 +603,9 @@ static int vl_forces(int pot, const double *table, int nsp, const int32_t *speci
                      const int64_t *sys, const uint8_t *active, int64_t n, int64_t ns,
                      double cutoff, int flags, P *energy, P *forces, P *stress, P *energies,
                      P *stresses, VlWork &w, cudaStream_t st) {
-  k_vl_sys_geom<P><<<grid_for(ns), kBlock, 0, st>>>(cell, ns, w.b.sys_lo, w.b.sys_hi, w.rslack,
-                                                    cutoff, w.sv, w.svf, w.band, w.cur);
+  k_vl_sys_geom<P><<<grid_for(27 * ns), kBlock, 0, st>>>(cell, ns, w.b.sys_lo, w.b.sys_hi,
+                                                         w.rslack, cutoff, w.sv, w.svf, w.band,
+                                                         w.cur);
   k_vl_frame<P><<<grid_for(n), kBlock, 0, st>>>(pos, cell, sys, species, n, w.perm, w.rwrap,
                                                 w.wpos, w.wpos32);
   const bool f64 = flags & TSB_MATH_FP64;
