@@ -59,7 +59,6 @@ struct VlWork {
   int32_t *sys_exp;    // [S] rebuild this system
   int32_t *sys_built;  // [S]
   int32_t *perm;       // [N] atom of each slot (identity until a system is built)
-  int32_t *islot;      // [N] slot of each atom in the fresh bins of a build
   int32_t *ecount;     // [S] atoms to rebuild per system
   int64_t *eoff;       // [S+1] their exclusive prefix (work list of the build)
   double4 *wpos;       // [N] current frame positions by slot, species in the high word
@@ -86,7 +85,6 @@ static void carve_vl(Carver &c, VlWork &w, int64_t n, int64_t ns) {
   w.fdef = c.take<double>(9 * ns);
   w.dmax = c.take<double>(ns);
   w.perm = c.take<int32_t>(n);
-  w.islot = c.take<int32_t>(n);
   w.ecount = c.take<int32_t>(ns);
   w.eoff = c.take<int64_t>(ns + 1);
   w.wpos = c.take<double4>(n);
@@ -174,12 +172,6 @@ __global__ void k_vl_iota(int32_t *perm, int64_t n) {
   if (i < n) perm[i] = (int32_t)i;
 }
 
-// slot of each atom in the fresh bin order
-__global__ void k_vl_islot(const int32_t *sidx, int64_t n, int32_t *islot) {
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p < n) islot[sidx[p]] = (int32_t)p;
-}
-
 // atoms of expired systems, for the work list of the build
 __global__ void k_vl_exp_counts(const int32_t *sys_exp, const int64_t *lo, const int64_t *hi,
                                 int64_t ns, int32_t *ecount) {
@@ -190,15 +182,19 @@ __global__ void k_vl_exp_counts(const int32_t *sys_exp, const int64_t *lo, const
 // List search for the atoms of expired systems over fresh bins (cutoff + skin),
 // one warp per atom.  Work item t (< eoff[ns]) is atom t - eoff[s] of system s,
 // the last system with eoff[s] <= t (bisection; empty systems are skipped); a
-// fixed grid of warps strides over the items.  The warp walks the atom's search
-// window row by row: bins of a row and image are adjacent in bin order, so each
-// span of candidates is contiguous and the lanes test 32 of them at a time; hits
-// are compacted with a ballot, so the list order (row, span, candidate) is fixed
-// and the writes of a span are coalesced.
-__global__ void __launch_bounds__(256)
+// fixed grid of warps strides over the items.  The atom's search window is cut
+// into spans: a row of bins (fixed x and y bin) within one periodic image along
+// z is a contiguous run of candidates in bin order.  Each lane takes one span
+// (32 at a time) and the warp steps through candidate t of every span together,
+// two steps per iteration, so the loads of all spans are in flight at once
+// instead of one span after another.  Hits are compacted with a ballot, so the
+// list order (step, span) is fixed and the writes of a step are coalesced.  A
+// rebuilt system's slots are its fresh bin order, so a candidate's bin-order
+// index is its slot.
+__global__ void __launch_bounds__(256, 4)
     k_vl_build(BinData b, int64_t n, int64_t ns, double rcs2, const int64_t *eoff,
-               const int32_t *islot, uint32_t *list, int32_t *cnt, int max_nb, int32_t *flags,
-               int32_t *perm, double4 *ref, int32_t *rwrap) {
+               uint32_t *list, int32_t *cnt, int max_nb, int32_t *flags, int32_t *perm,
+               double4 *ref, int32_t *rwrap) {
   const int lane = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;
   const int64_t n_work = eoff[ns];
@@ -228,54 +224,69 @@ __global__ void __launch_bounds__(256)
       lo[k] = (int)f0;
       hi[k] = (int)f1;
     }
-    const int nb1 = G.nb[1], nb2 = G.nb[2];
+    const int nb0 = G.nb[0], nb1 = G.nb[1], nb2 = G.nb[2];
+    const int nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1;
+    const int iz_lo = G.per[2] ? floordiv_dev(lo[2], nb2) : 0;
+    const int nzs = G.per[2] ? floordiv_dev(hi[2], nb2) - iz_lo + 1 : (hi[2] >= lo[2]);
+    const int n_spans = nx > 0 && ny > 0 ? nx * ny * nzs : 0;
     int c = 0;
-    for (int cx = lo[0]; cx <= hi[0]; ++cx) {
-      const int ix = G.per[0] ? floordiv_dev(cx, G.nb[0]) : 0;
-      const int bx = cx - ix * G.nb[0];
-      for (int cy = lo[1]; cy <= hi[1]; ++cy) {
+    for (int base = 0; base < n_spans; base += 32) {
+      // this lane's span: candidates q0..q1-1 with image shift (sx, sy, sz)
+      const int k = base + lane;
+      int64_t q0 = 0, q1 = 0;
+      double sx = 0.0, sy = 0.0, sz = 0.0;
+      uint32_t code = 0;
+      bool in_range = true, zero_shift = false;
+      if (k < n_spans) {
+        const int zs = k % nzs, r = k / nzs;
+        const int cx = lo[0] + r / ny, cy = lo[1] + r % ny;
+        const int ix = G.per[0] ? floordiv_dev(cx, nb0) : 0;
         const int iy = G.per[1] ? floordiv_dev(cy, nb1) : 0;
-        const int by = cy - iy * nb1;
+        const int iz = iz_lo + zs;
+        const int bx = cx - ix * nb0, by = cy - iy * nb1;
+        const int bz0 = max(lo[2], iz * nb2) - iz * nb2;
+        const int bz1 = min(hi[2], iz * nb2 + nb2 - 1) - iz * nb2;
         const int row = G.bin_base + (bx * nb1 + by) * nb2;
-        for (int cz = lo[2]; cz <= hi[2];) {
-          const int iz = G.per[2] ? floordiv_dev(cz, nb2) : 0;
-          const int bz = cz - iz * nb2;
-          const int bz_end = min(nb2 - 1, bz + (hi[2] - cz));  // last bin of this image
-          cz += bz_end - bz + 1;
-          const double sx = ix * G.cell[0] + iy * G.cell[3] + iz * G.cell[6];
-          const double sy = ix * G.cell[1] + iy * G.cell[4] + iz * G.cell[7];
-          const double sz = ix * G.cell[2] + iy * G.cell[5] + iz * G.cell[8];
-          const bool zero_shift = (ix | iy | iz) == 0;
-          const bool in_range =
-              ix >= -1 && ix <= 1 && iy >= -1 && iy <= 1 && iz >= -1 && iz <= 1;
-          const uint32_t code = (uint32_t)((ix + 1) * 9 + (iy + 1) * 3 + (iz + 1));
-          const int64_t q1 = b.bin_start[row + bz_end + 1];
-          for (int64_t q0 = b.bin_start[row + bz]; q0 < q1; q0 += 32) {
-            const int64_t q = q0 + lane;
-            bool hit = false;
-            int j = 0;
-            if (q < q1) {
-              const double4 o = b.spos[q];
-              const double dx = (o.x + sx) - w.x;
-              const double dy = (o.y + sy) - w.y;
-              const double dz = (o.z + sz) - w.z;
-              j = tag_atom(o.w);
-              hit = dx * dx + dy * dy + dz * dz < rcs2 && !(j == i && zero_shift);
-            }
-            const unsigned m = __ballot_sync(0xffffffffu, hit);
-            if (m == 0u) continue;
-            if (!in_range) {  // a hit beyond the first images: cell narrower than rc + skin
-              if (lane == 0) atomicMax(&flags[1], 1 << 30);
-              continue;
-            }
-            if (hit) {
-              const int k = c + __popc(m & lt_mask);
-              if (k < max_nb) list[(size_t)k * n + p] = ((uint32_t)islot[j] << 5) | code;
-            }
-            c += __popc(m);
-          }
-        }
+        q0 = b.bin_start[row + bz0];
+        q1 = b.bin_start[row + bz1 + 1];
+        sx = ix * G.cell[0] + iy * G.cell[3] + iz * G.cell[6];
+        sy = ix * G.cell[1] + iy * G.cell[4] + iz * G.cell[7];
+        sz = ix * G.cell[2] + iy * G.cell[5] + iz * G.cell[8];
+        zero_shift = (ix | iy | iz) == 0;
+        in_range = ix >= -1 && ix <= 1 && iy >= -1 && iy <= 1 && iz >= -1 && iz <= 1;
+        code = (uint32_t)((ix + 1) * 9 + (iy + 1) * 3 + (iz + 1));
       }
+      const int len = __reduce_max_sync(0xffffffffu, (unsigned)(q1 - q0));
+      // test candidate q: a hit beyond the first images means a cell narrower
+      // than cutoff + skin (the build fails)
+#define TSB_VL_TEST(Q, O)                                                                    \
+  {                                                                                          \
+    bool hit = false;                                                                        \
+    if ((Q) < q1) {                                                                          \
+      const double dx = ((O).x + sx) - w.x;                                                  \
+      const double dy = ((O).y + sy) - w.y;                                                  \
+      const double dz = ((O).z + sz) - w.z;                                                  \
+      hit = dx * dx + dy * dy + dz * dz < rcs2 && !((Q) == p && zero_shift);                 \
+    }                                                                                        \
+    if (__any_sync(0xffffffffu, hit && !in_range) && lane == 0)                              \
+      atomicMax(&flags[1], 1 << 30);                                                         \
+    hit = hit && in_range;                                                                   \
+    const unsigned m = __ballot_sync(0xffffffffu, hit);                                      \
+    if (hit) {                                                                               \
+      const int kk = c + __popc(m & lt_mask);                                                \
+      if (kk < max_nb) list[(size_t)kk * n + p] = ((uint32_t)(Q) << 5) | code;               \
+    }                                                                                        \
+    c += __popc(m);                                                                          \
+  }
+      for (int st = 0; st < len; st += 2) {
+        const int64_t qa = q0 + st, qb = qa + 1;
+        double4 oa = make_double4(0.0, 0.0, 0.0, 0.0), ob = oa;
+        if (qa < q1) oa = b.spos[qa];
+        if (qb < q1) ob = b.spos[qb];
+        TSB_VL_TEST(qa, oa)
+        TSB_VL_TEST(qb, ob)
+      }
+#undef TSB_VL_TEST
     }
     if (lane == 0) {
       cnt[p] = c < max_nb ? c : max_nb;
@@ -570,7 +581,6 @@ static int vl_build(const P *pos, const P *cell, const uint8_t *pbc, const int64
   cudaMemsetAsync(flags + 1, 0, sizeof(int32_t), st);
   const double rcs = cutoff + skin;
   TSB_TRY(prepare_bins<P>(pos, cell, pbc, sys, n, ns, rcs, w.b, st, species));
-  k_vl_islot<<<grid_for(n), kBlock, 0, st>>>(w.b.sidx, n, w.islot);
   k_vl_exp_counts<<<grid_for(ns), kBlock, 0, st>>>(w.sys_exp, w.b.sys_lo, w.b.sys_hi, ns,
                                                    w.ecount);
   TSB_TRY(exclusive_scan(w.ecount, w.eoff, ns, w.b.scan_tmp, st));
@@ -578,9 +588,8 @@ static int vl_build(const P *pos, const P *cell, const uint8_t *pbc, const int64
   int dev = 0, n_sm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-  k_vl_build<<<(unsigned)(n_sm * 8), 256, 0, st>>>(w.b, n, ns, rcs * rcs, w.eoff, w.islot, list,
-                                                    counts, max_nb, flags, w.perm, w.ref,
-                                                    w.rwrap);
+  k_vl_build<<<(unsigned)(n_sm * 8), 256, 0, st>>>(w.b, n, ns, rcs * rcs, w.eoff, list, counts,
+                                                    max_nb, flags, w.perm, w.ref, w.rwrap);
   k_vl_sys_built<<<grid_for(ns), kBlock, 0, st>>>(w.b.geom, ns, w.sys_exp, w.sys_built, skin,
                                                   w.rinv, w.rframe, w.rslack);
   TSB_CHECK_LAUNCH();
