@@ -281,11 +281,14 @@ int tsb_npt_crescale_tri(void *positions, void *momenta, const void *masses,
  * The workspace (tsb_vlist_workspace_size) holds the list frame and must be kept
  * by the caller between calls; tsb_vlist_reset marks every system unbuilt.
  * tsb_vlist_check: flags[0] = 1 when any active system must be rebuilt.
- * tsb_vlist_build: rebins the batch and rebuilds the expired systems' lists
- *   (list[k * N + slot] = slot of j << 5 | image code, counts [N] by slot);
- *   flags[1] = 1 << 30 when a periodic cell is narrower than cutoff + skin, else
- *   the largest neighbour count when it exceeded max_neighbors (regrow, reset and
- *   build again), else 0.
+ * tsb_vlist_build: rebins and rebuilds the expired systems' lists
+ *   (list[k * N + slot] = slot of j << 5 | image code, counts [N] by slot).
+ *   max_system_atoms = the largest system's atom count (0: unknown); when it is
+ *   at most 4096 only the expired systems are rebinned, one block each, else the
+ *   whole batch is.  flags[1] = 1 << 30 when a periodic cell is narrower than
+ *   cutoff + skin, 1 << 29 when a system exceeds a max_system_atoms of at most
+ *   4096, else the largest neighbour count when it exceeded max_neighbors (regrow,
+ *   reset and build again), else 0.
  * tsb_vlist_forces: energy [S], forces [N,3], stress [S,3,3], per-atom energies
  *   [N] and stresses [N,3,3] per out_flags (TSB_MATH_FP64: FP64 pair function),
  *   for the systems with sys_active != 0 (NULL: all).  LJ, Morse, soft sphere. */
@@ -299,8 +302,8 @@ int tsb_vlist_check(const void *positions, const void *cell_row, const int64_t *
 int tsb_vlist_build(const void *positions, const void *cell_row, const uint8_t *pbc,
                     const int64_t *system_idx, const int32_t *species, int64_t n_atoms,
                     int64_t n_systems, int dtype, double cutoff, double skin, uint32_t *list,
-                    int32_t *counts, int max_neighbors, int32_t *flags, void *workspace,
-                    size_t workspace_bytes, void *stream);
+                    int32_t *counts, int max_neighbors, int64_t max_system_atoms,
+                    int32_t *flags, void *workspace, size_t workspace_bytes, void *stream);
 int tsb_vlist_forces(int potential, const double *table, int n_species, const int32_t *species,
                      const uint32_t *list, const int32_t *counts, const void *positions,
                      const void *cell_row, const int64_t *system_idx, const uint8_t *sys_active,

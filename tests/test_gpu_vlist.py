@@ -240,3 +240,57 @@ def test_vlist_fp32_path_decides_near_cutoff_pairs_in_fp64(rel):
     st.cell = torch.einsum("ij,njk->nik", F, st.cell).contiguous()
     check()
     assert vm.n_builds == 1
+
+
+def _argon_batch(shapes, jitter=0.1, seed=0):
+    from tsb import workloads
+
+    parts = [workloads.argon_fcc(n, jitter=jitter, seed=seed + k) for k, n in enumerate(shapes)]
+    off = np.cumsum([0] + [len(p["positions"]) for p in parts])
+    return {
+        "positions": np.concatenate([p["positions"] for p in parts]),
+        "masses": np.concatenate([p["masses"] for p in parts]),
+        "cell": np.concatenate([p["cell"] for p in parts]),
+        "pbc": parts[0]["pbc"],
+        "atomic_numbers": np.concatenate([p["atomic_numbers"] for p in parts]),
+        "system_idx": np.concatenate([np.full(off[k + 1] - off[k], k, dtype=np.int64)
+                                      for k in range(len(parts))]),
+    }
+
+
+def test_vlist_batch_with_a_large_system_rebins_the_batch():
+    """Systems of at most 4096 atoms are rebinned one block each; a batch with a
+    larger one takes the batch-wide binning.  Both give the per-call pairs."""
+    from tsb import models
+    from tsb.state import state_from_arrays
+
+    st = state_from_arrays(_argon_batch([(3, 3, 3), (11, 11, 10), (4, 3, 3)]), device="cuda")
+    assert st.n_atoms - 108 - 144 > 4096
+    mk = lambda: models.LennardJonesModel(sigma=3.405, epsilon=0.0104, cutoff=8.5,  # noqa
+                                          compute_stress=True, precision="fp64")
+    vm, ref = models.VerletListModel(mk(), skin=1.0), mk()
+    _cmp(vm(st), ref(st), 1e-10)
+    assert vm.max_system_atoms > 4096
+    g = torch.Generator(device="cuda").manual_seed(3)
+    st.positions = (st.positions + 0.4 * torch.randn(st.positions.shape, device="cuda",
+                                                     dtype=st.dtype, generator=g)).contiguous()
+    _cmp(vm(st), ref(st), 1e-10)
+    assert vm.n_builds == 2
+
+
+def test_vlist_understated_max_system_atoms_is_reported():
+    """The per-system binning reports a system above its size limit (and leaves it
+    unsearched) instead of overrunning its shared-memory tables."""
+    from tsb import models
+    from tsb.state import state_from_arrays
+
+    st = state_from_arrays(_argon_batch([(3, 3, 3), (11, 11, 10)]), device="cuda")
+    mk = lambda: models.LennardJonesModel(sigma=3.405, epsilon=0.0104, cutoff=8.5,  # noqa
+                                          compute_stress=True, precision="fp64")
+    vm, ref = models.VerletListModel(mk(), skin=1.0), mk()
+    vm._ensure(st, st.positions, st.cell.mT.contiguous())
+    vm.max_system_atoms = 200
+    with pytest.raises(RuntimeError):
+        vm(st)
+    vm._key = None  # re-derive the sizes: the batch-wide path
+    _cmp(vm(st), ref(st), 1e-10)

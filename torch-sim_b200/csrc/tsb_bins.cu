@@ -47,7 +47,8 @@ __device__ inline int64_t block_excl_scan(int64_t v, int64_t *total) {
   return r;
 }
 
-__global__ void k_scan_tiles(const int32_t *in, int64_t *out, int64_t n, int64_t *sums) {
+__global__ void k_scan_tiles(const int32_t *in, int64_t *out, int64_t n, int64_t *sums,
+                             int64_t *total) {
   __shared__ int64_t tot;
   int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
   int64_t v[kScanItems];
@@ -63,7 +64,10 @@ __global__ void k_scan_tiles(const int32_t *in, int64_t *out, int64_t n, int64_t
     if (base + k < n) out[base + k] = pre;
     pre += v[k];
   }
-  if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+  if (threadIdx.x == 0) {
+    sums[blockIdx.x] = tot;
+    if (total) *total = tot;  // single tile: the scan is complete
+  }
 }
 
 __global__ void k_scan_sums(int64_t *sums, int64_t nb, int64_t *out_total) {
@@ -91,9 +95,13 @@ int exclusive_scan(const int32_t *in, int64_t *out, int64_t n, int64_t *tmp,
                    cudaStream_t st) {
   int64_t tiles = (n + kScanTile - 1) / kScanTile;
   if (tiles < 1) tiles = 1;
-  k_scan_tiles<<<(unsigned)tiles, kBlock, 0, st>>>(in, out, n, tmp);
-  k_scan_sums<<<1, kBlock, 0, st>>>(tmp, tiles, out + n);
-  k_scan_add<<<grid_for(n), kBlock, 0, st>>>(out, n, tmp);
+  if (tiles == 1) {
+    k_scan_tiles<<<1, kBlock, 0, st>>>(in, out, n, tmp, out + n);
+  } else {
+    k_scan_tiles<<<(unsigned)tiles, kBlock, 0, st>>>(in, out, n, tmp, nullptr);
+    k_scan_sums<<<1, kBlock, 0, st>>>(tmp, tiles, out + n);
+    k_scan_add<<<grid_for(n), kBlock, 0, st>>>(out, n, tmp);
+  }
   TSB_CHECK_LAUNCH();
   return TSB_OK;
 }
@@ -130,11 +138,8 @@ __device__ inline void inv3(const double *a, double *r) {
 }
 
 template <class P>
-__global__ void k_geom_setup(const P *cell_row, const uint8_t *pbc, int64_t ns,
-                             double cutoff, const int64_t *lo, const int64_t *hi,
-                             SysGeom *g) {
-  int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= ns) return;
+__device__ SysGeom geom_setup_one(const P *cell_row, const uint8_t *pbc, int64_t s,
+                                  double cutoff, const int64_t *lo, const int64_t *hi) {
   SysGeom G;
   for (int k = 0; k < 9; ++k) G.cell[k] = (double)cell_row[s * 9 + k];
   double d = det3(G.cell);
@@ -165,7 +170,16 @@ __global__ void k_geom_setup(const P *cell_row, const uint8_t *pbc, int64_t ns,
   G.count = (int32_t)(hi[s] - lo[s]);
   G.bin_base = 0;
   G.nbins = 1;
-  g[s] = G;
+  return G;
+}
+
+template <class P>
+__global__ void k_geom_setup(const P *cell_row, const uint8_t *pbc, int64_t ns,
+                             double cutoff, const int64_t *lo, const int64_t *hi,
+                             SysGeom *g) {
+  int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  g[s] = geom_setup_one<P>(cell_row, pbc, s, cutoff, lo, hi);
 }
 
 __device__ inline void frame_u(const SysGeom &G, double x, double y, double z, double *u) {
@@ -174,12 +188,11 @@ __device__ inline void frame_u(const SysGeom &G, double x, double y, double z, d
   u[2] = G.T[6] * x + G.T[7] * y + G.T[8] * z;
 }
 
-// One block per system: extents of non-periodic axes, then the bin grid.
+// Extents of non-periodic axes, then the bin grid of one system; called by
+// every thread of a block, thread 0 writes the grid into G.
 template <class P>
-__global__ void k_geom_bins(const P *pos, SysGeom *g, int32_t *sys_nbins) {
+__device__ void geom_bins_block(const P *pos, SysGeom &G) {
   __shared__ double smin[3][kBlock / 32], smax[3][kBlock / 32];
-  const int s = blockIdx.x;
-  SysGeom &G = g[s];
   double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
   bool need = !(G.per[0] && G.per[1] && G.per[2]);
   if (need) {
@@ -237,7 +250,15 @@ __global__ void k_geom_bins(const P *pos, SysGeom *g, int32_t *sys_nbins) {
     G.scale[k] = nbd[k] / len[k];
   }
   G.nbins = G.nb[0] * G.nb[1] * G.nb[2];
-  sys_nbins[s] = G.nbins;
+}
+
+
+// One block per system: extents of non-periodic axes, then the bin grid.
+template <class P>
+__global__ void k_geom_bins(const P *pos, SysGeom *g, int32_t *sys_nbins) {
+  const int s = blockIdx.x;
+  geom_bins_block<P>(pos, g[s]);
+  if (threadIdx.x == 0) sys_nbins[s] = g[s].nbins;
 }
 
 __global__ void k_set_binbase(SysGeom *g, const int64_t *off, int64_t ns) {
@@ -245,20 +266,14 @@ __global__ void k_set_binbase(SysGeom *g, const int64_t *off, int64_t ns) {
   if (s < ns) g[s].bin_base = (int32_t)off[s];
 }
 
-template <class P>
-__global__ void k_bin_assign(const P *pos, const SysGeom *g, const int32_t *sys_of,
-                             int64_t n, int32_t *wrap, int32_t *bin_of,
-                             int32_t *bin_count, double4 *wpos) {
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const SysGeom &G = g[sys_of[i]];
-  double r[3] = {(double)pos[3 * i], (double)pos[3 * i + 1], (double)pos[3 * i + 2]};
+// bin of one atom: integer wrap W on periodic axes, wrapped position w, bin
+// coordinates c (clamped into the grid)
+__device__ inline void bin_atom(const SysGeom &G, const double *r, int *W, int *c, double *w) {
   double u[3];
   frame_u(G, r[0], r[1], r[2], u);
-  int W[3] = {0, 0, 0};
-  int c[3];
   for (int k = 0; k < 3; ++k) {
     double uk = u[k];
+    W[k] = 0;
     if (G.per[k]) {
       double f = floor(uk);
       f = isfinite(f) ? fmin(fmax(f, -1e9), 1e9) : 0.0;
@@ -271,9 +286,21 @@ __global__ void k_bin_assign(const P *pos, const SysGeom *g, const int32_t *sys_
     c[k] = (int)cc;
   }
   // wrapped position w = r - W @ cell
-  double w[3];
   for (int m = 0; m < 3; ++m)
     w[m] = r[m] - (W[0] * G.cell[m] + W[1] * G.cell[3 + m] + W[2] * G.cell[6 + m]);
+}
+
+template <class P>
+__global__ void k_bin_assign(const P *pos, const SysGeom *g, const int32_t *sys_of,
+                             int64_t n, int32_t *wrap, int32_t *bin_of,
+                             int32_t *bin_count, double4 *wpos) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const SysGeom &G = g[sys_of[i]];
+  double r[3] = {(double)pos[3 * i], (double)pos[3 * i + 1], (double)pos[3 * i + 2]};
+  int W[3], c[3];
+  double w[3];
+  bin_atom(G, r, W, c, w);
   int b = G.bin_base + (c[0] * G.nb[1] + c[1]) * G.nb[2] + c[2];
   wrap[3 * i] = W[0];
   wrap[3 * i + 1] = W[1];
@@ -316,6 +343,129 @@ __global__ void k_bin_sort(const int64_t *bin_start, int64_t nbins_total, int32_
     spos[p] = w;
   }
 }
+
+// Per-system binning for batches of small systems (at most kSysBinMaxAtoms
+// atoms each): one block per selected system does the geometry, the bin
+// assignment, the counting sort (histogram and scan in shared memory) and the
+// gather into bin order, so one launch replaces the batch-wide passes and
+// systems not selected keep their bins untouched.  Bin regions are static
+// (system s owns bins [2 lo_s + s, 2 (lo_s + count_s) + s], room for the
+// 2 count_s + 1 bins and the sentinel its grid may use), so no scan over the
+// batch is needed.  Order inside a bin is ascending atom index, as
+// k_bin_sort gives: atoms are placed a block-sized chunk at a time, one warp
+// after another, each lane taking its slot after the lower lanes with the same
+// bin.
+template <class P>
+__global__ void __launch_bounds__(kBlock)
+    k_bins_sys(const P *pos, const P *cell_row, const uint8_t *pbc, double cutoff,
+               int32_t *only, const int32_t *species, BinData b, int32_t *err) {
+  __shared__ int32_t cur[2 * kSysBinMaxAtoms + 2];
+  __shared__ int16_t lbin[kSysBinMaxAtoms];
+  __shared__ int64_t chunk_tot;
+  const int64_t s = blockIdx.x;
+  if (only && !only[s]) return;
+  SysGeom &G = b.geom[s];
+  if (threadIdx.x == 0) G = geom_setup_one<P>(cell_row, pbc, s, cutoff, b.sys_lo, b.sys_hi);
+  __syncthreads();
+  const int count = G.count;
+  if (count == 0) return;
+  if (count > kSysBinMaxAtoms) {
+    // not for this path: deselected (no search runs over it), with an empty
+    // one-bin grid, and reported
+    if (threadIdx.x == 0) {
+      G.bin_base = (int32_t)(2 * G.start + s);
+      b.bin_start[G.bin_base] = G.start;
+      b.bin_start[G.bin_base + 1] = G.start;
+      if (only) only[s] = 0;
+      atomicMax(err, kSysBinErr);
+    }
+    return;
+  }
+  geom_bins_block<P>(pos, G);
+  __syncthreads();
+  const int64_t start = G.start;
+  const int nbins = G.nbins;  // <= 2 count
+  const int64_t base = 2 * start + s;
+  if (threadIdx.x == 0) G.bin_base = (int32_t)base;
+  for (int k = threadIdx.x; k <= nbins; k += blockDim.x) cur[k] = 0;
+  __syncthreads();
+  for (int a = threadIdx.x; a < count; a += blockDim.x) {
+    const int64_t i = start + a;
+    const double r[3] = {(double)pos[3 * i], (double)pos[3 * i + 1], (double)pos[3 * i + 2]};
+    int W[3], c[3];
+    double w[3];
+    bin_atom(G, r, W, c, w);
+    const int lb = (c[0] * G.nb[1] + c[1]) * G.nb[2] + c[2];
+    b.wrap[3 * i] = W[0];
+    b.wrap[3 * i + 1] = W[1];
+    b.wrap[3 * i + 2] = W[2];
+    b.wpos[i] = make_double4(w[0], w[1], w[2], 0.0);
+    lbin[a] = (int16_t)lb;
+    atomicAdd(&cur[lb], 1);
+  }
+  __syncthreads();
+  // exclusive scan of cur[0..nbins] (cur[nbins] = 0 becomes the total), each
+  // thread a contiguous run of entries
+  const int per = (nbins + 1 + blockDim.x - 1) / blockDim.x;
+  const int k0 = threadIdx.x * per, k1 = min(k0 + per, nbins + 1);
+  int64_t run = 0;
+  for (int k = k0; k < k1; ++k) run += cur[k];
+  int64_t pre = block_excl_scan(run, &chunk_tot);
+  for (int k = k0; k < k1; ++k) {
+    const int v = cur[k];
+    cur[k] = (int32_t)pre;
+    b.bin_start[base + k] = start + pre;
+    pre += v;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  for (int c0 = 0; c0 < count; c0 += blockDim.x) {
+    const int a = c0 + threadIdx.x;
+    const int lb = a < count ? (int)lbin[a] : -1;
+    for (int wv = 0; wv < (int)(blockDim.x >> 5); ++wv) {
+      if (warp == wv) {
+        const unsigned peers = __match_any_sync(0xffffffffu, lb);
+        const int rank = __popc(peers & lt);
+        const int at = lb >= 0 ? cur[lb] : 0;
+        __syncwarp();
+        if (lb >= 0) {
+          if (rank == 0) cur[lb] = at + __popc(peers);
+          const int64_t slot = start + at + rank, i = start + a;
+          double4 w = b.wpos[i];
+          const unsigned long long hi =
+              species ? (unsigned long long)(uint32_t)species[i] : 0ull;
+          w.w = __longlong_as_double((long long)((hi << 32) | (uint32_t)i));
+          b.spos[slot] = w;
+          b.sidx[slot] = (int32_t)i;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+template <class P>
+int prepare_bins_sys(const P *positions, const P *cell_row, const uint8_t *pbc,
+                     const int64_t *system_idx, int64_t n, int64_t ns, double cutoff,
+                     BinData &b, cudaStream_t st, const int32_t *species, int32_t *only,
+                     int32_t *err) {
+  cudaMemsetAsync(b.sys_lo, 0, sizeof(int64_t) * ns, st);
+  cudaMemsetAsync(b.sys_hi, 0, sizeof(int64_t) * ns, st);
+  if (n > 0) k_sys_bounds<<<grid_for(n), kBlock, 0, st>>>(system_idx, n, b.sys_lo, b.sys_hi,
+                                                         b.sys_of);
+  k_bins_sys<P><<<(unsigned)ns, kBlock, 0, st>>>(positions, cell_row, pbc, cutoff, only, species,
+                                                 b, err);
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
+
+template int prepare_bins_sys<float>(const float *, const float *, const uint8_t *,
+                                     const int64_t *, int64_t, int64_t, double, BinData &,
+                                     cudaStream_t, const int32_t *, int32_t *, int32_t *);
+template int prepare_bins_sys<double>(const double *, const double *, const uint8_t *,
+                                      const int64_t *, int64_t, int64_t, double, BinData &,
+                                      cudaStream_t, const int32_t *, int32_t *, int32_t *);
 
 int64_t bin_capacity(int64_t n_atoms, int64_t n_systems) {
   return 2 * n_atoms + n_systems + 1;

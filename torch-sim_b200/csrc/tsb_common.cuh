@@ -125,4 +125,19 @@ int prepare_bins(const P *positions, const P *cell_row, const uint8_t *pbc,
                  double search_cutoff, BinData &b, cudaStream_t st,
                  const int32_t *species = nullptr);
 
+// Largest system the per-system binning takes, and the status it reports
+// (atomicMax into *err) for a larger one.
+constexpr int kSysBinMaxAtoms = 4096;
+constexpr int32_t kSysBinErr = 1 << 29;
+
+// Per-system binning of the systems with only[s] != 0 (all when only is null),
+// each of at most kSysBinMaxAtoms atoms, into the same BinData layout (static
+// bin regions: bin_base = 2 sys_lo + s).  A larger selected system gets an empty
+// grid, is deselected (only[s] = 0) and raises *err to kSysBinErr.
+template <class P>
+int prepare_bins_sys(const P *positions, const P *cell_row, const uint8_t *pbc,
+                     const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
+                     double search_cutoff, BinData &b, cudaStream_t st, const int32_t *species,
+                     int32_t *only, int32_t *err);
+
 }  // namespace tsb

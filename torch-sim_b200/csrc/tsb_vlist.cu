@@ -576,11 +576,16 @@ static int vl_check(const P *pos, const P *cell, const int64_t *sys, const uint8
 template <class P>
 static int vl_build(const P *pos, const P *cell, const uint8_t *pbc, const int64_t *sys,
                     const int32_t *species, int64_t n, int64_t ns, double cutoff, double skin,
-                    uint32_t *list, int32_t *counts, int max_nb, int32_t *flags, VlWork &w,
-                    cudaStream_t st) {
+                    uint32_t *list, int32_t *counts, int max_nb, int64_t max_sys,
+                    int32_t *flags, VlWork &w, cudaStream_t st) {
   cudaMemsetAsync(flags + 1, 0, sizeof(int32_t), st);
   const double rcs = cutoff + skin;
-  TSB_TRY(prepare_bins<P>(pos, cell, pbc, sys, n, ns, rcs, w.b, st, species));
+  // batches of small systems rebin only the expired systems, one block each
+  if (max_sys > 0 && max_sys <= kSysBinMaxAtoms)
+    TSB_TRY(prepare_bins_sys<P>(pos, cell, pbc, sys, n, ns, rcs, w.b, st, species, w.sys_exp,
+                                flags + 1));
+  else
+    TSB_TRY(prepare_bins<P>(pos, cell, pbc, sys, n, ns, rcs, w.b, st, species));
   k_vl_exp_counts<<<grid_for(ns), kBlock, 0, st>>>(w.sys_exp, w.b.sys_lo, w.b.sys_hi, ns,
                                                    w.ecount);
   TSB_TRY(exclusive_scan(w.ecount, w.eoff, ns, w.b.scan_tmp, st));
@@ -695,8 +700,8 @@ extern "C" int tsb_vlist_build(const void *positions, const void *cell_row, cons
                                const int64_t *system_idx, const int32_t *species,
                                int64_t n_atoms, int64_t n_systems, int dtype, double cutoff,
                                double skin, uint32_t *list, int32_t *counts, int max_neighbors,
-                               int32_t *flags, void *workspace, size_t workspace_bytes,
-                               void *stream) {
+                               int64_t max_system_atoms, int32_t *flags, void *workspace,
+                               size_t workspace_bytes, void *stream) {
   if (n_atoms < 1 || n_systems < 1 || !positions || !cell_row || !pbc || !system_idx ||
       !list || !counts || !flags || max_neighbors < 1 || !(cutoff > 0.0) || !(skin >= 0.0))
     return TSB_ERR_INVALID_ARG;
@@ -709,11 +714,11 @@ extern "C" int tsb_vlist_build(const void *positions, const void *cell_row, cons
   if (dtype == TSB_F64)
     return vl_build<double>((const double *)positions, (const double *)cell_row, pbc,
                             system_idx, species, n_atoms, n_systems, cutoff, skin, list,
-                            counts, max_neighbors, flags, w, st);
+                            counts, max_neighbors, max_system_atoms, flags, w, st);
   if (dtype == TSB_F32)
     return vl_build<float>((const float *)positions, (const float *)cell_row, pbc, system_idx,
                            species, n_atoms, n_systems, cutoff, skin, list, counts,
-                           max_neighbors, flags, w, st);
+                           max_neighbors, max_system_atoms, flags, w, st);
   return TSB_ERR_INVALID_ARG;
 }
 

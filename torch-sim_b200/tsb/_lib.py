@@ -87,7 +87,7 @@ PROTOTYPES = {
     "tsb_vlist_check": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _int, _dbl, _dbl, _vp, _vp, _sz,
                                _vp]),
     "tsb_vlist_build": (_int, [_vp, _vp, _vp, _vp, _vp, _i64, _i64, _int, _dbl, _dbl, _vp, _vp,
-                               _int, _vp, _vp, _sz, _vp]),
+                               _int, _i64, _vp, _vp, _sz, _vp]),
     "tsb_vlist_forces": (_int, [_int, _vp, _int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64,
                                 _int, _dbl, _int, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
     "tsb_fire_workspace_size": (_sz, [_i64]),

@@ -59,6 +59,7 @@ class VerletListModel(ModelInterface):
         dev = pos.device
         rcs = self.model.cutoff + self.skin
         counts = torch.bincount(sysi, minlength=ns).double()
+        self.max_system_atoms = int(counts.max()) if ns else 0
         vol = torch.linalg.det(cell_row.double()).abs().clamp_min(1e-30)
         dens = float((counts / vol).max())
         est = int(4.19 * rcs ** 3 * dens * 1.35) + 16
@@ -89,8 +90,8 @@ class VerletListModel(ModelInterface):
                 return
             L.call("tsb_vlist_build", L.ptr(pos), L.ptr(cell_row), L.ptr(pbc), L.ptr(sysi),
                    L.ptr(species), n, ns, dt, cutoff, self.skin, L.ptr(self.list),
-                   L.ptr(self.counts), self.cap, L.ptr(self.flags), L.ptr(self.ws),
-                   self.ws.numel(), L.stream_ptr(dev))
+                   L.ptr(self.counts), self.cap, self.max_system_atoms, L.ptr(self.flags),
+                   L.ptr(self.ws), self.ws.numel(), L.stream_ptr(dev))
             self.n_builds += 1
             st = int(self.flags[1].item())
             if st == 0:
@@ -98,6 +99,9 @@ class VerletListModel(ModelInterface):
             if st >= (1 << 30):
                 raise ValueError("VerletListModel needs every periodic cell width >= "
                                  "cutoff + skin")
+            if st == (1 << 29):
+                raise RuntimeError("tsb_vlist_build: a system is larger than "
+                                   "max_system_atoms")
             # a list overflowed: regrow and rebuild every system
             self.cap = int(st * 1.2) + 8
             self.list = torch.empty(self.cap * n, dtype=torch.int32, device=dev)
@@ -190,6 +194,9 @@ class VerletListModel(ModelInterface):
             if st >= (1 << 30):
                 raise ValueError("VerletListModel needs every periodic cell width >= "
                                  "cutoff + skin")
+            if st == (1 << 29):
+                raise RuntimeError("tsb_vlist_build: a system is larger than "
+                                   "max_system_atoms")
             self.s_cap = int(st * 1.2) + 8
             self.s_list = torch.empty(self.s_cap * state.n_atoms, dtype=torch.int32,
                                       device=state.device)
