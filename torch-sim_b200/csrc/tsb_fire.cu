@@ -92,29 +92,38 @@ __device__ inline void store_m3(P *p, const M3 &m) {
   for (int k = 0; k < 9; ++k) p[k] = (P)m.a[k];
 }
 
-// count atoms whose velocity has no NaN (the ASE step skips mixing on the
-// first step, when every velocity of the batch is NaN: fire.py:303-310)
+// does any atom have a velocity without NaN?  (the ASE step skips mixing on the
+// first step, when every velocity of the batch is NaN: fire.py:303-310)  Warps
+// stride over the atoms and stop as soon as one of them has found one, so the
+// usual case (finite velocities) costs one load per warp.
 template <class P>
-__global__ void k_count_finite_v(const P *v, int64_t n, int32_t *count) {
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  bool fin = false;
-  if (i < n) fin = !(isnan((double)v[3 * i]) || isnan((double)v[3 * i + 1]) ||
-                     isnan((double)v[3 * i + 2]));
-  unsigned b = __ballot_sync(0xffffffffu, fin);
-  if ((threadIdx.x & 31) == 0 && b) atomicAdd(count, __popc(b));
+__global__ void k_any_finite_v(const P *v, int64_t n, int32_t *found) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i - threadIdx.x % 32 < n;
+       i += stride) {
+    if (*(volatile int32_t *)found) return;
+    const bool fin = i < n && !(isnan((double)v[3 * i]) || isnan((double)v[3 * i + 1]) ||
+                                isnan((double)v[3 * i + 2]));
+    if (__any_sync(0xffffffffu, fin)) {
+      if ((threadIdx.x & 31) == 0) atomicExch(found, 1);
+      return;
+    }
+  }
 }
 
 // ASE-FIRE step in three launches: (a) one block per system for the power,
 // mixing and velocity step with its FP64 sums, (b) one thread per system for the
 // cell velocity, the max_step factor and the Frechet cell update (3x3 algebra,
 // kept out of (a) so that the per-system blocks stay light on registers), (c) one
-// thread per atom for the position update.
+// thread per atom for the position update.  (a) reads the system's atoms twice:
+// once for the power and norms (velocities with NaN read as 0), once for the
+// mixing, the Euler step and the step-length sum.
 template <class P>
 __global__ void __launch_bounds__(kFireThreads) k_fire_ase_vel(FireArgs<P> A,
-                                                               const int32_t *n_finite,
+                                                               const int32_t *any_finite,
                                                                double *scr) {
   __shared__ double sh[100];
-  __shared__ double s_alpha, s_vs, s_fs;
+  __shared__ double s_alpha, s_vs, s_fs, s_dt;
   __shared__ int s_pos;
   const int s = blockIdx.x;
   if (A.active && !A.active[s]) return;
@@ -122,20 +131,17 @@ __global__ void __launch_bounds__(kFireThreads) k_fire_ase_vel(FireArgs<P> A,
   const int tid = threadIdx.x;
   const bool cellf = A.cell_filter != 0;
   const FireHyper &h = A.h;
-  // 1. NaN velocities -> 0 (nan_to_num_, fire.py:304-307)
-  for (int64_t i = a0 + tid; i < a1; i += blockDim.x)
-    for (int k = 0; k < 3; ++k)
-      if (isnan((double)A.v[3 * i + k])) A.v[3 * i + k] = (P)0;
-  if (tid == 0 && cellf)
-    for (int k = 0; k < 9; ++k)
-      if (isnan((double)A.cell_vel[9 * s + k])) A.cell_vel[9 * s + k] = (P)0;
-  __syncthreads();
-  const bool all_nan = (*n_finite == 0);
+  // NaN velocities read as 0 (nan_to_num_, fire.py:304-307)
+  auto vel = [&](int64_t j) {
+    const double x = (double)A.v[j];
+    return isnan(x) ? 0.0 : x;
+  };
+  const bool all_nan = (*any_finite == 0);
   if (!all_nan) {
     double pw = 0, vv = 0, ff = 0;
     for (int64_t i = a0 + tid; i < a1; i += blockDim.x)
       for (int k = 0; k < 3; ++k) {
-        const double fk = (double)A.f[3 * i + k], vk = (double)A.v[3 * i + k];
+        const double fk = (double)A.f[3 * i + k], vk = vel(3 * i + k);
         pw += fk * vk;
         vv += vk * vk;
         ff += fk * fk;
@@ -144,6 +150,7 @@ __global__ void __launch_bounds__(kFireThreads) k_fire_ase_vel(FireArgs<P> A,
     if (tid == 0) {
       if (cellf)
         for (int k = 0; k < 9; ++k) {
+          if (isnan((double)A.cell_vel[9 * s + k])) A.cell_vel[9 * s + k] = (P)0;
           const double cf = (double)A.cell_force[9 * s + k], cv = (double)A.cell_vel[9 * s + k];
           pw += cf * cv;
           vv += cv * cv;
@@ -178,23 +185,28 @@ __global__ void __launch_bounds__(kFireThreads) k_fire_ase_vel(FireArgs<P> A,
       s_alpha = (double)(P)alpha;
       s_vs = vsc;
       s_fs = fsc;
+      s_dt = (double)(P)dt;
     }
-    __syncthreads();
-    const double al = s_alpha, ratio = s_vs / (s_fs + h.eps);
-    const bool pos = s_pos;
-    for (int64_t i = a0 + tid; i < a1; i += blockDim.x)
-      for (int k = 0; k < 3; ++k) {
-        const double vk = (double)A.v[3 * i + k];
-        const double mix = (double)A.f[3 * i + k] * ratio;
-        A.v[3 * i + k] = (P)(pos ? (1.0 - al) * vk + al * mix : 0.0);
-      }
+  } else if (tid == 0) {
+    if (cellf)
+      for (int k = 0; k < 9; ++k)
+        if (isnan((double)A.cell_vel[9 * s + k])) A.cell_vel[9 * s + k] = (P)0;
+    s_dt = (double)A.dt[s];
   }
-  // 2. Euler step (no mass, ASE) and the max_step clamp (fire.py:369-391)
-  const double dts = (double)A.dt[s];
+  __syncthreads();
+  // mixing (fire.py:348-367), then the Euler step (no mass, ASE) and the sum for
+  // the max_step clamp (fire.py:369-391)
+  const double al = all_nan ? 0.0 : s_alpha;
+  const double ratio = all_nan ? 0.0 : s_vs / (s_fs + h.eps);
+  const bool pos = all_nan ? false : s_pos;
+  const double dts = s_dt;
   double drs = 0, dummy1 = 0, dummy2 = 0;
   for (int64_t i = a0 + tid; i < a1; i += blockDim.x)
     for (int k = 0; k < 3; ++k) {
-      const double vk = (double)(P)((double)A.v[3 * i + k] + (double)A.f[3 * i + k] * dts);
+      const double fk = (double)A.f[3 * i + k];
+      double vk = vel(3 * i + k);
+      if (!all_nan) vk = (double)(P)(pos ? (1.0 - al) * vk + al * (fk * ratio) : 0.0);
+      vk = (double)(P)(vk + fk * dts);
       A.v[3 * i + k] = (P)vk;
       const double d = (double)(P)(vk * dts);
       drs += d * d;
@@ -479,6 +491,15 @@ static void carve_fire(Carver &c, FireWork &w, int64_t ns) {
   w.scr = c.take<double>(kFireScr * ns);
 }
 
+// grid of the finite-velocity probe: up to 4 blocks per SM
+static unsigned fire_probe_grid(int64_t n) {
+  int dev = 0, n_sm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t g = (n + kBlock - 1) / kBlock;
+  return (unsigned)(g < 4 * (int64_t)n_sm ? (g > 0 ? g : 1) : 4 * (int64_t)n_sm);
+}
+
 static int prep_bounds(FireWork &w, const int64_t *sys, int64_t n, int64_t ns,
                        cudaStream_t st) {
   cudaMemsetAsync(w.lo, 0, sizeof(int64_t) * ns, st);
@@ -520,8 +541,8 @@ static int fire_call(int which, int cell_filter, void *positions, void *velociti
                 w.lo, w.hi, h};
   if (which == 0) {
     if (n_atoms > 0)
-      k_count_finite_v<P><<<grid_for(n_atoms), kBlock, 0, st>>>((const P *)velocities, n_atoms,
-                                                                 w.counter);
+      k_any_finite_v<P><<<fire_probe_grid(n_atoms), kBlock, 0, st>>>((const P *)velocities,
+                                                                      n_atoms, w.counter);
     k_fire_ase_vel<P><<<(unsigned)n_systems, kFireThreads, 0, st>>>(A, w.counter, w.scr);
     k_fire_ase_cell<P><<<grid_for(n_systems, 128), 128, 0, st>>>(A, n_systems, w.scr);
     if (n_atoms > 0)
