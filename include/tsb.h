@@ -100,7 +100,9 @@ int tsb_nl_build(const void *positions, const void *cell_row, const uint8_t *pbc
  * stresses [N,3,3] are written in `dtype`; outputs not requested by
  * `out_flags` may be NULL.  `sys_active` [S] uint8 (optional): systems with 0
  * are skipped and their outputs left untouched (converged systems of a batched
- * relaxation). */
+ * relaxation).  `max_system_atoms`: the largest system's atom count (0 =
+ * unknown); at most 4096 bins each system in one block (one launch), larger or
+ * unknown bins the whole batch in passes; either is correct. */
 size_t tsb_pair_workspace_size(int64_t n_atoms, int64_t n_systems);
 int tsb_pair_forward(int potential, const double *table, int n_species,
                      const int32_t *species, const void *positions,
@@ -108,7 +110,7 @@ int tsb_pair_forward(int potential, const double *table, int n_species,
                      const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
                      int dtype, double cutoff, int out_flags, void *energy,
                      void *forces, void *stress, void *energies, void *stresses,
-                     const uint8_t *sys_active, void *workspace,
+                     const uint8_t *sys_active, int64_t max_system_atoms, void *workspace,
                      size_t workspace_bytes, void *stream);
 
 /* ---- integrator steps (elementwise, per-system parameters) ---------------
@@ -285,10 +287,10 @@ int tsb_npt_crescale_tri(void *positions, void *momenta, const void *masses,
  *   (list[k * N + slot] = slot of j << 5 | image code, counts [N] by slot).
  *   max_system_atoms = the largest system's atom count (0: unknown); when it is
  *   at most 4096 only the expired systems are rebinned, one block each, else the
- *   whole batch is.  flags[1] = 1 << 30 when a periodic cell is narrower than
- *   cutoff + skin, 1 << 29 when a system exceeds a max_system_atoms of at most
- *   4096, else the largest neighbour count when it exceeded max_neighbors (regrow,
- *   reset and build again), else 0.
+ *   whole batch is (the hint selects the faster way; either is correct).
+ *   flags[1] = 1 << 30 when a periodic cell is narrower than cutoff + skin, else
+ *   the largest neighbour count when it exceeded max_neighbors (regrow, reset and
+ *   build again), else 0.
  * tsb_vlist_forces: energy [S], forces [N,3], stress [S,3,3], per-atom energies
  *   [N] and stresses [N,3,3] per out_flags (TSB_MATH_FP64: FP64 pair function),
  *   for the systems with sys_active != 0 (NULL: all).  LJ, Morse, soft sphere. */
@@ -321,22 +323,24 @@ int tsb_vlist_forces(int potential, const double *table, int n_species, const in
  * tsb_rdf_hist: hist [S, n_bins] = sum over pairs r < r_max of
  *   exp(-(r - c_b)^2 / (2 width^2)), c_b = (b + 1/2) r_max / n_bins.
  * tsb_rdf_hist_grad: grad_positions [N,3] = d(sum_sb dl_dhist_sb hist_sb)/dq.
- * per_atom for tsb_adjoint_workspace_size: 2*ns*ns (hvp) or n_bins (rdf). */
+ * per_atom for tsb_adjoint_workspace_size: 2*ns*ns (hvp) or n_bins (rdf).
+ * max_system_atoms: as for tsb_pair_forward. */
 size_t tsb_adjoint_workspace_size(int64_t n_atoms, int64_t n_systems, int64_t per_atom);
 int tsb_lj_hvp(const double *table, int n_species, const int32_t *species,
                const double *positions, const double *cell_row, const uint8_t *pbc,
                const int64_t *system_idx, int64_t n_atoms, int64_t n_systems, double cutoff,
                const double *v, double coef, double *lam_q, double *grad_params,
-               void *workspace, size_t workspace_bytes, void *stream);
+               int64_t max_system_atoms, void *workspace, size_t workspace_bytes,
+               void *stream);
 int tsb_rdf_hist(const double *positions, const double *cell_row, const uint8_t *pbc,
                  const int64_t *system_idx, int64_t n_atoms, int64_t n_systems, double r_max,
-                 int n_bins, double width, double *hist, void *workspace,
-                 size_t workspace_bytes, void *stream);
+                 int n_bins, double width, double *hist, int64_t max_system_atoms,
+                 void *workspace, size_t workspace_bytes, void *stream);
 int tsb_rdf_hist_grad(const double *positions, const double *cell_row, const uint8_t *pbc,
                       const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
                       double r_max, int n_bins, double width, const double *dl_dhist,
-                      double *grad_positions, void *workspace, size_t workspace_bytes,
-                      void *stream);
+                      double *grad_positions, int64_t max_system_atoms, void *workspace,
+                      size_t workspace_bytes, void *stream);
 
 /* ---- FIRE + Frechet cell filter -----------------------------------------
  * Per-system state arrays (dtype): dt [S], alpha [S], n_pos [S] int32; cell,

@@ -67,3 +67,42 @@ def test_lj_hvp_warp_and_thread_kernels_agree():
     lb, gb = hvp(b, v[a.n_atoms:])
     assert _rel(torch.cat([la, lb]), lam_big) < 1e-10
     assert _rel(torch.cat([ga, gb]), g_big) < 1e-10
+
+
+def test_per_system_and_batch_wide_binning_agree_exactly(monkeypatch):
+    """Batches of systems of at most 4096 atoms are binned one block per system
+    (static bin regions); the batch-wide passes give the same bins and the same
+    in-bin order (ascending atom index), so forces, energies and stresses agree
+    bit for bit."""
+    from tsb import _lib as L
+    from tsb import adjoint, models, workloads
+    from tsb.state import state_from_arrays
+
+    d = workloads.copper_batch(64, 8, 512, seed=5, jitter=0.05)
+    st = state_from_arrays(d, device="cuda")
+    m = models.MorseModel(sigma=2.866, epsilon=0.3429, alpha=1.3588, cutoff=6.0,
+                          compute_stress=True, per_atom_energies=True)
+    per_sys = m(st)
+    assert L.max_system_atoms(st.system_idx, st.n_systems) <= 4096
+    monkeypatch.setattr(L, "max_system_atoms", lambda *_: 0)
+    batch = m(st)
+    for k in ("energy", "forces", "stress", "energies"):
+        assert torch.equal(per_sys[k], batch[k]), k
+    monkeypatch.undo()
+
+    d = workloads.argon_species_batch(40, (3, 3, 3), seed=1, jitter=0.05)
+    st = state_from_arrays(d, device="cuda")
+    table = adjoint.lj_table(*adjoint.argon_pair_params(perturb=0.05, seed=2))
+    v = torch.randn((st.n_atoms, 3), dtype=torch.float64, device="cuda",
+                    generator=torch.Generator(device="cuda").manual_seed(4))
+    out = []
+    for hint in (None, 0):
+        if hint is not None:
+            monkeypatch.setattr(L, "max_system_atoms", lambda *_: hint)
+        P = adjoint.make_problem(st, 1, 1.0)
+        lam = torch.zeros_like(v)
+        gp = torch.zeros((st.n_systems, 2, 2, 2), dtype=torch.float64, device="cuda")
+        adjoint._hvp(st.positions.contiguous(), table, v, 0.5, lam, gp, P)
+        out.append((lam, gp, adjoint.histogram(st.positions.contiguous(), P)))
+    for a, b in zip(*out):
+        assert torch.equal(a, b)

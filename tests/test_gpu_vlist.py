@@ -278,9 +278,10 @@ def test_vlist_batch_with_a_large_system_rebins_the_batch():
     assert vm.n_builds == 2
 
 
-def test_vlist_understated_max_system_atoms_is_reported():
-    """The per-system binning reports a system above its size limit (and leaves it
-    unsearched) instead of overrunning its shared-memory tables."""
+def test_vlist_understated_max_system_atoms_still_exact():
+    """The size hint only picks the binning: a system above the per-system
+    kernel's shared-memory limit under a small hint is binned through global
+    memory, with the same pairs."""
     from tsb import models
     from tsb.state import state_from_arrays
 
@@ -290,7 +291,4 @@ def test_vlist_understated_max_system_atoms_is_reported():
     vm, ref = models.VerletListModel(mk(), skin=1.0), mk()
     vm._ensure(st, st.positions, st.cell.mT.contiguous())
     vm.max_system_atoms = 200
-    with pytest.raises(RuntimeError):
-        vm(st)
-    vm._key = None  # re-derive the sizes: the batch-wide path
     _cmp(vm(st), ref(st), 1e-10)

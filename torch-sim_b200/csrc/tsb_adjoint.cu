@@ -207,8 +207,8 @@ extern "C" int tsb_lj_hvp(const double *table, int n_species, const int32_t *spe
                           const double *positions, const double *cell_row, const uint8_t *pbc,
                           const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
                           double cutoff, const double *v, double coef, double *lam_q,
-                          double *grad_params, void *workspace, size_t workspace_bytes,
-                          void *stream) {
+                          double *grad_params, int64_t max_system_atoms, void *workspace,
+                          size_t workspace_bytes, void *stream) {
   if (n_species < 1 || n_species > kAdjMaxSpecies || !table || (n_species > 1 && !species) ||
       n_atoms < 1 || n_systems < 1 || !positions || !cell_row || !pbc || !system_idx || !v ||
       !lam_q || !grad_params || !(cutoff > 0.0))
@@ -219,8 +219,8 @@ extern "C" int tsb_lj_hvp(const double *table, int n_species, const int32_t *spe
   carve_adj(c, w, n_atoms, n_systems, per_atom);
   if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
-  TSB_TRY(prepare_bins<double>(positions, cell_row, pbc, system_idx, n_atoms, n_systems, cutoff,
-                               w.b, st, species));
+  TSB_TRY(prepare_bins_any<double>(positions, cell_row, pbc, system_idx, n_atoms, n_systems,
+                                   cutoff, w.b, st, species, max_system_atoms));
   if (n_atoms <= kGroupSearchMaxAtoms)
     k_lj_hvp<kSearchGroup><<<grid_for(kSearchGroup * n_atoms, 128), 128, 0, st>>>(
         w.b, n_atoms, table, n_species, species, cutoff, v, coef, lam_q, w.part);
@@ -236,7 +236,8 @@ extern "C" int tsb_lj_hvp(const double *table, int n_species, const int32_t *spe
 extern "C" int tsb_rdf_hist(const double *positions, const double *cell_row, const uint8_t *pbc,
                             const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
                             double r_max, int n_bins, double width, double *hist,
-                            void *workspace, size_t workspace_bytes, void *stream) {
+                            int64_t max_system_atoms, void *workspace, size_t workspace_bytes,
+                            void *stream) {
   if (n_atoms < 1 || n_systems < 1 || !positions || !cell_row || !pbc || !system_idx || !hist ||
       n_bins < 1 || !(r_max > 0.0) || !(width > 0.0))
     return TSB_ERR_INVALID_ARG;
@@ -245,8 +246,8 @@ extern "C" int tsb_rdf_hist(const double *positions, const double *cell_row, con
   carve_adj(c, w, n_atoms, n_systems, n_bins);
   if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
-  TSB_TRY(prepare_bins<double>(positions, cell_row, pbc, system_idx, n_atoms, n_systems, r_max,
-                               w.b, st));
+  TSB_TRY(prepare_bins_any<double>(positions, cell_row, pbc, system_idx, n_atoms, n_systems,
+                                   r_max, w.b, st, nullptr, max_system_atoms));
   k_rdf_part<<<grid_for(n_atoms, 128), 128, 0, st>>>(w.b, n_atoms, r_max, n_bins, width, w.part);
   k_sum_parts<<<(unsigned)n_systems, 64, 0, st>>>(w.b.geom, w.part, n_bins, hist, 0);
   TSB_CHECK_LAUNCH();
@@ -257,7 +258,8 @@ extern "C" int tsb_rdf_hist_grad(const double *positions, const double *cell_row
                                  const uint8_t *pbc, const int64_t *system_idx, int64_t n_atoms,
                                  int64_t n_systems, double r_max, int n_bins, double width,
                                  const double *dl_dhist, double *grad_positions,
-                                 void *workspace, size_t workspace_bytes, void *stream) {
+                                 int64_t max_system_atoms, void *workspace,
+                                 size_t workspace_bytes, void *stream) {
   if (n_atoms < 1 || n_systems < 1 || !positions || !cell_row || !pbc || !system_idx ||
       !dl_dhist || !grad_positions || n_bins < 1 || !(r_max > 0.0) || !(width > 0.0))
     return TSB_ERR_INVALID_ARG;
@@ -266,8 +268,8 @@ extern "C" int tsb_rdf_hist_grad(const double *positions, const double *cell_row
   carve_adj(c, w, n_atoms, n_systems, n_bins);
   if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
-  TSB_TRY(prepare_bins<double>(positions, cell_row, pbc, system_idx, n_atoms, n_systems, r_max,
-                               w.b, st));
+  TSB_TRY(prepare_bins_any<double>(positions, cell_row, pbc, system_idx, n_atoms, n_systems,
+                                   r_max, w.b, st, nullptr, max_system_atoms));
   k_rdf_grad<<<grid_for(n_atoms, 128), 128, 0, st>>>(w.b, n_atoms, r_max, n_bins, width,
                                                      dl_dhist, grad_positions);
   TSB_CHECK_LAUNCH();

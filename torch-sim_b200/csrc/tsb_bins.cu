@@ -344,23 +344,24 @@ __global__ void k_bin_sort(const int64_t *bin_start, int64_t nbins_total, int32_
   }
 }
 
-// Per-system binning for batches of small systems (at most kSysBinMaxAtoms
-// atoms each): one block per selected system does the geometry, the bin
-// assignment, the counting sort (histogram and scan in shared memory) and the
+// Per-system binning for batches of small systems: one block per selected
+// system does the geometry, the bin assignment, the counting sort and the
 // gather into bin order, so one launch replaces the batch-wide passes and
 // systems not selected keep their bins untouched.  Bin regions are static
 // (system s owns bins [2 lo_s + s, 2 (lo_s + count_s) + s], room for the
 // 2 count_s + 1 bins and the sentinel its grid may use), so no scan over the
-// batch is needed.  Order inside a bin is ascending atom index, as
-// k_bin_sort gives: atoms are placed a block-sized chunk at a time, one warp
-// after another, each lane taking its slot after the lower lanes with the same
-// bin.
+// batch is needed.  Order inside a bin is ascending atom index, as k_bin_sort
+// gives: atoms are placed a block-sized chunk at a time, one warp after
+// another, each lane taking its slot after the lower lanes with the same bin.
+// Systems of at most kSysBinMaxAtoms atoms keep the histogram and the atoms'
+// bins in shared memory; a larger one uses its regions of bin_count / bin_of
+// (correct, but one block does all of its work).
 template <class P>
 __global__ void __launch_bounds__(kBlock)
     k_bins_sys(const P *pos, const P *cell_row, const uint8_t *pbc, double cutoff,
-               int32_t *only, const int32_t *species, BinData b, int32_t *err) {
-  __shared__ int32_t cur[2 * kSysBinMaxAtoms + 2];
-  __shared__ int16_t lbin[kSysBinMaxAtoms];
+               const int32_t *only, const int32_t *species, BinData b) {
+  __shared__ int32_t cur_s[2 * kSysBinMaxAtoms + 2];
+  __shared__ int16_t lbin_s[kSysBinMaxAtoms];
   __shared__ int64_t chunk_tot;
   const int64_t s = blockIdx.x;
   if (only && !only[s]) return;
@@ -369,23 +370,14 @@ __global__ void __launch_bounds__(kBlock)
   __syncthreads();
   const int count = G.count;
   if (count == 0) return;
-  if (count > kSysBinMaxAtoms) {
-    // not for this path: deselected (no search runs over it), with an empty
-    // one-bin grid, and reported
-    if (threadIdx.x == 0) {
-      G.bin_base = (int32_t)(2 * G.start + s);
-      b.bin_start[G.bin_base] = G.start;
-      b.bin_start[G.bin_base + 1] = G.start;
-      if (only) only[s] = 0;
-      atomicMax(err, kSysBinErr);
-    }
-    return;
-  }
   geom_bins_block<P>(pos, G);
   __syncthreads();
   const int64_t start = G.start;
   const int nbins = G.nbins;  // <= 2 count
   const int64_t base = 2 * start + s;
+  const bool small = count <= kSysBinMaxAtoms;
+  int32_t *cur = small ? cur_s : b.bin_count + base;
+  int32_t *lbin_g = b.bin_of + start;
   if (threadIdx.x == 0) G.bin_base = (int32_t)base;
   for (int k = threadIdx.x; k <= nbins; k += blockDim.x) cur[k] = 0;
   __syncthreads();
@@ -400,14 +392,17 @@ __global__ void __launch_bounds__(kBlock)
     b.wrap[3 * i + 1] = W[1];
     b.wrap[3 * i + 2] = W[2];
     b.wpos[i] = make_double4(w[0], w[1], w[2], 0.0);
-    lbin[a] = (int16_t)lb;
+    if (small)
+      lbin_s[a] = (int16_t)lb;
+    else
+      lbin_g[a] = lb;
     atomicAdd(&cur[lb], 1);
   }
   __syncthreads();
   // exclusive scan of cur[0..nbins] (cur[nbins] = 0 becomes the total), each
   // thread a contiguous run of entries
   const int per = (nbins + 1 + blockDim.x - 1) / blockDim.x;
-  const int k0 = threadIdx.x * per, k1 = min(k0 + per, nbins + 1);
+  const int k0 = min((int)threadIdx.x * per, nbins + 1), k1 = min(k0 + per, nbins + 1);
   int64_t run = 0;
   for (int k = k0; k < k1; ++k) run += cur[k];
   int64_t pre = block_excl_scan(run, &chunk_tot);
@@ -422,7 +417,7 @@ __global__ void __launch_bounds__(kBlock)
   const unsigned lt = (1u << lane) - 1u;
   for (int c0 = 0; c0 < count; c0 += blockDim.x) {
     const int a = c0 + threadIdx.x;
-    const int lb = a < count ? (int)lbin[a] : -1;
+    const int lb = a < count ? (small ? (int)lbin_s[a] : lbin_g[a]) : -1;
     for (int wv = 0; wv < (int)(blockDim.x >> 5); ++wv) {
       if (warp == wv) {
         const unsigned peers = __match_any_sync(0xffffffffu, lb);
@@ -448,24 +443,38 @@ __global__ void __launch_bounds__(kBlock)
 template <class P>
 int prepare_bins_sys(const P *positions, const P *cell_row, const uint8_t *pbc,
                      const int64_t *system_idx, int64_t n, int64_t ns, double cutoff,
-                     BinData &b, cudaStream_t st, const int32_t *species, int32_t *only,
-                     int32_t *err) {
+                     BinData &b, cudaStream_t st, const int32_t *species, const int32_t *only) {
   cudaMemsetAsync(b.sys_lo, 0, sizeof(int64_t) * ns, st);
   cudaMemsetAsync(b.sys_hi, 0, sizeof(int64_t) * ns, st);
   if (n > 0) k_sys_bounds<<<grid_for(n), kBlock, 0, st>>>(system_idx, n, b.sys_lo, b.sys_hi,
                                                          b.sys_of);
   k_bins_sys<P><<<(unsigned)ns, kBlock, 0, st>>>(positions, cell_row, pbc, cutoff, only, species,
-                                                 b, err);
+                                                 b);
   TSB_CHECK_LAUNCH();
   return TSB_OK;
 }
 
-template int prepare_bins_sys<float>(const float *, const float *, const uint8_t *,
-                                     const int64_t *, int64_t, int64_t, double, BinData &,
-                                     cudaStream_t, const int32_t *, int32_t *, int32_t *);
-template int prepare_bins_sys<double>(const double *, const double *, const uint8_t *,
-                                      const int64_t *, int64_t, int64_t, double, BinData &,
-                                      cudaStream_t, const int32_t *, int32_t *, int32_t *);
+template <class P>
+int prepare_bins_any(const P *positions, const P *cell_row, const uint8_t *pbc,
+                     const int64_t *system_idx, int64_t n, int64_t ns, double cutoff,
+                     BinData &b, cudaStream_t st, const int32_t *species,
+                     int64_t max_system_atoms) {
+  if (max_system_atoms > 0 && max_system_atoms <= kSysBinMaxAtoms)
+    return prepare_bins_sys<P>(positions, cell_row, pbc, system_idx, n, ns, cutoff, b, st,
+                               species, nullptr);
+  return prepare_bins<P>(positions, cell_row, pbc, system_idx, n, ns, cutoff, b, st, species);
+}
+
+#define TSB_BINS_INST(P)                                                                       \
+  template int prepare_bins_sys<P>(const P *, const P *, const uint8_t *, const int64_t *,     \
+                                   int64_t, int64_t, double, BinData &, cudaStream_t,          \
+                                   const int32_t *, const int32_t *);                          \
+  template int prepare_bins_any<P>(const P *, const P *, const uint8_t *, const int64_t *,     \
+                                   int64_t, int64_t, double, BinData &, cudaStream_t,          \
+                                   const int32_t *, int64_t);
+TSB_BINS_INST(float)
+TSB_BINS_INST(double)
+#undef TSB_BINS_INST
 
 int64_t bin_capacity(int64_t n_atoms, int64_t n_systems) {
   return 2 * n_atoms + n_systems + 1;

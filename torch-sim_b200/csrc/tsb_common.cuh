@@ -125,19 +125,27 @@ int prepare_bins(const P *positions, const P *cell_row, const uint8_t *pbc,
                  double search_cutoff, BinData &b, cudaStream_t st,
                  const int32_t *species = nullptr);
 
-// Largest system the per-system binning takes, and the status it reports
-// (atomicMax into *err) for a larger one.
+// Systems up to this size are binned with shared-memory tables by the
+// per-system binning.
 constexpr int kSysBinMaxAtoms = 4096;
-constexpr int32_t kSysBinErr = 1 << 29;
 
 // Per-system binning of the systems with only[s] != 0 (all when only is null),
-// each of at most kSysBinMaxAtoms atoms, into the same BinData layout (static
-// bin regions: bin_base = 2 sys_lo + s).  A larger selected system gets an empty
-// grid, is deselected (only[s] = 0) and raises *err to kSysBinErr.
+// one block each, into the same BinData layout (static bin regions: bin_base =
+// 2 sys_lo + s).  Fast for systems of at most kSysBinMaxAtoms atoms; larger ones
+// are binned correctly but slowly.
 template <class P>
 int prepare_bins_sys(const P *positions, const P *cell_row, const uint8_t *pbc,
                      const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
                      double search_cutoff, BinData &b, cudaStream_t st, const int32_t *species,
-                     int32_t *only, int32_t *err);
+                     const int32_t *only);
+
+// prepare_bins_sys over every system when the caller's max_system_atoms (the
+// largest system's atom count, 0 = unknown) is at most kSysBinMaxAtoms, else the
+// batch-wide prepare_bins.
+template <class P>
+int prepare_bins_any(const P *positions, const P *cell_row, const uint8_t *pbc,
+                     const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
+                     double search_cutoff, BinData &b, cudaStream_t st, const int32_t *species,
+                     int64_t max_system_atoms);
 
 }  // namespace tsb

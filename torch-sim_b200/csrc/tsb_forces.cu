@@ -152,8 +152,9 @@ static int pair_forward(int pot, const double *table, int nsp, const int32_t *sp
                         const P *pos, const P *cell, const uint8_t *pbc, const int64_t *sys,
                         int64_t n, int64_t ns, double cutoff, int flags, P *energy,
                         P *forces, P *stress, P *energies, P *stresses,
-                        const uint8_t *active, PairWork &w, cudaStream_t st) {
-  TSB_TRY(prepare_bins<P>(pos, cell, pbc, sys, n, ns, cutoff, w.b, st, species));
+                        const uint8_t *active, int64_t max_sys, PairWork &w,
+                        cudaStream_t st) {
+  TSB_TRY(prepare_bins_any<P>(pos, cell, pbc, sys, n, ns, cutoff, w.b, st, species, max_sys));
   const bool f64 = flags & TSB_MATH_FP64;
   if (n > 0) {
 #define TSB_LAUNCH(POT)                                                                    \
@@ -200,7 +201,8 @@ extern "C" int tsb_pair_forward(int potential, const double *table, int n_specie
                                 const int64_t *system_idx, int64_t n_atoms,
                                 int64_t n_systems, int dtype, double cutoff, int out_flags,
                                 void *energy, void *forces, void *stress, void *energies,
-                                void *stresses, const uint8_t *sys_active, void *workspace,
+                                void *stresses, const uint8_t *sys_active,
+                                int64_t max_system_atoms, void *workspace,
                                 size_t workspace_bytes, void *stream) {
   if (potential < TSB_POT_LJ || potential > TSB_POT_PLIFE) return TSB_ERR_INVALID_ARG;
   if (n_species < 1 || n_species > kMaxSpecies || !table) return TSB_ERR_INVALID_ARG;
@@ -224,10 +226,11 @@ extern "C" int tsb_pair_forward(int potential, const double *table, int n_specie
                                 (const double *)positions, (const double *)cell_row, pbc,
                                 system_idx, n_atoms, n_systems, cutoff, out_flags,
                                 (double *)energy, (double *)forces, (double *)stress,
-                                (double *)energies, (double *)stresses, sys_active, w, st);
+                                (double *)energies, (double *)stresses, sys_active,
+                                max_system_atoms, w, st);
   return pair_forward<float>(potential, table, n_species, species, (const float *)positions,
                              (const float *)cell_row, pbc, system_idx, n_atoms, n_systems,
                              cutoff, out_flags, (float *)energy, (float *)forces,
                              (float *)stress, (float *)energies, (float *)stresses, sys_active,
-                             w, st);
+                             max_system_atoms, w, st);
 }

@@ -582,8 +582,7 @@ static int vl_build(const P *pos, const P *cell, const uint8_t *pbc, const int64
   const double rcs = cutoff + skin;
   // batches of small systems rebin only the expired systems, one block each
   if (max_sys > 0 && max_sys <= kSysBinMaxAtoms)
-    TSB_TRY(prepare_bins_sys<P>(pos, cell, pbc, sys, n, ns, rcs, w.b, st, species, w.sys_exp,
-                                flags + 1));
+    TSB_TRY(prepare_bins_sys<P>(pos, cell, pbc, sys, n, ns, rcs, w.b, st, species, w.sys_exp));
   else
     TSB_TRY(prepare_bins<P>(pos, cell, pbc, sys, n, ns, rcs, w.b, st, species));
   k_vl_exp_counts<<<grid_for(ns), kBlock, 0, st>>>(w.sys_exp, w.b.sys_lo, w.b.sys_hi, ns,

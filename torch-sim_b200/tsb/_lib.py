@@ -46,18 +46,19 @@ PROTOTYPES = {
                             _vp, _vp, _i64, _vp, _vp, _sz, _vp]),
     "tsb_pair_workspace_size": (_sz, [_i64, _i64]),
     "tsb_pair_forward": (_int, [_int, _vp, _int, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _int,
-                                _dbl, _int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
+                                _dbl, _int, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _sz,
+                                _vp]),
     "tsb_md_kick": (_int, [_vp, _vp, _vp, _vp, _dbl, _i64, _int, _vp]),
     "tsb_md_drift": (_int, [_vp, _vp, _vp, _vp, _vp, _dbl, _i64, _int, _vp]),
     "tsb_md_baoab_boa": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _u64, _u64,
                                 _i64, _int, _vp]),
     "tsb_adjoint_workspace_size": (_sz, [_i64, _i64, _i64]),
     "tsb_lj_hvp": (_int, [_vp, _int, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _dbl, _vp, _dbl, _vp,
-                          _vp, _vp, _sz, _vp]),
-    "tsb_rdf_hist": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _dbl, _int, _dbl, _vp, _vp, _sz,
-                            _vp]),
+                          _vp, _i64, _vp, _sz, _vp]),
+    "tsb_rdf_hist": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _dbl, _int, _dbl, _vp, _i64, _vp,
+                            _sz, _vp]),
     "tsb_rdf_hist_grad": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _dbl, _int, _dbl, _vp, _vp,
-                                 _vp, _sz, _vp]),
+                                 _i64, _vp, _sz, _vp]),
     "tsb_verlet_workspace_size": (_sz, [_i64]),
     "tsb_verlet_build": (_int, [_vp, _vp, _i64, _int, _dbl, _dbl, _vp, _vp, _int, _vp, _vp,
                                 _vp, _vp, _sz, _vp]),
@@ -177,6 +178,25 @@ def call(name: str, *args):
     if st != TSB_OK:
         raise TsbError(name, st)
     return st
+
+
+_MAX_SYS_CACHE: dict = {}
+
+
+def max_system_atoms(system_idx: torch.Tensor, n_systems: int) -> int:
+    """Largest system's atom count (the binning hint of the C ABI), cached per
+    system_idx tensor version (one device read when it changes)."""
+    key = (system_idx.data_ptr(), system_idx._version, system_idx.shape[0], n_systems)
+    hit = _MAX_SYS_CACHE.get(key)
+    if hit is None:
+        if system_idx.numel() == 0:
+            hit = 0
+        else:
+            hit = int(torch.bincount(system_idx, minlength=n_systems).max())
+        if len(_MAX_SYS_CACHE) > 64:
+            _MAX_SYS_CACHE.clear()
+        _MAX_SYS_CACHE[key] = hit
+    return hit
 
 
 def ptr(t: torch.Tensor | None) -> int | None:

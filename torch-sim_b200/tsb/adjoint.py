@@ -56,6 +56,11 @@ class TrajectoryProblem:
     def n_systems(self):
         return self.cell_row.shape[0]
 
+    @property
+    def max_sys(self):
+        """Largest system's atom count (binning hint; cached per system_idx)."""
+        return L.max_system_atoms(self.system_idx, self.n_systems)
+
 
 def lj_table(sigma: torch.Tensor, epsilon: torch.Tensor) -> torch.Tensor:
     ns = sigma.shape[0]
@@ -80,8 +85,8 @@ def forces(q, table, P: TrajectoryProblem, ws=None):
         ws = L.Workspace.get(dev, L.load().tsb_pair_workspace_size(n, s))
     L.call("tsb_pair_forward", L.POT_LJ, L.ptr(table), P.n_species, L.ptr(P.species), L.ptr(q),
            L.ptr(P.cell_row), L.ptr(P.pbc), L.ptr(P.system_idx), n, s, L.F64, P.cutoff,
-           L.OUT_FORCES | L.MATH_FP64, L.ptr(e), L.ptr(f), None, None, None, None, L.ptr(ws),
-           ws.numel(), L.stream_ptr(dev))
+           L.OUT_FORCES | L.MATH_FP64, L.ptr(e), L.ptr(f), None, None, None, None, P.max_sys,
+           L.ptr(ws), ws.numel(), L.stream_ptr(dev))
     return e, f
 
 
@@ -89,8 +94,8 @@ def histogram(q, P: TrajectoryProblem):
     h = torch.empty((P.n_systems, P.n_bins), dtype=torch.float64, device=q.device)
     ws = _ws(q.device, P.n_atoms, P.n_systems, P.n_bins)
     L.call("tsb_rdf_hist", L.ptr(q), L.ptr(P.cell_row), L.ptr(P.pbc), L.ptr(P.system_idx),
-           P.n_atoms, P.n_systems, P.r_max, P.n_bins, P.width, L.ptr(h), L.ptr(ws), ws.numel(),
-           L.stream_ptr(q.device))
+           P.n_atoms, P.n_systems, P.r_max, P.n_bins, P.width, L.ptr(h), P.max_sys, L.ptr(ws),
+           ws.numel(), L.stream_ptr(q.device))
     return h
 
 
@@ -99,7 +104,7 @@ def _hist_grad(q, dl_dh, P):
     ws = _ws(q.device, P.n_atoms, P.n_systems, P.n_bins)
     L.call("tsb_rdf_hist_grad", L.ptr(q), L.ptr(P.cell_row), L.ptr(P.pbc), L.ptr(P.system_idx),
            P.n_atoms, P.n_systems, P.r_max, P.n_bins, P.width, L.ptr(dl_dh.contiguous()),
-           L.ptr(g), L.ptr(ws), ws.numel(), L.stream_ptr(q.device))
+           L.ptr(g), P.max_sys, L.ptr(ws), ws.numel(), L.stream_ptr(q.device))
     return g
 
 
@@ -108,7 +113,7 @@ def _hvp(q, table, v, coef, lam_q, gparams, P, ws=None):
         ws = _ws(q.device, P.n_atoms, P.n_systems, 2 * P.n_species ** 2)
     L.call("tsb_lj_hvp", L.ptr(table), P.n_species, L.ptr(P.species), L.ptr(q),
            L.ptr(P.cell_row), L.ptr(P.pbc), L.ptr(P.system_idx), P.n_atoms, P.n_systems,
-           P.cutoff, L.ptr(v), float(coef), L.ptr(lam_q), L.ptr(gparams), L.ptr(ws),
+           P.cutoff, L.ptr(v), float(coef), L.ptr(lam_q), L.ptr(gparams), P.max_sys, L.ptr(ws),
            ws.numel(), L.stream_ptr(q.device))
 
 
@@ -338,13 +343,15 @@ def make_problem(state, n_steps, dt, *, cutoff=8.5125, checkpoint_every=20, targ
     lut[z] = torch.arange(len(z), dtype=torch.int32, device=state.device)
     n_sys = state.n_systems
     pbc = L.pbc_rows(state.pbc, n_sys, state.positions.device).bool()
-    return TrajectoryProblem(cell_row=state.cell.mT.double().contiguous(),
-                             pbc=pbc.to(torch.uint8).contiguous(),
-                             system_idx=state.system_idx.contiguous(),
-                             species=lut[state.atomic_numbers].contiguous(),
-                             masses=state.masses.double().contiguous(), n_species=len(z),
-                             n_steps=int(n_steps), dt=float(dt), cutoff=float(cutoff),
-                             target=target, checkpoint_every=int(checkpoint_every))
+    P = TrajectoryProblem(cell_row=state.cell.mT.double().contiguous(),
+                          pbc=pbc.to(torch.uint8).contiguous(),
+                          system_idx=state.system_idx.contiguous(),
+                          species=lut[state.atomic_numbers].contiguous(),
+                          masses=state.masses.double().contiguous(), n_species=len(z),
+                          n_steps=int(n_steps), dt=float(dt), cutoff=float(cutoff),
+                          target=target, checkpoint_every=int(checkpoint_every))
+    P.max_sys  # noqa: B018  (reads the size once, outside any graph capture)
+    return P
 
 
 def argon_pair_params(n_species=2, sigma=3.405, epsilon=0.0104, perturb=0.0, seed=0,

@@ -164,8 +164,8 @@ class PairTableModel(ModelInterface):
         L.call("tsb_pair_forward", self.kind, L.ptr(table), self.n_species, L.ptr(species),
                L.ptr(pos), L.ptr(cell_row), L.ptr(pbc), L.ptr(sys_idx), n, n_sys,
                L.dtype_code(dt), self.cutoff, flags, L.ptr(energy), L.ptr(forces),
-               L.ptr(stress), L.ptr(energies), L.ptr(stresses), L.ptr(sys_active), L.ptr(ws),
-               ws.numel(), L.stream_ptr(dev))
+               L.ptr(stress), L.ptr(energies), L.ptr(stresses), L.ptr(sys_active),
+               L.max_system_atoms(sys_idx, n_sys), L.ptr(ws), ws.numel(), L.stream_ptr(dev))
 
 
 def single_species_table(sigma, epsilon, alpha=0.0, rc=np.inf, eshift=0.0):

@@ -99,9 +99,6 @@ class VerletListModel(ModelInterface):
             if st >= (1 << 30):
                 raise ValueError("VerletListModel needs every periodic cell width >= "
                                  "cutoff + skin")
-            if st == (1 << 29):
-                raise RuntimeError("tsb_vlist_build: a system is larger than "
-                                   "max_system_atoms")
             # a list overflowed: regrow and rebuild every system
             self.cap = int(st * 1.2) + 8
             self.list = torch.empty(self.cap * n, dtype=torch.int32, device=dev)
@@ -194,9 +191,6 @@ class VerletListModel(ModelInterface):
             if st >= (1 << 30):
                 raise ValueError("VerletListModel needs every periodic cell width >= "
                                  "cutoff + skin")
-            if st == (1 << 29):
-                raise RuntimeError("tsb_vlist_build: a system is larger than "
-                                   "max_system_atoms")
             self.s_cap = int(st * 1.2) + 8
             self.s_list = torch.empty(self.s_cap * state.n_atoms, dtype=torch.int32,
                                       device=state.device)
