@@ -326,6 +326,19 @@ int tsb_vlist_forces(int potential, const double *table, int n_species, const in
  * per_atom for tsb_adjoint_workspace_size: 2*ns*ns (hvp) or n_bins (rdf).
  * max_system_atoms: as for tsb_pair_forward. */
 size_t tsb_adjoint_workspace_size(int64_t n_atoms, int64_t n_systems, int64_t per_atom);
+/* Velocity-Verlet pieces of the trajectory and its adjoint (FP64, [N,3] arrays,
+ * inv_m [N]); each product and sum rounded on its own, as the tensor expressions
+ * of nve.py:118-130 round them:
+ * tsb_vv_kick_drift: p_out = p + f * half_dt;  q_out = q + (p_out * inv_m) * dt
+ * tsb_vv_kick:       p_out = p + f * half_dt
+ * tsb_adj_kick:      lam_p += lam_q * (dt * inv_m) */
+int tsb_vv_kick_drift(const double *q, const double *p, const double *f, const double *inv_m,
+                      double half_dt, double dt, double *q_out, double *p_out, int64_t n_atoms,
+                      void *stream);
+int tsb_vv_kick(const double *p, const double *f, double half_dt, double *p_out,
+                int64_t n_atoms, void *stream);
+int tsb_adj_kick(double *lam_p, const double *lam_q, const double *inv_m, double dt,
+                 int64_t n_atoms, void *stream);
 int tsb_lj_hvp(const double *table, int n_species, const int32_t *species,
                const double *positions, const double *cell_row, const uint8_t *pbc,
                const int64_t *system_idx, int64_t n_atoms, int64_t n_systems, double cutoff,

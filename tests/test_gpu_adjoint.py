@@ -114,3 +114,30 @@ def test_adjoint_vs_finite_differences_200_steps():
         dq = dq.view_as(q0)
         fd = (L(s, e, q0 + dq) - L(s, e, q0 - dq)) / (2 * h)
         assert abs(float(gq.flatten()[k]) - fd) <= 1e-4 * abs(fd), (k, float(gq.flatten()[k]), fd)
+
+
+def test_vv_kernels_round_like_the_tensor_expressions():
+    """The fused velocity-Verlet and adjoint-kick launches give bitwise the
+    results of the element-wise tensor expressions they replace."""
+    from tsb import _lib as L
+
+    g = torch.Generator(device="cuda").manual_seed(7)
+    n = 1000
+    r = lambda: torch.randn((n, 3), dtype=torch.float64, device="cuda", generator=g)  # noqa
+    q, p, f, lam_q = r(), r(), r(), r()
+    inv_m = 1.0 / (1.0 + torch.rand(n, dtype=torch.float64, device="cuda", generator=g) * 40)
+    dt = 0.0123456789
+    st = L.stream_ptr(q.device)
+    q1, p1 = torch.empty_like(q), torch.empty_like(p)
+    L.call("tsb_vv_kick_drift", L.ptr(q), L.ptr(p), L.ptr(f), L.ptr(inv_m), dt / 2, dt,
+           L.ptr(q1), L.ptr(p1), n, st)
+    ph = p + f * (dt / 2)
+    assert torch.equal(p1, ph)
+    assert torch.equal(q1, q + (ph * inv_m.unsqueeze(-1)) * dt)
+    p2 = torch.empty_like(p)
+    L.call("tsb_vv_kick", L.ptr(p1), L.ptr(f), dt / 2, L.ptr(p2), n, st)
+    assert torch.equal(p2, p1 + f * (dt / 2))
+    lam_p = r()
+    expect = lam_p + lam_q * (dt * inv_m.unsqueeze(-1))
+    L.call("tsb_adj_kick", L.ptr(lam_p), L.ptr(lam_q), L.ptr(inv_m), dt, n, st)
+    assert torch.equal(lam_p, expect)

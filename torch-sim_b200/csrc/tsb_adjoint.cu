@@ -128,6 +128,17 @@ __global__ void __launch_bounds__(128)
 
 // Gaussian-smeared histogram of pair distances r < r_max (each unordered pair
 // once): h_b = sum_pairs exp(-(r - c_b)^2 / (2 w^2)), c_b = (b + 1/2) r_max / B.
+// A pair adds to the bins with |r - c_b| <= kRdfWindow w only: a term beyond is
+// below exp(-72) ~ 5e-32 of a pair's peak term, under FP64 rounding of any bin
+// the pair reaches.
+constexpr double kRdfWindow = 12.0;
+
+__device__ inline void rdf_window(double r, double bw, double width, int nb, int &k0, int &k1) {
+  const double reach = kRdfWindow * width;
+  k0 = max(0, (int)ceil((r - reach) / bw - 0.5));
+  k1 = min(nb - 1, (int)floor((r + reach) / bw - 0.5));
+}
+
 __global__ void __launch_bounds__(128)
     k_rdf_part(BinData b, int64_t n, double r_max, int nb, double width, double *part) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -141,7 +152,9 @@ __global__ void __launch_bounds__(128)
   search_neighbors(G, b.spos, b.bin_start, i, w.x, w.y, w.z, r_max * r_max, false,
                    [&](int, int, int, int, double, double, double, double d2) {
                      const double r = sqrt(d2);
-                     for (int k = 0; k < nb; ++k) {
+                     int k0, k1;
+                     rdf_window(r, bw, width, nb, k0, k1);
+                     for (int k = k0; k <= k1; ++k) {
                        const double x = r - (k + 0.5) * bw;
                        h[k] += 0.5 * exp(-x * x * inv2w2);  // each pair is visited twice
                      }
@@ -165,7 +178,9 @@ __global__ void __launch_bounds__(128)
                    [&](int, int, int, int, double dx, double dy, double dz, double d2) {
                      const double r = sqrt(d2);
                      double dlr = 0.0;
-                     for (int k = 0; k < nb; ++k) {
+                     int k0, k1;
+                     rdf_window(r, bw, width, nb, k0, k1);
+                     for (int k = k0; k <= k1; ++k) {
                        const double x = r - (k + 0.5) * bw;
                        dlr += dh[k] * (-x * iw2) * exp(-x * x * inv2w2);
                      }
@@ -191,9 +206,69 @@ __global__ void k_sum_parts(const SysGeom *g, const double *part, int width, dou
   }
 }
 
+// Velocity-Verlet updates of the trajectory and its adjoint, one launch each,
+// with the rounding of the element-wise tensor expressions they replace
+// (nve.py:118-130 written as p + f * (dt / 2); q + (p * inv_m) * dt): every
+// product and sum is rounded on its own (no fused multiply-add), so the results
+// are bitwise those of the tensor expressions.
+__global__ void k_vv_kick_drift(const double *q, const double *p, const double *f,
+                                const double *inv_m, double half_dt, double dt, double *q_out,
+                                double *p_out, int64_t n3) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n3) return;
+  const double ph = __dadd_rn(p[k], __dmul_rn(f[k], half_dt));
+  p_out[k] = ph;
+  q_out[k] = __dadd_rn(q[k], __dmul_rn(__dmul_rn(ph, inv_m[k / 3]), dt));
+}
+
+__global__ void k_vv_kick(const double *p, const double *f, double half_dt, double *p_out,
+                          int64_t n3) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n3) p_out[k] = __dadd_rn(p[k], __dmul_rn(f[k], half_dt));
+}
+
+// lam_p += lam_q * (dt * inv_m)
+__global__ void k_adj_kick(double *lam_p, const double *lam_q, const double *inv_m, double dt,
+                           int64_t n3) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n3) lam_p[k] = __dadd_rn(lam_p[k], __dmul_rn(lam_q[k], __dmul_rn(dt, inv_m[k / 3])));
+}
+
 }  // namespace tsb
 
 using namespace tsb;
+
+extern "C" int tsb_vv_kick_drift(const double *q, const double *p, const double *f,
+                                 const double *inv_m, double half_dt, double dt, double *q_out,
+                                 double *p_out, int64_t n_atoms, void *stream) {
+  if (n_atoms < 0 || (n_atoms > 0 && (!q || !p || !f || !inv_m || !q_out || !p_out)))
+    return TSB_ERR_INVALID_ARG;
+  if (n_atoms == 0) return TSB_OK;
+  k_vv_kick_drift<<<grid_for(3 * n_atoms), kBlock, 0, (cudaStream_t)stream>>>(
+      q, p, f, inv_m, half_dt, dt, q_out, p_out, 3 * n_atoms);
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
+
+extern "C" int tsb_vv_kick(const double *p, const double *f, double half_dt, double *p_out,
+                           int64_t n_atoms, void *stream) {
+  if (n_atoms < 0 || (n_atoms > 0 && (!p || !f || !p_out))) return TSB_ERR_INVALID_ARG;
+  if (n_atoms == 0) return TSB_OK;
+  k_vv_kick<<<grid_for(3 * n_atoms), kBlock, 0, (cudaStream_t)stream>>>(p, f, half_dt, p_out,
+                                                                        3 * n_atoms);
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
+
+extern "C" int tsb_adj_kick(double *lam_p, const double *lam_q, const double *inv_m, double dt,
+                            int64_t n_atoms, void *stream) {
+  if (n_atoms < 0 || (n_atoms > 0 && (!lam_p || !lam_q || !inv_m))) return TSB_ERR_INVALID_ARG;
+  if (n_atoms == 0) return TSB_OK;
+  k_adj_kick<<<grid_for(3 * n_atoms), kBlock, 0, (cudaStream_t)stream>>>(lam_p, lam_q, inv_m, dt,
+                                                                         3 * n_atoms);
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
 
 extern "C" size_t tsb_adjoint_workspace_size(int64_t n_atoms, int64_t n_systems,
                                              int64_t per_atom) {

@@ -118,13 +118,23 @@ def _hvp(q, table, v, coef, lam_q, gparams, P, ws=None):
 
 
 def _vv_step(q, p, f, table, P, inv_m, ws=None):
-    """One velocity-Verlet step (same floating-point order as nve.py:118-130)."""
-    dt = P.dt
-    p = p + f * (dt / 2)
-    q = q + (p * inv_m) * dt
-    _, f = forces(q, table, P, ws)
-    p = p + f * (dt / 2)
-    return q, p, f
+    """One velocity-Verlet step (same floating-point order as nve.py:118-130:
+    p + f * (dt / 2), q + (p * inv_m) * dt, each product and sum rounded on its
+    own), the kick-drift and the closing kick one launch each."""
+    dt, n, st = P.dt, q.shape[0], L.stream_ptr(q.device)
+    q_new, p_half = torch.empty_like(q), torch.empty_like(p)
+    L.call("tsb_vv_kick_drift", L.ptr(q), L.ptr(p), L.ptr(f), L.ptr(inv_m), dt / 2, dt,
+           L.ptr(q_new), L.ptr(p_half), n, st)
+    _, f = forces(q_new, table, P, ws)
+    p_new = torch.empty_like(p)
+    L.call("tsb_vv_kick", L.ptr(p_half), L.ptr(f), dt / 2, L.ptr(p_new), n, st)
+    return q_new, p_new, f
+
+
+def _adj_kick(lam_p, lam_q, inv_m, P):
+    """lam_p += lam_q * (dt * inv_m), in place, one launch."""
+    L.call("tsb_adj_kick", L.ptr(lam_p), L.ptr(lam_q), L.ptr(inv_m), P.dt, lam_p.shape[0],
+           L.stream_ptr(lam_p.device))
 
 
 class _Graphs:
@@ -151,7 +161,7 @@ class _Graphs:
         self.lam_p = torch.zeros_like(self.q0)
         self.gpar = torch.zeros((P.n_systems, P.n_species, P.n_species, 2), dtype=f64,
                                 device=dev)
-        self.inv_m = (1.0 / P.masses).unsqueeze(-1)
+        self.inv_m = (1.0 / P.masses).contiguous()
         lib = L.load()
         self.ws_pair = torch.empty(lib.tsb_pair_workspace_size(n, P.n_systems),
                                    dtype=torch.uint8, device=dev)
@@ -207,7 +217,7 @@ class _Graphs:
 
             def body():
                 for k in range(length - 1, -1, -1):
-                    self.lam_p.add_(self.lam_q * (P.dt * self.inv_m))
+                    _adj_kick(self.lam_p, self.lam_q, self.inv_m, P)
                     coef = P.dt / 2 if (first and k == 0) else P.dt
                     _hvp(seg[k], self.table, self.lam_p, coef, self.lam_q, self.gpar, P,
                          self.ws_adj)
@@ -246,7 +256,7 @@ def integrate(q0, p0, table, P: TrajectoryProblem, keep_checkpoints=True, use_gr
     ``use_graphs`` each checkpoint segment replays one CUDA graph."""
     if use_graphs and q0.is_cuda and P.n_steps > 0:
         return _integrate_graphs(q0, p0, table, P, keep_checkpoints)
-    inv_m = (1.0 / P.masses).unsqueeze(-1)
+    inv_m = (1.0 / P.masses).contiguous()
     q, p = q0.contiguous(), p0.contiguous()
     _, f = forces(q, table, P)
     ckpt = {0: (q, p)}
@@ -292,7 +302,7 @@ def loss_and_grad(sigma, epsilon, q0, p0, P: TrajectoryProblem, use_graphs=True)
     lam_p = torch.zeros_like(lam_q)
     gpar = torch.zeros((P.n_systems, P.n_species, P.n_species, 2), dtype=torch.float64,
                        device=q0.device)
-    inv_m = (1.0 / P.masses).unsqueeze(-1)
+    inv_m = (1.0 / P.masses).contiguous()
     starts = sorted(ckpt)
     for c in reversed(starts):
         end = min(c + P.checkpoint_every, P.n_steps)
@@ -303,7 +313,7 @@ def loss_and_grad(sigma, epsilon, q0, p0, P: TrajectoryProblem, use_graphs=True)
             q, p, f = _vv_step(q, p, f, table, P, inv_m)
             seg.append(q)
         for k in range(end - 1, c - 1, -1):
-            lam_p = lam_p + lam_q * (P.dt * inv_m)
+            _adj_kick(lam_p, lam_q, inv_m, P)
             _hvp(seg[k - c], table, lam_p, P.dt if k > 0 else P.dt / 2, lam_q, gpar, P)
     g = gpar.sum(0)
     # sigma_ab and sigma_ba are one parameter: symmetrise the gradient
