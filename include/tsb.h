@@ -306,6 +306,17 @@ int tsb_vlist_build(const void *positions, const void *cell_row, const uint8_t *
                     int64_t n_systems, int dtype, double cutoff, double skin, uint32_t *list,
                     int32_t *counts, int max_neighbors, int64_t max_system_atoms,
                     int32_t *flags, void *workspace, size_t workspace_bytes, void *stream);
+/* tsb_vlist_lj_hvp: the adjoint's LJ Hessian-vector product (as tsb_lj_hvp:
+ *   lam_q += coef * J_F(q)^T v, grad_params [S, ns, ns, 2] += coef *
+ *   dF/d(sigma, epsilon)^T v) over lists built for `positions` (FP64; rows of
+ *   `table` as for tsb_lj_hvp); scratch of tsb_vlist_hvp_scratch_size bytes. */
+size_t tsb_vlist_hvp_scratch_size(int64_t n_atoms, int n_species);
+int tsb_vlist_lj_hvp(const double *table, int n_species, const int32_t *species,
+                     const uint32_t *list, const int32_t *counts, const double *positions,
+                     const double *cell_row, const int64_t *system_idx, int64_t n_atoms,
+                     int64_t n_systems, double cutoff, const double *v, double coef,
+                     double *lam_q, double *grad_params, void *scratch, size_t scratch_bytes,
+                     void *workspace, size_t workspace_bytes, void *stream);
 int tsb_vlist_forces(int potential, const double *table, int n_species, const int32_t *species,
                      const uint32_t *list, const int32_t *counts, const void *positions,
                      const void *cell_row, const int64_t *system_idx, const uint8_t *sys_active,

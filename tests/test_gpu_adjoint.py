@@ -141,3 +141,33 @@ def test_vv_kernels_round_like_the_tensor_expressions():
     expect = lam_p + lam_q * (dt * inv_m.unsqueeze(-1))
     L.call("tsb_adj_kick", L.ptr(lam_p), L.ptr(lam_q), L.ptr(inv_m), dt, n, st)
     assert torch.equal(lam_p, expect)
+
+
+def test_list_forces_and_hvp_match_the_per_call_search():
+    """The captured segments take forces and Hessian-vector products over
+    batched Verlet lists: the same pairs as the per-call search, summed in list
+    order (max|d|/max|ref| <= 1e-10), also after the atoms have moved."""
+    from tsb import adjoint
+
+    P, s, e, q0, p0 = _config5(n_sys=12, n_steps=1)
+    table = adjoint.lj_table(s, e)
+    lf = adjoint._ListForces(P)
+    g = torch.Generator(device="cuda").manual_seed(9)
+    v = torch.randn(q0.shape, dtype=torch.float64, device="cuda", generator=g)
+
+    def rel(a, b):
+        return float((a - b).abs().max() / b.abs().max())
+
+    q = q0.clone()
+    for step in range(3):
+        _, f_ref = adjoint.forces(q, table, P)
+        _, f = lf(q, table)
+        assert rel(f, f_ref) <= 1e-10, step
+        lam_ref, lam = torch.zeros_like(q), torch.zeros_like(q)
+        gp_ref = torch.zeros((P.n_systems, 2, 2, 2), dtype=torch.float64, device="cuda")
+        gp = torch.zeros_like(gp_ref)
+        adjoint._hvp(q, table, v, 0.7, lam_ref, gp_ref, P)
+        lf.hvp(q, table, v, 0.7, lam, gp)
+        assert rel(lam, lam_ref) <= 1e-10 and rel(gp, gp_ref) <= 1e-10, step
+        q = q + 0.3 * torch.randn(q.shape, dtype=torch.float64, device="cuda", generator=g)
+    lf.check()

@@ -12,11 +12,10 @@
 //
 // Also: the Gaussian-smeared pair-distance histogram of each system and its
 // gradient with respect to positions (the trajectory loss).
+#include "tsb_ljhvp.cuh"
 #include "tsb_search.cuh"
 
 namespace tsb {
-
-constexpr int kAdjMaxSpecies = 4;
 
 struct AdjWork {
   BinData b;
@@ -28,31 +27,15 @@ static void carve_adj(Carver &c, AdjWork &w, int64_t n, int64_t ns, int64_t per_
   w.part = c.take<double>(n * per_atom);
 }
 
-// LJ: V = 4 eps (s^12 - s^6), s = sigma / r (lennard_jones.py:23-47)
-//   V'  = -(24 eps / r)(2 s^12 - s^6)
-//   V'' = (24 eps / r^2)(26 s^12 - 7 s^6)
-//   dV'/deps = V' / eps ;  dV'/dsigma = -(144 eps / (r sigma))(4 s^12 - s^6)
 // LANES > 1: LANES lanes per atom (small batches; fixed-order reduction of the lanes'
-// partial sums), LANES = 1: one thread per atom.
+// partial sums), LANES = 1: one thread per atom.  Pair arithmetic: lj_hvp_pair.
 template <int LANES>
 __global__ void __launch_bounds__(128)
     k_lj_hvp(BinData b, int64_t n, const double *__restrict__ table, int nsp,
              const int32_t *__restrict__ species, double cutoff, const double *__restrict__ v,
              double coef, double *__restrict__ lam_q, double *__restrict__ gpart) {
-  // per species pair: sigma^2, 1/sigma, epsilon, 1/epsilon, cutoff^2 (one FP64
-  // division per neighbour pair remains, 1/r)
-  __shared__ double sig2[kAdjMaxSpecies * kAdjMaxSpecies], isig[kAdjMaxSpecies * kAdjMaxSpecies],
-      eps[kAdjMaxSpecies * kAdjMaxSpecies], ieps[kAdjMaxSpecies * kAdjMaxSpecies],
-      rc2[kAdjMaxSpecies * kAdjMaxSpecies];
-  for (int k = threadIdx.x; k < nsp * nsp; k += blockDim.x) {
-    const double sg = table[5 * k], ep = table[5 * k + 1];
-    sig2[k] = sg * sg;
-    isig[k] = 1.0 / sg;
-    eps[k] = ep;
-    ieps[k] = 1.0 / ep;
-    const double r = fmin(cutoff, table[5 * k + 3]);
-    rc2[k] = r * r;
-  }
+  __shared__ LjHvpTable T;
+  lj_hvp_table(T, table, nsp, cutoff);
   __syncthreads();
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t p = t / LANES;
@@ -64,36 +47,15 @@ __global__ void __launch_bounds__(128)
   const double vi0 = v[3 * i], vi1 = v[3 * i + 1], vi2 = v[3 * i + 2];
   double hx = 0, hy = 0, hz = 0;
   // parameter gradients of the pairs (si, t) by neighbour species t, in registers
-  // (a static select below keeps them out of local memory)
+  // (a static select keeps them out of local memory)
   double gs[kAdjMaxSpecies], ge[kAdjMaxSpecies];
 #pragma unroll
   for (int t2 = 0; t2 < kAdjMaxSpecies; ++t2) gs[t2] = ge[t2] = 0.0;
   auto pair = [&](int j, int, int, int, double dx, double dy, double dz, double d2, int sp) {
-                     const int sj = min(max(sp, 0), nsp - 1);
-                     const int k = si * nsp + sj;
-                     if (!(d2 < rc2[k]) || !(d2 > 0.0)) return;
-                     const double r = sqrt(d2), ir = 1.0 / r, ir2 = ir * ir;
-                     const double ux = dx * ir, uy = dy * ir, uz = dz * ir;
-                     const double s2 = sig2[k] * ir2, s6 = s2 * s2 * s2, s12 = s6 * s6;
-                     const double e = eps[k];
-                     const double vp = -(24.0 * e * ir) * (2.0 * s12 - s6);
-                     const double vpp = (24.0 * e * ir2) * (26.0 * s12 - 7.0 * s6);
-                     const double w0 = vi0 - v[3 * j], w1 = vi1 - v[3 * j + 1], w2 = vi2 - v[3 * j + 2];
-                     const double uw = ux * w0 + uy * w1 + uz * w2;
-                     const double a = vpp - vp * ir;  // K w = a (u.w) u + (V'/r) w
-                     hx += a * uw * ux + vp * ir * w0;
-                     hy += a * uw * uy + vp * ir * w1;
-                     hz += a * uw * uz + vp * ir * w2;
-                     const double uvi = ux * vi0 + uy * vi1 + uz * vi2;
-                     const double dge = (vp * ieps[k]) * uvi;
-                     const double dgs = (-(144.0 * e * ir * isig[k]) * (4.0 * s12 - s6)) * uvi;
-#pragma unroll
-                     for (int t2 = 0; t2 < kAdjMaxSpecies; ++t2)
-                       if (t2 == sj) {
-                         ge[t2] += dge;
-                         gs[t2] += dgs;
-                       }
-                   };
+    const int sj = min(max(sp, 0), nsp - 1);
+    lj_hvp_pair(T, si * nsp + sj, sj, dx, dy, dz, d2, vi0, vi1, vi2, v[3 * j], v[3 * j + 1],
+                v[3 * j + 2], hx, hy, hz, gs, ge);
+  };
   if constexpr (LANES > 1) {
     group_search_neighbors<LANES>(G, b.spos, b.bin_start, i, w.x, w.y, w.z, cutoff * cutoff, false,
                           pair);

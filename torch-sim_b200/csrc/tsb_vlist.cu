@@ -37,6 +37,7 @@
 // positions, so the pair set is the FP64 one.  B = sum of the cell rows' norms +
 // skin/2 for a fully periodic system (frame positions stay within the cell plus
 // the allowed drift); systems with an open axis always take the FP64 test.
+#include "tsb_ljhvp.cuh"
 #include "tsb_pair.cuh"
 #include "tsb_search.cuh"
 #include "tsb_sysreduce.cuh"
@@ -646,9 +647,139 @@ static int vl_forces(int pot, const double *table, int nsp, const int32_t *speci
   return TSB_OK;
 }
 
+// Lennard-Jones Hessian-vector product over the lists (the adjoint's HVP with the
+// lists in place of the per-call search): lam_q -= coef (H v) per atom and the
+// per-atom parameter partials, LANES lanes per slot over its entries (fixed-order
+// butterfly reduction).  v is read in slot order (vs).
+template <int LANES>
+__global__ void __launch_bounds__(128)
+    k_vl_lj_hvp(const double4 *__restrict__ wpos, const uint32_t *__restrict__ list,
+                const int32_t *__restrict__ cnt, int64_t n, const int32_t *__restrict__ perm,
+                const int64_t *__restrict__ sys, const double *__restrict__ sv,
+                const double *__restrict__ table, int nsp, double cutoff,
+                const double *__restrict__ vs, double coef, double *__restrict__ lam_q,
+                double *__restrict__ gpart) {
+  __shared__ LjHvpTable T;
+  lj_hvp_table(T, table, nsp, cutoff);
+  __syncthreads();
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t p = t / LANES;
+  const int lane = (int)(t % LANES);
+  if (p >= n) return;  // whole groups: LANES divides the block
+  const int64_t i = perm[p];
+  const int64_t s = sys[i];
+  const double4 wi = wpos[p];
+  const int si = min(max(tag_species(wi.w), 0), nsp - 1);
+  const double vi0 = vs[3 * p], vi1 = vs[3 * p + 1], vi2 = vs[3 * p + 2];
+  const double *svs = sv + 81 * s;
+  double hx = 0, hy = 0, hz = 0;
+  double gs[kAdjMaxSpecies], ge[kAdjMaxSpecies];
+#pragma unroll
+  for (int t2 = 0; t2 < kAdjMaxSpecies; ++t2) gs[t2] = ge[t2] = 0.0;
+  const int c = cnt[p];
+  for (int k = lane; k < c; k += LANES) {
+    const uint32_t e = list[(size_t)k * n + p];
+    const int64_t js = e >> 5;
+    const int code = (int)(e & 31u);
+    const double4 wj = wpos[js];
+    const double dx = wj.x - wi.x + svs[3 * code];
+    const double dy = wj.y - wi.y + svs[3 * code + 1];
+    const double dz = wj.z - wi.z + svs[3 * code + 2];
+    const int sj = min(max(tag_species(wj.w), 0), nsp - 1);
+    lj_hvp_pair(T, si * nsp + sj, sj, dx, dy, dz, dx * dx + dy * dy + dz * dz, vi0, vi1, vi2,
+                vs[3 * js], vs[3 * js + 1], vs[3 * js + 2], hx, hy, hz, gs, ge);
+  }
+  if constexpr (LANES > 1) {
+    hx = group_sum<LANES>(hx);
+    hy = group_sum<LANES>(hy);
+    hz = group_sum<LANES>(hz);
+#pragma unroll
+    for (int t2 = 0; t2 < kAdjMaxSpecies; ++t2) {
+      gs[t2] = group_sum<LANES>(gs[t2]);
+      ge[t2] = group_sum<LANES>(ge[t2]);
+    }
+    if (lane != 0) return;
+  }
+  // J_F^T v = -H v
+  lam_q[3 * i] -= coef * hx;
+  lam_q[3 * i + 1] -= coef * hy;
+  lam_q[3 * i + 2] -= coef * hz;
+  double *g = gpart + (size_t)i * (2 * nsp * nsp);
+  for (int k = 0; k < nsp * nsp; ++k) {
+    g[2 * k] = 0.0;
+    g[2 * k + 1] = 0.0;
+  }
+#pragma unroll
+  for (int t2 = 0; t2 < kAdjMaxSpecies; ++t2)
+    if (t2 < nsp) {
+      g[2 * (si * nsp + t2)] = coef * gs[t2];
+      g[2 * (si * nsp + t2) + 1] = coef * ge[t2];
+    }
+}
+
+// v [N,3] by atom -> vs [N,3] by slot
+__global__ void k_vl_gather3(const double *v, const int32_t *perm, int64_t n, double *vs) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < 3 * n) vs[k] = v[3 * (int64_t)perm[k / 3] + k % 3];
+}
+
+// out[s, k] += sum over the atoms of system s of part[i, k] (atom order)
+__global__ void k_vl_sum_parts(const SysGeom *g, const double *part, int width, double *out) {
+  const int s = blockIdx.x;
+  const SysGeom &G = g[s];
+  for (int k = threadIdx.x; k < width; k += blockDim.x) {
+    double t = 0.0;
+    for (int a = 0; a < G.count; ++a) t += part[(size_t)(G.start + a) * width + k];
+    out[(size_t)s * width + k] += t;
+  }
+}
+
 }  // namespace tsb
 
 using namespace tsb;
+
+extern "C" size_t tsb_vlist_hvp_scratch_size(int64_t n_atoms, int n_species) {
+  return sizeof(double) * (size_t)n_atoms * (3 + 2 * (size_t)n_species * n_species) + 512;
+}
+
+extern "C" int tsb_vlist_lj_hvp(const double *table, int n_species, const int32_t *species,
+                                const uint32_t *list, const int32_t *counts,
+                                const double *positions, const double *cell_row,
+                                const int64_t *system_idx, int64_t n_atoms, int64_t n_systems,
+                                double cutoff, const double *v, double coef, double *lam_q,
+                                double *grad_params, void *scratch, size_t scratch_bytes,
+                                void *workspace, size_t workspace_bytes, void *stream) {
+  if (n_species < 1 || n_species > kAdjMaxSpecies || !table || (n_species > 1 && !species) ||
+      n_atoms < 1 || n_systems < 1 || !list || !counts || !positions || !cell_row ||
+      !system_idx || !v || !lam_q || !grad_params || !(cutoff > 0.0))
+    return TSB_ERR_INVALID_ARG;
+  Carver c(workspace, workspace_bytes);
+  VlWork w;
+  carve_vl(c, w, n_atoms, n_systems);
+  if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
+  const int width = 2 * n_species * n_species;
+  Carver cs(scratch, scratch_bytes);
+  double *vs = cs.take<double>(3 * n_atoms);
+  double *part = cs.take<double>(n_atoms * width);
+  if (!cs.ok || !scratch) return TSB_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  k_vl_sys_geom<double><<<grid_for(27 * n_systems), kBlock, 0, st>>>(
+      cell_row, n_systems, w.b.sys_lo, w.b.sys_hi, w.rslack, cutoff, w.sv, w.svf, w.band, w.cur);
+  k_vl_frame<double><<<grid_for(n_atoms), kBlock, 0, st>>>(
+      positions, cell_row, system_idx, species, n_atoms, w.perm, w.rwrap, w.wpos, w.wpos32);
+  k_vl_gather3<<<grid_for(3 * n_atoms), kBlock, 0, st>>>(v, w.perm, n_atoms, vs);
+  if (n_atoms <= kGroupSearchMaxAtoms)
+    k_vl_lj_hvp<kSearchGroup><<<grid_for(kSearchGroup * n_atoms, 128), 128, 0, st>>>(
+        w.wpos, list, counts, n_atoms, w.perm, system_idx, w.sv, table, n_species, cutoff, vs,
+        coef, lam_q, part);
+  else
+    k_vl_lj_hvp<1><<<grid_for(n_atoms, 128), 128, 0, st>>>(
+        w.wpos, list, counts, n_atoms, w.perm, system_idx, w.sv, table, n_species, cutoff, vs,
+        coef, lam_q, part);
+  k_vl_sum_parts<<<(unsigned)n_systems, 64, 0, st>>>(w.cur, part, width, grad_params);
+  TSB_CHECK_LAUNCH();
+  return TSB_OK;
+}
 
 extern "C" size_t tsb_vlist_workspace_size(int64_t n_atoms, int64_t n_systems) {
   Carver c(nullptr, (size_t)-1);

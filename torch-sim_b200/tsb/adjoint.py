@@ -117,15 +117,16 @@ def _hvp(q, table, v, coef, lam_q, gparams, P, ws=None):
            ws.numel(), L.stream_ptr(q.device))
 
 
-def _vv_step(q, p, f, table, P, inv_m, ws=None):
+def _vv_step(q, p, f, table, P, inv_m, ws=None, force_fn=None):
     """One velocity-Verlet step (same floating-point order as nve.py:118-130:
     p + f * (dt / 2), q + (p * inv_m) * dt, each product and sum rounded on its
-    own), the kick-drift and the closing kick one launch each."""
+    own), the kick-drift and the closing kick one launch each.  ``force_fn(q,
+    table)`` replaces the per-call neighbour search when given."""
     dt, n, st = P.dt, q.shape[0], L.stream_ptr(q.device)
     q_new, p_half = torch.empty_like(q), torch.empty_like(p)
     L.call("tsb_vv_kick_drift", L.ptr(q), L.ptr(p), L.ptr(f), L.ptr(inv_m), dt / 2, dt,
            L.ptr(q_new), L.ptr(p_half), n, st)
-    _, f = forces(q_new, table, P, ws)
+    _, f = force_fn(q_new, table) if force_fn else forces(q_new, table, P, ws)
     p_new = torch.empty_like(p)
     L.call("tsb_vv_kick", L.ptr(p_half), L.ptr(f), dt / 2, L.ptr(p_new), n, st)
     return q_new, p_new, f
@@ -137,6 +138,90 @@ def _adj_kick(lam_p, lam_q, inv_m, P):
            L.stream_ptr(lam_p.device))
 
 
+class _ListOverflow(RuntimeError):
+    pass
+
+
+def _lists_fit(P, skin):
+    """Every periodic plane spacing at least cutoff + skin (the lists' limit)."""
+    inv = torch.linalg.inv(P.cell_row)
+    width = 1.0 / inv.norm(dim=1)  # [S, 3]: spacing of the planes of lattice vector k
+    per = P.pbc.bool()
+    return bool(((width >= P.cutoff + skin) | ~per).all())
+
+
+class _ListForces:
+    """FP64 LJ energy and forces of a trajectory through batched Verlet lists
+    (``tsb_vlist_check`` / ``_build`` / ``_forces``): every call checks the
+    lists and rebuilds the expired systems on the device, so a captured graph
+    needs no host decision.  The pairs inside the cutoff are those of the
+    per-call search; only the order of their sums follows the lists.  A list
+    overflow (more neighbours than ``cap``) is kept in ``sticky`` and read by
+    the host after a graph replay."""
+
+    def __init__(self, P: "TrajectoryProblem", skin: float = 1.0, cap: int = 0):
+        n, ns, dev = P.n_atoms, P.n_systems, P.cell_row.device
+        self.P, self.skin = P, float(skin)
+        rcs = P.cutoff + self.skin
+        counts = torch.bincount(P.system_idx, minlength=ns).double()
+        vol = torch.linalg.det(P.cell_row).abs().clamp_min(1e-30)
+        dens = float((counts / vol).max())
+        self.cap = max(cap, min(4096, int(4.19 * rcs ** 3 * dens * 1.35) + 16))
+        self.list = torch.empty(self.cap * n, dtype=torch.int32, device=dev)
+        self.counts = torch.empty(n, dtype=torch.int32, device=dev)
+        self.flags = torch.zeros(2, dtype=torch.int32, device=dev)
+        self.sticky = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.ws = torch.empty(L.load().tsb_vlist_workspace_size(n, ns), dtype=torch.uint8,
+                              device=dev)
+        self.e = torch.empty(ns, dtype=torch.float64, device=dev)
+        self.scratch = torch.empty(L.load().tsb_vlist_hvp_scratch_size(n, P.n_species),
+                                   dtype=torch.uint8, device=dev)
+        L.call("tsb_vlist_reset", n, ns, L.ptr(self.ws), self.ws.numel(), L.stream_ptr(dev))
+
+    def _update(self, q):
+        P, st = self.P, L.stream_ptr(q.device)
+        n, ns = P.n_atoms, P.n_systems
+        L.call("tsb_vlist_check", L.ptr(q), L.ptr(P.cell_row), L.ptr(P.system_idx), None, n, ns,
+               L.F64, P.cutoff, self.skin, L.ptr(self.flags), L.ptr(self.ws), self.ws.numel(),
+               st)
+        L.call("tsb_vlist_build", L.ptr(q), L.ptr(P.cell_row), L.ptr(P.pbc),
+               L.ptr(P.system_idx), L.ptr(P.species), n, ns, L.F64, P.cutoff, self.skin,
+               L.ptr(self.list), L.ptr(self.counts), self.cap, P.max_sys, L.ptr(self.flags),
+               L.ptr(self.ws), self.ws.numel(), st)
+        torch.maximum(self.sticky, self.flags[1:], out=self.sticky)
+
+    def __call__(self, q, table):
+        P, st = self.P, L.stream_ptr(q.device)
+        n, ns = P.n_atoms, P.n_systems
+        self._update(q)
+        f = torch.empty((n, 3), dtype=torch.float64, device=q.device)
+        L.call("tsb_vlist_forces", L.POT_LJ, L.ptr(table), P.n_species, L.ptr(P.species),
+               L.ptr(self.list), L.ptr(self.counts), L.ptr(q), L.ptr(P.cell_row),
+               L.ptr(P.system_idx), None, n, ns, L.F64, P.cutoff,
+               L.OUT_FORCES | L.MATH_FP64, L.ptr(self.e), L.ptr(f), None, None, None,
+               L.ptr(self.ws), self.ws.numel(), st)
+        return self.e, f
+
+    def hvp(self, q, table, v, coef, lam_q, gparams):
+        """lam_q += coef J_F(q)^T v and the parameter gradients (as ``_hvp``)."""
+        P, st = self.P, L.stream_ptr(q.device)
+        self._update(q)
+        L.call("tsb_vlist_lj_hvp", L.ptr(table), P.n_species, L.ptr(P.species),
+               L.ptr(self.list), L.ptr(self.counts), L.ptr(q), L.ptr(P.cell_row),
+               L.ptr(P.system_idx), P.n_atoms, P.n_systems, P.cutoff, L.ptr(v), float(coef),
+               L.ptr(lam_q), L.ptr(gparams), L.ptr(self.scratch), self.scratch.numel(),
+               L.ptr(self.ws), self.ws.numel(), st)
+
+    def check(self):
+        """Raise _ListOverflow (after growing the list) if any call overflowed."""
+        st = int(self.sticky.item())
+        if st == 0:
+            return
+        if st >= (1 << 30):
+            raise ValueError("adjoint Verlet lists need every cell width >= cutoff + 1 A")
+        raise _ListOverflow(st)
+
+
 class _Graphs:
     """CUDA graphs of the checkpoint segments of one problem.
 
@@ -146,14 +231,16 @@ class _Graphs:
     force / HVP launches and torch element-wise ops) is stream-ordered and
     allocates nothing once its workspace exists, so each part is captured once
     and replayed: one graph launch per segment instead of some forty host calls
-    per step.  The graphs read and write the static buffers below; results are
-    bitwise those of the step-by-step path (forces are recomputed at a segment
-    start, from the same positions, by the same deterministic kernels)."""
+    per step.  The graphs read and write the static buffers below.  Forces come
+    from batched Verlet lists kept across steps and segments (``_ListForces``):
+    the per-call search's pairs, summed in list order, so results agree with the
+    step-by-step path to rounding."""
 
-    def __init__(self, P: TrajectoryProblem, table: torch.Tensor):
+    def __init__(self, P: TrajectoryProblem, table: torch.Tensor, cap: int = 0):
         dev = P.cell_row.device
         n, f64 = P.n_atoms, torch.float64
         self.P = P
+        self.lf = _ListForces(P, cap=cap) if _lists_fit(P, 1.0) else None
         self.table = table.clone().contiguous()
         self.q0 = torch.zeros((n, 3), dtype=f64, device=dev)
         self.p0 = torch.zeros_like(self.q0)
@@ -193,18 +280,22 @@ class _Graphs:
         if length not in self.fwd:
             P = self.P
 
+            fn = self.lf or (lambda q, t: forces(q, t, P, self.ws_pair))
+
             def body():
                 q, p = self.q0, self.p0
-                _, f = forces(q, self.table, P, self.ws_pair)
+                _, f = fn(q, self.table)
                 seg = [q]
                 for k in range(length):
-                    q, p, f = _vv_step(q, p, f, self.table, P, self.inv_m, self.ws_pair)
+                    q, p, f = _vv_step(q, p, f, self.table, P, self.inv_m, force_fn=fn)
                     if k < length - 1:
                         seg.append(q)
                 self.out[length] = (seg, q, p)
 
             self.fwd[length] = self._capture(body)
         self.fwd[length].replay()
+        if self.lf is not None:
+            self.lf.check()
         return self.out[length]
 
     def backward(self, length, first):
@@ -219,11 +310,16 @@ class _Graphs:
                 for k in range(length - 1, -1, -1):
                     _adj_kick(self.lam_p, self.lam_q, self.inv_m, P)
                     coef = P.dt / 2 if (first and k == 0) else P.dt
-                    _hvp(seg[k], self.table, self.lam_p, coef, self.lam_q, self.gpar, P,
-                         self.ws_adj)
+                    if self.lf is not None:
+                        self.lf.hvp(seg[k], self.table, self.lam_p, coef, self.lam_q, self.gpar)
+                    else:
+                        _hvp(seg[k], self.table, self.lam_p, coef, self.lam_q, self.gpar, P,
+                             self.ws_adj)
 
             self.bwd[key] = self._capture(body, keep=(self.lam_q, self.lam_p, self.gpar))
         self.bwd[key].replay()
+        if self.lf is not None:
+            self.lf.check()
 
 
 def _graphs_for(P: TrajectoryProblem, table: torch.Tensor) -> _Graphs:
@@ -234,6 +330,17 @@ def _graphs_for(P: TrajectoryProblem, table: torch.Tensor) -> _Graphs:
     else:
         G.table.copy_(table)
     return G
+
+
+def _retry_on_overflow(fn, P, table):
+    """Run ``fn``; when a Verlet list overflowed, rebuild the graphs with a larger
+    list and run it again."""
+    for _ in range(4):
+        try:
+            return fn()
+        except _ListOverflow as e:
+            P.__dict__["_graphs"] = _Graphs(P, table, cap=int(int(e.args[0]) * 1.2) + 8)
+    raise RuntimeError("adjoint: Verlet list kept overflowing")
 
 
 def _integrate_graphs(q0, p0, table, P, keep_checkpoints):
@@ -255,7 +362,8 @@ def integrate(q0, p0, table, P: TrajectoryProblem, keep_checkpoints=True, use_gr
     the checkpoints {step: (q, p)} every ``P.checkpoint_every`` steps).  With
     ``use_graphs`` each checkpoint segment replays one CUDA graph."""
     if use_graphs and q0.is_cuda and P.n_steps > 0:
-        return _integrate_graphs(q0, p0, table, P, keep_checkpoints)
+        return _retry_on_overflow(
+            lambda: _integrate_graphs(q0, p0, table, P, keep_checkpoints), P, table)
     inv_m = (1.0 / P.masses).contiguous()
     q, p = q0.contiguous(), p0.contiguous()
     _, f = forces(q, table, P)
@@ -294,7 +402,8 @@ def loss_and_grad(sigma, epsilon, q0, p0, P: TrajectoryProblem, use_graphs=True)
     loss, h = loss_of(qT, P)
     lam_q = _hist_grad(qT, 2.0 * (h - P.target), P)
     if use_graphs and q0.is_cuda and P.n_steps > 0:
-        lam_q, lam_p, gpar = _adjoint_graphs(table, ckpt, lam_q, P)
+        lam_q, lam_p, gpar = _retry_on_overflow(
+            lambda: _adjoint_graphs(table, ckpt, lam_q, P), P, table)
         g = gpar.sum(0)
         gs = g[..., 0] + g[..., 0].T - torch.diag(torch.diagonal(g[..., 0]))
         ge = g[..., 1] + g[..., 1].T - torch.diag(torch.diagonal(g[..., 1]))
