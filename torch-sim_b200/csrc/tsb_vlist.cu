@@ -375,7 +375,7 @@ __global__ void k_vl_frame(const P *pos, const P *cell_row, const int64_t *sys,
 __device__ __forceinline__ int vl_species(double w) { return tag_species(w); }
 __device__ __forceinline__ int vl_species(float w) { return __float_as_int(w); }
 
-template <int POT, class R, class P>
+template <int POT, class R, class P, int LANES>
 __global__ void __launch_bounds__(kVlBlock)
     k_vl_forces(const double4 *__restrict__ wpos, const float4 *__restrict__ wpos32,
                 const uint32_t *__restrict__ list, const int32_t *__restrict__ cnt, int64_t n,
@@ -411,20 +411,29 @@ __global__ void __launch_bounds__(kVlBlock)
     shifts = sv;
     wg = wpos;
   }
-  const int64_t p0 = (int64_t)blockIdx.x * blockDim.x;
+  // LANES lanes per slot (small batches: more threads in flight; each lane takes
+  // every LANES-th entry and a fixed butterfly sums the lanes), else one thread
+  const int64_t p0 = (int64_t)blockIdx.x * (blockDim.x / LANES);
   const int64_t s_lo = sys[perm[p0]];
-  const int64_t s_hi = sys[perm[min(p0 + (int64_t)blockDim.x, n) - 1]];
+  const int64_t s_hi = sys[perm[min(p0 + (int64_t)(blockDim.x / LANES), n) - 1]];
   const int n_st = (int)min(s_hi - s_lo + 1, (int64_t)kVlSmemSys);
   for (int k = threadIdx.x; k < 81 * n_st; k += blockDim.x) ssv[k] = shifts[81 * s_lo + k];
   if constexpr (F32)
     for (int k = threadIdx.x; k < n_st; k += blockDim.x) sband[k] = band[s_lo + k];
   __syncthreads();
-  const int64_t p = p0 + threadIdx.x;
-  if (p >= n) return;
-  const int64_t i = perm[p];
-  const int64_t s = sys[i];
-  if (active && !active[s]) return;
-  const Pos4 wi = wg[p];
+  const int64_t p = p0 + threadIdx.x / LANES;
+  const int lane = threadIdx.x % LANES;
+  // a group whose slot is past the end or inactive still takes part in the
+  // lane sums (with no entries) and leaves before writing
+  bool valid = p < n;
+  int64_t i = 0, s = s_lo;
+  if (valid) {
+    i = perm[p];
+    s = sys[i];
+    valid = !active || active[s];
+  }
+  if (LANES == 1 && !valid) return;
+  const Pos4 wi = wg[valid ? p : p0];
   const int si = min(max(vl_species(wi.w), 0), ns_species - 1);
   const PairPrm<R> *row = prm + si * ns_species;
   const double *rc2row = prc2 + si * ns_species;
@@ -434,7 +443,7 @@ __global__ void __launch_bounds__(kVlBlock)
   float bnd = 0.f;
   if constexpr (F32) bnd = staged ? sband[s - s_lo] : band[s];
   const bool want_vir = flags & (TSB_OUT_STRESS | TSB_OUT_STRESSES);
-  const int c = cnt[p];
+  const int c = valid ? cnt[p] : 0;
   double fx = 0.0, fy = 0.0, fz = 0.0, ei = 0.0;
   double vxx = 0, vyy = 0, vzz = 0, vyz = 0, vxz = 0, vxy = 0;
   // one entry E with neighbour frame position WJ.  FP64 path: FP64 displacement
@@ -499,10 +508,30 @@ __global__ void __launch_bounds__(kVlBlock)
       }                                                                                      \
     }                                                                                        \
   }
+  const uint32_t *lp = list + p;
+  if constexpr (LANES > 1) {
+    for (int k = lane; k < c; k += LANES) {
+      const uint32_t e = lp[(size_t)k * n];
+      const Pos4 wj = wg[e >> 5];
+      TSB_VLPAIR(e, wj)
+    }
+    fx = group_sum<LANES>(fx);
+    fy = group_sum<LANES>(fy);
+    fz = group_sum<LANES>(fz);
+    ei = group_sum<LANES>(ei);
+    if (want_vir) {
+      vxx = group_sum<LANES>(vxx);
+      vyy = group_sum<LANES>(vyy);
+      vzz = group_sum<LANES>(vzz);
+      vyz = group_sum<LANES>(vyz);
+      vxz = group_sum<LANES>(vxz);
+      vxy = group_sum<LANES>(vxy);
+    }
+    if (!valid || lane != 0) return;
+  } else {
   // four entries per iteration; the next four list words are loaded one
   // iteration ahead so their DRAM latency overlaps the current gathers and math
   int k = 0;
-  const uint32_t *lp = list + p;
   uint32_t e0 = 0, e1 = 0, e2 = 0, e3 = 0;
   if (c >= 4) {
     e0 = lp[0];
@@ -534,6 +563,7 @@ __global__ void __launch_bounds__(kVlBlock)
     const uint32_t e = lp[(size_t)k * n];
     const Pos4 wj = wg[e >> 5];
     TSB_VLPAIR(e, wj)
+  }
   }
 #undef TSB_VLPAIR
   if (flags & TSB_OUT_FORCES) {
@@ -606,9 +636,15 @@ static void vl_launch(VlWork &w, const uint32_t *list, const int32_t *counts, in
                       const int64_t *sys, const double *table, int nsp, double cutoff,
                       int flags, P *forces, P *energies, P *stresses, const uint8_t *active,
                       cudaStream_t st) {
-  k_vl_forces<POT, R, P><<<grid_for(n, kVlBlock), kVlBlock, 0, st>>>(
-      w.wpos, w.wpos32, list, counts, n, w.perm, sys, w.sv, w.svf, w.band, table, nsp, cutoff,
-      flags, forces, energies, stresses, w.cur, w.e_half, w.vir_half, active);
+  if (n <= kGroupSearchMaxAtoms)
+    k_vl_forces<POT, R, P, kSearchGroup><<<grid_for(kSearchGroup * n, kVlBlock), kVlBlock, 0,
+                                            st>>>(
+        w.wpos, w.wpos32, list, counts, n, w.perm, sys, w.sv, w.svf, w.band, table, nsp,
+        cutoff, flags, forces, energies, stresses, w.cur, w.e_half, w.vir_half, active);
+  else
+    k_vl_forces<POT, R, P, 1><<<grid_for(n, kVlBlock), kVlBlock, 0, st>>>(
+        w.wpos, w.wpos32, list, counts, n, w.perm, sys, w.sv, w.svf, w.band, table, nsp,
+        cutoff, flags, forces, energies, stresses, w.cur, w.e_half, w.vir_half, active);
 }
 
 template <class P>
