@@ -418,24 +418,30 @@ __global__ void __launch_bounds__(kBlock)
   for (int c0 = 0; c0 < count; c0 += blockDim.x) {
     const int a = c0 + threadIdx.x;
     const int lb = a < count ? (small ? (int)lbin_s[a] : lbin_g[a]) : -1;
+    // the atom's tagged position is loaded before the warp-by-warp slot
+    // assignment, so the serialised part touches shared memory only
+    const int64_t i = start + a;
+    double4 wv4 = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (lb >= 0) {
+      wv4 = b.wpos[i];
+      const unsigned long long hi = species ? (unsigned long long)(uint32_t)species[i] : 0ull;
+      wv4.w = __longlong_as_double((long long)((hi << 32) | (uint32_t)i));
+    }
+    int at = 0, rank = 0;
     for (int wv = 0; wv < (int)(blockDim.x >> 5); ++wv) {
       if (warp == wv) {
         const unsigned peers = __match_any_sync(0xffffffffu, lb);
-        const int rank = __popc(peers & lt);
-        const int at = lb >= 0 ? cur[lb] : 0;
+        rank = __popc(peers & lt);
+        at = lb >= 0 ? cur[lb] : 0;
         __syncwarp();
-        if (lb >= 0) {
-          if (rank == 0) cur[lb] = at + __popc(peers);
-          const int64_t slot = start + at + rank, i = start + a;
-          double4 w = b.wpos[i];
-          const unsigned long long hi =
-              species ? (unsigned long long)(uint32_t)species[i] : 0ull;
-          w.w = __longlong_as_double((long long)((hi << 32) | (uint32_t)i));
-          b.spos[slot] = w;
-          b.sidx[slot] = (int32_t)i;
-        }
+        if (lb >= 0 && rank == 0) cur[lb] = at + __popc(peers);
       }
       __syncthreads();
+    }
+    if (lb >= 0) {
+      const int64_t slot = start + at + rank;
+      b.spos[slot] = wv4;
+      b.sidx[slot] = (int32_t)i;
     }
   }
 }
