@@ -90,7 +90,7 @@ __global__ void k_verlet_frame(const P *pos, const double *ref, const int32_t *w
 }
 
 template <int POT, class P>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
     k_verlet_forces(const double4 *__restrict__ wpos, const uint32_t *__restrict__ list,
                     const int32_t *__restrict__ cnt, int64_t n, const double *__restrict__ cell,
                     const double *__restrict__ table, int ns_species, double cutoff,
@@ -118,7 +118,8 @@ __global__ void __launch_bounds__(256)
     const int c = cnt[i];
     double fx = 0.0, fy = 0.0, fz = 0.0;
     // one pair (entry E, neighbour position WJ): FP64 displacement, cutoff test,
-    // force and virial accumulation; FP32 pair function of r^2
+    // force and virial accumulation; FP32 pair function of r^2, evaluated for
+    // every entry and masked beyond the cutoff (no divergent branch)
 #define TSB_VPAIR(E, WJ)                                                                     \
   {                                                                                          \
     const int code = (int)((E) & 31u);                                                       \
@@ -127,9 +128,12 @@ __global__ void __launch_bounds__(256)
     const double dz = (WJ).z - wi.z + sv[3 * code + 2];                                      \
     const int sj = (int)__double_as_longlong((WJ).w);                                        \
     const double d2 = dx * dx + dy * dy + dz * dz;                                           \
-    if (d2 < prc2[si * ns_species + sj]) {                                                   \
+    {                                                                                        \
+      const bool in_ = d2 < prc2[si * ns_species + sj];                                      \
       float ep, fr;                                                                          \
       pair_eval_fast<POT>(row[sj], (float)d2, ep, fr);                                       \
+      fr = in_ ? fr : 0.f;                                                                   \
+      ep = in_ ? ep : 0.f;                                                                   \
       const double gr = (double)fr;                                                          \
       const double gx = gr * dx, gy = gr * dy, gz = gr * dz;                                 \
       fx -= gx;                                                                              \
@@ -146,22 +150,41 @@ __global__ void __launch_bounds__(256)
       }                                                                                      \
     }                                                                                        \
   }
-    // four entries per iteration: their list words and positions load together
+    // four entries per iteration; the next four list words are loaded one
+    // iteration ahead so their DRAM latency overlaps the current gathers and math
     int k = 0;
+    const uint32_t *lp = list + i;
+    uint32_t e0 = 0, e1 = 0, e2 = 0, e3 = 0;
+    if (c >= 4) {
+      e0 = lp[0];
+      e1 = lp[(size_t)n];
+      e2 = lp[(size_t)2 * n];
+      e3 = lp[(size_t)3 * n];
+    }
     for (; k + 4 <= c; k += 4) {
-      const uint32_t e0 = list[(size_t)k * n + i], e1 = list[(size_t)(k + 1) * n + i];
-      const uint32_t e2 = list[(size_t)(k + 2) * n + i], e3 = list[(size_t)(k + 3) * n + i];
+      uint32_t f0 = 0, f1 = 0, f2 = 0, f3 = 0;
+      if (k + 8 <= c) {
+        const uint32_t *q = lp + (size_t)(k + 4) * n;
+        f0 = q[0];
+        f1 = q[(size_t)n];
+        f2 = q[(size_t)2 * n];
+        f3 = q[(size_t)3 * n];
+      }
       const double4 w0 = wpos[e0 >> 5], w1 = wpos[e1 >> 5];
       const double4 w2 = wpos[e2 >> 5], w3 = wpos[e3 >> 5];
       TSB_VPAIR(e0, w0)
       TSB_VPAIR(e1, w1)
       TSB_VPAIR(e2, w2)
       TSB_VPAIR(e3, w3)
+      e0 = f0;
+      e1 = f1;
+      e2 = f2;
+      e3 = f3;
     }
     for (; k < c; ++k) {
-      const uint32_t e0 = list[(size_t)k * n + i];
-      const double4 w0 = wpos[e0 >> 5];
-      TSB_VPAIR(e0, w0)
+      const uint32_t e = lp[(size_t)k * n];
+      const double4 wj = wpos[e >> 5];
+      TSB_VPAIR(e, wj)
     }
 #undef TSB_VPAIR
     forces[3 * i] = (P)fx;
