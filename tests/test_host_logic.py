@@ -89,3 +89,77 @@ def test_pbc_rows_accepts_every_reference_form():
     assert L.pbc_rows(True, 4, "cpu").is_contiguous()
     with pytest.raises(ValueError):
         L.pbc_rows(torch.ones(5, dtype=torch.bool), 4, "cpu")
+
+
+def test_max_system_atoms_hint_is_cached_per_system_idx_version():
+    from tsb import _lib as L
+
+    sysi = torch.tensor([0, 0, 0, 1, 1, 2, 2, 2, 2], dtype=torch.int64)
+    assert L.max_system_atoms(sysi, 3) == 4
+    assert L.max_system_atoms(sysi, 4) == 4  # an empty trailing system
+    sysi[4] = 0  # in place: a new version, a new count
+    assert L.max_system_atoms(sysi, 3) == 4
+    sysi[:] = 1
+    assert L.max_system_atoms(sysi, 3) == 9
+    assert L.max_system_atoms(torch.zeros(0, dtype=torch.int64), 1) == 0
+
+
+def test_adjoint_list_width_rule():
+    """Verlet lists inside the adjoint graphs need every periodic plane spacing
+    >= cutoff + skin; an open axis does not count."""
+    from tsb import adjoint
+
+    class P:
+        cutoff = 8.5
+
+    c = torch.eye(3, dtype=torch.float64)
+    hexa = torch.tensor([[10.0, 0, 0], [5.0, 8.66, 0], [0, 0, 10.0]], dtype=torch.float64)
+    P.cell_row = torch.stack([15.78 * c, hexa])
+    P.pbc = torch.ones((2, 3), dtype=torch.uint8)
+    assert not adjoint._lists_fit(P, 1.0)  # the hexagonal cell's a-b planes are 8.66 A apart
+    P.pbc[1, :2] = 0
+    assert adjoint._lists_fit(P, 1.0)
+    P.cell_row = torch.stack([15.78 * c, 15.78 * c])
+    P.pbc = torch.ones((2, 3), dtype=torch.uint8)
+    assert adjoint._lists_fit(P, 1.0) and not adjoint._lists_fit(P, 7.5)
+
+
+def test_adjoint_overflow_retry_regrows_and_gives_up():
+    from tsb import adjoint
+
+    made = []
+
+    class FakeGraphs:
+        def __init__(self, P, table, cap=0):
+            made.append(cap)
+
+    class P:
+        pass
+
+    P = P()
+    calls = {"n": 0}
+
+    def flaky():
+        calls["n"] += 1
+        if calls["n"] < 3:
+            raise adjoint._ListOverflow(100 * calls["n"])
+        return "ok"
+
+    orig = adjoint._Graphs
+    adjoint._Graphs = FakeGraphs
+    try:
+        assert adjoint._retry_on_overflow(flaky, P, None) == "ok"
+        assert made == [128, 248]  # 1.2 x the reported count + 8
+        made.clear()
+
+        def always():
+            raise adjoint._ListOverflow(64)
+
+        try:
+            adjoint._retry_on_overflow(always, P, None)
+            raise AssertionError("no error")
+        except RuntimeError as e:
+            assert "overflowing" in str(e)
+        assert len(made) == 4
+    finally:
+        adjoint._Graphs = orig
