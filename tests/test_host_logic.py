@@ -163,3 +163,32 @@ def test_adjoint_overflow_retry_regrows_and_gives_up():
         assert len(made) == 4
     finally:
         adjoint._Graphs = orig
+
+
+def test_fp32_distance_band_bounds_the_rounding():
+    """The mixed-precision Verlet-list path decides a pair from FP32 positions
+    unless its FP32 r^2 lies within a band of the cutoff.  The band rests on the
+    bound |r2_f32 - r2| <= 2^-24 (17.3 B r + 6.5 r^2) for coordinates and shifts
+    of magnitude <= B and r near the cutoff; check it on random pairs laid out as
+    the kernel forms them ((x_j - x_i) + shift, then the sum of squares)."""
+    rng = np.random.default_rng(0)
+    u = 2.0 ** -24
+    worst = 0.0
+    for B, rc in ((20.0, 2.5), (60.0, 8.5), (800.0, 8.5), (300.0, 6.0)):
+        m = 200_000
+        xi = rng.uniform(-B / 2, B / 2, (m, 3))
+        d = rng.normal(size=(m, 3))
+        d *= (rc * rng.uniform(0.98, 1.02, m) / np.linalg.norm(d, axis=1))[:, None]
+        shift = rng.choice([-1.0, 0.0, 1.0], (m, 3)) * (B / 2)
+        xj = xi + d - shift  # so that (xj - xi) + shift = d exactly in real arithmetic
+        ok = np.all(np.abs(xj) <= B, axis=1)
+        xi, xj, shift, d = xi[ok], xj[ok], shift[ok], d[ok]
+        r2 = np.sum(((xj - xi) + shift) ** 2, axis=1)  # FP64 reference
+        f = np.float32
+        a = (xj.astype(f) - xi.astype(f)) + shift.astype(f)
+        r2f = (a[:, 0] * a[:, 0] + a[:, 1] * a[:, 1]) + a[:, 2] * a[:, 2]
+        bound = u * (17.3 * B * rc + 6.5 * rc * rc)
+        ratio = np.abs(r2f.astype(np.float64) - r2).max() / bound
+        worst = max(worst, ratio)
+        assert ratio <= 1.0, (B, rc, ratio)
+    assert worst > 0.01  # the test exercises rounding at all
