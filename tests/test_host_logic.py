@@ -192,3 +192,23 @@ def test_fp32_distance_band_bounds_the_rounding():
         worst = max(worst, ratio)
         assert ratio <= 1.0, (B, rc, ratio)
     assert worst > 0.01  # the test exercises rounding at all
+
+
+def test_histogram_window_drops_only_negligible_terms():
+    """The loss histogram adds a pair only to the bins within 12 widths of its
+    distance; every dropped term is below exp(-72) of the pair's peak term, far
+    under the FP64 rounding of the bins it does reach."""
+    rng = np.random.default_rng(1)
+    r_max, nb, w = 8.0, 64, 0.05
+    bw = r_max / nb
+    c = (np.arange(nb) + 0.5) * bw
+    r = rng.uniform(0.5, r_max, 20000)
+    g = np.exp(-((r[:, None] - c[None, :]) ** 2) / (2 * w * w))
+    full = g.sum(0)
+    k0 = np.maximum(0, np.ceil((r - 12 * w) / bw - 0.5)).astype(int)
+    k1 = np.minimum(nb - 1, np.floor((r + 12 * w) / bw - 0.5)).astype(int)
+    kk = np.arange(nb)[None, :]
+    win = np.where((kk >= k0[:, None]) & (kk <= k1[:, None]), g, 0.0).sum(0)
+    dropped = np.where((kk < k0[:, None]) | (kk > k1[:, None]), g, 0.0)
+    assert dropped.max() <= np.exp(-72.0)
+    np.testing.assert_allclose(win, full, rtol=1e-15, atol=1e-28)
