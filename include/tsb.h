@@ -479,7 +479,11 @@ int tsb_npt_langevin_iso_post(void *momenta, const void *masses, const void *for
  * Verlet list (cutoff + skin, rebuilt on the device when an atom moved more
  * than skin/2) in shared memory, and steps it without leaving the kernel.
  * positions/momenta/forces are float64 [N,3] in/out; energy [S] float64 out
- * (potential energy after the last step); n_rebuilds [S] int32 out (optional).
+ * (potential energy after the last step); stress [S,3,3] float64 out
+ * (optional, NULL skips it): the stress after the last step, -W/V with the
+ * virial W = sum over pairs of r (x) f (pair_potential.py:200-274); per-atom
+ * energy and virial terms are summed in FP64 in a fixed order;
+ * n_rebuilds [S] int32 out (optional).
  * `order` [S] int32 (optional) is the order in which CTAs pick systems
  * (largest first balances the tail).  A system whose images or neighbours do
  * not fit the shared-memory tables at the requested skin is rebuilt with a
@@ -488,7 +492,9 @@ int tsb_npt_langevin_iso_post(void *momenta, const void *masses, const void *for
  * TSB_ERR_UNSUPPORTED for a system that does not fit even with zero skin
  * (its positions and momenta are left unchanged, its forces are not);
  * status[1] its index, status[2] which table (1 images, 2 neighbour slots),
- * status[3] the size that did not fit.  While a system runs, its rows of
+ * status[3] the size that did not fit; or TSB_ERR_INVALID_ARG with status[1]
+ * an atom whose system index lies outside [0, n_systems), status[2] = 3 and
+ * status[3] that index (the atom is left out of every system).  While a system runs, its rows of
  * `forces` hold FP64 positions (the kernel decides whether a pair is inside
  * the cutoff on them when FP32 rounding could flip the decision); the final
  * forces are written over them.
@@ -506,7 +512,7 @@ int tsb_fused_md(int integrator, int potential, const double *table, int n_speci
                  const int32_t *order, double cutoff, double skin, int64_t n_steps,
                  const double *dt_sys, const double *kT_sys, const double *gamma_sys,
                  uint64_t seed, uint64_t counter, uint64_t *counter_dev, double *energy,
-                 int32_t *n_rebuilds, int32_t *status, void *workspace,
+                 double *stress, int32_t *n_rebuilds, int32_t *status, void *workspace,
                  size_t workspace_bytes, void *stream);
 
 /* ---- fused persistent batched MD with a Nose-Hoover chain or V-rescale ----
@@ -529,7 +535,7 @@ int tsb_fused_md_nvt(int thermostat, int potential, const double *table, int n_s
                      double *chain_xi, double *chain_pxi, double *chain_Q, double *chain_ke,
                      const double *chain_dt, int chain_length, int chain_steps, int sy_steps,
                      uint64_t seed, uint64_t counter, uint64_t *counter_dev, double *energy,
-                     int32_t *n_rebuilds, int32_t *status, void *workspace,
+                     double *stress, int32_t *n_rebuilds, int32_t *status, void *workspace,
                      size_t workspace_bytes, void *stream);
 
 /* ---- fused persistent batched MD, every integrator, with trajectory frames ----
@@ -551,7 +557,7 @@ int tsb_fused_md_ex(int integrator, int potential, const double *table, int n_sp
                     int chain_length, int chain_steps, int sy_steps, uint64_t seed,
                     uint64_t counter, uint64_t *counter_dev, float *frame_x, double *frame_e,
                     int64_t report_every, int64_t n_frames, double *energy,
-                    int32_t *n_rebuilds, int32_t *status, void *workspace,
+                    double *stress, int32_t *n_rebuilds, int32_t *status, void *workspace,
                     size_t workspace_bytes, void *stream);
 
 /* ---- allocation-free fused MD -------------------------------------------

@@ -70,6 +70,7 @@ def test_static_entry_matches_workspace_entry_on_two_calls():
             if name == "tsb_fused_md":
                 a = list(args)
                 a.insert(22, None)  # counter_dev: none, the counter is passed by value
+                a.insert(24, None)  # stress: not requested
                 rc = lib.tsb_fused_md(*a, L.ptr(ws), ws.numel(), stream)
             else:
                 rc = lib.tsb_fused_md_static(*args, stream)
@@ -105,3 +106,76 @@ def test_static_entry_rejects_too_many_systems():
     assert rc == L.TSB_ERR_CAPACITY
     torch.cuda.synchronize()
     assert torch.equal(x, md.positions)  # nothing was launched
+
+
+def test_static_entry_allocates_nothing():
+    """After a first call on the device (which looks up the array's address),
+    further calls leave the device's free memory and torch's allocator untouched."""
+    from tsb import _lib as L
+
+    lib = L.load()
+    md, m = _setup(n_sys=12, seed=5)
+    dev = md.device
+    x, p, f = md.positions.clone(), md.momenta.clone(), md.forces.clone()
+    energy = torch.zeros(md.n_systems, dtype=torch.float64, device=dev)
+    status = torch.zeros(4, dtype=torch.int32, device=dev)
+    args, keep = _args(md, m, x, p, f, energy, None, status, 10, 0)
+    stream = L.stream_ptr(dev)
+    assert lib.tsb_fused_md_static(*args, stream) == L.TSB_OK  # warm-up
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(dev)
+    alloc0, reserved0 = torch.cuda.memory_allocated(dev), torch.cuda.memory_reserved(dev)
+    for _ in range(3):
+        assert lib.tsb_fused_md_static(*args, stream) == L.TSB_OK
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(dev)
+    assert free1 == free0
+    assert torch.cuda.memory_allocated(dev) == alloc0
+    assert torch.cuda.memory_reserved(dev) == reserved0
+    assert status.tolist()[0] == 0
+
+
+def test_static_entry_reports_a_bad_system_index_and_recovers():
+    """A system index outside [0, n_systems) is reported in the status word and
+    nothing is written outside the fixed array; the next valid call on the same
+    array still equals the workspace entry."""
+    from tsb import _lib as L
+
+    lib = L.load()
+    md, m = _setup(n_sys=6, seed=8)
+    dev = md.device
+    stream = L.stream_ptr(dev)
+    bad = md.system_idx.clone()
+    bad[-1] = md.n_systems  # one past the last system (still sorted)
+    x, p, f = md.positions.clone(), md.momenta.clone(), md.forces.clone()
+    energy = torch.zeros(md.n_systems, dtype=torch.float64, device=dev)
+    status = torch.zeros(4, dtype=torch.int32, device=dev)
+    args, keep = _args(md, m, x, p, f, energy, None, status, 5, 0)
+    args = list(args)
+    args[10] = L.ptr(bad)
+    assert lib.tsb_fused_md_static(*args, stream) == L.TSB_OK
+    torch.cuda.synchronize()
+    st = status.tolist()
+    assert st[0] == L.TSB_ERR_INVALID_ARG and st[2] == 3 and st[1] == md.n_atoms - 1, st
+    # valid calls afterwards: static == workspace entry, bitwise
+    outs = []
+    for name in ("tsb_fused_md_static", "tsb_fused_md"):
+        x, p, f = md.positions.clone(), md.momenta.clone(), md.forces.clone()
+        energy = torch.zeros(md.n_systems, dtype=torch.float64, device=dev)
+        status = torch.full((4,), -7, dtype=torch.int32, device=dev)
+        args, keep = _args(md, m, x, p, f, energy, None, status, 20, 0)
+        if name == "tsb_fused_md":
+            ws = torch.empty(lib.tsb_fused_workspace_size(md.n_atoms, md.n_systems),
+                             dtype=torch.uint8, device=dev)
+            a = list(args)
+            a.insert(22, None)
+            a.insert(24, None)
+            rc = lib.tsb_fused_md(*a, L.ptr(ws), ws.numel(), stream)
+        else:
+            rc = lib.tsb_fused_md_static(*args, stream)
+        assert rc == L.TSB_OK
+        torch.cuda.synchronize()
+        assert status.tolist()[0] == 0
+        outs.append((x, p, energy))
+    for u, v in zip(*outs):
+        torch.testing.assert_close(u, v, rtol=0.0, atol=0.0)

@@ -95,6 +95,9 @@ struct FusedArgs {
   float *frame_x;
   double *frame_e;
   int64_t rep_every, n_frames, n_atoms_total;
+  // per-system stress [S, 3, 3] at the last step (optional): -W / V with the
+  // virial W = sum over pairs of r (x) f, accumulated in FP64
+  double *stress;
 };
 
 // per-system geometry, computed by thread 0 into shared memory
@@ -120,6 +123,9 @@ struct FusedGeom {
   int nbins;
   int n, tpa, ok;
   int64_t start;
+  // potential energy and virial (xx, yy, zz, yz, xz, xy) of the system at the
+  // last energy step, FP64 sums in a fixed order (thread 0)
+  double esum7[7];
 };
 
 // Margins of the image region, bins, FP32 error bounds and core radii for the
@@ -239,6 +245,21 @@ __device__ inline double block_sum_to0(double v, double *sh) {
   if (threadIdx.x == 0)
     for (int w = 0; w < kFusedThreads / 32; ++w) t += sh[w];
   return t;
+}
+
+// Warp sum of one FP64 value (fixed order), stored by lane 0 into sh[warp]
+__device__ __forceinline__ void warp_sum_store(double t, double *sh) {
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = t;
+}
+
+// Thread 0: out[c] = sum over warps of sh[c][warp], c < 7 (fixed order)
+__device__ __noinline__ void warps_sum7(const double (*sh)[kFusedThreads / 32], double *out) {
+  for (int c = 0; c < 7; ++c) {
+    double t = 0.0;
+    for (int w = 0; w < kFusedThreads / 32; ++w) t += sh[c][w];
+    out[c] = t;
+  }
 }
 
 // FP32 standard normals for the O-step (Philox4x32-10 + Box-Muller).
@@ -383,6 +404,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
   __shared__ int s_scan[33];
   __shared__ int s_work;
   __shared__ double s_red[kFusedThreads / 32];
+  __shared__ double s_red7[7][kFusedThreads / 32];
 
   const int tid = threadIdx.x;
   const int nsp2 = A.n_species * A.n_species;
@@ -452,6 +474,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       if (g.n <= 0) {
         g.ok = 0;
         A.energy[s] = 0.0;
+        if (A.stress)
+          for (int k = 0; k < 9; ++k) A.stress[9 * s + k] = 0.0;
         if (A.n_rebuilds) A.n_rebuilds[s] = 0;
       } else if (g.n > kFusedMaxAtoms || !rep_ok) {
         g.ok = 0;
@@ -490,7 +514,6 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     int gbeg = 0, gcnt = 0;            // the owned atom's ghost slots [gbeg, gbeg + gcnt)
     int ncore = 0, nshell = 0, rebuilds = 0;
     bool failed = false;
-    float ei = 0.0f;
     float yb0 = 0.f, yb1 = 0.f, yb2 = 0.f;  // wrapped position at the build (FP32)
 
     // ------------------------------------------------------------- rebuild
@@ -686,6 +709,17 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     // Four list entries per iteration, branch-free (out-of-range pairs are
     // evaluated and masked), so the loads and the math of the four pairs
     // overlap.  Core pairs need no cutoff test.
+  // pair virial fr d (x) d (the same for d and -d), FP32 products summed in FP64
+#define TSB_VIR1(FR, DX, DY, DZ)                                                             \
+  {                                                                                          \
+    const float tx_ = (FR) * (DX), ty_ = (FR) * (DY), tz_ = (FR) * (DZ);                     \
+    vxx += (double)(tx_ * (DX));                                                             \
+    vyy += (double)(ty_ * (DY));                                                             \
+    vzz += (double)(tz_ * (DZ));                                                             \
+    vyz += (double)(ty_ * (DZ));                                                             \
+    vxz += (double)(tx_ * (DZ));                                                             \
+    vxy += (double)(tx_ * (DY));                                                             \
+  }
 #define TSB_PAIR_CORE(Q, WITH_E)                                                             \
   {                                                                                          \
     const float4 q = (Q);                                                                    \
@@ -697,7 +731,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     fx -= fr * rx;                                                                           \
     fy -= fr * ry;                                                                           \
     fz -= fr * rz;                                                                           \
-    if (WITH_E) en += ep;                                                                    \
+    if (WITH_E) {                                                                            \
+      en += (double)ep;                                                                      \
+      TSB_VIR1(fr, rx, ry, rz)                                                               \
+    }                                                                                        \
   }
 #define TSB_PAIR_SHELL(Q, E, WITH_E)                                                         \
   {                                                                                          \
@@ -715,7 +752,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     fx -= fr * rx;                                                                           \
     fy -= fr * ry;                                                                           \
     fz -= fr * rz;                                                                           \
-    if (WITH_E) en += in_ ? ep : 0.f;                                                        \
+    if (WITH_E) {                                                                            \
+      en += in_ ? (double)ep : 0.0;                                                          \
+      TSB_VIR1(fr, rx, ry, rz)                                                               \
+    }                                                                                        \
   }
   // two list entries at once (FP32x2); displacement xi - q so that the force
   // accumulates as f += fr * d
@@ -743,11 +783,16 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     f2x = __ffma2_rn(fr, dx, f2x);                                                           \
     f2y = __ffma2_rn(fr, dy, f2y);                                                           \
     f2z = __ffma2_rn(fr, dz, f2z);                                                           \
-    if (WITH_E) en += e2.x + e2.y;                                                           \
+    if (WITH_E) {                                                                            \
+      en += (double)e2.x + (double)e2.y;                                                     \
+      TSB_VIR1(fr.x, dx.x, dy.x, dz.x)                                                       \
+      TSB_VIR1(fr.y, dx.y, dy.y, dz.y)                                                       \
+    }                                                                                        \
   }
 #define TSB_FORCES(WITH_E)                                                                   \
   {                                                                                          \
-    float fx = 0.f, fy = 0.f, fz = 0.f, en = 0.f;                                            \
+    float fx = 0.f, fy = 0.f, fz = 0.f;                                                      \
+    double en = 0.0, vxx = 0.0, vyy = 0.0, vzz = 0.0, vyz = 0.0, vxz = 0.0, vxy = 0.0;        \
     if (own) {                                                                               \
       const float4 xi = s_ext[a];                                                            \
       const float band_ = g.band;                                                            \
@@ -831,12 +876,33 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       fx += __shfl_xor_sync(0xffffffffu, fx, o);                                             \
       fy += __shfl_xor_sync(0xffffffffu, fy, o);                                             \
       fz += __shfl_xor_sync(0xffffffffu, fz, o);                                             \
-      if (WITH_E) en += __shfl_xor_sync(0xffffffffu, en, o);                                 \
+      if (WITH_E) {                                                                          \
+        en += __shfl_xor_sync(0xffffffffu, en, o);                                           \
+        vxx += __shfl_xor_sync(0xffffffffu, vxx, o);                                         \
+        vyy += __shfl_xor_sync(0xffffffffu, vyy, o);                                         \
+        vzz += __shfl_xor_sync(0xffffffffu, vzz, o);                                         \
+        vyz += __shfl_xor_sync(0xffffffffu, vyz, o);                                         \
+        vxz += __shfl_xor_sync(0xffffffffu, vxz, o);                                         \
+        vxy += __shfl_xor_sync(0xffffffffu, vxy, o);                                         \
+      }                                                                                      \
     }                                                                                        \
     F0 = fx;                                                                                 \
     F1 = fy;                                                                                 \
     F2 = fz;                                                                                 \
-    if (WITH_E) ei = en;                                                                     \
+    if (WITH_E) {                                                                            \
+      /* each pair is seen from both ends: half weight; FP64 sums over the block */         \
+      const double h_ = lead ? 0.5 : 0.0;                                                    \
+      warp_sum_store(h_ * en, s_red7[0]);                                                    \
+      warp_sum_store(h_ * vxx, s_red7[1]);                                                   \
+      warp_sum_store(h_ * vyy, s_red7[2]);                                                   \
+      warp_sum_store(h_ * vzz, s_red7[3]);                                                   \
+      warp_sum_store(h_ * vyz, s_red7[4]);                                                   \
+      warp_sum_store(h_ * vxz, s_red7[5]);                                                   \
+      warp_sum_store(h_ * vxy, s_red7[6]);                                                   \
+      __syncthreads();                                                                       \
+      if (tid == 0) warps_sum7(s_red7, g.esum7);                                             \
+      __syncthreads();                                                                       \
+    }                                                                                        \
   }
 
     TSB_REBUILD()
@@ -954,9 +1020,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
           o[1] = (float)x1;
           o[2] = (float)x2;
         }
-        const double e_sys = block_sum_to0(lead ? 0.5 * (double)ei : 0.0, s_red);
-        if (tid == 0) A.frame_e[f * A.n_sys + s] = e_sys;
-        __syncthreads();
+        if (tid == 0) A.frame_e[f * A.n_sys + s] = g.esum7[0];
       }
     }
     if (failed) continue;
@@ -965,6 +1029,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
 #undef TSB_PAIR_CORE
 #undef TSB_PAIR_SHELL
 #undef TSB_PAIR2
+#undef TSB_VIR1
 #undef EXT
 #undef TSB_REBUILD
 #undef TSB_FILE_PAIR
@@ -981,14 +1046,24 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       A.f[3 * gi + 1] = F1;
       A.f[3 * gi + 2] = F2;
     }
-    double ev = lead ? 0.5 * (double)ei : 0.0;
-    for (int o = 16; o > 0; o >>= 1) ev += __shfl_xor_sync(0xffffffffu, ev, o);
-    if ((tid & 31) == 0) s_red[tid >> 5] = ev;
-    __syncthreads();
     if (tid == 0) {
-      double t = 0.0;
-      for (int k = 0; k < kFusedThreads / 32; ++k) t += s_red[k];
-      A.energy[s] = t;
+      A.energy[s] = g.esum7[0];
+      if (A.stress) {
+        // stress = -W / V (torch_sim/models/pair_potential.py:200-274)
+        const double *w = g.esum7 + 1;
+        const double *C = g.C;
+        const double vol = fabs(C[0] * (C[4] * C[8] - C[5] * C[7]) -
+                                C[1] * (C[3] * C[8] - C[5] * C[6]) +
+                                C[2] * (C[3] * C[7] - C[4] * C[6]));
+        const double iv = -1.0 / vol;
+        double *o = A.stress + 9 * s;
+        o[0] = w[0] * iv;
+        o[4] = w[1] * iv;
+        o[8] = w[2] * iv;
+        o[5] = o[7] = w[3] * iv;
+        o[2] = o[6] = w[4] * iv;
+        o[1] = o[3] = w[5] * iv;
+      }
       if (A.n_rebuilds) A.n_rebuilds[s] = rebuilds;
       if (A.integrator == TSB_INT_NOSE_HOOVER) {
         for (int j = 0; j < A.M; ++j) {
@@ -1022,10 +1097,19 @@ __global__ void k_advance_counter(uint64_t *counter_dev, int64_t n_steps) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *counter_dev += (uint64_t)n_steps;
 }
 
-__global__ void k_bounds_fused(const int64_t *sys, int64_t n, int64_t *lo, int64_t *hi) {
+// Atom range [lo[s], hi[s]) of every system from the sorted system index.  An
+// index outside [0, n_sys) is reported in status (code, atom, 3, index) and
+// skipped, so nothing is written outside lo/hi.
+__global__ void k_bounds_fused(const int64_t *sys, int64_t n, int64_t n_sys, int64_t *lo,
+                               int64_t *hi, int32_t *status) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int64_t s = sys[i];
+  if (s < 0 || s >= n_sys) {
+    report(status, TSB_ERR_INVALID_ARG, i, 3, (int)(s < INT32_MIN ? INT32_MIN
+                                                    : s > INT32_MAX ? INT32_MAX : s));
+    return;
+  }
   if (i == 0 || sys[i - 1] != s) lo[s] = i;
   if (i == n - 1 || sys[i + 1] != s) hi[s] = i + 1;
 }
@@ -1045,9 +1129,9 @@ extern "C" int tsb_fused_md(int integrator, int potential, const double *table,
                             double cutoff, double skin, int64_t n_steps,
                             const double *dt_sys, const double *kT_sys,
                             const double *gamma_sys, uint64_t seed, uint64_t counter,
-                            uint64_t *counter_dev, double *energy, int32_t *n_rebuilds,
-                            int32_t *status, void *workspace, size_t workspace_bytes,
-                            void *stream) {
+                            uint64_t *counter_dev, double *energy, double *stress,
+                            int32_t *n_rebuilds, int32_t *status, void *workspace,
+                            size_t workspace_bytes, void *stream) {
   if (integrator != TSB_INT_NVE && integrator != TSB_INT_LANGEVIN) return TSB_ERR_INVALID_ARG;
   if (potential < TSB_POT_LJ || potential > TSB_POT_SOFT) return TSB_ERR_INVALID_ARG;
   if (n_species < 1 || !table || (n_species > 1 && !species)) return TSB_ERR_INVALID_ARG;
@@ -1074,11 +1158,13 @@ extern "C" int tsb_fused_md(int integrator, int potential, const double *table,
   cudaMemsetAsync(hi, 0, sizeof(int64_t) * n_systems, st);
   cudaMemsetAsync(queue, 0, sizeof(int32_t) * 4, st);
   cudaMemsetAsync(status, 0, sizeof(int32_t) * 4, st);
-  k_bounds_fused<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, lo, hi);
+  k_bounds_fused<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, n_systems, lo,
+                                                       hi, status);
   FusedArgs A{integrator, potential, n_species, table, species, positions, momenta, forces,
               masses, cell_row, lo, hi, n_systems, order, cutoff, skin, n_steps, dt_sys,
               kT_sys, gamma_sys, seed, counter, counter_dev, energy, n_rebuilds, queue,
               status};
+  A.stress = stress;
   const bool multi = n_species > 1;
   if (potential == TSB_POT_LJ) {
     multi ? launch_fused<TSB_POT_LJ, true>(A, grid, st) : launch_fused<TSB_POT_LJ, false>(A, grid, st);
@@ -1105,8 +1191,8 @@ extern "C" int tsb_fused_md_nvt(int thermostat, int potential, const double *tab
                                 double *chain_Q, double *chain_ke, const double *chain_dt,
                                 int chain_length, int chain_steps, int sy_steps, uint64_t seed,
                                 uint64_t counter, uint64_t *counter_dev, double *energy,
-                                int32_t *n_rebuilds, int32_t *status, void *workspace,
-                                size_t workspace_bytes, void *stream) {
+                                double *stress, int32_t *n_rebuilds, int32_t *status,
+                                void *workspace, size_t workspace_bytes, void *stream) {
   if (thermostat != TSB_INT_NOSE_HOOVER && thermostat != TSB_INT_VRESCALE)
     return TSB_ERR_INVALID_ARG;
   if (potential < TSB_POT_LJ || potential > TSB_POT_SOFT) return TSB_ERR_INVALID_ARG;
@@ -1139,12 +1225,14 @@ extern "C" int tsb_fused_md_nvt(int thermostat, int potential, const double *tab
   cudaMemsetAsync(hi, 0, sizeof(int64_t) * n_systems, st);
   cudaMemsetAsync(queue, 0, sizeof(int32_t) * 4, st);
   cudaMemsetAsync(status, 0, sizeof(int32_t) * 4, st);
-  k_bounds_fused<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, lo, hi);
+  k_bounds_fused<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, n_systems, lo,
+                                                       hi, status);
   FusedArgs A{thermostat, potential, n_species, table, species, positions, momenta, forces,
               masses, cell_row, lo, hi, n_systems, order, cutoff, skin, n_steps, dt_sys,
               kT_sys, nullptr, seed, counter, counter_dev, energy, n_rebuilds, queue,
               status, chain_xi, chain_pxi, chain_Q, chain_ke, tau_sys, chain_dt,
               chain_length, chain_steps, sy_steps};
+  A.stress = stress;
   const bool multi = n_species > 1;
   if (potential == TSB_POT_LJ) {
     multi ? launch_fused<TSB_POT_LJ, true>(A, grid, st) : launch_fused<TSB_POT_LJ, false>(A, grid, st);
@@ -1173,8 +1261,8 @@ extern "C" int tsb_fused_md_ex(int integrator, int potential, const double *tabl
                                int chain_steps, int sy_steps, uint64_t seed, uint64_t counter,
                                uint64_t *counter_dev, float *frame_x, double *frame_e,
                                int64_t report_every, int64_t n_frames, double *energy,
-                               int32_t *n_rebuilds, int32_t *status, void *workspace,
-                               size_t workspace_bytes, void *stream) {
+                               double *stress, int32_t *n_rebuilds, int32_t *status,
+                               void *workspace, size_t workspace_bytes, void *stream) {
   if (integrator < TSB_INT_NVE || integrator > TSB_INT_VRESCALE) return TSB_ERR_INVALID_ARG;
   if (potential < TSB_POT_LJ || potential > TSB_POT_SOFT) return TSB_ERR_INVALID_ARG;
   if (n_species < 1 || !table || (n_species > 1 && !species)) return TSB_ERR_INVALID_ARG;
@@ -1210,13 +1298,15 @@ extern "C" int tsb_fused_md_ex(int integrator, int potential, const double *tabl
   cudaMemsetAsync(hi, 0, sizeof(int64_t) * n_systems, st);
   cudaMemsetAsync(queue, 0, sizeof(int32_t) * 4, st);
   cudaMemsetAsync(status, 0, sizeof(int32_t) * 4, st);
-  k_bounds_fused<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, lo, hi);
+  k_bounds_fused<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, n_systems, lo,
+                                                       hi, status);
   FusedArgs A{integrator, potential, n_species, table, species, positions, momenta, forces,
               masses, cell_row, lo, hi, n_systems, order, cutoff, skin, n_steps, dt_sys,
               kT_sys, gamma_sys, seed, counter, counter_dev, energy, n_rebuilds, queue,
               status, chain_xi, chain_pxi, chain_Q, chain_ke, tau_sys, chain_dt,
               chain_length, chain_steps, sy_steps, frame_x, frame_e,
               report_every > 0 && n_frames > 0 ? report_every : 0, n_frames, n_atoms};
+  A.stress = stress;
   const bool multi = n_species > 1;
   if (potential == TSB_POT_LJ) {
     multi ? launch_fused<TSB_POT_LJ, true>(A, grid, st) : launch_fused<TSB_POT_LJ, false>(A, grid, st);
@@ -1255,16 +1345,25 @@ constexpr int kMaxDevices = 64;
 static void *g_fused_static_ptr[kMaxDevices];
 static std::mutex g_fused_static_mu;
 
-static int fused_static_scratch(void **out) {
+// The address is looked up again on every call made outside stream capture (a
+// cudaDeviceReset or a reloaded module may have moved the array); during a
+// capture the address cached by the last uncaptured call on this device is used.
+static int fused_static_scratch(void **out, cudaStream_t st) {
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return TSB_ERR_CUDA;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) {
+    (void)cudaGetLastError();  // e.g. the legacy stream queried while another captures
+    cs = cudaStreamCaptureStatusActive;
+  }
   std::lock_guard<std::mutex> lock(g_fused_static_mu);
-  if (!g_fused_static_ptr[dev]) {
+  if (cs == cudaStreamCaptureStatusNone) {
     void *p = nullptr;
     if (cudaGetSymbolAddress(&p, g_fused_static_scratch) != cudaSuccess || !p)
       return TSB_ERR_CUDA;
     g_fused_static_ptr[dev] = p;
   }
+  if (!g_fused_static_ptr[dev]) return TSB_ERR_CUDA;  // first call made inside a capture
   *out = g_fused_static_ptr[dev];
   return TSB_OK;
 }
@@ -1292,13 +1391,13 @@ extern "C" int tsb_fused_md_static(int integrator, int potential, const double *
   if (integrator == TSB_INT_LANGEVIN && (!kT_sys || !gamma_sys)) return TSB_ERR_INVALID_ARG;
   // the fixed scratch holds the atom ranges of at most kStaticMaxSystems systems
   if (n_systems > kStaticMaxSystems) return TSB_ERR_CAPACITY;
+  cudaStream_t st = (cudaStream_t)stream;
   void *scratch = nullptr;
-  TSB_TRY(fused_static_scratch(&scratch));
+  TSB_TRY(fused_static_scratch(&scratch, st));
   char *base = (char *)scratch;
   int64_t *lo = (int64_t *)base;
   int64_t *hi = lo + kStaticMaxSystems;
   int32_t *queue = (int32_t *)(hi + kStaticMaxSystems);
-  cudaStream_t st = (cudaStream_t)stream;
   int dev = 0, n_sm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
@@ -1310,7 +1409,8 @@ extern "C" int tsb_fused_md_static(int integrator, int potential, const double *
   cudaMemsetAsync(hi, 0, sizeof(int64_t) * n_systems, st);
   cudaMemsetAsync(queue, 0, sizeof(int32_t) * 4, st);
   cudaMemsetAsync(status, 0, sizeof(int32_t) * 4, st);
-  k_bounds_fused<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, lo, hi);
+  k_bounds_fused<<<grid_for(n_atoms), kBlock, 0, st>>>(system_idx, n_atoms, n_systems, lo,
+                                                       hi, status);
   FusedArgs A{integrator, potential, n_species, table, species, positions, momenta, forces,
               masses, cell_row, lo, hi, n_systems, order, cutoff, skin, n_steps, dt_sys,
               kT_sys, gamma_sys, seed, counter, nullptr, energy, n_rebuilds, queue, status};

@@ -11,6 +11,7 @@ import glob
 import os
 import shutil
 import subprocess
+from concurrent.futures import ThreadPoolExecutor
 
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(os.path.dirname(PKG_DIR), "csrc")
@@ -20,8 +21,9 @@ LIB_PATH = os.path.join(PKG_DIR, "libtsb.so")
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
 ]
+OBJ_DIR = os.path.join(PKG_DIR, "_build")
 
 
 def nvcc_path() -> str:
@@ -43,17 +45,40 @@ def needs_build() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    """Compile csrc/*.cu into libtsb.so (skipped when up to date)."""
-    if not force and not needs_build():
+def build(force: bool = False, verbose: bool = False, out: str | None = None,
+          src_override: dict | None = None) -> str:
+    """Compile csrc/*.cu into libtsb.so (skipped when up to date).
+
+    Each translation unit is compiled to an object in parallel, then the objects
+    are linked into the shared library.  ``out`` writes the library elsewhere and
+    ``src_override`` maps a source's base name to a replacement file (both for
+    building variants side by side with the product library).
+    """
+    out = out or LIB_PATH
+    if not force and out == LIB_PATH and not src_override and not needs_build():
         return LIB_PATH
-    tmp = LIB_PATH + ".tmp"
-    cmd = [nvcc_path(), *NVCC_FLAGS, "-I", INCLUDE, *sources(), "-o", tmp]
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    tag = os.path.splitext(os.path.basename(out))[0]
+    nvcc = nvcc_path()
+    srcs = [(src_override or {}).get(os.path.basename(s), s) for s in sources()]
+
+    def compile_one(src):
+        obj = os.path.join(OBJ_DIR, f"{tag}.{os.path.splitext(os.path.basename(src))[0]}.o")
+        cmd = [nvcc, *NVCC_FLAGS, "-I", INCLUDE, "-I", CSRC, "-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(srcs), os.cpu_count() or 1))) as ex:
+        objs = list(ex.map(compile_one, srcs))
+    tmp = out + ".tmp"
+    cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", *objs, "-o", tmp]
     if verbose:
-        print(" ".join(cmd))
+        print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)
-    os.replace(tmp, LIB_PATH)
-    return LIB_PATH
+    os.replace(tmp, out)
+    return out
 
 
 if __name__ == "__main__":

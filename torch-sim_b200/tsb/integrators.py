@@ -859,6 +859,7 @@ class FusedMD:
         self.species = model._species(state.atomic_numbers)
         self.table = model.table if model.table.device == dev else model.table.to(dev)
         self.energy = torch.zeros(self.n_sys, dtype=f64, device=dev)
+        self.stress = torch.zeros((self.n_sys, 3, 3), dtype=f64, device=dev)
         self.rebuilds = torch.zeros(self.n_sys, dtype=torch.int32, device=dev)
         self.status = torch.zeros(4, dtype=torch.int32, device=dev)
         self.ws = torch.empty(self.lib.tsb_fused_workspace_size(self.n, self.n_sys),
@@ -901,7 +902,7 @@ class FusedMD:
                    g("cxi"), g("cpxi"), g("cQ"), g("cke"), g("cdt"),
                    self.M if nh else 0, self.nc if nh else 0, self.nsy if nh else 0,
                    self.seed, 0, L.ptr(self.counter_dev), L.ptr(fx), L.ptr(fe), int(every),
-                   int(fx.shape[0]), L.ptr(self.energy), L.ptr(self.rebuilds),
+                   int(fx.shape[0]), L.ptr(self.energy), L.ptr(self.stress), L.ptr(self.rebuilds),
                    L.ptr(self.status), L.ptr(self.ws), self.ws.numel(), st)
             return
         if self.integ in (L.INT_NOSE_HOOVER, L.INT_VRESCALE):
@@ -914,16 +915,16 @@ class FusedMD:
                    L.ptr(self.kT_s), L.ptr(self.tau_s), g("cxi"), g("cpxi"), g("cQ"), g("cke"),
                    g("cdt"), self.M if nh else 0, self.nc if nh else 0, self.nsy if nh else 0,
                    self.seed, 0, L.ptr(self.counter_dev), L.ptr(self.energy),
-                   L.ptr(self.rebuilds), L.ptr(self.status), L.ptr(self.ws), self.ws.numel(),
-                   st)
+                   L.ptr(self.stress), L.ptr(self.rebuilds), L.ptr(self.status), L.ptr(self.ws),
+                   self.ws.numel(), st)
             return
         L.call("tsb_fused_md", self.integ, m.kind, L.ptr(self.table), m.n_species,
                L.ptr(self.species), L.ptr(self.x), L.ptr(self.p), L.ptr(self.f), L.ptr(self.m),
                L.ptr(self.cell_row), L.ptr(self.sys_idx), self.n, self.n_sys,
                L.ptr(self.order), m.cutoff, self.skin, int(n_steps), L.ptr(self.dt_s),
                L.ptr(self.kT_s), L.ptr(self.g_s), self.seed, 0, L.ptr(self.counter_dev),
-               L.ptr(self.energy), L.ptr(self.rebuilds), L.ptr(self.status), L.ptr(self.ws),
-               self.ws.numel(), st)
+               L.ptr(self.energy), L.ptr(self.stress), L.ptr(self.rebuilds), L.ptr(self.status),
+               L.ptr(self.ws), self.ws.numel(), st)
 
     def graph(self, n_steps: int) -> "torch.cuda.CUDAGraph":
         """CUDA graph of one ``launch(n_steps)``; ``g.replay()`` advances every system
@@ -951,7 +952,8 @@ class FusedMD:
     def check(self) -> None:
         st = self.status.tolist()
         if st[0] != 0:
-            what = {1: "periodic images", 2: "neighbour slots"}.get(st[2], "atoms")
+            what = {1: "periodic images", 2: "neighbour slots",
+                    3: "system index of atom"}.get(st[2], "atoms")
             raise FusedMDError(f"fused MD: system {st[1]}: {L.status_string(st[0])} "
                                f"({what}: {st[3]})")
 
