@@ -42,15 +42,14 @@ WORKLOAD = ("2048 Cu fcc systems (8-512 atoms, strain +-2%, shear +-3deg), Morse
 INTEGRATOR_NAMES = {"nvt_nose_hoover": "NVT Nose-Hoover chain (3 x 3 x 3)",
                     "nvt_vrescale": "NVT V-rescale (tau 10 dt)", "nve": "NVE velocity Verlet"}
 ALG_BYTES_PER_ATOM_STEP = 76  # streaming state r/w: 48 B FP64 pos + 24 B mom + 4 B type/mass
-# algorithmic compute per atom-step of the Morse workload (rho = 0.0850 / A^3, rc = 6 A):
-# 38.5 half-list pairs, ~45 FP32 flops and one exp per pair
-HALF_PAIRS_PER_ATOM = 38.5
+# algorithmic compute per half-list pair of the Morse workload: ~45 FP32 flops and
+# one exp (the half pairs within the cutoff are counted on the workload itself)
 FLOPS_PER_PAIR = 45
 
 
 def sm_peaks(device):
     """Nominal FP32 (FMA = 2 flops, 128 lanes/SM) and MUFU (16 lanes/SM) peaks at
-    the maximum SM clock."""
+    the maximum SM clock (the measured-peaks file has no FP32 or MUFU figure)."""
     import torch
 
     props = torch.cuda.get_device_properties(device)
@@ -58,6 +57,24 @@ def sm_peaks(device):
     fp32 = props.multi_processor_count * 128 * 2 * ghz / 1e3  # TFLOP/s
     sfu = props.multi_processor_count * 16 * ghz  # G ops/s
     return fp32, sfu
+
+
+def pair_counts(x, cell_row, system_idx, cutoff, skin, n_systems):
+    """(half-list pairs within the cutoff, list entries within cutoff + skin, both
+    per atom) of one configuration, from the neighbour-list drop-in: the
+    algorithmic pairs of a step and the pair evaluations of a fused step (every
+    atom evaluates its full list at cutoff + skin)."""
+    import torch
+
+    from tsb import neighbors
+
+    pbc = torch.ones((n_systems, 3), dtype=torch.bool, device=x.device)
+    n = x.shape[0]
+    p_rc = neighbors.torchsim_nl(x, cell_row, pbc, cutoff, system_idx,
+                                 n_systems=n_systems)[0].shape[1]
+    p_list = neighbors.torchsim_nl(x, cell_row, pbc, cutoff + skin, system_idx,
+                                   n_systems=n_systems)[0].shape[1]
+    return p_rc / 2 / n, p_list / n
 
 
 def parse():
@@ -158,18 +175,6 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per fused launch from the committed ncu summary (or None)."""
-    p = os.path.join(REPO, "profiles", "fused_md_ncu.md")
-    try:
-        for line in open(p):
-            if line.startswith("dram_bytes_per_launch_full_workload:"):
-                return float(line.split(":")[1].split()[0])
-    except OSError:
-        pass
-    return None
-
-
 def build_workload(n_systems, seed, device):
     import torch
 
@@ -187,7 +192,7 @@ def build_workload(n_systems, seed, device):
     return d, md, model
 
 
-def cpu_baseline(d, budget_s=20.0, processes=1, n_steps=2, seed=0):
+def cpu_baseline(d, budget_s=20.0, processes=None, n_steps=2, seed=0):
     """Oracle port on the host: a bounded sample of systems (see oracle/cpu_md.py)."""
     import numpy as np
 
@@ -195,6 +200,8 @@ def cpu_baseline(d, budget_s=20.0, processes=1, n_steps=2, seed=0):
     from oracle import cpu_md
     from tsb import workloads as W
 
+    if processes is None:  # all host cores, as the --impl reference arm uses
+        processes = cpu_md.cpu_count()
     rng = np.random.default_rng(seed)
     n_sys = int(d["system_idx"].max()) + 1
     systems = rng.permutation(n_sys)
@@ -557,12 +564,19 @@ def main():
     t_plain = replicas.max_over_ranks(pa.elapsed_time(pb) / 1e3, device)
     plain_value = replicas.weak_scaling_value(n_atoms * args.plain_steps, t_plain, ws)
 
+    # pair counts of the final configuration: algorithmic half pairs within the
+    # cutoff, and the list entries each atom evaluates per fused step
+    half_pairs, evals = pair_counts(runner.x, runner.cell_row, md.system_idx, model.cutoff,
+                                    runner.skin, md.n_systems)
+
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
         fp32_peak, sfu_peak = sm_peaks(device)
         alg_bytes = n_atoms * args.md_steps * ALG_BYTES_PER_ATOM_STEP
         achieved = alg_bytes / avg_launch_s / 1e9
-        traffic = profiled_traffic()
+        # per-launch rate of the dominant kernel (CUDA events around each launch)
+        rate = n_atoms * args.md_steps / avg_launch_s
+        fp32_achieved = rate * half_pairs * FLOPS_PER_PAIR / 1e12
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup,
@@ -574,28 +588,31 @@ def main():
                        "n_systems": args.n_systems,
                        "atoms_per_gpu": n_atoms, "md_steps_per_step": args.md_steps,
                        "verlet_skin_A": runner.skin,
-                       "skin_source": "autotuner" if args.skin == "auto" else "argument", "precision": "FP32 pair math, FP64 state",
+                       "skin_source": "autotuner" if args.skin == "auto" else "argument",
+                       "precision": "FP32 pair math, FP64 state",
                        "mean_steps_between_list_rebuilds": rebuild_interval,
                        "l2": "256 MB buffer written between timed launches",
                        "parallelism": f"replicas x{ws} (independent systems per rank)"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "peak_source": peak_kind,
-                         "algorithmic_bytes_per_atom_step": ALG_BYTES_PER_ATOM_STEP,
-                         "kernel": "k_fused_md"},
-            # the binding bound of this shared-memory-resident kernel is inside the SM
-            "roofline_sm": {"bound": "fp32 issue", "kernel": "k_fused_md",
-                            "achieved": value * HALF_PAIRS_PER_ATOM * FLOPS_PER_PAIR / 1e12,
-                            "peak": fp32_peak, "unit": "TFLOP/s",
-                            "frac": value * HALF_PAIRS_PER_ATOM * FLOPS_PER_PAIR / 1e12
-                            / fp32_peak,
-                            "exp_per_s": value * HALF_PAIRS_PER_ATOM,
-                            "sfu_peak_per_s": sfu_peak * 1e9,
-                            "sfu_frac": value * HALF_PAIRS_PER_ATOM / (sfu_peak * 1e9),
-                            "algorithm": f"{HALF_PAIRS_PER_ATOM} half-list pairs x "
-                                         f"{FLOPS_PER_PAIR} FP32 flops + 1 exp per atom-step",
-                            "peak_source": "nominal: SMs x 128 FP32 lanes x 2 x max SM clock; "
-                                           "MUFU 16 lanes/SM"},
+            # the binding bound of this shared-memory-resident kernel is FP32 and
+            # MUFU issue inside the SM: algorithmic flops = half pairs within the
+            # cutoff x 45 FP32 flops; one exp per half pair
+            "roofline": {"bound": "fp32", "kernel": "k_fused_md", "achieved": fp32_achieved,
+                         "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": fp32_achieved / fp32_peak, "traffic": None,
+                         "peak_source": "nominal: SMs x 128 FP32 lanes x 2 x max SM clock "
+                                        "(no measured FP32 peak)",
+                         "half_pairs_per_atom_step": half_pairs,
+                         "pair_evaluations_per_atom_step": evals,
+                         "flops_per_half_pair": FLOPS_PER_PAIR,
+                         "exp_per_s": rate * half_pairs,
+                         "sfu_peak_per_s": sfu_peak * 1e9,
+                         "sfu_frac": rate * half_pairs / (sfu_peak * 1e9)},
+            # the streaming-design HBM bound, for comparison: this kernel keeps the
+            # per-step state in shared memory and registers
+            "roofline_hbm": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                             "algorithmic_bytes_per_atom_step": ALG_BYTES_PER_ATOM_STEP,
+                             "kernel": "k_fused_md"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "force_err_vs_fp64": force_err,
@@ -604,7 +621,7 @@ def main():
                                    "step (cell list + FP32 pair forces + integrator kernels "
                                    "each call)",
                            "fused_over_plain": value / plain_value},
-            "gpu_launches": 2 * args.steps,
+            "gpu_launches": 3 * args.steps,  # k_bounds_fused, k_fused_md, k_advance_counter
             "clocks": clocks.summary(),
             "per_launch_ms": per_launch_ms,
         }

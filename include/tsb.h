@@ -120,7 +120,9 @@ int tsb_pair_forward(int potential, const double *table, int n_species,
  * tsb_md_baoab_boa: the B(dt/2) A(dt/2) O(dt) A(dt/2) part of nvt_langevin_step
  *   (torch_sim/integrators/nvt.py:144-240, _ou_step :27-86).  The O-step noise
  *   is read from `noise` [N,3] when non-NULL, else drawn from a counter-based
- *   Philox4x32-10 stream keyed by (seed, atom, counter). */
+ *   Philox4x32-10 stream keyed by (seed, atom, counter + *counter_dev); when
+ *   counter_dev is not NULL the call also advances *counter_dev by one on the
+ *   stream, so a captured CUDA graph draws fresh noise on every replay. */
 int tsb_md_kick(void *momenta, const void *forces, const int64_t *system_idx,
                 const double *dt_sys, double scale, int64_t n_atoms, int dtype,
                 void *stream);
@@ -131,7 +133,8 @@ int tsb_md_baoab_boa(void *positions, void *momenta, const void *forces,
                      const void *masses, const int64_t *system_idx,
                      const double *dt_sys, const double *kT_sys,
                      const double *gamma_sys, const void *noise, uint64_t seed,
-                     uint64_t counter, int64_t n_atoms, int dtype, void *stream);
+                     uint64_t counter, uint64_t *counter_dev, int64_t n_atoms, int dtype,
+                     void *stream);
 
 /* ---- Verlet-list forces for large periodic systems ----------------------
  * One fully periodic system whose cell widths are all >= cutoff + skin

@@ -35,9 +35,11 @@ __global__ void k_drift(P *q, const P *p, const P *m, const int64_t *sys, const 
 template <class P>
 __global__ void k_baoab_boa(P *q, P *p, const P *f, const P *m, const int64_t *sys,
                             const double *dt_s, const double *kT_s, const double *g_s,
-                            const P *noise, uint64_t seed, uint64_t counter, int64_t n) {
+                            const P *noise, uint64_t seed, uint64_t counter,
+                            const uint64_t *counter_dev, int64_t n) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (counter_dev) counter += *counter_dev;
   const int64_t s = sys[i];
   const P dt = (P)dt_s[s];
   const P half = dt / (P)2;
@@ -60,6 +62,12 @@ __global__ void k_baoab_boa(P *q, P *p, const P *f, const P *m, const int64_t *s
     q[3 * i + k] = qq[k] + (pp[k] / mi) * half;
     p[3 * i + k] = pp[k];
   }
+}
+
+// advances the device-resident noise counter by one step (after the kernel that
+// read it, in stream order)
+__global__ void k_advance_step_counter(uint64_t *counter_dev) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *counter_dev += 1ull;
 }
 
 }  // namespace tsb
@@ -111,7 +119,8 @@ extern "C" int tsb_md_baoab_boa(void *positions, void *momenta, const void *forc
                                 const void *masses, const int64_t *system_idx,
                                 const double *dt_sys, const double *kT_sys,
                                 const double *gamma_sys, const void *noise, uint64_t seed,
-                                uint64_t counter, int64_t n_atoms, int dtype, void *stream) {
+                                uint64_t counter, uint64_t *counter_dev, int64_t n_atoms,
+                                int dtype, void *stream) {
   if (n_atoms < 0 || (n_atoms > 0 && (!positions || !momenta || !forces || !masses ||
                                       !system_idx || !dt_sys || !kT_sys || !gamma_sys)))
     return TSB_ERR_INVALID_ARG;
@@ -121,13 +130,15 @@ extern "C" int tsb_md_baoab_boa(void *positions, void *momenta, const void *forc
     k_baoab_boa<double><<<grid_for(n_atoms), kBlock, 0, st>>>(
         (double *)positions, (double *)momenta, (const double *)forces,
         (const double *)masses, system_idx, dt_sys, kT_sys, gamma_sys,
-        (const double *)noise, seed, counter, n_atoms);
+        (const double *)noise, seed, counter, counter_dev, n_atoms);
   else if (dtype == TSB_F32)
     k_baoab_boa<float><<<grid_for(n_atoms), kBlock, 0, st>>>(
         (float *)positions, (float *)momenta, (const float *)forces, (const float *)masses,
-        system_idx, dt_sys, kT_sys, gamma_sys, (const float *)noise, seed, counter, n_atoms);
+        system_idx, dt_sys, kT_sys, gamma_sys, (const float *)noise, seed, counter, counter_dev,
+        n_atoms);
   else
     return TSB_ERR_INVALID_ARG;
+  if (counter_dev) k_advance_step_counter<<<1, 32, 0, st>>>(counter_dev);
   TSB_CHECK_LAUNCH();
   return TSB_OK;
 }

@@ -9,6 +9,8 @@ kernels reached through the C ABI in ``include/tsb.h``:
 * ``tsb.integrators.nve_step`` / ``nvt_langevin_step`` (+ ``*_init``)
 * ``tsb.optimizers.fire_init`` / ``fire_step`` (ASE / VV FIRE, Frechet filter)
 * ``tsb.integrators.run_md``              persistent fused batched MD
+* ``tsb.ops``                             the same kernels as ``torch.ops.tsb.*``
+  operators (CUDA and fake implementations), which the drop-ins call
 
 Submodules are imported lazily; importing ``tsb`` does not load the CUDA library.
 """
@@ -17,7 +19,7 @@ import importlib
 
 __version__ = "0.1.0"
 _SUBMODULES = ("neighbors", "models", "integrators", "optimizers", "state", "workloads",
-               "build", "adjoint")
+               "build", "adjoint", "ops")
 
 
 def __getattr__(name):

@@ -51,7 +51,7 @@ PROTOTYPES = {
     "tsb_md_kick": (_int, [_vp, _vp, _vp, _vp, _dbl, _i64, _int, _vp]),
     "tsb_md_drift": (_int, [_vp, _vp, _vp, _vp, _vp, _dbl, _i64, _int, _vp]),
     "tsb_md_baoab_boa": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _u64, _u64,
-                                _i64, _int, _vp]),
+                                _vp, _i64, _int, _vp]),
     "tsb_adjoint_workspace_size": (_sz, [_i64, _i64, _i64]),
     "tsb_vv_kick_drift": (_int, [_vp, _vp, _vp, _vp, _dbl, _dbl, _vp, _vp, _i64, _vp]),
     "tsb_vv_kick": (_int, [_vp, _vp, _dbl, _vp, _i64, _vp]),

@@ -32,6 +32,7 @@ from __future__ import annotations
 import torch
 
 from . import _lib as L
+from . import ops as _ops  # noqa: F401  (registers torch.ops.tsb.*)
 from .state import MDState
 
 
@@ -43,12 +44,19 @@ def _per_system(x, n_sys: int, device) -> torch.Tensor:
 
 
 def initialize_momenta(positions, masses, system_idx, kT, generator=None):
-    """p = sqrt(m kT) N(0,1) minus the per-system mean (md.py:113-166)."""
+    """p = sqrt(m kT) N(0,1) minus the per-system mean (md.py:113-166).
+
+    The normals are drawn on the generator's device (the positions' device when
+    ``generator`` is None) and moved to the positions' device, so a CPU generator
+    seeded as the reference seeds ``state.rng`` replays the reference's draw for
+    a state that lives on the GPU."""
     kT = torch.as_tensor(kT, device=positions.device, dtype=positions.dtype)
     if kT.ndim > 0:
         kT = kT[system_idx]
-    p = torch.randn(positions.shape, device=positions.device, dtype=positions.dtype,
-                    generator=generator) * torch.sqrt(masses * kT).unsqueeze(-1)
+    draw_dev = generator.device if generator is not None else positions.device
+    z = torch.randn(positions.shape, device=draw_dev, dtype=positions.dtype,
+                    generator=generator).to(positions.device)
+    p = z * torch.sqrt(masses * kT).unsqueeze(-1)
     n_sys = int(system_idx[-1]) + 1
     counts = torch.bincount(system_idx, minlength=n_sys)
     # per-system sums from an FP64 prefix sum over the contiguous systems: a fixed
@@ -58,6 +66,12 @@ def initialize_momenta(positions, masses, system_idx, kT, generator=None):
     ends = counts.cumsum(0)
     mean = ((cs[ends] - cs[ends - counts]) / counts.view(-1, 1)).to(p.dtype)
     return torch.where((counts > 1)[system_idx].view(-1, 1), p - mean[system_idx], p)
+
+
+def _i64(v: int) -> int:
+    """A uint64 (seed, counter) as the signed int64 an operator argument holds."""
+    v = int(v) & (2**64 - 1)
+    return v - 2**64 if v >= 2**63 else v
 
 
 def _seed_of(state) -> int:
@@ -92,15 +106,24 @@ def nvt_langevin_init(state, model, *, kT, **_kw) -> MDState:
 
 
 def _kick(state, dt_s, scale):
-    L.call("tsb_md_kick", L.ptr(state.momenta), L.ptr(state.forces),
-           L.ptr(state.system_idx), L.ptr(dt_s), float(scale), state.n_atoms,
-           L.dtype_code(state.dtype), L.stream_ptr(state.device))
+    torch.ops.tsb.md_kick_(state.momenta, state.forces, state.system_idx, dt_s, float(scale))
 
 
 def _drift(state, dt_s, scale):
-    L.call("tsb_md_drift", L.ptr(state.positions), L.ptr(state.momenta),
-           L.ptr(state.masses), L.ptr(state.system_idx), L.ptr(dt_s), float(scale),
-           state.n_atoms, L.dtype_code(state.dtype), L.stream_ptr(state.device))
+    torch.ops.tsb.md_drift_(state.positions, state.momenta, state.masses, state.system_idx,
+                            dt_s, float(scale))
+
+
+def use_device_counter(state, counter_dev: torch.Tensor | None = None):
+    """Keep the state's Langevin noise counter on the device: every
+    ``nvt_langevin_step`` then draws with counter ``state._philox_counter +
+    counter_dev`` and advances ``counter_dev`` on the stream, so a step loop
+    captured in a CUDA graph draws fresh noise on every replay.  Returns the
+    counter tensor (int64 [1])."""
+    if counter_dev is None:
+        counter_dev = torch.zeros(1, dtype=torch.int64, device=state.device)
+    state._philox_counter_dev = counter_dev
+    return counter_dev
 
 
 def _prepare(state):
@@ -144,11 +167,13 @@ def nvt_langevin_step(state, model, *, dt, kT, gamma=None, noise=None, **_kw):
         noise = noise.to(device=state.device, dtype=state.dtype).contiguous()
     seed = getattr(state, "_philox_seed", _seed_of(state))
     counter = getattr(state, "_philox_counter", 0)
-    L.call("tsb_md_baoab_boa", L.ptr(state.positions), L.ptr(state.momenta),
-           L.ptr(state.forces), L.ptr(state.masses), L.ptr(state.system_idx), L.ptr(dt_s),
-           L.ptr(kT_s), L.ptr(g_s), L.ptr(noise), seed & (2**64 - 1), counter,
-           state.n_atoms, L.dtype_code(state.dtype), L.stream_ptr(state.device))
-    state._philox_seed, state._philox_counter = seed, counter + 1
+    counter_dev = getattr(state, "_philox_counter_dev", None)
+    torch.ops.tsb.md_baoab_boa_(state.positions, state.momenta, state.forces, state.masses,
+                                state.system_idx, dt_s, kT_s, g_s, noise, _i64(seed),
+                                _i64(counter), counter_dev)
+    state._philox_seed = seed
+    if counter_dev is None:
+        state._philox_counter = counter + 1
     _apply_model(state, model)
     _kick(state, dt_s, 0.5)
     return state
@@ -884,47 +909,24 @@ class FusedMD:
         return int(self.counter_dev.item())
 
     def launch(self, n_steps: int, stream: int | None = None, frames=None) -> None:
-        """Advance every system by n_steps in one persistent launch.  ``frames`` =
-        (frame_x float32 [F, N, 3], frame_e float64 [F, S], report_every) makes the
-        kernel write positions and potential energies every report_every steps
-        (F frames at most)."""
+        """Advance every system by n_steps in one persistent launch (on the current
+        stream; ``stream`` is accepted for compatibility and must be None or the
+        current stream).  ``frames`` = (frame_x float32 [F, N, 3], frame_e float64
+        [F, S], report_every) makes the kernel write positions and potential
+        energies every report_every steps (F frames at most)."""
+        if stream is not None and stream != L.stream_ptr(self.dev):
+            raise ValueError("FusedMD.launch runs on the current CUDA stream")
         m = self.model
-        st = stream if stream is not None else L.stream_ptr(self.dev)
-        if frames is not None:
-            fx, fe, every = frames
-            nh = self.integ == L.INT_NOSE_HOOVER
-            g = (lambda name: L.ptr(getattr(self, name, None)) if nh else None)  # noqa: E731
-            L.call("tsb_fused_md_ex", self.integ, m.kind, L.ptr(self.table), m.n_species,
-                   L.ptr(self.species), L.ptr(self.x), L.ptr(self.p), L.ptr(self.f),
-                   L.ptr(self.m), L.ptr(self.cell_row), L.ptr(self.sys_idx), self.n, self.n_sys,
-                   L.ptr(self.order), m.cutoff, self.skin, int(n_steps), L.ptr(self.dt_s),
-                   L.ptr(self.kT_s), L.ptr(self.g_s), L.ptr(getattr(self, "tau_s", None)),
-                   g("cxi"), g("cpxi"), g("cQ"), g("cke"), g("cdt"),
-                   self.M if nh else 0, self.nc if nh else 0, self.nsy if nh else 0,
-                   self.seed, 0, L.ptr(self.counter_dev), L.ptr(fx), L.ptr(fe), int(every),
-                   int(fx.shape[0]), L.ptr(self.energy), L.ptr(self.stress), L.ptr(self.rebuilds),
-                   L.ptr(self.status), L.ptr(self.ws), self.ws.numel(), st)
-            return
-        if self.integ in (L.INT_NOSE_HOOVER, L.INT_VRESCALE):
-            nh = self.integ == L.INT_NOSE_HOOVER
-            g = (lambda name: L.ptr(getattr(self, name)) if nh else None)  # noqa: E731
-            L.call("tsb_fused_md_nvt", self.integ, m.kind, L.ptr(self.table), m.n_species,
-                   L.ptr(self.species), L.ptr(self.x), L.ptr(self.p), L.ptr(self.f),
-                   L.ptr(self.m), L.ptr(self.cell_row), L.ptr(self.sys_idx), self.n, self.n_sys,
-                   L.ptr(self.order), m.cutoff, self.skin, int(n_steps), L.ptr(self.dt_s),
-                   L.ptr(self.kT_s), L.ptr(self.tau_s), g("cxi"), g("cpxi"), g("cQ"), g("cke"),
-                   g("cdt"), self.M if nh else 0, self.nc if nh else 0, self.nsy if nh else 0,
-                   self.seed, 0, L.ptr(self.counter_dev), L.ptr(self.energy),
-                   L.ptr(self.stress), L.ptr(self.rebuilds), L.ptr(self.status), L.ptr(self.ws),
-                   self.ws.numel(), st)
-            return
-        L.call("tsb_fused_md", self.integ, m.kind, L.ptr(self.table), m.n_species,
-               L.ptr(self.species), L.ptr(self.x), L.ptr(self.p), L.ptr(self.f), L.ptr(self.m),
-               L.ptr(self.cell_row), L.ptr(self.sys_idx), self.n, self.n_sys,
-               L.ptr(self.order), m.cutoff, self.skin, int(n_steps), L.ptr(self.dt_s),
-               L.ptr(self.kT_s), L.ptr(self.g_s), self.seed, 0, L.ptr(self.counter_dev),
-               L.ptr(self.energy), L.ptr(self.stress), L.ptr(self.rebuilds), L.ptr(self.status),
-               L.ptr(self.ws), self.ws.numel(), st)
+        nh = self.integ == L.INT_NOSE_HOOVER
+        g = (lambda name: getattr(self, name, None) if nh else None)  # noqa: E731
+        fx, fe, every = frames if frames is not None else (None, None, 0)
+        torch.ops.tsb.fused_md_(
+            self.integ, m.kind, self.table, m.n_species, self.species, self.x, self.p, self.f,
+            self.m, self.cell_row, self.sys_idx, self.order, m.cutoff, self.skin, int(n_steps),
+            self.dt_s, self.kT_s, self.g_s, getattr(self, "tau_s", None), g("cxi"), g("cpxi"),
+            g("cQ"), g("cke"), g("cdt"), self.M if nh else 0, self.nc if nh else 0,
+            self.nsy if nh else 0, _i64(self.seed), 0, self.counter_dev, fx, fe, int(every),
+            self.energy, self.stress, self.rebuilds, self.status, self.ws)
 
     def graph(self, n_steps: int) -> "torch.cuda.CUDAGraph":
         """CUDA graph of one ``launch(n_steps)``; ``g.replay()`` advances every system

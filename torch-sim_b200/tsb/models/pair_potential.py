@@ -23,6 +23,7 @@ import numpy as np
 import torch
 
 from .. import _lib as L
+from .. import ops as _ops  # noqa: F401  (registers torch.ops.tsb.*)
 from .interface import ModelInterface
 
 KIND = {"lj": L.POT_LJ, "morse": L.POT_MORSE, "soft_sphere": L.POT_SOFT,
@@ -105,25 +106,21 @@ class PairTableModel(ModelInterface):
         if state.dtype != self._dtype:
             raise TypeError(
                 f"SimState dtype {state.dtype} does not match model dtype {self._dtype}.")
-        pos = state.positions
-        L.require_cuda(pos, "state.positions")
-        dev, dt = pos.device, pos.dtype
-        n, n_sys = pos.shape[0], state.n_systems
-        energy = torch.empty(n_sys, dtype=dt, device=dev)
-        forces = torch.empty((n, 3), dtype=dt, device=dev) if self._compute_forces else None
-        stress = torch.empty((n_sys, 3, 3), dtype=dt, device=dev) if self._compute_stress else None
-        energies = torch.empty(n, dtype=dt, device=dev) if self.per_atom_energies else None
-        stresses = (torch.empty((n, 3, 3), dtype=dt, device=dev)
-                    if self.per_atom_stresses else None)
-        self._launch(state, energy, forces, stress, energies, stresses, None)
+        L.require_cuda(state.positions, "state.positions")
+        n_sys = state.n_systems
+        flags = self._flags(self._compute_forces, self._compute_stress, self.per_atom_energies,
+                            self.per_atom_stresses)
+        energy, forces, stress, energies, stresses = torch.ops.tsb.pair_forward(
+            *self._inputs(state), self.kind, self.n_species, self.cutoff, flags, n_sys,
+            L.max_system_atoms(state.system_idx, n_sys))
         out = {"energy": energy}
-        if forces is not None:
+        if self._compute_forces:
             out["forces"] = forces
-        if stress is not None:
+        if self._compute_stress:
             out["stress"] = stress
-        if energies is not None:
+        if self.per_atom_energies:
             out["energies"] = energies
-        if stresses is not None:
+        if self.per_atom_stresses:
             out["stresses"] = stresses
         return out
 
@@ -140,32 +137,37 @@ class PairTableModel(ModelInterface):
         self._launch(state, energy, forces, stress if self._compute_stress else None, None,
                      None, sys_active)
 
-    def _launch(self, state, energy, forces, stress, energies, stresses, sys_active):
+    def _inputs(self, state):
+        """(positions, cell_row, pbc, system_idx, species, table) as the operators take them."""
         pos = state.positions.contiguous()
-        dev, dt = pos.device, pos.dtype
-        n, n_sys = pos.shape[0], state.n_systems
-        cell_row = state.cell.mT.contiguous()
-        pbc = L.pbc_rows(state.pbc, n_sys, dev)
-        sys_idx = state.system_idx.contiguous()
-        species = self._species(state.atomic_numbers)
+        dev = pos.device
+        n_sys = state.n_systems
         table = self.table if self.table.device == dev else self.table.to(dev)
+        return (pos, state.cell.mT.contiguous(), L.pbc_rows(state.pbc, n_sys, dev),
+                state.system_idx.contiguous(), self._species(state.atomic_numbers), table)
+
+    def _flags(self, forces, stress, energies, stresses):
         flags = 0
-        if forces is not None:
+        if forces:
             flags |= L.OUT_FORCES
-        if stress is not None:
+        if stress:
             flags |= L.OUT_STRESS
-        if energies is not None:
+        if energies:
             flags |= L.OUT_ENERGIES
-        if stresses is not None:
+        if stresses:
             flags |= L.OUT_STRESSES
         if self.precision == "fp64":
             flags |= L.MATH_FP64
-        ws = L.Workspace.get(dev, L.load().tsb_pair_workspace_size(n, n_sys))
-        L.call("tsb_pair_forward", self.kind, L.ptr(table), self.n_species, L.ptr(species),
-               L.ptr(pos), L.ptr(cell_row), L.ptr(pbc), L.ptr(sys_idx), n, n_sys,
-               L.dtype_code(dt), self.cutoff, flags, L.ptr(energy), L.ptr(forces),
-               L.ptr(stress), L.ptr(energies), L.ptr(stresses), L.ptr(sys_active),
-               L.max_system_atoms(sys_idx, n_sys), L.ptr(ws), ws.numel(), L.stream_ptr(dev))
+        return flags
+
+    def _launch(self, state, energy, forces, stress, energies, stresses, sys_active):
+        if energies is not None or stresses is not None:
+            raise ValueError("per-atom outputs are returned by forward(), not written into")
+        n_sys = state.n_systems
+        flags = self._flags(forces is not None, stress is not None, False, False)
+        torch.ops.tsb.pair_forward_into_(
+            *self._inputs(state), self.kind, self.n_species, self.cutoff, flags, n_sys,
+            L.max_system_atoms(state.system_idx, n_sys), energy, forces, stress, sys_active)
 
 
 def single_species_table(sigma, epsilon, alpha=0.0, rc=np.inf, eshift=0.0):

@@ -26,6 +26,7 @@ from __future__ import annotations
 import torch
 
 from .. import _lib as L
+from .. import ops as _ops  # noqa: F401  (registers torch.ops.tsb.*)
 from .interface import ModelInterface
 from .pair_potential import PairTableModel
 
@@ -80,18 +81,15 @@ class VerletListModel(ModelInterface):
     # ---------------------------------------------------------------- lists
     def _update_lists(self, state, pos, cell_row, pbc, sysi, species, active):
         n, ns, dev = state.n_atoms, state.n_systems, pos.device
-        dt = L.dtype_code(pos.dtype)
         cutoff = self.model.cutoff
         while True:
-            L.call("tsb_vlist_check", L.ptr(pos), L.ptr(cell_row), L.ptr(sysi), L.ptr(active),
-                   n, ns, dt, cutoff, self.skin, L.ptr(self.flags), L.ptr(self.ws),
-                   self.ws.numel(), L.stream_ptr(dev))
+            torch.ops.tsb.vlist_check_(pos, cell_row, sysi, active, ns, cutoff, self.skin,
+                                       self.flags, self.ws)
             if not int(self.flags[0].item()):
                 return
-            L.call("tsb_vlist_build", L.ptr(pos), L.ptr(cell_row), L.ptr(pbc), L.ptr(sysi),
-                   L.ptr(species), n, ns, dt, cutoff, self.skin, L.ptr(self.list),
-                   L.ptr(self.counts), self.cap, self.max_system_atoms, L.ptr(self.flags),
-                   L.ptr(self.ws), self.ws.numel(), L.stream_ptr(dev))
+            torch.ops.tsb.vlist_build_(pos, cell_row, pbc, sysi, species, ns, cutoff, self.skin,
+                                       self.list, self.counts, self.cap, self.max_system_atoms,
+                                       self.flags, self.ws)
             self.n_builds += 1
             st = int(self.flags[1].item())
             if st == 0:
@@ -130,11 +128,9 @@ class VerletListModel(ModelInterface):
             flags |= L.OUT_STRESSES
         if m.precision == "fp64":
             flags |= L.MATH_FP64
-        L.call("tsb_vlist_forces", m.kind, L.ptr(table), m.n_species, L.ptr(species),
-               L.ptr(self.list), L.ptr(self.counts), L.ptr(pos), L.ptr(cell_row), L.ptr(sysi),
-               L.ptr(active), state.n_atoms, n_sys, L.dtype_code(pos.dtype), m.cutoff, flags,
-               L.ptr(energy), L.ptr(forces), L.ptr(stress), L.ptr(energies), L.ptr(stresses),
-               L.ptr(self.ws), self.ws.numel(), L.stream_ptr(pos.device))
+        torch.ops.tsb.vlist_forces_(m.kind, table, m.n_species, species, self.list, self.counts,
+                                    pos, cell_row, sysi, active, n_sys, m.cutoff, flags, energy,
+                                    forces, stress, energies, stresses, self.ws)
 
     # ------------------------------------------------- one large system
     def _single_ok(self, state):

@@ -21,6 +21,7 @@ from __future__ import annotations
 import torch
 
 from . import _lib as L
+from . import ops as _ops  # noqa: F401  (registers torch.ops.tsb.*)
 
 
 def _normalize(cell: torch.Tensor, pbc: torch.Tensor, n_systems: int):
@@ -62,26 +63,14 @@ def torchsim_nl(positions: torch.Tensor, cell: torch.Tensor, pbc: torch.Tensor,
     pos = positions.contiguous()
     sys_idx = system_idx.to(torch.int64).contiguous()
     flags = (L.NL_SELF_INTERACTION if self_interaction else 0) | (L.NL_HALF if half else 0)
-    ws_bytes = L.load().tsb_nl_workspace_size(n_atoms, n_systems)
-    ws = L.Workspace.get(dev, ws_bytes)
-    n_pairs = torch.zeros(1, dtype=torch.int64, device=dev)
-    stream = L.stream_ptr(dev)
     key = (n_atoms, n_systems, float(cutoff), flags)
     cap = _capacity_hint.get(key, 0)
-    for _ in range(2):
-        mapping = torch.empty((2, max(cap, 1)), dtype=torch.int64, device=dev)
-        sysmap = torch.empty(max(cap, 1), dtype=torch.int64, device=dev)
-        shifts = torch.empty((max(cap, 1), 3), dtype=dtype, device=dev)
-        L.call("tsb_nl_build", L.ptr(pos), L.ptr(cell_row), L.ptr(pbc_u8), L.ptr(sys_idx),
-               n_atoms, n_systems, L.dtype_code(dtype), float(cutoff), flags,
-               L.ptr(mapping), mapping.shape[1], L.ptr(sysmap), L.ptr(shifts), cap,
-               L.ptr(n_pairs), L.ptr(ws), ws.numel(), stream)
-        p = int(n_pairs.item())
-        if p <= cap:
-            break
-        cap = int(p * 1.15) + 16
-    _capacity_hint[key] = cap
-    return mapping[:, :p].contiguous(), sysmap[:p].contiguous(), shifts[:p].contiguous()
+    mapping, sysmap, shifts = torch.ops.tsb.nl_build(pos, cell_row, pbc_u8, sys_idx,
+                                                     float(cutoff), flags, n_systems, cap)
+    p = mapping.shape[1]
+    if p > cap:
+        _capacity_hint[key] = int(p * 1.15) + 16
+    return mapping, sysmap, shifts
 
 
 # names of the reference backends this replaces

@@ -23,6 +23,7 @@ from __future__ import annotations
 import torch
 
 from . import _lib as L
+from . import ops as _ops  # noqa: F401  (registers torch.ops.tsb.*)
 from .state import CellFireState, FireState
 
 ASE, VV = "ase_fire", "vv_fire"
@@ -56,10 +57,9 @@ def _eval_model(state, model, active=None):
 
 
 def _cell_forces(state, init, active=None):
-    L.call("tsb_frechet_cell_forces", L.ptr(state.cell_forces), L.ptr(state.stress),
-           L.ptr(state.cell), L.ptr(state.reference_cell), L.ptr(state.pressure),
-           L.ptr(state.cell_factor), state.n_systems, int(init), L.ptr(active),
-           L.dtype_code(state.dtype), L.stream_ptr(state.device))
+    torch.ops.tsb.frechet_cell_forces_(state.cell_forces, state.stress, state.cell,
+                                       state.reference_cell, state.pressure, state.cell_factor,
+                                       int(init), active)
 
 
 def fire_init(state, model, *, dt_start=0.1, alpha_start=0.1, fire_flavor=ASE,
@@ -108,22 +108,16 @@ def fire_init(state, model, *, dt_start=0.1, alpha_start=0.1, fire_flavor=ASE,
 
 def _fire_kernel(name, state, hyper, active):
     is_cell = isinstance(state, CellFireState)
-    ws = L.Workspace.get(state.device, L.load().tsb_fire_workspace_size(state.n_systems))
-    P = L.ptr
-    L.call(name, 1 if is_cell else 0, P(state.positions), P(state.velocities),
-           P(state.forces), P(state.masses), P(state.system_idx), state.n_atoms,
-           state.n_systems, P(state.dt), P(state.alpha), P(state.n_pos),
-           P(state.cell) if is_cell else None,
-           P(state.reference_cell) if is_cell else None,
-           P(state.cell_factor) if is_cell else None,
-           P(state.cell_positions) if is_cell else None,
-           P(state.cell_velocities) if is_cell else None,
-           P(state.cell_forces) if is_cell else None,
-           P(state.cell_masses) if is_cell else None, P(active),
-           float(hyper["dt_max"]), int(hyper["n_min"]), float(hyper["f_inc"]),
-           float(hyper["f_dec"]), float(hyper["alpha_start"]), float(hyper["f_alpha"]),
-           float(hyper["max_step"]), float(hyper["eps"]), L.dtype_code(state.dtype), P(ws),
-           ws.numel(), L.stream_ptr(state.device))
+    c = (lambda k: getattr(state, k)) if is_cell else (lambda k: None)  # noqa: E731
+    op = {"tsb_fire_ase_pre": torch.ops.tsb.fire_ase_pre_,
+          "tsb_fire_vv_pre": torch.ops.tsb.fire_vv_pre_,
+          "tsb_fire_vv_post": torch.ops.tsb.fire_vv_post_}[name]
+    op(1 if is_cell else 0, state.positions, state.velocities, state.forces, state.masses,
+       state.system_idx, state.dt, state.alpha, state.n_pos, c("cell"), c("reference_cell"),
+       c("cell_factor"), c("cell_positions"), c("cell_velocities"), c("cell_forces"),
+       c("cell_masses"), active, float(hyper["dt_max"]), int(hyper["n_min"]),
+       float(hyper["f_inc"]), float(hyper["f_dec"]), float(hyper["alpha_start"]),
+       float(hyper["f_alpha"]), float(hyper["max_step"]), float(hyper["eps"]))
 
 
 def _contiguous(state):
@@ -175,10 +169,8 @@ def converged_mask(state, fmax, include_cell_forces, active, n_active):
     cf = state.cell_forces if (include_cell_forces and isinstance(state, CellFireState)) else None
     if include_cell_forces and cf is None:
         raise ValueError("cell_forces not found in state")
-    ws = L.Workspace.get(state.device, L.load().tsb_fire_workspace_size(state.n_systems))
-    L.call("tsb_fire_converged", L.ptr(state.forces), L.ptr(state.system_idx), state.n_atoms,
-           state.n_systems, L.ptr(cf), float(fmax), L.ptr(active), L.ptr(n_active),
-           L.dtype_code(state.dtype), L.ptr(ws), ws.numel(), L.stream_ptr(state.device))
+    torch.ops.tsb.fire_converged_(state.forces, state.system_idx, state.n_systems, cf,
+                                  float(fmax), active, n_active)
 
 
 def optimize(state, model, *, fmax=1e-3, max_steps=10000, cell_filter="frechet",
