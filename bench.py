@@ -95,6 +95,8 @@ def parse():
                     help="batched_md: integrator inside the fused kernel and the plain path")
     ap.add_argument("--list-skin", type=float, default=1.5,
                     help="relax workload: Verlet-list skin in A (0 = cell-list search per call)")
+    ap.add_argument("--graph-steps", type=int, default=50,
+                    help="relax workload: FIRE steps per CUDA-graph replay (0 = eager loop)")
     ap.add_argument("--workload", default="batched_md",
                     choices=["batched_md", "single_large", "relax", "adjoint"])
     return ap.parse_args()
@@ -349,7 +351,8 @@ def run_relax(args):
     with ClockSampler(0) as clocks:
         a.record()
         st, steps, conv = optimizers.optimize(st, m, fmax=1e-3, max_steps=args.md_steps * 20,
-                                              cell_filter="frechet", check_every=50)
+                                              cell_filter="frechet", check_every=50,
+                                              graph_steps=args.graph_steps)
         b.record()
         torch.cuda.synchronize()
     t = a.elapsed_time(b) / 1e3
@@ -364,6 +367,7 @@ def run_relax(args):
             "data": "synthetic (Kob-Andersen 80:20, rho = 1.2 sigma^-3, uniform random)",
             "config": {"workload": "relax", "systems": st.n_systems, "atoms": n,
                        "fire_steps": steps, "converged": int(conv.sum()),
+                       "graph_steps_per_replay": args.graph_steps,
                        "time_to_all_converged_s": t, "fmax": 1e-3,
                        "neighbour_lists": (f"Verlet, skin {args.list_skin} A, "
                                            f"{m.n_builds} builds" if args.list_skin > 0

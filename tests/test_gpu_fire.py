@@ -128,3 +128,35 @@ def test_fire_nan_isolation():
     other = ~sel
     assert torch.equal(a.positions[other], b.positions[other])
     assert torch.isfinite(b.positions).all()
+
+
+def test_graph_replayed_relax_equals_eager_steps():
+    """The relax loop as CUDA-graph replays (FIRE + Frechet step, device-decided
+    Verlet-list rebuilds, convergence mask) equals the same steps run eagerly,
+    bitwise, and leaves converged systems frozen."""
+    from tsb import models, optimizers, workloads
+    from tsb.state import state_from_arrays
+
+    d = workloads.kob_andersen_batch(5, 64, 200, seed=12)
+    outs = []
+    for graph in (False, True):
+        st = state_from_arrays(d, device="cuda")
+        m = models.VerletListModel(_ka_model(), skin=1.0)
+        st = optimizers.fire_init(st, m, cell_filter="frechet")
+        n_steps, k = 60, 20
+        if graph:
+            st, steps, conv = optimizers.optimize(st, m, fmax=1e-9, max_steps=n_steps,
+                                                  cell_filter="frechet", graph_steps=k)
+            assert steps == n_steps
+        else:
+            active = torch.ones(st.n_systems, dtype=torch.uint8, device="cuda")
+            n_active = torch.zeros(1, dtype=torch.int32, device="cuda")
+            optimizers.converged_mask(st, 1e-9, True, active, n_active)
+            for _ in range(n_steps):
+                optimizers.fire_step(st, m, active=active)
+                optimizers.converged_mask(st, 1e-9, True, active, n_active)
+        torch.cuda.synchronize()
+        outs.append((st.positions.clone(), st.cell.clone(), st.energy.clone(),
+                     st.forces.clone(), m.n_builds))
+    for a, b in zip(outs[0][:4], outs[1][:4]):
+        assert torch.equal(a, b)

@@ -192,7 +192,53 @@ def test_fused_rejects_unsupported():
                             energy=torch.zeros(1, dtype=torch.float64, device="cuda"),
                             forces=torch.zeros_like(st.positions))
     with pytest.raises(integrators.FusedMDError):
-        integrators.run_md(md, m, 1, integrator="nve", dt=0.1)
+        integrators.FusedMD(md, m, integrator="nve", dt=0.1)
+
+
+def test_run_md_routes_oversized_systems_and_bins():
+    """A batch with systems above the fused kernel's 512 atoms: those advance
+    through the per-call steps (as they would alone), the rest through the fused
+    kernel (in memory-bounded bins when max_memory_scaler is given), each system
+    exactly as when it runs by itself (torch_sim/autobatching.py:475-765 is the
+    admission policy this replaces)."""
+    from tsb import integrators, models, workloads
+    from tsb.state import select_systems, state_from_arrays
+
+    big = workloads.argon_fcc((6, 6, 6), jitter=0.05, seed=4)
+    small = workloads.argon_fcc((3, 3, 3), jitter=0.05, seed=5, n_systems=3)
+    from tsb.workloads import _pack  # noqa: PLC2701
+
+    def split(d):
+        out = []
+        off = np.concatenate([[0], np.cumsum(np.bincount(d["system_idx"]))])
+        for s in range(len(off) - 1):
+            a, b = off[s], off[s + 1]
+            out.append({"positions": d["positions"][a:b], "cell_row": d["cell"][s].T,
+                        "masses": d["masses"][a:b], "atomic_numbers": d["atomic_numbers"][a:b]})
+        return out
+
+    systems = split(small)[:1] + split(big) + split(small)[1:]
+    d = _pack(systems)
+    st = state_from_arrays(d, device="cuda")
+    st.rng = 3
+    m = models.LennardJonesModel(sigma=3.405, epsilon=0.0104)
+    md = integrators.nve_init(st, m, kT=40 * workloads.KB_EV)
+    dt = 0.002 * workloads.METAL_TIME
+    ref = [integrators.run_md(select_systems(md, [s]), m, 20, integrator="nve", dt=dt, skin=0.5)
+           if s != 1 else None for s in range(4)]
+    alone = select_systems(md, [1])
+    for _ in range(20):
+        alone = integrators.nve_step(alone, m, dt=dt)
+    ref[1] = alone
+    for scaler in (None, 3000.0):
+        out, reb = integrators.run_md(md.clone(), m, 20, integrator="nve", dt=dt, skin=0.5,
+                                      return_rebuilds=True, max_memory_scaler=scaler)
+        assert int(reb[1]) == -1 and bool((reb[[0, 2, 3]] >= 1).all())
+        for s in range(4):
+            got = select_systems(out, [s])
+            assert torch.equal(got.positions, ref[s].positions), (scaler, s)
+            assert torch.equal(got.momenta, ref[s].momenta), (scaler, s)
+            assert torch.equal(got.energy, ref[s].energy), (scaler, s)
 
 
 def test_fused_adaptive_skin_same_physics():

@@ -973,9 +973,51 @@ class FusedMD:
         return s
 
 
+def _scatter_back(state, sub, systems, chain: bool):
+    """Write a sub-state's per-atom and per-system results into ``state``."""
+    dev = state.device
+    sel = torch.as_tensor(sorted(systems), dtype=torch.long, device=dev)
+    keep = torch.zeros(state.n_systems, dtype=torch.bool, device=dev)
+    keep[sel] = True
+    atoms = keep[state.system_idx]
+    for name in ("positions", "momenta", "forces"):
+        getattr(state, name)[atoms] = getattr(sub, name).to(getattr(state, name).dtype)
+    state.energy[sel] = sub.energy.to(state.energy.dtype)
+    if chain:
+        for name in ("positions", "momenta", "masses", "kinetic_energy"):
+            getattr(state.chain, name)[sel] = getattr(sub.chain, name)
+
+
+def _run_fused(state, model, n_steps, integrator, dt, kT, gamma, skin, seed, check, tau):
+    r = FusedMD(state, model, integrator=integrator, dt=dt, kT=kT, gamma=gamma, skin=skin,
+                seed=seed, tau=tau)
+    r.launch(n_steps)
+    if check:
+        r.check()
+    r.write_back()
+    return r.rebuilds
+
+
+def _run_per_call(state, model, n_steps, integrator, dt, kT, gamma, seed, tau):
+    """Systems too large for the fused kernel: the per-call step functions."""
+    if seed is not None:
+        state._philox_seed = seed
+    for _ in range(n_steps):
+        if integrator == "nve":
+            nve_step(state, model, dt=dt)
+        elif integrator == "nvt_langevin":
+            nvt_langevin_step(state, model, dt=dt, kT=kT, gamma=gamma)
+        elif integrator == "nvt_vrescale":
+            nvt_vrescale_step(model, state, dt=dt, kT=kT, tau=tau)
+        else:
+            nvt_nose_hoover_step(state, model, dt=dt, kT=kT)
+    return state
+
+
 def run_md(state, model, n_steps: int, *, integrator: str = "nvt_langevin", dt, kT=None,
            gamma=None, skin: float | str = 0.7, seed: int | None = None, check: bool = True,
-           return_rebuilds: bool = False, tau=None):
+           return_rebuilds: bool = False, tau=None, max_memory_scaler: float | None = None,
+           memory_scales_with: str = "n_atoms_x_density"):
     """Advance every system ``n_steps`` in ONE persistent kernel launch.
 
     Same update rules as ``nve_step`` / ``nvt_langevin_step`` (Langevin noise
@@ -985,16 +1027,60 @@ def run_md(state, model, n_steps: int, *, integrator: str = "nvt_langevin", dt, 
     Verlet list (cutoff + skin)
     rebuilt when any atom of a system moved more than skin/2.  ``model`` must be
     a :class:`tsb.models.PairTableModel` (LJ / Morse / soft sphere, any species
-    table); all axes must be periodic and systems may have up to
-    ``tsb_fused_max_atoms()`` (512) atoms.  ``state`` is updated in place
+    table); all axes must be periodic.  ``state`` is updated in place
     (positions, momenta, forces, energy).
+
+    Admission (the reference autobatcher's role, torch_sim/autobatching.py:475-765):
+    systems with more atoms than ``tsb_fused_max_atoms()`` (512) advance through
+    the per-call step functions instead of the fused kernel; with
+    ``max_memory_scaler`` the other systems run in launches whose summed memory
+    cost (``memory_scales_with``, see ``tsb.autobatching``) stays below it.
+    ``return_rebuilds`` gives per-system list builds (-1 for systems advanced per
+    call).
     """
-    r = FusedMD(state, model, integrator=integrator, dt=dt, kT=kT, gamma=gamma, skin=skin,
-                seed=seed, tau=tau)
-    r.launch(n_steps)
-    if check:
-        r.check()
-    r.write_back()
-    if return_rebuilds:
-        return state, r.rebuilds
-    return state
+    counts = torch.bincount(state.system_idx, minlength=state.n_systems)
+    big = counts > L.load().tsb_fused_max_atoms()
+    any_big = bool(big.any())
+    if not any_big and max_memory_scaler is None:
+        rebuilds = _run_fused(state, model, n_steps, integrator, dt, kT, gamma, skin, seed,
+                              check, tau)
+        return (state, rebuilds) if return_rebuilds else state
+    from .autobatching import BinningAutoBatcher
+    from .state import select_systems
+
+    if any_big and integrator == "nvt_nose_hoover":
+        raise FusedMDError("systems above the fused-kernel limit need nve, nvt_langevin or "
+                           "nvt_vrescale")
+    chain = integrator == "nvt_nose_hoover"
+    rebuilds = torch.full((state.n_systems,), -1, dtype=torch.int32, device=state.device)
+    small_idx = torch.nonzero(~big).flatten().tolist()
+    big_idx = torch.nonzero(big).flatten().tolist()
+    if small_idx:
+        sub = select_systems(state, small_idx) if any_big else state
+        if max_memory_scaler is None:
+            groups = [(sub, list(range(len(small_idx))))]
+        else:
+            ab = BinningAutoBatcher(model, memory_scales_with=memory_scales_with,
+                                    max_memory_scaler=max_memory_scaler)
+            ab.load_states(sub)
+            groups = list(ab)
+        for part, idx in groups:
+            if part is not sub:
+                for k in ("_philox_seed", "_philox_counter"):
+                    if hasattr(sub, k):
+                        setattr(part, k, getattr(sub, k))
+            rb = _run_fused(part, model, n_steps, integrator, dt, kT, gamma, skin, seed, check,
+                            tau)
+            if part is not sub:
+                _scatter_back(sub, part, idx, chain)
+            rebuilds[torch.as_tensor([small_idx[i] for i in idx], device=state.device)] = rb
+        if sub is not state:
+            _scatter_back(state, sub, small_idx, chain)
+    if big_idx:
+        sub = select_systems(state, big_idx)
+        for k in ("_philox_seed", "_philox_counter"):
+            if hasattr(state, k):
+                setattr(sub, k, getattr(state, k))
+        _run_per_call(sub, model, n_steps, integrator, dt, kT, gamma, seed, tau)
+        _scatter_back(state, sub, big_idx, chain)
+    return (state, rebuilds) if return_rebuilds else state

@@ -48,6 +48,10 @@ class VerletListModel(ModelInterface):
         self.n_builds = 0
         self._key = None
         self._last_single = False
+        # graph-safe mode: the rebuild is decided on the device (no host reads),
+        # list overflow is recorded in a sticky device flag (see set_graph_safe)
+        self.graph_safe = False
+        self.sticky = None
 
     # -------------------------------------------------------------- buffers
     def _ensure(self, state, pos, cell_row):
@@ -78,10 +82,46 @@ class VerletListModel(ModelInterface):
     def _reset(self, n, ns, dev):
         L.call("tsb_vlist_reset", n, ns, L.ptr(self.ws), self.ws.numel(), L.stream_ptr(dev))
 
+    def set_graph_safe(self, on: bool = True) -> None:
+        """Graph-safe mode for CUDA-graph capture of step loops: every call checks
+        the lists and launches the rebuild unconditionally (the rebuild kernels
+        only touch the systems the check marked as expired), and nothing is read
+        back to the host.  A list that overflows or a cell narrower than cutoff +
+        skin is recorded in ``self.sticky`` (device int32 [1], maximum over
+        calls); ``check_overflow()`` reads it after a replay."""
+        self.graph_safe = bool(on)
+
+    def check_overflow(self) -> int:
+        """0, or the neighbour count that overflowed the lists since the last
+        reset (1 << 30 for a cell narrower than cutoff + skin)."""
+        return 0 if self.sticky is None else int(self.sticky.item())
+
+    def grow(self, needed: int, state) -> None:
+        """Regrow the lists to hold ``needed`` neighbours per atom and mark every
+        system for a rebuild (after an overflow seen by check_overflow)."""
+        if needed >= (1 << 30):
+            raise ValueError("VerletListModel needs every periodic cell width >= cutoff + skin")
+        dev = state.positions.device
+        self.cap = int(needed * 1.2) + 8
+        self.list = torch.empty(self.cap * state.n_atoms, dtype=torch.int32, device=dev)
+        self._reset(state.n_atoms, state.n_systems, dev)
+        if self.sticky is not None:
+            self.sticky.zero_()
+
     # ---------------------------------------------------------------- lists
     def _update_lists(self, state, pos, cell_row, pbc, sysi, species, active):
         n, ns, dev = state.n_atoms, state.n_systems, pos.device
         cutoff = self.model.cutoff
+        if self.graph_safe:
+            if self.sticky is None or self.sticky.device != dev:
+                self.sticky = torch.zeros(1, dtype=torch.int32, device=dev)
+            torch.ops.tsb.vlist_check_(pos, cell_row, sysi, active, ns, cutoff, self.skin,
+                                       self.flags, self.ws)
+            torch.ops.tsb.vlist_build_(pos, cell_row, pbc, sysi, species, ns, cutoff, self.skin,
+                                       self.list, self.counts, self.cap, self.max_system_atoms,
+                                       self.flags, self.ws)
+            torch.maximum(self.sticky, self.flags[1:], out=self.sticky)
+            return
         while True:
             torch.ops.tsb.vlist_check_(pos, cell_row, sysi, active, ns, cutoff, self.skin,
                                        self.flags, self.ws)

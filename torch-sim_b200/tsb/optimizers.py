@@ -173,13 +173,92 @@ def converged_mask(state, fmax, include_cell_forces, active, n_active):
                                   float(fmax), active, n_active)
 
 
+_GRAPH_FIELDS = ("positions", "velocities", "forces", "energy", "stress", "dt", "alpha", "n_pos",
+                 "cell", "cell_positions", "cell_velocities", "cell_forces")
+
+
+def _snapshot(state):
+    return {k: getattr(state, k).clone() for k in _GRAPH_FIELDS
+            if isinstance(getattr(state, k, None), torch.Tensor)}
+
+
+def _restore(state, snap):
+    for k, v in snap.items():
+        getattr(state, k).copy_(v)
+
+
+def _optimize_graph(state, model, fmax, max_steps, fire_flavor, include_cell_forces, active,
+                    n_active, graph_steps, step_kwargs):
+    """The relax loop as CUDA-graph replays of ``graph_steps`` (FIRE step +
+    device convergence mask) each; the host reads the number of active systems
+    once per replay.  Needs a model whose calls read nothing back to the host
+    (a VerletListModel in graph-safe mode, or a per-call PairTableModel)."""
+    from .models.verlet import VerletListModel
+
+    vl = model if isinstance(model, VerletListModel) else None
+    if vl is not None:
+        vl.set_graph_safe(True)
+    dev = state.device
+
+    def body():
+        for _ in range(graph_steps):
+            fire_step(state, model, fire_flavor=fire_flavor, active=active, **step_kwargs)
+            converged_mask(state, fmax, include_cell_forces, active, n_active)
+
+    steps = 0
+    try:
+        while steps < max_steps:
+            # warm-up pass outside capture (workspaces, cached sizes), undone after
+            snap = _snapshot(state)
+            act0 = active.clone()
+            s = torch.cuda.Stream(dev)
+            s.wait_stream(torch.cuda.current_stream(dev))
+            with torch.cuda.stream(s):
+                fire_step(state, model, fire_flavor=fire_flavor, active=active, **step_kwargs)
+                converged_mask(state, fmax, include_cell_forces, active, n_active)
+            torch.cuda.current_stream(dev).wait_stream(s)
+            torch.cuda.synchronize(dev)
+            _restore(state, snap)
+            active.copy_(act0)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                body()
+            regrow = False
+            while steps < max_steps:
+                snap = _snapshot(state)
+                act0 = active.clone()
+                g.replay()
+                over = vl.check_overflow() if vl is not None else 0
+                if over:
+                    # a list overflowed inside the replay: undo it, grow, recapture
+                    _restore(state, snap)
+                    active.copy_(act0)
+                    vl.grow(over, state)
+                    regrow = True
+                    break
+                steps += graph_steps
+                if int(n_active.item()) == 0:
+                    return steps
+            del g
+            if not regrow:
+                break
+    finally:
+        if vl is not None:
+            vl.set_graph_safe(False)
+    return steps
+
+
 def optimize(state, model, *, fmax=1e-3, max_steps=10000, cell_filter="frechet",
              fire_flavor=ASE, include_cell_forces=None, check_every=20, init_kwargs=None,
-             **step_kwargs):
+             graph_steps=0, **step_kwargs):
     """Relax every system of the batch to max|F| < fmax with FIRE.
 
     Converged systems are frozen on the device after every step; the host reads
     the number of still-active systems every ``check_every`` steps to stop.
+    With ``graph_steps`` > 0 the loop runs as replays of one CUDA graph of
+    ``graph_steps`` steps (FIRE step, device-decided Verlet-list rebuilds,
+    convergence mask), read back once per replay; the step count is then a
+    multiple of graph_steps, and converged systems stay frozen inside a replay.
     Returns ``(state, steps, converged)``; ``converged`` is a bool [S] tensor.
     """
     if include_cell_forces is None:
@@ -192,6 +271,11 @@ def optimize(state, model, *, fmax=1e-3, max_steps=10000, cell_filter="frechet",
     n_active = torch.zeros(1, dtype=torch.int32, device=state.device)
     steps = 0
     converged_mask(state, fmax, include_cell_forces, active, n_active)
+    if graph_steps > 0:
+        _contiguous(state)
+        steps = _optimize_graph(state, model, fmax, max_steps, fire_flavor, include_cell_forces,
+                                active, n_active, int(graph_steps), step_kwargs)
+        return state, steps, active == 0
     while steps < max_steps:
         fire_step(state, model, fire_flavor=fire_flavor, active=active, **step_kwargs)
         converged_mask(state, fmax, include_cell_forces, active, n_active)
