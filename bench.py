@@ -591,7 +591,7 @@ def main():
                        WORKLOAD.replace("NVT-Langevin BAOAB", INTEGRATOR_NAMES[args.integrator]),
                        "n_systems": args.n_systems,
                        "atoms_per_gpu": n_atoms, "md_steps_per_step": args.md_steps,
-                       "verlet_skin_A": runner.skin,
+                       "verlet_skin_A": runner.skin, "lanes_per_atom_max": runner.lanes,
                        "skin_source": "autotuner" if args.skin == "auto" else "argument",
                        "precision": "FP32 pair math, FP64 state",
                        "mean_steps_between_list_rebuilds": rebuild_interval,

@@ -548,7 +548,10 @@ int tsb_fused_md_nvt(int thermostat, int potential, const double *table, int n_s
  * f = step / report_every - 1 (f < n_frames): positions as float32 into
  * frame_x [n_frames, N, 3] and each system's potential energy into
  * frame_e [n_frames, S] -- the device side of the reference's
- * TrajectoryReporter (torch_sim/trajectory.py:267-340, coerce_to_float32). */
+ * TrajectoryReporter (torch_sim/trajectory.py:267-340, coerce_to_float32).
+ * lanes_max (0 or a power of two <= 32; 0 means 32) caps the threads that share
+ * one atom's neighbour list in small systems (a launch shape the autotuner
+ * picks; results do not depend on it). */
 int tsb_fused_md_ex(int integrator, int potential, const double *table, int n_species,
                     const int32_t *species, double *positions, double *momenta,
                     double *forces, const double *masses, const double *cell_row,
@@ -559,7 +562,7 @@ int tsb_fused_md_ex(int integrator, int potential, const double *table, int n_sp
                     double *chain_Q, double *chain_ke, const double *chain_dt,
                     int chain_length, int chain_steps, int sy_steps, uint64_t seed,
                     uint64_t counter, uint64_t *counter_dev, float *frame_x, double *frame_e,
-                    int64_t report_every, int64_t n_frames, double *energy,
+                    int64_t report_every, int64_t n_frames, int lanes_max, double *energy,
                     double *stress, int32_t *n_rebuilds, int32_t *status, void *workspace,
                     size_t workspace_bytes, void *stream);
 

@@ -59,3 +59,35 @@ def test_fused_md_with_auto_skin(tmp_path, monkeypatch):
     r.check()
     b = integrators.run_md(md.clone(), m, 40, skin=0.3, **kw)
     np.testing.assert_allclose(r.x.cpu(), b.positions.cpu(), atol=1e-5)
+
+
+def test_lane_tuner_and_lane_invariance(tmp_path):
+    """The lane cap is timed and cached like the skin; trajectories with 4 and 32
+    lanes per atom agree to FP32 rounding (only the split of each list over
+    threads, and so the summation order, changes)."""
+    from tsb import autotune, integrators, workloads
+
+    md, m = _setup(16, seed=8)
+    kw = dict(integrator="nve", dt=0.002 * workloads.METAL_TIME)
+    cache = autotune.TuneCache(str(tmp_path / "t.json"))
+    calls = []
+
+    def timer(runner, n):
+        calls.append(runner.lanes)
+        return autotune._time_launch(runner, n)
+
+    best = autotune.tune_fused_lanes(md, m, skin=0.5, candidates=(4, 32), n_steps=30,
+                                     sample_systems=8, cache=cache, timer=timer, **kw)
+    assert best in (4, 32) and sorted(calls) == [4, 32]
+    calls.clear()
+    assert autotune.tune_fused_lanes(md, m, skin=0.5, candidates=(4, 32), cache=cache,
+                                     timer=timer, **kw) == best and calls == []
+    out = []
+    for lanes in (4, 32):
+        r = integrators.FusedMD(md.clone(), m, skin=0.5, lanes=lanes, **kw)
+        r.launch(40)
+        torch.cuda.synchronize()
+        r.check()
+        out.append((r.x.cpu().numpy(), r.energy.cpu().numpy()))
+    np.testing.assert_allclose(out[0][0], out[1][0], atol=1e-5)
+    np.testing.assert_allclose(out[0][1], out[1][1], rtol=1e-5)

@@ -98,6 +98,9 @@ struct FusedArgs {
   // per-system stress [S, 3, 3] at the last step (optional): -W / V with the
   // virial W = sum over pairs of r (x) f, accumulated in FP64
   double *stress;
+  // most lanes per atom (a power of two in 1..32; 0 means 32): small systems
+  // get the largest lane count with atoms x lanes <= kFusedThreads
+  int lanes_max;
 };
 
 // per-system geometry, computed by thread 0 into shared memory
@@ -469,7 +472,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       }
       const bool rep_ok = isfinite(d) && d != 0.0 && set_margins(g, A.cutoff, rc2d, nsp2);
       int tpa = 1;
-      while (tpa < 32 && g.n * tpa * 2 <= kFusedThreads) tpa *= 2;
+      const int lmax = A.lanes_max > 0 ? min(A.lanes_max, 32) : 32;
+      while (tpa * 2 <= lmax && g.n * tpa * 2 <= kFusedThreads) tpa *= 2;
       g.tpa = tpa;
       if (g.n <= 0) {
         g.ok = 0;
@@ -1260,9 +1264,10 @@ extern "C" int tsb_fused_md_ex(int integrator, int potential, const double *tabl
                                double *chain_ke, const double *chain_dt, int chain_length,
                                int chain_steps, int sy_steps, uint64_t seed, uint64_t counter,
                                uint64_t *counter_dev, float *frame_x, double *frame_e,
-                               int64_t report_every, int64_t n_frames, double *energy,
-                               double *stress, int32_t *n_rebuilds, int32_t *status,
-                               void *workspace, size_t workspace_bytes, void *stream) {
+                               int64_t report_every, int64_t n_frames, int lanes_max,
+                               double *energy, double *stress, int32_t *n_rebuilds,
+                               int32_t *status, void *workspace, size_t workspace_bytes,
+                               void *stream) {
   if (integrator < TSB_INT_NVE || integrator > TSB_INT_VRESCALE) return TSB_ERR_INVALID_ARG;
   if (potential < TSB_POT_LJ || potential > TSB_POT_SOFT) return TSB_ERR_INVALID_ARG;
   if (n_species < 1 || !table || (n_species > 1 && !species)) return TSB_ERR_INVALID_ARG;
@@ -1281,6 +1286,7 @@ extern "C" int tsb_fused_md_ex(int integrator, int potential, const double *tabl
       return TSB_ERR_INVALID_ARG;
   }
   if (report_every < 0 || n_frames < 0) return TSB_ERR_INVALID_ARG;
+  if (lanes_max < 0 || lanes_max > 32 || (lanes_max & (lanes_max - 1))) return TSB_ERR_INVALID_ARG;
   if (report_every > 0 && n_frames > 0 && (!frame_x || !frame_e)) return TSB_ERR_INVALID_ARG;
   Carver c(workspace, workspace_bytes);
   int64_t *lo = c.take<int64_t>(n_systems);
@@ -1307,6 +1313,7 @@ extern "C" int tsb_fused_md_ex(int integrator, int potential, const double *tabl
               chain_length, chain_steps, sy_steps, frame_x, frame_e,
               report_every > 0 && n_frames > 0 ? report_every : 0, n_frames, n_atoms};
   A.stress = stress;
+  A.lanes_max = lanes_max;
   const bool multi = n_species > 1;
   if (potential == TSB_POT_LJ) {
     multi ? launch_fused<TSB_POT_LJ, true>(A, grid, st) : launch_fused<TSB_POT_LJ, false>(A, grid, st);

@@ -1,7 +1,10 @@
 """Project-written autotuner for launch parameters that depend on the workload.
 
-The persistent fused MD kernel has one parameter whose best value depends on
-the physics rather than on the GPU alone: the Verlet skin.  A wider skin puts
+The persistent fused MD kernel has two tunable parameters: the Verlet skin
+(physics) and the launch shape of small systems, i.e. how many threads share
+one atom's neighbour list (``lanes``: 4, 8, 16 or 32 at most; more lanes split
+each list finer, but every lane repeats the atom's integration step).  First
+the skin.  A wider skin puts
 more pairs in the list (more pair evaluations every step); a narrower one makes
 atoms leave it sooner (more list rebuilds).  Where the balance lies depends on
 temperature, density, cutoff, time step and system sizes, so
@@ -9,7 +12,8 @@ temperature, density, cutoff, time step and system sizes, so
 systems and keeps the fastest, cached per device and workload signature in a
 JSON file (``TSB_AUTOTUNE_CACHE``, default ``~/.cache/tsb/autotune.json``).
 Results do not depend on the skin (only the rebuild rate does), so any choice
-is safe.  ``FusedMD(..., skin="auto")`` and ``run_md(..., skin="auto")`` use it.
+is safe.  Then, at that skin, :func:`tune_fused_lanes` times the lane caps the
+same way.  ``FusedMD(..., skin="auto")`` and ``run_md(..., skin="auto")`` use both.
 """
 
 from __future__ import annotations
@@ -23,6 +27,7 @@ import threading
 import torch
 
 DEFAULT_SKINS = (0.3, 0.5, 0.7, 1.0, 1.4)
+DEFAULT_LANES = (4, 8, 16, 32)
 
 
 def cache_path() -> str:
@@ -151,4 +156,56 @@ def tune_fused_skin(state, model, *, integrator: str = "nvt_langevin", dt, kT=No
     best = select_best(timings)
     cache.put(key, {"skin": best, "timings_ms": {str(k): v for k, v in timings.items()},
                     "n_steps": n_steps, "sample_systems": len(idx)})
+    return best
+
+
+def _sample(state, sample_systems):
+    from .state import select_systems
+
+    dev = state.device
+    if sample_systems is None:
+        n_sm = (torch.cuda.get_device_properties(dev).multi_processor_count
+                if dev.type == "cuda" else 1)
+        sample_systems = 2 * n_sm
+    idx = spread_sample(state.n_systems, sample_systems)
+    sample = select_systems(state, idx) if len(idx) < state.n_systems else state
+
+    def per_sys(v):
+        if v is None or not torch.is_tensor(v) or v.ndim == 0:
+            return v
+        return v.to(dev)[torch.as_tensor(idx, device=dev)]
+
+    return sample, per_sys, len(idx)
+
+
+def tune_fused_lanes(state, model, *, skin: float, integrator: str = "nvt_langevin", dt,
+                     kT=None, gamma=None, candidates=DEFAULT_LANES, n_steps: int = 200,
+                     sample_systems: int | None = None, cache: TuneCache | None = None,
+                     force: bool = False, timer=_time_launch) -> int:
+    """Lane cap (threads per atom) for ``FusedMD`` at a given skin, timed like
+    :func:`tune_fused_skin` and cached under the same workload signature; ties
+    go to fewer lanes."""
+    from .integrators import FusedMD
+
+    cache = cache or TuneCache()
+    dev = state.device
+    name = torch.cuda.get_device_name(dev) if dev.type == "cuda" else str(dev)
+    key = (f"fused_lanes|skin{_sig(skin, 3)}|" +
+           fused_signature(state, model, integrator, dt, kT, name))
+    if not force:
+        rec = cache.get(key)
+        if rec is not None and int(rec.get("lanes", -1)) in [int(c) for c in candidates]:
+            return int(rec["lanes"])
+    sample, per_sys, n_sample = _sample(state, sample_systems)
+    timings = {}
+    for lanes in candidates:
+        r = FusedMD(sample.clone(), model, integrator=integrator, dt=per_sys(dt),
+                    kT=per_sys(kT), gamma=per_sys(gamma), skin=float(skin), seed=0,
+                    lanes=int(lanes))
+        r.launch(n_steps)
+        timings[int(lanes)] = float(timer(r, n_steps))
+        r.check()
+    best = min(timings, key=lambda k: (timings[k], k))
+    cache.put(key, {"lanes": best, "timings_ms": {str(k): v for k, v in timings.items()},
+                    "n_steps": n_steps, "sample_systems": n_sample})
     return best

@@ -826,7 +826,8 @@ class FusedMD:
     """
 
     def __init__(self, state, model, *, integrator: str = "nvt_langevin", dt, kT=None,
-                 gamma=None, skin: float | str = 0.7, seed: int | None = None, tau=None):
+                 gamma=None, skin: float | str = 0.7, seed: int | None = None, tau=None,
+                 lanes: int | str | None = None):
         from .models.pair_potential import PairTableModel
 
         if not isinstance(model, PairTableModel):
@@ -896,7 +897,18 @@ class FusedMD:
 
             skin = tune_fused_skin(state, model, integrator=integrator, dt=dt, kT=kT,
                                    gamma=gamma)
+            if lanes is None:
+                lanes = "auto"
         self.skin = float(skin)
+        # threads per atom at most (small systems); "auto": the project autotuner
+        self.lanes = 32 if lanes is None else lanes
+        if self.lanes == "auto":
+            from .autotune import tune_fused_lanes
+
+            self.lanes = tune_fused_lanes(state, model, skin=self.skin, integrator=integrator,
+                                          dt=dt, kT=kT, gamma=gamma)
+        if self.lanes not in (1, 2, 4, 8, 16, 32):
+            raise ValueError(f"lanes must be a power of two in 1..32, got {self.lanes!r}")
         self.seed = (seed if seed is not None
                      else getattr(state, "_philox_seed", _seed_of(state))) & (2**64 - 1)
         # Philox counter lives on the device so that graph replays advance it
@@ -926,7 +938,7 @@ class FusedMD:
             self.dt_s, self.kT_s, self.g_s, getattr(self, "tau_s", None), g("cxi"), g("cpxi"),
             g("cQ"), g("cke"), g("cdt"), self.M if nh else 0, self.nc if nh else 0,
             self.nsy if nh else 0, _i64(self.seed), 0, self.counter_dev, fx, fe, int(every),
-            self.energy, self.stress, self.rebuilds, self.status, self.ws)
+            self.lanes, self.energy, self.stress, self.rebuilds, self.status, self.ws)
 
     def graph(self, n_steps: int) -> "torch.cuda.CUDAGraph":
         """CUDA graph of one ``launch(n_steps)``; ``g.replay()`` advances every system
