@@ -80,7 +80,8 @@ def test_initial_momenta_replay_the_reference_draw(c1):
     g = torch.Generator(device="cpu").manual_seed(2024)
     p = integrators.initialize_momenta(pos, torch.as_tensor(c1["init/masses"], device=dev),
                                        torch.as_tensor(c1["init/system_idx"], device=dev),
-                                       torch.as_tensor(float(c1["kT"]), device=dev), g)
+                                       torch.tensor(float(c1["kT"]), dtype=torch.float64,
+                                                    device=dev), g)
     np.testing.assert_allclose(p.cpu().numpy(), c1["lj/momenta"][0], rtol=1e-12, atol=1e-15)
 
 

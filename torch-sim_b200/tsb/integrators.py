@@ -37,7 +37,14 @@ from .state import MDState
 
 
 def _per_system(x, n_sys: int, device) -> torch.Tensor:
-    t = torch.as_tensor(x, dtype=torch.float64, device=device)
+    """Per-system float64 [S] on the device.  A scalar (Python number or a
+    one-element CPU tensor) becomes a fill on the device, with no host-to-device
+    copy, so the step functions can be captured in a CUDA graph."""
+    if torch.is_tensor(x) and x.device.type == "cpu" and x.numel() == 1:
+        x = float(x)
+    if not torch.is_tensor(x):
+        return torch.full((n_sys,), float(x), dtype=torch.float64, device=device)
+    t = x.to(device=device, dtype=torch.float64)
     if t.ndim == 0:
         t = t.expand(n_sys)
     return t.contiguous()
