@@ -50,18 +50,20 @@ def test_per_call_langevin_loop_captured_in_a_cuda_graph():
     # eager: 2 k steps
     for _ in range(2 * k):
         a = integrators.nvt_langevin_step(a, m, **kw)
-    # warm-up outside capture on a copy (workspaces, cached sizes), then capture
-    w = b.clone()
-    w._philox_seed, w._philox_counter = 11, 0
-    integrators.use_device_counter(w)
-    integrators.nvt_langevin_step(w, m, **kw)
-    torch.cuda.synchronize()
+    # warm-up on the state to be captured (workspaces, cached sizes), on a side
+    # stream, then put its state back
+    snap = {f: getattr(b, f).clone() for f in ("positions", "momenta", "forces", "energy")}
     g = torch.cuda.CUDAGraph()
     s = torch.cuda.Stream()
     s.wait_stream(torch.cuda.current_stream())
     with torch.cuda.stream(s):
-        integrators.nvt_langevin_step(w, m, **kw)  # warm-up on the capture stream
+        integrators.nvt_langevin_step(b, m, **kw)
     torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    for f, v in snap.items():
+        setattr(b, f, v.clone())
+    b._philox_counter = 0
+    b._philox_counter_dev.zero_()
     torch.cuda.synchronize()
     with torch.cuda.graph(g):
         for _ in range(k):

@@ -106,6 +106,7 @@ struct FusedArgs {
 // per-system geometry, computed by thread 0 into shared memory
 struct FusedGeom {
   double C[9];    // row-vector cell
+  float Cf[9];    // the same in FP32 (image shifts between list builds)
   double T[9];    // inv(C)^T: fractional coordinates u = T r
   double ctr[3];  // cell centre
   double tn[3];   // |row k of T|
@@ -155,14 +156,23 @@ __device__ inline bool set_margins(FusedGeom &g, double cutoff, const double *rc
     g.rep[k] = (int)ceil(g.h[k]);
     ok = ok && g.rep[k] <= 15;
   }
-  double ymax = 0.0;
+  double ymax = 0.0, ypmax = 0.0;
   for (int m = 0; m < 3; ++m) {
-    double y = 0.0;
-    for (int k = 0; k < 3; ++k) y += (0.5 + g.h[k]) * fabs(g.C[3 * k + m]);
+    double y = 0.0, yp = 0.0;
+    for (int k = 0; k < 3; ++k) {
+      y += (0.5 + g.h[k]) * fabs(g.C[3 * k + m]);
+      yp += (0.5 + g.rep[k]) * fabs(g.C[3 * k + m]);
+    }
     ymax = fmax(ymax, y);
+    ypmax = fmax(ypmax, yp);
   }
+  // Between list builds the images are refreshed in FP32 as fl(fl32(y) + s Cf):
+  // each coordinate is then off by at most 2^-24 (|y| + 4 |s C| + |y + s C|)
+  // <= 6 2^-24 Y', Y' = max_m sum_k (1/2 + rep_k) |C_km| (at the build they are
+  // fl32 of the FP64 image, off by 2^-24 Y <= 2^-24 Y'), so the band of the
+  // FP32 cutoff test uses 6 Y' for Y.
   g.band = (float)(2.0 * 5.9604644775390625e-8 *
-                   (4.0 * 1.7320508075688772 * ymax * cutoff + 6.0 * cutoff * cutoff));
+                   (4.0 * 1.7320508075688772 * 6.0 * ypmax * cutoff + 6.0 * cutoff * cutoff));
   const double margin = 1e-6 * (4.0 * ymax + R);
   g.build2 = (float)((R + margin) * (R + margin));
   for (int k = 0; k < nsp2; ++k) {
@@ -434,7 +444,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       g.n = (int)(A.hi[s] - g.start);
       g.ok = 1;
       double *C = g.C, *T = g.T;
-      for (int k = 0; k < 9; ++k) C[k] = A.cell_row[9 * s + k];
+      for (int k = 0; k < 9; ++k) {
+        C[k] = A.cell_row[9 * s + k];
+        g.Cf[k] = (float)C[k];
+      }
       const double d = C[0] * (C[4] * C[8] - C[5] * C[7]) - C[1] * (C[3] * C[8] - C[5] * C[6]) +
                        C[2] * (C[3] * C[7] - C[4] * C[6]);
       const double id = 1.0 / d;
@@ -968,11 +981,13 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       }
       // all warps are done reading the previous positions
       __syncthreads();
-      // refresh: the lanes of each atom rewrite the atom and its own images
+      // refresh: the lanes of each atom rewrite the atom and its own images, the
+      // images in FP32 from the atom's FP32 position and the FP32 cell
       if (own) {
+        const float fy0 = (float)y0, fy1 = (float)y1, fy2 = (float)y2;
         for (int it = lane; it <= gcnt; it += tpa) {
           if (it == 0) {
-            s_ext[a] = image_of(g, y0, y1, y2, 0, 0, 0, sp);
+            s_ext[a] = make_float4(fy0, fy1, fy2, __int_as_float(sp));
             Y[3 * a] = y0;
             Y[3 * a + 1] = y1;
             Y[3 * a + 2] = y2;
@@ -980,7 +995,13 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
             const int gg = gbeg + it - 1;
             int owner, sx, sy, sz;
             unpack_ghost(s_gshift[gg - n], owner, sx, sy, sz);
-            s_ext[gg] = image_of(g, y0, y1, y2, sx, sy, sz, sp);
+            const float fx = (float)sx, fyy = (float)sy, fz = (float)sz;
+            float4 e;
+            e.x = fy0 + fmaf(fz, g.Cf[6], fmaf(fyy, g.Cf[3], fx * g.Cf[0]));
+            e.y = fy1 + fmaf(fz, g.Cf[7], fmaf(fyy, g.Cf[4], fx * g.Cf[1]));
+            e.z = fy2 + fmaf(fz, g.Cf[8], fmaf(fyy, g.Cf[5], fx * g.Cf[2]));
+            e.w = __int_as_float(sp);
+            s_ext[gg] = e;
           }
         }
       }

@@ -221,10 +221,30 @@ def dtype_code(dtype: torch.dtype) -> int:
     raise TypeError(f"tsb kernels support float32/float64, got {dtype}")
 
 
+_PBC_CACHE: dict = {}
+
+
 def pbc_rows(pbc, n_systems: int, device) -> torch.Tensor:
     """Periodic flags as a contiguous uint8 [S, 3] tensor from a bool, a 0-d or
-    [3] tensor (every system alike), an [S, 3] tensor or a flat [3 S] one."""
-    p = torch.as_tensor(pbc, device=device)
+    [3] tensor (every system alike), an [S, 3] tensor or a flat [3 S] one.
+
+    Flags given on the host (a bool, a list or a CPU tensor) are converted once
+    and cached per (flags, S, device), so later calls -- inside a CUDA-graph
+    capture too -- copy nothing from the host."""
+    if not (torch.is_tensor(pbc) and pbc.device.type == "cuda"):
+        flags = torch.as_tensor(pbc).reshape(-1).tolist()
+        key = (tuple(bool(f) for f in flags), int(n_systems), str(torch.device(device)))
+        hit = _PBC_CACHE.get(key)
+        if hit is None:
+            if len(_PBC_CACHE) > 64:
+                _PBC_CACHE.clear()
+            hit = _pbc_rows(torch.as_tensor(pbc, device=device), n_systems)
+            _PBC_CACHE[key] = hit
+        return hit
+    return _pbc_rows(pbc, n_systems)
+
+
+def _pbc_rows(p: torch.Tensor, n_systems: int) -> torch.Tensor:
     if p.ndim == 0:
         p = p.reshape(1).expand(3)
     if p.ndim == 1 and p.shape[0] == 3:

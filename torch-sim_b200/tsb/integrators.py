@@ -42,9 +42,9 @@ def _per_system(x, n_sys: int, device) -> torch.Tensor:
     copy, so the step functions can be captured in a CUDA graph."""
     if torch.is_tensor(x) and x.device.type == "cpu" and x.numel() == 1:
         x = float(x)
-    if not torch.is_tensor(x):
+    if isinstance(x, (int, float)):
         return torch.full((n_sys,), float(x), dtype=torch.float64, device=device)
-    t = x.to(device=device, dtype=torch.float64)
+    t = torch.as_tensor(x, dtype=torch.float64, device=device)
     if t.ndim == 0:
         t = t.expand(n_sys)
     return t.contiguous()
@@ -150,13 +150,30 @@ def _apply_model(state, model):
     return out
 
 
+def _update_forces(state, model):
+    """Forces and energy of the new positions written into the state's own
+    tensors when the model can (``forward_into``), so the tensors a step reads
+    and writes keep their identity from step to step -- what lets a captured CUDA
+    graph of several steps be replayed; otherwise the model's outputs replace
+    them, as the reference's steps do (``state.forces = model_output["forces"]``)."""
+    f, e = getattr(state, "forces", None), getattr(state, "energy", None)
+    n_sys = state.n_systems
+    if (hasattr(model, "forward_into") and torch.is_tensor(f) and torch.is_tensor(e)
+            and f.is_contiguous() and e.is_contiguous() and f.shape == state.positions.shape
+            and tuple(e.shape) == (n_sys,) and f.dtype == e.dtype == state.dtype
+            and f.device == e.device == state.device):
+        model.forward_into(state, energy=e, forces=f)
+        return
+    _apply_model(state, model)
+
+
 def nve_step(state, model, *, dt, **_kw):
     """B(dt/2) A(dt) force B(dt/2) (nve.py:74-130)."""
     _prepare(state)
     dt_s = _per_system(dt, state.n_systems, state.device)
     _kick(state, dt_s, 0.5)
     _drift(state, dt_s, 1.0)
-    _apply_model(state, model)
+    _update_forces(state, model)
     _kick(state, dt_s, 0.5)
     return state
 
@@ -181,7 +198,7 @@ def nvt_langevin_step(state, model, *, dt, kT, gamma=None, noise=None, **_kw):
     state._philox_seed = seed
     if counter_dev is None:
         state._philox_counter = counter + 1
-    _apply_model(state, model)
+    _update_forces(state, model)
     _kick(state, dt_s, 0.5)
     return state
 
@@ -275,7 +292,7 @@ def nvt_nose_hoover_step(state, model, *, dt, kT, **_kw):
     _nhc_half(state, kT_s, recompute=False)
     _kick(state, dt_s, 0.5)
     _drift(state, dt_s, 1.0)
-    _apply_model(state, model)
+    _update_forces(state, model)
     _kick(state, dt_s, 0.5)
     _nhc_half(state, kT_s, recompute=True)
     return state
@@ -328,7 +345,7 @@ def nvt_vrescale_step(model, state, *, dt, kT, tau=None, noise=None, **_kw):
     state._philox_seed, state._philox_counter = seed, counter + 1
     _kick(state, dt_s, 0.5)
     _drift(state, dt_s, 1.0)
-    _apply_model(state, model)
+    _update_forces(state, model)
     _kick(state, dt_s, 0.5)
     return state
 

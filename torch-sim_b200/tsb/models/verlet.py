@@ -302,6 +302,15 @@ class VerletListModel(ModelInterface):
         for t in (energy, forces, stress):
             if t is not None and not t.is_contiguous():
                 raise ValueError("forward_into needs contiguous output buffers")
+        if sys_active is None and self._single_ok(state):
+            # one large system: its own kernels, results copied into the buffers
+            self._last_single = True
+            out = self._single_forward(state)
+            energy.copy_(out["energy"])
+            forces.copy_(out["forces"])
+            if stress is not None and "stress" in out:
+                stress.copy_(out["stress"])
+            return
         self._last_single = False
         self._run(state, energy, forces, stress if self._compute_stress else None, None, None,
                   sys_active)
