@@ -166,3 +166,67 @@ def full_to_half_list(mapping, system_mapping, shifts):
         keep = keep.copy()
         keep[same] = first > 0
     return mapping[:, keep], system_mapping[keep], shifts[keep]
+
+
+def neighbor_list_cells(positions, cell_row, cutoff, self_interaction=False):
+    """Full neighbour list of ONE fully periodic system by a cell list, for
+    systems too large for the all-pairs restatement (tens of thousands of atoms).
+
+    The reference's single-system linked cell (transforms.py:843-1006) bins
+    atoms into cells at least ``cutoff`` wide and pairs each cell with its 27
+    neighbours.  Here: positions wrapped into the cell (transforms.py:160-210),
+    fractional bins of at least ``cutoff`` in every direction (n_k =
+    floor(1 / (cutoff |b_k|)), b_k the reciprocal rows; requires n_k >= 3), and
+    for every bin and each of the 27 neighbour offsets the distances between all
+    atom pairs, with the periodic shift the offset implies.  Returns the pair set
+    in the layout and order of :func:`neighbor_list` (shifts valid for the
+    unwrapped input positions, torch_nl.py:214).
+    """
+    pos = np.asarray(positions, dtype=np.float64)
+    C = np.asarray(cell_row, dtype=np.float64).reshape(3, 3)
+    n = pos.shape[0]
+    T = np.linalg.inv(C)                      # fractional u = r @ T (row vectors)
+    u = pos @ T
+    wshift = np.floor(u)
+    uw = u - wshift
+    wrapped = uw @ C
+    recip = np.linalg.inv(C).T                # rows b_k
+    nb = np.floor(1.0 / (cutoff * np.linalg.norm(recip, axis=1))).astype(int)
+    if (nb < 3).any():
+        raise ValueError("neighbor_list_cells needs every cell width >= 3 cutoffs")
+    b = np.minimum((uw * nb).astype(int), nb - 1)
+    lin = (b[:, 0] * nb[1] + b[:, 1]) * nb[2] + b[:, 2]
+    order = np.argsort(lin, kind="stable")
+    counts = np.bincount(lin, minlength=int(np.prod(nb)))
+    start = np.concatenate([[0], np.cumsum(counts)])
+    rc2 = cutoff * cutoff
+    out_i, out_j, out_s = [], [], []
+    offs = np.array([(a, bb, c) for a in (-1, 0, 1) for bb in (-1, 0, 1) for c in (-1, 0, 1)])
+    bins3 = np.stack(np.unravel_index(np.arange(int(np.prod(nb))), nb), 1)
+    for off in offs:
+        nbr = bins3 + off
+        shift = np.floor_divide(nbr, nb)      # lattice shift of the neighbour bin
+        nbr = nbr - shift * nb
+        nlin = (nbr[:, 0] * nb[1] + nbr[:, 1]) * nb[2] + nbr[:, 2]
+        for bi in np.nonzero(counts)[0]:
+            bj = nlin[bi]
+            if counts[bj] == 0:
+                continue
+            ii = order[start[bi]:start[bi + 1]]
+            jj = order[start[bj]:start[bj + 1]]
+            s = shift[bi].astype(np.float64)
+            d = wrapped[jj][None, :, :] + (s @ C)[None, None, :] - wrapped[ii][:, None, :]
+            d2 = np.einsum("ijk,ijk->ij", d, d)
+            m = d2 < rc2
+            if not self_interaction and not s.any():
+                m &= ii[:, None] != jj[None, :]
+            a, c = np.nonzero(m)
+            out_i.append(ii[a])
+            out_j.append(jj[c])
+            out_s.append(np.broadcast_to(s, (len(a), 3)))
+    i = np.concatenate(out_i)
+    j = np.concatenate(out_j)
+    S = np.concatenate(out_s)
+    # the pair (i, j, S) on wrapped positions is (i, j, S + w_i - w_j) on the inputs
+    S = S + wshift[i] - wshift[j]
+    return sort_pairs(np.stack([i, j]), np.zeros(len(i), np.int64), S)

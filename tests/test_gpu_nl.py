@@ -123,3 +123,28 @@ def test_nl_large_system_properties():
     # fcc shells within 8.5 A at a = 5.26: 12 + 6 + 24 + 12 + 24 = 78 neighbours;
     # the 0.1 A jitter moves a few across the cutoff
     assert abs(m.shape[1] / n - 78.0) < 4.0
+
+
+@pytest.mark.parametrize("rc", [8.5, 9.5])
+def test_nl_32k_atom_pair_set_is_exact(rc):
+    """Config-2 geometry at 32,000 atoms (argon fcc 20x20x20, N(0, 0.1 A)
+    jitter, slightly sheared cell): the full pair set at the cutoff and at
+    cutoff + skin equals the oracle's integer-exactly (torch_nl.py:156-215)."""
+    from oracle import neighbors as onl
+    from tsb import neighbors, workloads
+
+    d = workloads.argon_fcc((20, 20, 20), jitter=0.1, seed=2)
+    rng = np.random.default_rng(4)
+    F = np.eye(3) + rng.normal(0, 0.01, (3, 3))
+    pos = d["positions"] @ F.T
+    C = d["cell"][0].T @ F.T
+    ref = onl.neighbor_list_cells(pos, C, rc)
+    dev = torch.device("cuda")
+    m, sm, sh = neighbors.torchsim_nl(torch.as_tensor(pos, device=dev),
+                                      torch.as_tensor(C, device=dev),
+                                      torch.ones(3, dtype=torch.bool, device=dev), rc,
+                                      torch.zeros(len(pos), dtype=torch.int64, device=dev))
+    got = onl.sort_pairs(m.cpu().numpy(), sm.cpu().numpy(), sh.cpu().numpy())
+    assert got[0].shape == ref[0].shape, (got[0].shape, ref[0].shape)
+    assert np.array_equal(got[0], ref[0])
+    assert np.array_equal(np.rint(got[2]).astype(np.int64), np.rint(ref[2]).astype(np.int64))

@@ -99,3 +99,22 @@ def test_trajectory_replay_matches_step_oracle(integrator):
     np.testing.assert_allclose(out["positions"], st["positions"], rtol=0, atol=1e-12)
     np.testing.assert_allclose(out["momenta"], st["momenta"], rtol=1e-10, atol=1e-12)
     np.testing.assert_allclose(out["energy"], st["energy"], rtol=1e-11)
+
+
+@pytest.mark.parametrize("cells,rc", [((4, 4, 4), 5.0), ((5, 4, 6), 6.3), ((6, 6, 6), 8.5)])
+def test_cell_list_oracle_equals_all_pairs_oracle(cells, rc):
+    """The cell-list restatement (for systems too large for all pairs) gives the
+    all-pairs oracle's pair set exactly on sheared, jittered cells with atoms
+    outside the cell."""
+    from oracle import neighbors as onl
+    from tsb import workloads
+
+    d = workloads.argon_fcc(cells, jitter=0.1, seed=3)
+    rng = np.random.default_rng(1)
+    F = np.eye(3) + rng.normal(0, 0.02, (3, 3))
+    pos = d["positions"] @ F.T + rng.normal(0, 2.0, d["positions"].shape)
+    C = d["cell"][0].T @ F.T
+    a = onl.neighbor_list_cells(pos, C, rc)
+    b = onl.neighbor_list(pos, C[None], np.ones(3, bool), rc, np.zeros(len(pos), np.int64))
+    assert np.array_equal(a[0], b[0])
+    assert np.array_equal(np.rint(a[2]), np.rint(b[2]))
