@@ -551,7 +551,13 @@ int tsb_fused_md_nvt(int thermostat, int potential, const double *table, int n_s
  * TrajectoryReporter (torch_sim/trajectory.py:267-340, coerce_to_float32).
  * lanes_max (0 or a power of two <= 32; 0 means 32) caps the threads that share
  * one atom's neighbour list in small systems (a launch shape the autotuner
- * picks; results do not depend on it). */
+ * picks; results do not depend on it).  n_wide >= 0 (with `order`) splits the
+ * systems over two block shapes: order[0 .. n_wide) run in 512-thread blocks,
+ * one per SM, and order[n_wide .. S) in 256-thread blocks, two per SM -- those
+ * systems must have at most 256 atoms and fit the narrow blocks' image table of
+ * 1968 entries at the given skin (else the skin is halved for them, or
+ * TSB_ERR_CAPACITY is reported); n_wide < 0 runs every system in 512-thread
+ * blocks. */
 int tsb_fused_md_ex(int integrator, int potential, const double *table, int n_species,
                     const int32_t *species, double *positions, double *momenta,
                     double *forces, const double *masses, const double *cell_row,
@@ -562,9 +568,9 @@ int tsb_fused_md_ex(int integrator, int potential, const double *table, int n_sp
                     double *chain_Q, double *chain_ke, const double *chain_dt,
                     int chain_length, int chain_steps, int sy_steps, uint64_t seed,
                     uint64_t counter, uint64_t *counter_dev, float *frame_x, double *frame_e,
-                    int64_t report_every, int64_t n_frames, int lanes_max, double *energy,
-                    double *stress, int32_t *n_rebuilds, int32_t *status, void *workspace,
-                    size_t workspace_bytes, void *stream);
+                    int64_t report_every, int64_t n_frames, int lanes_max, int64_t n_wide,
+                    double *energy, double *stress, int32_t *n_rebuilds, int32_t *status,
+                    void *workspace, size_t workspace_bytes, void *stream);
 
 /* ---- allocation-free fused MD -------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device

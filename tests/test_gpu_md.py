@@ -274,3 +274,25 @@ def test_fused_graph_replay_matches_direct_launches():
     b.check()
     assert a.counter == b.counter == 50
     assert torch.equal(a.x, b.x) and torch.equal(a.p, b.p) and torch.equal(a.energy, b.energy)
+
+
+def test_block_shapes_agree():
+    """The same batch run with every system in 512-thread blocks and with small
+    systems in 256-thread blocks (two per SM): the trajectories agree to FP32
+    rounding (the lane split of each neighbour list, and so the summation order,
+    differs) and both shapes are used."""
+    from tsb import integrators, workloads
+
+    md, m = _cu_state(24, seed=4)
+    kw = dict(integrator="nve", dt=0.002 * workloads.METAL_TIME, skin=0.5)
+    a = integrators.FusedMD(md.clone(), m, shapes="wide", **kw)
+    b = integrators.FusedMD(md.clone(), m, shapes="auto", **kw)
+    assert a.n_wide == -1 and 0 < b.n_wide < md.n_systems
+    for r in (a, b):
+        r.launch(40)
+        torch.cuda.synchronize()
+        r.check()
+    np.testing.assert_allclose(b.x.cpu().numpy(), a.x.cpu().numpy(), atol=1e-5)
+    np.testing.assert_allclose(b.energy.cpu().numpy(), a.energy.cpu().numpy(), rtol=1e-5)
+    np.testing.assert_allclose(b.stress.cpu().numpy(), a.stress.cpu().numpy(), rtol=1e-4,
+                               atol=1e-7)

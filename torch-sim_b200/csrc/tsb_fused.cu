@@ -40,6 +40,7 @@
 //     forces are held in registers and written over them at the end).
 #include <math.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "tsb_pair.cuh"
@@ -48,24 +49,46 @@
 
 namespace tsb {
 
-constexpr int kFusedThreads = 512;
 constexpr int kFusedMaxAtoms = 512;
-constexpr int kExtMax = 3328;        // atoms + ghost images per system
-constexpr int kListLen = 144;        // Verlet-list slots per thread (multiple of 4)
-constexpr int kListGroups = kListLen / 4;
-constexpr int kMaxBins = 2048;       // spatial bins over the image region
 constexpr int kFusedMaxSpecies = 4;
 constexpr int kMaxGrid = 296;        // upper bound on persistent CTAs
-constexpr size_t kSmemList = (size_t)kListGroups * kFusedThreads * sizeof(uint2);
-constexpr size_t kSmemExt = (size_t)kExtMax * sizeof(float4);
-constexpr size_t kSmemGhost = (size_t)kExtMax * sizeof(uint32_t);
-constexpr size_t kSmemSorted = (size_t)kExtMax * sizeof(uint16_t);
-constexpr size_t kSmemBins = (size_t)kMaxBins * sizeof(int);
-constexpr size_t kFusedSmem = kSmemList + kSmemExt + kSmemGhost + kSmemSorted + kSmemBins;
-// the bin of every entry is kept in the list area while the list is rebuilt
-static_assert(kExtMax * sizeof(uint16_t) <= kSmemList, "bin ids alias the list");
-static_assert(kMaxBins <= 4 * kFusedThreads, "bin scan: four bins per thread");
-static_assert((kExtMax - 1) * sizeof(float4) <= 0xFFFF, "list entries are 16-bit byte offsets");
+
+// Two block shapes.  Wide: 512 threads, one block per SM, any system of up to
+// 512 atoms.  Narrow: 256 threads and half the shared memory, two blocks per
+// SM, for systems of up to 256 atoms whose images fit its smaller table -- two
+// independent systems per SM hide each other's barrier and latency stalls
+// (1.4x the throughput of the wide shape on systems of up to 128 atoms).
+template <int NT>
+struct FusedShape;
+template <>
+struct FusedShape<512> {
+  static constexpr int kThreads = 512, kMinBlocks = 1;
+  static constexpr int kExtMax = 3328;   // atoms + ghost images per system
+  static constexpr int kListLen = 144;   // Verlet-list slots per thread (multiple of 4)
+  static constexpr int kMaxBins = 2048;  // spatial bins over the image region
+};
+template <>
+struct FusedShape<256> {
+  static constexpr int kThreads = 256, kMinBlocks = 2;
+  static constexpr int kExtMax = 1968;
+  static constexpr int kListLen = 128;
+  static constexpr int kMaxBins = 1024;
+};
+template <int NT>
+struct FusedSmem {
+  using S = FusedShape<NT>;
+  static constexpr size_t kList = (size_t)(S::kListLen / 4) * NT * sizeof(uint2);
+  static constexpr size_t kExt = (size_t)S::kExtMax * sizeof(float4);
+  static constexpr size_t kGhost = (size_t)S::kExtMax * sizeof(uint32_t);
+  static constexpr size_t kSorted = (size_t)S::kExtMax * sizeof(uint16_t);
+  static constexpr size_t kBins = (size_t)S::kMaxBins * sizeof(int);
+  static constexpr size_t kTotal = kList + kExt + kGhost + kSorted + kBins;
+  // the bin of every entry is kept in the list area while the list is rebuilt
+  static_assert(S::kExtMax * sizeof(uint16_t) <= kList, "bin ids alias the list");
+  static_assert(S::kMaxBins <= 4 * NT, "bin scan: four bins per thread");
+  static_assert((S::kExtMax - 1) * sizeof(float4) <= 0xFFFF,
+                "list entries are 16-bit byte offsets");
+};
 
 struct FusedArgs {
   int integrator, potential, n_species;
@@ -99,8 +122,10 @@ struct FusedArgs {
   // virial W = sum over pairs of r (x) f, accumulated in FP64
   double *stress;
   // most lanes per atom (a power of two in 1..32; 0 means 32): small systems
-  // get the largest lane count with atoms x lanes <= kFusedThreads
+  // get the largest lane count with atoms x lanes <= the block's threads
   int lanes_max;
+  // systems this launch takes from `order` (order[0 .. n_work)); 0: all n_sys
+  int64_t n_work;
 };
 
 // per-system geometry, computed by thread 0 into shared memory
@@ -147,6 +172,7 @@ struct FusedGeom {
 //     narrows the core radius.
 // Bins: width >= R |T_k| / 2 in fractional coordinate k, so two points closer
 // than R differ by at most 2 bins per axis; coarsened until <= kMaxBins.
+template <int kMaxBins>
 __device__ inline bool set_margins(FusedGeom &g, double cutoff, const double *rc2d, int nsp2) {
   bool ok = true;
   const double R = cutoff + g.skin;
@@ -218,7 +244,8 @@ __device__ inline void report(int32_t *status, int code, int64_t sys, int what, 
   }
 }
 
-// Block-wide exclusive scan of one int per thread (512 threads).
+// Block-wide exclusive scan of one int per thread (NT threads).
+template <int NT>
 __device__ inline int block_excl_scan_i(int v, int *total, int *sh) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int inc = v;
@@ -230,7 +257,7 @@ __device__ inline int block_excl_scan_i(int v, int *total, int *sh) {
   if (lane == 31) sh[warp] = inc;
   __syncthreads();
   if (warp == 0) {
-    const int nw = kFusedThreads / 32;
+    const int nw = NT / 32;
     int w = lane < nw ? sh[lane] : 0;
     int wi = w;
 #pragma unroll
@@ -250,13 +277,14 @@ __device__ inline int block_excl_scan_i(int v, int *total, int *sh) {
 
 // FP64 sum over the block in a fixed order (shuffles inside each warp, then the
 // warps in order); the result is valid in thread 0 only
+template <int NT>
 __device__ inline double block_sum_to0(double v, double *sh) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
   __syncthreads();
   double t = 0.0;
   if (threadIdx.x == 0)
-    for (int w = 0; w < kFusedThreads / 32; ++w) t += sh[w];
+    for (int w = 0; w < NT / 32; ++w) t += sh[w];
   return t;
 }
 
@@ -267,10 +295,11 @@ __device__ __forceinline__ void warp_sum_store(double t, double *sh) {
 }
 
 // Thread 0: out[c] = sum over warps of sh[c][warp], c < 7 (fixed order)
-__device__ __noinline__ void warps_sum7(const double (*sh)[kFusedThreads / 32], double *out) {
+template <int NT>
+__device__ __noinline__ void warps_sum7(const double (*sh)[NT / 32], double *out) {
   for (int c = 0; c < 7; ++c) {
     double t = 0.0;
-    for (int w = 0; w < kFusedThreads / 32; ++w) t += sh[c][w];
+    for (int w = 0; w < NT / 32; ++w) t += sh[c][w];
     out[c] = t;
   }
 }
@@ -399,8 +428,18 @@ __device__ __forceinline__ float2 pair_fr2(const Prm2 &k, const PairPrm<float> &
   }
 }
 
-template <int POT, bool MULTI>
-__global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
+template <int POT, bool MULTI, int NT>
+__global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(FusedArgs A) {
+  // the block shape's table sizes (these names shadow nothing at namespace scope)
+  constexpr int kFusedThreads = NT;
+  constexpr int kListLen = FusedShape<NT>::kListLen;
+  constexpr int kListGroups = kListLen / 4;
+  constexpr int kExtMax = FusedShape<NT>::kExtMax;
+  constexpr int kMaxBins = FusedShape<NT>::kMaxBins;
+  constexpr size_t kSmemList = FusedSmem<NT>::kList;
+  constexpr size_t kSmemExt = FusedSmem<NT>::kExt;
+  constexpr size_t kSmemGhost = FusedSmem<NT>::kGhost;
+  constexpr size_t kSmemSorted = FusedSmem<NT>::kSorted;
   // single-species LJ / Morse: pairs evaluated two at a time in FP32x2
   constexpr bool kPaired = !MULTI && POT != TSB_POT_SOFT;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -437,7 +476,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     if (tid == 0) s_work = atomicAdd(A.queue, 1);
     __syncthreads();
     const int64_t w = s_work;
-    if (w >= A.n_sys) break;
+    if (w >= (A.n_work > 0 ? A.n_work : A.n_sys)) break;
     const int64_t s = A.order ? A.order[w] : w;
     if (tid == 0) {
       g.start = A.lo[s];
@@ -483,7 +522,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
           }
         }
       }
-      const bool rep_ok = isfinite(d) && d != 0.0 && set_margins(g, A.cutoff, rc2d, nsp2);
+      const bool rep_ok = isfinite(d) && d != 0.0 && set_margins<kMaxBins>(g, A.cutoff, rc2d, nsp2);
       int tpa = 1;
       const int lmax = A.lanes_max > 0 ? min(A.lanes_max, 32) : 32;
       while (tpa * 2 <= lmax && g.n * tpa * 2 <= kFusedThreads) tpa *= 2;
@@ -494,7 +533,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
         if (A.stress)
           for (int k = 0; k < 9; ++k) A.stress[9 * s + k] = 0.0;
         if (A.n_rebuilds) A.n_rebuilds[s] = 0;
-      } else if (g.n > kFusedMaxAtoms || !rep_ok) {
+      } else if (g.n > (kFusedMaxAtoms < kFusedThreads ? kFusedMaxAtoms : kFusedThreads) ||
+                 !rep_ok) {
         g.ok = 0;
         report(A.status, TSB_ERR_UNSUPPORTED, s, 0, g.n);
       }
@@ -595,7 +635,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       }                                                                                      \
     }                                                                                        \
     int total;                                                                               \
-    const int goff = block_excl_scan_i(gcount, &total, s_scan);                              \
+    const int goff = block_excl_scan_i<NT>(gcount, &total, s_scan);                              \
     /* broadcast the lead's ghost range to the other lanes of its atom */                    \
     gbeg = __shfl_sync(0xffffffffu, n + goff, (threadIdx.x & 31) & ~(tpa - 1));              \
     gcnt = __shfl_sync(0xffffffffu, gcount, (threadIdx.x & 31) & ~(tpa - 1));                \
@@ -644,7 +684,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
           sum += c4[q];                                                                      \
         }                                                                                    \
         int tot_;                                                                            \
-        int off = block_excl_scan_i(sum, &tot_, s_scan);                                     \
+        int off = block_excl_scan_i<NT>(sum, &tot_, s_scan);                                     \
         for (int q = 0; q < 4; ++q) {                                                        \
           if (b0 + q < nbins) s_bin[b0 + q] = off;                                           \
           off += c4[q];                                                                      \
@@ -717,7 +757,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
     }                                                                                        \
     if (tid == 0) {                                                                          \
       g.skin = g.skin > 0.05 ? 0.5 * g.skin : 0.0;                                           \
-      set_margins(g, A.cutoff, rc2d, nsp2);                                                  \
+      set_margins<kMaxBins>(g, A.cutoff, rc2d, nsp2);                                                  \
     }                                                                                        \
     __syncthreads();                                                                         \
   }
@@ -917,7 +957,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       warp_sum_store(h_ * vxz, s_red7[5]);                                                   \
       warp_sum_store(h_ * vxy, s_red7[6]);                                                   \
       __syncthreads();                                                                       \
-      if (tid == 0) warps_sum7(s_red7, g.esum7);                                             \
+      if (tid == 0) warps_sum7<NT>(s_red7, g.esum7);                                             \
       __syncthreads();                                                                       \
     }                                                                                        \
   }
@@ -930,7 +970,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       // energy (nvt.py:715-741), or the first Nose-Hoover half step with the
       // kinetic energy carried from the last one (nvt.py:462-470)
       if (A.integrator == TSB_INT_VRESCALE) {
-        const double k2 = block_sum_to0(lead ? (px * px + py * py + pz * pz) * inv_m : 0.0,
+        const double k2 = block_sum_to0<NT>(lead ? (px * px + py * py + pz * pz) * inv_m : 0.0,
                                         s_red);
         if (tid == 0)
           g.th_scale = vrescale_lambda(k2, g.nf, g.kt, dt, g.tau, nullptr, A.seed, s,
@@ -1023,7 +1063,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fused_md(FusedArgs A) {
       }
       if (A.integrator == TSB_INT_NOSE_HOOVER) {
         // second half step with the kinetic energy after velocity Verlet
-        const double k2 = block_sum_to0(lead ? (px * px + py * py + pz * pz) * inv_m : 0.0,
+        const double k2 = block_sum_to0<NT>(lead ? (px * px + py * py + pz * pz) * inv_m : 0.0,
                                         s_red);
         if (tid == 0) {
           g.cke = 0.5 * k2;
@@ -1139,11 +1179,55 @@ __global__ void k_bounds_fused(const int64_t *sys, int64_t n, int64_t n_sys, int
   if (i == n - 1 || sys[i + 1] != s) hi[s] = i + 1;
 }
 
-template <int POT, bool MULTI>
+template <int POT, bool MULTI, int NT>
 static void launch_fused(const FusedArgs &A, int64_t grid, cudaStream_t st) {
-  cudaFuncSetAttribute(k_fused_md<POT, MULTI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)kFusedSmem);
-  k_fused_md<POT, MULTI><<<(unsigned)grid, kFusedThreads, kFusedSmem, st>>>(A);
+  cudaFuncSetAttribute(k_fused_md<POT, MULTI, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)FusedSmem<NT>::kTotal);
+  k_fused_md<POT, MULTI, NT><<<(unsigned)grid, NT, FusedSmem<NT>::kTotal, st>>>(A);
+}
+
+template <int NT>
+static void launch_shape(const FusedArgs &A, int64_t grid, cudaStream_t st) {
+  const bool multi = A.n_species > 1;
+  if (A.potential == TSB_POT_LJ) {
+    multi ? launch_fused<TSB_POT_LJ, true, NT>(A, grid, st)
+          : launch_fused<TSB_POT_LJ, false, NT>(A, grid, st);
+  } else if (A.potential == TSB_POT_MORSE) {
+    multi ? launch_fused<TSB_POT_MORSE, true, NT>(A, grid, st)
+          : launch_fused<TSB_POT_MORSE, false, NT>(A, grid, st);
+  } else {
+    multi ? launch_fused<TSB_POT_SOFT, true, NT>(A, grid, st)
+          : launch_fused<TSB_POT_SOFT, false, NT>(A, grid, st);
+  }
+}
+
+// One persistent launch over all systems (wide blocks), or, with an order whose
+// first n_wide systems need wide blocks, a wide launch over those and a narrow
+// launch (two blocks per SM) over the rest, one after the other on the stream.
+// queue[0] and queue[1] are the two launches' work counters (zeroed before).
+static void launch_all(FusedArgs A, int64_t n_wide, int32_t *queue, cudaStream_t st) {
+  int dev = 0, n_sm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t n = A.n_sys;
+  if (!A.order || n_wide < 0 || n_wide >= n) {
+    A.n_work = n;
+    A.queue = queue;
+    launch_shape<512>(A, std::min<int64_t>(std::min<int64_t>(n_sm, kMaxGrid), n), st);
+    return;
+  }
+  if (n_wide > 0) {
+    FusedArgs W = A;
+    W.n_work = n_wide;
+    W.queue = queue;
+    launch_shape<512>(W, std::min<int64_t>(std::min<int64_t>(n_sm, kMaxGrid), n_wide), st);
+  }
+  FusedArgs Nw = A;
+  Nw.order = A.order + n_wide;
+  Nw.n_work = n - n_wide;
+  Nw.queue = queue + 1;
+  launch_shape<256>(Nw, std::min<int64_t>(std::min<int64_t>(2 * n_sm, 2 * kMaxGrid), n - n_wide),
+                    st);
 }
 
 extern "C" int tsb_fused_md(int integrator, int potential, const double *table,
@@ -1173,12 +1257,6 @@ extern "C" int tsb_fused_md(int integrator, int potential, const double *table,
   int32_t *queue = c.take<int32_t>(4);
   if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
-  int dev = 0, n_sm = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-  int64_t grid = n_sm;
-  if (grid > kMaxGrid) grid = kMaxGrid;
-  if (grid > n_systems) grid = n_systems;
   cudaMemsetAsync(lo, 0, sizeof(int64_t) * n_systems, st);
   cudaMemsetAsync(hi, 0, sizeof(int64_t) * n_systems, st);
   cudaMemsetAsync(queue, 0, sizeof(int32_t) * 4, st);
@@ -1190,16 +1268,7 @@ extern "C" int tsb_fused_md(int integrator, int potential, const double *table,
               kT_sys, gamma_sys, seed, counter, counter_dev, energy, n_rebuilds, queue,
               status};
   A.stress = stress;
-  const bool multi = n_species > 1;
-  if (potential == TSB_POT_LJ) {
-    multi ? launch_fused<TSB_POT_LJ, true>(A, grid, st) : launch_fused<TSB_POT_LJ, false>(A, grid, st);
-  } else if (potential == TSB_POT_MORSE) {
-    multi ? launch_fused<TSB_POT_MORSE, true>(A, grid, st)
-          : launch_fused<TSB_POT_MORSE, false>(A, grid, st);
-  } else {
-    multi ? launch_fused<TSB_POT_SOFT, true>(A, grid, st)
-          : launch_fused<TSB_POT_SOFT, false>(A, grid, st);
-  }
+  launch_all(A, -1, queue, st);
   if (counter_dev) k_advance_counter<<<1, 32, 0, st>>>(counter_dev, n_steps);
   TSB_CHECK_LAUNCH();
   return TSB_OK;
@@ -1240,12 +1309,6 @@ extern "C" int tsb_fused_md_nvt(int thermostat, int potential, const double *tab
   int32_t *queue = c.take<int32_t>(4);
   if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
-  int dev = 0, n_sm = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-  int64_t grid = n_sm;
-  if (grid > kMaxGrid) grid = kMaxGrid;
-  if (grid > n_systems) grid = n_systems;
   cudaMemsetAsync(lo, 0, sizeof(int64_t) * n_systems, st);
   cudaMemsetAsync(hi, 0, sizeof(int64_t) * n_systems, st);
   cudaMemsetAsync(queue, 0, sizeof(int32_t) * 4, st);
@@ -1258,16 +1321,7 @@ extern "C" int tsb_fused_md_nvt(int thermostat, int potential, const double *tab
               status, chain_xi, chain_pxi, chain_Q, chain_ke, tau_sys, chain_dt,
               chain_length, chain_steps, sy_steps};
   A.stress = stress;
-  const bool multi = n_species > 1;
-  if (potential == TSB_POT_LJ) {
-    multi ? launch_fused<TSB_POT_LJ, true>(A, grid, st) : launch_fused<TSB_POT_LJ, false>(A, grid, st);
-  } else if (potential == TSB_POT_MORSE) {
-    multi ? launch_fused<TSB_POT_MORSE, true>(A, grid, st)
-          : launch_fused<TSB_POT_MORSE, false>(A, grid, st);
-  } else {
-    multi ? launch_fused<TSB_POT_SOFT, true>(A, grid, st)
-          : launch_fused<TSB_POT_SOFT, false>(A, grid, st);
-  }
+  launch_all(A, -1, queue, st);
   if (counter_dev) k_advance_counter<<<1, 32, 0, st>>>(counter_dev, n_steps);
   TSB_CHECK_LAUNCH();
   return TSB_OK;
@@ -1286,7 +1340,8 @@ extern "C" int tsb_fused_md_ex(int integrator, int potential, const double *tabl
                                int chain_steps, int sy_steps, uint64_t seed, uint64_t counter,
                                uint64_t *counter_dev, float *frame_x, double *frame_e,
                                int64_t report_every, int64_t n_frames, int lanes_max,
-                               double *energy, double *stress, int32_t *n_rebuilds,
+                               int64_t n_wide, double *energy, double *stress,
+                               int32_t *n_rebuilds,
                                int32_t *status, void *workspace, size_t workspace_bytes,
                                void *stream) {
   if (integrator < TSB_INT_NVE || integrator > TSB_INT_VRESCALE) return TSB_ERR_INVALID_ARG;
@@ -1308,6 +1363,7 @@ extern "C" int tsb_fused_md_ex(int integrator, int potential, const double *tabl
   }
   if (report_every < 0 || n_frames < 0) return TSB_ERR_INVALID_ARG;
   if (lanes_max < 0 || lanes_max > 32 || (lanes_max & (lanes_max - 1))) return TSB_ERR_INVALID_ARG;
+  if (n_wide >= 0 && !order) return TSB_ERR_INVALID_ARG;
   if (report_every > 0 && n_frames > 0 && (!frame_x || !frame_e)) return TSB_ERR_INVALID_ARG;
   Carver c(workspace, workspace_bytes);
   int64_t *lo = c.take<int64_t>(n_systems);
@@ -1315,12 +1371,6 @@ extern "C" int tsb_fused_md_ex(int integrator, int potential, const double *tabl
   int32_t *queue = c.take<int32_t>(4);
   if (!c.ok || !workspace) return TSB_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
-  int dev = 0, n_sm = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-  int64_t grid = n_sm;
-  if (grid > kMaxGrid) grid = kMaxGrid;
-  if (grid > n_systems) grid = n_systems;
   cudaMemsetAsync(lo, 0, sizeof(int64_t) * n_systems, st);
   cudaMemsetAsync(hi, 0, sizeof(int64_t) * n_systems, st);
   cudaMemsetAsync(queue, 0, sizeof(int32_t) * 4, st);
@@ -1335,16 +1385,7 @@ extern "C" int tsb_fused_md_ex(int integrator, int potential, const double *tabl
               report_every > 0 && n_frames > 0 ? report_every : 0, n_frames, n_atoms};
   A.stress = stress;
   A.lanes_max = lanes_max;
-  const bool multi = n_species > 1;
-  if (potential == TSB_POT_LJ) {
-    multi ? launch_fused<TSB_POT_LJ, true>(A, grid, st) : launch_fused<TSB_POT_LJ, false>(A, grid, st);
-  } else if (potential == TSB_POT_MORSE) {
-    multi ? launch_fused<TSB_POT_MORSE, true>(A, grid, st)
-          : launch_fused<TSB_POT_MORSE, false>(A, grid, st);
-  } else {
-    multi ? launch_fused<TSB_POT_SOFT, true>(A, grid, st)
-          : launch_fused<TSB_POT_SOFT, false>(A, grid, st);
-  }
+  launch_all(A, n_wide, queue, st);
   if (counter_dev) k_advance_counter<<<1, 32, 0, st>>>(counter_dev, n_steps);
   TSB_CHECK_LAUNCH();
   return TSB_OK;
@@ -1426,12 +1467,6 @@ extern "C" int tsb_fused_md_static(int integrator, int potential, const double *
   int64_t *lo = (int64_t *)base;
   int64_t *hi = lo + kStaticMaxSystems;
   int32_t *queue = (int32_t *)(hi + kStaticMaxSystems);
-  int dev = 0, n_sm = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-  int64_t grid = n_sm;
-  if (grid > kMaxGrid) grid = kMaxGrid;
-  if (grid > n_systems) grid = n_systems;
   // the array keeps the previous call's contents: clear what must start at zero
   cudaMemsetAsync(lo, 0, sizeof(int64_t) * n_systems, st);
   cudaMemsetAsync(hi, 0, sizeof(int64_t) * n_systems, st);
@@ -1442,16 +1477,7 @@ extern "C" int tsb_fused_md_static(int integrator, int potential, const double *
   FusedArgs A{integrator, potential, n_species, table, species, positions, momenta, forces,
               masses, cell_row, lo, hi, n_systems, order, cutoff, skin, n_steps, dt_sys,
               kT_sys, gamma_sys, seed, counter, nullptr, energy, n_rebuilds, queue, status};
-  const bool multi = n_species > 1;
-  if (potential == TSB_POT_LJ) {
-    multi ? launch_fused<TSB_POT_LJ, true>(A, grid, st) : launch_fused<TSB_POT_LJ, false>(A, grid, st);
-  } else if (potential == TSB_POT_MORSE) {
-    multi ? launch_fused<TSB_POT_MORSE, true>(A, grid, st)
-          : launch_fused<TSB_POT_MORSE, false>(A, grid, st);
-  } else {
-    multi ? launch_fused<TSB_POT_SOFT, true>(A, grid, st)
-          : launch_fused<TSB_POT_SOFT, false>(A, grid, st);
-  }
+  launch_all(A, -1, queue, st);
   TSB_CHECK_LAUNCH();
   return TSB_OK;
 }

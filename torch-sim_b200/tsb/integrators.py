@@ -839,6 +839,27 @@ def _system_order(state):
     return order, max_atoms
 
 
+NARROW_MAX_ATOMS = 256      # systems the 256-thread blocks of the fused kernel take
+NARROW_MAX_IMAGES = 1968    # their table of atoms + periodic images
+
+
+def _split_order(state, cutoff: float, skin: float):
+    """(order, n_wide): systems for 512-thread blocks first, then those for the
+    256-thread blocks (two per SM), each group largest first.  A system goes to
+    the narrow blocks when it has at most 256 atoms and its atoms and images
+    within cutoff + skin of the cell -- about n prod_k (1 + 2 R / d_k), d_k the
+    cell's plane spacings -- fit 85 % of their table."""
+    counts = torch.bincount(state.system_idx, minlength=state.n_systems).to(torch.float64)
+    cell_row = state.cell.mT.to(torch.float64)
+    recip = torch.linalg.inv(cell_row).mT          # rows: reciprocal vectors, |b_k| = 1/d_k
+    h = (cutoff + skin) * recip.norm(dim=-1)       # [S, 3] image margins, fractional
+    images = counts * torch.prod(1.0 + 2.0 * h, dim=-1)
+    narrow = (counts <= NARROW_MAX_ATOMS) & (images <= 0.85 * NARROW_MAX_IMAGES)
+    key = torch.where(narrow, counts, counts + 1e6)  # wide ones sort first
+    order = torch.argsort(key, descending=True, stable=True).to(torch.int32).contiguous()
+    return order, int((~narrow).sum())
+
+
 class FusedMD:
     """Preallocated persistent fused-MD runner (no host synchronisation per launch).
 
@@ -851,7 +872,7 @@ class FusedMD:
 
     def __init__(self, state, model, *, integrator: str = "nvt_langevin", dt, kT=None,
                  gamma=None, skin: float | str = 0.7, seed: int | None = None, tau=None,
-                 lanes: int | str | None = None):
+                 lanes: int | str | None = None, shapes: str = "auto"):
         from .models.pair_potential import PairTableModel
 
         if not isinstance(model, PairTableModel):
@@ -933,6 +954,15 @@ class FusedMD:
                                           dt=dt, kT=kT, gamma=gamma)
         if self.lanes not in (1, 2, 4, 8, 16, 32):
             raise ValueError(f"lanes must be a power of two in 1..32, got {self.lanes!r}")
+        # block shapes: "auto" puts small systems in 256-thread blocks (two per
+        # SM) and the rest in 512-thread blocks; "wide" runs all in 512-thread blocks
+        if shapes not in ("auto", "wide"):
+            raise ValueError(f"shapes must be 'auto' or 'wide', got {shapes!r}")
+        self.shapes = shapes
+        if shapes == "auto":
+            self.order, self.n_wide = _split_order(state, model.cutoff, self.skin)
+        else:
+            self.n_wide = -1
         self.seed = (seed if seed is not None
                      else getattr(state, "_philox_seed", _seed_of(state))) & (2**64 - 1)
         # Philox counter lives on the device so that graph replays advance it
@@ -962,7 +992,8 @@ class FusedMD:
             self.dt_s, self.kT_s, self.g_s, getattr(self, "tau_s", None), g("cxi"), g("cpxi"),
             g("cQ"), g("cke"), g("cdt"), self.M if nh else 0, self.nc if nh else 0,
             self.nsy if nh else 0, _i64(self.seed), 0, self.counter_dev, fx, fe, int(every),
-            self.lanes, self.energy, self.stress, self.rebuilds, self.status, self.ws)
+            self.lanes, self.n_wide, self.energy, self.stress, self.rebuilds, self.status,
+            self.ws)
 
     def graph(self, n_steps: int) -> "torch.cuda.CUDAGraph":
         """CUDA graph of one ``launch(n_steps)``; ``g.replay()`` advances every system
