@@ -245,3 +245,33 @@ def test_reference_shaped_state_through_a_step_function():
         md = integrators.nve_step(md, m, dt=0.001 * workloads.METAL_TIME)
     assert md.positions.shape == st.positions.shape
     assert torch.isfinite(md.energy).all() and not torch.equal(md.energy, e0)
+
+
+@pytest.mark.parametrize("name", ["nve", "nvt_langevin"])
+def test_steps_driven_like_the_reference_runner(name):
+    """ts.integrate with an (init, step) tuple (torch_sim/runners.py:308-396)
+    converts the timestep (ps) and temperature (K) to internal units as 0-d
+    tensors on the state's device, then calls init_func(state=, model=, kT=, dt=)
+    and step_func(state=, model=, dt=, kT=) by keyword.  The tsb pairs take
+    exactly that and give the same trajectory as calls with plain floats."""
+    from tsb import integrators, workloads
+
+    init, step = {"nve": (integrators.nve_init, integrators.nve_step),
+                  "nvt_langevin": (integrators.nvt_langevin_init,
+                                   integrators.nvt_langevin_step)}[name]
+    md0, m = _cu_md(3, seed=8)
+    st = md0.clone()
+    dev, dt_ = st.device, st.dtype
+    timestep, temperature = 0.002, 800.0                 # ps, K (the runner's inputs)
+    kTs = torch.as_tensor(temperature, dtype=dt_, device=dev).expand(4) * workloads.KB_EV
+    dt = torch.as_tensor(timestep * workloads.METAL_TIME, dtype=dt_, device=dev)
+    a = init(state=st, model=m, kT=kTs[0], dt=dt)
+    a._philox_seed, a._philox_counter = 5, 0
+    for k in range(4):
+        a = step(state=a, model=m, dt=dt, kT=kTs[k])
+    b = init(md0.clone(), m, kT=temperature * workloads.KB_EV)
+    b._philox_seed, b._philox_counter = 5, 0
+    for _ in range(4):
+        b = step(b, m, dt=float(dt), kT=temperature * workloads.KB_EV)
+    torch.testing.assert_close(a.positions, b.positions, rtol=0, atol=0)
+    torch.testing.assert_close(a.momenta, b.momenta, rtol=0, atol=0)

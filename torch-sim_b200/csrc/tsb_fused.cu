@@ -440,6 +440,9 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
   constexpr size_t kSmemExt = FusedSmem<NT>::kExt;
   constexpr size_t kSmemGhost = FusedSmem<NT>::kGhost;
   constexpr size_t kSmemSorted = FusedSmem<NT>::kSorted;
+  // the last image slot holds a point far from everything: list padding entries
+  // point at it and contribute nothing (outside every cutoff and FP64 band)
+  constexpr int kSentinel = kExtMax - 1;
   // single-species LJ / Morse: pairs evaluated two at a time in FP32x2
   constexpr bool kPaired = !MULTI && POT != TSB_POT_SOFT;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -471,6 +474,7 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
   const double rc2d0 = rc2d[0];
   const uint64_t counter0 = A.counter + (A.counter_dev ? *A.counter_dev : 0ull);
 
+  if (tid == 0) s_ext[kSentinel] = make_float4(1e18f, 1e18f, 1e18f, __int_as_float(0));
   for (;;) {
     __syncthreads();
     if (tid == 0) s_work = atomicAdd(A.queue, 1);
@@ -640,7 +644,7 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
     gbeg = __shfl_sync(0xffffffffu, n + goff, (threadIdx.x & 31) & ~(tpa - 1));              \
     gcnt = __shfl_sync(0xffffffffu, gcount, (threadIdx.x & 31) & ~(tpa - 1));                \
     const int n_ext = n + total;                                                             \
-    if (n_ext > kExtMax) {                                                                   \
+    if (n_ext > kSentinel) { /* the last slot is the sentinel */                             \
       over = 1;                                                                              \
       over_size = n_ext;                                                                     \
     } else {                                                                                 \
@@ -737,6 +741,25 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
               TSB_FILE_PAIR(e0, q0)                                                          \
             }                                                                                \
           }                                                                                  \
+        }                                                                                    \
+      }                                                                                      \
+      if (own && ncore + nshell <= kListLen) {                                               \
+        /* whole groups of four: the last ncore % 4 core pairs join the shell (they  */      \
+        /* pass its cutoff test anyway), and the shell is padded to a multiple of 4 */       \
+        /* with the far sentinel entry, so no lane has a partial group to handle    */       \
+        const int extra_ = ncore & 3;                                                        \
+        for (int k_ = 0; k_ < extra_; ++k_) {                                                \
+          const int from_ = ncore - 1 - k_, to_ = kListLen - 1 - nshell;                     \
+          list16[(((to_ >> 2) * kFusedThreads + tid) << 2) | (to_ & 3)] =                    \
+              list16[(((from_ >> 2) * kFusedThreads + tid) << 2) | (from_ & 3)];             \
+          ++nshell;                                                                          \
+        }                                                                                    \
+        ncore -= extra_;                                                                     \
+        while (nshell & 3) {                                                                 \
+          const int to_ = kListLen - 1 - nshell;                                             \
+          list16[(((to_ >> 2) * kFusedThreads + tid) << 2) | (to_ & 3)] =                    \
+              (uint16_t)(kSentinel << 4);                                                    \
+          ++nshell;                                                                          \
         }                                                                                    \
       }                                                                                      \
       if (__syncthreads_or(ncore + nshell > kListLen)) {                                     \
@@ -1201,10 +1224,28 @@ static void launch_shape(const FusedArgs &A, int64_t grid, cudaStream_t st) {
   }
 }
 
+// A second stream per device for the narrow launch, created on first use.
+constexpr int kSideDevices = 64;
+static cudaStream_t g_side_stream[kSideDevices];
+static std::mutex g_side_mu;
+
+static cudaStream_t side_stream() {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kSideDevices) return nullptr;
+  std::lock_guard<std::mutex> lock(g_side_mu);
+  if (!g_side_stream[dev] &&
+      cudaStreamCreateWithFlags(&g_side_stream[dev], cudaStreamNonBlocking) != cudaSuccess)
+    g_side_stream[dev] = nullptr;
+  return g_side_stream[dev];
+}
+
 // One persistent launch over all systems (wide blocks), or, with an order whose
 // first n_wide systems need wide blocks, a wide launch over those and a narrow
-// launch (two blocks per SM) over the rest, one after the other on the stream.
-// queue[0] and queue[1] are the two launches' work counters (zeroed before).
+// launch (two blocks per SM) over the rest.  The narrow launch goes on a side
+// stream forked from `st` after the wide one, so its blocks take the SMs the
+// wide blocks leave at the end of their work (the two launches' tails overlap),
+// and `st` waits for it before anything after this call.  queue[0] and
+// queue[1] are the two launches' work counters (zeroed before).
 static void launch_all(FusedArgs A, int64_t n_wide, int32_t *queue, cudaStream_t st) {
   int dev = 0, n_sm = 148;
   cudaGetDevice(&dev);
@@ -1216,18 +1257,33 @@ static void launch_all(FusedArgs A, int64_t n_wide, int32_t *queue, cudaStream_t
     launch_shape<512>(A, std::min<int64_t>(std::min<int64_t>(n_sm, kMaxGrid), n), st);
     return;
   }
+  FusedArgs Nw = A;
+  Nw.order = A.order + n_wide;
+  Nw.n_work = n - n_wide;
+  Nw.queue = queue + 1;
+  const int64_t grid_n = std::min<int64_t>(std::min<int64_t>(2 * n_sm, 2 * kMaxGrid), n - n_wide);
+  cudaStream_t side = n_wide > 0 ? side_stream() : nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  if (side && (cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) != cudaSuccess ||
+               cudaEventCreateWithFlags(&join, cudaEventDisableTiming) != cudaSuccess))
+    side = nullptr;
+  if (side) cudaEventRecord(fork, st);
   if (n_wide > 0) {
     FusedArgs W = A;
     W.n_work = n_wide;
     W.queue = queue;
     launch_shape<512>(W, std::min<int64_t>(std::min<int64_t>(n_sm, kMaxGrid), n_wide), st);
   }
-  FusedArgs Nw = A;
-  Nw.order = A.order + n_wide;
-  Nw.n_work = n - n_wide;
-  Nw.queue = queue + 1;
-  launch_shape<256>(Nw, std::min<int64_t>(std::min<int64_t>(2 * n_sm, 2 * kMaxGrid), n - n_wide),
-                    st);
+  if (side) {
+    cudaStreamWaitEvent(side, fork, 0);
+    launch_shape<256>(Nw, grid_n, side);
+    cudaEventRecord(join, side);
+    cudaStreamWaitEvent(st, join, 0);
+  } else {
+    launch_shape<256>(Nw, grid_n, st);
+  }
+  if (fork) cudaEventDestroy(fork);
+  if (join) cudaEventDestroy(join);
 }
 
 extern "C" int tsb_fused_md(int integrator, int potential, const double *table,

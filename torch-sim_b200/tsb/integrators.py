@@ -67,11 +67,13 @@ def initialize_momenta(positions, masses, system_idx, kT, generator=None):
     n_sys = int(system_idx[-1]) + 1
     counts = torch.bincount(system_idx, minlength=n_sys)
     # per-system sums from an FP64 prefix sum over the contiguous systems: a fixed
-    # summation order (index_add_ on the GPU sums in a run-dependent order)
-    cs = torch.cat([torch.zeros((1, 3), dtype=torch.float64, device=p.device),
-                    p.to(torch.float64).cumsum(0)])
+    # summation order (index_add_ on the GPU sums in a run-dependent order); the
+    # scan runs along the contiguous dimension of p^T (a scan down the 3 columns
+    # of p would be three long serial scans)
+    cs = torch.cat([torch.zeros((3, 1), dtype=torch.float64, device=p.device),
+                    p.to(torch.float64).T.contiguous().cumsum(1)], dim=1)
     ends = counts.cumsum(0)
-    mean = ((cs[ends] - cs[ends - counts]) / counts.view(-1, 1)).to(p.dtype)
+    mean = ((cs[:, ends] - cs[:, ends - counts]) / counts.view(1, -1)).T.to(p.dtype)
     return torch.where((counts > 1)[system_idx].view(-1, 1), p - mean[system_idx], p)
 
 
