@@ -60,10 +60,10 @@ def sm_peaks(device):
 
 
 def pair_counts(x, cell_row, system_idx, cutoff, skin, n_systems):
-    """(half-list pairs within the cutoff, list entries within cutoff + skin, both
-    per atom) of one configuration, from the neighbour-list drop-in: the
-    algorithmic pairs of a step and the pair evaluations of a fused step (every
-    atom evaluates its full list at cutoff + skin)."""
+    """(half-list pairs within the cutoff, full-list entries within cutoff + skin,
+    both per atom) of one configuration, from the neighbour-list drop-in: the
+    algorithmic pairs of a step and the size of the lists the fused kernel
+    evaluates every step at that skin."""
     import torch
 
     from tsb import neighbors
@@ -606,7 +606,10 @@ def main():
                          "peak_source": "nominal: SMs x 128 FP32 lanes x 2 x max SM clock "
                                         "(no measured FP32 peak)",
                          "half_pairs_per_atom_step": half_pairs,
-                         "pair_evaluations_per_atom_step": evals,
+                         # full-list entries within cutoff + skin (each atom evaluates
+                         # its own list every step; systems whose shared-memory tables
+                         # overflow at this skin run at a halved one, with fewer)
+                         "list_entries_per_atom_at_skin": evals,
                          "flops_per_half_pair": FLOPS_PER_PAIR,
                          "exp_per_s": rate * half_pairs,
                          "sfu_peak_per_s": sfu_peak * 1e9,
