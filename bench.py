@@ -88,6 +88,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skin", default="auto",
                     help="Verlet skin in A, or 'auto' (project autotuner, cached per workload)")
+    ap.add_argument("--prune", default=None,
+                    help="pruning skin of the list's shell in A (0: off), or 'auto'; default: "
+                         "'auto' with --skin auto, else a fixed fraction of the skin")
     ap.add_argument("--plain-steps", type=int, default=20,
                     help="MD steps of the plain per-call path timed beside the fused kernel")
     ap.add_argument("--integrator", default="nvt_langevin",
@@ -461,7 +464,10 @@ def main():
                                  gamma=10.0 / W.METAL_TIME if args.integrator == "nvt_langevin"
                                  else None,
                                  skin=args.skin if args.skin == "auto" else float(args.skin),
-                                 seed=1234 + rank)
+                                 seed=1234 + rank,
+                                 prune=(None if args.prune is None else
+                                        args.prune if args.prune == "auto" else
+                                        float(args.prune)))
     stream = torch.cuda.current_stream(device)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
 
@@ -569,9 +575,14 @@ def main():
     plain_value = replicas.weak_scaling_value(n_atoms * args.plain_steps, t_plain, ws)
 
     # pair counts of the final configuration: algorithmic half pairs within the
-    # cutoff, and the list entries each atom evaluates per fused step
+    # cutoff, the list entries each atom holds, and those it evaluates per fused
+    # step (within cutoff + pruning skin, when the shell is pruned)
     half_pairs, evals = pair_counts(runner.x, runner.cell_row, md.system_idx, model.cutoff,
                                     runner.skin, md.n_systems)
+    evaluated = evals
+    if 0.0 < runner.prune < runner.skin:
+        evaluated = pair_counts(runner.x, runner.cell_row, md.system_idx, model.cutoff,
+                                runner.prune, md.n_systems)[1]
 
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
@@ -591,7 +602,8 @@ def main():
                        WORKLOAD.replace("NVT-Langevin BAOAB", INTEGRATOR_NAMES[args.integrator]),
                        "n_systems": args.n_systems,
                        "atoms_per_gpu": n_atoms, "md_steps_per_step": args.md_steps,
-                       "verlet_skin_A": runner.skin, "lanes_per_atom_max": runner.lanes,
+                       "verlet_skin_A": runner.skin, "prune_skin_A": runner.prune,
+                       "lanes_per_atom_max": runner.lanes,
                        "skin_source": "autotuner" if args.skin == "auto" else "argument",
                        "precision": "FP32 pair math, FP64 state",
                        "mean_steps_between_list_rebuilds": rebuild_interval,
@@ -606,10 +618,12 @@ def main():
                          "peak_source": "nominal: SMs x 128 FP32 lanes x 2 x max SM clock "
                                         "(no measured FP32 peak)",
                          "half_pairs_per_atom_step": half_pairs,
-                         # full-list entries within cutoff + skin (each atom evaluates
-                         # its own list every step; systems whose shared-memory tables
-                         # overflow at this skin run at a halved one, with fewer)
+                         # full-list entries within cutoff + skin (each atom holds its
+                         # own list; systems whose shared-memory tables overflow at this
+                         # skin run at a halved one, with fewer), and the entries it
+                         # evaluates per step: those within cutoff + pruning skin
                          "list_entries_per_atom_at_skin": evals,
+                         "list_entries_per_atom_evaluated": evaluated,
                          "flops_per_half_pair": FLOPS_PER_PAIR,
                          "exp_per_s": rate * half_pairs,
                          "sfu_peak_per_s": sfu_peak * 1e9,
@@ -628,7 +642,8 @@ def main():
                                    "step (cell list + FP32 pair forces + integrator kernels "
                                    "each call)",
                            "fused_over_plain": value / plain_value},
-            "gpu_launches": 3 * args.steps,  # k_bounds_fused, k_fused_md, k_advance_counter
+            # k_bounds_fused, k_fused_md (one launch per block shape), k_advance_counter
+            "gpu_launches": (3 + (0 < runner.n_wide < md.n_systems)) * args.steps,
             "clocks": clocks.summary(),
             "per_launch_ms": per_launch_ms,
         }

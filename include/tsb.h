@@ -557,7 +557,11 @@ int tsb_fused_md_nvt(int thermostat, int potential, const double *table, int n_s
  * systems must have at most 256 atoms and fit the narrow blocks' image table of
  * 1968 entries at the given skin (else the skin is halved for them, or
  * TSB_ERR_CAPACITY is reported); n_wide < 0 runs every system in 512-thread
- * blocks. */
+ * blocks.  prune_skin (0 <= prune_skin; 0 or >= skin: off) prunes the list
+ * between builds: only the pairs of the list's shell that lie within
+ * cutoff + prune_skin are evaluated, and the shell is pruned again whenever an
+ * atom moved more than prune_skin / 2 since the last pruning.  Results do not
+ * depend on it beyond FP32 summation order. */
 int tsb_fused_md_ex(int integrator, int potential, const double *table, int n_species,
                     const int32_t *species, double *positions, double *momenta,
                     double *forces, const double *masses, const double *cell_row,
@@ -569,8 +573,8 @@ int tsb_fused_md_ex(int integrator, int potential, const double *table, int n_sp
                     int chain_length, int chain_steps, int sy_steps, uint64_t seed,
                     uint64_t counter, uint64_t *counter_dev, float *frame_x, double *frame_e,
                     int64_t report_every, int64_t n_frames, int lanes_max, int64_t n_wide,
-                    double *energy, double *stress, int32_t *n_rebuilds, int32_t *status,
-                    void *workspace, size_t workspace_bytes, void *stream);
+                    double prune_skin, double *energy, double *stress, int32_t *n_rebuilds,
+                    int32_t *status, void *workspace, size_t workspace_bytes, void *stream);
 
 /* ---- allocation-free fused MD -------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device

@@ -88,6 +88,8 @@ struct FusedSmem {
   static_assert(S::kMaxBins <= 4 * NT, "bin scan: four bins per thread");
   static_assert((S::kExtMax - 1) * sizeof(float4) <= 0xFFFF,
                 "list entries are 16-bit byte offsets");
+  static_assert(kBins >= (size_t)NT * sizeof(float4), "atom positions alias the bin table");
+  static_assert((kList + kExt + kGhost + kSorted) % 16 == 0, "bin table 16-byte aligned");
 };
 
 struct FusedArgs {
@@ -126,6 +128,10 @@ struct FusedArgs {
   int lanes_max;
   // systems this launch takes from `order` (order[0 .. n_work)); 0: all n_sys
   int64_t n_work;
+  // dynamic pruning of the list's shell (0: off): between list builds only the
+  // shell pairs within cutoff + prune are evaluated, and the shell is pruned
+  // again whenever an atom moved more than prune / 2 since the last pruning
+  double prune;
 };
 
 // per-system geometry, computed by thread 0 into shared memory
@@ -139,6 +145,9 @@ struct FusedGeom {
   double iw[3];   // 1 / bin width, fractional
   double skin;    // this system's current Verlet skin
   double half_skin2;    // (skin / 2)^2: rebuild when an atom moved further
+  double half_prune2;   // (prune / 2)^2: prune the shell again when an atom moved further
+  float act2;     // FP32 r^2 below which a shell pair stays in the pruned shell
+  int prune_on;   // 0 < prune < skin
   double dt, half, c1;  // time step, dt / 2, Langevin exp(-gamma dt)
   // thermostat scalars of this system (thread 0), and the momentum factor it
   // hands to all threads
@@ -173,7 +182,8 @@ struct FusedGeom {
 // Bins: width >= R |T_k| / 2 in fractional coordinate k, so two points closer
 // than R differ by at most 2 bins per axis; coarsened until <= kMaxBins.
 template <int kMaxBins>
-__device__ inline bool set_margins(FusedGeom &g, double cutoff, const double *rc2d, int nsp2) {
+__device__ inline bool set_margins(FusedGeom &g, double cutoff, double prune, const double *rc2d,
+                                   int nsp2) {
   bool ok = true;
   const double R = cutoff + g.skin;
   g.half_skin2 = 0.25 * g.skin * g.skin;
@@ -201,6 +211,19 @@ __device__ inline bool set_margins(FusedGeom &g, double cutoff, const double *rc
                    (4.0 * 1.7320508075688772 * 6.0 * ypmax * cutoff + 6.0 * cutoff * cutoff));
   const double margin = 1e-6 * (4.0 * ymax + R);
   g.build2 = (float)((R + margin) * (R + margin));
+  // Pruned shell: a pair whose FP32 distance at the pruning is at least
+  // cutoff + prune + pm, pm = 1e-6 (8 Y' + R), is left out until the next
+  // pruning.  Until then no atom moves more than prune / 2 from its position at
+  // the pruning (tested in FP64 against that position rounded to FP32), so the
+  // exact distance stays above the cutoff: pm covers the FP32 distance error
+  // (image coordinates off by <= 6 2^-24 Y', the atom by 2^-24 Y <= 2^-24 Y',
+  // so |d| is off by <= 7 sqrt3 2^-24 Y' plus ~2^-23 R from the arithmetic) and
+  // the FP32 rounding of both reference positions (2 sqrt3 2^-24 Y').
+  const double pr = (prune > 0.0 && prune < g.skin) ? prune : 0.0;
+  g.prune_on = pr > 0.0;
+  g.half_prune2 = pr > 0.0 ? 0.25 * pr * pr : INFINITY;
+  const double pm = 1e-6 * (8.0 * ypmax + R);
+  g.act2 = (float)((cutoff + pr + pm) * (cutoff + pr + pm));
   for (int k = 0; k < nsp2; ++k) {
     const double cr = sqrt(rc2d[k]) - g.skin - margin;
     g.core2[k] = cr > 0.0 ? (float)(cr * cr) : -1.0f;
@@ -453,6 +476,9 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
   int *s_bin = (int *)(smem + kSmemList + kSmemExt + kSmemGhost + kSmemSorted);
   uint16_t *list16 = (uint16_t *)s_list;
   uint16_t *s_ebin = (uint16_t *)s_list;  // bin of each entry, during a rebuild only
+  // the atoms' new FP32 positions, from the integrator phase of a step to the
+  // image refresh of the same step (the bin table is free then)
+  float4 *s_pos = (float4 *)s_bin;
   __shared__ FusedGeom g;
   __shared__ PairPrm<float> prm[kFusedMaxSpecies * kFusedMaxSpecies];
   __shared__ double rc2d[kFusedMaxSpecies * kFusedMaxSpecies];
@@ -526,7 +552,8 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
           }
         }
       }
-      const bool rep_ok = isfinite(d) && d != 0.0 && set_margins<kMaxBins>(g, A.cutoff, rc2d, nsp2);
+      const bool rep_ok =
+          isfinite(d) && d != 0.0 && set_margins<kMaxBins>(g, A.cutoff, A.prune, rc2d, nsp2);
       int tpa = 1;
       const int lmax = A.lanes_max > 0 ? min(A.lanes_max, 32) : 32;
       while (tpa * 2 <= lmax && g.n * tpa * 2 <= kFusedThreads) tpa *= 2;
@@ -572,10 +599,12 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
         c2m = sqrt(A.kT[s] * (1.0 - exp(-2.0 * (A.gamma[s] * A.dt[s])))) * sqrt(mass);
     }
     int Wx = 0, Wy = 0, Wz = 0;        // integer wrap of the owned atom at the last build
-    int gbeg = 0, gcnt = 0;            // the owned atom's ghost slots [gbeg, gbeg + gcnt)
     int ncore = 0, nshell = 0, rebuilds = 0;
+    int nact = 0;                      // shell entries kept by the last pruning
+    int n_ext = 0;                     // atoms + images in the table
     bool failed = false;
     float yb0 = 0.f, yb1 = 0.f, yb2 = 0.f;  // wrapped position at the build (FP32)
+    float zp0 = 0.f, zp1 = 0.f, zp2 = 0.f;  // wrapped position at the last pruning (FP32)
 
     // ------------------------------------------------------------- rebuild
     // Wrap the owned atom and create its periodic images inside the
@@ -640,10 +669,7 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
     }                                                                                        \
     int total;                                                                               \
     const int goff = block_excl_scan_i<NT>(gcount, &total, s_scan);                              \
-    /* broadcast the lead's ghost range to the other lanes of its atom */                    \
-    gbeg = __shfl_sync(0xffffffffu, n + goff, (threadIdx.x & 31) & ~(tpa - 1));              \
-    gcnt = __shfl_sync(0xffffffffu, gcount, (threadIdx.x & 31) & ~(tpa - 1));                \
-    const int n_ext = n + total;                                                             \
+    n_ext = n + total;                                                                       \
     if (n_ext > kSentinel) { /* the last slot is the sentinel */                             \
       over = 1;                                                                              \
       over_size = n_ext;                                                                     \
@@ -659,7 +685,7 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
         s_ebin[a] = (uint16_t)((bin_coord(g, f0, 0) * g.nb[1] + bin_coord(g, f1, 1)) *       \
                                    g.nb[2] +                                                 \
                                bin_coord(g, f2, 2));                                         \
-        int gg = gbeg;                                                                       \
+        int gg = n + goff; /* the lead's ghost slots */                                      \
         for (int sx = -g.rep[0]; gcount && sx <= g.rep[0]; ++sx) {                           \
           if (!in_margin(g, f0 + sx, 0)) continue;                                           \
           const int bx = bin_coord(g, f0 + sx, 0);                                           \
@@ -780,9 +806,46 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
     }                                                                                        \
     if (tid == 0) {                                                                          \
       g.skin = g.skin > 0.05 ? 0.5 * g.skin : 0.0;                                           \
-      set_margins<kMaxBins>(g, A.cutoff, rc2d, nsp2);                                                  \
+      set_margins<kMaxBins>(g, A.cutoff, A.prune, rc2d, nsp2);                                                  \
     }                                                                                        \
     __syncthreads();                                                                         \
+  }
+
+    // ------------------------------------------------------------ pruning
+    // Each thread reorders its own shell entries (no other thread reads them):
+    // those closer than sqrt(act2) now go first (in their previous order) and
+    // are the only shell entries the force loop evaluates until the next
+    // pruning; (P0, P1, P2) is the atom's FP32 position the next pruning test
+    // measures from.  Without pruning, the whole shell is evaluated.
+#define TSB_PRUNE(P0, P1, P2)                                                                \
+  if (g.prune_on) {                                                                          \
+    if (own) {                                                                               \
+      const float4 xi_ = s_ext[a];                                                           \
+      const float act2_ = g.act2;                                                            \
+      int w_ = 0;                                                                            \
+      for (int k_ = 0; k_ < nshell; ++k_) {                                                  \
+        const int sk_ = kListLen - 1 - k_;                                                   \
+        const int ik_ = (((sk_ >> 2) * kFusedThreads + tid) << 2) | (sk_ & 3);               \
+        const uint16_t e_ = list16[ik_];                                                     \
+        const float4 q_ = EXT(e_);                                                           \
+        const float dx_ = q_.x - xi_.x, dy_ = q_.y - xi_.y, dz_ = q_.z - xi_.z;              \
+        if (dx_ * dx_ + dy_ * dy_ + dz_ * dz_ < act2_) {                                     \
+          if (w_ != k_) {                                                                    \
+            const int sw_ = kListLen - 1 - w_;                                               \
+            const int iw_ = (((sw_ >> 2) * kFusedThreads + tid) << 2) | (sw_ & 3);           \
+            list16[ik_] = list16[iw_];                                                       \
+            list16[iw_] = e_;                                                                \
+          }                                                                                  \
+          ++w_;                                                                              \
+        }                                                                                    \
+      }                                                                                      \
+      nact = w_;                                                                             \
+    }                                                                                        \
+    zp0 = (P0);                                                                              \
+    zp1 = (P1);                                                                              \
+    zp2 = (P2);                                                                              \
+  } else {                                                                                   \
+    nact = nshell;                                                                           \
   }
 
     // ------------------------------------------------------------ pair loop
@@ -879,7 +942,9 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
       const PairPrm<float> *row = prm + sp * A.n_species;                                    \
       (void)row;                                                                             \
       const int full = ncore >> 2, rem = ncore & 3;                                          \
-      const int sfull = nshell >> 2, srem = nshell & 3;                                      \
+      /* the pruned shell in whole groups of four (a group's tail entries beyond */           \
+      /* nact are shell entries outside the cutoff, or the far sentinel)         */           \
+      const int sfull = (nact + 3) >> 2, srem = 0;                                           \
       if constexpr (kPaired) {                                                               \
         float2 f2x = make_float2(0.f, 0.f), f2y = f2x, f2z = f2x;                            \
         /* the next group's list word loads one iteration ahead (in-bounds index) */         \
@@ -987,6 +1052,7 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
 
     TSB_REBUILD()
     if (failed) continue;
+    TSB_PRUNE(yb0, yb1, yb2)
     for (int64_t step = 0; step < A.n_steps; ++step) {
       const double dt = g.dt, half = g.half, c1 = g.c1;
       // thermostat before the step: V-rescale factor from the current kinetic
@@ -1034,43 +1100,52 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
           x2 += (pz * inv_m) * dt;
         }
       }
-      // displacement since the build, in FP64 on the wrapped position
+      // displacement since the build and since the last pruning, in FP64 on
+      // the wrapped position; the new FP32 position goes to the staging table
       double y0 = 0.0, y1 = 0.0, y2 = 0.0;
-      bool moved = false;
+      bool moved = false, pmoved = false;
       if (own) {
         wrapped(g, x0, x1, x2, Wx, Wy, Wz, y0, y1, y2);
         const double d0 = y0 - yb0, d1 = y1 - yb1, d2 = y2 - yb2;
         moved = d0 * d0 + d1 * d1 + d2 * d2 > g.half_skin2;
+        const double e0 = y0 - zp0, e1 = y1 - zp1, e2 = y2 - zp2;
+        pmoved = e0 * e0 + e1 * e1 + e2 * e2 > g.half_prune2;
+        if (lead) s_pos[a] = make_float4((float)y0, (float)y1, (float)y2, __int_as_float(sp));
       }
       // all warps are done reading the previous positions
       __syncthreads();
-      // refresh: the lanes of each atom rewrite the atom and its own images, the
-      // images in FP32 from the atom's FP32 position and the FP32 cell
-      if (own) {
-        const float fy0 = (float)y0, fy1 = (float)y1, fy2 = (float)y2;
-        for (int it = lane; it <= gcnt; it += tpa) {
-          if (it == 0) {
-            s_ext[a] = make_float4(fy0, fy1, fy2, __int_as_float(sp));
-            Y[3 * a] = y0;
-            Y[3 * a + 1] = y1;
-            Y[3 * a + 2] = y2;
-          } else {
-            const int gg = gbeg + it - 1;
-            int owner, sx, sy, sz;
-            unpack_ghost(s_gshift[gg - n], owner, sx, sy, sz);
-            const float fx = (float)sx, fyy = (float)sy, fz = (float)sz;
-            float4 e;
-            e.x = fy0 + fmaf(fz, g.Cf[6], fmaf(fyy, g.Cf[3], fx * g.Cf[0]));
-            e.y = fy1 + fmaf(fz, g.Cf[7], fmaf(fyy, g.Cf[4], fx * g.Cf[1]));
-            e.z = fy2 + fmaf(fz, g.Cf[8], fmaf(fyy, g.Cf[5], fx * g.Cf[2]));
-            e.w = __int_as_float(sp);
-            s_ext[gg] = e;
-          }
+      // refresh: every thread rewrites an even share of the table -- atoms from
+      // the staging table, images in FP32 from their owner's FP32 position and
+      // the FP32 cell
+      if (lead) {
+        Y[3 * a] = y0;
+        Y[3 * a + 1] = y1;
+        Y[3 * a + 2] = y2;
+      }
+      for (int e = tid; e < n_ext; e += kFusedThreads) {
+        if (e < n) {
+          s_ext[e] = s_pos[e];
+        } else {
+          int owner, sx, sy, sz;
+          unpack_ghost(s_gshift[e - n], owner, sx, sy, sz);
+          const float4 o = s_pos[owner];
+          const float fx = (float)sx, fyy = (float)sy, fz = (float)sz;
+          float4 q;
+          q.x = o.x + fmaf(fz, g.Cf[6], fmaf(fyy, g.Cf[3], fx * g.Cf[0]));
+          q.y = o.y + fmaf(fz, g.Cf[7], fmaf(fyy, g.Cf[4], fx * g.Cf[1]));
+          q.z = o.z + fmaf(fz, g.Cf[8], fmaf(fyy, g.Cf[5], fx * g.Cf[2]));
+          q.w = o.w;
+          s_ext[e] = q;
         }
       }
-      if (__syncthreads_or(moved)) {
-        TSB_REBUILD()
-        if (failed) break;
+      if (__syncthreads_or(moved || pmoved)) {
+        if (__syncthreads_or(moved)) {
+          TSB_REBUILD()
+          if (failed) break;
+          TSB_PRUNE(yb0, yb1, yb2)
+        } else {
+          TSB_PRUNE((float)y0, (float)y1, (float)y2)
+        }
       }
       const bool report = A.rep_every > 0 && (step + 1) % A.rep_every == 0 &&
                           (step + 1) / A.rep_every <= A.n_frames;
@@ -1120,6 +1195,7 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
 #undef TSB_VIR1
 #undef EXT
 #undef TSB_REBUILD
+#undef TSB_PRUNE
 #undef TSB_FILE_PAIR
     // ---- write back + FP64 energy reduction (each pair seen from both ends)
     __syncthreads();  // every lane is done reading Y before forces overwrite it
@@ -1396,10 +1472,9 @@ extern "C" int tsb_fused_md_ex(int integrator, int potential, const double *tabl
                                int chain_steps, int sy_steps, uint64_t seed, uint64_t counter,
                                uint64_t *counter_dev, float *frame_x, double *frame_e,
                                int64_t report_every, int64_t n_frames, int lanes_max,
-                               int64_t n_wide, double *energy, double *stress,
-                               int32_t *n_rebuilds,
-                               int32_t *status, void *workspace, size_t workspace_bytes,
-                               void *stream) {
+                               int64_t n_wide, double prune_skin, double *energy,
+                               double *stress, int32_t *n_rebuilds, int32_t *status,
+                               void *workspace, size_t workspace_bytes, void *stream) {
   if (integrator < TSB_INT_NVE || integrator > TSB_INT_VRESCALE) return TSB_ERR_INVALID_ARG;
   if (potential < TSB_POT_LJ || potential > TSB_POT_SOFT) return TSB_ERR_INVALID_ARG;
   if (n_species < 1 || !table || (n_species > 1 && !species)) return TSB_ERR_INVALID_ARG;
@@ -1420,6 +1495,7 @@ extern "C" int tsb_fused_md_ex(int integrator, int potential, const double *tabl
   if (report_every < 0 || n_frames < 0) return TSB_ERR_INVALID_ARG;
   if (lanes_max < 0 || lanes_max > 32 || (lanes_max & (lanes_max - 1))) return TSB_ERR_INVALID_ARG;
   if (n_wide >= 0 && !order) return TSB_ERR_INVALID_ARG;
+  if (!(prune_skin >= 0.0) || !std::isfinite(prune_skin)) return TSB_ERR_INVALID_ARG;
   if (report_every > 0 && n_frames > 0 && (!frame_x || !frame_e)) return TSB_ERR_INVALID_ARG;
   Carver c(workspace, workspace_bytes);
   int64_t *lo = c.take<int64_t>(n_systems);
@@ -1441,6 +1517,7 @@ extern "C" int tsb_fused_md_ex(int integrator, int potential, const double *tabl
               report_every > 0 && n_frames > 0 ? report_every : 0, n_frames, n_atoms};
   A.stress = stress;
   A.lanes_max = lanes_max;
+  A.prune = prune_skin;
   launch_all(A, n_wide, queue, st);
   if (counter_dev) k_advance_counter<<<1, 32, 0, st>>>(counter_dev, n_steps);
   TSB_CHECK_LAUNCH();

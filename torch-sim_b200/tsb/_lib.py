@@ -120,7 +120,8 @@ PROTOTYPES = {
     "tsb_fused_md_ex": (_int, [_int, _int, _vp, _int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64,
                                _i64, _vp, _dbl, _dbl, _i64, _vp, _vp, _vp, _vp, _vp, _vp,
                                _vp, _vp, _vp, _int, _int, _int, _u64, _u64, _vp, _vp, _vp,
-                               _i64, _i64, _int, _i64, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
+                               _i64, _i64, _int, _i64, _dbl, _vp, _vp, _vp, _vp, _vp, _sz,
+                               _vp]),
     "tsb_npt_workspace_size": (_sz, [_i64]),
     "tsb_npt_langevin_iso_pre": (_int, [_vp, _vp, _vp, _vp, _vp, _i64, _i64, _int, _vp, _vp,
                                         _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,

@@ -1,7 +1,8 @@
 """Project-written autotuner for launch parameters that depend on the workload.
 
-The persistent fused MD kernel has two tunable parameters: the Verlet skin
-(physics) and the launch shape of small systems, i.e. how many threads share
+The persistent fused MD kernel has three tunable parameters: the Verlet skin
+and the pruning skin of the list's shell (physics), and the launch shape of
+small systems, i.e. how many threads share
 one atom's neighbour list (``lanes``: 4, 8, 16 or 32 at most; more lanes split
 each list finer, but every lane repeats the atom's integration step).  First
 the skin.  A wider skin puts
@@ -12,8 +13,12 @@ temperature, density, cutoff, time step and system sizes, so
 systems and keeps the fastest, cached per device and workload signature in a
 JSON file (``TSB_AUTOTUNE_CACHE``, default ``~/.cache/tsb/autotune.json``).
 Results do not depend on the skin (only the rebuild rate does), so any choice
-is safe.  Then, at that skin, :func:`tune_fused_lanes` times the lane caps the
-same way.  ``FusedMD(..., skin="auto")`` and ``run_md(..., skin="auto")`` use both.
+is safe.  Skins are timed with the shell pruned at a fixed fraction of the
+skin; then, at the chosen skin, :func:`tune_fused_prune` times pruning skins
+(0 = every list pair evaluated every step; a narrower pruning skin evaluates
+fewer pairs but prunes the shell more often), and :func:`tune_fused_lanes` the
+lane caps, the same way.  ``FusedMD(..., skin="auto")`` and
+``run_md(..., skin="auto")`` use all three.
 """
 
 from __future__ import annotations
@@ -28,6 +33,7 @@ import torch
 
 DEFAULT_SKINS = (0.3, 0.5, 0.7, 1.0, 1.4)
 DEFAULT_LANES = (4, 8, 16, 32)
+DEFAULT_PRUNE_FRACTIONS = (0.0, 0.2, 0.35, 0.5)
 
 
 def cache_path() -> str:
@@ -149,7 +155,8 @@ def tune_fused_skin(state, model, *, integrator: str = "nvt_langevin", dt, kT=No
     timings = {}
     for skin in candidates:
         r = FusedMD(sample.clone(), model, integrator=integrator, dt=per_sys(dt),
-                    kT=per_sys(kT), gamma=per_sys(gamma), skin=float(skin), seed=0)
+                    kT=per_sys(kT), gamma=per_sys(gamma), skin=float(skin), seed=0,
+                    prune=None)
         r.launch(n_steps)
         timings[float(skin)] = float(timer(r, n_steps))
         r.check()
@@ -178,19 +185,54 @@ def _sample(state, sample_systems):
     return sample, per_sys, len(idx)
 
 
+def tune_fused_prune(state, model, *, skin: float, integrator: str = "nvt_langevin", dt,
+                     kT=None, gamma=None, fractions=DEFAULT_PRUNE_FRACTIONS, n_steps: int = 200,
+                     sample_systems: int | None = None, cache: TuneCache | None = None,
+                     force: bool = False, timer=_time_launch) -> float:
+    """Pruning skin (Angstrom) for ``FusedMD`` at a given skin: candidates are
+    ``fractions`` of the skin, timed like :func:`tune_fused_skin` and cached under
+    the same workload signature; ties go to the smaller pruning skin."""
+    from .integrators import FusedMD
+
+    cache = cache or TuneCache()
+    dev = state.device
+    name = torch.cuda.get_device_name(dev) if dev.type == "cuda" else str(dev)
+    key = (f"fused_prune|skin{_sig(skin, 3)}|" +
+           fused_signature(state, model, integrator, dt, kT, name))
+    candidates = sorted({round(float(f) * float(skin), 6) for f in fractions})
+    if not force:
+        rec = cache.get(key)
+        if rec is not None and float(rec.get("prune", -1)) in candidates:
+            return float(rec["prune"])
+    sample, per_sys, n_sample = _sample(state, sample_systems)
+    timings = {}
+    for prune in candidates:
+        r = FusedMD(sample.clone(), model, integrator=integrator, dt=per_sys(dt),
+                    kT=per_sys(kT), gamma=per_sys(gamma), skin=float(skin), seed=0,
+                    prune=float(prune))
+        r.launch(n_steps)
+        timings[float(prune)] = float(timer(r, n_steps))
+        r.check()
+    best = select_best(timings)
+    cache.put(key, {"prune": best, "timings_ms": {str(k): v for k, v in timings.items()},
+                    "n_steps": n_steps, "sample_systems": n_sample})
+    return best
+
+
 def tune_fused_lanes(state, model, *, skin: float, integrator: str = "nvt_langevin", dt,
                      kT=None, gamma=None, candidates=DEFAULT_LANES, n_steps: int = 200,
                      sample_systems: int | None = None, cache: TuneCache | None = None,
-                     force: bool = False, timer=_time_launch) -> int:
-    """Lane cap (threads per atom) for ``FusedMD`` at a given skin, timed like
-    :func:`tune_fused_skin` and cached under the same workload signature; ties
-    go to fewer lanes."""
+                     force: bool = False, timer=_time_launch, prune: float | None = None) -> int:
+    """Lane cap (threads per atom) for ``FusedMD`` at a given skin (and pruning
+    skin), timed like :func:`tune_fused_skin` and cached under the same workload
+    signature; ties go to fewer lanes."""
     from .integrators import FusedMD
 
     cache = cache or TuneCache()
     dev = state.device
     name = torch.cuda.get_device_name(dev) if dev.type == "cuda" else str(dev)
     key = (f"fused_lanes|skin{_sig(skin, 3)}|" +
+           (f"prune{_sig(prune, 3)}|" if prune is not None else "") +
            fused_signature(state, model, integrator, dt, kT, name))
     if not force:
         rec = cache.get(key)
@@ -201,7 +243,7 @@ def tune_fused_lanes(state, model, *, skin: float, integrator: str = "nvt_langev
     for lanes in candidates:
         r = FusedMD(sample.clone(), model, integrator=integrator, dt=per_sys(dt),
                     kT=per_sys(kT), gamma=per_sys(gamma), skin=float(skin), seed=0,
-                    lanes=int(lanes))
+                    lanes=int(lanes), prune=prune)
         r.launch(n_steps)
         timings[int(lanes)] = float(timer(r, n_steps))
         r.check()

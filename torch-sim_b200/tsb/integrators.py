@@ -29,6 +29,8 @@ kernel launch (see csrc/tsb_fused.cu).
 
 from __future__ import annotations
 
+import math
+
 import torch
 
 from . import _lib as L
@@ -842,6 +844,7 @@ def _system_order(state):
 
 
 NARROW_MAX_ATOMS = 256      # systems the 256-thread blocks of the fused kernel take
+PRUNE_FRACTION = 0.35       # default pruning skin of the fused kernel, relative to its skin
 NARROW_MAX_IMAGES = 1968    # their table of atoms + periodic images
 
 
@@ -874,7 +877,8 @@ class FusedMD:
 
     def __init__(self, state, model, *, integrator: str = "nvt_langevin", dt, kT=None,
                  gamma=None, skin: float | str = 0.7, seed: int | None = None, tau=None,
-                 lanes: int | str | None = None, shapes: str = "auto"):
+                 lanes: int | str | None = None, shapes: str = "auto",
+                 prune: float | str | None = None):
         from .models.pair_potential import PairTableModel
 
         if not isinstance(model, PairTableModel):
@@ -946,14 +950,30 @@ class FusedMD:
                                    gamma=gamma)
             if lanes is None:
                 lanes = "auto"
+            if prune is None:
+                prune = "auto"
         self.skin = float(skin)
+        # pruning skin of the list's shell (Angstrom; 0: off): None is a fixed
+        # fraction of the skin, "auto" the project autotuner
+        if prune is None:
+            prune = PRUNE_FRACTION * self.skin
+        elif prune == "auto":
+            from .autotune import tune_fused_prune
+
+            prune = tune_fused_prune(state, model, skin=self.skin, integrator=integrator,
+                                     dt=dt, kT=kT, gamma=gamma)
+        elif isinstance(prune, str):
+            raise ValueError(f"prune must be a number, None or 'auto', got {prune!r}")
+        if not (float(prune) >= 0.0 and math.isfinite(float(prune))):
+            raise ValueError(f"prune must be >= 0, got {prune!r}")
+        self.prune = float(prune)
         # threads per atom at most (small systems); "auto": the project autotuner
         self.lanes = 32 if lanes is None else lanes
         if self.lanes == "auto":
             from .autotune import tune_fused_lanes
 
             self.lanes = tune_fused_lanes(state, model, skin=self.skin, integrator=integrator,
-                                          dt=dt, kT=kT, gamma=gamma)
+                                          dt=dt, kT=kT, gamma=gamma, prune=self.prune)
         if self.lanes not in (1, 2, 4, 8, 16, 32):
             raise ValueError(f"lanes must be a power of two in 1..32, got {self.lanes!r}")
         # block shapes: "auto" puts small systems in 256-thread blocks (two per
@@ -994,8 +1014,8 @@ class FusedMD:
             self.dt_s, self.kT_s, self.g_s, getattr(self, "tau_s", None), g("cxi"), g("cpxi"),
             g("cQ"), g("cke"), g("cdt"), self.M if nh else 0, self.nc if nh else 0,
             self.nsy if nh else 0, _i64(self.seed), 0, self.counter_dev, fx, fe, int(every),
-            self.lanes, self.n_wide, self.energy, self.stress, self.rebuilds, self.status,
-            self.ws)
+            self.lanes, self.n_wide, self.prune, self.energy, self.stress, self.rebuilds,
+            self.status, self.ws)
 
     def graph(self, n_steps: int) -> "torch.cuda.CUDAGraph":
         """CUDA graph of one ``launch(n_steps)``; ``g.replay()`` advances every system
@@ -1057,9 +1077,10 @@ def _scatter_back(state, sub, systems, chain: bool):
             getattr(state.chain, name)[sel] = getattr(sub.chain, name)
 
 
-def _run_fused(state, model, n_steps, integrator, dt, kT, gamma, skin, seed, check, tau):
+def _run_fused(state, model, n_steps, integrator, dt, kT, gamma, skin, seed, check, tau,
+               prune=None):
     r = FusedMD(state, model, integrator=integrator, dt=dt, kT=kT, gamma=gamma, skin=skin,
-                seed=seed, tau=tau)
+                seed=seed, tau=tau, prune=prune)
     r.launch(n_steps)
     if check:
         r.check()
@@ -1086,7 +1107,7 @@ def _run_per_call(state, model, n_steps, integrator, dt, kT, gamma, seed, tau):
 def run_md(state, model, n_steps: int, *, integrator: str = "nvt_langevin", dt, kT=None,
            gamma=None, skin: float | str = 0.7, seed: int | None = None, check: bool = True,
            return_rebuilds: bool = False, tau=None, max_memory_scaler: float | None = None,
-           memory_scales_with: str = "n_atoms_x_density"):
+           memory_scales_with: str = "n_atoms_x_density", prune: float | str | None = None):
     """Advance every system ``n_steps`` in ONE persistent kernel launch.
 
     Same update rules as ``nve_step`` / ``nvt_langevin_step`` (Langevin noise
@@ -1094,7 +1115,10 @@ def run_md(state, model, n_steps: int, *, integrator: str = "nvt_langevin", dt, 
     ``nvt_nose_hoover_init``; its chain is updated) / ``nvt_vrescale_step`` (``tau``,
     default 10 dt; same Philox draws as the step function), with a device-side
     Verlet list (cutoff + skin)
-    rebuilt when any atom of a system moved more than skin/2.  ``model`` must be
+    rebuilt when any atom of a system moved more than skin/2; between builds only
+    the list's pairs within cutoff + ``prune`` are evaluated (re-pruned when an
+    atom moved more than prune/2; default a fixed fraction of the skin, 0 off,
+    "auto" tuned).  ``model`` must be
     a :class:`tsb.models.PairTableModel` (LJ / Morse / soft sphere, any species
     table); all axes must be periodic.  ``state`` is updated in place
     (positions, momenta, forces, energy).
@@ -1112,7 +1136,7 @@ def run_md(state, model, n_steps: int, *, integrator: str = "nvt_langevin", dt, 
     any_big = bool(big.any())
     if not any_big and max_memory_scaler is None:
         rebuilds = _run_fused(state, model, n_steps, integrator, dt, kT, gamma, skin, seed,
-                              check, tau)
+                              check, tau, prune)
         return (state, rebuilds) if return_rebuilds else state
     from .autobatching import BinningAutoBatcher
     from .state import select_systems
@@ -1139,7 +1163,7 @@ def run_md(state, model, n_steps: int, *, integrator: str = "nvt_langevin", dt, 
                     if hasattr(sub, k):
                         setattr(part, k, getattr(sub, k))
             rb = _run_fused(part, model, n_steps, integrator, dt, kT, gamma, skin, seed, check,
-                            tau)
+                            tau, prune)
             if part is not sub:
                 _scatter_back(sub, part, idx, chain)
             rebuilds[torch.as_tensor([small_idx[i] for i in idx], device=state.device)] = rb

@@ -194,8 +194,8 @@ _define("md_baoab_boa_(Tensor(a!) positions, Tensor(b!) momenta, Tensor forces, 
 def _fused_md(integrator, kind, table, n_species, species, positions, momenta, forces, masses,
               cell_row, system_idx, order, cutoff, skin, n_steps, dt, kT, gamma, tau, chain_xi,
               chain_pxi, chain_q, chain_ke, chain_dt, chain_length, chain_steps, sy_steps, seed,
-              counter, counter_dev, frame_x, frame_e, report_every, lanes_max, n_wide, energy,
-              stress, n_rebuilds, status, workspace):
+              counter, counter_dev, frame_x, frame_e, report_every, lanes_max, n_wide,
+              prune_skin, energy, stress, n_rebuilds, status, workspace):
     n_frames = frame_x.shape[0] if frame_x is not None else 0
     L.call("tsb_fused_md_ex", int(integrator), int(kind), _P(table), int(n_species),
            _P(species), _P(positions), _P(momenta), _P(forces), _P(masses), _P(cell_row),
@@ -204,7 +204,7 @@ def _fused_md(integrator, kind, table, n_species, species, positions, momenta, f
            _P(chain_pxi), _P(chain_q), _P(chain_ke), _P(chain_dt), int(chain_length),
            int(chain_steps), int(sy_steps), _u64(seed), _u64(counter), _P(counter_dev),
            _P(frame_x), _P(frame_e), int(report_every), int(n_frames), int(lanes_max),
-           int(n_wide), _P(energy), _P(stress),
+           int(n_wide), float(prune_skin), _P(energy), _P(stress),
            _P(n_rebuilds), _P(status), _P(workspace), workspace.numel(), _stream(positions))
 
 
@@ -216,7 +216,7 @@ _define("fused_md_(int integrator, int kind, Tensor table, int n_species, Tensor
         "Tensor(g!)? chain_ke, Tensor? chain_dt, int chain_length, int chain_steps, "
         "int sy_steps, int seed, int counter, Tensor(h!)? counter_dev, Tensor(i!)? frame_x, "
         "Tensor(j!)? frame_e, int report_every, int lanes_max, int n_wide, "
-        "Tensor(k!) energy, "
+        "float prune_skin, Tensor(k!) energy, "
         "Tensor(l!)? stress, "
         "Tensor(m!)? n_rebuilds, Tensor(n!) status, Tensor(o!) workspace) -> ()",
         _fused_md, _noop)
