@@ -16,9 +16,10 @@ the oracle can replay a fused-kernel trajectory with the very same noise:
 * ``fused_normals``   the three Langevin normals per atom and step of the
   fused MD kernel: counter (atom, step), key = seed; Box-Muller on 24-bit
   uniforms u = (w >> 8 + 1) 2^-24 for the radii and t = (w >> 8) 2^-23 for the
-  angles pi t.  The kernel evaluates these in FP32 (logf, sqrtf, sincospif);
-  here they are evaluated in FP64 from the same integers, so the two agree to
-  FP32 rounding (a few 1e-7 relative).
+  angles pi t.  The kernel evaluates these in FP32 with the hardware's
+  approximate log2, sine and cosine (on pi (t - 1), negated); here they are
+  evaluated in FP64 from the same integers, so the two agree to a few 1e-6
+  absolute.
 * ``step_normals``    the four FP64 normals per atom and step of the per-call
   BAOAB kernel (32-bit uniforms, FP64 Box-Muller).
 * ``thermo_normal`` / ``gamma_deviate``  the per-system draws of the V-rescale

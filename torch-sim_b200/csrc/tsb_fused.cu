@@ -88,8 +88,9 @@ struct FusedSmem {
   static_assert(S::kMaxBins <= 4 * NT, "bin scan: four bins per thread");
   static_assert((S::kExtMax - 1) * sizeof(float4) <= 0xFFFF,
                 "list entries are 16-bit byte offsets");
-  static_assert(kBins >= (size_t)NT * sizeof(float4), "atom positions alias the bin table");
-  static_assert((kList + kExt + kGhost + kSorted) % 16 == 0, "bin table 16-byte aligned");
+  static_assert(kSorted + kBins >= (size_t)NT * 3 * sizeof(double),
+                "atom positions alias the sort and bin tables");
+  static_assert((kList + kExt + kGhost) % 8 == 0, "sort table 8-byte aligned");
 };
 
 struct FusedArgs {
@@ -137,7 +138,6 @@ struct FusedArgs {
 // per-system geometry, computed by thread 0 into shared memory
 struct FusedGeom {
   double C[9];    // row-vector cell
-  float Cf[9];    // the same in FP32 (image shifts between list builds)
   double T[9];    // inv(C)^T: fractional coordinates u = T r
   double ctr[3];  // cell centre
   double tn[3];   // |row k of T|
@@ -156,6 +156,12 @@ struct FusedGeom {
   float band;     // FP32 r^2 within +-band of cutoff^2: decide in FP64
   float build2;   // list radius^2 used by the FP32 build test
   float core2[kFusedMaxSpecies * kFusedMaxSpecies];  // core-pair bound^2 per pair type
+  // search window of the list build, FP32: bin width and margin h in
+  // fractional coordinates, 1 / width, plane window (list radius) |T_k| + eps,
+  // |a_k|^2, and 1 / lambda with lambda a lower bound of the smallest
+  // eigenvalue of D^-1 G D^-1 (G = C C^T, D = diag |a_k|), so that
+  // |d|^2 >= lambda sum_k |a_k|^2 du_k^2 for any fractional offset du
+  float sw[3], sh[3], siw[3], stw[3], alen2[3], ilam;
   int rep[3];
   int nb[3];
   int nbins;
@@ -202,23 +208,21 @@ __device__ inline bool set_margins(FusedGeom &g, double cutoff, double prune, co
     ymax = fmax(ymax, y);
     ypmax = fmax(ypmax, yp);
   }
-  // Between list builds the images are refreshed in FP32 as fl(fl32(y) + s Cf):
-  // each coordinate is then off by at most 2^-24 (|y| + 4 |s C| + |y + s C|)
-  // <= 6 2^-24 Y', Y' = max_m sum_k (1/2 + rep_k) |C_km| (at the build they are
-  // fl32 of the FP64 image, off by 2^-24 Y <= 2^-24 Y'), so the band of the
-  // FP32 cutoff test uses 6 Y' for Y.
+  // Every table entry is fl32 of its FP64 value (atoms and images alike, at
+  // the build and at every refresh), off by at most 2^-24 Y per coordinate.
   g.band = (float)(2.0 * 5.9604644775390625e-8 *
-                   (4.0 * 1.7320508075688772 * 6.0 * ypmax * cutoff + 6.0 * cutoff * cutoff));
+                   (4.0 * 1.7320508075688772 * ymax * cutoff + 6.0 * cutoff * cutoff));
   const double margin = 1e-6 * (4.0 * ymax + R);
   g.build2 = (float)((R + margin) * (R + margin));
   // Pruned shell: a pair whose FP32 distance at the pruning is at least
-  // cutoff + prune + pm, pm = 1e-6 (8 Y' + R), is left out until the next
-  // pruning.  Until then no atom moves more than prune / 2 from its position at
-  // the pruning (tested in FP64 against that position rounded to FP32), so the
-  // exact distance stays above the cutoff: pm covers the FP32 distance error
-  // (image coordinates off by <= 6 2^-24 Y', the atom by 2^-24 Y <= 2^-24 Y',
-  // so |d| is off by <= 7 sqrt3 2^-24 Y' plus ~2^-23 R from the arithmetic) and
-  // the FP32 rounding of both reference positions (2 sqrt3 2^-24 Y').
+  // cutoff + prune + pm, pm = 1e-6 (8 Y' + R) (Y' = max_m sum_k (1/2 + rep_k)
+  // |C_km| >= Y), is left out until the next pruning.  Until then no atom moves
+  // more than prune / 2 from its position at the pruning (tested in FP64
+  // against that position rounded to FP32), so the exact distance stays above
+  // the cutoff: pm covers the FP32 distance error (each coordinate of both
+  // entries off by <= 2^-24 Y, so |d| by <= 2 sqrt3 2^-24 Y, plus ~2^-23 R from
+  // the arithmetic) and the FP32 rounding of both reference positions
+  // (2 sqrt3 2^-24 Y), with a wide margin.
   const double pr = (prune > 0.0 && prune < g.skin) ? prune : 0.0;
   g.prune_on = pr > 0.0;
   g.half_prune2 = pr > 0.0 ? 0.25 * pr * pr : INFINITY;
@@ -249,6 +253,13 @@ __device__ inline bool set_margins(FusedGeom &g, double cutoff, double prune, co
       g.nbins = (int)tot;
       break;
     }
+  }
+  const double rb = sqrt((double)g.build2);
+  for (int k = 0; k < 3; ++k) {
+    g.sw[k] = g.iw[k] > 0.0 ? (float)(1.0 / g.iw[k]) : 1e30f;
+    g.sh[k] = (float)g.h[k];
+    g.siw[k] = (float)g.iw[k];
+    g.stw[k] = (float)(rb * g.tn[k]) + 1e-5f;
   }
   return ok;
 }
@@ -327,22 +338,45 @@ __device__ __noinline__ void warps_sum7(const double (*sh)[NT / 32], double *out
   }
 }
 
-// FP32 standard normals for the O-step (Philox4x32-10 + Box-Muller).
+// PTX approximate base-2 logarithm, sine and cosine (hardware MUFU; absolute
+// errors ~2^-22 for lg2 near 1 and ~2^-21 for sin / cos on [-pi, pi]).
+__device__ __forceinline__ float lg2_ftz(float x) {
+  float y;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float sin_ftz(float x) {
+  float y;
+  asm("sin.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float cos_ftz(float x) {
+  float y;
+  asm("cos.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// FP32 standard normals for the O-step (Philox4x32-10 + Box-Muller): radii
+// sqrt(-2 ln u), u = (w >> 8 + 1) 2^-24 in (0, 1], and angles pi t,
+// t = (w >> 8) 2^-23 in [0, 2), evaluated as -cos / -sin of pi (t - 1) (t - 1
+// is exact) so that the hardware sine and cosine see arguments in [-pi, pi).
+// The values agree with the FP64 Box-Muller of the same integers to a few
+// 1e-6 absolute.
 __device__ inline void normal3f(uint64_t seed, uint64_t atom, uint64_t counter, float *z) {
   U4 c{(uint32_t)atom, (uint32_t)(atom >> 32), (uint32_t)counter, (uint32_t)(counter >> 32)};
   U4 r = philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
   const float k24 = 5.9604644775390625e-8f;  // 2^-24
+  const float m2ln2 = -1.3862943611198906f;   // -2 ln 2
+  const float pi = 3.14159265358979f;
   const float u1 = (float)((r.x >> 8) + 1u) * k24;  // (0, 1]
   const float u2 = (float)((r.z >> 8) + 1u) * k24;
-  const float r1 = sqrtf(-2.0f * logf(u1));
-  const float r2 = sqrtf(-2.0f * logf(u2));
-  float s1, c1, s2, c2;
-  sincospif((float)(r.y >> 8) * (2.0f * k24), &s1, &c1);
-  sincospif((float)(r.w >> 8) * (2.0f * k24), &s2, &c2);
-  z[0] = r1 * c1;
-  z[1] = r1 * s1;
-  z[2] = r2 * c2;
-  (void)s2;
+  const float r1 = sqrtf(fmaxf(m2ln2 * lg2_ftz(u1), 0.0f));
+  const float r2 = sqrtf(fmaxf(m2ln2 * lg2_ftz(u2), 0.0f));
+  const float a1 = pi * ((float)(r.y >> 8) * (2.0f * k24) - 1.0f);
+  const float a2 = pi * ((float)(r.w >> 8) * (2.0f * k24) - 1.0f);
+  z[0] = -r1 * cos_ftz(a1);
+  z[1] = -r1 * sin_ftz(a1);
+  z[2] = -r2 * cos_ftz(a2);
 }
 
 // ghost slot word: shift (sx, sy, sz) in [-15, 15] as 5-bit fields, owner atom above
@@ -476,14 +510,19 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
   int *s_bin = (int *)(smem + kSmemList + kSmemExt + kSmemGhost + kSmemSorted);
   uint16_t *list16 = (uint16_t *)s_list;
   uint16_t *s_ebin = (uint16_t *)s_list;  // bin of each entry, during a rebuild only
-  // the atoms' new FP32 positions, from the integrator phase of a step to the
-  // image refresh of the same step (the bin table is free then)
-  float4 *s_pos = (float4 *)s_bin;
+  // the atoms' new FP64 wrapped positions [n, 3], from the integrator phase of
+  // a step to the image refresh of the same step (the sort and bin tables of
+  // the list build are free then)
+  double *s_posd = (double *)s_sorted;
   __shared__ FusedGeom g;
   __shared__ PairPrm<float> prm[kFusedMaxSpecies * kFusedMaxSpecies];
   __shared__ double rc2d[kFusedMaxSpecies * kFusedMaxSpecies];
   __shared__ int s_scan[33];
   __shared__ int s_work;
+  // per-step decisions (bit 1 rebuild the list, bit 2 prune it), OR-ed by the
+  // warps before the refresh barrier; two slots by step parity, so that the
+  // slot of the next step is cleared while this one is read
+  __shared__ int s_flags[2];
   __shared__ double s_red[kFusedThreads / 32];
   __shared__ double s_red7[7][kFusedThreads / 32];
 
@@ -509,14 +548,12 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
     if (w >= (A.n_work > 0 ? A.n_work : A.n_sys)) break;
     const int64_t s = A.order ? A.order[w] : w;
     if (tid == 0) {
+      s_flags[0] = s_flags[1] = 0;
       g.start = A.lo[s];
       g.n = (int)(A.hi[s] - g.start);
       g.ok = 1;
       double *C = g.C, *T = g.T;
-      for (int k = 0; k < 9; ++k) {
-        C[k] = A.cell_row[9 * s + k];
-        g.Cf[k] = (float)C[k];
-      }
+      for (int k = 0; k < 9; ++k) C[k] = A.cell_row[9 * s + k];
       const double d = C[0] * (C[4] * C[8] - C[5] * C[7]) - C[1] * (C[3] * C[8] - C[5] * C[6]) +
                        C[2] * (C[3] * C[7] - C[4] * C[6]);
       const double id = 1.0 / d;
@@ -533,6 +570,23 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
         g.tn[k] = sqrt(T[3 * k] * T[3 * k] + T[3 * k + 1] * T[3 * k + 1] +
                        T[3 * k + 2] * T[3 * k + 2]);
         g.ctr[k] = 0.5 * (C[k] + C[3 + k] + C[6 + k]);
+      }
+      {
+        // Gram matrix of the lattice vectors and a Gershgorin lower bound of the
+        // smallest eigenvalue of its unit-diagonal form (cosines off the diagonal)
+        double G[3][3];
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j)
+            G[i][j] = C[3 * i] * C[3 * j] + C[3 * i + 1] * C[3 * j + 1] + C[3 * i + 2] * C[3 * j + 2];
+        double lam = 1.0;
+        for (int i = 0; i < 3; ++i) {
+          double off = 0.0;
+          for (int j = 0; j < 3; ++j)
+            if (j != i) off += fabs(G[i][j]) / sqrt(G[i][i] * G[j][j]);
+          lam = fmin(lam, 1.0 - off);
+          g.alen2[i] = (float)(G[i][i] * (1.0 - 1e-6));
+        }
+        g.ilam = lam > 0.05 ? (float)(1.0 / lam) * 1.0001f : 1e30f;
       }
       g.skin = A.skin;
       g.dt = A.dt[s];
@@ -745,26 +799,43 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
         const float build2 = g.build2;                                                       \
         const float core0 = g.core2[0];                                                      \
         const int a16 = a << 4;                                                              \
-        const int bx = bin_coord(g, f0, 0), by = bin_coord(g, f1, 1);                        \
-        const int bz = bin_coord(g, f2, 2);                                                  \
-        const int zlo = max(bz - 2, 0), zhi = min(bz + 2, g.nb[2] - 1);                      \
-        for (int cx = max(bx - 2, 0); cx <= min(bx + 2, g.nb[0] - 1); ++cx) {                \
-          for (int cy = max(by - 2, 0); cy <= min(by + 2, g.nb[1] - 1); ++cy) {              \
+        /* bins within the list radius in each fractional coordinate; per bin row */        \
+        /* (cx, cy) the z range left by the row's gaps gx, gy to the atom:          */       \
+        /* |d|^2 >= lambda (|a_x|^2 gx^2 + |a_y|^2 gy^2 + |a_z|^2 du_z^2)           */       \
+        const float fx_ = (float)f0, fy_ = (float)f1, fz_ = (float)f2;                       \
+        const float rl2_ = g.build2 * 1.00001f * g.ilam;                                     \
+        const int xlo_ = max((int)floorf((fx_ - g.stw[0] + g.sh[0]) * g.siw[0]), 0);         \
+        const int xhi_ = min((int)floorf((fx_ + g.stw[0] + g.sh[0]) * g.siw[0]), g.nb[0] - 1); \
+        const int ylo_ = max((int)floorf((fy_ - g.stw[1] + g.sh[1]) * g.siw[1]), 0);         \
+        const int yhi_ = min((int)floorf((fy_ + g.stw[1] + g.sh[1]) * g.siw[1]), g.nb[1] - 1); \
+        for (int cx = xlo_; cx <= xhi_; ++cx) {                                              \
+          const float bl_ = (float)cx * g.sw[0] - g.sh[0];                                   \
+          const float gx_ = fmaxf(fmaxf(bl_ - fx_, fx_ - (bl_ + g.sw[0])) - 1e-5f, 0.0f);    \
+          const float qx_ = rl2_ - g.alen2[0] * gx_ * gx_;                                   \
+          for (int cy = ylo_; cy <= yhi_; ++cy) {                                            \
+            const float cl_ = (float)cy * g.sw[1] - g.sh[1];                                 \
+            const float gy_ = fmaxf(fmaxf(cl_ - fy_, fy_ - (cl_ + g.sw[1])) - 1e-5f, 0.0f);  \
+            const float rem_ = qx_ - g.alen2[1] * gy_ * gy_;                                 \
+            if (rem_ < 0.0f) continue;                                                       \
+            const float zw_ = fminf(g.stw[2], sqrtf(rem_ / g.alen2[2]) + 1e-5f);             \
+            const int zlo = max((int)floorf((fz_ - zw_ + g.sh[2]) * g.siw[2]), 0);           \
+            const int zhi = min((int)floorf((fz_ + zw_ + g.sh[2]) * g.siw[2]), g.nb[2] - 1); \
+            if (zlo > zhi) continue;                                                         \
             const int row = (cx * g.nb[1] + cy) * g.nb[2];                                   \
             const int plo = (row + zlo) ? s_bin[row + zlo - 1] : 0;                          \
             const int phi = s_bin[row + zhi];                                                \
-            /* two candidates per iteration (independent loads), kept in order */            \
-            int p_ = plo + lane;                                                             \
-            for (; p_ + tpa < phi; p_ += 2 * tpa) {                                          \
-              const int e0 = s_sorted[p_], e1 = s_sorted[p_ + tpa];                          \
-              const float4 q0 = EXT(e0), q1 = EXT(e1);                                       \
+            /* four candidates per iteration (independent loads), kept in order; */          \
+            /* positions past the row read the far sentinel entry instead        */          \
+            for (int p_ = plo + lane; p_ < phi; p_ += 4 * tpa) {                             \
+              const int e0 = s_sorted[p_];                                                   \
+              const int e1 = p_ + tpa < phi ? s_sorted[p_ + tpa] : kSentinel << 4;           \
+              const int e2 = p_ + 2 * tpa < phi ? s_sorted[p_ + 2 * tpa] : kSentinel << 4;   \
+              const int e3 = p_ + 3 * tpa < phi ? s_sorted[p_ + 3 * tpa] : kSentinel << 4;   \
+              const float4 q0 = EXT(e0), q1 = EXT(e1), q2 = EXT(e2), q3 = EXT(e3);           \
               TSB_FILE_PAIR(e0, q0)                                                          \
               TSB_FILE_PAIR(e1, q1)                                                          \
-            }                                                                                \
-            if (p_ < phi) {                                                                  \
-              const int e0 = s_sorted[p_];                                                   \
-              const float4 q0 = EXT(e0);                                                     \
-              TSB_FILE_PAIR(e0, q0)                                                          \
+              TSB_FILE_PAIR(e2, q2)                                                          \
+              TSB_FILE_PAIR(e3, q3)                                                          \
             }                                                                                \
           }                                                                                  \
         }                                                                                    \
@@ -813,37 +884,59 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
 
     // ------------------------------------------------------------ pruning
     // Each thread reorders its own shell entries (no other thread reads them):
-    // those closer than sqrt(act2) now go first (in their previous order) and
-    // are the only shell entries the force loop evaluates until the next
-    // pruning; (P0, P1, P2) is the atom's FP32 position the next pruning test
+    // those closer than sqrt(act2) go first, in their previous order, and are
+    // the only shell entries the force loop evaluates until the next pruning.
+    // The atom's FP32 position in the table is the one the next pruning test
     // measures from.  Without pruning, the whole shell is evaluated.
-#define TSB_PRUNE(P0, P1, P2)                                                                \
+#define TSB_PRUNE_STEP(I, E, ACT)                                                            \
+  if (ACT) {                                                                                 \
+    const int k_ = 4 * j_ + (I);                                                             \
+    if (w_ != k_) { /* the inactive entry at w_ moves to k_ */                               \
+      const int sw_ = kListLen - 1 - w_, sk_ = kListLen - 1 - k_;                            \
+      const int iw_ = (((sw_ >> 2) * kFusedThreads + tid) << 2) | (sw_ & 3);                 \
+      const int ik_ = (((sk_ >> 2) * kFusedThreads + tid) << 2) | (sk_ & 3);                 \
+      list16[ik_] = list16[iw_];                                                             \
+      list16[iw_] = (uint16_t)(E);                                                           \
+    }                                                                                        \
+    ++w_;                                                                                    \
+  }
+#define TSB_PRUNE()                                                                          \
   if (g.prune_on) {                                                                          \
     if (own) {                                                                               \
       const float4 xi_ = s_ext[a];                                                           \
       const float act2_ = g.act2;                                                            \
       int w_ = 0;                                                                            \
-      for (int k_ = 0; k_ < nshell; ++k_) {                                                  \
-        const int sk_ = kListLen - 1 - k_;                                                   \
-        const int ik_ = (((sk_ >> 2) * kFusedThreads + tid) << 2) | (sk_ & 3);               \
-        const uint16_t e_ = list16[ik_];                                                     \
-        const float4 q_ = EXT(e_);                                                           \
-        const float dx_ = q_.x - xi_.x, dy_ = q_.y - xi_.y, dz_ = q_.z - xi_.z;              \
-        if (dx_ * dx_ + dy_ * dy_ + dz_ * dz_ < act2_) {                                     \
-          if (w_ != k_) {                                                                    \
-            const int sw_ = kListLen - 1 - w_;                                               \
-            const int iw_ = (((sw_ >> 2) * kFusedThreads + tid) << 2) | (sw_ & 3);           \
-            list16[ik_] = list16[iw_];                                                       \
-            list16[iw_] = e_;                                                                \
-          }                                                                                  \
-          ++w_;                                                                              \
+      /* groups of four shell entries (shell entry 4j + i sits in slot        */             \
+      /* kListLen - 1 - 4j - i), the next group's word loaded one ahead; the  */             \
+      /* group's four distances first, then its entries in order             */             \
+      uint2 gn_ = s_list[(kListGroups - 1) * kFusedThreads + tid];                           \
+      for (int j_ = 0; j_ < (nshell >> 2); ++j_) {                                           \
+        const uint2 ge_ = gn_;                                                               \
+        gn_ = s_list[max(kListGroups - 2 - j_, 0) * kFusedThreads + tid];                    \
+        const uint32_t e0_ = ge_.y >> 16, e1_ = ge_.y & 0xFFFFu;                             \
+        const uint32_t e2_ = ge_.x >> 16, e3_ = ge_.x & 0xFFFFu;                             \
+        const float4 q0_ = EXT(e0_), q1_ = EXT(e1_), q2_ = EXT(e2_), q3_ = EXT(e3_);         \
+        bool a0_, a1_, a2_, a3_;                                                             \
+        {                                                                                    \
+          float dx_ = q0_.x - xi_.x, dy_ = q0_.y - xi_.y, dz_ = q0_.z - xi_.z;               \
+          a0_ = dx_ * dx_ + dy_ * dy_ + dz_ * dz_ < act2_;                                   \
+          dx_ = q1_.x - xi_.x, dy_ = q1_.y - xi_.y, dz_ = q1_.z - xi_.z;                     \
+          a1_ = dx_ * dx_ + dy_ * dy_ + dz_ * dz_ < act2_;                                   \
+          dx_ = q2_.x - xi_.x, dy_ = q2_.y - xi_.y, dz_ = q2_.z - xi_.z;                     \
+          a2_ = dx_ * dx_ + dy_ * dy_ + dz_ * dz_ < act2_;                                   \
+          dx_ = q3_.x - xi_.x, dy_ = q3_.y - xi_.y, dz_ = q3_.z - xi_.z;                     \
+          a3_ = dx_ * dx_ + dy_ * dy_ + dz_ * dz_ < act2_;                                   \
         }                                                                                    \
+        TSB_PRUNE_STEP(0, e0_, a0_)                                                          \
+        TSB_PRUNE_STEP(1, e1_, a1_)                                                          \
+        TSB_PRUNE_STEP(2, e2_, a2_)                                                          \
+        TSB_PRUNE_STEP(3, e3_, a3_)                                                          \
       }                                                                                      \
       nact = w_;                                                                             \
+      zp0 = xi_.x;                                                                           \
+      zp1 = xi_.y;                                                                           \
+      zp2 = xi_.z;                                                                           \
     }                                                                                        \
-    zp0 = (P0);                                                                              \
-    zp1 = (P1);                                                                              \
-    zp2 = (P2);                                                                              \
   } else {                                                                                   \
     nact = nshell;                                                                           \
   }
@@ -1052,7 +1145,7 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
 
     TSB_REBUILD()
     if (failed) continue;
-    TSB_PRUNE(yb0, yb1, yb2)
+    TSB_PRUNE()
     for (int64_t step = 0; step < A.n_steps; ++step) {
       const double dt = g.dt, half = g.half, c1 = g.c1;
       // thermostat before the step: V-rescale factor from the current kinetic
@@ -1101,51 +1194,53 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
         }
       }
       // displacement since the build and since the last pruning, in FP64 on
-      // the wrapped position; the new FP32 position goes to the staging table
+      // the wrapped position; the new position goes to the staging table
       double y0 = 0.0, y1 = 0.0, y2 = 0.0;
-      bool moved = false, pmoved = false;
+      int flag = 0;
       if (own) {
         wrapped(g, x0, x1, x2, Wx, Wy, Wz, y0, y1, y2);
         const double d0 = y0 - yb0, d1 = y1 - yb1, d2 = y2 - yb2;
-        moved = d0 * d0 + d1 * d1 + d2 * d2 > g.half_skin2;
+        if (d0 * d0 + d1 * d1 + d2 * d2 > g.half_skin2) flag |= 1;
         const double e0 = y0 - zp0, e1 = y1 - zp1, e2 = y2 - zp2;
-        pmoved = e0 * e0 + e1 * e1 + e2 * e2 > g.half_prune2;
-        if (lead) s_pos[a] = make_float4((float)y0, (float)y1, (float)y2, __int_as_float(sp));
+        const double ee = e0 * e0 + e1 * e1 + e2 * e2;
+        if (ee > g.half_prune2) flag |= 2;
+        if (lead) {
+          s_posd[3 * a] = y0;
+          s_posd[3 * a + 1] = y1;
+          s_posd[3 * a + 2] = y2;
+        }
       }
       // all warps are done reading the previous positions
       __syncthreads();
-      // refresh: every thread rewrites an even share of the table -- atoms from
-      // the staging table, images in FP32 from their owner's FP32 position and
-      // the FP32 cell
+      // refresh: every thread rewrites an even share of the table, each entry
+      // fl32 of its FP64 value (atom, or owner + lattice shift), so that the
+      // rounding errors of different entries are independent (FP32 shift
+      // arithmetic would give every image of one shift the same error)
       if (lead) {
         Y[3 * a] = y0;
         Y[3 * a + 1] = y1;
         Y[3 * a + 2] = y2;
       }
       for (int e = tid; e < n_ext; e += kFusedThreads) {
-        if (e < n) {
-          s_ext[e] = s_pos[e];
-        } else {
-          int owner, sx, sy, sz;
-          unpack_ghost(s_gshift[e - n], owner, sx, sy, sz);
-          const float4 o = s_pos[owner];
-          const float fx = (float)sx, fyy = (float)sy, fz = (float)sz;
-          float4 q;
-          q.x = o.x + fmaf(fz, g.Cf[6], fmaf(fyy, g.Cf[3], fx * g.Cf[0]));
-          q.y = o.y + fmaf(fz, g.Cf[7], fmaf(fyy, g.Cf[4], fx * g.Cf[1]));
-          q.z = o.z + fmaf(fz, g.Cf[8], fmaf(fyy, g.Cf[5], fx * g.Cf[2]));
-          q.w = o.w;
-          s_ext[e] = q;
-        }
+        const int sp_e = __float_as_int(s_ext[e].w);
+        int owner = e, sx = 0, sy = 0, sz = 0;
+        if (e >= n) unpack_ghost(s_gshift[e - n], owner, sx, sy, sz);
+        s_ext[e] = image_of(g, s_posd[3 * owner], s_posd[3 * owner + 1],
+                            s_posd[3 * owner + 2], sx, sy, sz, sp_e);
       }
-      if (__syncthreads_or(moved || pmoved)) {
-        if (__syncthreads_or(moved)) {
-          TSB_REBUILD()
-          if (failed) break;
-          TSB_PRUNE(yb0, yb1, yb2)
-        } else {
-          TSB_PRUNE((float)y0, (float)y1, (float)y2)
-        }
+      {
+        const int wf = __reduce_or_sync(0xffffffffu, flag);
+        if ((tid & 31) == 0 && wf) atomicOr(&s_flags[step & 1], wf);
+      }
+      __syncthreads();
+      const int fl = s_flags[step & 1];
+      if (tid == 0) s_flags[(step + 1) & 1] = 0;
+      if (fl & 1) {
+        TSB_REBUILD()
+        if (failed) break;
+        TSB_PRUNE()
+      } else if (fl & 2) {
+        TSB_PRUNE()
       }
       const bool report = A.rep_every > 0 && (step + 1) % A.rep_every == 0 &&
                           (step + 1) / A.rep_every <= A.n_frames;
@@ -1196,6 +1291,7 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
 #undef EXT
 #undef TSB_REBUILD
 #undef TSB_PRUNE
+#undef TSB_PRUNE_STEP
 #undef TSB_FILE_PAIR
     // ---- write back + FP64 energy reduction (each pair seen from both ends)
     __syncthreads();  // every lane is done reading Y before forces overwrite it

@@ -31,9 +31,9 @@ import threading
 
 import torch
 
-DEFAULT_SKINS = (0.3, 0.5, 0.7, 1.0, 1.4)
+DEFAULT_SKINS = (0.5, 0.7, 1.0, 1.2, 1.4)
 DEFAULT_LANES = (4, 8, 16, 32)
-DEFAULT_PRUNE_FRACTIONS = (0.0, 0.2, 0.35, 0.5)
+DEFAULT_PRUNE_FRACTIONS = (0.0, 0.25, 0.375, 0.5)
 
 
 def cache_path() -> str:

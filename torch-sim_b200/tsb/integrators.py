@@ -844,7 +844,7 @@ def _system_order(state):
 
 
 NARROW_MAX_ATOMS = 256      # systems the 256-thread blocks of the fused kernel take
-PRUNE_FRACTION = 0.35       # default pruning skin of the fused kernel, relative to its skin
+PRUNE_FRACTION = 0.375      # default pruning skin of the fused kernel, relative to its skin
 NARROW_MAX_IMAGES = 1968    # their table of atoms + periodic images
 
 
