@@ -88,6 +88,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skin", default="auto",
                     help="Verlet skin in A, or 'auto' (project autotuner, cached per workload)")
+    ap.add_argument("--lanes", default=None,
+                    help="most threads per atom of small systems (power of two <= 32), or "
+                         "'auto'; default: 'auto' with --skin auto, else 32")
     ap.add_argument("--prune", default=None,
                     help="pruning skin of the list's shell in A (0: off), or 'auto'; default: "
                          "'auto' with --skin auto, else a fixed fraction of the skin")
@@ -467,7 +470,10 @@ def main():
                                  seed=1234 + rank,
                                  prune=(None if args.prune is None else
                                         args.prune if args.prune == "auto" else
-                                        float(args.prune)))
+                                        float(args.prune)),
+                                 lanes=(None if args.lanes is None else
+                                        args.lanes if args.lanes == "auto" else
+                                        int(args.lanes)))
     stream = torch.cuda.current_stream(device)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
 
@@ -501,11 +507,13 @@ def main():
     value = replicas.weak_scaling_value(n_atoms * args.md_steps * args.steps, t_max, ws)
     avg_launch_s = statistics.mean(per_launch_ms) / 1e3
 
-    # ---- end to end through the C ABI with host buffers (pinned), copies timed
+    # ---- end to end through the C ABI with host buffers (pinned), copies timed;
+    # every e2e step starts from the state reached after the timed launches (a
+    # hot, equilibrating trajectory like the timed ones, not the initial lattice)
     f64 = torch.float64
-    hx = md.positions.to(f64).cpu().pin_memory()
-    hp = md.momenta.to(f64).cpu().pin_memory()
-    hf = md.forces.to(f64).cpu().pin_memory()
+    hx = runner.x.cpu().pin_memory()
+    hp = runner.p.cpu().pin_memory()
+    hf = runner.f.cpu().pin_memory()
     ox = torch.empty_like(hx).pin_memory()
     op = torch.empty_like(hp).pin_memory()
     oe = torch.empty(md.n_systems, dtype=f64).pin_memory()

@@ -884,33 +884,41 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
 
     // ------------------------------------------------------------ pruning
     // Each thread reorders its own shell entries (no other thread reads them):
-    // those closer than sqrt(act2) go first, in their previous order, and are
-    // the only shell entries the force loop evaluates until the next pruning.
-    // The atom's FP32 position in the table is the one the next pruning test
-    // measures from.  Without pruning, the whole shell is evaluated.
+    // those closer than sqrt(act2) go to the front part [0, nact), which is all
+    // the force loop evaluates of the shell until the next pruning.  After a
+    // list build the whole shell is partitioned (FROM = 0).  Between builds only
+    // the entries outside the front part are examined (FROM = nact): those now
+    // within reach join it; entries of the front part that moved out stay in it
+    // (they are evaluated with the cutoff test, so results do not change) until
+    // the next build.  The atom's FP32 position in the table is the one the
+    // next pruning test measures from.  Without pruning, the whole shell is
+    // evaluated.
 #define TSB_PRUNE_STEP(I, E, ACT)                                                            \
-  if (ACT) {                                                                                 \
+  {                                                                                          \
     const int k_ = 4 * j_ + (I);                                                             \
-    if (w_ != k_) { /* the inactive entry at w_ moves to k_ */                               \
-      const int sw_ = kListLen - 1 - w_, sk_ = kListLen - 1 - k_;                            \
-      const int iw_ = (((sw_ >> 2) * kFusedThreads + tid) << 2) | (sw_ & 3);                 \
-      const int ik_ = (((sk_ >> 2) * kFusedThreads + tid) << 2) | (sk_ & 3);                 \
-      list16[ik_] = list16[iw_];                                                             \
-      list16[iw_] = (uint16_t)(E);                                                           \
+    if ((ACT) && k_ >= from_) {                                                              \
+      if (w_ != k_) { /* the entry at w_ (outside reach) moves to k_ */                      \
+        const int sw_ = kListLen - 1 - w_, sk_ = kListLen - 1 - k_;                          \
+        const int iw_ = (((sw_ >> 2) * kFusedThreads + tid) << 2) | (sw_ & 3);              \
+        const int ik_ = (((sk_ >> 2) * kFusedThreads + tid) << 2) | (sk_ & 3);              \
+        list16[ik_] = list16[iw_];                                                           \
+        list16[iw_] = (uint16_t)(E);                                                         \
+      }                                                                                      \
+      ++w_;                                                                                  \
     }                                                                                        \
-    ++w_;                                                                                    \
   }
-#define TSB_PRUNE()                                                                          \
+#define TSB_PRUNE(FROM)                                                                      \
   if (g.prune_on) {                                                                          \
     if (own) {                                                                               \
       const float4 xi_ = s_ext[a];                                                           \
       const float act2_ = g.act2;                                                            \
-      int w_ = 0;                                                                            \
+      const int from_ = (FROM);                                                              \
+      int w_ = from_;                                                                        \
       /* groups of four shell entries (shell entry 4j + i sits in slot        */             \
       /* kListLen - 1 - 4j - i), the next group's word loaded one ahead; the  */             \
       /* group's four distances first, then its entries in order             */             \
-      uint2 gn_ = s_list[(kListGroups - 1) * kFusedThreads + tid];                           \
-      for (int j_ = 0; j_ < (nshell >> 2); ++j_) {                                           \
+      uint2 gn_ = s_list[max(kListGroups - 1 - (from_ >> 2), 0) * kFusedThreads + tid];    \
+      for (int j_ = from_ >> 2; j_ < (nshell >> 2); ++j_) {                                  \
         const uint2 ge_ = gn_;                                                               \
         gn_ = s_list[max(kListGroups - 2 - j_, 0) * kFusedThreads + tid];                    \
         const uint32_t e0_ = ge_.y >> 16, e1_ = ge_.y & 0xFFFFu;                             \
@@ -1145,7 +1153,7 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
 
     TSB_REBUILD()
     if (failed) continue;
-    TSB_PRUNE()
+    TSB_PRUNE(0)
     for (int64_t step = 0; step < A.n_steps; ++step) {
       const double dt = g.dt, half = g.half, c1 = g.c1;
       // thermostat before the step: V-rescale factor from the current kinetic
@@ -1238,9 +1246,9 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
       if (fl & 1) {
         TSB_REBUILD()
         if (failed) break;
-        TSB_PRUNE()
+        TSB_PRUNE(0)
       } else if (fl & 2) {
-        TSB_PRUNE()
+        TSB_PRUNE(nact)
       }
       const bool report = A.rep_every > 0 && (step + 1) % A.rep_every == 0 &&
                           (step + 1) / A.rep_every <= A.n_frames;
