@@ -88,6 +88,8 @@ struct FusedSmem {
   static_assert(S::kMaxBins <= 4 * NT, "bin scan: four bins per thread");
   static_assert((S::kExtMax - 1) * sizeof(float4) <= 0xFFFF,
                 "list entries are 16-bit byte offsets");
+  static_assert(kList >= (size_t)S::kExtMax * (sizeof(float4) + sizeof(uint32_t)),
+                "the bin-order copy of the table fits the list area");
   static_assert(kSorted + kBins >= (size_t)NT * 3 * sizeof(double),
                 "atom positions alias the sort and bin tables");
   static_assert((kList + kExt + kGhost) % 8 == 0, "sort table 8-byte aligned");
@@ -392,19 +394,16 @@ __device__ __forceinline__ void unpack_ghost(uint32_t r, int &owner, int &sx, in
 }
 
 // Exact (FP64) squared distance between the home image of atom a and table
-// entry e (an atom, or a ghost = owner + shift @ C), from the FP64 wrapped
-// positions Y [n, 3] of the system.  Rarely called (pairs within the band).
-__device__ __noinline__ double exact_r2(const double *Y, const uint32_t *s_gshift,
-                                        const FusedGeom &g, int n, int a, int e) {
-  int j = e;
-  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-  if (e >= n) {
-    int sx, sy, sz;
-    unpack_ghost(s_gshift[e - n], j, sx, sy, sz);
-    s0 = sx * g.C[0] + sy * g.C[3] + sz * g.C[6];
-    s1 = sx * g.C[1] + sy * g.C[4] + sz * g.C[7];
-    s2 = sx * g.C[2] + sy * g.C[5] + sz * g.C[8];
-  }
+// table entry e (owner atom + lattice shift @ C, from its descriptor), from the
+// FP64 wrapped positions Y [n, 3] of the system.  Rarely called (pairs within
+// the band).
+__device__ __noinline__ double exact_r2(const double *Y, const uint32_t *s_desc,
+                                        const FusedGeom &g, int a, int e) {
+  int j, sx, sy, sz;
+  unpack_ghost(s_desc[e], j, sx, sy, sz);
+  const double s0 = sx * g.C[0] + sy * g.C[3] + sz * g.C[6];
+  const double s1 = sx * g.C[1] + sy * g.C[4] + sz * g.C[7];
+  const double s2 = sx * g.C[2] + sy * g.C[5] + sz * g.C[8];
   const double dx = (Y[3 * j] + s0) - Y[3 * a];
   const double dy = (Y[3 * j + 1] + s1) - Y[3 * a + 1];
   const double dz = (Y[3 * j + 2] + s2) - Y[3 * a + 2];
@@ -470,8 +469,8 @@ __device__ __forceinline__ float2 pair_fr2(const Prm2 &k, const PairPrm<float> &
       e.x = q.a1 * x.x * (x.x - 2.0f) - q.a4;
       e.y = q.a1 * x.y * (x.y - 2.0f) - q.a4;
     }
-    // -2 alpha D x (1 - x) / r = x (x - 1) (2 alpha D / r)
-    return __fmul2_rn(__fmul2_rn(x, __fadd2_rn(x, k.c3)), __fmul2_rn(k.c2, ir));
+    // -2 alpha D x (1 - x) / r = (x x - x) (2 alpha D / r)
+    return __fmul2_rn(__ffma2_rn(x, x, make_float2(-x.x, -x.y)), __fmul2_rn(k.c2, ir));
   } else {
     const float2 ir2 = make_float2(rcp_ftz(r2.x), rcp_ftz(r2.y));
     const float2 s2 = __fmul2_rn(k.c0, ir2);
@@ -655,6 +654,7 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
     int Wx = 0, Wy = 0, Wz = 0;        // integer wrap of the owned atom at the last build
     int ncore = 0, nshell = 0, rebuilds = 0;
     int nact = 0;                      // shell entries kept by the last pruning
+    int aslot16 = 0;                   // byte offset of the owned atom's table entry
     int n_ext = 0;                     // atoms + images in the table
     bool failed = false;
     float yb0 = 0.f, yb1 = 0.f, yb2 = 0.f;  // wrapped position at the build (FP32)
@@ -792,13 +792,35 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
         }                                                                                    \
       }                                                                                      \
       __syncthreads();                                                                       \
+      /* the table in bin order: entry p becomes generated entry s_sorted[p], its  */        \
+      /* descriptor (owner, shift) beside it (atoms: shift 0); staged in the list   */       \
+      /* area (free until the scan files entries), then copied back              */          \
+      {                                                                                      \
+        float4 *t_ext_ = (float4 *)s_list;                                                   \
+        uint32_t *t_desc_ = (uint32_t *)(t_ext_ + kExtMax);                                  \
+        for (int p = tid; p < n_ext; p += kFusedThreads) {                                   \
+          const int e = s_sorted[p] >> 4;                                                    \
+          t_ext_[p] = s_ext[e];                                                              \
+          t_desc_[p] = e < n ? pack_ghost(e, 0, 0, 0) : s_gshift[e - n];                     \
+        }                                                                                    \
+        __syncthreads();                                                                     \
+        uint16_t *aslot_ = s_sorted; /* slot of each atom's own entry */                     \
+        for (int p = tid; p < n_ext; p += kFusedThreads) {                                   \
+          const uint32_t d = t_desc_[p];                                                     \
+          s_ext[p] = t_ext_[p];                                                              \
+          s_gshift[p] = d;                                                                   \
+          if ((d & 0x7FFFu) == 0) aslot_[d >> 15] = (uint16_t)p;                             \
+        }                                                                                    \
+        __syncthreads();                                                                     \
+        aslot16 = own ? (int)aslot_[a] << 4 : 0;                                             \
+      }                                                                                      \
       ncore = 0;                                                                             \
       nshell = 0;                                                                            \
       if (own) {                                                                             \
-        const float4 xi = s_ext[a];                                                          \
+        const float4 xi = EXT(aslot16);                                                      \
         const float build2 = g.build2;                                                       \
         const float core0 = g.core2[0];                                                      \
-        const int a16 = a << 4;                                                              \
+        const int a16 = aslot16;                                                             \
         /* bins within the list radius in each fractional coordinate; per bin row */        \
         /* (cx, cy) the z range left by the row's gaps gx, gy to the atom:          */       \
         /* |d|^2 >= lambda (|a_x|^2 gx^2 + |a_y|^2 gy^2 + |a_z|^2 du_z^2)           */       \
@@ -827,10 +849,10 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
             /* four candidates per iteration (independent loads), kept in order; */          \
             /* positions past the row read the far sentinel entry instead        */          \
             for (int p_ = plo + lane; p_ < phi; p_ += 4 * tpa) {                             \
-              const int e0 = s_sorted[p_];                                                   \
-              const int e1 = p_ + tpa < phi ? s_sorted[p_ + tpa] : kSentinel << 4;           \
-              const int e2 = p_ + 2 * tpa < phi ? s_sorted[p_ + 2 * tpa] : kSentinel << 4;   \
-              const int e3 = p_ + 3 * tpa < phi ? s_sorted[p_ + 3 * tpa] : kSentinel << 4;   \
+              const int e0 = p_ << 4;                                                        \
+              const int e1 = p_ + tpa < phi ? (p_ + tpa) << 4 : kSentinel << 4;              \
+              const int e2 = p_ + 2 * tpa < phi ? (p_ + 2 * tpa) << 4 : kSentinel << 4;      \
+              const int e3 = p_ + 3 * tpa < phi ? (p_ + 3 * tpa) << 4 : kSentinel << 4;      \
               const float4 q0 = EXT(e0), q1 = EXT(e1), q2 = EXT(e2), q3 = EXT(e3);           \
               TSB_FILE_PAIR(e0, q0)                                                          \
               TSB_FILE_PAIR(e1, q1)                                                          \
@@ -910,7 +932,7 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
 #define TSB_PRUNE(FROM)                                                                      \
   if (g.prune_on) {                                                                          \
     if (own) {                                                                               \
-      const float4 xi_ = s_ext[a];                                                           \
+      const float4 xi_ = EXT(aslot16);                                                       \
       const float act2_ = g.act2;                                                            \
       const int from_ = (FROM);                                                              \
       int w_ = from_;                                                                        \
@@ -990,7 +1012,7 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
     pair_eval_fast<POT>(pq, r2, ep, fr);                                                     \
     bool in_ = r2 < pq.a3;                                                                   \
     if (fabsf(r2 - pq.a3) < band_)                                                           \
-      in_ = exact_r2(Y, s_gshift, g, n, a, (int)((E) >> 4)) <                                \
+      in_ = exact_r2(Y, s_gshift, g, a, (int)((E) >> 4)) <                                \
             (MULTI ? rc2d[sp * A.n_species + __float_as_int(q.w)] : rc2d0);                  \
     fr = in_ ? fr : 0.f;                                                                     \
     fx -= fr * rx;                                                                           \
@@ -1010,7 +1032,8 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
     const float2 dy = make_float2(xi.y - qa.y, xi.y - qb.y);                                 \
     const float2 dz = make_float2(xi.z - qa.z, xi.z - qb.z);                                 \
     float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));                  \
-    r2 = make_float2(fmaxf(r2.x, 1e-30f), fmaxf(r2.y, 1e-30f));                              \
+    /* shell entries include the far sentinel; core pairs are never at r = 0 */          \
+    if (SHELL) r2 = make_float2(fmaxf(r2.x, 1e-30f), fmaxf(r2.y, 1e-30f));                   \
     float2 e2;                                                                               \
     float2 fr = pair_fr2<POT, WITH_E>(k2, p0, r2, e2);                                       \
     if (SHELL) {                                                                             \
@@ -1018,8 +1041,8 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
       const bool near_a = fabsf(r2.x - p0.a3) < band_;                                       \
       const bool near_b = fabsf(r2.y - p0.a3) < band_;                                       \
       if (near_a || near_b) { /* rare: one branch for both pairs */                          \
-        if (near_a) ina = exact_r2(Y, s_gshift, g, n, a, (int)((EA) >> 4)) < rc2d0;          \
-        if (near_b) inb = exact_r2(Y, s_gshift, g, n, a, (int)((EB) >> 4)) < rc2d0;          \
+        if (near_a) ina = exact_r2(Y, s_gshift, g, a, (int)((EA) >> 4)) < rc2d0;          \
+        if (near_b) inb = exact_r2(Y, s_gshift, g, a, (int)((EB) >> 4)) < rc2d0;          \
       }                                                                                      \
       fr = make_float2(ina ? fr.x : 0.f, inb ? fr.y : 0.f);                                  \
       if (WITH_E) e2 = make_float2(ina ? e2.x : 0.f, inb ? e2.y : 0.f);                      \
@@ -1038,7 +1061,7 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
     float fx = 0.f, fy = 0.f, fz = 0.f;                                                      \
     double en = 0.0, vxx = 0.0, vyy = 0.0, vzz = 0.0, vyz = 0.0, vxz = 0.0, vxy = 0.0;        \
     if (own) {                                                                               \
-      const float4 xi = s_ext[a];                                                            \
+      const float4 xi = EXT(aslot16);                                                        \
       const float band_ = g.band;                                                            \
       const PairPrm<float> *row = prm + sp * A.n_species;                                    \
       (void)row;                                                                             \
@@ -1231,8 +1254,8 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
       }
       for (int e = tid; e < n_ext; e += kFusedThreads) {
         const int sp_e = __float_as_int(s_ext[e].w);
-        int owner = e, sx = 0, sy = 0, sz = 0;
-        if (e >= n) unpack_ghost(s_gshift[e - n], owner, sx, sy, sz);
+        int owner, sx, sy, sz;
+        unpack_ghost(s_gshift[e], owner, sx, sy, sz);
         s_ext[e] = image_of(g, s_posd[3 * owner], s_posd[3 * owner + 1],
                             s_posd[3 * owner + 2], sx, sy, sz, sp_e);
       }
