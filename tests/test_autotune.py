@@ -86,3 +86,24 @@ def test_cached_skin_is_returned_without_running(tmp_path):
 
     assert autotune.tune_fused_skin(md, m, integrator="nve", dt=0.2, cache=cache,
                                     timer=boom) == 0.5
+
+
+def test_cached_prune_is_returned_without_running(tmp_path):
+    """The pruning skin is cached per (skin, workload) like the skin; candidates are
+    fractions of the skin, so a cached value outside them is ignored."""
+    from tsb import autotune, models
+
+    md = _md_cpu()
+    m = models.MorseModel(sigma=2.866, epsilon=0.3429, alpha=1.3588, cutoff=6.0, device="cpu")
+    cache = autotune.TuneCache(str(tmp_path / "t.json"))
+    key = ("fused_prune|skin" + autotune._sig(1.2, 3) + "|" +
+           autotune.fused_signature(md, m, "nve", 0.2, None, "cpu"))
+    cache.put(key, {"prune": 0.3})
+
+    def boom(*_a):
+        raise AssertionError("must not time anything")
+
+    assert autotune.tune_fused_prune(md, m, skin=1.2, integrator="nve", dt=0.2, cache=cache,
+                                     timer=boom) == 0.3
+    cache.put(key, {"prune": 0.31})  # not a candidate fraction of 1.2: would be re-tuned
+    assert 0.31 not in sorted({round(f * 1.2, 6) for f in autotune.DEFAULT_PRUNE_FRACTIONS})

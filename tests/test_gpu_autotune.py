@@ -91,3 +91,30 @@ def test_lane_tuner_and_lane_invariance(tmp_path):
         out.append((r.x.cpu().numpy(), r.energy.cpu().numpy()))
     np.testing.assert_allclose(out[0][0], out[1][0], atol=1e-5)
     np.testing.assert_allclose(out[0][1], out[1][1], rtol=1e-5)
+
+
+def test_prune_tuner_times_fractions_and_caches(tmp_path):
+    """The pruning skin is timed over fractions of the skin and cached; a
+    FusedMD with skin="auto" carries a pruning skin below its skin."""
+    from tsb import autotune, integrators, workloads
+
+    md, m = _setup(16, seed=9)
+    kw = dict(integrator="nve", dt=0.002 * workloads.METAL_TIME)
+    cache = autotune.TuneCache(str(tmp_path / "t.json"))
+    calls = []
+
+    def timer(runner, n):
+        calls.append(runner.prune)
+        return autotune._time_launch(runner, n)
+
+    best = autotune.tune_fused_prune(md, m, skin=1.0, fractions=(0.0, 0.3), n_steps=30,
+                                     sample_systems=8, cache=cache, timer=timer, **kw)
+    assert best in (0.0, 0.3) and sorted(calls) == [0.0, 0.3]
+    calls.clear()
+    assert autotune.tune_fused_prune(md, m, skin=1.0, fractions=(0.0, 0.3), cache=cache,
+                                     timer=timer, **kw) == best and calls == []
+    r = integrators.FusedMD(md.clone(), m, skin=1.0, prune=best, **kw)
+    r.launch(20)
+    torch.cuda.synchronize()
+    r.check()
+    assert 0.0 <= r.prune < r.skin
