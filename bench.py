@@ -103,6 +103,9 @@ def parse():
                     help="relax workload: Verlet-list skin in A (0 = cell-list search per call)")
     ap.add_argument("--graph-steps", type=int, default=50,
                     help="relax workload: FIRE steps per CUDA-graph replay (0 = eager loop)")
+    ap.add_argument("--ref-plain-systems", type=int, default=2048,
+                    help="batched_md: systems of the reference's own torch path timed on the "
+                         "GPU (baseline/_ref; halved until it fits; 0: skip)")
     ap.add_argument("--workload", default="batched_md",
                     choices=["batched_md", "single_large", "relax", "adjoint"])
     return ap.parse_args()
@@ -224,6 +227,30 @@ def cpu_baseline(d, budget_s=20.0, processes=None, n_steps=2, seed=0):
     return {"value": a / t, "unit": UNIT, "cores": processes, "kind": "port",
             "sample": f"{take} of {n_sys} systems ({atoms} atoms) x {n_steps} BAOAB steps, "
                       f"numpy oracle (NL + Morse + BAOAB), {t:.1f} s"}
+
+
+def reference_plain_path(n_systems, systems, device="cuda:0", steps=3, timeout_s=900):
+    """The reference's own torch path (MorseModel + nvt_langevin_step, float64:
+    its float32 misses the 1e-5 force bar) timed in a child process
+    (baseline/ref_plain_gpu.py) on this GPU, or on the host cores with
+    device="cpu"; or why it could not be."""
+    import subprocess
+
+    script = os.path.join(REPO, "baseline", "ref_plain_gpu.py")
+    if not os.path.isdir(os.path.join(REPO, "baseline", "_ref", "torch_sim")):
+        return {"unavailable": "reference not installed in baseline/_ref "
+                               "(python baseline/install_ref.py)"}
+    cmd = [sys.executable, script, "--n-systems", str(n_systems), "--systems", str(systems),
+           "--steps", str(steps), "--warmup", "1", "--dtype", "float64", "--device", device]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout_s)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": f"reference path did not finish in {timeout_s} s"}
+    lines = [x for x in r.stdout.splitlines() if x.startswith("{")]
+    if r.returncode != 0 or not lines:
+        tail = (r.stderr or r.stdout).strip().splitlines()[-1:] or ["no output"]
+        return {"unavailable": f"reference path failed (rc {r.returncode}): {tail[0][:200]}"}
+    return json.loads(lines[-1])
 
 
 def run_reference(args):
@@ -655,8 +682,27 @@ def main():
             "clocks": clocks.summary(),
             "per_launch_ms": per_launch_ms,
         }
+        if args.ref_plain_systems > 0 and ws == 1 and args.integrator == "nvt_langevin":
+            # the metric's plain GPU path as the reference itself runs it
+            ref = reference_plain_path(args.n_systems, args.ref_plain_systems,
+                                       f"cuda:{device.index or 0}")
+            if "value" in ref:
+                ref["fused_over_reference_plain"] = value / ref["value"]
+            line["plain_path_reference"] = ref
         if not args.no_cpu_baseline and ws == 1:
             line["cpu_baseline"] = cpu_baseline(d)
+            if args.integrator == "nvt_langevin":
+                # the reference's own torch path on the host cores (a random
+                # sample of the systems; reported baseline only)
+                cref = reference_plain_path(args.n_systems, 64, "cpu", steps=2)
+                if "value" in cref:
+                    cref = {"value": cref["value"], "unit": UNIT, "cores": cref["threads"],
+                            "kind": "reference",
+                            "sample": f"{cref['systems']} of {cref['of_systems']} systems "
+                                      f"({cref['atoms']} atoms) x {cref['md_steps']} steps, "
+                                      "float64, torch threads = host cores",
+                            "what": cref["what"]}
+                line["cpu_reference"] = cref
         print(json.dumps(line), flush=True)
     if ws > 1:
         torch.distributed.destroy_process_group()

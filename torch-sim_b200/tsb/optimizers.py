@@ -88,8 +88,11 @@ def fire_init(state, model, *, dt_start=0.1, alpha_start=0.1, fire_flavor=ASE,
         cfac = counts
     else:
         cfac = torch.as_tensor(cell_factor, dtype=dt_, device=dev).expand(n_sys).contiguous()
-    masses = torch.zeros(n_sys, dtype=dt_, device=dev).index_add_(0, state.system_idx,
-                                                                   state.masses)
+    # cell masses (cell_filters.py:97-101): summed on the host, in atom order, so
+    # that repeated runs get bitwise equal values (a GPU index_add_ sums in a
+    # run-dependent order)
+    masses = torch.zeros(n_sys, dtype=dt_).index_add_(
+        0, state.system_idx.cpu(), state.masses.to(dt_).cpu()).to(dev)
     st = CellFireState.from_state(
         state, **common, reference_cell=state.cell.clone().contiguous(), cell_filter="frechet",
         cell_factor=cfac.contiguous(),
