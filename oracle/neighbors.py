@@ -147,6 +147,23 @@ def sort_pairs(mapping, system_mapping, shifts):
     return mapping[:, order], system_mapping[order], shifts[order]
 
 
+def pair_set_digest(mapping, shifts):
+    """SHA-256 of a pair set (one system) independent of its order: each pair
+    (i, j, sx, sy, sz) packed into one int64 key (i, j < 2^19, |s| <= 3),
+    keys sorted ascending, little-endian bytes hashed.  Test infrastructure for
+    comparing pair sets too large to store (tens of millions of pairs)."""
+    import hashlib
+
+    m = np.asarray(mapping, dtype=np.int64)
+    si = np.rint(np.asarray(shifts, dtype=np.float64)).astype(np.int64)
+    if m.size and (m.min() < 0 or m.max() >= 1 << 19 or np.abs(si).max() > 3):
+        raise ValueError("pair_set_digest: index or shift outside the packed range")
+    key = (((m[0] << 19) | m[1]) << 9) | ((si[:, 0] + 4) << 6) | ((si[:, 1] + 4) << 3) | (
+        si[:, 2] + 4)
+    key = np.sort(key).astype("<i8")
+    return hashlib.sha256(key.tobytes()).hexdigest(), int(key.size)
+
+
 def full_to_half_list(mapping, system_mapping, shifts):
     """Keep i<j, and for i==j the copy whose first non-zero shift is > 0.
 

@@ -1,5 +1,7 @@
 """GPU neighbour list vs the reference's pair sets (bit-exact) and the oracle."""
 
+import os
+
 import numpy as np
 import pytest
 import torch
@@ -7,6 +9,7 @@ import torch
 from oracle import neighbors as onl
 
 pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 NL_CASES = ["ar_fcc444", "cu_tri_batch", "slab_pbc_TTF", "cluster_nopbc",
             "tiny_self_images", "rhombohedral_unwrapped"]
@@ -148,3 +151,32 @@ def test_nl_32k_atom_pair_set_is_exact(rc):
     assert got[0].shape == ref[0].shape, (got[0].shape, ref[0].shape)
     assert np.array_equal(got[0], ref[0])
     assert np.array_equal(np.rint(got[2]).astype(np.int64), np.rint(ref[2]).astype(np.int64))
+
+
+@pytest.mark.parametrize("rc", [8.5, 9.5])
+def test_nl_500k_atom_pair_set_matches_reference_digest(rc):
+    """Config 2 at full size (argon fcc 50x50x50, 500,000 atoms, N(0, 0.1 A)):
+    the full pair set at the cutoff and at cutoff + skin hashes to the digest of
+    the reference's own torch_nl_linked_cell on the same input
+    (tests/golden/nl500k.json, made by make_nl500k.py; torch_nl.py:156-215).
+    Pairs are packed into int64 keys and sorted on the GPU, then hashed."""
+    import hashlib
+    import json
+
+    from tsb import neighbors, workloads
+
+    with open(os.path.join(GOLDEN, "nl500k.json")) as f:
+        want = json.load(f)["cutoffs"][str(rc)]
+    d = workloads.argon_fcc((50, 50, 50), jitter=0.1, seed=0)
+    dev = torch.device("cuda")
+    pos = torch.as_tensor(d["positions"], dtype=torch.float64, device=dev)
+    cell_row = torch.as_tensor(d["cell"][0].T.copy(), dtype=torch.float64, device=dev)
+    m, _, sh = neighbors.torchsim_nl(pos, cell_row, torch.ones(3, dtype=torch.bool, device=dev),
+                                     rc, torch.zeros(len(pos), dtype=torch.int64, device=dev))
+    assert m.shape[1] == want["n_pairs"]
+    si = torch.round(sh).to(torch.int64)
+    assert int(m.min()) >= 0 and int(m.max()) < (1 << 19) and int(si.abs().max()) <= 3
+    key = (((m[0] << 19) | m[1]) << 9) | ((si[:, 0] + 4) << 6) | ((si[:, 1] + 4) << 3) | (
+        si[:, 2] + 4)
+    key = torch.sort(key).values.cpu().numpy().astype("<i8")
+    assert hashlib.sha256(key.tobytes()).hexdigest() == want["sha256"]
