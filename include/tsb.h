@@ -555,7 +555,7 @@ int tsb_fused_md_nvt(int thermostat, int potential, const double *table, int n_s
  * systems over two block shapes: order[0 .. n_wide) run in 512-thread blocks,
  * one per SM, and order[n_wide .. S) in 256-thread blocks, two per SM -- those
  * systems must have at most 256 atoms and fit the narrow blocks' image table of
- * 1968 entries at the given skin (else the skin is halved for them, or
+ * 1968 entries at the given skin (else their skin shrinks until it fits, or
  * TSB_ERR_CAPACITY is reported); n_wide < 0 runs every system in 512-thread
  * blocks.  prune_skin (0 <= prune_skin; 0 or >= skin: off) prunes the list
  * between builds: only the pairs of the list's shell that lie within

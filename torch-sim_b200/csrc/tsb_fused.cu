@@ -665,7 +665,8 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
     // cutoff+skin margin of the cell; bin all entries (counting sort, index
     // order inside a bin); every atom scans the 5x5x5 bins around its own and
     // files each neighbour as core or shell.  If the shared-memory tables
-    // overflow, the skin of this system is halved.
+    // overflow, the skin of this system shrinks by 10 % and the build is
+    // retried (for the rest of the launch it keeps the skin that fits).
     //
     // list entries and the bin-sorted entry order hold byte offsets (entry * 16)
     // into the image table
@@ -898,7 +899,7 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
       break;                                                                                 \
     }                                                                                        \
     if (tid == 0) {                                                                          \
-      g.skin = g.skin > 0.05 ? 0.5 * g.skin : 0.0;                                           \
+      g.skin = g.skin > 0.05 ? 0.9 * g.skin : 0.0;                                           \
       set_margins<kMaxBins>(g, A.cutoff, A.prune, rc2d, nsp2);                                                  \
     }                                                                                        \
     __syncthreads();                                                                         \
