@@ -402,9 +402,12 @@ def run_relax(args):
                        "fire_steps": steps, "converged": int(conv.sum()),
                        "graph_steps_per_replay": args.graph_steps,
                        "time_to_all_converged_s": t, "fmax": 1e-3,
-                       "neighbour_lists": (f"Verlet, skin {args.list_skin} A, "
-                                           f"{m.n_builds} builds" if args.list_skin > 0
-                                           else "cell-list search per call")},
+                       "neighbour_lists": (
+                           f"Verlet, skin {args.list_skin} A, expired systems rebuilt "
+                           + ("on the device inside the graph (not counted on the host)"
+                              if args.graph_steps > 0
+                              else f"by host decision ({m.n_builds} builds)")
+                           if args.list_skin > 0 else "cell-list search per call")},
             "force_err_vs_fp64": {"max_abs_eV_per_A": err, "over_fmax": err / 1e-3},
             "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
