@@ -62,11 +62,16 @@ def installed() -> bool:
 
 
 def install(ref_root: str = "/root/reference", verbose: bool = False) -> bool:
-    """Install the reference into baseline/_ref; True if it is there afterwards."""
+    """Install the reference into baseline/_ref; True if it is there afterwards.
+    An existing install is kept only while it matches the source tree."""
+    src_pkg = os.path.join(ref_root, "torch_sim")
+    if not os.path.isdir(src_pkg):
+        return installed()
     if installed():
-        return True
-    if not os.path.isdir(os.path.join(ref_root, "torch_sim")):
-        return False
+        dst_pkg = os.path.join(TARGET, "torch_sim")
+        if _same_tree(src_pkg, dst_pkg) and _same_tree(dst_pkg, src_pkg):
+            return True
+        shutil.rmtree(TARGET)
     with tempfile.TemporaryDirectory(prefix="tsref_src_") as tmp:
         src = os.path.join(tmp, "torch-sim")
         os.makedirs(src)
