@@ -101,6 +101,9 @@ def parse():
                     help="batched_md: integrator inside the fused kernel and the plain path")
     ap.add_argument("--list-skin", type=float, default=1.5,
                     help="relax workload: Verlet-list skin in A (0 = cell-list search per call)")
+    ap.add_argument("--list-prune", type=float, default=None,
+                    help="relax workload: pruning skin of the Verlet lists in A (default "
+                         "0: off)")
     ap.add_argument("--graph-steps", type=int, default=50,
                     help="relax workload: FIRE steps per CUDA-graph replay (0 = eager loop)")
     ap.add_argument("--ref-plain-systems", type=int, default=2048,
@@ -377,7 +380,7 @@ def run_relax(args):
     st = state_from_arrays(d, device=dev)
     m = models.kob_andersen_model(compute_stress=True, device=dev)
     if args.list_skin > 0:
-        m = models.VerletListModel(m, skin=args.list_skin)
+        m = models.VerletListModel(m, skin=args.list_skin, prune=args.list_prune)
     st = optimizers.fire_init(st, m, cell_filter="frechet")
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -403,7 +406,8 @@ def run_relax(args):
                        "graph_steps_per_replay": args.graph_steps,
                        "time_to_all_converged_s": t, "fmax": 1e-3,
                        "neighbour_lists": (
-                           f"Verlet, skin {args.list_skin} A, expired systems rebuilt "
+                           f"Verlet, skin {args.list_skin} A, pruned to cutoff + "
+                           f"{getattr(m, 'prune', 0.0):.3g} A, expired systems rebuilt "
                            + ("on the device inside the graph (not counted on the host)"
                               if args.graph_steps > 0
                               else f"by host decision ({m.n_builds} builds)")

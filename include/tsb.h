@@ -286,6 +286,10 @@ int tsb_npt_crescale_tri(void *positions, void *momenta, const void *masses,
  * The workspace (tsb_vlist_workspace_size) holds the list frame and must be kept
  * by the caller between calls; tsb_vlist_reset marks every system unbuilt.
  * tsb_vlist_check: flags[0] = 1 when any active system must be rebuilt.
+ *   prune_skin (0 <= prune_skin; 0 or >= skin: off) also marks the systems whose
+ *   pruned lists must be formed again: 2 max|u'| + (cutoff + prune_skin)
+ *   |F' - I| > prune_skin, with F' and u' measured since the system's last
+ *   pruning (and every system rebuilt since it).
  * tsb_vlist_build: rebins and rebuilds the expired systems' lists
  *   (list[k * N + slot] = slot of j << 5 | image code, counts [N] by slot).
  *   max_system_atoms = the largest system's atom count (0: unknown); when it is
@@ -296,14 +300,19 @@ int tsb_npt_crescale_tri(void *positions, void *momenta, const void *masses,
  *   build again), else 0.
  * tsb_vlist_forces: energy [S], forces [N,3], stress [S,3,3], per-atom energies
  *   [N] and stresses [N,3,3] per out_flags (TSB_MATH_FP64: FP64 pair function),
- *   for the systems with sys_active != 0 (NULL: all).  LJ, Morse, soft sphere. */
+ *   for the systems with sys_active != 0 (NULL: all).  LJ, Morse, soft sphere.
+ *   prune_skin > 0 (the value given to the preceding tsb_vlist_check, which must
+ *   run before every call): the marked systems' lists are first reordered in
+ *   place so that the entries within their pair cutoff + prune_skin form a front
+ *   part, and only front parts are evaluated.  The pairs are those of the whole
+ *   lists; results equal theirs to FP64 rounding (another summation order). */
 size_t tsb_vlist_workspace_size(int64_t n_atoms, int64_t n_systems);
 int tsb_vlist_reset(int64_t n_atoms, int64_t n_systems, void *workspace,
                     size_t workspace_bytes, void *stream);
 int tsb_vlist_check(const void *positions, const void *cell_row, const int64_t *system_idx,
                     const uint8_t *sys_active, int64_t n_atoms, int64_t n_systems, int dtype,
-                    double cutoff, double skin, int32_t *flags, void *workspace,
-                    size_t workspace_bytes, void *stream);
+                    double cutoff, double skin, double prune_skin, int32_t *flags,
+                    void *workspace, size_t workspace_bytes, void *stream);
 int tsb_vlist_build(const void *positions, const void *cell_row, const uint8_t *pbc,
                     const int64_t *system_idx, const int32_t *species, int64_t n_atoms,
                     int64_t n_systems, int dtype, double cutoff, double skin, uint32_t *list,
@@ -321,11 +330,12 @@ int tsb_vlist_lj_hvp(const double *table, int n_species, const int32_t *species,
                      double *lam_q, double *grad_params, void *scratch, size_t scratch_bytes,
                      void *workspace, size_t workspace_bytes, void *stream);
 int tsb_vlist_forces(int potential, const double *table, int n_species, const int32_t *species,
-                     const uint32_t *list, const int32_t *counts, const void *positions,
+                     uint32_t *list, const int32_t *counts, const void *positions,
                      const void *cell_row, const int64_t *system_idx, const uint8_t *sys_active,
                      int64_t n_atoms, int64_t n_systems, int dtype, double cutoff,
-                     int out_flags, void *energy, void *forces, void *stress, void *energies,
-                     void *stresses, void *workspace, size_t workspace_bytes, void *stream);
+                     double prune_skin, int out_flags, void *energy, void *forces, void *stress,
+                     void *energies, void *stresses, void *workspace, size_t workspace_bytes,
+                     void *stream);
 
 /* ---- adjoint of NVE trajectories (species-matrix LJ, FP64) ---------------
  * No kernel of the reference corresponds: it differentiates trajectories with

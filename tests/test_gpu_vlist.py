@@ -292,3 +292,45 @@ def test_vlist_understated_max_system_atoms_still_exact():
     vm._ensure(st, st.positions, st.cell.mT.contiguous())
     vm.max_system_atoms = 200
     _cmp(vm(st), ref(st), 1e-10)
+
+
+@pytest.mark.parametrize("n_systems,n_max,precision",
+                         [(12, 400, "fp64"), (12, 400, "mixed"), (200, 1000, "fp64"),
+                          (200, 1000, "mixed")])
+def test_vlist_pruned_front_parts_equal_whole_lists(n_systems, n_max, precision):
+    """Pruned lists (each atom evaluates only the entries within its pair cutoff
+    + prune at the system's last pruning) give the results of the whole lists
+    through moves and strains that trigger re-prunings and rebuilds, to FP64
+    rounding (a re-pruned list sums its entries in another order), with several
+    lanes per list (12 systems) and one thread per list (200 systems, above
+    65,536 atoms); in FP64 also the per-call search's results."""
+    tol = 1e-12
+    from tsb import models
+
+    dtype = torch.float64
+    st = _ka(n_systems=n_systems, n_max=n_max, seed=7, dtype=dtype)
+    mk = lambda: models.kob_andersen_model(compute_stress=True, precision=precision,  # noqa
+                                           dtype=dtype)
+    pruned = models.VerletListModel(mk(), skin=1.0, prune=0.4)
+    whole = models.VerletListModel(mk(), skin=1.0, prune=0.0)
+    ref = mk()
+    g = torch.Generator(device="cuda").manual_seed(11)
+    eye = torch.eye(3, dtype=dtype, device="cuda")
+    for step in range(14):
+        if step:
+            eps = 6e-4 * torch.randn((st.n_systems, 3, 3), device="cuda", dtype=dtype,
+                                     generator=g)
+            F = eye + 0.5 * (eps + eps.mT)
+            st.positions = torch.einsum("nij,nj->ni", F[st.system_idx], st.positions) + \
+                0.04 * torch.randn(st.positions.shape, device="cuda", dtype=dtype,
+                                   generator=g)
+            st.cell = torch.einsum("nij,njk->nik", F, st.cell).contiguous()
+        a, b = pruned(st), whole(st)
+        for k in ("energy", "forces", "stress"):
+            x, y = a[k].cpu().numpy(), b[k].cpu().numpy()
+            assert np.abs(x - y).max() <= tol * np.abs(y).max(), (step, k)
+        # the per-call search's pairs (FP64 sums to 1e-10; in FP32 the two paths
+        # form displacements differently, which on these overlapping random boxes
+        # moves energies by ~1e-4, so there the whole lists are the reference)
+        if precision == "fp64":
+            _cmp(a, ref(st), 1e-10)

@@ -37,6 +37,18 @@
 // positions, so the pair set is the FP64 one.  B = sum of the cell rows' norms +
 // skin/2 for a fully periodic system (frame positions stay within the cell plus
 // the allowed drift); systems with an open axis always take the FP64 test.
+//
+// Pruning (prune_skin p, 0 < p < skin).  Each slot's list is partitioned in
+// place: the entries within r_c(ab) + p of the slot at the pruning (FP64 test)
+// form a front part, in their list order, and the force kernel evaluates only
+// that part.  The same bound with p for the skin and the pruning's cell and
+// positions for the build's keeps a pair left out of the front part outside its
+// cutoff: a system is pruned again, before the next force evaluation, when
+// 2 max|u'| + (cutoff + p) e' > p (u', e' the drift and deformation since the
+// pruning), and after every rebuild.  The pairs inside the cutoff are those of
+// the whole list; the order in which they are summed changes (the partition
+// keeps the front part's order, but a re-pruning partitions the list as the
+// last one left it), so results equal the whole list's to FP64 rounding.
 #include "tsb_ljhvp.cuh"
 #include "tsb_pair.cuh"
 #include "tsb_search.cuh"
@@ -72,6 +84,13 @@ struct VlWork {
   double *vir_half;    // [6N]
   double *part;        // [7 S chunks]
   int chunks;
+  // pruning (see the top of this file)
+  double *pinv;        // [9S] inverse of the cell at the last pruning (rows), or identity
+  double *pfdef;       // [9S] F' = pinv C of this call
+  double *pdmax;       // [S] allowed drift since the pruning for this call
+  int32_t *pexp;       // [S] prune this system before the next force evaluation
+  double4 *pref;       // [N] frame position of each atom at the last pruning
+  int32_t *pcnt;       // [N] entries in the front part of each slot's list
 };
 
 static void carve_vl(Carver &c, VlWork &w, int64_t n, int64_t ns) {
@@ -98,26 +117,57 @@ static void carve_vl(Carver &c, VlWork &w, int64_t n, int64_t ns) {
   w.vir_half = c.take<double>(6 * n);
   w.chunks = reduce_chunks(n, ns);
   w.part = w.chunks > 1 ? c.take<double>(7 * ns * w.chunks) : nullptr;
+  w.pinv = c.take<double>(9 * ns);
+  w.pfdef = c.take<double>(9 * ns);
+  w.pdmax = c.take<double>(ns);
+  w.pexp = c.take<int32_t>(ns);
+  w.pref = c.take<double4>(n);
+  w.pcnt = c.take<int32_t>(n);
 }
 
 // per system: deformation F = C0^-1 C since the build -> allowed drift (or expiry)
+// (and, with pruning, F' = C_p^-1 C since the pruning -> allowed drift, or a
+// pending pruning; a pending pruning is cleared only by the pruning itself)
 template <class P>
 __global__ void k_vl_sys_check(const P *cell_row, const uint8_t *active, int64_t ns,
                                double cutoff, double skin, const double *rinv,
                                const int32_t *rframe, const int32_t *built, double *fdef,
-                               double *dmax, int32_t *sys_exp, int32_t *flags) {
+                               double *dmax, int32_t *sys_exp, int32_t *flags, double prune,
+                               const double *pinv, double *pfdef, double *pdmax,
+                               int32_t *pexp) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= ns) return;
   if (active && !active[s]) {
     dmax[s] = INFINITY;
     sys_exp[s] = 0;
+    pdmax[s] = INFINITY;
     return;
   }
   if (!built[s]) {
     dmax[s] = -1.0;
     sys_exp[s] = 1;
     flags[0] = 1;
+    pdmax[s] = -1.0;
     return;
+  }
+  if (prune > 0.0) {
+    double ep2 = 0.0;
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) {
+        double f = r == c ? 1.0 : 0.0;
+        if (rframe[s]) {
+          f = 0.0;
+          for (int k = 0; k < 3; ++k)
+            f += pinv[9 * s + 3 * r + k] * (double)cell_row[9 * s + 3 * k + c];
+        }
+        pfdef[9 * s + 3 * r + c] = f;
+        const double d = f - (r == c ? 1.0 : 0.0);
+        ep2 += d * d;
+      }
+    const double ep = sqrt(ep2);
+    const double pd = ep < 1.0 ? 0.5 * (prune - (cutoff + prune) * ep) : -1.0;
+    pdmax[s] = pd;
+    if (!(pd >= 0.0)) pexp[s] = 1;
   }
   double F[9];
   double e2 = 0.0;
@@ -141,11 +191,13 @@ __global__ void k_vl_sys_check(const P *cell_row, const uint8_t *active, int64_t
 }
 
 // per atom: non-affine drift u_i = w_i - w0_i F against the system's allowance
+// (and, with pruning, u'_i = w_i - w_p,i F' against the pruning's allowance)
 template <class P>
 __global__ void k_vl_atom_check(const P *pos, const P *cell_row, const int64_t *sys,
                                 int64_t n, const int32_t *rwrap, const double4 *ref,
                                 const double *fdef, const double *dmax, int32_t *sys_exp,
-                                int32_t *flags) {
+                                int32_t *flags, double prune, const double4 *pref,
+                                const double *pfdef, const double *pdmax, int32_t *pexp) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int64_t s = sys[i];
@@ -155,16 +207,29 @@ __global__ void k_vl_atom_check(const P *pos, const P *cell_row, const int64_t *
   const double *F = fdef + 9 * s;
   const int W0 = rwrap[3 * i], W1 = rwrap[3 * i + 1], W2 = rwrap[3 * i + 2];
   const double4 r = ref[i];
+  double w[3];
   double d2 = 0.0;
   for (int m = 0; m < 3; ++m) {
-    const double w = (double)pos[3 * i + m] -
-                     (W0 * (double)C[m] + W1 * (double)C[3 + m] + W2 * (double)C[6 + m]);
-    const double d = w - (r.x * F[m] + r.y * F[3 + m] + r.z * F[6 + m]);
+    w[m] = (double)pos[3 * i + m] -
+           (W0 * (double)C[m] + W1 * (double)C[3 + m] + W2 * (double)C[6 + m]);
+    const double d = w[m] - (r.x * F[m] + r.y * F[3 + m] + r.z * F[6 + m]);
     d2 += d * d;
   }
   if (d2 > dm * dm) {
     sys_exp[s] = 1;
     flags[0] = 1;
+  }
+  if (prune > 0.0) {
+    const double pd = pdmax[s];
+    if (!(pd >= 0.0) || isinf(pd)) return;  // pending already, or inactive
+    const double *G = pfdef + 9 * s;
+    const double4 q = pref[i];
+    double e2 = 0.0;
+    for (int m = 0; m < 3; ++m) {
+      const double d = w[m] - (q.x * G[m] + q.y * G[3 + m] + q.z * G[6 + m]);
+      e2 += d * d;
+    }
+    if (e2 > pd * pd) pexp[s] = 1;
   }
 }
 
@@ -304,7 +369,8 @@ __global__ void __launch_bounds__(256, 4)
 
 // per rebuilt system: record C0^-1 (the transpose of the frame matrix T)
 __global__ void k_vl_sys_built(const SysGeom *g, int64_t ns, int32_t *sys_exp, int32_t *built,
-                               double skin, double *rinv, int32_t *rframe, double *rslack) {
+                               double skin, double *rinv, int32_t *rframe, double *rslack,
+                               int32_t *pexp) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= ns || !sys_exp[s]) return;
   const SysGeom &G = g[s];
@@ -314,6 +380,7 @@ __global__ void k_vl_sys_built(const SysGeom *g, int64_t ns, int32_t *sys_exp, i
   rslack[s] = G.active && G.per[0] && G.per[1] && G.per[2] ? 0.5 * skin : -1.0;
   built[s] = 1;
   sys_exp[s] = 0;
+  pexp[s] = 1;  // a new list: its front part is formed before the next forces
 }
 
 // per system for the force call: shift vectors (one thread per system and image
@@ -370,6 +437,80 @@ __global__ void k_vl_frame(const P *pos, const P *cell_row, const int64_t *sys,
   const unsigned long long hi = species ? (unsigned long long)(uint32_t)species[i] : 0ull;
   wpos[p] = make_double4(w[0], w[1], w[2], __longlong_as_double((long long)(hi << 32)));
   wpos32[p] = make_float4((float)w[0], (float)w[1], (float)w[2], __int_as_float((int)hi));
+}
+
+// Pruning of the systems marked in pexp: each slot's list is partitioned in
+// place (stable for the front part) into the entries within r_c(ab) + prune of
+// the slot's current frame position and the rest; the front count and the
+// atom's position at the pruning are recorded.  FP64 distances.
+__global__ void k_vl_prune(const double4 *__restrict__ wpos, uint32_t *list,
+                           const int32_t *__restrict__ cnt, int64_t n,
+                           const int32_t *__restrict__ perm, const int64_t *__restrict__ sys,
+                           const double *__restrict__ sv, const double *__restrict__ table,
+                           int pot, int nsp, double cutoff, double prune,
+                           const int32_t *__restrict__ pexp, const uint8_t *active,
+                           int32_t *pcnt, double4 *pref) {
+  __shared__ double reach2[kMaxSpecies * kMaxSpecies];
+  for (int k = threadIdx.x; k < nsp * nsp; k += blockDim.x) {
+    const double r = sqrt(pair_rc2(pot, table + 5 * k, cutoff)) + prune;
+    reach2[k] = r * r * (1.0 + 1e-10);
+  }
+  __syncthreads();
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int64_t i = perm[p];
+  const int64_t s = sys[i];
+  if (!pexp[s] || (active && !active[s])) return;
+  const double4 wi = wpos[p];
+  const int si = min(max(tag_species(wi.w), 0), nsp - 1);
+  const double *svs = sv + 81 * s;
+  const int c = cnt[p];
+  int front = 0;
+  for (int k = 0; k < c; ++k) {
+    const uint32_t e = list[(size_t)k * n + p];
+    const double4 wj = wpos[e >> 5];
+    const int code = (int)(e & 31u);
+    const double dx = wj.x - wi.x + svs[3 * code];
+    const double dy = wj.y - wi.y + svs[3 * code + 1];
+    const double dz = wj.z - wi.z + svs[3 * code + 2];
+    const int sj = min(max(tag_species(wj.w), 0), nsp - 1);
+    if (dx * dx + dy * dy + dz * dz < reach2[si * nsp + sj]) {
+      if (front != k) {
+        list[(size_t)k * n + p] = list[(size_t)front * n + p];
+        list[(size_t)front * n + p] = e;
+      }
+      ++front;
+    }
+  }
+  pcnt[p] = front;
+  pref[i] = make_double4(wi.x, wi.y, wi.z, 0.0);
+}
+
+// per pruned system: the cell's inverse at the pruning, and the mark cleared
+template <class P>
+__global__ void k_vl_sys_pruned(const P *cell_row, int64_t ns, const int32_t *rframe,
+                                const uint8_t *active, double *pinv, int32_t *pexp) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns || !pexp[s] || (active && !active[s])) return;
+  double C[9];
+  for (int k = 0; k < 9; ++k) C[k] = (double)cell_row[9 * s + k];
+  double inv[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  if (rframe[s]) {
+    const double d = C[0] * (C[4] * C[8] - C[5] * C[7]) - C[1] * (C[3] * C[8] - C[5] * C[6]) +
+                     C[2] * (C[3] * C[7] - C[4] * C[6]);
+    const double id = 1.0 / d;
+    inv[0] = (C[4] * C[8] - C[5] * C[7]) * id;
+    inv[1] = (C[2] * C[7] - C[1] * C[8]) * id;
+    inv[2] = (C[1] * C[5] - C[2] * C[4]) * id;
+    inv[3] = (C[5] * C[6] - C[3] * C[8]) * id;
+    inv[4] = (C[0] * C[8] - C[2] * C[6]) * id;
+    inv[5] = (C[2] * C[3] - C[0] * C[5]) * id;
+    inv[6] = (C[3] * C[7] - C[4] * C[6]) * id;
+    inv[7] = (C[1] * C[6] - C[0] * C[7]) * id;
+    inv[8] = (C[0] * C[4] - C[1] * C[3]) * id;
+  }
+  for (int k = 0; k < 9; ++k) pinv[9 * s + k] = inv[k];
+  pexp[s] = 0;
 }
 
 __device__ __forceinline__ int vl_species(double w) { return tag_species(w); }
@@ -592,14 +733,16 @@ __global__ void __launch_bounds__(kVlBlock)
 
 template <class P>
 static int vl_check(const P *pos, const P *cell, const int64_t *sys, const uint8_t *active,
-                    int64_t n, int64_t ns, double cutoff, double skin, int32_t *flags,
-                    VlWork &w, cudaStream_t st) {
+                    int64_t n, int64_t ns, double cutoff, double skin, double prune,
+                    int32_t *flags, VlWork &w, cudaStream_t st) {
   cudaMemsetAsync(flags, 0, 2 * sizeof(int32_t), st);
   k_vl_sys_check<P><<<grid_for(ns), kBlock, 0, st>>>(cell, active, ns, cutoff, skin, w.rinv,
                                                      w.rframe, w.sys_built, w.fdef, w.dmax,
-                                                     w.sys_exp, flags);
+                                                     w.sys_exp, flags, prune, w.pinv, w.pfdef,
+                                                     w.pdmax, w.pexp);
   k_vl_atom_check<P><<<grid_for(n), kBlock, 0, st>>>(pos, cell, sys, n, w.rwrap, w.ref, w.fdef,
-                                                     w.dmax, w.sys_exp, flags);
+                                                     w.dmax, w.sys_exp, flags, prune, w.pref,
+                                                     w.pfdef, w.pdmax, w.pexp);
   TSB_CHECK_LAUNCH();
   return TSB_OK;
 }
@@ -626,7 +769,7 @@ static int vl_build(const P *pos, const P *cell, const uint8_t *pbc, const int64
   k_vl_build<<<(unsigned)(n_sm * 8), 256, 0, st>>>(w.b, n, ns, rcs * rcs, w.eoff, list, counts,
                                                     max_nb, flags, w.perm, w.ref, w.rwrap);
   k_vl_sys_built<<<grid_for(ns), kBlock, 0, st>>>(w.b.geom, ns, w.sys_exp, w.sys_built, skin,
-                                                  w.rinv, w.rframe, w.rslack);
+                                                  w.rinv, w.rframe, w.rslack, w.pexp);
   TSB_CHECK_LAUNCH();
   return TSB_OK;
 }
@@ -649,15 +792,25 @@ static void vl_launch(VlWork &w, const uint32_t *list, const int32_t *counts, in
 
 template <class P>
 static int vl_forces(int pot, const double *table, int nsp, const int32_t *species,
-                     const uint32_t *list, const int32_t *counts, const P *pos, const P *cell,
+                     uint32_t *list, const int32_t *counts, const P *pos, const P *cell,
                      const int64_t *sys, const uint8_t *active, int64_t n, int64_t ns,
-                     double cutoff, int flags, P *energy, P *forces, P *stress, P *energies,
-                     P *stresses, VlWork &w, cudaStream_t st) {
+                     double cutoff, double prune, int flags, P *energy, P *forces, P *stress,
+                     P *energies, P *stresses, VlWork &w, cudaStream_t st) {
   k_vl_sys_geom<P><<<grid_for(27 * ns), kBlock, 0, st>>>(cell, ns, w.b.sys_lo, w.b.sys_hi,
                                                          w.rslack, cutoff, w.sv, w.svf, w.band,
                                                          w.cur);
   k_vl_frame<P><<<grid_for(n), kBlock, 0, st>>>(pos, cell, sys, species, n, w.perm, w.rwrap,
                                                 w.wpos, w.wpos32);
+  if (prune > 0.0) {
+    // systems marked by the check or rebuilt since their last pruning form their
+    // front parts; the force kernel then reads the front counts
+    k_vl_prune<<<grid_for(n), kBlock, 0, st>>>(w.wpos, list, counts, n, w.perm, sys, w.sv,
+                                               table, pot, nsp, cutoff, prune, w.pexp, active,
+                                               w.pcnt, w.pref);
+    k_vl_sys_pruned<P><<<grid_for(ns), kBlock, 0, st>>>(cell, ns, w.rframe, active, w.pinv,
+                                                        w.pexp);
+    counts = w.pcnt;
+  }
   const bool f64 = flags & TSB_MATH_FP64;
 #define TSB_VLL(POT)                                                                        \
   if (f64)                                                                                  \
@@ -835,6 +988,7 @@ extern "C" int tsb_vlist_reset(int64_t n_atoms, int64_t n_systems, void *workspa
   cudaMemsetAsync(w.sys_built, 0, sizeof(int32_t) * n_systems, st);
   cudaMemsetAsync(w.sys_exp, 0, sizeof(int32_t) * n_systems, st);
   cudaMemsetAsync(w.rslack, 0xff, sizeof(double) * n_systems, st);  // NaN: FP64 test
+  cudaMemsetAsync(w.pexp, 0xff, sizeof(int32_t) * n_systems, st);    // nonzero: prune
   k_vl_iota<<<grid_for(n_atoms), kBlock, 0, st>>>(w.perm, n_atoms);
   TSB_CHECK_LAUNCH();
   return TSB_OK;
@@ -843,11 +997,12 @@ extern "C" int tsb_vlist_reset(int64_t n_atoms, int64_t n_systems, void *workspa
 extern "C" int tsb_vlist_check(const void *positions, const void *cell_row,
                                const int64_t *system_idx, const uint8_t *sys_active,
                                int64_t n_atoms, int64_t n_systems, int dtype, double cutoff,
-                               double skin, int32_t *flags, void *workspace,
+                               double skin, double prune_skin, int32_t *flags, void *workspace,
                                size_t workspace_bytes, void *stream) {
   if (n_atoms < 1 || n_systems < 1 || !positions || !cell_row || !system_idx || !flags ||
-      !(cutoff > 0.0) || !(skin >= 0.0))
+      !(cutoff > 0.0) || !(skin >= 0.0) || !(prune_skin >= 0.0))
     return TSB_ERR_INVALID_ARG;
+  const double prune = prune_skin < skin ? prune_skin : 0.0;
   Carver c(workspace, workspace_bytes);
   VlWork w;
   carve_vl(c, w, n_atoms, n_systems);
@@ -855,10 +1010,10 @@ extern "C" int tsb_vlist_check(const void *positions, const void *cell_row,
   cudaStream_t st = (cudaStream_t)stream;
   if (dtype == TSB_F64)
     return vl_check<double>((const double *)positions, (const double *)cell_row, system_idx,
-                            sys_active, n_atoms, n_systems, cutoff, skin, flags, w, st);
+                            sys_active, n_atoms, n_systems, cutoff, skin, prune, flags, w, st);
   if (dtype == TSB_F32)
     return vl_check<float>((const float *)positions, (const float *)cell_row, system_idx,
-                           sys_active, n_atoms, n_systems, cutoff, skin, flags, w, st);
+                           sys_active, n_atoms, n_systems, cutoff, skin, prune, flags, w, st);
   return TSB_ERR_INVALID_ARG;
 }
 
@@ -889,16 +1044,17 @@ extern "C" int tsb_vlist_build(const void *positions, const void *cell_row, cons
 }
 
 extern "C" int tsb_vlist_forces(int potential, const double *table, int n_species,
-                                const int32_t *species, const uint32_t *list,
+                                const int32_t *species, uint32_t *list,
                                 const int32_t *counts, const void *positions,
                                 const void *cell_row, const int64_t *system_idx,
                                 const uint8_t *sys_active, int64_t n_atoms, int64_t n_systems,
-                                int dtype, double cutoff, int out_flags, void *energy,
+                                int dtype, double cutoff, double prune_skin, int out_flags,
+                                void *energy,
                                 void *forces, void *stress, void *energies, void *stresses,
                                 void *workspace, size_t workspace_bytes, void *stream) {
   if (potential < TSB_POT_LJ || potential > TSB_POT_SOFT || n_species < 1 ||
       n_species > kMaxSpecies || !table || n_atoms < 1 || n_systems < 1 || !list || !counts ||
-      !positions || !cell_row || !system_idx || !energy)
+      !positions || !cell_row || !system_idx || !energy || !(prune_skin >= 0.0))
     return TSB_ERR_INVALID_ARG;
   if (n_species > 1 && !species) return TSB_ERR_INVALID_ARG;
   if (((out_flags & TSB_OUT_FORCES) && !forces) || ((out_flags & TSB_OUT_STRESS) && !stress) ||
@@ -913,13 +1069,14 @@ extern "C" int tsb_vlist_forces(int potential, const double *table, int n_specie
   if (dtype == TSB_F64)
     return vl_forces<double>(potential, table, n_species, species, list, counts,
                              (const double *)positions, (const double *)cell_row, system_idx,
-                             sys_active, n_atoms, n_systems, cutoff, out_flags,
+                             sys_active, n_atoms, n_systems, cutoff, prune_skin, out_flags,
                              (double *)energy, (double *)forces, (double *)stress,
                              (double *)energies, (double *)stresses, w, st);
   if (dtype == TSB_F32)
     return vl_forces<float>(potential, table, n_species, species, list, counts,
                             (const float *)positions, (const float *)cell_row, system_idx,
-                            sys_active, n_atoms, n_systems, cutoff, out_flags, (float *)energy,
+                            sys_active, n_atoms, n_systems, cutoff, prune_skin, out_flags,
+                            (float *)energy,
                             (float *)forces, (float *)stress, (float *)energies,
                             (float *)stresses, w, st);
   return TSB_ERR_INVALID_ARG;

@@ -88,15 +88,15 @@ PROTOTYPES = {
                                    _vp, _vp, _vp, _vp, _sz, _vp]),
     "tsb_vlist_workspace_size": (_sz, [_i64, _i64]),
     "tsb_vlist_reset": (_int, [_i64, _i64, _vp, _sz, _vp]),
-    "tsb_vlist_check": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _int, _dbl, _dbl, _vp, _vp, _sz,
-                               _vp]),
+    "tsb_vlist_check": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _int, _dbl, _dbl, _dbl, _vp, _vp,
+                               _sz, _vp]),
     "tsb_vlist_build": (_int, [_vp, _vp, _vp, _vp, _vp, _i64, _i64, _int, _dbl, _dbl, _vp, _vp,
                                _int, _i64, _vp, _vp, _sz, _vp]),
     "tsb_vlist_hvp_scratch_size": (_sz, [_i64, _int]),
     "tsb_vlist_lj_hvp": (_int, [_vp, _int, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _dbl, _vp,
                                 _dbl, _vp, _vp, _vp, _sz, _vp, _sz, _vp]),
     "tsb_vlist_forces": (_int, [_int, _vp, _int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64,
-                                _int, _dbl, _int, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
+                                _int, _dbl, _dbl, _int, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
     "tsb_fire_workspace_size": (_sz, [_i64]),
     "tsb_fire_ase_pre": (_int, _FIRE_ARGS),
     "tsb_fire_vv_pre": (_int, _FIRE_ARGS),

@@ -182,8 +182,8 @@ class _ListForces:
         P, st = self.P, L.stream_ptr(q.device)
         n, ns = P.n_atoms, P.n_systems
         L.call("tsb_vlist_check", L.ptr(q), L.ptr(P.cell_row), L.ptr(P.system_idx), None, n, ns,
-               L.F64, P.cutoff, self.skin, L.ptr(self.flags), L.ptr(self.ws), self.ws.numel(),
-               st)
+               L.F64, P.cutoff, self.skin, 0.0, L.ptr(self.flags), L.ptr(self.ws),
+               self.ws.numel(), st)
         L.call("tsb_vlist_build", L.ptr(q), L.ptr(P.cell_row), L.ptr(P.pbc),
                L.ptr(P.system_idx), L.ptr(P.species), n, ns, L.F64, P.cutoff, self.skin,
                L.ptr(self.list), L.ptr(self.counts), self.cap, P.max_sys, L.ptr(self.flags),
@@ -197,7 +197,7 @@ class _ListForces:
         f = torch.empty((n, 3), dtype=torch.float64, device=q.device)
         L.call("tsb_vlist_forces", L.POT_LJ, L.ptr(table), P.n_species, L.ptr(P.species),
                L.ptr(self.list), L.ptr(self.counts), L.ptr(q), L.ptr(P.cell_row),
-               L.ptr(P.system_idx), None, n, ns, L.F64, P.cutoff,
+               L.ptr(P.system_idx), None, n, ns, L.F64, P.cutoff, 0.0,
                L.OUT_FORCES | L.MATH_FP64, L.ptr(self.e), L.ptr(f), None, None, None,
                L.ptr(self.ws), self.ws.numel(), st)
         return self.e, f

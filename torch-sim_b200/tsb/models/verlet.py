@@ -32,7 +32,17 @@ from .pair_potential import PairTableModel
 
 
 class VerletListModel(ModelInterface):
-    def __init__(self, model: PairTableModel, *, skin: float = 1.0, max_neighbors: int = 0):
+    def __init__(self, model: PairTableModel, *, skin: float = 1.0, max_neighbors: int = 0,
+                 prune: float | None = None):
+        """``prune`` (Angstrom, batched lists only): between rebuilds each atom
+        evaluates only the list entries that were within its pair cutoff +
+        ``prune`` at the system's last pruning; a system is pruned again when its
+        atoms' drift or its cell's deformation could bring a left-out pair inside
+        the cutoff.  Results equal those of the whole list to FP64 rounding.
+        Default 0 (off): on the FIRE + Frechet relax workload the non-affine
+        steps use up the drift allowance within a few steps and the re-prunings
+        cost more than the shorter lists save (0.54 against 0.47 ms per step
+        with 0.2 to 0.45 A)."""
         super().__init__()
         if not isinstance(model, PairTableModel):
             raise TypeError("VerletListModel wraps a tsb PairTableModel")
@@ -44,6 +54,11 @@ class VerletListModel(ModelInterface):
         self.per_atom_energies = getattr(model, "per_atom_energies", False)
         self.per_atom_stresses = getattr(model, "per_atom_stresses", False)
         self.skin = float(skin)
+        self.prune = 0.0 if prune is None else float(prune)
+        if not (0.0 <= self.prune):
+            raise ValueError("prune must be >= 0")
+        if self.prune >= self.skin:
+            self.prune = 0.0  # the whole list is within cutoff + skin anyway
         self.max_neighbors = int(max_neighbors)
         self.n_builds = 0
         self._key = None
@@ -116,7 +131,7 @@ class VerletListModel(ModelInterface):
             if self.sticky is None or self.sticky.device != dev:
                 self.sticky = torch.zeros(1, dtype=torch.int32, device=dev)
             torch.ops.tsb.vlist_check_(pos, cell_row, sysi, active, ns, cutoff, self.skin,
-                                       self.flags, self.ws)
+                                       self.prune, self.flags, self.ws)
             torch.ops.tsb.vlist_build_(pos, cell_row, pbc, sysi, species, ns, cutoff, self.skin,
                                        self.list, self.counts, self.cap, self.max_system_atoms,
                                        self.flags, self.ws)
@@ -124,7 +139,7 @@ class VerletListModel(ModelInterface):
             return
         while True:
             torch.ops.tsb.vlist_check_(pos, cell_row, sysi, active, ns, cutoff, self.skin,
-                                       self.flags, self.ws)
+                                       self.prune, self.flags, self.ws)
             if not int(self.flags[0].item()):
                 return
             torch.ops.tsb.vlist_build_(pos, cell_row, pbc, sysi, species, ns, cutoff, self.skin,
@@ -169,8 +184,8 @@ class VerletListModel(ModelInterface):
         if m.precision == "fp64":
             flags |= L.MATH_FP64
         torch.ops.tsb.vlist_forces_(m.kind, table, m.n_species, species, self.list, self.counts,
-                                    pos, cell_row, sysi, active, n_sys, m.cutoff, flags, energy,
-                                    forces, stress, energies, stresses, self.ws)
+                                    pos, cell_row, sysi, active, n_sys, m.cutoff, self.prune,
+                                    flags, energy, forces, stress, energies, stresses, self.ws)
 
     # ------------------------------------------------- one large system
     def _single_ok(self, state):

@@ -275,16 +275,17 @@ _define("fire_converged_(Tensor forces, Tensor system_idx, int n_systems, Tensor
 
 
 # ---------------------------------------------------------------- Verlet lists
-def _vlist_check(positions, cell_row, system_idx, sys_active, n_systems, cutoff, skin, flags,
-                 workspace):
+def _vlist_check(positions, cell_row, system_idx, sys_active, n_systems, cutoff, skin, prune,
+                 flags, workspace):
     L.call("tsb_vlist_check", _P(positions), _P(cell_row), _P(system_idx), _P(sys_active),
            positions.shape[0], int(n_systems), L.dtype_code(positions.dtype), float(cutoff),
-           float(skin), _P(flags), _P(workspace), workspace.numel(), _stream(positions))
+           float(skin), float(prune), _P(flags), _P(workspace), workspace.numel(),
+           _stream(positions))
 
 
 _define("vlist_check_(Tensor positions, Tensor cell_row, Tensor system_idx, Tensor? sys_active, "
-        "int n_systems, float cutoff, float skin, Tensor(a!) flags, Tensor(b!) workspace) -> ()",
-        _vlist_check, _noop)
+        "int n_systems, float cutoff, float skin, float prune, Tensor(a!) flags, "
+        "Tensor(b!) workspace) -> ()", _vlist_check, _noop)
 
 
 def _vlist_build(positions, cell_row, pbc, system_idx, species, n_systems, cutoff, skin, lst,
@@ -303,21 +304,23 @@ _define("vlist_build_(Tensor positions, Tensor cell_row, Tensor pbc, Tensor syst
 
 
 def _vlist_forces(kind, table, n_species, species, lst, counts, positions, cell_row,
-                  system_idx, sys_active, n_systems, cutoff, flags, energy, forces, stress,
-                  energies, stresses, workspace):
+                  system_idx, sys_active, n_systems, cutoff, prune, flags, energy, forces,
+                  stress, energies, stresses, workspace):
     nz = lambda t: _P(t) if (t is not None and t.numel()) else None  # noqa: E731
     L.call("tsb_vlist_forces", int(kind), _P(table), int(n_species), _P(species), _P(lst),
            _P(counts), _P(positions), _P(cell_row), _P(system_idx), _P(sys_active),
            positions.shape[0], int(n_systems), L.dtype_code(positions.dtype), float(cutoff),
-           int(flags), _P(energy), nz(forces), nz(stress), nz(energies), nz(stresses),
-           _P(workspace), workspace.numel(), _stream(positions))
+           float(prune), int(flags), _P(energy), nz(forces), nz(stress), nz(energies),
+           nz(stresses), _P(workspace), workspace.numel(), _stream(positions))
 
 
-_define("vlist_forces_(int kind, Tensor table, int n_species, Tensor? species, Tensor nlist, "
-        "Tensor counts, Tensor positions, Tensor cell_row, Tensor system_idx, "
-        "Tensor? sys_active, int n_systems, float cutoff, int flags, Tensor(a!) energy, "
-        "Tensor(b!)? forces, Tensor(c!)? stress, Tensor(d!)? energies, Tensor(e!)? stresses, "
-        "Tensor(f!) workspace) -> ()", _vlist_forces, _noop)
+# with prune > 0 the lists are reordered in place (front parts), so nlist is written
+_define("vlist_forces_(int kind, Tensor table, int n_species, Tensor? species, "
+        "Tensor(g!) nlist, Tensor counts, Tensor positions, Tensor cell_row, "
+        "Tensor system_idx, Tensor? sys_active, int n_systems, float cutoff, float prune, "
+        "int flags, Tensor(a!) energy, Tensor(b!)? forces, Tensor(c!)? stress, "
+        "Tensor(d!)? energies, Tensor(e!)? stresses, Tensor(f!) workspace) -> ()",
+        _vlist_forces, _noop)
 
 
 OPS = ("nl_build", "pair_forward", "pair_forward_into_", "md_kick_", "md_drift_",
