@@ -406,8 +406,10 @@ def run_relax(args):
                        "graph_steps_per_replay": args.graph_steps,
                        "time_to_all_converged_s": t, "fmax": 1e-3,
                        "neighbour_lists": (
-                           f"Verlet, skin {args.list_skin} A, pruned to cutoff + "
-                           f"{getattr(m, 'prune', 0.0):.3g} A, expired systems rebuilt "
+                           f"Verlet, skin {args.list_skin} A, "
+                           + (f"pruned to cutoff + {m.prune:.3g} A, "
+                              if getattr(m, "prune", 0.0) > 0 else "not pruned, ")
+                           + "expired systems rebuilt "
                            + ("on the device inside the graph (not counted on the host)"
                               if args.graph_steps > 0
                               else f"by host decision ({m.n_builds} builds)")
