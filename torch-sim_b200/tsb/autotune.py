@@ -123,8 +123,11 @@ def tune_fused_skin(state, model, *, integrator: str = "nvt_langevin", dt, kT=No
                     force: bool = False, timer=_time_launch) -> float:
     """Verlet skin for ``FusedMD`` on this workload (cached; see module doc).
 
-    Each candidate runs the fused kernel on a sample of the batch (two systems
-    per SM by default, spread over the batch) from the same starting point:
+    Each candidate runs the fused kernel on a sample of the batch (sixteen
+    systems per SM by default, spread over the batch: the whole batch up to
+    2,368 systems on a B200; with only a few systems per SM the launch time is
+    that of the SMs holding the largest systems and the ranking is noisy) from
+    the same starting point:
     ``n_steps`` steps of warm-up (the atoms leave their starting positions and
     the list rebuild rate settles), then ``n_steps`` timed steps.
     """
@@ -143,7 +146,7 @@ def tune_fused_skin(state, model, *, integrator: str = "nvt_langevin", dt, kT=No
     if sample_systems is None:
         n_sm = (torch.cuda.get_device_properties(dev).multi_processor_count
                 if dev.type == "cuda" else 1)
-        sample_systems = 2 * n_sm
+        sample_systems = 16 * n_sm
     idx = spread_sample(state.n_systems, sample_systems)
     sample = select_systems(state, idx) if len(idx) < state.n_systems else state
 
@@ -173,7 +176,7 @@ def _sample(state, sample_systems):
     if sample_systems is None:
         n_sm = (torch.cuda.get_device_properties(dev).multi_processor_count
                 if dev.type == "cuda" else 1)
-        sample_systems = 2 * n_sm
+        sample_systems = 16 * n_sm
     idx = spread_sample(state.n_systems, sample_systems)
     sample = select_systems(state, idx) if len(idx) < state.n_systems else state
 
