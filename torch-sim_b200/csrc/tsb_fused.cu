@@ -484,8 +484,11 @@ __device__ __forceinline__ float2 pair_fr2(const Prm2 &k, const PairPrm<float> &
   }
 }
 
-template <int POT, bool MULTI, int NT>
+template <int POT, bool MULTI, int NT, int INTEG>
 __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(FusedArgs A) {
+  // the integrator: fixed at compile time for the common single-species
+  // Langevin launches (the other integrators' code is then left out), else read
+  const int integ = INTEG >= 0 ? INTEG : A.integrator;
   // the block shape's table sizes (these names shadow nothing at namespace scope)
   constexpr int kFusedThreads = NT;
   constexpr int kListLen = FusedShape<NT>::kListLen;
@@ -590,12 +593,12 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
       g.skin = A.skin;
       g.dt = A.dt[s];
       g.half = g.dt / 2.0;
-      g.c1 = (A.integrator == TSB_INT_LANGEVIN) ? exp(-(A.gamma[s] * g.dt)) : 1.0;
-      if (A.integrator == TSB_INT_NOSE_HOOVER || A.integrator == TSB_INT_VRESCALE) {
+      g.c1 = (integ == TSB_INT_LANGEVIN) ? exp(-(A.gamma[s] * g.dt)) : 1.0;
+      if (integ == TSB_INT_NOSE_HOOVER || integ == TSB_INT_VRESCALE) {
         g.nf = 3.0 * (double)g.n - 3.0;  // COM motion removed (nvt.py:287-290)
         g.kt = A.kT[s];
         g.tau = A.tau[s];
-        if (A.integrator == TSB_INT_NOSE_HOOVER) {
+        if (integ == TSB_INT_NOSE_HOOVER) {
           g.cdt = A.cdt[s];
           g.cke = A.cke[s];
           for (int j = 0; j < A.M; ++j) {
@@ -648,7 +651,7 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
       const double mass = A.m[gi];
       inv_m = 1.0 / mass;
       sp = A.species ? min(max(A.species[gi], 0), A.n_species - 1) : 0;
-      if (A.integrator == TSB_INT_LANGEVIN)
+      if (integ == TSB_INT_LANGEVIN)
         c2m = sqrt(A.kT[s] * (1.0 - exp(-2.0 * (A.gamma[s] * A.dt[s])))) * sqrt(mass);
     }
     int Wx = 0, Wy = 0, Wz = 0;        // integer wrap of the owned atom at the last build
@@ -1183,7 +1186,7 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
       // thermostat before the step: V-rescale factor from the current kinetic
       // energy (nvt.py:715-741), or the first Nose-Hoover half step with the
       // kinetic energy carried from the last one (nvt.py:462-470)
-      if (A.integrator == TSB_INT_VRESCALE) {
+      if (integ == TSB_INT_VRESCALE) {
         const double k2 = block_sum_to0<NT>(lead ? (px * px + py * py + pz * pz) * inv_m : 0.0,
                                         s_red);
         if (tid == 0)
@@ -1194,7 +1197,7 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
         px *= sc;
         py *= sc;
         pz *= sc;
-      } else if (A.integrator == TSB_INT_NOSE_HOOVER) {
+      } else if (integ == TSB_INT_NOSE_HOOVER) {
         if (tid == 0)
           g.th_scale = nhc_half(g.cdt, A.M, A.nc, A.nsy, g.cq, g.cx, g.cv, g.cke, g.nf, g.kt);
         __syncthreads();
@@ -1207,7 +1210,7 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
         px += F0 * half;
         py += F1 * half;
         pz += F2 * half;
-        if (A.integrator == TSB_INT_LANGEVIN) {
+        if (integ == TSB_INT_LANGEVIN) {
           x0 += (px * inv_m) * half;
           x1 += (py * inv_m) * half;
           x2 += (pz * inv_m) * half;
@@ -1286,7 +1289,7 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
         py += F1 * g.half;
         pz += F2 * g.half;
       }
-      if (A.integrator == TSB_INT_NOSE_HOOVER) {
+      if (integ == TSB_INT_NOSE_HOOVER) {
         // second half step with the kinetic energy after velocity Verlet
         const double k2 = block_sum_to0<NT>(lead ? (px * px + py * py + pz * pz) * inv_m : 0.0,
                                         s_red);
@@ -1357,7 +1360,7 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
         o[1] = o[3] = w[5] * iv;
       }
       if (A.n_rebuilds) A.n_rebuilds[s] = rebuilds;
-      if (A.integrator == TSB_INT_NOSE_HOOVER) {
+      if (integ == TSB_INT_NOSE_HOOVER) {
         for (int j = 0; j < A.M; ++j) {
           A.cxi[s * A.M + j] = g.cx[j];
           A.cpxi[s * A.M + j] = g.cv[j];
@@ -1406,22 +1409,25 @@ __global__ void k_bounds_fused(const int64_t *sys, int64_t n, int64_t n_sys, int
   if (i == n - 1 || sys[i + 1] != s) hi[s] = i + 1;
 }
 
-template <int POT, bool MULTI, int NT>
+template <int POT, bool MULTI, int NT, int INTEG = -1>
 static void launch_fused(const FusedArgs &A, int64_t grid, cudaStream_t st) {
-  cudaFuncSetAttribute(k_fused_md<POT, MULTI, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)FusedSmem<NT>::kTotal);
-  k_fused_md<POT, MULTI, NT><<<(unsigned)grid, NT, FusedSmem<NT>::kTotal, st>>>(A);
+  cudaFuncSetAttribute(k_fused_md<POT, MULTI, NT, INTEG>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FusedSmem<NT>::kTotal);
+  k_fused_md<POT, MULTI, NT, INTEG><<<(unsigned)grid, NT, FusedSmem<NT>::kTotal, st>>>(A);
 }
 
 template <int NT>
 static void launch_shape(const FusedArgs &A, int64_t grid, cudaStream_t st) {
   const bool multi = A.n_species > 1;
+  const bool lgv = A.integrator == TSB_INT_LANGEVIN;
   if (A.potential == TSB_POT_LJ) {
-    multi ? launch_fused<TSB_POT_LJ, true, NT>(A, grid, st)
-          : launch_fused<TSB_POT_LJ, false, NT>(A, grid, st);
+    if (multi) launch_fused<TSB_POT_LJ, true, NT>(A, grid, st);
+    else if (lgv) launch_fused<TSB_POT_LJ, false, NT, TSB_INT_LANGEVIN>(A, grid, st);
+    else launch_fused<TSB_POT_LJ, false, NT>(A, grid, st);
   } else if (A.potential == TSB_POT_MORSE) {
-    multi ? launch_fused<TSB_POT_MORSE, true, NT>(A, grid, st)
-          : launch_fused<TSB_POT_MORSE, false, NT>(A, grid, st);
+    if (multi) launch_fused<TSB_POT_MORSE, true, NT>(A, grid, st);
+    else if (lgv) launch_fused<TSB_POT_MORSE, false, NT, TSB_INT_LANGEVIN>(A, grid, st);
+    else launch_fused<TSB_POT_MORSE, false, NT>(A, grid, st);
   } else {
     multi ? launch_fused<TSB_POT_SOFT, true, NT>(A, grid, st)
           : launch_fused<TSB_POT_SOFT, false, NT>(A, grid, st);
