@@ -1257,7 +1257,7 @@ __global__ void __launch_bounds__(NT, FusedShape<NT>::kMinBlocks) k_fused_md(Fus
         Y[3 * a + 2] = y2;
       }
       for (int e = tid; e < n_ext; e += kFusedThreads) {
-        const int sp_e = __float_as_int(s_ext[e].w);
+        const int sp_e = MULTI ? __float_as_int(s_ext[e].w) : 0;
         int owner, sx, sy, sz;
         unpack_ghost(s_gshift[e], owner, sx, sy, sz);
         s_ext[e] = image_of(g, s_posd[3 * owner], s_posd[3 * owner + 1],
