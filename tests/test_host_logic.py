@@ -212,3 +212,44 @@ def test_histogram_window_drops_only_negligible_terms():
     dropped = np.where((kk < k0[:, None]) | (kk > k1[:, None]), g, 0.0)
     assert dropped.max() <= np.exp(-72.0)
     np.testing.assert_allclose(win, full, rtol=1e-15, atol=1e-28)
+
+
+def test_verlet_list_prune_argument():
+    """VerletListModel's list pruning: off unless asked for, and a pruning skin
+    at or above the list skin (the whole list is within reach) turns it off."""
+    import pytest
+
+    from tsb import models
+
+    m = models.MorseModel(sigma=2.866, epsilon=0.3429, alpha=1.3588, cutoff=6.0, device="cpu")
+    assert models.VerletListModel(m, skin=1.5).prune == 0.0
+    assert models.VerletListModel(m, skin=1.5, prune=0.3).prune == 0.3
+    assert models.VerletListModel(m, skin=1.0, prune=1.2).prune == 0.0
+    with pytest.raises(ValueError):
+        models.VerletListModel(m, skin=1.0, prune=-0.1)
+
+
+def test_narrow_routing_uses_image_estimate():
+    """Systems of at most 256 atoms whose estimated atoms + images fit 95 % of
+    the narrow table take the two-per-SM blocks, largest first after the wide
+    ones; a thin cell (many images) stays wide."""
+    from tsb import integrators, workloads
+    from tsb.state import state_from_arrays
+
+    d = workloads.copper_batch(64, 8, 512, seed=3)
+    st = state_from_arrays(d, device="cpu")
+    order, n_wide = integrators._split_order(st, 6.0, 1.2)
+    counts = np.bincount(d["system_idx"])
+    order = order.numpy()
+    wide, narrow = order[:n_wide], order[n_wide:]
+    assert (counts[narrow] <= integrators.NARROW_MAX_ATOMS).all()
+    assert (counts[wide] > integrators.NARROW_MAX_ATOMS).sum() == \
+        (counts > integrators.NARROW_MAX_ATOMS).sum()
+    # each group largest first
+    assert (np.diff(counts[narrow]) <= 0).all() and (np.diff(counts[wide]) <= 0).all()
+    # the estimate: n * prod(1 + 2 R |b_k|) <= 0.95 * table for every narrow system
+    R = 7.2
+    for s in narrow:
+        cr = np.asarray(d["cell"][s]).T
+        h = R * np.linalg.norm(np.linalg.inv(cr).T, axis=1)
+        assert counts[s] * np.prod(1 + 2 * h) <= 0.95 * integrators.NARROW_MAX_IMAGES + 1e-9
